@@ -1,0 +1,115 @@
+"""ctypes binding of ``libartefact_b200.so`` (the C ABI in include/artefact_b200.h).
+
+The library is the only compute path: importing this module raises if it is
+missing, and every solver call goes to the CUDA kernels it contains.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+from pathlib import Path
+
+LIB_PATH = Path(__file__).resolve().parent / "libartefact_b200.so"
+
+ART_OK = 0
+ART_ERR_INVALID_ARGUMENT = -1
+ART_ERR_INVALID_DATA = -2
+ART_ERR_CUDA = -3
+ART_ERR_DECODE = -4
+ART_ERR_UNSUPPORTED = -5
+
+ART_COEF_F32 = 0
+ART_COEF_I16 = 1
+ART_INIT_DECODED = 0
+ART_INIT_SCALAR_COMPAT = 1
+
+
+class ArtChannel(C.Structure):
+    _fields_ = [
+        ("rounded_px_w", C.c_uint32),
+        ("rounded_px_h", C.c_uint32),
+        ("block_w", C.c_uint32),
+        ("block_h", C.c_uint32),
+        ("samp_h", C.c_uint32),
+        ("samp_v", C.c_uint32),
+        ("coef_type", C.c_uint32),
+        ("reserved", C.c_uint32),
+        ("dct_coefs", C.c_void_p),
+        ("quant_table", C.POINTER(C.c_float)),
+    ]
+
+
+class ArtOptions(C.Structure):
+    _fields_ = [
+        ("init_mode", C.c_uint32),
+        ("device", C.c_int32),
+        ("reserved", C.c_uint32 * 6),
+    ]
+
+
+class ArtError(RuntimeError):
+    """Raised when a C ABI call returns a negative status."""
+
+    def __init__(self, code: int, message: str):
+        super().__init__(f"[{code}] {message}")
+        self.code = code
+        self.message = message
+
+
+EXPORTS = {
+    "art_last_error": (C.c_char_p, []),
+    "art_version": (C.c_char_p, []),
+    "art_compute": (C.c_int32, [C.c_uint32, C.POINTER(ArtChannel), C.c_float, C.POINTER(C.c_float), C.c_uint32,
+                                C.c_uint32, C.c_uint32, C.c_uint64, C.POINTER(C.c_void_p), C.POINTER(ArtOptions)]),
+    "art_context_create": (C.c_int32, [C.c_int32, C.POINTER(C.c_void_p)]),
+    "art_context_destroy": (None, [C.c_void_p]),
+    "art_context_compute": (C.c_int32, [C.c_void_p, C.c_uint32, C.POINTER(ArtChannel), C.c_float,
+                                        C.POINTER(C.c_float), C.c_uint32, C.c_uint32, C.c_uint32,
+                                        C.POINTER(C.c_void_p), C.POINTER(ArtOptions)]),
+    "art_context_compute_device": (C.c_int32, [C.c_void_p, C.c_uint32, C.POINTER(ArtChannel), C.c_float,
+                                               C.POINTER(C.c_float), C.c_uint32, C.c_uint32, C.c_uint32,
+                                               C.POINTER(C.c_void_p), C.c_uint32, C.POINTER(ArtOptions),
+                                               C.c_void_p]),
+    "art_context_process": (C.c_int32, [C.c_void_p, C.c_uint32, C.POINTER(ArtChannel), C.POINTER(C.c_float),
+                                        C.POINTER(C.c_float), C.POINTER(C.c_uint32), C.c_int32, C.c_uint32,
+                                        C.c_uint32, C.c_void_p, C.POINTER(ArtOptions)]),
+    "art_context_synchronize": (C.c_int32, [C.c_void_p]),
+    "art_context_set_timing": (C.c_int32, [C.c_void_p, C.c_int32]),
+    "art_context_last_timing": (C.c_int32, [C.c_void_p, C.POINTER(C.c_float), C.POINTER(C.c_float),
+                                            C.POINTER(C.c_float), C.POINTER(C.c_uint32)]),
+    "art_jpeg_decode": (C.c_int32, [C.c_char_p, C.c_size_t, C.POINTER(C.c_void_p)]),
+    "art_jpeg_free": (None, [C.c_void_p]),
+    "art_jpeg_info": (C.c_int32, [C.c_void_p, C.POINTER(C.c_uint32), C.POINTER(C.c_uint32),
+                                  C.POINTER(C.c_uint32)]),
+    "art_jpeg_channel": (C.c_int32, [C.c_void_p, C.c_uint32, C.POINTER(ArtChannel)]),
+}
+
+_lib = None
+
+
+def lib() -> C.CDLL:
+    """Load the native library (building it first when ART_AUTOBUILD=1)."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if os.environ.get("ART_AUTOBUILD") == "1":
+        from . import build as _build
+
+        _build.build()
+    if not LIB_PATH.exists():
+        raise ImportError(
+            f"{LIB_PATH} is missing: build it with `python -m artefact_b200.build` "
+            "(there is no CPU fallback for the solver)")
+    handle = C.CDLL(str(LIB_PATH))
+    for name, (res, args) in EXPORTS.items():
+        fn = getattr(handle, name)
+        fn.restype = res
+        fn.argtypes = args
+    _lib = handle
+    return handle
+
+
+def check(rc: int) -> None:
+    if rc != ART_OK:
+        msg = lib().art_last_error().decode("utf-8", "replace")
+        raise ArtError(rc, msg)

@@ -1,0 +1,285 @@
+"""Host-side mirror of artefact-lib's public API, backed by the CUDA library.
+
+Names, argument meanings and error behaviour follow Delnegend/artefact
+``backend/artefact-lib`` (citations are file:line there):
+
+* :func:`compute` is ``pipeline_scalar::compute`` (pipeline_scalar/mod.rs:17-78),
+* :class:`Coefficient` / :class:`Jpeg` / :class:`JpegSource` are jpeg/mod.rs:8-42,
+* :class:`ValueCollection` and :class:`Artefact` are lib.rs:34-212.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import threading
+from dataclasses import dataclass, field
+from typing import Generic, List, Optional, Sequence, TypeVar, Union
+
+import numpy as np
+
+from . import _native as N
+
+T = TypeVar("T")
+
+
+@dataclass
+class Coefficient:
+    """One JPEG component as the solver receives it (jpeg/mod.rs:8-27)."""
+
+    rounded_px_w: int
+    rounded_px_h: int
+    block_w: int
+    block_h: int
+    horizontal_samp_factor: int
+    vertical_samp_factor: int
+    dct_coefs: np.ndarray  # block_w*block_h*64 values (float32 or int16), block raster, natural order
+    quant_table: np.ndarray  # 64 float32, natural order
+
+    @property
+    def rounded_px_count(self) -> int:
+        return self.rounded_px_w * self.rounded_px_h
+
+    @property
+    def block_count(self) -> int:
+        return self.block_w * self.block_h
+
+    def as_c(self, keep: list) -> N.ArtChannel:
+        coefs = self.dct_coefs
+        if coefs.dtype == np.int16:
+            ctype = N.ART_COEF_I16
+        else:
+            coefs = coefs.astype(np.float32, copy=False)
+            ctype = N.ART_COEF_F32
+        coefs = np.ascontiguousarray(coefs)
+        if coefs.size != self.block_count * 64:
+            raise ValueError("Invalid coef's image data length")
+        q = np.ascontiguousarray(self.quant_table, dtype=np.float32)
+        if q.size != 64:
+            raise ValueError("Invalid quant_table length")
+        keep.extend([coefs, q])
+        ch = N.ArtChannel()
+        ch.rounded_px_w, ch.rounded_px_h = self.rounded_px_w, self.rounded_px_h
+        ch.block_w, ch.block_h = self.block_w, self.block_h
+        ch.samp_h, ch.samp_v = self.horizontal_samp_factor, self.vertical_samp_factor
+        ch.coef_type = ctype
+        ch.dct_coefs = coefs.ctypes.data
+        ch.quant_table = q.ctypes.data_as(C.POINTER(C.c_float))
+        return ch
+
+
+@dataclass
+class JpegSource:
+    """``JpegSource::File(path)`` or ``JpegSource::Buffer(bytes)`` (jpeg/mod.rs:38-42)."""
+
+    path: Optional[str] = None
+    buffer: Optional[bytes] = None
+
+    @staticmethod
+    def File(path: str) -> "JpegSource":  # noqa: N802 - mirrors the Rust enum variant
+        return JpegSource(path=str(path))
+
+    @staticmethod
+    def Buffer(data: bytes) -> "JpegSource":  # noqa: N802
+        return JpegSource(buffer=bytes(data))
+
+    def read(self) -> bytes:
+        if self.buffer is not None:
+            return self.buffer
+        try:
+            with open(self.path, "rb") as fh:
+                return fh.read()
+        except OSError as e:
+            raise ArtefactError(f"Failed to read JPEG file '{self.path}': {e}") from e
+
+
+@dataclass
+class Jpeg:
+    """Decoded coefficient data of a JPEG (jpeg/mod.rs:29-36, jpeg/zune.rs:5-55)."""
+
+    nchannel: int
+    real_px_w: int
+    real_px_h: int
+    coefs: List[Coefficient] = field(default_factory=list)
+
+    @staticmethod
+    def from_source(source: JpegSource) -> "Jpeg":
+        data = source.read()
+        lib = N.lib()
+        handle = C.c_void_p()
+        rc = lib.art_jpeg_decode(data, len(data), C.byref(handle))
+        if rc != N.ART_OK:
+            raise ArtefactError(lib.art_last_error().decode("utf-8", "replace"))
+        try:
+            nch, rw, rh = C.c_uint32(), C.c_uint32(), C.c_uint32()
+            N.check(lib.art_jpeg_info(handle, C.byref(nch), C.byref(rw), C.byref(rh)))
+            coefs = []
+            for c in range(nch.value):
+                ch = N.ArtChannel()
+                N.check(lib.art_jpeg_channel(handle, c, C.byref(ch)))
+                n = ch.block_w * ch.block_h * 64
+                arr = np.ctypeslib.as_array(C.cast(ch.dct_coefs, C.POINTER(C.c_int16)), shape=(n,)).copy()
+                q = np.ctypeslib.as_array(ch.quant_table, shape=(64,)).copy()
+                coefs.append(Coefficient(ch.rounded_px_w, ch.rounded_px_h, ch.block_w, ch.block_h,
+                                         ch.samp_h, ch.samp_v, arr, q))
+            return Jpeg(nch.value, rw.value, rh.value, coefs)
+        finally:
+            lib.art_jpeg_free(handle)
+
+    def max_rounded(self):
+        """Largest rounded component size (lib.rs:108-116)."""
+        w = max(c.rounded_px_w for c in self.coefs)
+        h = max(c.rounded_px_h for c in self.coefs)
+        return w, h, w * h
+
+
+class ArtefactError(RuntimeError):
+    """Error of :meth:`Artefact.process` (the reference's ``Err(String)``)."""
+
+
+def _options(init_mode: int, device: int) -> N.ArtOptions:
+    o = N.ArtOptions()
+    o.init_mode = init_mode
+    o.device = device
+    return o
+
+
+def compute(nchannel: int, coefs: Sequence[Coefficient], weight: float, pweight: Sequence[float], iterations: int,
+            max_rounded_px_w: int, max_rounded_px_h: int, max_rounded_px_count: int, *,
+            init_mode: int = N.ART_INIT_DECODED, device: int = -1) -> List[np.ndarray]:
+    """Run the solver; the B200 replacement of ``pipeline_scalar::compute``.
+
+    Returns ``nchannel`` float32 planes of ``max_rounded_px_count`` values (row
+    stride ``max_rounded_px_w``), level-shifted like the reference's output.
+    Channel ``c`` uses ``pweight[c]`` (compute_step.rs:19-26).
+    """
+    lib = N.lib()
+    keep: list = []
+    chans = (N.ArtChannel * nchannel)(*[coefs[c].as_c(keep) for c in range(nchannel)])
+    pw = (C.c_float * 3)(*[float(v) for v in list(pweight)[:3]] + [0.0] * (3 - min(3, len(pweight))))
+    outs = [np.empty(max_rounded_px_count, dtype=np.float32) for _ in range(nchannel)]
+    ptrs = (C.c_void_p * nchannel)(*[o.ctypes.data for o in outs])
+    opts = _options(init_mode, device)
+    rc = lib.art_compute(nchannel, chans, float(weight), pw, int(iterations), max_rounded_px_w, max_rounded_px_h,
+                         max_rounded_px_count, ptrs, C.byref(opts))
+    N.check(rc)
+    return outs
+
+
+class ValueCollection(Generic[T]):
+    """``ValueCollection::ForAll(v)`` / ``ForEach([a, b, c])`` (lib.rs:34-47)."""
+
+    def __init__(self, values: Sequence[T]):
+        self._values = list(values)
+
+    @staticmethod
+    def ForAll(v: T) -> "ValueCollection[T]":  # noqa: N802
+        return ValueCollection([v, v, v])
+
+    @staticmethod
+    def ForEach(v: Sequence[T]) -> "ValueCollection[T]":  # noqa: N802
+        if len(v) != 3:
+            raise ValueError("ForEach takes exactly three values")
+        return ValueCollection(list(v))
+
+    def to_slice(self) -> List[T]:
+        return list(self._values)
+
+
+_tls = threading.local()
+
+
+def _context(device: int = -1):
+    ctxs = getattr(_tls, "ctxs", None)
+    if ctxs is None:
+        ctxs = _tls.ctxs = {}
+    if device not in ctxs:
+        h = C.c_void_p()
+        N.check(N.lib().art_context_create(device, C.byref(h)))
+        ctxs[device] = h
+    return ctxs[device]
+
+
+class Artefact:
+    """Builder of one restoration run (lib.rs:49-212); defaults 0.3 / 0.001 / 50."""
+
+    def __init__(self):
+        self._weight = ValueCollection.ForAll(0.3)
+        self._pweight = ValueCollection.ForAll(0.001)
+        self._iterations = ValueCollection.ForAll(50)
+        self._separate = False
+        self._benchmark = False
+        self._source: Optional[JpegSource] = None
+        self._init_mode = N.ART_INIT_DECODED
+        self._device = -1
+
+    @staticmethod
+    def default() -> "Artefact":
+        return Artefact()
+
+    def source(self, source: JpegSource) -> "Artefact":
+        self._source = source
+        return self
+
+    def weight(self, v: Union[ValueCollection, float]) -> "Artefact":
+        self._weight = v if isinstance(v, ValueCollection) else ValueCollection.ForAll(float(v))
+        return self
+
+    def pweight(self, v: Union[ValueCollection, float]) -> "Artefact":
+        self._pweight = v if isinstance(v, ValueCollection) else ValueCollection.ForAll(float(v))
+        return self
+
+    def iterations(self, v: Union[ValueCollection, int]) -> "Artefact":
+        self._iterations = v if isinstance(v, ValueCollection) else ValueCollection.ForAll(int(v))
+        return self
+
+    def benchmark(self, v: bool) -> "Artefact":
+        self._benchmark = bool(v)
+        return self
+
+    def separate_components(self, v: bool) -> "Artefact":
+        self._separate = bool(v)
+        return self
+
+    def init_mode(self, mode: int) -> "Artefact":
+        self._init_mode = int(mode)
+        return self
+
+    def device(self, device: int) -> "Artefact":
+        self._device = int(device)
+        return self
+
+    def process(self) -> np.ndarray:
+        """Decode, solve and convert to RGB8 (lib.rs:105-212).
+
+        Returns an ``(real_h, real_w, 3)`` uint8 array. Raises
+        :class:`ArtefactError` on decode errors, and with the message
+        ``"BENCHMARK"`` when benchmark mode is set (lib.rs:155-157).
+        """
+        if self._source is None:
+            raise ArtefactError("Source is not set")
+        try:
+            jpeg = Jpeg.from_source(self._source)
+        except ArtefactError as e:
+            raise ArtefactError(f"Failed to read JPEG: {e}") from e
+        return process_jpeg(jpeg, self._weight.to_slice(), self._pweight.to_slice(), self._iterations.to_slice(),
+                            self._separate, self._benchmark, init_mode=self._init_mode, device=self._device)
+
+
+def process_jpeg(jpeg: Jpeg, weight: Sequence[float], pweight: Sequence[float], iterations: Sequence[int],
+                 separate: bool, benchmark: bool = False, *, init_mode: int = N.ART_INIT_DECODED,
+                 device: int = -1) -> np.ndarray:
+    """Solver dispatch and output stage of ``Artefact::process`` on decoded data."""
+    lib = N.lib()
+    keep: list = []
+    n = jpeg.nchannel
+    chans = (N.ArtChannel * n)(*[c.as_c(keep) for c in jpeg.coefs])
+    w = (C.c_float * 3)(*[float(v) for v in weight])
+    pw = (C.c_float * 3)(*[float(v) for v in pweight])
+    it = (C.c_uint32 * 3)(*[int(v) for v in iterations])
+    rgb = None if benchmark else np.empty((jpeg.real_px_h, jpeg.real_px_w, 3), dtype=np.uint8)
+    opts = _options(init_mode, device)
+    rc = lib.art_context_process(_context(device), n, chans, w, pw, it, int(bool(separate)), jpeg.real_px_w,
+                                 jpeg.real_px_h, None if rgb is None else rgb.ctypes.data, C.byref(opts))
+    N.check(rc)
+    if benchmark:
+        raise ArtefactError("BENCHMARK")
+    return rgb

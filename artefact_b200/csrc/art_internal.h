@@ -1,0 +1,27 @@
+// Internal declarations shared by the host-side translation units.
+#pragma once
+
+#include <cstdint>
+#include <string>
+#include <vector>
+
+namespace art {
+
+struct JpegChannel {
+    uint32_t rounded_px_w = 0, rounded_px_h = 0, block_w = 0, block_h = 0;
+    uint32_t samp_h = 1, samp_v = 1;
+    float quant[64];
+    std::vector<int16_t> coefs;  // block raster, natural order inside a block
+};
+
+struct JpegImage {
+    uint32_t real_w = 0, real_h = 0;
+    std::vector<JpegChannel> channels;
+};
+
+bool decode_jpeg(const uint8_t *data, size_t len, JpegImage &out, std::string &err);
+
+// Thread-local error message for art_last_error().
+void set_error(const std::string &msg);
+
+}  // namespace art

@@ -1,0 +1,470 @@
+// Host-side baseline JPEG coefficient decoder.
+//
+// Stands in for the zune-jpeg fork that artefact-lib uses on the host
+// (backend/zune-jpeg/src/decoder.rs:187-206, mcu.rs:80-290, bitstream.rs:326-390,
+// headers.rs:115-178) and produces the same solver-input contract as
+// backend/artefact-lib/jpeg/zune.rs:22-46:
+//   * per component: rounded_px_w/h = image size rounded up to 8 * max sampling
+//     factor, divided by the component's sampling factor (misc.rs:209-249);
+//   * samp_h/samp_v = max sampling / component sampling (1 or 2);
+//   * quantised coefficients as int16 in natural (row-major, v*8+u) order within
+//     each 8x8 block, blocks in raster order over the component plane;
+//   * quantisation tables in natural order.
+// Sequential Huffman (SOF0/SOF1, 8-bit samples) with restart markers and
+// interleaved or single-component scans. Progressive and arithmetic coded
+// streams are rejected with an error.
+#include <cstdint>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "art_internal.h"
+
+namespace art {
+
+namespace {
+
+const uint8_t kZigzagToNatural[64] = {
+    0,  1,  8,  16, 9,  2,  3,  10, 17, 24, 32, 25, 18, 11, 4,  5,  12, 19, 26, 33, 40, 48,
+    41, 34, 27, 20, 13, 6,  7,  14, 21, 28, 35, 42, 49, 56, 57, 50, 43, 36, 29, 22, 15, 23,
+    30, 37, 44, 51, 58, 59, 52, 45, 38, 31, 39, 46, 53, 60, 61, 54, 47, 55, 62, 63};
+
+struct DecodeError {
+    std::string msg;
+};
+
+[[noreturn]] void fail(const std::string &m) { throw DecodeError{m}; }
+
+struct Huffman {
+    bool present = false;
+    // Canonical code description (ITU T.81 Annex C / F.2.2.3).
+    int32_t maxcode[18];
+    int32_t valptr[17];
+    int32_t mincode[17];
+    uint8_t vals[256];
+    // 9-bit lookahead: (length << 8) | value, 0 when the code is longer.
+    uint16_t fast[512];
+};
+
+void build_huffman(Huffman &h, const uint8_t counts[16], const uint8_t *symbols, int nsym)
+{
+    memset(&h, 0, sizeof(h));
+    memcpy(h.vals, symbols, nsym);
+    int code = 0, k = 0;
+    for (int len = 1; len <= 16; len++) {
+        h.valptr[len] = k;
+        h.mincode[len] = code;
+        code += counts[len - 1];
+        k += counts[len - 1];
+        h.maxcode[len] = counts[len - 1] ? code - 1 : -1;
+        if (code > (1 << len)) fail("Invalid Huffman table: code space overflow");
+        code <<= 1;
+    }
+    h.maxcode[17] = 0x7fffffff;
+    // Fill the lookahead table.
+    k = 0;
+    code = 0;
+    for (int len = 1; len <= 9; len++) {
+        for (int i = 0; i < counts[len - 1]; i++, k++) {
+            int c = h.mincode[len] + i;
+            int shift = 9 - len;
+            for (int f = 0; f < (1 << shift); f++) h.fast[(c << shift) | f] = (uint16_t)((len << 8) | symbols[k]);
+        }
+    }
+    h.present = true;
+}
+
+struct Component {
+    int id = 0;
+    int h = 1, v = 1, tq = 0;
+    int td = 0, ta = 0;
+    int dc_pred = 0;
+    uint32_t rounded_w = 0, rounded_h = 0, block_w = 0, block_h = 0;
+    std::vector<int16_t> coefs;
+};
+
+class Decoder {
+  public:
+    Decoder(const uint8_t *data, size_t len) : d_(data), n_(len) {}
+
+    void run(JpegImage &out);
+
+  private:
+    const uint8_t *d_;
+    size_t n_;
+    size_t pos_ = 0;
+    uint16_t qt_[4][64];
+    bool qt_present_[4] = {false, false, false, false};
+    Huffman dc_[4], ac_[4];
+    std::vector<Component> comps_;
+    bool have_sof_ = false;
+    int width_ = 0, height_ = 0;
+    int hmax_ = 1, vmax_ = 1;
+    int restart_interval_ = 0;
+    // Bit reader state.
+    uint32_t bitbuf_ = 0;
+    int bitcnt_ = 0;
+    bool hit_marker_ = false;
+
+    uint8_t u8()
+    {
+        if (pos_ >= n_) fail("No more bytes: unexpected end of JPEG stream");
+        return d_[pos_++];
+    }
+    uint16_t u16()
+    {
+        uint16_t a = u8();
+        return (uint16_t)((a << 8) | u8());
+    }
+    void parse_dqt();
+    void parse_dht();
+    void parse_sof(int marker);
+    void parse_sos();
+    void decode_scan(const std::vector<int> &scomp);
+    void fill_bits();
+    int get_bits(int n);
+    int decode_huff(const Huffman &h);
+    void decode_block(Component &c, int16_t *blk);
+    void reset_bits()
+    {
+        bitbuf_ = 0;
+        bitcnt_ = 0;
+        hit_marker_ = false;
+    }
+    void handle_restart();
+};
+
+void Decoder::parse_dqt()
+{
+    int len = u16();
+    if (len < 2) fail("Invalid DQT length. Length should be greater than 2");
+    len -= 2;
+    while (len > 0) {
+        int info = u8();
+        int prec = info >> 4, id = info & 15;
+        int need = 64 * (prec + 1) + 1;
+        if (need > len) fail("Invalid QT table: too few bytes left");
+        if (prec > 1) fail("Expected QT precision value of either 0 or 1");
+        if (id >= 4) fail("Too large table position for QT");
+        for (int i = 0; i < 64; i++) qt_[id][kZigzagToNatural[i]] = prec ? u16() : u8();
+        qt_present_[id] = true;
+        len -= need;
+    }
+}
+
+void Decoder::parse_dht()
+{
+    int len = u16();
+    if (len < 2) fail("Invalid Huffman length in image");
+    len -= 2;
+    while (len > 0) {
+        if (len < 17) fail("Invalid Huffman length in image");
+        int info = u8();
+        int tc = info >> 4, th = info & 15;
+        if (tc > 1 || th > 3) fail("Invalid Huffman table class or index");
+        uint8_t counts[16];
+        int total = 0;
+        for (int i = 0; i < 16; i++) {
+            counts[i] = u8();
+            total += counts[i];
+        }
+        if (total > 256 || 17 + total > len) fail("Invalid Huffman length in image");
+        uint8_t syms[256];
+        for (int i = 0; i < total; i++) syms[i] = u8();
+        build_huffman(tc ? ac_[th] : dc_[th], counts, syms, total);
+        len -= 17 + total;
+    }
+}
+
+void Decoder::parse_sof(int marker)
+{
+    if (marker == 0xC2 || marker == 0xC6 || marker == 0xCA || marker == 0xCE)
+        fail("Progressive JPEG is not supported by this decoder");
+    if (marker != 0xC0 && marker != 0xC1) fail("Unsupported JPEG coding process (lossless or arithmetic)");
+    if (have_sof_) fail("Duplicate start of frame");
+    int len = u16();
+    int prec = u8();
+    height_ = u16();
+    width_ = u16();
+    int nc = u8();
+    int expected = 8 + 3 * nc;
+    if (len != expected)
+        fail("Length of start of frame differs from expected " + std::to_string(expected) + ",value is " +
+             std::to_string(len));
+    if (prec != 8) fail("Only 8-bit sample precision is supported");
+    if (width_ == 0 || height_ == 0) fail("Zero image dimension");
+    if (nc != 1 && nc != 3 && nc != 4) fail("Unsupported number of components");
+    comps_.resize(nc);
+    for (int i = 0; i < nc; i++) {
+        Component &c = comps_[i];
+        c.id = u8();
+        int hv = u8();
+        c.h = hv >> 4;
+        c.v = hv & 15;
+        c.tq = u8();
+        if (c.h < 1 || c.h > 2 || c.v < 1 || c.v > 2) fail("Unknown sample factor, expected either 1 or 2");
+        if (c.tq > 3) fail("Invalid quantization table index");
+    }
+    if (nc == 1) comps_[0].h = comps_[0].v = 1;  // single-component scans are never interleaved
+    hmax_ = vmax_ = 1;
+    for (auto &c : comps_) {
+        if (c.h > hmax_) hmax_ = c.h;
+        if (c.v > vmax_) vmax_ = c.v;
+    }
+    // misc.rs:209-249: round to 8 * max sampling, then divide by the component's factor.
+    uint32_t mw = 8 * hmax_ - 1, mh = 8 * vmax_ - 1;
+    uint32_t rw = ((uint32_t)width_ + mw) & ~mw;
+    uint32_t rh = ((uint32_t)height_ + mh) & ~mh;
+    for (auto &c : comps_) {
+        int sf_h = hmax_ / c.h, sf_v = vmax_ / c.v;
+        c.rounded_w = rw / sf_h;
+        c.rounded_h = rh / sf_v;
+        c.block_w = c.rounded_w / 8;
+        c.block_h = c.rounded_h / 8;
+        c.coefs.assign((size_t)c.rounded_w * c.rounded_h, 0);
+    }
+    have_sof_ = true;
+}
+
+void Decoder::fill_bits()
+{
+    while (bitcnt_ <= 24) {
+        uint32_t byte = 0;
+        if (!hit_marker_ && pos_ < n_) {
+            byte = d_[pos_];
+            if (byte == 0xFF) {
+                uint8_t next = pos_ + 1 < n_ ? d_[pos_ + 1] : 0xD9;
+                if (next == 0x00) {
+                    pos_ += 2;
+                } else {
+                    hit_marker_ = true;  // leave the marker in place, feed zeros
+                    byte = 0;
+                }
+            } else {
+                pos_++;
+            }
+        }
+        bitbuf_ |= byte << (24 - bitcnt_);
+        bitcnt_ += 8;
+    }
+}
+
+int Decoder::get_bits(int n)
+{
+    if (n == 0) return 0;
+    fill_bits();
+    int v = (int)(bitbuf_ >> (32 - n));
+    bitbuf_ <<= n;
+    bitcnt_ -= n;
+    return v;
+}
+
+int Decoder::decode_huff(const Huffman &h)
+{
+    fill_bits();
+    uint32_t look = bitbuf_ >> 23;
+    uint16_t f = h.fast[look];
+    if (f) {
+        int l = f >> 8;
+        bitbuf_ <<= l;
+        bitcnt_ -= l;
+        return f & 0xFF;
+    }
+    int code = 0;
+    for (int len = 1; len <= 16; len++) {
+        code = (code << 1) | (int)(bitbuf_ >> 31);
+        bitbuf_ <<= 1;
+        bitcnt_--;
+        if (h.maxcode[len] >= 0 && code <= h.maxcode[len] && code >= h.mincode[len])
+            return h.vals[h.valptr[len] + code - h.mincode[len]];
+    }
+    fail("Bad Huffman code: corrupt JPEG entropy data");
+}
+
+static inline int extend(int v, int t) { return v < (1 << (t - 1)) ? v - (1 << t) + 1 : v; }
+
+void Decoder::decode_block(Component &c, int16_t *blk)
+{
+    const Huffman &dc = dc_[c.td], &ac = ac_[c.ta];
+    int t = decode_huff(dc);
+    if (t > 11) fail("Bad DC magnitude category");
+    int diff = t ? extend(get_bits(t), t) : 0;
+    c.dc_pred += diff;
+    blk[0] = (int16_t)c.dc_pred;
+    for (int k = 1; k < 64;) {
+        int rs = decode_huff(ac);
+        int r = rs >> 4, s = rs & 15;
+        if (s == 0) {
+            if (r != 15) break;  // EOB
+            k += 16;
+            continue;
+        }
+        k += r;
+        if (k > 63) fail("Coefficient index out of range: corrupt JPEG");
+        blk[kZigzagToNatural[k]] = (int16_t)extend(get_bits(s), s);
+        k++;
+    }
+}
+
+void Decoder::handle_restart()
+{
+    // Discard buffered bits, then expect RSTn.
+    reset_bits();
+    while (pos_ + 1 < n_ && !(d_[pos_] == 0xFF && d_[pos_ + 1] >= 0xD0 && d_[pos_ + 1] <= 0xD7)) {
+        if (d_[pos_] == 0xFF && d_[pos_ + 1] != 0x00 && d_[pos_ + 1] != 0xFF) break;
+        pos_++;
+    }
+    if (pos_ + 1 < n_ && d_[pos_] == 0xFF && d_[pos_ + 1] >= 0xD0 && d_[pos_ + 1] <= 0xD7) pos_ += 2;
+    for (auto &c : comps_) c.dc_pred = 0;
+}
+
+void Decoder::decode_scan(const std::vector<int> &scomp)
+{
+    reset_bits();
+    for (auto &c : comps_) c.dc_pred = 0;
+    int todo = restart_interval_;
+    if (scomp.size() == 1) {
+        // Non-interleaved: blocks covering ceil(component samples / 8).
+        Component &c = comps_[scomp[0]];
+        int cw = (width_ * c.h + hmax_ - 1) / hmax_, chh = (height_ * c.v + vmax_ - 1) / vmax_;
+        int bw = (cw + 7) / 8, bh = (chh + 7) / 8;
+        for (int by = 0; by < bh; by++)
+            for (int bx = 0; bx < bw; bx++) {
+                if (restart_interval_ && todo == 0) {
+                    handle_restart();
+                    todo = restart_interval_;
+                }
+                int16_t blk[64] = {0};
+                decode_block(c, blk);
+                if ((uint32_t)bx < c.block_w && (uint32_t)by < c.block_h)
+                    memcpy(&c.coefs[((size_t)by * c.block_w + bx) * 64], blk, sizeof(blk));
+                if (restart_interval_) todo--;
+            }
+        return;
+    }
+    int mcu_w = (width_ + 8 * hmax_ - 1) / (8 * hmax_), mcu_h = (height_ + 8 * vmax_ - 1) / (8 * vmax_);
+    for (int my = 0; my < mcu_h; my++)
+        for (int mx = 0; mx < mcu_w; mx++) {
+            if (restart_interval_ && todo == 0) {
+                handle_restart();
+                todo = restart_interval_;
+            }
+            for (int ci : scomp) {
+                Component &c = comps_[ci];
+                for (int v = 0; v < c.v; v++)
+                    for (int u = 0; u < c.h; u++) {
+                        int16_t blk[64] = {0};
+                        decode_block(c, blk);
+                        uint32_t bx = (uint32_t)(mx * c.h + u), by = (uint32_t)(my * c.v + v);
+                        if (bx < c.block_w && by < c.block_h)
+                            memcpy(&c.coefs[((size_t)by * c.block_w + bx) * 64], blk, sizeof(blk));
+                    }
+            }
+            if (restart_interval_) todo--;
+        }
+}
+
+void Decoder::parse_sos()
+{
+    int len = u16();
+    if (!have_sof_) {
+        if (len < 6 || len > 10) fail("Bad SOS length " + std::to_string(len) + ",corrupt jpeg");
+        fail("Scan found before start of frame");
+    }
+    int ns = u8();
+    if (ns < 1 || ns > 4 || len != 6 + 2 * ns) fail("Bad SOS length " + std::to_string(len) + ",corrupt jpeg");
+    std::vector<int> scomp;
+    for (int i = 0; i < ns; i++) {
+        int cid = u8();
+        int t = u8();
+        int idx = -1;
+        for (size_t k = 0; k < comps_.size(); k++)
+            if (comps_[k].id == cid) idx = (int)k;
+        if (idx < 0) fail("Scan references an unknown component");
+        comps_[idx].td = t >> 4;
+        comps_[idx].ta = t & 15;
+        if (comps_[idx].td > 3 || comps_[idx].ta > 3) fail("Invalid Huffman table index in scan");
+        if (!dc_[comps_[idx].td].present) fail("No DC table for component");
+        if (!ac_[comps_[idx].ta].present) fail("No AC table for component");
+        scomp.push_back(idx);
+    }
+    int ss = u8(), se = u8(), ahal = u8();
+    if (ss != 0 || se != 63 || ahal != 0) fail("Invalid spectral selection for a sequential scan");
+    decode_scan(scomp);
+}
+
+void Decoder::run(JpegImage &out)
+{
+    if (n_ < 2 || d_[0] != 0xFF || d_[1] != 0xD8) fail("Not a JPEG file: missing SOI marker");
+    pos_ = 2;
+    bool done = false;
+    while (!done) {
+        uint8_t b = u8();
+        if (b != 0xFF) fail("Expected a marker, found byte " + std::to_string(b));
+        uint8_t m = u8();
+        while (m == 0xFF) m = u8();
+        switch (m) {
+        case 0x00: fail("Bad marker 0xFF00 outside entropy-coded data");
+        case 0xD8: fail("Duplicate SOI marker");
+        case 0xD9: done = true; break;
+        case 0xDB: parse_dqt(); break;
+        case 0xC4: parse_dht(); break;
+        case 0xDD: {
+            int len = u16();
+            if (len != 4) fail("Bad DRI length");
+            restart_interval_ = u16();
+            break;
+        }
+        case 0xDA: parse_sos(); break;
+        case 0xC0: case 0xC1: case 0xC2: case 0xC3: case 0xC5: case 0xC6: case 0xC7:
+        case 0xC9: case 0xCA: case 0xCB: case 0xCD: case 0xCE: case 0xCF:
+            parse_sof(m);
+            break;
+        default:
+            if (m >= 0xD0 && m <= 0xD7) break;  // stray RST
+            {
+                int len = u16();
+                if (len < 2) fail("Bad marker segment length");
+                if (pos_ + (size_t)(len - 2) > n_) fail("No more bytes: unexpected end of JPEG stream");
+                pos_ += (size_t)(len - 2);
+            }
+        }
+        if (!done && pos_ >= n_) {
+            if (have_sof_) done = true;  // tolerate a missing EOI after decoded scans
+            else fail("No more bytes: unexpected end of JPEG stream");
+        }
+    }
+    if (!have_sof_) fail("No start of frame found");
+    out.real_w = (uint32_t)width_;
+    out.real_h = (uint32_t)height_;
+    out.channels.clear();
+    for (auto &c : comps_) {
+        if (!qt_present_[c.tq]) fail("No quantization table for component");
+        JpegChannel jc;
+        jc.rounded_px_w = c.rounded_w;
+        jc.rounded_px_h = c.rounded_h;
+        jc.block_w = c.block_w;
+        jc.block_h = c.block_h;
+        jc.samp_h = (uint32_t)(hmax_ / c.h);
+        jc.samp_v = (uint32_t)(vmax_ / c.v);
+        for (int j = 0; j < 64; j++) jc.quant[j] = (float)qt_[c.tq][j];
+        jc.coefs = std::move(c.coefs);
+        out.channels.push_back(std::move(jc));
+    }
+}
+
+}  // namespace
+
+bool decode_jpeg(const uint8_t *data, size_t len, JpegImage &out, std::string &err)
+{
+    try {
+        Decoder dec(data, len);
+        dec.run(out);
+        return true;
+    } catch (const DecodeError &e) {
+        err = e.msg;
+        return false;
+    }
+}
+
+}  // namespace art

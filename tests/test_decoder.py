@@ -1,0 +1,107 @@
+"""Host JPEG coefficient decoder (CPU only): check (a), bit-exact coefficients
+and quantisation tables, plus the reference decoder's error cases."""
+import io
+import json
+from pathlib import Path
+
+import numpy as np
+import pytest
+
+import jpeg_encoder as E
+import oracle_lib as O
+from artefact_b200 import synth
+from artefact_b200.api import ArtefactError, Jpeg, JpegSource
+
+GOLDEN = Path(__file__).resolve().parent / "golden"
+
+
+@pytest.mark.parametrize("case", json.loads((GOLDEN / "decoder_malformed.json").read_text()),
+                         ids=lambda c: c["name"])
+def test_malformed_streams_are_rejected(case):
+    """backend/zune-jpeg/tests/invalid_images.rs:12-66."""
+    with pytest.raises(ArtefactError) as ei:
+        Jpeg.from_source(JpegSource.Buffer(bytes(case["bytes"])))
+    if case["message"]:
+        assert case["message"] in str(ei.value)
+
+
+@pytest.mark.parametrize("name", ["gray_37x21", "420_100x70_rst3", "422_50x30", "444_24x40_rst5"])
+def test_golden_roundtrip_bit_exact(name):
+    j = Jpeg.from_source(JpegSource.File(str(GOLDEN / f"roundtrip_{name}.jpg")))
+    ref = np.load(GOLDEN / f"roundtrip_{name}.npz")
+    assert j.nchannel == len([k for k in ref.files if k.startswith("coefs")])
+    for i, c in enumerate(j.coefs):
+        bw, bh, sh, sv = ref[f"meta{i}"].tolist()
+        assert (c.block_w, c.block_h, c.horizontal_samp_factor, c.vertical_samp_factor) == (bw, bh, sh, sv)
+        assert (c.rounded_px_w, c.rounded_px_h) == (bw * 8, bh * 8)
+        assert c.dct_coefs.dtype == np.int16
+        assert np.array_equal(c.dct_coefs.reshape(-1, 64), ref[f"coefs{i}"])
+        assert np.array_equal(c.quant_table, ref[f"qt{i}"])
+
+
+@pytest.mark.parametrize("seed", range(6))
+def test_random_roundtrip_bit_exact(seed):
+    rng = np.random.default_rng(100 + seed)
+    samplings = [[(1, 1)], [(2, 2), (1, 1), (1, 1)], [(2, 1), (1, 1), (1, 1)], [(1, 1)] * 3]
+    samp = samplings[seed % len(samplings)]
+    w, h = int(rng.integers(1, 90)), int(rng.integers(1, 90))
+    comps, expect, (rw, rh) = E.random_image(rng, w, h, samp, qt_max=255 if seed % 2 else 1000)
+    data = E.encode(w, h, comps, restart_interval=int(rng.integers(0, 4)))
+    j = Jpeg.from_source(JpegSource.Buffer(data))
+    assert (j.real_px_w, j.real_px_h) == (w, h)
+    assert j.max_rounded()[:2] == (rw, rh)
+    for c, (coefs, qt, bw, bh, sh, sv) in zip(j.coefs, expect):
+        assert (c.block_w, c.block_h, c.horizontal_samp_factor, c.vertical_samp_factor) == (bw, bh, sh, sv)
+        assert np.array_equal(c.dct_coefs.reshape(-1, 64), coefs)
+        assert np.array_equal(c.quant_table, qt)
+
+
+def _pixels(c):
+    blocks = c.dct_coefs.reshape(-1, 64).astype(np.float64) * c.quant_table[None, :]
+    img = np.zeros((c.rounded_px_h, c.rounded_px_w))
+    for i, b in enumerate(blocks):
+        by, bx = divmod(i, c.block_w)
+        img[by * 8:by * 8 + 8, bx * 8:bx * 8 + 8] = O.idct8x8(b.reshape(8, 8), fp64=True)
+    return np.clip(img + 128, 0, 255)
+
+
+@pytest.mark.parametrize("w,h,sub,gray", [(64, 48, "4:4:4", True), (100, 70, "4:2:0", False),
+                                          (96, 64, "4:4:4", False), (33, 17, "4:2:0", False)])
+def test_pillow_pixels_agree(w, h, sub, gray):
+    """Dequantised IDCT of the decoded coefficients equals libjpeg's decode to rounding."""
+    from PIL import Image
+
+    data = synth.make_jpeg(w, h, 75, sub, gray, seed=3)
+    j = Jpeg.from_source(JpegSource.Buffer(data))
+    im = Image.open(io.BytesIO(data))
+    if not gray:
+        im.draft("YCbCr", im.size)
+    ref = np.asarray(im).astype(np.float64)
+    if gray:
+        ref = ref[..., None]
+    for ci, c in enumerate(j.coefs):
+        if c.horizontal_samp_factor != 1 or c.vertical_samp_factor != 1:
+            continue  # libjpeg upsamples chroma with its own filter
+        assert np.abs(_pixels(c)[:h, :w] - ref[..., ci]).max() <= 1.0
+
+
+def test_rounded_sizes_follow_max_sampling():
+    data = synth.make_jpeg(1920, 1080, 75, "4:2:0", False, seed=1)
+    j = Jpeg.from_source(JpegSource.Buffer(data))
+    assert [(c.rounded_px_w, c.rounded_px_h, c.horizontal_samp_factor) for c in j.coefs] == [
+        (1920, 1088, 1), (960, 544, 2), (960, 544, 2)]
+
+
+def test_progressive_is_reported_unsupported():
+    from PIL import Image
+
+    buf = io.BytesIO()
+    Image.fromarray(synth.channel_image(32, 32, 1)).save(buf, "JPEG", quality=80, progressive=True)
+    with pytest.raises(ArtefactError, match="Progressive"):
+        Jpeg.from_source(JpegSource.Buffer(buf.getvalue()))
+
+
+def test_truncated_stream_is_an_error():
+    data = synth.make_jpeg(64, 64, 75, "4:2:0", False, seed=2)
+    with pytest.raises(ArtefactError):
+        Jpeg.from_source(JpegSource.Buffer(data[:200]))
