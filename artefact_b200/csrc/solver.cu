@@ -31,285 +31,195 @@ namespace art {
 
 // ============================================================== kernels ====
 
-template <int TH>
-struct GradLayout {
-    static constexpr int NT = TILE_W * TH / 4;
-    static constexpr int YW = TILE_W + 4, YH = TH + 4;  // y with a 2-pixel halo
-    static constexpr int EW = TILE_W + 2, EH = TH + 2;  // per-pixel terms with a 1-pixel ring
-    static constexpr int YS = 3 * YH * YW;
-    static constexpr int PS = 3 * TH * TILE_W;
-    static constexpr int ES = 3 * EH * EW;
-    static constexpr int FLOATS = YS + PS + 5 * ES;
-    static constexpr size_t BYTES = FLOATS * sizeof(float);
-    static_assert(3 * TH * TILE_W <= ES, "x_k tile must fit in the aliased term array");
-};
-
-// Gradient of the objective at the FISTA point y (compute_step.rs:8-48), with
-// the per-channel sum of squares reduced to sigma_c = step / ||g_c||
-// (compute_step.rs:52-58).
-template <int TH>
-__global__ void __launch_bounds__(TILE_W *TH / 4) k_gradient(const ImgDev *__restrict__ imgs,
-                                                            const int2 *__restrict__ tilemap, int parity, float f)
+// Gradient of the objective at the FISTA point y_k (compute_step.rs:8-48) and
+// the per-channel sums of squares reduced to sigma_c = step / ||g_c||
+// (compute_step.rs:52-58). One warp per strip of SWEEP_OUT output columns and
+// strip_rows rows; lane L holds column xs - 2 + L. Lanes 1..30 form the
+// per-pixel terms, lanes 2..29 write g. Rows and columns outside the image are
+// read clamped (replicated edges make the reference's last-row/column forward
+// differences vanish, compute_step_tv.rs:105-120) and their terms are zero,
+// which reproduces the reference's scatter guards. Rows are prefetched two
+// ahead of use.
+template <int NCH>
+__global__ void __launch_bounds__(SWEEP_WARPS * 32) k_grad_sweep(const ImgDev *__restrict__ imgs,
+                                                                 const int2 *__restrict__ work)
 {
-    using L = GradLayout<TH>;
-    constexpr int NT = L::NT, YW = L::YW, YH = L::YH, EW = L::EW, EH = L::EH;
-    extern __shared__ float4 smem4[];
-    float *Ys = reinterpret_cast<float *>(smem4);
-    float *P = Ys + L::YS;
-    float *AU = P + L::PS;
-    float *U = AU + L::ES;
-    float *BV = U + L::ES;
-    float *V = BV + L::ES;
-    float *Wt = V + L::ES;
-    float *Xc = Wt;  // x_k of the tile; dead before Wt is written
-    __shared__ float s_q[3][64], s_iq[3][64];
-    __shared__ float s_red[NT / 32][3];
-    __shared__ double s_dred[NT / 32][3];
+    __shared__ float s_red[SWEEP_WARPS][NCH];
+    __shared__ double s_dred[SWEEP_WARPS][NCH];
     __shared__ int s_last;
-
-    const int tid = threadIdx.x;
-    const int2 tm = tilemap[blockIdx.x];
-    const ImgDev &im = imgs[tm.x];
-    const int nch = im.nch, W = im.W, H = im.H, pitch = im.pitch;
-    const int tx = tm.y % im.tiles_x, ty = tm.y / im.tiles_x;
-    const int x0 = tx * TILE_W, y0 = ty * TH;
+    const unsigned FULL = 0xffffffffu;
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int2 wk = work[blockIdx.x];
+    const ImgDev &im = imgs[wk.x];
+    const int W = im.W, H = im.H, pitch = im.pitch, R = im.strip_rows;
     const long long cs = im.cstride;
-    const float *cur = im.x[parity];
-    const float *prev = im.x[parity ^ 1];
+    const int strip = wk.y * SWEEP_WARPS + warp;
+    float ssq[NCH];
+#pragma unroll
+    for (int c = 0; c < NCH; c++) ssq[c] = 0.f;
 
-    for (int i = tid; i < nch * 64; i += NT) {
-        s_q[i >> 6][i & 63] = im.q[i >> 6][i & 63];
-        s_iq[i >> 6][i & 63] = im.invq2[i >> 6][i & 63];
-    }
-
-    // Phase 0: y = x_k + f (x_k - x_{k-1}) (mod.rs:54-57) on the tile plus a
-    // 2-pixel halo, coordinates clamped into the image (replicated edges make
-    // the forward differences vanish on the last row/column as the reference's
-    // edge tests do, compute_step_tv.rs:105-120).
-    for (int i = tid; i < YH * YW; i += NT) {
-        const int ey = i / YW, ex = i - ey * YW;
-        const int gy = min(max(y0 - 2 + ey, 0), H - 1), gx = min(max(x0 - 2 + ex, 0), W - 1);
-        const long long o = (long long)gy * pitch + gx;
-#pragma unroll
-        for (int c = 0; c < 3; c++) {
-            if (c < nch) {
-                const float a = __ldg(cur + c * cs + o), b = __ldg(prev + c * cs + o);
-                Ys[c * YH * YW + i] = fmaf(f, a - b, a);
-            }
-        }
-    }
-    {
-        const int r = tid >> 3, c4 = (tid & 7) * 4;
-        const int gy = y0 + r, gx = x0 + c4;
-        if (gy < H && gx < W) {
-#pragma unroll
-            for (int c = 0; c < 3; c++)
-                if (c < nch)
-                    *reinterpret_cast<float4 *>(&Xc[c * TH * TILE_W + r * TILE_W + c4]) =
-                        __ldg(reinterpret_cast<const float4 *>(cur + c * cs + (long long)gy * pitch + gx));
-        }
-    }
-    __syncthreads();
-
-    // DCT-distance gradient (compute_step_prob.rs:5-60): per coefficient block
-    // d = (cos - c q) / q^2, IDCT, times alpha_p, replicated to the sh x sv
-    // pixels of each component sample. cos is the clamped DCT of the (pooled)
-    // x_k, which equals the reference's stored copy (compute_projection.rs:82)
-    // up to rounding.
-    {
-        const int ntask = count_tasks<TH>(im);
-        const int lane8 = tid & 7, grp = tid >> 3;
-        for (int base = 0; base < ntask; base += NT / 8) {
-            const CellTask t = get_task<TH>(im, base + grp);
-            const bool act = t.c >= 0 && (x0 + t.cx0) < W && (y0 + t.cy0) < H;
-            const int cc = act ? t.c : 0;
-            const int sh = im.ch[cc].sh, sv = im.ch[cc].sv;
-            const float ap = act ? im.ch[cc].alpha_p : 0.f;
-            const bool doprob = act && ap != 0.f;
-            float *X = Xc + cc * TH * TILE_W;
-            float v[8];
-            if (doprob) {
-#pragma unroll
-                for (int k = 0; k < 8; k++) {
-                    float s = 0.f;
-                    for (int sy = 0; sy < sv; sy++)
-                        for (int sx = 0; sx < sh; sx++)
-                            s += X[(t.cy0 + k * sv + sy) * TILE_W + t.cx0 + lane8 * sh + sx];
-                    v[k] = s / (float)(sh * sv);
-                }
-                dct8(v);
-#pragma unroll
-                for (int k = 0; k < 8; k++) X[(t.cy0 + k * sv) * TILE_W + t.cx0 + lane8 * sh] = v[k];
-            }
-            __syncwarp();
-            if (doprob) {
-                float *row = X + (t.cy0 + lane8 * sv) * TILE_W + t.cx0;
-#pragma unroll
-                for (int u = 0; u < 8; u++) v[u] = row[u * sh];
-                dct8(v);
-                const ChanDev &cd = im.ch[cc];
-                const int bx = (x0 + t.cx0) / (8 * sh), by = (y0 + t.cy0) / (8 * sv);
-                float co[8];
-                load_coef_row(cd.coef + (long long)(by * 8 + lane8) * cd.cpitch + bx * 8, co);
-#pragma unroll
-                for (int u = 0; u < 8; u++) {
-                    const float q = s_q[cc][lane8 * 8 + u];
-                    const float lo = (co[u] - 0.5f) * q, hi = (co[u] + 0.5f) * q;
-                    const float cl = fminf(fmaxf(v[u], lo), hi);
-                    v[u] = (cl - co[u] * q) * s_iq[cc][lane8 * 8 + u];
-                }
-                idct8(v);
-#pragma unroll
-                for (int u = 0; u < 8; u++) row[u * sh] = v[u];
-            }
-            __syncwarp();
-            if (act) {
-                float *Pc = P + cc * TH * TILE_W;
-                if (doprob) {
-#pragma unroll
-                    for (int k = 0; k < 8; k++) v[k] = X[(t.cy0 + k * sv) * TILE_W + t.cx0 + lane8 * sh];
-                    idct8(v);
-                } else {
-#pragma unroll
-                    for (int k = 0; k < 8; k++) v[k] = 0.f;
-                }
-#pragma unroll
-                for (int k = 0; k < 8; k++)
-                    for (int sy = 0; sy < sv; sy++)
-                        for (int sx = 0; sx < sh; sx++)
-                            Pc[(t.cy0 + k * sv + sy) * TILE_W + t.cx0 + lane8 * sh + sx] = ap * v[k];
-            }
-            __syncwarp();
-        }
-    }
-    __syncthreads();
-
-    // Phase 1: for every pixel q of the tile and a 1-pixel ring, the TV terms
-    // (compute_step_tv.rs:98-146) and the TGV terms (compute_step_tv2.rs:42-135),
-    // both normalised by the norms coupled over channels. Terms of pixels
-    // outside the image are zero, which reproduces the reference's guards.
-    {
+    if (strip < im.nstrips) {
+        const int sxi = strip % im.strips_x, syi = strip / im.strips_x;
+        const int xs = sxi * SWEEP_OUT, ys = syi * R;
+        const int gx = xs - 2 + lane;
+        const int cx = min(max(gx, 0), W - 1);
+        const bool colin = gx >= 0 && gx < W;
+        const bool outlane = lane >= 2 && lane < 30 && gx < W;
+        const float *yp = im.y + cx;
+        float *gout = im.g + (outlane ? gx : 0);
         const float at = im.alpha_tv, ag = im.alpha_tgv;
-        for (int i = tid; i < EH * EW; i += NT) {
-            const int ey = i / EW, ex = i - ey * EW;
-            const int gxq = x0 - 1 + ex, gyq = y0 - 1 + ey;
-            const bool inside = gxq >= 0 && gxq < W && gyq >= 0 && gyq < H;
-            float dx[3], dy[3], gxx[3], gyy[3], gs[3];
+        auto rowoff = [&](int row) -> long long { return (long long)min(max(row, 0), H - 1) * pitch; };
+        // DCT-distance gradient plane of each channel at this lane's column,
+        // prefetched two output rows ahead like y.
+        const float *pcol[NCH];
+        int psv[NCH], ppitch[NCH];
+        bool pon[NCH];
+#pragma unroll
+        for (int c = 0; c < NCH; c++) {
+            const ChanDev &cd = im.ch[c];
+            pon[c] = cd.alpha_p != 0.f;
+            psv[c] = cd.sv;
+            ppitch[c] = cd.ppitch;
+            pcol[c] = cd.P + (outlane ? gx / cd.sh : 0);
+        }
+        auto pload = [&](int c, int row) -> float {
+            const int rr = min(max(row, 0), H - 1);
+            return pon[c] ? __ldg(pcol[c] + (long long)(rr / psv[c]) * ppitch[c]) : 0.f;
+        };
+
+        float yv[NCH], dxp[NCH], dyp[NCH], Gm[NCH], G0[NCH], Gp[NCH], q1[NCH], q2[NCH], p1[NCH], p2[NCH];
+        {
+            const long long o0 = rowoff(ys - 2), o1 = rowoff(ys - 1), o2 = rowoff(ys), o3 = rowoff(ys + 1);
+#pragma unroll
+            for (int c = 0; c < NCH; c++) {
+                const float y0 = __ldg(yp + c * cs + o0);
+                yv[c] = __ldg(yp + c * cs + o1);
+                q1[c] = __ldg(yp + c * cs + o2);
+                q2[c] = __ldg(yp + c * cs + o3);
+                p1[c] = pload(c, ys - 2);  // output row of step t = ys - 1
+                p2[c] = pload(c, ys - 1);
+                dxp[c] = __shfl_down_sync(FULL, y0, 1) - y0;
+                dyp[c] = yv[c] - y0;
+                Gm[c] = G0[c] = Gp[c] = 0.f;
+            }
+        }
+        for (int t = ys - 1; t <= ys + R; t++) {
+            float yn[NCH], pr[NCH];
+            {
+                const long long o = rowoff(t + 3);
+#pragma unroll
+                for (int c = 0; c < NCH; c++) {
+                    yn[c] = q1[c];
+                    q1[c] = q2[c];
+                    q2[c] = __ldg(yp + c * cs + o);
+                    pr[c] = p1[c];
+                    p1[c] = p2[c];
+                    p2[c] = pload(c, t + 1);
+                }
+            }
+            const bool inside = colin && t >= 0 && t < H;
+            float dx[NCH], dy[NCH], gxx[NCH], gyy[NCH], gs[NCH];
             float n1 = 0.f, n2 = 0.f;
 #pragma unroll
-            for (int c = 0; c < 3; c++) {
-                dx[c] = dy[c] = gxx[c] = gyy[c] = gs[c] = 0.f;
-                if (c < nch) {
-                    const float *Y = Ys + c * YH * YW + (ey + 1) * YW + (ex + 1);
-                    const float yc = Y[0], yr = Y[1], yl = Y[-1], yd = Y[YW], yu = Y[-YW];
-                    const float ydl = Y[YW - 1], yur = Y[-YW + 1];
-                    const float ddx = yr - yc, ddy = yd - yc;
-                    const float dxl = yc - yl, dyl = ydl - yl, dxu = yur - yu, dyu = yc - yu;
-                    const float axx = gxq > 0 ? ddx - dxl : 0.f;
-                    const float ayx = gxq > 0 ? ddy - dyl : 0.f;
-                    const float ayy = gyq > 0 ? ddy - dyu : 0.f;
-                    const float axy = gyq > 0 ? ddx - dxu : 0.f;
-                    const float s = 0.5f * (axy + ayx);
-                    n1 += ddx * ddx;
-                    n1 += ddy * ddy;
-                    n2 += ayy * ayy + (2.f * (s * s) + axx * axx);
-                    dx[c] = ddx;
-                    dy[c] = ddy;
-                    gxx[c] = axx;
-                    gyy[c] = ayy;
-                    gs[c] = s;
-                }
+            for (int c = 0; c < NCH; c++) {
+                dx[c] = __shfl_down_sync(FULL, yv[c], 1) - yv[c];
+                dy[c] = yn[c] - yv[c];
+                n1 += dx[c] * dx[c];
+                n1 += dy[c] * dy[c];
+            }
+#pragma unroll
+            for (int c = 0; c < NCH; c++) {
+                const float dxl = __shfl_up_sync(FULL, dx[c], 1), dyl = __shfl_up_sync(FULL, dy[c], 1);
+                const float axx = gx > 0 ? dx[c] - dxl : 0.f;
+                const float ayx = gx > 0 ? dy[c] - dyl : 0.f;
+                const float ayy = t > 0 ? dy[c] - dyp[c] : 0.f;
+                const float axy = t > 0 ? dx[c] - dxp[c] : 0.f;
+                const float s = 0.5f * (axy + ayx);
+                n2 += ayy * ayy + (2.f * (s * s) + axx * axx);
+                gxx[c] = axx;
+                gyy[c] = ayy;
+                gs[c] = s;
             }
             const float inv1 = (inside && n1 > 0.f) ? rsqrtf(n1) : 0.f;
             const float inv2 = (inside && n2 > 0.f) ? rsqrtf(n2) : 0.f;
-            const bool intile = ex >= 1 && ex <= TILE_W && ey >= 1 && ey <= TH;
 #pragma unroll
-            for (int c = 0; c < 3; c++) {
-                if (c < nch) {
-                    const float a = at * dx[c] * inv1, b = at * dy[c] * inv1;
-                    const float u = ag * (gs[c] + gxx[c]) * inv2;
-                    const float vv = ag * (gyy[c] + gs[c]) * inv2;
-                    const float w = ag * gs[c] * inv2;
-                    const int e = c * EH * EW + i;
-                    AU[e] = a + u;
-                    U[e] = u;
-                    BV[e] = b + vv;
-                    V[e] = vv;
-                    Wt[e] = w;
-                    if (intile) P[c * TH * TILE_W + (ey - 1) * TILE_W + (ex - 1)] += -(a + b) - 2.f * (u + vv - w);
+            for (int c = 0; c < NCH; c++) {
+                const float a = at * dx[c] * inv1, b = at * dy[c] * inv1;
+                const float u = ag * (gs[c] + gxx[c]) * inv2;
+                const float v = ag * (gyy[c] + gs[c]) * inv2;
+                const float w = ag * gs[c] * inv2;
+                const float aul = __shfl_up_sync(FULL, a + u, 1);
+                const float ur = __shfl_down_sync(FULL, u, 1);
+                const float wr = __shfl_down_sync(FULL, w, 1);
+                const float wl = __shfl_up_sync(FULL, w, 1);
+                G0[c] += (-(a + b) - 2.f * (u + v - w)) + (aul + ur);
+                Gp[c] += (b + v) - wr;
+                Gm[c] += v - wl;
+                dxp[c] = dx[c];
+                dyp[c] = dy[c];
+                yv[c] = yn[c];
+            }
+            const int ro = t - 1;
+            if (outlane && ro >= ys && ro < ys + R && ro < H) {
+#pragma unroll
+                for (int c = 0; c < NCH; c++) {
+                    const float gv = Gm[c] + pr[c];
+                    gout[c * cs + (long long)ro * pitch] = gv;
+                    ssq[c] = fmaf(gv, gv, ssq[c]);
                 }
+            }
+#pragma unroll
+            for (int c = 0; c < NCH; c++) {
+                Gm[c] = G0[c];
+                G0[c] = Gp[c];
+                Gp[c] = 0.f;
             }
         }
     }
-    __syncthreads();
 
-    // Phase 2: gather the neighbours' scattered terms, write g, sum g^2.
-    float ss[3] = {0.f, 0.f, 0.f};
-    {
-        const int r = tid >> 3, c4 = (tid & 7) * 4;
-        const int gy = y0 + r, gx = x0 + c4;
-        const bool valid = gy < H && gx < W;
+    // Fixed-order reduction: warp tree, then warps in order, then blocks in order.
 #pragma unroll
-        for (int c = 0; c < 3; c++) {
-            if (c < nch) {
-                float go[4];
+    for (int c = 0; c < NCH; c++) {
+        float s = ssq[c];
 #pragma unroll
-                for (int j = 0; j < 4; j++) {
-                    const int col = c4 + j;
-                    const int ep = c * EH * EW + (r + 1) * EW + (col + 1);
-                    const float gv = P[c * TH * TILE_W + r * TILE_W + col] + AU[ep - 1] + U[ep + 1] + BV[ep - EW] +
-                                     V[ep + EW] - Wt[ep + EW - 1] - Wt[ep - EW + 1];
-                    go[j] = gv;
-                    ss[c] = fmaf(gv, gv, ss[c]);
-                }
-                if (valid)
-                    *reinterpret_cast<float4 *>(im.g + c * cs + (long long)gy * pitch + gx) =
-                        make_float4(go[0], go[1], go[2], go[3]);
-                else
-                    ss[c] = 0.f;
-            }
-        }
-    }
-    // Deterministic block reduction of the three sums.
-#pragma unroll
-    for (int c = 0; c < 3; c++) {
-        float s = ss[c];
-#pragma unroll
-        for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
-        if ((tid & 31) == 0) s_red[tid >> 5][c] = s;
+        for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(FULL, s, o);
+        if (lane == 0) s_red[warp][c] = s;
     }
     __syncthreads();
-    if (tid == 0) {
-        for (int c = 0; c < 3; c++) {
+    if (threadIdx.x == 0) {
+#pragma unroll
+        for (int c = 0; c < NCH; c++) {
             float s = 0.f;
-            for (int w = 0; w < NT / 32; w++) s += s_red[w][c];
-            im.partial[tm.y * 4 + c] = s;
+            for (int w = 0; w < SWEEP_WARPS; w++) s += s_red[w][c];
+            im.partial[wk.y * 4 + c] = s;
         }
         __threadfence();
-        const unsigned prevc = atomicAdd(im.counter, 1u);
-        s_last = prevc == (unsigned)(im.ntiles - 1);
+        const unsigned done = atomicAdd(im.counter, 1u);
+        s_last = done == (unsigned)(im.ncta - 1);
     }
     __syncthreads();
     if (s_last) {
-        // Last tile of the image: fixed-order fp64 sum of all tile sums.
         __threadfence();
-        double acc[3] = {0.0, 0.0, 0.0};
-        for (int t = tid; t < im.ntiles; t += NT) {
+        double acc[NCH];
 #pragma unroll
-            for (int c = 0; c < 3; c++) acc[c] += (double)__ldcg(im.partial + t * 4 + c);
+        for (int c = 0; c < NCH; c++) acc[c] = 0.0;
+        for (int t = threadIdx.x; t < im.ncta; t += SWEEP_WARPS * 32) {
+#pragma unroll
+            for (int c = 0; c < NCH; c++) acc[c] += (double)__ldcg(im.partial + t * 4 + c);
         }
 #pragma unroll
-        for (int c = 0; c < 3; c++) {
+        for (int c = 0; c < NCH; c++) {
             double s = acc[c];
 #pragma unroll
-            for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
-            if ((tid & 31) == 0) s_dred[tid >> 5][c] = s;
+            for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(FULL, s, o);
+            if (lane == 0) s_dred[warp][c] = s;
         }
         __syncthreads();
-        if (tid == 0) {
-            for (int c = 0; c < 3; c++) {
+        if (threadIdx.x == 0) {
+#pragma unroll
+            for (int c = 0; c < NCH; c++) {
                 double s = 0.0;
-                for (int w = 0; w < NT / 32; w++) s += s_dred[w][c];
+                for (int w = 0; w < SWEEP_WARPS; w++) s += s_dred[w][c];
                 const double nrm = sqrt(s);
                 im.sigma[c] = nrm > 0.0 ? (float)((double)im.step / nrm) : 0.f;
             }
@@ -318,195 +228,166 @@ __global__ void __launch_bounds__(TILE_W *TH / 4) k_gradient(const ImgDev *__res
     }
 }
 
-template <int TH>
-struct UpdLayout {
-    static constexpr int NT = TILE_W * TH / 4;
-    static constexpr int XS = 3 * TH * TILE_W;
-    static constexpr int SCS = 72;  // scratch floats per 8-lane group (64 + bank padding)
-    static constexpr int FLOATS = XS + (NT / 8) * SCS;
-    static constexpr size_t BYTES = FLOATS * sizeof(float);
-};
-
-// Descent step and projection onto the quantisation box
-// (compute_step.rs:60-71, compute_projection.rs:8-122).
-template <int TH>
-__global__ void __launch_bounds__(TILE_W *TH / 4) k_update(const ImgDev *__restrict__ imgs,
-                                                          const int2 *__restrict__ tilemap, int ntiles_total,
-                                                          int parity, float f, int reverse)
+// Descent step and projection of coefficient blocks (compute_step.rs:60-71,
+// compute_projection.rs:8-122), the next FISTA point, and the next
+// DCT-distance gradient (compute_step_prob.rs:20-57) from the clamped
+// coefficients the reference keeps as cos (compute_projection.rs:82).
+// One warp per task {image, channel, block row, first block} covering four
+// blocks; lane group g = lane / 8 takes block first + g, lane r = lane % 8 row r
+// of it (SV full-resolution rows of 8 SH pixels). Every global load of a lane
+// is issued before any arithmetic. Row-wise 1-D transforms alternate with 8x8
+// transposes in shared memory, in the reference's order (columns, then rows).
+template <int SH, int SV>
+__global__ void __launch_bounds__(PROJ_WARPS * 32) k_project(const ImgDev *__restrict__ imgs,
+                                                            const int4 *__restrict__ tasks, int ntasks, float fnext)
 {
-    using L = UpdLayout<TH>;
-    constexpr int NT = L::NT;
-    extern __shared__ float4 smem4[];
-    float *Xs = reinterpret_cast<float *>(smem4);
-    float *Sc = Xs + L::XS;
-    __shared__ float s_q[3][64];
-
-    const int tid = threadIdx.x;
-    const int bid = reverse ? ntiles_total - 1 - (int)blockIdx.x : (int)blockIdx.x;
-    const int2 tm = tilemap[bid];
-    const ImgDev &im = imgs[tm.x];
-    const int nch = im.nch, W = im.W, H = im.H, pitch = im.pitch;
-    const int tx = tm.y % im.tiles_x, ty = tm.y / im.tiles_x;
-    const int x0 = tx * TILE_W, y0 = ty * TH;
+    constexpr bool SUB = SH * SV > 1;
+    constexpr int NV = 8 * SH;  // pixels per full-resolution row of a lane
+    __shared__ float s_t[PROJ_WARPS][2][4][8][9];
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int w = blockIdx.x * PROJ_WARPS + warp;
+    if (w >= ntasks) return;  // warp-uniform
+    const int4 tk = tasks[w];
+    const ImgDev &im = imgs[tk.x];
+    const int c = tk.y, by = tk.z, grp = lane >> 3, r = lane & 7;
+    const int bx = tk.w + grp;
+    const ChanDev &cd = im.ch[c];
+    const bool act = bx < cd.cw / 8;
+    float(*T0)[9] = s_t[warp][0][grp];
+    float(*T1)[9] = s_t[warp][1][grp];
     const long long cs = im.cstride;
-    const float *cur = im.x[parity];
-    float *prev = im.x[parity ^ 1];
+    const int pitch = im.pitch;
+    float *xw = im.x + c * cs, *yw = im.y + c * cs;
+    const float *gb = im.g + c * cs;
+    const float sg = im.sigma[c];
+    const float ap = cd.alpha_p;  // warp-uniform
+    const int bxa = act ? bx : 0;
+    const long long o0 = (long long)(by * 8 * SV + r * SV) * pitch + bxa * 8 * SH;
 
-    for (int i = tid; i < nch * 64; i += NT) s_q[i >> 6][i & 63] = im.q[i >> 6][i & 63];
-
-    const int r = tid >> 3, c4 = (tid & 7) * 4;
-    const int gy = y0 + r, gx = x0 + c4;
-    const bool valid = gy < H && gx < W;
-    const long long o = (long long)gy * pitch + gx;
-    if (valid) {
+    // All loads first: y, g and x of the lane's rows, its coefficient row and quantisation steps.
+    float yv[SV][NV], gv[SV][NV], xo[SV][NV];
 #pragma unroll
-        for (int c = 0; c < 3; c++) {
-            if (c < nch) {
-                const float sg = im.sigma[c];
-                const float4 a = __ldg(reinterpret_cast<const float4 *>(cur + c * cs + o));
-                const float4 b = *reinterpret_cast<const float4 *>(prev + c * cs + o);
-                const float4 g = __ldg(reinterpret_cast<const float4 *>(im.g + c * cs + o));
-                float4 xo;
-                xo.x = fmaf(-sg, g.x, fmaf(f, a.x - b.x, a.x));
-                xo.y = fmaf(-sg, g.y, fmaf(f, a.y - b.y, a.y));
-                xo.z = fmaf(-sg, g.z, fmaf(f, a.z - b.z, a.z));
-                xo.w = fmaf(-sg, g.w, fmaf(f, a.w - b.w, a.w));
-                *reinterpret_cast<float4 *>(&Xs[c * TH * TILE_W + r * TILE_W + c4]) = xo;
-            }
+    for (int sy = 0; sy < SV; sy++)
+#pragma unroll
+        for (int q4 = 0; q4 < NV / 4; q4++) {
+            const long long o = o0 + (long long)sy * pitch + 4 * q4;
+            const float4 a = *reinterpret_cast<const float4 *>(yw + o);
+            const float4 b = __ldg(reinterpret_cast<const float4 *>(gb + o));
+            const float4 x = *reinterpret_cast<const float4 *>(xw + o);
+            yv[sy][4 * q4] = a.x, yv[sy][4 * q4 + 1] = a.y, yv[sy][4 * q4 + 2] = a.z, yv[sy][4 * q4 + 3] = a.w;
+            gv[sy][4 * q4] = b.x, gv[sy][4 * q4 + 1] = b.y, gv[sy][4 * q4 + 2] = b.z, gv[sy][4 * q4 + 3] = b.w;
+            xo[sy][4 * q4] = x.x, xo[sy][4 * q4 + 1] = x.y, xo[sy][4 * q4 + 2] = x.z, xo[sy][4 * q4 + 3] = x.w;
         }
+    float co[8], qv[8], iq[8];
+    load_coef_row(cd.coef + (long long)(by * 8 + r) * cd.cpitch + bxa * 8, co);
+#pragma unroll
+    for (int u = 0; u < 8; u++) {
+        qv[u] = __ldg(&im.q[c][r * 8 + u]);
+        iq[u] = __ldg(&im.invq2[c][r * 8 + u]);
     }
-    __syncthreads();
 
-    {
-        const int ntask = count_tasks<TH>(im);
-        const int lane8 = tid & 7, grp = tid >> 3;
-        float *S = Sc + grp * L::SCS;
-        for (int base = 0; base < ntask; base += NT / 8) {
-            const CellTask t = get_task<TH>(im, base + grp);
-            const bool act = t.c >= 0 && (x0 + t.cx0) < W && (y0 + t.cy0) < H;
-            const int cc = act ? t.c : 0;
-            const int sh = im.ch[cc].sh, sv = im.ch[cc].sv;
-            float *X = Xs + cc * TH * TILE_W;
-            float v[8];
-            if (act) {
-                if (sh * sv == 1) {
+    // x' = y - sigma g; cell means for subsampled components, summed sample by
+    // sample (compute_projection.rs:18-32).
+    float m[8], mean[8];
 #pragma unroll
-                    for (int k = 0; k < 8; k++) v[k] = X[(t.cy0 + k) * TILE_W + t.cx0 + lane8];
-                } else {
-                    // compute_projection.rs:18-47: mean over the cell, keep the residual.
-                    const float inv = 1.f / (float)(sh * sv);
+    for (int u = 0; u < 8; u++) mean[u] = 0.f;
 #pragma unroll
-                    for (int k = 0; k < 8; k++) {
-                        float m = 0.f;
-                        for (int sy = 0; sy < sv; sy++)
-                            for (int sx = 0; sx < sh; sx++) m += X[(t.cy0 + k * sv + sy) * TILE_W + t.cx0 + lane8 * sh + sx];
-                        m *= inv;
-                        for (int sy = 0; sy < sv; sy++)
-                            for (int sx = 0; sx < sh; sx++) X[(t.cy0 + k * sv + sy) * TILE_W + t.cx0 + lane8 * sh + sx] -= m;
-                        v[k] = m;
-                    }
-                }
-                dct8(v);
+    for (int sy = 0; sy < SV; sy++)
 #pragma unroll
-                for (int k = 0; k < 8; k++) S[k * 8 + lane8] = v[k];
-            }
-            __syncwarp();
-            if (act) {
-#pragma unroll
-                for (int u = 0; u < 8; u++) v[u] = S[lane8 * 8 + u];
-                dct8(v);
-                const ChanDev &cd = im.ch[cc];
-                const int bx = (x0 + t.cx0) / (8 * sh), by = (y0 + t.cy0) / (8 * sv);
-                float co[8];
-                load_coef_row(cd.coef + (long long)(by * 8 + lane8) * cd.cpitch + bx * 8, co);
-#pragma unroll
-                for (int u = 0; u < 8; u++) {
-                    const float q = s_q[cc][lane8 * 8 + u];
-                    v[u] = fminf(fmaxf(v[u], (co[u] - 0.5f) * q), (co[u] + 0.5f) * q);
-                }
-                idct8(v);
-#pragma unroll
-                for (int u = 0; u < 8; u++) S[lane8 * 8 + u] = v[u];
-            }
-            __syncwarp();
-            if (act) {
-#pragma unroll
-                for (int k = 0; k < 8; k++) v[k] = S[k * 8 + lane8];
-                idct8(v);
-                if (sh * sv == 1) {
-#pragma unroll
-                    for (int k = 0; k < 8; k++) X[(t.cy0 + k) * TILE_W + t.cx0 + lane8] = v[k];
-                } else {
-#pragma unroll
-                    for (int k = 0; k < 8; k++)
-                        for (int sy = 0; sy < sv; sy++)
-                            for (int sx = 0; sx < sh; sx++) X[(t.cy0 + k * sv + sy) * TILE_W + t.cx0 + lane8 * sh + sx] += v[k];
-                }
-            }
-            __syncwarp();
+        for (int i = 0; i < NV; i++) {
+            yv[sy][i] = fmaf(-sg, gv[sy][i], yv[sy][i]);
+            mean[i / SH] += yv[sy][i];
         }
-    }
-    __syncthreads();
-
-    if (valid) {
 #pragma unroll
-        for (int c = 0; c < 3; c++)
-            if (c < nch)
-                *reinterpret_cast<float4 *>(prev + c * cs + o) =
-                    *reinterpret_cast<const float4 *>(&Xs[c * TH * TILE_W + r * TILE_W + c4]);
+    for (int u = 0; u < 8; u++) {
+        if (SUB) mean[u] /= (float)(SH * SV);
+        m[u] = mean[u];
     }
+    // DCT (dct8x8s order: columns, then rows).
+    transpose8(T0, r, m);
+    dct8(m);
+    transpose8(T0, r, m);
+    dct8(m);
+    // Clamp (compute_projection.rs:72-79) and (cos - c q) / q^2.
+    float d[8];
+#pragma unroll
+    for (int u = 0; u < 8; u++) {
+        const float cl = fminf(fmaxf(m[u], (co[u] - 0.5f) * qv[u]), (co[u] + 0.5f) * qv[u]);
+        m[u] = cl;
+        d[u] = (cl - co[u] * qv[u]) * iq[u];
+    }
+    // IDCT of the clamped coefficients and of d (idct8x8s order: columns, then rows).
+    transpose8(T0, r, m);
+    if (ap != 0.f) transpose8(T1, r, d);
+    idct8(m);
+    if (ap != 0.f) idct8(d);
+    transpose8(T0, r, m);
+    if (ap != 0.f) transpose8(T1, r, d);
+    idct8(m);
+    if (!act) return;
+    if (ap != 0.f) {
+        idct8(d);
+        float4 *pr = reinterpret_cast<float4 *>(cd.P + (long long)(by * 8 + r) * cd.ppitch + bx * 8);
+        pr[0] = make_float4(ap * d[0], ap * d[1], ap * d[2], ap * d[3]);
+        pr[1] = make_float4(ap * d[4], ap * d[5], ap * d[6], ap * d[7]);
+    }
+    // x_{k+1}: the projected block, or for subsampled components the residual
+    // x' - mean plus the projected mean (compute_projection.rs:108-121); then
+    // y_{k+1} = x_{k+1} + f (x_{k+1} - x_k) (mod.rs:54-57).
+#pragma unroll
+    for (int sy = 0; sy < SV; sy++)
+#pragma unroll
+        for (int q4 = 0; q4 < NV / 4; q4++) {
+            float xn[4], yn[4];
+#pragma unroll
+            for (int i = 0; i < 4; i++) {
+                const int k = 4 * q4 + i, u = k / SH;
+                xn[i] = SUB ? (yv[sy][k] - mean[u]) + m[u] : m[u];
+                yn[i] = fmaf(fnext, xn[i] - xo[sy][k], xn[i]);
+            }
+            const long long o = o0 + (long long)sy * pitch + 4 * q4;
+            *reinterpret_cast<float4 *>(xw + o) = make_float4(xn[0], xn[1], xn[2], xn[3]);
+            *reinterpret_cast<float4 *>(yw + o) = make_float4(yn[0], yn[1], yn[2], yn[3]);
+        }
 }
 
 // Initial image (coef.rs:24-92 with the single unboxing of
 // pipeline_simd_adaptive/coef.rs:69-95): IDCT of c*q per block, nearest
-// upsampling to full resolution, written to both state buffers (aux.rs:62-63).
-template <int TH>
-__global__ void __launch_bounds__(TILE_W *TH / 4) k_init(const ImgDev *__restrict__ imgs,
-                                                        const int2 *__restrict__ tilemap)
+// upsampling to full resolution, written as x_0 and y_0 (aux.rs:62-63).
+// Same lane layout as k_project.
+__global__ void __launch_bounds__(PROJ_WARPS * 32) k_init(const ImgDev *__restrict__ imgs,
+                                                         const int4 *__restrict__ tasks, int ntasks)
 {
-    constexpr int NT = TILE_W * TH / 4;
-    __shared__ float Sc[NT / 8][72];
-    const int tid = threadIdx.x;
-    const int2 tm = tilemap[blockIdx.x];
-    const ImgDev &im = imgs[tm.x];
-    const int W = im.W, H = im.H, pitch = im.pitch;
-    const int tx = tm.y % im.tiles_x, ty = tm.y / im.tiles_x;
-    const int x0 = tx * TILE_W, y0 = ty * TH;
-    const int ntask = count_tasks<TH>(im);
-    const int lane8 = tid & 7, grp = tid >> 3;
-    for (int base = 0; base < ntask; base += NT / 8) {
-        const CellTask t = get_task<TH>(im, base + grp);
-        const bool act = t.c >= 0 && (x0 + t.cx0) < W && (y0 + t.cy0) < H;
-        const int cc = act ? t.c : 0;
-        const ChanDev &cd = im.ch[cc];
-        const int sh = cd.sh, sv = cd.sv;
-        const int bx = (x0 + t.cx0) / (8 * sh), by = (y0 + t.cy0) / (8 * sv);
-        float v[8];
-        if (act) {
+    __shared__ float s_t[PROJ_WARPS][4][8][9];
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int w = blockIdx.x * PROJ_WARPS + warp;
+    if (w >= ntasks) return;
+    const int4 tk = tasks[w];
+    const ImgDev &im = imgs[tk.x];
+    const int c = tk.y, by = tk.z, grp = lane >> 3, r = lane & 7;
+    const int bx = tk.w + grp;
+    const ChanDev &cd = im.ch[c];
+    const bool act = bx < cd.cw / 8;
+    float(*T)[9] = s_t[warp][grp];
+    float a[8], co[8];
+    load_coef_row(cd.coef + (long long)(by * 8 + r) * cd.cpitch + (act ? bx : 0) * 8, co);
 #pragma unroll
-            for (int k = 0; k < 8; k++)
-                v[k] = (float)cd.coef[(long long)(by * 8 + k) * cd.cpitch + bx * 8 + lane8] * im.q[cc][k * 8 + lane8];
-            idct8(v);
+    for (int u = 0; u < 8; u++) a[u] = co[u] * __ldg(&im.q[c][r * 8 + u]);
+    transpose8(T, r, a);
+    idct8(a);
+    transpose8(T, r, a);
+    idct8(a);
+    if (!act) return;
+    const int sh = cd.sh, sv = cd.sv;
+    const long long base = c * im.cstride;
+    for (int sy = 0; sy < sv; sy++) {
+        const long long o = base + (long long)(by * 8 * sv + r * sv + sy) * im.pitch + bx * 8 * sh;
 #pragma unroll
-            for (int k = 0; k < 8; k++) Sc[grp][k * 8 + lane8] = v[k];
-        }
-        __syncwarp();
-        if (act) {
-#pragma unroll
-            for (int u = 0; u < 8; u++) v[u] = Sc[grp][lane8 * 8 + u];
-            idct8(v);
-            for (int sy = 0; sy < sv; sy++) {
-                const long long rowo = (long long)(y0 + t.cy0 + lane8 * sv + sy) * pitch;
-#pragma unroll
-                for (int u = 0; u < 8; u++)
-                    for (int sx = 0; sx < sh; sx++) {
-                        const long long off = cc * im.cstride + rowo + x0 + t.cx0 + u * sh + sx;
-                        im.x[0][off] = v[u];
-                        im.x[1][off] = v[u];
-                    }
+        for (int u = 0; u < 8; u++)
+            for (int sx = 0; sx < sh; sx++) {
+                im.x[o + u * sh + sx] = a[u];
+                im.y[o + u * sh + sx] = a[u];
             }
-        }
-        __syncwarp();
     }
 }
 
@@ -583,8 +464,8 @@ __global__ void k_upsample(const float *__restrict__ img, const ImgDev *__restri
     const int cy = min(y / cd.sv, cd.chh - 1), cx = min(x / cd.sh, cd.cw - 1);
     const float v = img[(long long)cy * cd.cw + cx];
     const long long off = c * im.cstride + (long long)y * im.pitch + x;
-    im.x[0][off] = v;
-    im.x[1][off] = v;
+    im.x[off] = v;
+    im.y[off] = v;
 }
 
 // Output stage of Artefact::process (lib.rs:159-211): luma + 128, YCbCr ->
@@ -683,14 +564,16 @@ std::vector<float> fista_factors(uint32_t iterations)
 }
 
 struct GraphKey {
-    int th = 0, ntiles = 0, nimg = 0;
+    int nch = 0, ncta = 0, ntasks = 0;
+    int mode_off[5] = {0, 0, 0, 0, 0};
     uint32_t iterations = 0;
     bool timing = false;
-    const void *desc = nullptr, *tilemap = nullptr;
+    const void *desc = nullptr, *work = nullptr, *tasks = nullptr;
     bool operator==(const GraphKey &o) const
     {
-        return th == o.th && ntiles == o.ntiles && nimg == o.nimg && iterations == o.iterations &&
-               timing == o.timing && desc == o.desc && tilemap == o.tilemap;
+        return nch == o.nch && ncta == o.ncta && ntasks == o.ntasks && iterations == o.iterations &&
+               timing == o.timing && desc == o.desc && work == o.work && tasks == o.tasks &&
+               std::equal(mode_off, mode_off + 5, o.mode_off);
     }
 };
 
@@ -701,18 +584,18 @@ struct GraphKey {
 struct ArtContext {
     int device = 0;
     cudaStream_t stream = nullptr;
-    art::DevBuf xbuf, gbuf, coefimg, stage, misc, desc, tilemap, compat, sepplanes, rgb;
-    art::ImgDev *h_desc = nullptr;  // pinned host copy of the descriptors
-    size_t h_desc_cap = 0;
-    std::vector<int2> h_tilemap;
+    art::DevBuf xbuf, gbuf, pbuf, coefimg, stage, misc, desc, work, tasks, compat, sepplanes, rgb;
+    art::ImgDev *h_desc = nullptr;  // host copy of the descriptor (pageable: copies of it are staged)
+    std::vector<int2> h_work;       // gradient-sweep blocks: {image, block index in image}
+    std::vector<int4> h_tasks;      // all block warps: {image, channel, block row, first block}
+    int mode_off[5] = {0, 0, 0, 0, 0};  // h_tasks sorted by sampling mode (1x1, 2x2, 2x1, 1x2)
     cudaGraphExec_t exec = nullptr;
     art::GraphKey key;
     bool timing = false;
     std::vector<cudaEvent_t> events;  // [0,1] loop; then 4 per iteration
     uint32_t timed_iterations = 0;
-    int last_th = 32;
-    int pending_error = 0;
-    float *final_planes = nullptr;  // device planes holding the result of the last solve
+    int strip_rows_override = 0;      // 0 = chosen per image size
+    float *final_planes = nullptr;    // device planes holding the result of the last solve
     int final_pitch = 0;
     long long final_cstride = 0;
 };
@@ -720,43 +603,23 @@ struct ArtContext {
 namespace art {
 namespace {
 
-int pick_tile_height(int W, int H)
+// Rows per gradient-sweep strip: enough strips to fill every SM several times
+// over, and as long as that allows so the 3 extra rows a strip reads stay small.
+int pick_strip_rows(const ArtContext *ctx, int W, int H)
 {
-    (void)W;
-    (void)H;
-    const char *env = getenv("ART_TILE_H");
-    if (env && atoi(env) == 16) return 16;
-    return 32;
+    if (ctx->strip_rows_override > 0) return ctx->strip_rows_override;
+    const char *env = getenv("ART_STRIP_ROWS");
+    if (env && atoi(env) > 0) return atoi(env);
+    const long long strips_x = (W + SWEEP_OUT - 1) / SWEEP_OUT;
+    int R = 128;
+    while (R > 16 && strips_x * ((H + R - 1) / R) < 148LL * 24) R /= 2;
+    return R;
 }
 
-// Raises the dynamic shared-memory limit of the tile kernels, once per device.
 int configure_kernels(int device)
 {
-    static std::mutex mu;
-    static std::vector<int> done;
-    std::lock_guard<std::mutex> lock(mu);
-    if ((int)done.size() <= device) done.resize(device + 1, 0);
-    if (done[device]) return ART_OK;
-    int status = ART_OK;
-    {
-        cudaError_t e = cudaFuncSetAttribute(k_gradient<32>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                             (int)GradLayout<32>::BYTES);
-        if (e == cudaSuccess)
-            e = cudaFuncSetAttribute(k_gradient<16>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                     (int)GradLayout<16>::BYTES);
-        if (e == cudaSuccess)
-            e = cudaFuncSetAttribute(k_update<32>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                     (int)UpdLayout<32>::BYTES);
-        if (e == cudaSuccess)
-            e = cudaFuncSetAttribute(k_update<16>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                     (int)UpdLayout<16>::BYTES);
-        if (e != cudaSuccess) {
-            set_error(std::string("cudaFuncSetAttribute: ") + cudaGetErrorString(e));
-            status = ART_ERR_CUDA;
-        }
-    }
-    if (status == ART_OK) done[device] = 1;
-    return status;
+    (void)device;
+    return ART_OK;
 }
 
 int validate(uint32_t nch, const ArtChannel *ch, float weight, const float *pweight, uint32_t W, uint32_t H)
@@ -790,40 +653,70 @@ int validate(uint32_t nch, const ArtChannel *ch, float weight, const float *pwei
 
 }  // namespace
 
+// Sampling mode of a component: 0 = 1x1, 1 = 2x2, 2 = 2x1 (h x v), 3 = 1x2.
+static int samp_mode(int sh, int sv) { return sh == 1 ? (sv == 1 ? 0 : 3) : (sv == 2 ? 1 : 2); }
+
+// Block tasks of one image grouped by sampling mode; inside a mode bottom
+// rows first and channels interleaved by full-resolution row band, so the
+// projection starts on the rows the gradient sweep touched last (still in L2).
+static void build_tasks(const ImgDev &d, int img, std::vector<int4> &out, int mode_off[5])
+{
+    struct Key {
+        int mode, row, c, by, bx0;
+    };
+    std::vector<Key> keys;
+    for (int c = 0; c < d.nch; c++) {
+        const ChanDev &cd = d.ch[c];
+        const int bw = cd.cw / 8, bh = cd.chh / 8;
+        for (int by = 0; by < bh; by++)
+            for (int bx0 = 0; bx0 < bw; bx0 += 4) keys.push_back({samp_mode(cd.sh, cd.sv), by * 8 * cd.sv, c, by, bx0});
+    }
+    std::stable_sort(keys.begin(), keys.end(), [](const Key &a, const Key &b) {
+        if (a.mode != b.mode) return a.mode < b.mode;
+        if (a.row != b.row) return a.row > b.row;
+        return a.c < b.c;
+    });
+    for (int m = 0; m < 5; m++) mode_off[m] = 0;
+    for (const Key &k : keys) {
+        out.push_back(make_int4(img, k.c, k.by, k.bx0));
+        mode_off[k.mode + 1]++;
+    }
+    for (int m = 1; m < 5; m++) mode_off[m] += mode_off[m - 1];
+}
+
 // Lays out buffers for one image, uploads descriptors, ingests coefficients
 // and queues the initialisation. `coef_src[c]` is a device pointer.
 static int prepare(ArtContext *ctx, uint32_t nch, const ArtChannel *ch, const void *const *coef_src, float weight,
                    const float *pweight, uint32_t iterations, uint32_t W, uint32_t H, int init_mode)
 {
     int rc;
-    const int th = pick_tile_height((int)W, (int)H);
     const int pitch = (int)align_up(W, 32);
     const size_t rows = align_up(H, 32);
     const long long cstride = (long long)pitch * (long long)rows;
-    const int tiles_x = (int)((W + TILE_W - 1) / TILE_W), tiles_y = (int)((H + th - 1) / th);
-    const int ntiles = tiles_x * tiles_y;
+    const int R = pick_strip_rows(ctx, (int)W, (int)H);
+    const int strips_x = (int)((W + SWEEP_OUT - 1) / SWEEP_OUT), strips_y = (int)((H + R - 1) / R);
+    const int nstrips = strips_x * strips_y;
+    const int ncta = (nstrips + SWEEP_WARPS - 1) / SWEEP_WARPS;
 
-    if ((rc = ctx->xbuf.ensure(2 * 3 * cstride * sizeof(float)))) return rc;
+    if ((rc = ctx->xbuf.ensure(2 * 3 * cstride * sizeof(float)))) return rc;  // x and y
     if ((rc = ctx->gbuf.ensure(3 * cstride * sizeof(float)))) return rc;
-    size_t coef_bytes = 0;
-    size_t coef_off[3];
-    int cpitch[3];
+    size_t coef_bytes = 0, p_floats = 0;
+    size_t coef_off[3], p_off[3];
+    int cpitch[3], ppitch[3];
     for (uint32_t c = 0; c < nch; c++) {
         cpitch[c] = (int)align_up(ch[c].rounded_px_w, 64);
         coef_off[c] = coef_bytes;
         coef_bytes += align_up((size_t)cpitch[c] * ch[c].rounded_px_h * sizeof(int16_t), 256);
+        ppitch[c] = (int)align_up(ch[c].rounded_px_w, 32);
+        p_off[c] = p_floats;
+        p_floats += align_up((size_t)ppitch[c] * ch[c].rounded_px_h, 64);
     }
     if ((rc = ctx->coefimg.ensure(coef_bytes))) return rc;
-    const size_t misc_bytes = align_up(ntiles * 4 * sizeof(float), 256) + 256;
+    if ((rc = ctx->pbuf.ensure(p_floats * sizeof(float)))) return rc;
+    const size_t misc_bytes = align_up((size_t)ncta * 4 * sizeof(float), 256) + 256;
     if ((rc = ctx->misc.ensure(misc_bytes))) return rc;
     if ((rc = ctx->desc.ensure(sizeof(ImgDev)))) return rc;
-    if ((rc = ctx->tilemap.ensure(ntiles * sizeof(int2)))) return rc;
-    if (!ctx->h_desc) {
-        // Pageable on purpose: cudaMemcpyAsync stages it before returning, so
-        // the next call may rewrite it while this solve is still queued.
-        ctx->h_desc = new ImgDev();
-        ctx->h_desc_cap = 1;
-    }
+    if (!ctx->h_desc) ctx->h_desc = new ImgDev();
 
     ImgDev &d = *ctx->h_desc;
     memset(&d, 0, sizeof(d));
@@ -831,13 +724,14 @@ static int prepare(ArtContext *ctx, uint32_t nch, const ArtChannel *ch, const vo
     d.W = (int)W;
     d.H = (int)H;
     d.pitch = pitch;
-    d.tiles_x = tiles_x;
-    d.tiles_y = tiles_y;
-    d.ntiles = ntiles;
-    d.th = th;
+    d.strips_x = strips_x;
+    d.strips_y = strips_y;
+    d.nstrips = nstrips;
+    d.strip_rows = R;
+    d.ncta = ncta;
     d.cstride = cstride;
-    d.x[0] = static_cast<float *>(ctx->xbuf.p);
-    d.x[1] = d.x[0] + 3 * cstride;
+    d.x = static_cast<float *>(ctx->xbuf.p);
+    d.y = d.x + 3 * cstride;
     d.g = static_cast<float *>(ctx->gbuf.p);
     // compute_step_tv.rs:130 and compute_step_tv2.rs:88-89, compute_step.rs:47.
     d.alpha_tv = 1.0f / sqrtf((float)nch);
@@ -847,7 +741,7 @@ static int prepare(ArtContext *ctx, uint32_t nch, const ArtChannel *ch, const vo
     d.step = radius / sqrtf(1.0f + (float)iterations);
     char *misc = static_cast<char *>(ctx->misc.p);
     d.partial = reinterpret_cast<float *>(misc);
-    d.sigma = reinterpret_cast<float *>(misc + align_up(ntiles * 4 * sizeof(float), 256));
+    d.sigma = reinterpret_cast<float *>(misc + align_up((size_t)ncta * 4 * sizeof(float), 256));
     d.counter = reinterpret_cast<unsigned *>(d.sigma + 4);
     unsigned *errflag = d.counter + 1;
     for (uint32_t c = 0; c < nch; c++) {
@@ -857,7 +751,9 @@ static int prepare(ArtContext *ctx, uint32_t nch, const ArtChannel *ch, const vo
         cd.sh = (int)ch[c].samp_h;
         cd.sv = (int)ch[c].samp_v;
         cd.cpitch = cpitch[c];
+        cd.ppitch = ppitch[c];
         cd.coef = reinterpret_cast<const int16_t *>(static_cast<char *>(ctx->coefimg.p) + coef_off[c]);
+        cd.P = static_cast<float *>(ctx->pbuf.p) + p_off[c];
         // compute_step.rs:20-31: alpha = pweight * 2 * 255 * sqrt(2).
         cd.alpha_p = pweight[c] * 2.0f * 255.0f * sqrtf(2.0f);
         for (int j = 0; j < 64; j++) {
@@ -866,15 +762,22 @@ static int prepare(ArtContext *ctx, uint32_t nch, const ArtChannel *ch, const vo
             d.invq2[c][j] = 1.0f / (q * q);
         }
     }
-    ctx->h_tilemap.resize(ntiles);
-    for (int t = 0; t < ntiles; t++) ctx->h_tilemap[t] = make_int2(0, t);
+    ctx->h_work.resize(ncta);
+    for (int i = 0; i < ncta; i++) ctx->h_work[i] = make_int2(0, i);
+    ctx->h_tasks.clear();
+    build_tasks(d, 0, ctx->h_tasks, ctx->mode_off);
+    const int ntasks = (int)ctx->h_tasks.size();
+    if ((rc = ctx->work.ensure(ncta * sizeof(int2)))) return rc;
+    if ((rc = ctx->tasks.ensure(ntasks * sizeof(int4)))) return rc;
 
     cudaStream_t s = ctx->stream;
     ART_CUDA(cudaMemcpyAsync(ctx->desc.p, &d, sizeof(ImgDev), cudaMemcpyHostToDevice, s));
-    ART_CUDA(cudaMemcpyAsync(ctx->tilemap.p, ctx->h_tilemap.data(), ntiles * sizeof(int2), cudaMemcpyHostToDevice, s));
+    ART_CUDA(cudaMemcpyAsync(ctx->work.p, ctx->h_work.data(), ncta * sizeof(int2), cudaMemcpyHostToDevice, s));
+    ART_CUDA(cudaMemcpyAsync(ctx->tasks.p, ctx->h_tasks.data(), ntasks * sizeof(int4), cudaMemcpyHostToDevice, s));
     ART_CUDA(cudaMemsetAsync(ctx->misc.p, 0, misc_bytes, s));
+    // The first DCT-distance gradient is zero: the reference starts from cos = c q (coef.rs:94-104).
+    ART_CUDA(cudaMemsetAsync(ctx->pbuf.p, 0, p_floats * sizeof(float), s));
     const ImgDev *ddesc = static_cast<const ImgDev *>(ctx->desc.p);
-    const int2 *dtm = static_cast<const int2 *>(ctx->tilemap.p);
     for (uint32_t c = 0; c < nch; c++) {
         const long long ncoef = (long long)ch[c].block_w * ch[c].block_h * 64;
         const int blocks = (int)((ncoef + 255) / 256);
@@ -898,44 +801,55 @@ static int prepare(ArtContext *ctx, uint32_t nch, const ArtChannel *ch, const vo
             k_upsample<<<(int)(((long long)W * H + 255) / 256), 256, 0, s>>>(a, ddesc, (int)c);
         }
     } else {
-        if (th == 16)
-            k_init<16><<<ntiles, GradLayout<16>::NT, 0, s>>>(ddesc, dtm);
-        else
-            k_init<32><<<ntiles, GradLayout<32>::NT, 0, s>>>(ddesc, dtm);
+        k_init<<<(ntasks + PROJ_WARPS - 1) / PROJ_WARPS, PROJ_WARPS * 32, 0, s>>>(
+            ddesc, static_cast<const int4 *>(ctx->tasks.p), ntasks);
     }
     ART_CUDA(cudaGetLastError());
-    ctx->last_th = th;
-    ctx->final_planes = d.x[iterations & 1];
+    ctx->final_planes = d.x;
     ctx->final_pitch = pitch;
     ctx->final_cstride = cstride;
     return ART_OK;
 }
 
-static void launch_iteration(ArtContext *ctx, int th, int ntiles, int it, float f)
+static void launch_iteration(ArtContext *ctx, int it, float fnext)
 {
+    const ImgDev &d = *ctx->h_desc;
     const ImgDev *ddesc = static_cast<const ImgDev *>(ctx->desc.p);
-    const int2 *dtm = static_cast<const int2 *>(ctx->tilemap.p);
+    const int2 *work = static_cast<const int2 *>(ctx->work.p);
+    const int4 *tasks = static_cast<const int4 *>(ctx->tasks.p);
+    const int ntasks = (int)ctx->h_tasks.size();
     cudaStream_t s = ctx->stream;
-    const int parity = it & 1;
     const bool tm = ctx->timing;
     if (tm) cudaEventRecordWithFlags(ctx->events[2 + 4 * it], s, cudaEventRecordExternal);
-    if (th == 16)
-        k_gradient<16><<<ntiles, GradLayout<16>::NT, GradLayout<16>::BYTES, s>>>(ddesc, dtm, parity, f);
+    if (d.nch == 3)
+        k_grad_sweep<3><<<d.ncta, SWEEP_WARPS * 32, 0, s>>>(ddesc, work);
+    else if (d.nch == 2)
+        k_grad_sweep<2><<<d.ncta, SWEEP_WARPS * 32, 0, s>>>(ddesc, work);
     else
-        k_gradient<32><<<ntiles, GradLayout<32>::NT, GradLayout<32>::BYTES, s>>>(ddesc, dtm, parity, f);
+        k_grad_sweep<1><<<d.ncta, SWEEP_WARPS * 32, 0, s>>>(ddesc, work);
     if (tm) cudaEventRecordWithFlags(ctx->events[3 + 4 * it], s, cudaEventRecordExternal);
     if (tm) cudaEventRecordWithFlags(ctx->events[4 + 4 * it], s, cudaEventRecordExternal);
-    if (th == 16)
-        k_update<16><<<ntiles, UpdLayout<16>::NT, UpdLayout<16>::BYTES, s>>>(ddesc, dtm, ntiles, parity, f, 1);
-    else
-        k_update<32><<<ntiles, UpdLayout<32>::NT, UpdLayout<32>::BYTES, s>>>(ddesc, dtm, ntiles, parity, f, 1);
+    (void)ntasks;
+    for (int m = 3; m >= 0; m--) {
+        const int n = ctx->mode_off[m + 1] - ctx->mode_off[m];
+        if (n == 0) continue;
+        const int4 *tk = tasks + ctx->mode_off[m];
+        const int grid = (n + PROJ_WARPS - 1) / PROJ_WARPS;
+        if (m == 0)
+            k_project<1, 1><<<grid, PROJ_WARPS * 32, 0, s>>>(ddesc, tk, n, fnext);
+        else if (m == 1)
+            k_project<2, 2><<<grid, PROJ_WARPS * 32, 0, s>>>(ddesc, tk, n, fnext);
+        else if (m == 2)
+            k_project<2, 1><<<grid, PROJ_WARPS * 32, 0, s>>>(ddesc, tk, n, fnext);
+        else
+            k_project<1, 2><<<grid, PROJ_WARPS * 32, 0, s>>>(ddesc, tk, n, fnext);
+    }
     if (tm) cudaEventRecordWithFlags(ctx->events[5 + 4 * it], s, cudaEventRecordExternal);
 }
 
 static int run_iterations(ArtContext *ctx, uint32_t iterations)
 {
     const ImgDev &d = *ctx->h_desc;
-    const int th = ctx->last_th, ntiles = d.ntiles;
     if (iterations == 0) return ART_OK;
     if (ctx->timing) {
         const size_t need = 2 + 4 * (size_t)iterations;
@@ -946,13 +860,15 @@ static int run_iterations(ArtContext *ctx, uint32_t iterations)
         }
     }
     GraphKey key;
-    key.th = th;
-    key.ntiles = ntiles;
-    key.nimg = 1;
+    key.nch = d.nch;
+    key.ncta = d.ncta;
+    key.ntasks = (int)ctx->h_tasks.size();
+    std::copy(ctx->mode_off, ctx->mode_off + 5, key.mode_off);
     key.iterations = iterations;
     key.timing = ctx->timing;
     key.desc = ctx->desc.p;
-    key.tilemap = ctx->tilemap.p;
+    key.work = ctx->work.p;
+    key.tasks = ctx->tasks.p;
     cudaStream_t s = ctx->stream;
     if (!ctx->exec || !(ctx->key == key)) {
         if (ctx->exec) {
@@ -963,7 +879,9 @@ static int run_iterations(ArtContext *ctx, uint32_t iterations)
         cudaGraph_t graph;
         ART_CUDA(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
         if (ctx->timing) cudaEventRecordWithFlags(ctx->events[0], s, cudaEventRecordExternal);
-        for (uint32_t it = 0; it < iterations; it++) launch_iteration(ctx, th, ntiles, (int)it, fs[it]);
+        // y_0 = x_0 (f_0 = 0); the projection of iteration k forms y_{k+1} with f_{k+1}.
+        for (uint32_t it = 0; it < iterations; it++)
+            launch_iteration(ctx, (int)it, it + 1 < iterations ? fs[it + 1] : 0.0f);
         if (ctx->timing) cudaEventRecordWithFlags(ctx->events[1], s, cudaEventRecordExternal);
         cudaError_t e = cudaStreamEndCapture(s, &graph);
         if (e != cudaSuccess) return fail(ART_ERR_CUDA, std::string("graph capture: ") + cudaGetErrorString(e));
@@ -1030,11 +948,13 @@ void art_context_destroy(ArtContext *ctx)
     for (auto e : ctx->events) cudaEventDestroy(e);
     ctx->xbuf.release();
     ctx->gbuf.release();
+    ctx->pbuf.release();
+    ctx->work.release();
+    ctx->tasks.release();
     ctx->coefimg.release();
     ctx->stage.release();
     ctx->misc.release();
     ctx->desc.release();
-    ctx->tilemap.release();
     ctx->compat.release();
     ctx->sepplanes.release();
     ctx->rgb.release();
@@ -1087,9 +1007,10 @@ int32_t art_context_compute_device(ArtContext *ctx, uint32_t nchannel, const Art
     if (init_mode != ART_INIT_DECODED && init_mode != ART_INIT_SCALAR_COMPAT)
         return fail(ART_ERR_INVALID_ARGUMENT, "unknown init mode");
     ART_CUDA(cudaSetDevice(ctx->device));
+    // `stream` NULL is the legacy default stream, as everywhere in CUDA.
     cudaStream_t user = static_cast<cudaStream_t>(stream);
     cudaEvent_t join = nullptr;
-    if (user && user != ctx->stream) {
+    if (user != ctx->stream) {
         // Order the context's stream after the caller's work.
         ART_CUDA(cudaEventCreateWithFlags(&join, cudaEventDisableTiming));
         ART_CUDA(cudaEventRecord(join, user));

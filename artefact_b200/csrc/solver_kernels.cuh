@@ -1,21 +1,26 @@
 // Device code of the B200 restoration solver.
 //
 // One solver iteration of backend/artefact-lib/pipeline_scalar (mod.rs:49-75,
-// compute_step.rs:8-72) runs as two kernels over 32 x TH pixel tiles of every
-// channel at once:
-//   k_gradient  FISTA extrapolation y = x_k + f (x_k - x_{k-1}) on the tile and a
-//               2-pixel halo; the channel-coupled TV (compute_step_tv.rs:29-93)
-//               and TGV (compute_step_tv2.rs:32-136) gradients, written as a
-//               gather of the reference's scatter; the DCT-distance gradient
-//               (compute_step_prob.rs:5-60) with the lagged coefficients
-//               recomputed as the clamped DCT of x_k; writes g and the tile's
-//               sum of g^2 per channel; the last tile of an image reduces those
-//               sums in a fixed order and stores sigma_c = step / ||g_c||.
-//   k_update    y again, x' = y - sigma_c g (compute_step.rs:52-66), then the
-//               projection onto the quantisation box per 8x8 coefficient block
-//               (compute_projection.rs:8-122): mean-pool for subsampled
-//               components, DCT, clamp to [(c-1/2)q, (c+1/2)q], IDCT, add the
-//               residual back; writes x_{k+1} over x_{k-1}.
+// compute_step.rs:8-72) runs as two kernels:
+//   k_grad_sweep  one warp walks down a 28-column strip of all channels (32
+//                 lanes with a 2-column halo) of the FISTA point y_k, keeping a
+//                 rolling window in registers: channel-coupled TV (compute_step_tv.rs:29-93)
+//                 and TGV (compute_step_tv2.rs:32-136) gradients written as a
+//                 gather of the reference's scatter (horizontal neighbours by
+//                 warp shuffles), plus the DCT-distance gradient plane the last
+//                 projection left (compute_step_prob.rs:5-60); writes g and
+//                 sums g^2 per channel; the last block of an image reduces the
+//                 sums in a fixed order and stores sigma_c = step / ||g_c||.
+//   k_project     eight lanes per 8x8 coefficient block (lane = block row; a
+//                 16x16 / 16x8 cell of full-resolution pixels for subsampled
+//                 components), transposes through shared memory:
+//                 x' = y_k - sigma_c g (compute_step.rs:60-66), mean pooling,
+//                 DCT, clamp to [(c-1/2)q, (c+1/2)q], IDCT, residual
+//                 (compute_projection.rs:8-122); writes x_{k+1} over x_k and the
+//                 next FISTA point y_{k+1} = x_{k+1} + f_{k+1} (x_{k+1} - x_k)
+//                 (mod.rs:50-59) over y_k, and, from the clamped coefficients it
+//                 keeps (the reference's cos, compute_projection.rs:82), the next
+//                 DCT-distance gradient alpha_p * IDCT((cos - c q) / q^2).
 // The 8x8 transforms are Ooura's separable butterflies (utils/dct.rs:30-169).
 #pragma once
 
@@ -24,32 +29,38 @@
 
 namespace art {
 
-constexpr int TILE_W = 32;
-
 struct ChanDev {
     int cw, chh;   // component plane size (rounded_px_w/h)
     int sh, sv;    // sampling factors relative to the max (1 or 2)
     int cpitch;    // int16 elements per row of the coefficient image
-    int pad0;
+    int ppitch;    // floats per row of the DCT-distance gradient plane
     const int16_t *coef;  // coefficient image: coef(8by+v, 8bx+u) = block (bx,by), index v*8+u
+    float *P;             // alpha_p * IDCT((cos - c q) / q^2) at component resolution
     float alpha_p;        // pweight * 2 * 255 * sqrt(2); 0 disables the DCT-distance term
     float pad1;
 };
 
 struct ImgDev {
     int nch, W, H, pitch;  // full-resolution plane size; pitch in floats
-    int tiles_x, tiles_y, ntiles, th;
+    int strips_x, strips_y, nstrips, strip_rows;  // gradient sweep strips (28 columns x strip_rows)
+    int ncta;              // gradient-sweep blocks of this image
+    int pad0;
     long long cstride;     // floats between channel planes
-    float *x[2];           // state buffers; channel c at x[b] + c * cstride
+    float *x;              // iterate x_k; channel c at x + c * cstride
+    float *y;              // FISTA point y_k = x_k + f_k (x_k - x_{k-1})
     float *g;              // gradient planes
     float alpha_tv, alpha_tgv, step, pad;
     float *sigma;          // [4] per channel step / ||g||
-    float *partial;        // [ntiles * 4] per-tile sums of g^2
-    unsigned int *counter; // tiles done in the current iteration
+    float *partial;        // [ncta * 4] per-block sums of g^2
+    unsigned int *counter; // sweep blocks done in the current iteration
     ChanDev ch[3];
     float q[3][64];
     float invq2[3][64];
 };
+
+constexpr int SWEEP_OUT = 28;   // output columns per warp strip
+constexpr int SWEEP_WARPS = 8;  // warps (strips) per sweep block
+constexpr int PROJ_WARPS = 4;   // warps per projection block (4 coefficient blocks per warp)
 
 // ---------------------------------------------------------------- transforms
 #define ART_C1R 0.49039264020161522456f
@@ -123,8 +134,7 @@ __device__ __forceinline__ void dct8(float *a)
     a[5] = ART_C3R * x3i + ART_C3I * x3r;
 }
 
-// Clamp one row of 8 DCT coefficients (v = row) to their quantisation
-// intervals; returns the clamped values in a[] (compute_projection.rs:72-79).
+// The 8 quantised coefficients of one block row (int16) as floats.
 __device__ __forceinline__ void load_coef_row(const int16_t *row, float *c)
 {
     const uint4 raw = *reinterpret_cast<const uint4 *>(row);
@@ -136,37 +146,48 @@ __device__ __forceinline__ void load_coef_row(const int16_t *row, float *c)
     }
 }
 
-// Cell tasks: one 8x8 coefficient block of one channel, covering an
-// (8 sh) x (8 sv) full-resolution cell, handled by 8 consecutive lanes.
-struct CellTask {
-    int c, cx0, cy0;  // channel, cell origin inside the tile (full resolution)
-};
-
-template <int TH>
-__device__ __forceinline__ int count_tasks(const ImgDev &im)
+// 2-D transforms of a register-resident 8x8 block, columns first then rows,
+// as dct8x8s / idct8x8s do (utils/dct.rs:30-169).
+__device__ __forceinline__ void dct8x8_regs(float *a)
 {
-    int n = 0;
-    for (int c = 0; c < im.nch; c++) n += (TILE_W / (8 * im.ch[c].sh)) * (TH / (8 * im.ch[c].sv));
-    return n;
+#pragma unroll
+    for (int j = 0; j < 8; j++) {
+        float v[8];
+#pragma unroll
+        for (int k = 0; k < 8; k++) v[k] = a[k * 8 + j];
+        dct8(v);
+#pragma unroll
+        for (int k = 0; k < 8; k++) a[k * 8 + j] = v[k];
+    }
+#pragma unroll
+    for (int j = 0; j < 8; j++) dct8(a + j * 8);
 }
 
-template <int TH>
-__device__ __forceinline__ CellTask get_task(const ImgDev &im, int t)
+__device__ __forceinline__ void idct8x8_regs(float *a)
 {
-    CellTask r{0, 0, 0};
-    for (int c = 0; c < im.nch; c++) {
-        int sh = im.ch[c].sh, sv = im.ch[c].sv;
-        int ncx = TILE_W / (8 * sh), n = ncx * (TH / (8 * sv));
-        if (t < n) {
-            r.c = c;
-            r.cx0 = (t % ncx) * 8 * sh;
-            r.cy0 = (t / ncx) * 8 * sv;
-            return r;
-        }
-        t -= n;
+#pragma unroll
+    for (int j = 0; j < 8; j++) {
+        float v[8];
+#pragma unroll
+        for (int k = 0; k < 8; k++) v[k] = a[k * 8 + j];
+        idct8(v);
+#pragma unroll
+        for (int k = 0; k < 8; k++) a[k * 8 + j] = v[k];
     }
-    r.c = -1;
-    return r;
+#pragma unroll
+    for (int j = 0; j < 8; j++) idct8(a + j * 8);
+}
+
+// 8x8 transpose among the 8 lanes (r = lane & 7) of a lane group through a
+// 8x9 shared scratch: a lane holding row r leaves holding column r, and back.
+__device__ __forceinline__ void transpose8(float (*T)[9], int r, float *v)
+{
+    __syncwarp();
+#pragma unroll
+    for (int u = 0; u < 8; u++) T[r][u] = v[u];
+    __syncwarp();
+#pragma unroll
+    for (int k = 0; k < 8; k++) v[k] = T[k][r];
 }
 
 }  // namespace art

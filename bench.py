@@ -304,19 +304,20 @@ def main():
     u_launch = statistics.mean(upd_ms) / iters
     loop = statistics.mean(loop_ms)
 
-    # Algorithmic bytes (per launch): gradient kernel reads x_k, x_{k-1} and the
-    # int16 coefficients and writes g; update kernel reads x_k, x_{k-1}, g and the
-    # coefficients and writes x_{k+1}.
+    # Algorithmic bytes (per launch): the gradient sweep reads x_k, x_{k-1} and
+    # the DCT-distance gradient plane (component resolution) and writes g; the
+    # projection reads x_k, x_{k-1}, g and the int16 coefficients and writes
+    # x_{k+1} and the next DCT-distance gradient plane.
     n_full = W * H
     nc = [c.rounded_px_w * c.rounded_px_h for c in jpeg.coefs]
-    grad_bytes = sum(12 * n_full + 2 * x for x in nc)
-    upd_bytes = sum(16 * n_full + 2 * x for x in nc)
+    grad_bytes = sum(12 * n_full + 4 * x for x in nc)
+    upd_bytes = sum(16 * n_full + 6 * x for x in nc)
     iter_bytes = sum(20 * n_full + 4 * x for x in nc)  # two-sweep minimum per iteration
     peak, peak_kind = load_peaks()
     if g_launch >= u_launch:
-        dom, dbytes, dms = "k_gradient", grad_bytes, g_launch
+        dom, dbytes, dms = "k_grad_sweep", grad_bytes, g_launch
     else:
-        dom, dbytes, dms = "k_update", upd_bytes, u_launch
+        dom, dbytes, dms = "k_project", upd_bytes, u_launch
     achieved = dbytes / (dms * 1e-3) / 1e9
     traffic = None
     tf = ROOT / "profiles" / "traffic.json"
@@ -335,7 +336,8 @@ def main():
                "sample": "one full solve of the workload (50 iterations) by the fp32 C restatement of "
                          "pipeline_scalar on one host thread"}
 
-    gpu_launches = args.steps * (nch + 1 + 2 * iters)
+    modes = len({(c.horizontal_samp_factor, c.vertical_samp_factor) for c in jpeg.coefs})
+    gpu_launches = args.steps * (nch + 1 + (1 + modes) * iters)
     if rank == 0:
         line = {
             "metric": METRIC, "value": value, "unit": "MPix/s", "n_gpus": world, "steps": args.steps,

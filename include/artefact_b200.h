@@ -94,8 +94,10 @@ int32_t art_context_compute(ArtContext *ctx, uint32_t nchannel, const ArtChannel
 /*
  * Device-resident variant: ArtChannel.dct_coefs points to device memory (the
  * 64-entry quant_table stays a host pointer), out_planes_device[c] to device buffers of max_rounded_px_h rows of
- * out_pitch floats. Work is queued on `stream` (a cudaStream_t, NULL = the
- * context's own stream) and this call returns without synchronising.
+ * out_pitch floats. The work runs on the context's stream, ordered after the
+ * work already queued on `stream` (a cudaStream_t; NULL is the legacy default
+ * stream) and before anything queued on `stream` afterwards; the call returns
+ * without synchronising.
  * Replaces the same reference entry point as art_compute.
  */
 int32_t art_context_compute_device(ArtContext *ctx, uint32_t nchannel, const ArtChannel *coefs, float weight,
