@@ -65,39 +65,38 @@ __global__ void __launch_bounds__(SWEEP_WARPS * 32) k_grad_sweep(const ImgDev *_
         const int cx = min(max(gx, 0), W - 1);
         const bool colin = gx >= 0 && gx < W;
         const bool outlane = lane >= 2 && lane < 30 && gx < W;
+        const int cs = (int)im.cstride;
         const float *yp = im.y + cx;
         float *gout = im.g + (outlane ? gx : 0);
         const float at = im.alpha_tv, ag = im.alpha_tgv;
-        auto rowoff = [&](int row) -> long long { return (long long)min(max(row, 0), H - 1) * pitch; };
         // DCT-distance gradient plane of each channel at this lane's column,
         // prefetched two output rows ahead like y.
         const float *pcol[NCH];
-        int psv[NCH], ppitch[NCH];
+        int psh[NCH], ppitch[NCH];
         bool pon[NCH];
 #pragma unroll
         for (int c = 0; c < NCH; c++) {
             const ChanDev &cd = im.ch[c];
             pon[c] = cd.alpha_p != 0.f;
-            psv[c] = cd.sv;
+            psh[c] = cd.sv - 1;
             ppitch[c] = cd.ppitch;
-            pcol[c] = cd.P + (outlane ? gx / cd.sh : 0);
+            pcol[c] = cd.P + (outlane ? (gx >> (cd.sh - 1)) : 0);
         }
-        auto pload = [&](int c, int row) -> float {
-            const int rr = min(max(row, 0), H - 1);
-            return pon[c] ? __ldg(pcol[c] + (long long)(rr / psv[c]) * ppitch[c]) : 0.f;
-        };
+        const int Hm1 = H - 1;
+        auto yrow = [&](int row) -> int { return min(max(row, 0), Hm1) * pitch; };
 
         float yv[NCH], dxp[NCH], dyp[NCH], Gm[NCH], G0[NCH], Gp[NCH], q1[NCH], q2[NCH], p1[NCH], p2[NCH];
         {
-            const long long o0 = rowoff(ys - 2), o1 = rowoff(ys - 1), o2 = rowoff(ys), o3 = rowoff(ys + 1);
+            const int o0 = yrow(ys - 2), o1 = yrow(ys - 1), o2 = yrow(ys), o3 = yrow(ys + 1);
+            const int r0 = max(ys - 2, 0), r1 = max(ys - 1, 0);
 #pragma unroll
             for (int c = 0; c < NCH; c++) {
                 const float y0 = __ldg(yp + c * cs + o0);
                 yv[c] = __ldg(yp + c * cs + o1);
                 q1[c] = __ldg(yp + c * cs + o2);
                 q2[c] = __ldg(yp + c * cs + o3);
-                p1[c] = pload(c, ys - 2);  // output row of step t = ys - 1
-                p2[c] = pload(c, ys - 1);
+                p1[c] = pon[c] ? __ldg(pcol[c] + (r0 >> psh[c]) * ppitch[c]) : 0.f;  // output row of step ys - 1
+                p2[c] = pon[c] ? __ldg(pcol[c] + (r1 >> psh[c]) * ppitch[c]) : 0.f;
                 dxp[c] = __shfl_down_sync(FULL, y0, 1) - y0;
                 dyp[c] = yv[c] - y0;
                 Gm[c] = G0[c] = Gp[c] = 0.f;
@@ -106,7 +105,8 @@ __global__ void __launch_bounds__(SWEEP_WARPS * 32) k_grad_sweep(const ImgDev *_
         for (int t = ys - 1; t <= ys + R; t++) {
             float yn[NCH], pr[NCH];
             {
-                const long long o = rowoff(t + 3);
+                const int o = min(t + 3, Hm1) * pitch;
+                const int pr1 = min(t + 1, Hm1);
 #pragma unroll
                 for (int c = 0; c < NCH; c++) {
                     yn[c] = q1[c];
@@ -114,7 +114,7 @@ __global__ void __launch_bounds__(SWEEP_WARPS * 32) k_grad_sweep(const ImgDev *_
                     q2[c] = __ldg(yp + c * cs + o);
                     pr[c] = p1[c];
                     p1[c] = p2[c];
-                    p2[c] = pload(c, t + 1);
+                    p2[c] = pon[c] ? __ldg(pcol[c] + (pr1 >> psh[c]) * ppitch[c]) : 0.f;
                 }
             }
             const bool inside = colin && t >= 0 && t < H;
@@ -127,13 +127,16 @@ __global__ void __launch_bounds__(SWEEP_WARPS * 32) k_grad_sweep(const ImgDev *_
                 n1 += dx[c] * dx[c];
                 n1 += dy[c] * dy[c];
             }
+            const bool tx0 = gx > 0, ty0 = t > 0;
 #pragma unroll
             for (int c = 0; c < NCH; c++) {
-                const float dxl = __shfl_up_sync(FULL, dx[c], 1), dyl = __shfl_up_sync(FULL, dy[c], 1);
-                const float axx = gx > 0 ? dx[c] - dxl : 0.f;
-                const float ayx = gx > 0 ? dy[c] - dyl : 0.f;
-                const float ayy = t > 0 ? dy[c] - dyp[c] : 0.f;
-                const float axy = t > 0 ? dx[c] - dxp[c] : 0.f;
+                // At the left edge and the top row the backward differences are
+                // zero (compute_step_tv2.rs:53-69): take the neighbour equal to self.
+                const float dxs = __shfl_up_sync(FULL, dx[c], 1), dys = __shfl_up_sync(FULL, dy[c], 1);
+                const float dxl = tx0 ? dxs : dx[c], dyl = tx0 ? dys : dy[c];
+                const float dxu = ty0 ? dxp[c] : dx[c], dyu = ty0 ? dyp[c] : dy[c];
+                const float axx = dx[c] - dxl, ayx = dy[c] - dyl;
+                const float ayy = dy[c] - dyu, axy = dx[c] - dxu;
                 const float s = 0.5f * (axy + ayx);
                 n2 += ayy * ayy + (2.f * (s * s) + axx * axx);
                 gxx[c] = axx;
@@ -142,12 +145,13 @@ __global__ void __launch_bounds__(SWEEP_WARPS * 32) k_grad_sweep(const ImgDev *_
             }
             const float inv1 = (inside && n1 > 0.f) ? rsqrtf(n1) : 0.f;
             const float inv2 = (inside && n2 > 0.f) ? rsqrtf(n2) : 0.f;
+            const float at1 = at * inv1, ag2 = ag * inv2;
 #pragma unroll
             for (int c = 0; c < NCH; c++) {
-                const float a = at * dx[c] * inv1, b = at * dy[c] * inv1;
-                const float u = ag * (gs[c] + gxx[c]) * inv2;
-                const float v = ag * (gyy[c] + gs[c]) * inv2;
-                const float w = ag * gs[c] * inv2;
+                const float a = at1 * dx[c], b = at1 * dy[c];
+                const float u = ag2 * (gs[c] + gxx[c]);
+                const float v = ag2 * (gyy[c] + gs[c]);
+                const float w = ag2 * gs[c];
                 const float aul = __shfl_up_sync(FULL, a + u, 1);
                 const float ur = __shfl_down_sync(FULL, u, 1);
                 const float wr = __shfl_down_sync(FULL, w, 1);
@@ -161,10 +165,11 @@ __global__ void __launch_bounds__(SWEEP_WARPS * 32) k_grad_sweep(const ImgDev *_
             }
             const int ro = t - 1;
             if (outlane && ro >= ys && ro < ys + R && ro < H) {
+                const int go = ro * pitch;
 #pragma unroll
                 for (int c = 0; c < NCH; c++) {
                     const float gv = Gm[c] + pr[c];
-                    gout[c * cs + (long long)ro * pitch] = gv;
+                    gout[c * cs + go] = gv;
                     ssq[c] = fmaf(gv, gv, ssq[c]);
                 }
             }
@@ -233,80 +238,83 @@ __global__ void __launch_bounds__(SWEEP_WARPS * 32) k_grad_sweep(const ImgDev *_
 // DCT-distance gradient (compute_step_prob.rs:20-57) from the clamped
 // coefficients the reference keeps as cos (compute_projection.rs:82).
 // One warp per task {image, channel, block row, first block} covering four
-// blocks; lane group g = lane / 8 takes block first + g, lane r = lane % 8 row r
-// of it (SV full-resolution rows of 8 SH pixels). Every global load of a lane
-// is issued before any arithmetic. Row-wise 1-D transforms alternate with 8x8
-// transposes in shared memory, in the reference's order (columns, then rows).
+// blocks; lane group g = lane / 8 takes block first + g and lane j = lane % 8
+// its component column j, i.e. SH full-resolution columns over 8 SV rows, so
+// every global access of the warp is one contiguous 128-256 byte run. The
+// separable 1-D transforms run on columns or rows of the block, switching with
+// 8x8 transposes in shared memory, in the reference's order (columns first).
 template <int SH, int SV>
 __global__ void __launch_bounds__(PROJ_WARPS * 32) k_project(const ImgDev *__restrict__ imgs,
                                                             const int4 *__restrict__ tasks, int ntasks, float fnext)
 {
     constexpr bool SUB = SH * SV > 1;
-    constexpr int NV = 8 * SH;  // pixels per full-resolution row of a lane
+    constexpr int NR = 8 * SV;  // full-resolution rows of a lane
     __shared__ float s_t[PROJ_WARPS][2][4][8][9];
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int w = blockIdx.x * PROJ_WARPS + warp;
     if (w >= ntasks) return;  // warp-uniform
     const int4 tk = tasks[w];
     const ImgDev &im = imgs[tk.x];
-    const int c = tk.y, by = tk.z, grp = lane >> 3, r = lane & 7;
+    const int c = tk.y, by = tk.z, grp = lane >> 3, j = lane & 7;
     const int bx = tk.w + grp;
     const ChanDev &cd = im.ch[c];
     const bool act = bx < cd.cw / 8;
     float(*T0)[9] = s_t[warp][0][grp];
     float(*T1)[9] = s_t[warp][1][grp];
-    const long long cs = im.cstride;
+    const int cs = (int)im.cstride;
     const int pitch = im.pitch;
     float *xw = im.x + c * cs, *yw = im.y + c * cs;
     const float *gb = im.g + c * cs;
     const float sg = im.sigma[c];
     const float ap = cd.alpha_p;  // warp-uniform
     const int bxa = act ? bx : 0;
-    const long long o0 = (long long)(by * 8 * SV + r * SV) * pitch + bxa * 8 * SH;
+    const int o0 = by * 8 * SV * pitch + (bxa * 8 + j) * SH;
 
-    // All loads first: y, g and x of the lane's rows, its coefficient row and quantisation steps.
-    float yv[SV][NV], gv[SV][NV], xo[SV][NV];
+    // Loads first: y and g of the lane's column(s), then its block's
+    // coefficient row j and quantisation steps (used after the transpose);
+    // x_k is read again at the end, for the FISTA point.
+    float yv[NR][SH], gv[NR][SH];
 #pragma unroll
-    for (int sy = 0; sy < SV; sy++)
-#pragma unroll
-        for (int q4 = 0; q4 < NV / 4; q4++) {
-            const long long o = o0 + (long long)sy * pitch + 4 * q4;
-            const float4 a = *reinterpret_cast<const float4 *>(yw + o);
-            const float4 b = __ldg(reinterpret_cast<const float4 *>(gb + o));
-            const float4 x = *reinterpret_cast<const float4 *>(xw + o);
-            yv[sy][4 * q4] = a.x, yv[sy][4 * q4 + 1] = a.y, yv[sy][4 * q4 + 2] = a.z, yv[sy][4 * q4 + 3] = a.w;
-            gv[sy][4 * q4] = b.x, gv[sy][4 * q4 + 1] = b.y, gv[sy][4 * q4 + 2] = b.z, gv[sy][4 * q4 + 3] = b.w;
-            xo[sy][4 * q4] = x.x, xo[sy][4 * q4 + 1] = x.y, xo[sy][4 * q4 + 2] = x.z, xo[sy][4 * q4 + 3] = x.w;
+    for (int k = 0; k < NR; k++) {
+        const int o = o0 + k * pitch;
+        if (SH == 1) {
+            yv[k][0] = yw[o];
+            gv[k][0] = __ldg(gb + o);
+        } else {
+            const float2 a = *reinterpret_cast<const float2 *>(yw + o);
+            const float2 b = __ldg(reinterpret_cast<const float2 *>(gb + o));
+            yv[k][0] = a.x, yv[k][SH - 1] = a.y;
+            gv[k][0] = b.x, gv[k][SH - 1] = b.y;
         }
+    }
     float co[8], qv[8], iq[8];
-    load_coef_row(cd.coef + (long long)(by * 8 + r) * cd.cpitch + bxa * 8, co);
+    load_coef_row(cd.coef + (by * 8 + j) * cd.cpitch + bxa * 8, co);
 #pragma unroll
     for (int u = 0; u < 8; u++) {
-        qv[u] = __ldg(&im.q[c][r * 8 + u]);
-        iq[u] = __ldg(&im.invq2[c][r * 8 + u]);
+        qv[u] = __ldg(&im.q[c][j * 8 + u]);
+        iq[u] = __ldg(&im.invq2[c][j * 8 + u]);
     }
 
     // x' = y - sigma g; cell means for subsampled components, summed sample by
     // sample (compute_projection.rs:18-32).
     float m[8], mean[8];
 #pragma unroll
-    for (int u = 0; u < 8; u++) mean[u] = 0.f;
+    for (int k = 0; k < 8; k++) {
+        float acc = 0.f;
 #pragma unroll
-    for (int sy = 0; sy < SV; sy++)
+        for (int sy = 0; sy < SV; sy++)
 #pragma unroll
-        for (int i = 0; i < NV; i++) {
-            yv[sy][i] = fmaf(-sg, gv[sy][i], yv[sy][i]);
-            mean[i / SH] += yv[sy][i];
-        }
-#pragma unroll
-    for (int u = 0; u < 8; u++) {
-        if (SUB) mean[u] /= (float)(SH * SV);
-        m[u] = mean[u];
+            for (int sx = 0; sx < SH; sx++) {
+                const float v = fmaf(-sg, gv[k * SV + sy][sx], yv[k * SV + sy][sx]);
+                yv[k * SV + sy][sx] = v;
+                acc += v;
+            }
+        mean[k] = SUB ? acc / (float)(SH * SV) : acc;
+        m[k] = mean[k];
     }
-    // DCT (dct8x8s order: columns, then rows).
-    transpose8(T0, r, m);
+    // DCT, columns then rows (dct8x8s); the lane then holds coefficient row j.
     dct8(m);
-    transpose8(T0, r, m);
+    transpose8(T0, j, m);
     dct8(m);
     // Clamp (compute_projection.rs:72-79) and (cos - c q) / q^2.
     float d[8];
@@ -316,39 +324,56 @@ __global__ void __launch_bounds__(PROJ_WARPS * 32) k_project(const ImgDev *__res
         m[u] = cl;
         d[u] = (cl - co[u] * qv[u]) * iq[u];
     }
-    // IDCT of the clamped coefficients and of d (idct8x8s order: columns, then rows).
-    transpose8(T0, r, m);
-    if (ap != 0.f) transpose8(T1, r, d);
+    // IDCT of the clamped coefficients and of d, columns then rows (idct8x8s),
+    // then back to this lane's column.
+    transpose8(T0, j, m);
+    if (ap != 0.f) transpose8(T1, j, d);
     idct8(m);
     if (ap != 0.f) idct8(d);
-    transpose8(T0, r, m);
-    if (ap != 0.f) transpose8(T1, r, d);
+    transpose8(T0, j, m);
+    if (ap != 0.f) transpose8(T1, j, d);
     idct8(m);
+    if (ap != 0.f) idct8(d);
+    transpose8(T0, j, m);
+    if (ap != 0.f) transpose8(T1, j, d);
     if (!act) return;
     if (ap != 0.f) {
-        idct8(d);
-        float4 *pr = reinterpret_cast<float4 *>(cd.P + (long long)(by * 8 + r) * cd.ppitch + bx * 8);
-        pr[0] = make_float4(ap * d[0], ap * d[1], ap * d[2], ap * d[3]);
-        pr[1] = make_float4(ap * d[4], ap * d[5], ap * d[6], ap * d[7]);
+        float *P = cd.P + by * 8 * cd.ppitch + bx * 8 + j;
+#pragma unroll
+        for (int k = 0; k < 8; k++) P[k * cd.ppitch] = ap * d[k];
     }
     // x_{k+1}: the projected block, or for subsampled components the residual
     // x' - mean plus the projected mean (compute_projection.rs:108-121); then
     // y_{k+1} = x_{k+1} + f (x_{k+1} - x_k) (mod.rs:54-57).
+    float xo[NR][SH];
 #pragma unroll
-    for (int sy = 0; sy < SV; sy++)
-#pragma unroll
-        for (int q4 = 0; q4 < NV / 4; q4++) {
-            float xn[4], yn[4];
-#pragma unroll
-            for (int i = 0; i < 4; i++) {
-                const int k = 4 * q4 + i, u = k / SH;
-                xn[i] = SUB ? (yv[sy][k] - mean[u]) + m[u] : m[u];
-                yn[i] = fmaf(fnext, xn[i] - xo[sy][k], xn[i]);
-            }
-            const long long o = o0 + (long long)sy * pitch + 4 * q4;
-            *reinterpret_cast<float4 *>(xw + o) = make_float4(xn[0], xn[1], xn[2], xn[3]);
-            *reinterpret_cast<float4 *>(yw + o) = make_float4(yn[0], yn[1], yn[2], yn[3]);
+    for (int k = 0; k < NR; k++) {
+        const int o = o0 + k * pitch;
+        if (SH == 1) {
+            xo[k][0] = xw[o];
+        } else {
+            const float2 x = *reinterpret_cast<const float2 *>(xw + o);
+            xo[k][0] = x.x, xo[k][SH - 1] = x.y;
         }
+    }
+#pragma unroll
+    for (int k = 0; k < NR; k++) {
+        const int kc = k / SV;
+        float xn[SH], yn[SH];
+#pragma unroll
+        for (int sx = 0; sx < SH; sx++) {
+            xn[sx] = SUB ? (yv[k][sx] - mean[kc]) + m[kc] : m[kc];
+            yn[sx] = fmaf(fnext, xn[sx] - xo[k][sx], xn[sx]);
+        }
+        const int o = o0 + k * pitch;
+        if (SH == 1) {
+            xw[o] = xn[0];
+            yw[o] = yn[0];
+        } else {
+            *reinterpret_cast<float2 *>(xw + o) = make_float2(xn[0], xn[SH - 1]);
+            *reinterpret_cast<float2 *>(yw + o) = make_float2(yn[0], yn[SH - 1]);
+        }
+    }
 }
 
 // Initial image (coef.rs:24-92 with the single unboxing of
@@ -693,6 +718,8 @@ static int prepare(ArtContext *ctx, uint32_t nch, const ArtChannel *ch, const vo
     const int pitch = (int)align_up(W, 32);
     const size_t rows = align_up(H, 32);
     const long long cstride = (long long)pitch * (long long)rows;
+    if (3 * cstride >= (1LL << 31))
+        return fail(ART_ERR_INVALID_ARGUMENT, "image too large: three padded planes must stay below 2^31 floats");
     const int R = pick_strip_rows(ctx, (int)W, (int)H);
     const int strips_x = (int)((W + SWEEP_OUT - 1) / SWEEP_OUT), strips_y = (int)((H + R - 1) / R);
     const int nstrips = strips_x * strips_y;
