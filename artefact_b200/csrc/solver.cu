@@ -69,10 +69,10 @@ __global__ void __launch_bounds__(SWEEP_WARPS * 32) k_grad_sweep(const ImgDev *_
         const float *yp = im.y + cx;
         float *gout = im.g + (outlane ? gx : 0);
         const float at = im.alpha_tv, ag = im.alpha_tgv;
-        // DCT-distance gradient plane of each channel at this lane's column,
-        // prefetched two output rows ahead like y.
-        const float *pcol[NCH];
-        int psh[NCH], ppitch[NCH];
+        // DCT-distance gradient plane of each channel at this lane's column
+        // (offsets from the first channel's plane), prefetched one row ahead.
+        const float *pbase = im.ch[0].P;
+        int pcol[NCH], psh[NCH], ppitch[NCH];
         bool pon[NCH];
 #pragma unroll
         for (int c = 0; c < NCH; c++) {
@@ -80,23 +80,22 @@ __global__ void __launch_bounds__(SWEEP_WARPS * 32) k_grad_sweep(const ImgDev *_
             pon[c] = cd.alpha_p != 0.f;
             psh[c] = cd.sv - 1;
             ppitch[c] = cd.ppitch;
-            pcol[c] = cd.P + (outlane ? (gx >> (cd.sh - 1)) : 0);
+            pcol[c] = (int)(cd.P - pbase) + (outlane ? (gx >> (cd.sh - 1)) : 0);
         }
         const int Hm1 = H - 1;
         auto yrow = [&](int row) -> int { return min(max(row, 0), Hm1) * pitch; };
 
-        float yv[NCH], dxp[NCH], dyp[NCH], Gm[NCH], G0[NCH], Gp[NCH], q1[NCH], q2[NCH], p1[NCH], p2[NCH];
+        float yv[NCH], dxp[NCH], dyp[NCH], Gm[NCH], G0[NCH], Gp[NCH], q1[NCH], q2[NCH], p1[NCH];
         {
             const int o0 = yrow(ys - 2), o1 = yrow(ys - 1), o2 = yrow(ys), o3 = yrow(ys + 1);
-            const int r0 = max(ys - 2, 0), r1 = max(ys - 1, 0);
+            const int r0 = max(ys - 2, 0);
 #pragma unroll
             for (int c = 0; c < NCH; c++) {
                 const float y0 = __ldg(yp + c * cs + o0);
                 yv[c] = __ldg(yp + c * cs + o1);
                 q1[c] = __ldg(yp + c * cs + o2);
                 q2[c] = __ldg(yp + c * cs + o3);
-                p1[c] = pon[c] ? __ldg(pcol[c] + (r0 >> psh[c]) * ppitch[c]) : 0.f;  // output row of step ys - 1
-                p2[c] = pon[c] ? __ldg(pcol[c] + (r1 >> psh[c]) * ppitch[c]) : 0.f;
+                p1[c] = pon[c] ? __ldg(pbase + pcol[c] + (r0 >> psh[c]) * ppitch[c]) : 0.f;  // output row of step ys - 1
                 dxp[c] = __shfl_down_sync(FULL, y0, 1) - y0;
                 dyp[c] = yv[c] - y0;
                 Gm[c] = G0[c] = Gp[c] = 0.f;
@@ -106,15 +105,14 @@ __global__ void __launch_bounds__(SWEEP_WARPS * 32) k_grad_sweep(const ImgDev *_
             float yn[NCH], pr[NCH];
             {
                 const int o = min(t + 3, Hm1) * pitch;
-                const int pr1 = min(t + 1, Hm1);
+                const int pr1 = min(max(t, 0), Hm1);
 #pragma unroll
                 for (int c = 0; c < NCH; c++) {
                     yn[c] = q1[c];
                     q1[c] = q2[c];
                     q2[c] = __ldg(yp + c * cs + o);
                     pr[c] = p1[c];
-                    p1[c] = p2[c];
-                    p2[c] = pon[c] ? __ldg(pcol[c] + (pr1 >> psh[c]) * ppitch[c]) : 0.f;
+                    p1[c] = pon[c] ? __ldg(pbase + pcol[c] + (pr1 >> psh[c]) * ppitch[c]) : 0.f;
                 }
             }
             const bool inside = colin && t >= 0 && t < H;
@@ -238,65 +236,81 @@ __global__ void __launch_bounds__(SWEEP_WARPS * 32) k_grad_sweep(const ImgDev *_
 // DCT-distance gradient (compute_step_prob.rs:20-57) from the clamped
 // coefficients the reference keeps as cos (compute_projection.rs:82).
 // One warp per task {image, channel, block row, first block} covering four
-// blocks; lane group g = lane / 8 takes block first + g and lane j = lane % 8
-// its component column j, i.e. SH full-resolution columns over 8 SV rows, so
-// every global access of the warp is one contiguous 128-256 byte run. The
-// separable 1-D transforms run on columns or rows of the block, switching with
-// 8x8 transposes in shared memory, in the reference's order (columns first).
+// blocks. The warp's region of y, g and x (8 SV rows x 32 SH columns) is
+// staged into shared memory with asynchronous 16-byte copies, one round trip;
+// then lane group g = lane / 8 takes block first + g and lane j = lane % 8 its
+// component column j (SH full-resolution columns). The separable 1-D
+// transforms run on columns or rows of the block, switching with 8x8
+// transposes in shared memory, in the reference's order (columns first).
+template <int SH, int SV>
+struct ProjShape {
+    static constexpr int NR = 8 * SV;       // rows of the region
+    static constexpr int NC = 32 * SH;      // columns of the region
+    static constexpr int RS = NC + 4;       // padded row stride (floats)
+    static constexpr int REGION = NR * RS;  // floats per staged plane
+};
+
 template <int SH, int SV>
 __global__ void __launch_bounds__(PROJ_WARPS * 32) k_project(const ImgDev *__restrict__ imgs,
                                                             const int4 *__restrict__ tasks, int ntasks, float fnext)
 {
+    using S = ProjShape<SH, SV>;
     constexpr bool SUB = SH * SV > 1;
-    constexpr int NR = 8 * SV;  // full-resolution rows of a lane
+    constexpr int NR = S::NR, NC = S::NC, RS = S::RS;
+    extern __shared__ float4 s_dyn[];
     __shared__ float s_t[PROJ_WARPS][2][4][8][9];
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int w = blockIdx.x * PROJ_WARPS + warp;
     if (w >= ntasks) return;  // warp-uniform
+    float *sy_ = reinterpret_cast<float *>(s_dyn) + warp * 3 * S::REGION;  // y, g, x regions
+    float *sg_ = sy_ + S::REGION, *sx_ = sg_ + S::REGION;
     const int4 tk = tasks[w];
     const ImgDev &im = imgs[tk.x];
     const int c = tk.y, by = tk.z, grp = lane >> 3, j = lane & 7;
     const int bx = tk.w + grp;
     const ChanDev &cd = im.ch[c];
-    const bool act = bx < cd.cw / 8;
-    float(*T0)[9] = s_t[warp][0][grp];
-    float(*T1)[9] = s_t[warp][1][grp];
+    const int bw = cd.cw / 8;
+    const bool act = bx < bw;
     const int cs = (int)im.cstride;
     const int pitch = im.pitch;
     float *xw = im.x + c * cs, *yw = im.y + c * cs;
     const float *gb = im.g + c * cs;
-    const float sg = im.sigma[c];
-    const float ap = cd.alpha_p;  // warp-uniform
-    const int bxa = act ? bx : 0;
-    const int o0 = by * 8 * SV * pitch + (bxa * 8 + j) * SH;
-
-    // Loads first: y and g of the lane's column(s), then its block's
-    // coefficient row j and quantisation steps (used after the transpose);
-    // x_k is read again at the end, for the FISTA point.
-    float yv[NR][SH], gv[NR][SH];
-#pragma unroll
-    for (int k = 0; k < NR; k++) {
-        const int o = o0 + k * pitch;
-        if (SH == 1) {
-            yv[k][0] = yw[o];
-            gv[k][0] = __ldg(gb + o);
-        } else {
-            const float2 a = *reinterpret_cast<const float2 *>(yw + o);
-            const float2 b = __ldg(reinterpret_cast<const float2 *>(gb + o));
-            yv[k][0] = a.x, yv[k][SH - 1] = a.y;
-            gv[k][0] = b.x, gv[k][SH - 1] = b.y;
+    // Stage the region: rows of NC floats, 16-byte chunks; chunks of blocks
+    // past the end of the block row are skipped.
+    {
+        const int X0 = tk.w * 8 * SH;
+        const int ncol = min(NC, (bw - tk.w) * 8 * SH);  // valid columns, a multiple of 8
+        const long long r0 = (long long)(by * 8 * SV) * pitch + X0;
+        constexpr int CPR = NC / 4;  // 16-byte chunks per row
+        for (int i = lane; i < NR * CPR; i += 32) {
+            const int row = i / CPR, ch = i - row * CPR;
+            if (ch * 4 < ncol) {
+                const long long go = r0 + (long long)row * pitch + ch * 4;
+                const int so = row * RS + ch * 4;
+                cp_async16(sy_ + so, yw + go);
+                cp_async16(sg_ + so, gb + go);
+                cp_async16(sx_ + so, xw + go);
+            }
         }
     }
+    // Meanwhile: coefficient row j of this lane's block and its quantisation steps.
     float co[8], qv[8], iq[8];
-    load_coef_row(cd.coef + (by * 8 + j) * cd.cpitch + bxa * 8, co);
+    load_coef_row(cd.coef + (by * 8 + j) * cd.cpitch + (act ? bx : 0) * 8, co);
 #pragma unroll
     for (int u = 0; u < 8; u++) {
         qv[u] = __ldg(&im.q[c][j * 8 + u]);
         iq[u] = __ldg(&im.invq2[c][j * 8 + u]);
     }
+    const float sg = im.sigma[c];
+    const float ap = cd.alpha_p;  // warp-uniform
+    float(*T0)[9] = s_t[warp][0][grp];
+    float(*T1)[9] = s_t[warp][1][grp];
+    cp_async_wait_all();
+    __syncwarp();
 
-    // x' = y - sigma g; cell means for subsampled components, summed sample by
-    // sample (compute_projection.rs:18-32).
+    // x' = y - sigma g (kept in the y region); cell means for subsampled
+    // components, summed sample by sample (compute_projection.rs:18-32).
+    const int cb = (grp * 8 + j) * SH;  // first region column of this lane
     float m[8], mean[8];
 #pragma unroll
     for (int k = 0; k < 8; k++) {
@@ -305,8 +319,9 @@ __global__ void __launch_bounds__(PROJ_WARPS * 32) k_project(const ImgDev *__res
         for (int sy = 0; sy < SV; sy++)
 #pragma unroll
             for (int sx = 0; sx < SH; sx++) {
-                const float v = fmaf(-sg, gv[k * SV + sy][sx], yv[k * SV + sy][sx]);
-                yv[k * SV + sy][sx] = v;
+                const int so = (k * SV + sy) * RS + cb + sx;
+                const float v = fmaf(-sg, sg_[so], sy_[so]);
+                sy_[so] = v;
                 acc += v;
             }
         mean[k] = SUB ? acc / (float)(SH * SV) : acc;
@@ -345,25 +360,16 @@ __global__ void __launch_bounds__(PROJ_WARPS * 32) k_project(const ImgDev *__res
     // x_{k+1}: the projected block, or for subsampled components the residual
     // x' - mean plus the projected mean (compute_projection.rs:108-121); then
     // y_{k+1} = x_{k+1} + f (x_{k+1} - x_k) (mod.rs:54-57).
-    float xo[NR][SH];
-#pragma unroll
-    for (int k = 0; k < NR; k++) {
-        const int o = o0 + k * pitch;
-        if (SH == 1) {
-            xo[k][0] = xw[o];
-        } else {
-            const float2 x = *reinterpret_cast<const float2 *>(xw + o);
-            xo[k][0] = x.x, xo[k][SH - 1] = x.y;
-        }
-    }
+    const int o0 = by * 8 * SV * pitch + bx * 8 * SH + j * SH;
 #pragma unroll
     for (int k = 0; k < NR; k++) {
         const int kc = k / SV;
         float xn[SH], yn[SH];
 #pragma unroll
         for (int sx = 0; sx < SH; sx++) {
-            xn[sx] = SUB ? (yv[k][sx] - mean[kc]) + m[kc] : m[kc];
-            yn[sx] = fmaf(fnext, xn[sx] - xo[k][sx], xn[sx]);
+            const int so = k * RS + cb + sx;
+            xn[sx] = SUB ? (sy_[so] - mean[kc]) + m[kc] : m[kc];
+            yn[sx] = fmaf(fnext, xn[sx] - sx_[so], xn[sx]);
         }
         const int o = o0 + k * pitch;
         if (SH == 1) {
@@ -637,13 +643,33 @@ int pick_strip_rows(const ArtContext *ctx, int W, int H)
     if (env && atoi(env) > 0) return atoi(env);
     const long long strips_x = (W + SWEEP_OUT - 1) / SWEEP_OUT;
     int R = 128;
-    while (R > 16 && strips_x * ((H + R - 1) / R) < 148LL * 24) R /= 2;
+    while (R > 32 && strips_x * ((H + R - 1) / R) < 148LL * 16) R /= 2;
     return R;
 }
 
+template <int SH, int SV>
+constexpr int proj_smem()
+{
+    return PROJ_WARPS * 3 * ProjShape<SH, SV>::REGION * (int)sizeof(float);
+}
+
+// Raises the dynamic shared-memory limit of the projection kernels, once per device.
 int configure_kernels(int device)
 {
-    (void)device;
+    static std::mutex mu;
+    static std::vector<int> done;
+    std::lock_guard<std::mutex> lock(mu);
+    if ((int)done.size() <= device) done.resize(device + 1, 0);
+    if (done[device]) return ART_OK;
+    cudaError_t e = cudaFuncSetAttribute(k_project<1, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, proj_smem<1, 1>());
+    if (e == cudaSuccess)
+        e = cudaFuncSetAttribute(k_project<2, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize, proj_smem<2, 2>());
+    if (e == cudaSuccess)
+        e = cudaFuncSetAttribute(k_project<2, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, proj_smem<2, 1>());
+    if (e == cudaSuccess)
+        e = cudaFuncSetAttribute(k_project<1, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize, proj_smem<1, 2>());
+    if (e != cudaSuccess) return fail(ART_ERR_CUDA, std::string("cudaFuncSetAttribute: ") + cudaGetErrorString(e));
+    done[device] = 1;
     return ART_OK;
 }
 
@@ -863,13 +889,13 @@ static void launch_iteration(ArtContext *ctx, int it, float fnext)
         const int4 *tk = tasks + ctx->mode_off[m];
         const int grid = (n + PROJ_WARPS - 1) / PROJ_WARPS;
         if (m == 0)
-            k_project<1, 1><<<grid, PROJ_WARPS * 32, 0, s>>>(ddesc, tk, n, fnext);
+            k_project<1, 1><<<grid, PROJ_WARPS * 32, proj_smem<1, 1>(), s>>>(ddesc, tk, n, fnext);
         else if (m == 1)
-            k_project<2, 2><<<grid, PROJ_WARPS * 32, 0, s>>>(ddesc, tk, n, fnext);
+            k_project<2, 2><<<grid, PROJ_WARPS * 32, proj_smem<2, 2>(), s>>>(ddesc, tk, n, fnext);
         else if (m == 2)
-            k_project<2, 1><<<grid, PROJ_WARPS * 32, 0, s>>>(ddesc, tk, n, fnext);
+            k_project<2, 1><<<grid, PROJ_WARPS * 32, proj_smem<2, 1>(), s>>>(ddesc, tk, n, fnext);
         else
-            k_project<1, 2><<<grid, PROJ_WARPS * 32, 0, s>>>(ddesc, tk, n, fnext);
+            k_project<1, 2><<<grid, PROJ_WARPS * 32, proj_smem<1, 2>(), s>>>(ddesc, tk, n, fnext);
     }
     if (tm) cudaEventRecordWithFlags(ctx->events[5 + 4 * it], s, cudaEventRecordExternal);
 }

@@ -190,4 +190,17 @@ __device__ __forceinline__ void transpose8(float (*T)[9], int r, float *v)
     for (int k = 0; k < 8; k++) v[k] = T[k][r];
 }
 
+// Asynchronous global -> shared copies of 16 bytes (L2 only), and their fence.
+__device__ __forceinline__ void cp_async16(void *smem, const void *gmem)
+{
+    const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(s), "l"(gmem) : "memory");
+}
+
+__device__ __forceinline__ void cp_async_wait_all()
+{
+    asm volatile("cp.async.commit_group;\n" ::: "memory");
+    asm volatile("cp.async.wait_group 0;\n" ::: "memory");
+}
+
 }  // namespace art
