@@ -73,6 +73,9 @@ EXPORTS = {
     "art_context_process": (C.c_int32, [C.c_void_p, C.c_uint32, C.POINTER(ArtChannel), C.POINTER(C.c_float),
                                         C.POINTER(C.c_float), C.POINTER(C.c_uint32), C.c_int32, C.c_uint32,
                                         C.c_uint32, C.c_void_p, C.POINTER(ArtOptions)]),
+    "art_solve_noalloc": (C.c_int32, [C.c_uint32, C.POINTER(ArtChannel), C.c_float, C.POINTER(C.c_float),
+                                      C.c_uint32, C.c_uint32, C.c_uint32, C.POINTER(C.c_void_p), C.c_uint32,
+                                      C.c_void_p]),
     "art_context_synchronize": (C.c_int32, [C.c_void_p]),
     "art_context_set_timing": (C.c_int32, [C.c_void_p, C.c_int32]),
     "art_context_last_timing": (C.c_int32, [C.c_void_p, C.POINTER(C.c_float), C.POINTER(C.c_float),

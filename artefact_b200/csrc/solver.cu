@@ -1260,3 +1260,242 @@ extern "C" int32_t art_compute(uint32_t nchannel, const ArtChannel *coefs, float
     return art_context_compute(v[device], nchannel, coefs, weight, pweight, iterations, max_w, max_h, out_planes,
                                opts);
 }
+
+// ============================================ allocation-free entry point ====
+//
+// art_solve_noalloc runs the same kernels as art_context_compute_device, but
+// takes every scratch buffer (iterate, FISTA point, gradient, DCT-distance and
+// coefficient planes, norm partials, descriptor, work lists) from one
+// file-scope device array of ART_NOALLOC_SCRATCH_BYTES instead of cudaMalloc.
+// It is for callers that must not allocate device memory themselves: callers
+// whose device memory is owned by another allocator (a framework's caching
+// allocator, a server that partitions each GPU up front) and callers that
+// cannot afford the device-wide synchronisation cudaMalloc and cudaFree may
+// imply. Every GPU that loads this library holds the array until the process
+// exits. All calls share it and it keeps the last call's contents, so each call
+// clears what must start at zero; calls whose GPU work overlaps (from two host
+// threads, or on two streams) race on it.
+
+#define ART_NOALLOC_SCRATCH_BYTES (64ull << 20)
+
+static __device__ __align__(256) unsigned char g_noalloc_scratch[ART_NOALLOC_SCRATCH_BYTES];
+
+namespace art {
+namespace {
+
+struct NoallocSeg {
+    int c, base, bw4, bh;  // channel, first task, tasks per block row, block rows
+};
+
+struct NoallocPlan {
+    NoallocSeg seg[3];
+    int nseg;
+};
+
+// Writes the descriptor and the two work lists into the scratch array (the
+// descriptor arrives by value as a kernel parameter, so no host buffer is copied).
+__global__ void k_noalloc_setup(ImgDev d, ImgDev *dst, int2 *work, int ncta, int4 *tasks, int ntasks,
+                                NoallocPlan plan)
+{
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i == 0) *dst = d;
+    if (i < ncta) work[i] = make_int2(0, i);
+    if (i < ntasks) {
+        int s = 0;
+        while (s + 1 < plan.nseg && i >= plan.seg[s + 1].base) s++;
+        const NoallocSeg &g = plan.seg[s];
+        const int k = i - g.base, by = k / g.bw4, bx0 = (k % g.bw4) * 4;
+        tasks[i] = make_int4(0, g.c, by, bx0);
+    }
+}
+
+std::mutex g_noalloc_mu;
+std::vector<void *> g_noalloc_base;  // per device, resolved once
+
+// Device address of the scratch array on the current device, resolved once
+// per device with that device current.
+int noalloc_scratch(int device, unsigned char **out)
+{
+    std::lock_guard<std::mutex> lock(g_noalloc_mu);
+    if ((int)g_noalloc_base.size() <= device) g_noalloc_base.resize(device + 1, nullptr);
+    if (!g_noalloc_base[device]) {
+        void *p = nullptr;
+        const cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+        if (e != cudaSuccess || !p)
+            return fail(ART_ERR_CUDA, std::string("cudaGetSymbolAddress(scratch): ") + cudaGetErrorString(e));
+        g_noalloc_base[device] = p;
+    }
+    *out = static_cast<unsigned char *>(g_noalloc_base[device]);
+    return ART_OK;
+}
+
+}  // namespace
+}  // namespace art
+
+extern "C" int32_t art_solve_noalloc(uint32_t nchannel, const ArtChannel *coefs, float weight,
+                                     const float pweight[3], uint32_t iterations, uint32_t max_w, uint32_t max_h,
+                                     float *const *out_planes_device, uint32_t out_pitch, void *stream)
+{
+    using namespace art;
+    int rc = validate(nchannel, coefs, weight, pweight, max_w, max_h);
+    if (rc) return rc;
+    if (!out_planes_device || out_pitch < max_w) return fail(ART_ERR_INVALID_ARGUMENT, "bad output planes");
+    for (uint32_t c = 0; c < nchannel; c++)
+        if (!out_planes_device[c]) return fail(ART_ERR_INVALID_ARGUMENT, "null output plane");
+    int device = 0;
+    ART_CUDA(cudaGetDevice(&device));
+    unsigned char *base = nullptr;
+    if ((rc = noalloc_scratch(device, &base))) return rc;
+    if ((rc = configure_kernels(device))) return rc;
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+
+    // Layout inside the scratch array (the same geometry prepare() uses).
+    const uint32_t W = max_w, H = max_h, nch = nchannel;
+    const int pitch = (int)align_up(W, 32);
+    const long long cstride = (long long)pitch * (long long)align_up(H, 32);
+    if (3 * cstride >= (1LL << 31))
+        return fail(ART_ERR_INVALID_ARGUMENT, "image too large: three padded planes must stay below 2^31 floats");
+    const int R = 32;
+    const int strips_x = (int)((W + SWEEP_OUT - 1) / SWEEP_OUT), strips_y = (int)((H + R - 1) / R);
+    const int nstrips = strips_x * strips_y, ncta = (nstrips + SWEEP_WARPS - 1) / SWEEP_WARPS;
+    size_t off = 0;
+    auto take = [&](size_t bytes) {
+        const size_t o = off;
+        off = align_up(off + bytes, 256);
+        return o;
+    };
+    const size_t o_x = take(3 * nch * cstride * sizeof(float));
+    size_t o_coef[3], o_p[3];
+    int cpitch[3], ppitch[3];
+    for (uint32_t c = 0; c < nch; c++) {
+        cpitch[c] = (int)align_up(coefs[c].rounded_px_w, 64);
+        ppitch[c] = (int)align_up(coefs[c].rounded_px_w, 32);
+        o_coef[c] = take((size_t)cpitch[c] * coefs[c].rounded_px_h * sizeof(int16_t));
+        o_p[c] = take((size_t)ppitch[c] * coefs[c].rounded_px_h * sizeof(float));
+    }
+    const size_t o_misc = take(align_up((size_t)ncta * 4 * sizeof(float), 256) + 256);
+    const size_t o_desc = take(sizeof(ImgDev));
+    const size_t o_work = take((size_t)ncta * sizeof(int2));
+    // Tasks grouped by sampling mode (channels of one mode in channel order).
+    NoallocPlan plan{};
+    int mode_off[5] = {0, 0, 0, 0, 0};
+    int ntasks = 0;
+    for (int m = 0; m < 4; m++) {
+        mode_off[m] = ntasks;
+        for (uint32_t c = 0; c < nch; c++) {
+            if (samp_mode((int)coefs[c].samp_h, (int)coefs[c].samp_v) != m) continue;
+            const int bw4 = (int)((coefs[c].block_w + 3) / 4);
+            plan.seg[plan.nseg++] = NoallocSeg{(int)c, ntasks, bw4, (int)coefs[c].block_h};
+            ntasks += bw4 * (int)coefs[c].block_h;
+        }
+    }
+    mode_off[4] = ntasks;
+    const size_t o_tasks = take((size_t)ntasks * sizeof(int4));
+    if (off > ART_NOALLOC_SCRATCH_BYTES)
+        return fail(ART_ERR_INVALID_ARGUMENT, "image needs " + std::to_string(off >> 20) +
+                                                  " MiB of scratch; art_solve_noalloc has " +
+                                                  std::to_string(ART_NOALLOC_SCRATCH_BYTES >> 20) + " MiB");
+
+    ImgDev d;
+    memset(&d, 0, sizeof(d));
+    d.nch = (int)nch;
+    d.W = (int)W;
+    d.H = (int)H;
+    d.pitch = pitch;
+    d.strips_x = strips_x;
+    d.strips_y = strips_y;
+    d.nstrips = nstrips;
+    d.strip_rows = R;
+    d.ncta = ncta;
+    d.cstride = cstride;
+    d.x = reinterpret_cast<float *>(base + o_x);
+    d.y = d.x + nch * cstride;
+    d.g = d.y + nch * cstride;
+    d.alpha_tv = 1.0f / sqrtf((float)nch);
+    d.alpha_tgv = (weight / sqrtf(2.0f)) / sqrtf((float)nch);
+    d.step = (sqrtf((float)((uint64_t)W * H)) / 2.0f) / sqrtf(1.0f + (float)iterations);
+    unsigned char *misc = base + o_misc;
+    d.partial = reinterpret_cast<float *>(misc);
+    d.sigma = reinterpret_cast<float *>(misc + align_up((size_t)ncta * 4 * sizeof(float), 256));
+    d.counter = reinterpret_cast<unsigned *>(d.sigma + 4);
+    unsigned *errflag = d.counter + 1;
+    for (uint32_t c = 0; c < nch; c++) {
+        ChanDev &cd = d.ch[c];
+        cd.cw = (int)coefs[c].rounded_px_w;
+        cd.chh = (int)coefs[c].rounded_px_h;
+        cd.sh = (int)coefs[c].samp_h;
+        cd.sv = (int)coefs[c].samp_v;
+        cd.cpitch = cpitch[c];
+        cd.ppitch = ppitch[c];
+        cd.coef = reinterpret_cast<const int16_t *>(base + o_coef[c]);
+        cd.P = reinterpret_cast<float *>(base + o_p[c]);
+        cd.alpha_p = pweight[c] * 2.0f * 255.0f * sqrtf(2.0f);
+        for (int j = 0; j < 64; j++) {
+            const float q = coefs[c].quant_table[j];
+            d.q[c][j] = q;
+            d.invq2[c][j] = 1.0f / (q * q);
+        }
+    }
+    ImgDev *ddesc = reinterpret_cast<ImgDev *>(base + o_desc);
+    int2 *work = reinterpret_cast<int2 *>(base + o_work);
+    int4 *tasks = reinterpret_cast<int4 *>(base + o_tasks);
+
+    // Clear what must start at zero: the norm partials, counter and error flag,
+    // and the first DCT-distance gradient planes.
+    ART_CUDA(cudaMemsetAsync(misc, 0, o_desc - o_misc, s));
+    for (uint32_t c = 0; c < nch; c++)
+        ART_CUDA(cudaMemsetAsync(d.ch[c].P, 0, (size_t)ppitch[c] * coefs[c].rounded_px_h * sizeof(float), s));
+    const int nset = std::max(ncta, ntasks);
+    k_noalloc_setup<<<(nset + 255) / 256, 256, 0, s>>>(d, ddesc, work, ncta, tasks, ntasks, plan);
+    for (uint32_t c = 0; c < nch; c++) {
+        const long long ncoef = (long long)coefs[c].block_w * coefs[c].block_h * 64;
+        k_ingest<<<(int)((ncoef + 255) / 256), 256, 0, s>>>(coefs[c].dct_coefs, (int)coefs[c].coef_type,
+                                                             (int)coefs[c].block_w, ncoef,
+                                                             const_cast<int16_t *>(d.ch[c].coef), cpitch[c], errflag);
+    }
+    k_init<<<(ntasks + PROJ_WARPS - 1) / PROJ_WARPS, PROJ_WARPS * 32, 0, s>>>(ddesc, tasks, ntasks);
+    // FISTA factors as fista_factors() forms them, one step ahead (no host buffer).
+    float term = 1.0f;
+    auto next_factor = [&term]() {
+        volatile float t2 = term * term;
+        volatile float inner = 4.0f * t2 + 1.0f;
+        const float next = (float)(((double)1.0f + (double)sqrtf(inner)) / 2.0);
+        const float f = (term - 1.0f) / next;
+        term = next;
+        return f;
+    };
+    next_factor();  // f_0 = 0: y_0 = x_0
+    for (uint32_t it = 0; it < iterations; it++) {
+        const float fnext = it + 1 < iterations ? next_factor() : 0.0f;
+        if (nch == 3)
+            k_grad_sweep<3><<<ncta, SWEEP_WARPS * 32, 0, s>>>(ddesc, work);
+        else if (nch == 2)
+            k_grad_sweep<2><<<ncta, SWEEP_WARPS * 32, 0, s>>>(ddesc, work);
+        else
+            k_grad_sweep<1><<<ncta, SWEEP_WARPS * 32, 0, s>>>(ddesc, work);
+        for (int m = 3; m >= 0; m--) {
+            const int n = mode_off[m + 1] - mode_off[m];
+            if (n == 0) continue;
+            const int4 *tk = tasks + mode_off[m];
+            const int grid = (n + PROJ_WARPS - 1) / PROJ_WARPS;
+            if (m == 0)
+                k_project<1, 1><<<grid, PROJ_WARPS * 32, proj_smem<1, 1>(), s>>>(ddesc, tk, n, fnext);
+            else if (m == 1)
+                k_project<2, 2><<<grid, PROJ_WARPS * 32, proj_smem<2, 2>(), s>>>(ddesc, tk, n, fnext);
+            else if (m == 2)
+                k_project<2, 1><<<grid, PROJ_WARPS * 32, proj_smem<2, 1>(), s>>>(ddesc, tk, n, fnext);
+            else
+                k_project<1, 2><<<grid, PROJ_WARPS * 32, proj_smem<1, 2>(), s>>>(ddesc, tk, n, fnext);
+        }
+    }
+    ART_CUDA(cudaGetLastError());
+    for (uint32_t c = 0; c < nch; c++)
+        ART_CUDA(cudaMemcpy2DAsync(out_planes_device[c], (size_t)out_pitch * sizeof(float), d.x + c * cstride,
+                                   (size_t)pitch * sizeof(float), (size_t)W * sizeof(float), H,
+                                   cudaMemcpyDeviceToDevice, s));
+    unsigned flag = 0;
+    ART_CUDA(cudaMemcpyAsync(&flag, errflag, sizeof(flag), cudaMemcpyDeviceToHost, s));
+    ART_CUDA(cudaStreamSynchronize(s));
+    if (flag) return fail(ART_ERR_INVALID_DATA, "coefficients must be integers in [-32768, 32767]");
+    return ART_OK;
+}

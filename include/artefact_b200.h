@@ -133,6 +133,26 @@ int32_t art_context_set_timing(ArtContext *ctx, int32_t enabled);
 int32_t art_context_last_timing(ArtContext *ctx, float *loop_ms, float *gradient_ms, float *update_ms,
                                 uint32_t *launches);
 
+/*
+ * Allocation-free solve. No counterpart in the reference: artefact-lib runs
+ * on the CPU and owns its buffers. For callers that must not allocate device
+ * memory -- their GPU memory belongs to another allocator (a framework's
+ * caching allocator, a server that partitions each GPU up front), or they
+ * cannot afford the device-wide synchronisation cudaMalloc/cudaFree may
+ * imply. Same kernels and results as art_context_compute_device, but every
+ * scratch buffer comes from one fixed 64 MiB array in device memory that the
+ * library holds on every GPU it is loaded on until the process exits; images
+ * that need more (about 1 megapixel per channel) are rejected with
+ * ART_ERR_INVALID_ARGUMENT. dct_coefs and out_planes_device are device
+ * pointers, quant_table a host pointer; work runs on `stream` (NULL = legacy
+ * default stream) and the call returns when it is done. The first call on a
+ * device resolves the array's address there. All calls share the array, so
+ * calls whose GPU work overlaps race; each call clears what must start at zero.
+ */
+int32_t art_solve_noalloc(uint32_t nchannel, const ArtChannel *coefs, float weight, const float pweight[3],
+                          uint32_t iterations, uint32_t max_rounded_px_w, uint32_t max_rounded_px_h,
+                          float *const *out_planes_device, uint32_t out_pitch, void *stream);
+
 /* ---- host JPEG front end (stand-in for jpeg/zune.rs:5-55 on the host) ---- */
 
 typedef struct ArtJpeg ArtJpeg;
