@@ -47,6 +47,19 @@ class ArtOptions(C.Structure):
     ]
 
 
+class ArtImage(C.Structure):
+    _fields_ = [
+        ("nchannel", C.c_uint32),
+        ("max_rounded_px_w", C.c_uint32),
+        ("max_rounded_px_h", C.c_uint32),
+        ("out_pitch", C.c_uint32),
+        ("channels", C.POINTER(ArtChannel)),
+        ("weight", C.c_float),
+        ("pweight", C.c_float * 3),
+        ("out_planes", C.POINTER(C.c_void_p)),
+    ]
+
+
 class ArtError(RuntimeError):
     """Raised when a C ABI call returns a negative status."""
 
@@ -76,6 +89,13 @@ EXPORTS = {
     "art_solve_noalloc": (C.c_int32, [C.c_uint32, C.POINTER(ArtChannel), C.c_float, C.POINTER(C.c_float),
                                       C.c_uint32, C.c_uint32, C.c_uint32, C.POINTER(C.c_void_p), C.c_uint32,
                                       C.c_void_p]),
+    "art_context_compute_batch": (C.c_int32, [C.c_void_p, C.c_uint32, C.POINTER(ArtImage), C.c_uint32,
+                                              C.POINTER(ArtOptions)]),
+    "art_context_compute_batch_device": (C.c_int32, [C.c_void_p, C.c_uint32, C.POINTER(ArtImage), C.c_uint32,
+                                                     C.POINTER(ArtOptions), C.c_void_p]),
+    "art_context_autotune": (C.c_int32, [C.c_void_p, C.c_uint32, C.POINTER(C.c_uint32), C.POINTER(C.c_uint32),
+                                         C.c_uint32, C.c_uint32, C.c_uint32, C.POINTER(C.c_uint32)]),
+    "art_context_tune_cache": (C.c_int32, [C.c_void_p, C.c_char_p, C.c_int32]),
     "art_context_synchronize": (C.c_int32, [C.c_void_p]),
     "art_context_set_timing": (C.c_int32, [C.c_void_p, C.c_int32]),
     "art_context_last_timing": (C.c_int32, [C.c_void_p, C.POINTER(C.c_float), C.POINTER(C.c_float),

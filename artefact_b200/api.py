@@ -283,3 +283,91 @@ def process_jpeg(jpeg: Jpeg, weight: Sequence[float], pweight: Sequence[float], 
     if benchmark:
         raise ArtefactError("BENCHMARK")
     return rgb
+
+
+class Context:
+    """An explicit solver context (``art_context_*``): one CUDA stream, device
+    buffers, the captured iteration graph and the autotuner's cache, reused
+    across calls. Not to be shared by two threads at once."""
+
+    def __init__(self, device: int = -1):
+        self._h = C.c_void_p()
+        N.check(N.lib().art_context_create(device, C.byref(self._h)))
+
+    def close(self) -> None:
+        if self._h:
+            N.lib().art_context_destroy(self._h)
+            self._h = C.c_void_p()
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    @property
+    def handle(self) -> C.c_void_p:
+        return self._h
+
+    def compute(self, nchannel: int, coefs: Sequence[Coefficient], weight: float, pweight: Sequence[float],
+                iterations: int, max_rounded_px_w: int, max_rounded_px_h: int,
+                init_mode: int = N.ART_INIT_DECODED) -> List[np.ndarray]:
+        keep: list = []
+        chans = (N.ArtChannel * nchannel)(*[coefs[c].as_c(keep) for c in range(nchannel)])
+        pw = (C.c_float * 3)(*[float(v) for v in list(pweight)[:3]])
+        outs = [np.empty(max_rounded_px_w * max_rounded_px_h, np.float32) for _ in range(nchannel)]
+        ptrs = (C.c_void_p * nchannel)(*[o.ctypes.data for o in outs])
+        N.check(N.lib().art_context_compute(self._h, nchannel, chans, float(weight), pw, int(iterations),
+                                            max_rounded_px_w, max_rounded_px_h, ptrs, C.byref(_options(init_mode, -1))))
+        return outs
+
+    def compute_batch(self, jobs: Sequence[dict], iterations: int,
+                      init_mode: int = N.ART_INIT_DECODED) -> List[List[np.ndarray]]:
+        """Solve many images together (one launch per kernel and iteration over
+        all of them, the loop in one CUDA graph). Each job is a dict with keys
+        ``coefs`` (list of :class:`Coefficient`), ``weight``, ``pweight`` and
+        optionally ``nchannel``, ``max_w``, ``max_h`` (default: from the coefs)."""
+        keep: list = []
+        imgs = (N.ArtImage * len(jobs))()
+        results = []
+        for i, job in enumerate(jobs):
+            coefs = job["coefs"]
+            n = job.get("nchannel", len(coefs))
+            w = job.get("max_w", max(c.rounded_px_w for c in coefs))
+            h = job.get("max_h", max(c.rounded_px_h for c in coefs))
+            chans = (N.ArtChannel * n)(*[coefs[c].as_c(keep) for c in range(n)])
+            outs = [np.empty(w * h, np.float32) for _ in range(n)]
+            ptrs = (C.c_void_p * n)(*[o.ctypes.data for o in outs])
+            keep += [chans, ptrs]
+            im = imgs[i]
+            im.nchannel, im.max_rounded_px_w, im.max_rounded_px_h, im.out_pitch = n, w, h, w
+            im.channels = C.cast(chans, C.POINTER(N.ArtChannel))
+            im.weight = float(job.get("weight", 0.3))
+            pw = list(job.get("pweight", [0.001] * 3))
+            im.pweight = (C.c_float * 3)(*[float(v) for v in (pw + [0.0] * 3)[:3]])
+            im.out_planes = C.cast(ptrs, C.POINTER(C.c_void_p))
+            results.append(outs)
+        N.check(N.lib().art_context_compute_batch(self._h, len(jobs), imgs, int(iterations),
+                                                  C.byref(_options(init_mode, -1))))
+        return results
+
+    def autotune(self, nchannel: int, samp_h: Sequence[int], samp_v: Sequence[int], max_w: int, max_h: int,
+                 iterations: int = 10) -> int:
+        """Time the sweep strip heights for this geometry; returns (and caches) the fastest."""
+        sh = (C.c_uint32 * 3)(*(list(samp_h) + [1, 1, 1])[:3])
+        sv = (C.c_uint32 * 3)(*(list(samp_v) + [1, 1, 1])[:3])
+        out = C.c_uint32()
+        N.check(N.lib().art_context_autotune(self._h, nchannel, sh, sv, max_w, max_h, iterations, C.byref(out)))
+        return out.value
+
+    def save_tune_cache(self, path: str) -> None:
+        N.check(N.lib().art_context_tune_cache(self._h, str(path).encode(), 1))
+
+    def load_tune_cache(self, path: str) -> None:
+        N.check(N.lib().art_context_tune_cache(self._h, str(path).encode(), 0))

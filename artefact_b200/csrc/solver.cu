@@ -19,7 +19,11 @@
 #include <cstdio>
 #include <cstring>
 #include <memory>
+#include <array>
+#include <fstream>
+#include <map>
 #include <mutex>
+#include <sstream>
 #include <string>
 #include <vector>
 
@@ -595,17 +599,27 @@ std::vector<float> fista_factors(uint32_t iterations)
 }
 
 struct GraphKey {
-    int nch = 0, ncta = 0, ntasks = 0;
+    int nimg = 0, wcount[4] = {0, 0, 0, 0};
     int mode_off[5] = {0, 0, 0, 0, 0};
     uint32_t iterations = 0;
     bool timing = false;
     const void *desc = nullptr, *work = nullptr, *tasks = nullptr;
     bool operator==(const GraphKey &o) const
     {
-        return nch == o.nch && ncta == o.ncta && ntasks == o.ntasks && iterations == o.iterations &&
-               timing == o.timing && desc == o.desc && work == o.work && tasks == o.tasks &&
+        return nimg == o.nimg && iterations == o.iterations && timing == o.timing && desc == o.desc &&
+               work == o.work && tasks == o.tasks && std::equal(wcount, wcount + 4, o.wcount) &&
                std::equal(mode_off, mode_off + 5, o.mode_off);
     }
+};
+
+// One image of a solve: geometry, weights and device coefficient pointers.
+struct ImageSpec {
+    uint32_t nch;
+    const ArtChannel *ch;
+    const void *src[3];
+    float weight;
+    float pweight[3];
+    uint32_t W, H;
 };
 
 }  // namespace
@@ -615,35 +629,60 @@ struct GraphKey {
 struct ArtContext {
     int device = 0;
     cudaStream_t stream = nullptr;
-    art::DevBuf xbuf, gbuf, pbuf, coefimg, stage, misc, desc, work, tasks, compat, sepplanes, rgb;
-    art::ImgDev *h_desc = nullptr;  // host copy of the descriptor (pageable: copies of it are staged)
-    std::vector<int2> h_work;       // gradient-sweep blocks: {image, block index in image}
-    std::vector<int4> h_tasks;      // all block warps: {image, channel, block row, first block}
-    int mode_off[5] = {0, 0, 0, 0, 0};  // h_tasks sorted by sampling mode (1x1, 2x2, 2x1, 1x2)
+    art::DevBuf xbuf, pbuf, coefimg, stage, misc, desc, work, tasks, compat, sepplanes, rgb;
+    std::vector<art::ImgDev> h_desc;  // per image (pageable: copies of it are staged)
+    std::vector<int2> h_work;         // sweep blocks {image, block in image}, grouped by channel count 3, 2, 1
+    int wstart[4] = {0, 0, 0, 0}, wcount[4] = {0, 0, 0, 0};  // by channel count
+    std::vector<int4> h_tasks;        // block warps {image, channel, block row, first block}
+    int mode_off[5] = {0, 0, 0, 0, 0};  // h_tasks grouped by sampling mode (1x1, 2x2, 2x1, 1x2)
+    unsigned *errflag = nullptr;
     cudaGraphExec_t exec = nullptr;
     art::GraphKey key;
     bool timing = false;
     std::vector<cudaEvent_t> events;  // [0,1] loop; then 4 per iteration
     uint32_t timed_iterations = 0;
-    int strip_rows_override = 0;      // 0 = chosen per image size
-    float *final_planes = nullptr;    // device planes holding the result of the last solve
-    int final_pitch = 0;
-    long long final_cstride = 0;
+    int strip_rows_override = 0;      // 0 = tuning cache, else size heuristic
+    std::map<std::string, int> tune;  // autotuned strip rows by geometry bucket
 };
 
 namespace art {
 namespace {
 
-// Rows per gradient-sweep strip: enough strips to fill every SM several times
-// over, and as long as that allows so the 3 extra rows a strip reads stay small.
-int pick_strip_rows(const ArtContext *ctx, int W, int H)
+int pow2_bucket(uint32_t v)
+{
+    int b = 256;
+    while ((uint32_t)b < v && b < 65536) b *= 2;
+    return b;
+}
+
+// Key of a geometry bucket for the autotuner: channel count, sampling of
+// each channel, width and height rounded up to a power of two.
+std::string tune_key(uint32_t nch, const uint32_t *sh, const uint32_t *sv, uint32_t W, uint32_t H)
+{
+    std::string k = "n" + std::to_string(nch) + "-s";
+    for (uint32_t c = 0; c < nch; c++) k += std::to_string(sh[c]) + std::to_string(sv[c]);
+    k += "-w" + std::to_string(pow2_bucket(W)) + "-h" + std::to_string(pow2_bucket(H));
+    return k;
+}
+
+// Rows per gradient-sweep strip for one image: the autotuner's choice for its
+// bucket, else enough strips (over the whole batch) to fill every SM several
+// times over with strips as long as that allows, so the 3 extra rows a strip
+// reads stay small.
+int pick_strip_rows(const ArtContext *ctx, const ImageSpec &sp, long long batch_px)
 {
     if (ctx->strip_rows_override > 0) return ctx->strip_rows_override;
     const char *env = getenv("ART_STRIP_ROWS");
     if (env && atoi(env) > 0) return atoi(env);
-    const long long strips_x = (W + SWEEP_OUT - 1) / SWEEP_OUT;
+    uint32_t sh[3], sv[3];
+    for (uint32_t c = 0; c < sp.nch; c++) {
+        sh[c] = sp.ch[c].samp_h;
+        sv[c] = sp.ch[c].samp_v;
+    }
+    auto it = ctx->tune.find(tune_key(sp.nch, sh, sv, sp.W, sp.H));
+    if (it != ctx->tune.end()) return it->second;
     int R = 128;
-    while (R > 32 && strips_x * ((H + R - 1) / R) < 148LL * 16) R /= 2;
+    while (R > 32 && batch_px / ((long long)SWEEP_OUT * R) < 148LL * 16) R /= 2;
     return R;
 }
 
@@ -699,6 +738,8 @@ int validate(uint32_t nch, const ArtChannel *ch, float weight, const float *pwei
                 return fail(ART_ERR_INVALID_DATA, "quantisation steps must lie in (0, 65535]");
         }
     }
+    if (3LL * (long long)align_up(W, 32) * (long long)align_up(H, 32) >= (1LL << 31))
+        return fail(ART_ERR_INVALID_ARGUMENT, "image too large: three padded planes must stay below 2^31 floats");
     return ART_OK;
 }
 
@@ -707,10 +748,10 @@ int validate(uint32_t nch, const ArtChannel *ch, float weight, const float *pwei
 // Sampling mode of a component: 0 = 1x1, 1 = 2x2, 2 = 2x1 (h x v), 3 = 1x2.
 static int samp_mode(int sh, int sv) { return sh == 1 ? (sv == 1 ? 0 : 3) : (sv == 2 ? 1 : 2); }
 
-// Block tasks of one image grouped by sampling mode; inside a mode bottom
+// Block tasks of one image appended per sampling mode; inside a mode bottom
 // rows first and channels interleaved by full-resolution row band, so the
 // projection starts on the rows the gradient sweep touched last (still in L2).
-static void build_tasks(const ImgDev &d, int img, std::vector<int4> &out, int mode_off[5])
+static void build_tasks(const ImgDev &d, int img, std::vector<int4> per_mode[4])
 {
     struct Key {
         int mode, row, c, by, bx0;
@@ -723,166 +764,174 @@ static void build_tasks(const ImgDev &d, int img, std::vector<int4> &out, int mo
             for (int bx0 = 0; bx0 < bw; bx0 += 4) keys.push_back({samp_mode(cd.sh, cd.sv), by * 8 * cd.sv, c, by, bx0});
     }
     std::stable_sort(keys.begin(), keys.end(), [](const Key &a, const Key &b) {
-        if (a.mode != b.mode) return a.mode < b.mode;
         if (a.row != b.row) return a.row > b.row;
         return a.c < b.c;
     });
-    for (int m = 0; m < 5; m++) mode_off[m] = 0;
-    for (const Key &k : keys) {
-        out.push_back(make_int4(img, k.c, k.by, k.bx0));
-        mode_off[k.mode + 1]++;
-    }
-    for (int m = 1; m < 5; m++) mode_off[m] += mode_off[m - 1];
+    for (const Key &k : keys) per_mode[k.mode].push_back(make_int4(img, k.c, k.by, k.bx0));
 }
 
-// Lays out buffers for one image, uploads descriptors, ingests coefficients
-// and queues the initialisation. `coef_src[c]` is a device pointer.
-static int prepare(ArtContext *ctx, uint32_t nch, const ArtChannel *ch, const void *const *coef_src, float weight,
-                   const float *pweight, uint32_t iterations, uint32_t W, uint32_t H, int init_mode)
+// Lays out the buffers of a batch of images, uploads descriptors and work
+// lists, ingests coefficients and queues the initialisation.
+static int prepare_batch(ArtContext *ctx, const std::vector<ImageSpec> &specs, uint32_t iterations, int init_mode)
 {
     int rc;
-    const int pitch = (int)align_up(W, 32);
-    const size_t rows = align_up(H, 32);
-    const long long cstride = (long long)pitch * (long long)rows;
-    if (3 * cstride >= (1LL << 31))
-        return fail(ART_ERR_INVALID_ARGUMENT, "image too large: three padded planes must stay below 2^31 floats");
-    const int R = pick_strip_rows(ctx, (int)W, (int)H);
-    const int strips_x = (int)((W + SWEEP_OUT - 1) / SWEEP_OUT), strips_y = (int)((H + R - 1) / R);
-    const int nstrips = strips_x * strips_y;
-    const int ncta = (nstrips + SWEEP_WARPS - 1) / SWEEP_WARPS;
-
-    if ((rc = ctx->xbuf.ensure(2 * 3 * cstride * sizeof(float)))) return rc;  // x and y
-    if ((rc = ctx->gbuf.ensure(3 * cstride * sizeof(float)))) return rc;
-    size_t coef_bytes = 0, p_floats = 0;
-    size_t coef_off[3], p_off[3];
-    int cpitch[3], ppitch[3];
-    for (uint32_t c = 0; c < nch; c++) {
-        cpitch[c] = (int)align_up(ch[c].rounded_px_w, 64);
-        coef_off[c] = coef_bytes;
-        coef_bytes += align_up((size_t)cpitch[c] * ch[c].rounded_px_h * sizeof(int16_t), 256);
-        ppitch[c] = (int)align_up(ch[c].rounded_px_w, 32);
-        p_off[c] = p_floats;
-        p_floats += align_up((size_t)ppitch[c] * ch[c].rounded_px_h, 64);
-    }
-    if ((rc = ctx->coefimg.ensure(coef_bytes))) return rc;
-    if ((rc = ctx->pbuf.ensure(p_floats * sizeof(float)))) return rc;
-    const size_t misc_bytes = align_up((size_t)ncta * 4 * sizeof(float), 256) + 256;
-    if ((rc = ctx->misc.ensure(misc_bytes))) return rc;
-    if ((rc = ctx->desc.ensure(sizeof(ImgDev)))) return rc;
-    if (!ctx->h_desc) ctx->h_desc = new ImgDev();
-
-    ImgDev &d = *ctx->h_desc;
-    memset(&d, 0, sizeof(d));
-    d.nch = (int)nch;
-    d.W = (int)W;
-    d.H = (int)H;
-    d.pitch = pitch;
-    d.strips_x = strips_x;
-    d.strips_y = strips_y;
-    d.nstrips = nstrips;
-    d.strip_rows = R;
-    d.ncta = ncta;
-    d.cstride = cstride;
-    d.x = static_cast<float *>(ctx->xbuf.p);
-    d.y = d.x + 3 * cstride;
-    d.g = static_cast<float *>(ctx->gbuf.p);
-    // compute_step_tv.rs:130 and compute_step_tv2.rs:88-89, compute_step.rs:47.
-    d.alpha_tv = 1.0f / sqrtf((float)nch);
-    d.alpha_tgv = (weight / sqrtf(2.0f)) / sqrtf((float)nch);
-    // mod.rs:45 and :71.
-    const float radius = sqrtf((float)((uint64_t)W * H)) / 2.0f;
-    d.step = radius / sqrtf(1.0f + (float)iterations);
-    char *misc = static_cast<char *>(ctx->misc.p);
-    d.partial = reinterpret_cast<float *>(misc);
-    d.sigma = reinterpret_cast<float *>(misc + align_up((size_t)ncta * 4 * sizeof(float), 256));
-    d.counter = reinterpret_cast<unsigned *>(d.sigma + 4);
-    unsigned *errflag = d.counter + 1;
-    for (uint32_t c = 0; c < nch; c++) {
-        ChanDev &cd = d.ch[c];
-        cd.cw = (int)ch[c].rounded_px_w;
-        cd.chh = (int)ch[c].rounded_px_h;
-        cd.sh = (int)ch[c].samp_h;
-        cd.sv = (int)ch[c].samp_v;
-        cd.cpitch = cpitch[c];
-        cd.ppitch = ppitch[c];
-        cd.coef = reinterpret_cast<const int16_t *>(static_cast<char *>(ctx->coefimg.p) + coef_off[c]);
-        cd.P = static_cast<float *>(ctx->pbuf.p) + p_off[c];
-        // compute_step.rs:20-31: alpha = pweight * 2 * 255 * sqrt(2).
-        cd.alpha_p = pweight[c] * 2.0f * 255.0f * sqrtf(2.0f);
-        for (int j = 0; j < 64; j++) {
-            const float q = ch[c].quant_table[j];
-            d.q[c][j] = q;
-            d.invq2[c][j] = 1.0f / (q * q);
+    const int nimg = (int)specs.size();
+    long long batch_px = 0;
+    for (const auto &sp : specs) batch_px += (long long)sp.W * sp.H;
+    std::vector<size_t> o_x(nimg), o_misc(nimg);
+    std::vector<std::array<size_t, 3>> o_coef(nimg), o_p(nimg);
+    size_t x_floats = 0, coef_bytes = 0, p_floats = 0, misc_bytes = 256;  // misc starts with the error flag
+    ctx->h_desc.assign(nimg, ImgDev());
+    for (int i = 0; i < nimg; i++) {
+        const ImageSpec &sp = specs[i];
+        ImgDev &d = ctx->h_desc[i];
+        memset(&d, 0, sizeof(d));
+        const int pitch = (int)align_up(sp.W, 32);
+        const long long cstride = (long long)pitch * (long long)align_up(sp.H, 32);
+        const int R = pick_strip_rows(ctx, sp, batch_px);
+        d.nch = (int)sp.nch;
+        d.W = (int)sp.W;
+        d.H = (int)sp.H;
+        d.pitch = pitch;
+        d.strip_rows = R;
+        d.strips_x = (int)((sp.W + SWEEP_OUT - 1) / SWEEP_OUT);
+        d.strips_y = (int)((sp.H + R - 1) / R);
+        d.nstrips = d.strips_x * d.strips_y;
+        d.ncta = (d.nstrips + SWEEP_WARPS - 1) / SWEEP_WARPS;
+        d.cstride = cstride;
+        // compute_step_tv.rs:130 and compute_step_tv2.rs:88-89, compute_step.rs:47.
+        d.alpha_tv = 1.0f / sqrtf((float)sp.nch);
+        d.alpha_tgv = (sp.weight / sqrtf(2.0f)) / sqrtf((float)sp.nch);
+        // mod.rs:45 and :71.
+        d.step = (sqrtf((float)((uint64_t)sp.W * sp.H)) / 2.0f) / sqrtf(1.0f + (float)iterations);
+        o_x[i] = x_floats;
+        x_floats += align_up((size_t)3 * sp.nch * cstride, 64);
+        o_misc[i] = misc_bytes;
+        misc_bytes += align_up((size_t)d.ncta * 4 * sizeof(float), 256) + 256;
+        for (uint32_t c = 0; c < sp.nch; c++) {
+            ChanDev &cd = d.ch[c];
+            cd.cw = (int)sp.ch[c].rounded_px_w;
+            cd.chh = (int)sp.ch[c].rounded_px_h;
+            cd.sh = (int)sp.ch[c].samp_h;
+            cd.sv = (int)sp.ch[c].samp_v;
+            cd.cpitch = (int)align_up(cd.cw, 64);
+            cd.ppitch = (int)align_up(cd.cw, 32);
+            // compute_step.rs:20-31: alpha = pweight * 2 * 255 * sqrt(2).
+            cd.alpha_p = sp.pweight[c] * 2.0f * 255.0f * sqrtf(2.0f);
+            o_coef[i][c] = coef_bytes;
+            coef_bytes += align_up((size_t)cd.cpitch * cd.chh * sizeof(int16_t), 256);
+            o_p[i][c] = p_floats;
+            p_floats += align_up((size_t)cd.ppitch * cd.chh, 64);
+            for (int j = 0; j < 64; j++) {
+                const float q = sp.ch[c].quant_table[j];
+                d.q[c][j] = q;
+                d.invq2[c][j] = 1.0f / (q * q);
+            }
         }
     }
-    ctx->h_work.resize(ncta);
-    for (int i = 0; i < ncta; i++) ctx->h_work[i] = make_int2(0, i);
+    if ((rc = ctx->xbuf.ensure(x_floats * sizeof(float)))) return rc;
+    if ((rc = ctx->coefimg.ensure(coef_bytes))) return rc;
+    if ((rc = ctx->pbuf.ensure(p_floats * sizeof(float)))) return rc;
+    if ((rc = ctx->misc.ensure(misc_bytes))) return rc;
+    if ((rc = ctx->desc.ensure(nimg * sizeof(ImgDev)))) return rc;
+    float *xb = static_cast<float *>(ctx->xbuf.p);
+    char *misc = static_cast<char *>(ctx->misc.p);
+    ctx->errflag = reinterpret_cast<unsigned *>(misc);
+    std::vector<int2> wk[4];
+    std::vector<int4> per_mode[4];
+    for (int i = 0; i < nimg; i++) {
+        ImgDev &d = ctx->h_desc[i];
+        d.x = xb + o_x[i];
+        d.y = d.x + d.nch * d.cstride;
+        d.g = d.y + d.nch * d.cstride;
+        d.partial = reinterpret_cast<float *>(misc + o_misc[i]);
+        d.sigma = reinterpret_cast<float *>(misc + o_misc[i] + align_up((size_t)d.ncta * 4 * sizeof(float), 256));
+        d.counter = reinterpret_cast<unsigned *>(d.sigma + 4);
+        for (int c = 0; c < d.nch; c++) {
+            d.ch[c].coef = reinterpret_cast<const int16_t *>(static_cast<char *>(ctx->coefimg.p) + o_coef[i][c]);
+            d.ch[c].P = static_cast<float *>(ctx->pbuf.p) + o_p[i][c];
+        }
+        for (int b = 0; b < d.ncta; b++) wk[d.nch].push_back(make_int2(i, b));
+        build_tasks(d, i, per_mode);
+    }
+    ctx->h_work.clear();
+    for (int n = 3; n >= 1; n--) {
+        ctx->wstart[n] = (int)ctx->h_work.size();
+        ctx->wcount[n] = (int)wk[n].size();
+        ctx->h_work.insert(ctx->h_work.end(), wk[n].begin(), wk[n].end());
+    }
     ctx->h_tasks.clear();
-    build_tasks(d, 0, ctx->h_tasks, ctx->mode_off);
-    const int ntasks = (int)ctx->h_tasks.size();
-    if ((rc = ctx->work.ensure(ncta * sizeof(int2)))) return rc;
+    for (int m = 0; m < 4; m++) {
+        ctx->mode_off[m] = (int)ctx->h_tasks.size();
+        ctx->h_tasks.insert(ctx->h_tasks.end(), per_mode[m].begin(), per_mode[m].end());
+    }
+    ctx->mode_off[4] = (int)ctx->h_tasks.size();
+    const int nwork = (int)ctx->h_work.size(), ntasks = (int)ctx->h_tasks.size();
+    if ((rc = ctx->work.ensure(nwork * sizeof(int2)))) return rc;
     if ((rc = ctx->tasks.ensure(ntasks * sizeof(int4)))) return rc;
 
     cudaStream_t s = ctx->stream;
-    ART_CUDA(cudaMemcpyAsync(ctx->desc.p, &d, sizeof(ImgDev), cudaMemcpyHostToDevice, s));
-    ART_CUDA(cudaMemcpyAsync(ctx->work.p, ctx->h_work.data(), ncta * sizeof(int2), cudaMemcpyHostToDevice, s));
+    ART_CUDA(cudaMemcpyAsync(ctx->desc.p, ctx->h_desc.data(), nimg * sizeof(ImgDev), cudaMemcpyHostToDevice, s));
+    ART_CUDA(cudaMemcpyAsync(ctx->work.p, ctx->h_work.data(), nwork * sizeof(int2), cudaMemcpyHostToDevice, s));
     ART_CUDA(cudaMemcpyAsync(ctx->tasks.p, ctx->h_tasks.data(), ntasks * sizeof(int4), cudaMemcpyHostToDevice, s));
     ART_CUDA(cudaMemsetAsync(ctx->misc.p, 0, misc_bytes, s));
     // The first DCT-distance gradient is zero: the reference starts from cos = c q (coef.rs:94-104).
     ART_CUDA(cudaMemsetAsync(ctx->pbuf.p, 0, p_floats * sizeof(float), s));
     const ImgDev *ddesc = static_cast<const ImgDev *>(ctx->desc.p);
-    for (uint32_t c = 0; c < nch; c++) {
-        const long long ncoef = (long long)ch[c].block_w * ch[c].block_h * 64;
-        const int blocks = (int)((ncoef + 255) / 256);
-        k_ingest<<<blocks, 256, 0, s>>>(coef_src[c], (int)ch[c].coef_type, (int)ch[c].block_w, ncoef,
-                                        const_cast<int16_t *>(d.ch[c].coef), cpitch[c], errflag);
+    for (int i = 0; i < nimg; i++) {
+        const ImageSpec &sp = specs[i];
+        for (uint32_t c = 0; c < sp.nch; c++) {
+            const long long ncoef = (long long)sp.ch[c].block_w * sp.ch[c].block_h * 64;
+            k_ingest<<<(int)((ncoef + 255) / 256), 256, 0, s>>>(
+                sp.src[c], (int)sp.ch[c].coef_type, (int)sp.ch[c].block_w, ncoef,
+                const_cast<int16_t *>(ctx->h_desc[i].ch[c].coef), ctx->h_desc[i].ch[c].cpitch, ctx->errflag);
+        }
     }
     if (init_mode == ART_INIT_SCALAR_COMPAT) {
         size_t need = 0;
-        for (uint32_t c = 0; c < nch; c++) need = std::max(need, (size_t)ch[c].rounded_px_w * ch[c].rounded_px_h);
+        for (const auto &sp : specs)
+            for (uint32_t c = 0; c < sp.nch; c++)
+                need = std::max(need, (size_t)sp.ch[c].rounded_px_w * sp.ch[c].rounded_px_h);
         if ((rc = ctx->compat.ensure(2 * need * sizeof(float)))) return rc;
-        for (uint32_t c = 0; c < nch; c++) {
-            const long long nc = (long long)ch[c].rounded_px_w * ch[c].rounded_px_h;
-            float *a = static_cast<float *>(ctx->compat.p), *b = a + need;
-            ART_CUDA(cudaMemsetAsync(a, 0, nc * sizeof(float), s));
-            const int nb = (int)(ch[c].block_w * ch[c].block_h);
-            const int grid = (int)((nc + 255) / 256);
-            for (int i = 0; i < nb; i++) {
-                k_compat_step<<<grid, 256, 0, s>>>(a, b, ddesc, (int)c, i, nc);
-                std::swap(a, b);
+        for (int i = 0; i < nimg; i++) {
+            const ImageSpec &sp = specs[i];
+            for (uint32_t c = 0; c < sp.nch; c++) {
+                const long long nc = (long long)sp.ch[c].rounded_px_w * sp.ch[c].rounded_px_h;
+                float *a = static_cast<float *>(ctx->compat.p), *b = a + need;
+                ART_CUDA(cudaMemsetAsync(a, 0, nc * sizeof(float), s));
+                const int nb = (int)(sp.ch[c].block_w * sp.ch[c].block_h);
+                const int grid = (int)((nc + 255) / 256);
+                for (int blk = 0; blk < nb; blk++) {
+                    k_compat_step<<<grid, 256, 0, s>>>(a, b, ddesc + i, (int)c, blk, nc);
+                    std::swap(a, b);
+                }
+                k_upsample<<<(int)(((long long)sp.W * sp.H + 255) / 256), 256, 0, s>>>(a, ddesc + i, (int)c);
             }
-            k_upsample<<<(int)(((long long)W * H + 255) / 256), 256, 0, s>>>(a, ddesc, (int)c);
         }
     } else {
         k_init<<<(ntasks + PROJ_WARPS - 1) / PROJ_WARPS, PROJ_WARPS * 32, 0, s>>>(
             ddesc, static_cast<const int4 *>(ctx->tasks.p), ntasks);
     }
     ART_CUDA(cudaGetLastError());
-    ctx->final_planes = d.x;
-    ctx->final_pitch = pitch;
-    ctx->final_cstride = cstride;
     return ART_OK;
 }
 
 static void launch_iteration(ArtContext *ctx, int it, float fnext)
 {
-    const ImgDev &d = *ctx->h_desc;
     const ImgDev *ddesc = static_cast<const ImgDev *>(ctx->desc.p);
     const int2 *work = static_cast<const int2 *>(ctx->work.p);
     const int4 *tasks = static_cast<const int4 *>(ctx->tasks.p);
-    const int ntasks = (int)ctx->h_tasks.size();
     cudaStream_t s = ctx->stream;
     const bool tm = ctx->timing;
     if (tm) cudaEventRecordWithFlags(ctx->events[2 + 4 * it], s, cudaEventRecordExternal);
-    if (d.nch == 3)
-        k_grad_sweep<3><<<d.ncta, SWEEP_WARPS * 32, 0, s>>>(ddesc, work);
-    else if (d.nch == 2)
-        k_grad_sweep<2><<<d.ncta, SWEEP_WARPS * 32, 0, s>>>(ddesc, work);
-    else
-        k_grad_sweep<1><<<d.ncta, SWEEP_WARPS * 32, 0, s>>>(ddesc, work);
+    if (ctx->wcount[3])
+        k_grad_sweep<3><<<ctx->wcount[3], SWEEP_WARPS * 32, 0, s>>>(ddesc, work + ctx->wstart[3]);
+    if (ctx->wcount[2])
+        k_grad_sweep<2><<<ctx->wcount[2], SWEEP_WARPS * 32, 0, s>>>(ddesc, work + ctx->wstart[2]);
+    if (ctx->wcount[1])
+        k_grad_sweep<1><<<ctx->wcount[1], SWEEP_WARPS * 32, 0, s>>>(ddesc, work + ctx->wstart[1]);
     if (tm) cudaEventRecordWithFlags(ctx->events[3 + 4 * it], s, cudaEventRecordExternal);
     if (tm) cudaEventRecordWithFlags(ctx->events[4 + 4 * it], s, cudaEventRecordExternal);
-    (void)ntasks;
     for (int m = 3; m >= 0; m--) {
         const int n = ctx->mode_off[m + 1] - ctx->mode_off[m];
         if (n == 0) continue;
@@ -900,9 +949,10 @@ static void launch_iteration(ArtContext *ctx, int it, float fnext)
     if (tm) cudaEventRecordWithFlags(ctx->events[5 + 4 * it], s, cudaEventRecordExternal);
 }
 
+// Replays (capturing first if the work changed shape) the fixed-count
+// iteration loop as one CUDA graph.
 static int run_iterations(ArtContext *ctx, uint32_t iterations)
 {
-    const ImgDev &d = *ctx->h_desc;
     if (iterations == 0) return ART_OK;
     if (ctx->timing) {
         const size_t need = 2 + 4 * (size_t)iterations;
@@ -913,9 +963,8 @@ static int run_iterations(ArtContext *ctx, uint32_t iterations)
         }
     }
     GraphKey key;
-    key.nch = d.nch;
-    key.ncta = d.ncta;
-    key.ntasks = (int)ctx->h_tasks.size();
+    key.nimg = (int)ctx->h_desc.size();
+    std::copy(ctx->wcount, ctx->wcount + 4, key.wcount);
     std::copy(ctx->mode_off, ctx->mode_off + 5, key.mode_off);
     key.iterations = iterations;
     key.timing = ctx->timing;
@@ -951,11 +1000,20 @@ static int run_iterations(ArtContext *ctx, uint32_t iterations)
     return ART_OK;
 }
 
+// Result planes of image i: base pointer, pitch and channel stride.
+static void result_planes(const ArtContext *ctx, int i, const float **base, int *pitch, long long *cstride)
+{
+    const ImgDev &d = ctx->h_desc[i];
+    *base = d.x;
+    *pitch = d.pitch;
+    *cstride = d.cstride;
+}
+
 static int check_errflag(ArtContext *ctx)
 {
+    if (!ctx->errflag) return ART_OK;
     unsigned flag = 0;
-    const ImgDev &d = *ctx->h_desc;
-    ART_CUDA(cudaMemcpy(&flag, d.counter + 1, sizeof(unsigned), cudaMemcpyDeviceToHost));
+    ART_CUDA(cudaMemcpy(&flag, ctx->errflag, sizeof(unsigned), cudaMemcpyDeviceToHost));
     if (flag) return fail(ART_ERR_INVALID_DATA, "coefficients must be integers in [-32768, 32767]");
     return ART_OK;
 }
@@ -1000,7 +1058,6 @@ void art_context_destroy(ArtContext *ctx)
     if (ctx->exec) cudaGraphExecDestroy(ctx->exec);
     for (auto e : ctx->events) cudaEventDestroy(e);
     ctx->xbuf.release();
-    ctx->gbuf.release();
     ctx->pbuf.release();
     ctx->work.release();
     ctx->tasks.release();
@@ -1011,7 +1068,6 @@ void art_context_destroy(ArtContext *ctx)
     ctx->compat.release();
     ctx->sepplanes.release();
     ctx->rgb.release();
-    delete ctx->h_desc;
     if (ctx->stream) cudaStreamDestroy(ctx->stream);
     delete ctx;
 }
@@ -1069,16 +1125,20 @@ int32_t art_context_compute_device(ArtContext *ctx, uint32_t nchannel, const Art
         ART_CUDA(cudaEventRecord(join, user));
         ART_CUDA(cudaStreamWaitEvent(ctx->stream, join, 0));
     }
-    const void *src[3];
-    for (uint32_t c = 0; c < nchannel; c++) src[c] = coefs[c].dct_coefs;
-    rc = prepare(ctx, nchannel, coefs, src, weight, pweight, iterations, max_w, max_h, init_mode);
+    ImageSpec sp{nchannel, coefs, {nullptr, nullptr, nullptr}, weight, {pweight[0], pweight[1], pweight[2]}, max_w,
+                 max_h};
+    for (uint32_t c = 0; c < nchannel; c++) sp.src[c] = coefs[c].dct_coefs;
+    rc = prepare_batch(ctx, {sp}, iterations, init_mode);
     if (!rc) rc = run_iterations(ctx, iterations);
     if (!rc) {
+        const float *fb;
+        int fp;
+        long long fcs;
+        result_planes(ctx, 0, &fb, &fp, &fcs);
         for (uint32_t c = 0; c < nchannel; c++) {
-            cudaError_t e = cudaMemcpy2DAsync(out_planes_device[c], (size_t)out_pitch * sizeof(float),
-                                              ctx->final_planes + c * ctx->final_cstride,
-                                              (size_t)ctx->final_pitch * sizeof(float), (size_t)max_w * sizeof(float),
-                                              max_h, cudaMemcpyDeviceToDevice, ctx->stream);
+            cudaError_t e = cudaMemcpy2DAsync(out_planes_device[c], (size_t)out_pitch * sizeof(float), fb + c * fcs,
+                                              (size_t)fp * sizeof(float), (size_t)max_w * sizeof(float), max_h,
+                                              cudaMemcpyDeviceToDevice, ctx->stream);
             if (e != cudaSuccess) rc = fail(ART_ERR_CUDA, std::string("output copy: ") + cudaGetErrorString(e));
         }
     }
@@ -1097,8 +1157,7 @@ int32_t art_context_synchronize(ArtContext *ctx)
     if (!ctx) return fail(ART_ERR_INVALID_ARGUMENT, "null context");
     ART_CUDA(cudaSetDevice(ctx->device));
     ART_CUDA(cudaStreamSynchronize(ctx->stream));
-    if (ctx->h_desc) return check_errflag(ctx);
-    return ART_OK;
+    return check_errflag(ctx);
 }
 
 static int solve_host(ArtContext *ctx, uint32_t nchannel, const ArtChannel *coefs, float weight,
@@ -1116,15 +1175,16 @@ static int solve_host(ArtContext *ctx, uint32_t nchannel, const ArtChannel *coef
         total += align_up((size_t)coefs[c].block_w * coefs[c].block_h * 64 * es, 256);
     }
     if ((rc = ctx->stage.ensure(total))) return rc;
-    const void *src[3];
+    ImageSpec sp{nchannel, coefs, {nullptr, nullptr, nullptr}, weight, {pweight[0], pweight[1], pweight[2]}, max_w,
+                 max_h};
     for (uint32_t c = 0; c < nchannel; c++) {
         const size_t es = coefs[c].coef_type == ART_COEF_I16 ? 2 : 4;
         char *dst = static_cast<char *>(ctx->stage.p) + off[c];
         ART_CUDA(cudaMemcpyAsync(dst, coefs[c].dct_coefs, (size_t)coefs[c].block_w * coefs[c].block_h * 64 * es,
                                  cudaMemcpyHostToDevice, ctx->stream));
-        src[c] = dst;
+        sp.src[c] = dst;
     }
-    rc = prepare(ctx, nchannel, coefs, src, weight, pweight, iterations, max_w, max_h, init_mode);
+    rc = prepare_batch(ctx, {sp}, iterations, init_mode);
     if (!rc) rc = run_iterations(ctx, iterations);
     return rc;
 }
@@ -1144,10 +1204,14 @@ int32_t art_context_compute(ArtContext *ctx, uint32_t nchannel, const ArtChannel
         cudaStreamSynchronize(ctx->stream);
         return rc;
     }
+    const float *fb;
+    int fp;
+    long long fcs;
+    result_planes(ctx, 0, &fb, &fp, &fcs);
     for (uint32_t c = 0; c < nchannel; c++)
-        ART_CUDA(cudaMemcpy2DAsync(out_planes[c], (size_t)max_w * sizeof(float),
-                                   ctx->final_planes + c * ctx->final_cstride, (size_t)ctx->final_pitch * sizeof(float),
-                                   (size_t)max_w * sizeof(float), max_h, cudaMemcpyDeviceToHost, ctx->stream));
+        ART_CUDA(cudaMemcpy2DAsync(out_planes[c], (size_t)max_w * sizeof(float), fb + c * fcs,
+                                   (size_t)fp * sizeof(float), (size_t)max_w * sizeof(float), max_h,
+                                   cudaMemcpyDeviceToHost, ctx->stream));
     ART_CUDA(cudaStreamSynchronize(ctx->stream));
     return check_errflag(ctx);
 }
@@ -1180,8 +1244,12 @@ int32_t art_context_process(ArtContext *ctx, uint32_t nchannel, const ArtChannel
             cudaStreamSynchronize(ctx->stream);
             return rc;
         }
-        for (int c = 0; c < 3; c++) planes[c] = ctx->final_planes + c * ctx->final_cstride;
-        pitch = ctx->final_pitch;
+        const float *fb;
+        int fp;
+        long long fcs;
+        result_planes(ctx, 0, &fb, &fp, &fcs);
+        for (int c = 0; c < 3; c++) planes[c] = fb + c * fcs;
+        pitch = fp;
     } else {
         // lib.rs:133-153: each component alone, compute(1, [coef], weight[c], pweight, iterations[c]),
         // so every component uses pweight[0].
@@ -1197,9 +1265,12 @@ int32_t art_context_process(ArtContext *ctx, uint32_t nchannel, const ArtChannel
             }
             if (c < nout) {
                 float *dst = static_cast<float *>(ctx->sepplanes.p) + c * plane;
-                ART_CUDA(cudaMemcpy2DAsync(dst, (size_t)W * sizeof(float), ctx->final_planes,
-                                           (size_t)ctx->final_pitch * sizeof(float), (size_t)W * sizeof(float), H,
-                                           cudaMemcpyDeviceToDevice, ctx->stream));
+                const float *fb;
+                int fp;
+                long long fcs;
+                result_planes(ctx, 0, &fb, &fp, &fcs);
+                ART_CUDA(cudaMemcpy2DAsync(dst, (size_t)W * sizeof(float), fb, (size_t)fp * sizeof(float),
+                                           (size_t)W * sizeof(float), H, cudaMemcpyDeviceToDevice, ctx->stream));
                 planes[c] = dst;
             }
             ART_CUDA(cudaStreamSynchronize(ctx->stream));
@@ -1219,6 +1290,229 @@ int32_t art_context_process(ArtContext *ctx, uint32_t nchannel, const ArtChannel
     }
     ART_CUDA(cudaStreamSynchronize(ctx->stream));
     return check_errflag(ctx);
+}
+
+
+// ---------------------------------------------------------------- batches --
+
+static int batch_specs(const ArtImage *images, uint32_t nimages, std::vector<ImageSpec> &specs)
+{
+    specs.clear();
+    for (uint32_t i = 0; i < nimages; i++) {
+        const ArtImage &im = images[i];
+        int rc = validate(im.nchannel, im.channels, im.weight, im.pweight, im.max_rounded_px_w, im.max_rounded_px_h);
+        if (rc) return fail(rc, "image " + std::to_string(i) + ": " + g_err);
+        if (!im.out_planes) return fail(ART_ERR_INVALID_ARGUMENT, "image " + std::to_string(i) + ": null output planes");
+        for (uint32_t c = 0; c < im.nchannel; c++)
+            if (!im.out_planes[c]) return fail(ART_ERR_INVALID_ARGUMENT, "image " + std::to_string(i) + ": null plane");
+        ImageSpec sp{im.nchannel, im.channels, {nullptr, nullptr, nullptr}, im.weight,
+                     {im.pweight[0], im.pweight[1], im.pweight[2]}, im.max_rounded_px_w, im.max_rounded_px_h};
+        for (uint32_t c = 0; c < im.nchannel; c++) sp.src[c] = im.channels[c].dct_coefs;
+        specs.push_back(sp);
+    }
+    return ART_OK;
+}
+
+int32_t art_context_compute_batch(ArtContext *ctx, uint32_t nimages, const ArtImage *images, uint32_t iterations,
+                                  const ArtOptions *opts)
+{
+    if (!ctx || !images || nimages == 0) return fail(ART_ERR_INVALID_ARGUMENT, "null context or empty batch");
+    ART_CUDA(cudaSetDevice(ctx->device));
+    const int init_mode = opts ? (int)opts->init_mode : ART_INIT_DECODED;
+    std::vector<ImageSpec> specs;
+    int rc = batch_specs(images, nimages, specs);
+    if (rc) return rc;
+    // Host coefficients of every image through one device staging buffer.
+    size_t total = 0;
+    for (auto &sp : specs)
+        for (uint32_t c = 0; c < sp.nch; c++)
+            total += align_up((size_t)sp.ch[c].block_w * sp.ch[c].block_h * 64 *
+                                  (sp.ch[c].coef_type == ART_COEF_I16 ? 2 : 4), 256);
+    if ((rc = ctx->stage.ensure(total))) return rc;
+    size_t off = 0;
+    for (auto &sp : specs)
+        for (uint32_t c = 0; c < sp.nch; c++) {
+            const size_t n = (size_t)sp.ch[c].block_w * sp.ch[c].block_h * 64 * (sp.ch[c].coef_type == ART_COEF_I16 ? 2 : 4);
+            char *dst = static_cast<char *>(ctx->stage.p) + off;
+            ART_CUDA(cudaMemcpyAsync(dst, sp.ch[c].dct_coefs, n, cudaMemcpyHostToDevice, ctx->stream));
+            sp.src[c] = dst;
+            off += align_up(n, 256);
+        }
+    rc = prepare_batch(ctx, specs, iterations, init_mode);
+    if (!rc) rc = run_iterations(ctx, iterations);
+    if (rc) {
+        cudaStreamSynchronize(ctx->stream);
+        return rc;
+    }
+    for (uint32_t i = 0; i < nimages; i++) {
+        const float *fb;
+        int fp;
+        long long fcs;
+        result_planes(ctx, (int)i, &fb, &fp, &fcs);
+        const ArtImage &im = images[i];
+        for (uint32_t c = 0; c < im.nchannel; c++)
+            ART_CUDA(cudaMemcpy2DAsync(im.out_planes[c], (size_t)im.max_rounded_px_w * sizeof(float), fb + c * fcs,
+                                       (size_t)fp * sizeof(float), (size_t)im.max_rounded_px_w * sizeof(float),
+                                       im.max_rounded_px_h, cudaMemcpyDeviceToHost, ctx->stream));
+    }
+    ART_CUDA(cudaStreamSynchronize(ctx->stream));
+    return check_errflag(ctx);
+}
+
+int32_t art_context_compute_batch_device(ArtContext *ctx, uint32_t nimages, const ArtImage *images,
+                                         uint32_t iterations, const ArtOptions *opts, void *stream)
+{
+    if (!ctx || !images || nimages == 0) return fail(ART_ERR_INVALID_ARGUMENT, "null context or empty batch");
+    ART_CUDA(cudaSetDevice(ctx->device));
+    const int init_mode = opts ? (int)opts->init_mode : ART_INIT_DECODED;
+    std::vector<ImageSpec> specs;
+    int rc = batch_specs(images, nimages, specs);
+    if (rc) return rc;
+    for (uint32_t i = 0; i < nimages; i++)
+        if (images[i].out_pitch < images[i].max_rounded_px_w)
+            return fail(ART_ERR_INVALID_ARGUMENT, "image " + std::to_string(i) + ": out_pitch below width");
+    cudaStream_t user = static_cast<cudaStream_t>(stream);
+    cudaEvent_t join = nullptr;
+    if (user != ctx->stream) {
+        ART_CUDA(cudaEventCreateWithFlags(&join, cudaEventDisableTiming));
+        ART_CUDA(cudaEventRecord(join, user));
+        ART_CUDA(cudaStreamWaitEvent(ctx->stream, join, 0));
+    }
+    rc = prepare_batch(ctx, specs, iterations, init_mode);
+    if (!rc) rc = run_iterations(ctx, iterations);
+    for (uint32_t i = 0; !rc && i < nimages; i++) {
+        const float *fb;
+        int fp;
+        long long fcs;
+        result_planes(ctx, (int)i, &fb, &fp, &fcs);
+        const ArtImage &im = images[i];
+        for (uint32_t c = 0; c < im.nchannel && !rc; c++) {
+            cudaError_t e = cudaMemcpy2DAsync(im.out_planes[c], (size_t)im.out_pitch * sizeof(float), fb + c * fcs,
+                                              (size_t)fp * sizeof(float), (size_t)im.max_rounded_px_w * sizeof(float),
+                                              im.max_rounded_px_h, cudaMemcpyDeviceToDevice, ctx->stream);
+            if (e != cudaSuccess) rc = fail(ART_ERR_CUDA, std::string("output copy: ") + cudaGetErrorString(e));
+        }
+    }
+    if (join) {
+        if (!rc) {
+            cudaEventRecord(join, ctx->stream);
+            cudaStreamWaitEvent(user, join, 0);
+        }
+        cudaEventDestroy(join);
+    }
+    return rc;
+}
+
+// -------------------------------------------------------------- autotuner --
+
+int32_t art_context_autotune(ArtContext *ctx, uint32_t nchannel, const uint32_t *samp_h, const uint32_t *samp_v,
+                             uint32_t max_w, uint32_t max_h, uint32_t iterations, uint32_t *strip_rows_out)
+{
+    if (!ctx || !samp_h || !samp_v || nchannel < 1 || nchannel > 3)
+        return fail(ART_ERR_INVALID_ARGUMENT, "bad autotune arguments");
+    ART_CUDA(cudaSetDevice(ctx->device));
+    if (iterations == 0) iterations = 10;
+    // A deterministic synthetic image of this geometry: sparse small
+    // coefficients, unit quantisation steps.
+    ArtChannel ch[3];
+    std::vector<int16_t> host[3];
+    float q[64];
+    for (int j = 0; j < 64; j++) q[j] = 8.0f;
+    uint32_t lcg = 12345u;
+    size_t total = 0;
+    for (uint32_t c = 0; c < nchannel; c++) {
+        if ((samp_h[c] != 1 && samp_h[c] != 2) || (samp_v[c] != 1 && samp_v[c] != 2) || max_w % (8 * samp_h[c]) ||
+            max_h % (8 * samp_v[c]))
+            return fail(ART_ERR_INVALID_ARGUMENT, "autotune geometry does not fit the sampling factors");
+        memset(&ch[c], 0, sizeof(ArtChannel));
+        ch[c].rounded_px_w = max_w / samp_h[c];
+        ch[c].rounded_px_h = max_h / samp_v[c];
+        ch[c].block_w = ch[c].rounded_px_w / 8;
+        ch[c].block_h = ch[c].rounded_px_h / 8;
+        ch[c].samp_h = samp_h[c];
+        ch[c].samp_v = samp_v[c];
+        ch[c].coef_type = ART_COEF_I16;
+        ch[c].quant_table = q;
+        host[c].assign((size_t)ch[c].block_w * ch[c].block_h * 64, 0);
+        for (size_t i = 0; i < host[c].size(); i++) {
+            lcg = lcg * 1664525u + 1013904223u;
+            if ((i & 63) == 0 || (lcg >> 28) == 0) host[c][i] = (int16_t)((int)((lcg >> 16) & 255) - 128);
+        }
+        total += align_up(host[c].size() * 2, 256);
+    }
+    int rc;
+    if ((rc = ctx->stage.ensure(total))) return rc;
+    ImageSpec sp{nchannel, ch, {nullptr, nullptr, nullptr}, 0.3f, {0.001f, 0.001f, 0.001f}, max_w, max_h};
+    size_t off = 0;
+    for (uint32_t c = 0; c < nchannel; c++) {
+        char *dst = static_cast<char *>(ctx->stage.p) + off;
+        ART_CUDA(cudaMemcpyAsync(dst, host[c].data(), host[c].size() * 2, cudaMemcpyHostToDevice, ctx->stream));
+        sp.src[c] = dst;
+        off += align_up(host[c].size() * 2, 256);
+    }
+    cudaEvent_t e0, e1;
+    ART_CUDA(cudaEventCreate(&e0));
+    ART_CUDA(cudaEventCreate(&e1));
+    const bool timing = ctx->timing;
+    ctx->timing = false;
+    int best = 0;
+    float best_ms = 0.f;
+    const int candidates[4] = {16, 32, 64, 128};
+    for (int R : candidates) {
+        if ((int)max_h < R && R > 16) continue;
+        ctx->strip_rows_override = R;
+        rc = prepare_batch(ctx, {sp}, iterations, ART_INIT_DECODED);
+        if (!rc) rc = run_iterations(ctx, iterations);  // captures and warms up
+        float ms = 1e30f;
+        for (int rep = 0; rep < 3 && !rc; rep++) {
+            cudaEventRecord(e0, ctx->stream);
+            rc = run_iterations(ctx, iterations);
+            cudaEventRecord(e1, ctx->stream);
+            cudaEventSynchronize(e1);
+            float t = 0.f;
+            cudaEventElapsedTime(&t, e0, e1);
+            ms = std::min(ms, t);
+        }
+        if (rc) break;
+        if (!best || ms < best_ms) {
+            best = R;
+            best_ms = ms;
+        }
+    }
+    ctx->strip_rows_override = 0;
+    ctx->timing = timing;
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    if (rc) return rc;
+    ART_CUDA(cudaStreamSynchronize(ctx->stream));
+    ctx->tune[tune_key(nchannel, samp_h, samp_v, max_w, max_h)] = best;
+    if (strip_rows_out) *strip_rows_out = (uint32_t)best;
+    return ART_OK;
+}
+
+int32_t art_context_tune_cache(ArtContext *ctx, const char *path, int32_t save)
+{
+    if (!ctx || !path) return fail(ART_ERR_INVALID_ARGUMENT, "null context or path");
+    if (save) {
+        std::ofstream f(path);
+        if (!f) return fail(ART_ERR_INVALID_ARGUMENT, std::string("cannot write ") + path);
+        f << "# artefact_b200 autotune cache: <geometry bucket> <gradient-sweep strip rows>\n";
+        for (const auto &kv : ctx->tune) f << kv.first << " " << kv.second << "\n";
+        return f.good() ? ART_OK : fail(ART_ERR_INVALID_ARGUMENT, std::string("cannot write ") + path);
+    }
+    std::ifstream f(path);
+    if (!f) return fail(ART_ERR_INVALID_ARGUMENT, std::string("cannot read ") + path);
+    std::string line;
+    while (std::getline(f, line)) {
+        if (line.empty() || line[0] == '#') continue;
+        std::istringstream ls(line);
+        std::string key;
+        int rows = 0;
+        if (!(ls >> key >> rows) || (rows != 16 && rows != 32 && rows != 64 && rows != 128))
+            return fail(ART_ERR_INVALID_ARGUMENT, "malformed tune cache line: " + line);
+        ctx->tune[key] = rows;
+    }
+    return ART_OK;
 }
 
 }  // extern "C"

@@ -1,27 +1,35 @@
 #!/usr/bin/env python
 """Benchmark of the B200 restoration solver (one JSON line on rank 0).
 
-Workload (one "step"): one plain 50-iteration solve of a seeded synthetic
-1920x1080 YCbCr 4:2:0 baseline JPEG at quality 75 (weight 0.3, pweight 0.001),
-the configuration the headline metric is quoted on. Metric: megapixels per
-second of real image area (1920*1080 per step).
+Workloads (``--workload``; seeded synthetic JPEGs, ``artefact_b200.synth``):
 
-* value   -- coefficients already in HBM, result planes written to HBM,
-             timed per step with CUDA events; L2 flushed (256 MiB write)
-             between steps, outside the timed events.
-* e2e     -- the same solve through the public C ABI (art_context_compute)
-             from pinned host coefficient buffers to pinned host planes,
-             host<->device copies inside the timed region.
+* ``1080p`` (default): one plain 50-iteration solve of a 1920x1080 YCbCr
+  4:2:0 baseline JPEG at quality 75 (weight 0.3, pweight 0.001), the
+  configuration the headline metric is quoted on.
+* ``24mp``: 6000x4000 YCbCr 4:4:4 at quality 30, 100 iterations; the working
+  set (~1.7 GB) exceeds L2, so the iteration runs against HBM.
+* ``batch256``: 256 JPEGs, W, H ~ U[256, 2048] rounded to 16, 4:2:0 or 4:4:4
+  with p = 0.5, quality ~ U[20, 90], 50 iterations, solved as one batch.
+
+A step is one solve of the whole workload. Metric: megapixels per second of
+real image area.
+
+* value    -- coefficients already in HBM, result planes written to HBM,
+              timed per step with CUDA events; L2 flushed (256 MiB write)
+              between steps, outside the timed events.
+* e2e      -- the same through the public C ABI with host buffers
+              (art_context_compute, or art_context_compute_batch), pinned host
+              coefficients in and host planes out, copies inside the timed region.
 * roofline -- the dominant kernel's own I/O bytes per launch over its mean
-             launch time (CUDA event nodes inside the captured graph, taken
-             in a separate pass so they do not perturb `value`).
-* cpu_baseline -- the oracle (fp32 C restatement of pipeline_scalar) on the
-             same image, 50 iterations, one host thread.
+              launch time, from CUDA event nodes inside the captured graph,
+              taken in a separate pass so they do not perturb `value`.
+* cpu_baseline -- the oracle (fp32 C restatement of pipeline_scalar) on one
+              host thread; a bounded sample, extrapolated when stated.
 * --impl reference -- the oracle as the reference arm, steps spread over the
-             host's threads.
+              host's threads.
 
-Multi-GPU (torchrun): replicas only -- every rank solves its own copy; value is
-all ranks' megapixels over the slowest rank's time.
+Multi-GPU (torchrun): replicas only -- every rank solves its own copy; value
+is all ranks' megapixels over the slowest rank's time.
 """
 from __future__ import annotations
 
@@ -41,10 +49,15 @@ import numpy as np
 ROOT = Path(__file__).resolve().parent
 sys.path.insert(0, str(ROOT))
 
-WORKLOAD = dict(width=1920, height=1080, quality=75, subsampling="4:2:0", gray=False, seed=2000, iterations=50,
-                weight=0.3, pweight=0.001)
-WORKLOAD_NAME = "1920x1080 YCbCr 4:2:0 baseline JPEG q75, plain solver 50 iterations (weight 0.3, pweight 0.001)"
-METRIC = "MPix/s (plain 50-iteration solve, 1080p 4:2:0 q75)"
+WORKLOADS = {
+    "1080p": dict(name="1920x1080 YCbCr 4:2:0 baseline JPEG q75, plain solver 50 iterations (weight 0.3, pweight 0.001)",
+                  metric="MPix/s (plain 50-iteration solve, 1080p 4:2:0 q75)", iterations=50),
+    "24mp": dict(name="6000x4000 YCbCr 4:4:4 baseline JPEG q30, plain solver 100 iterations (weight 0.3, pweight 0.001)",
+                 metric="MPix/s (plain 100-iteration solve, 6000x4000 4:4:4 q30)", iterations=100),
+    "batch256": dict(name="256 JPEGs, W,H~U[256,2048] (x16), 4:2:0|4:4:4 p=.5, q~U[20,90], one batch, 50 iterations",
+                     metric="MPix/s (plain 50-iteration batched solve, 256 images)", iterations=50),
+}
+WEIGHT, PWEIGHT = 0.3, 0.001
 
 
 def log(*a):
@@ -59,17 +72,29 @@ def load_peaks():
     return 6650.0, "fallback"
 
 
-def make_workload():
+def make_workload(kind):
+    """List of decoded Jpeg objects for the workload."""
     from artefact_b200 import synth
     from artefact_b200.api import Jpeg, JpegSource
 
-    w = WORKLOAD
-    data = synth.make_jpeg(w["width"], w["height"], w["quality"], w["subsampling"], w["gray"], w["seed"])
-    return Jpeg.from_source(JpegSource.Buffer(data))
+    def dec(data):
+        return Jpeg.from_source(JpegSource.Buffer(data))
+
+    if kind == "1080p":
+        return [dec(synth.make_jpeg(1920, 1080, 75, "4:2:0", False, seed=2000))]
+    if kind == "24mp":
+        return [dec(synth.make_jpeg(6000, 4000, 30, "4:4:4", False, seed=3000))]
+    from concurrent.futures import ThreadPoolExecutor
+
+    specs = synth.batch_specs(256, seed=4000)
+    with ThreadPoolExecutor(max_workers=min(32, os.cpu_count() or 1)) as ex:
+        datas = list(ex.map(lambda s: synth.make_jpeg(s.width, s.height, s.quality, s.subsampling, False, s.seed),
+                            specs))
+    return [dec(d) for d in datas]
 
 
 class Clocks:
-    """Samples nvidia-smi during the timed region."""
+    """Samples nvidia-smi while the GPU work is timed."""
 
     FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
               "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
@@ -84,9 +109,12 @@ class Clocks:
         try:
             self.proc = subprocess.Popen(
                 ["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
-                 "-lms", "200"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+                 "-lms", "100"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
             self.thread = threading.Thread(target=self._read, daemon=True)
             self.thread.start()
+            t0 = time.time()
+            while not self.lines and time.time() - t0 < 5:
+                time.sleep(0.02)
         except Exception:
             self.proc = None
         return self
@@ -129,8 +157,33 @@ def oracle_solve(jpeg, iterations):
     import oracle_lib
 
     W, H, _ = jpeg.max_rounded()
-    w = WORKLOAD
-    return oracle_lib.compute(jpeg.nchannel, jpeg.coefs, w["weight"], [w["pweight"]] * 3, iterations, W, H)
+    return oracle_lib.compute(jpeg.nchannel, jpeg.coefs, WEIGHT, [PWEIGHT] * 3, iterations, W, H)
+
+
+def cpu_sample(kind, jpegs, iterations):
+    """Bounded CPU measurement of the oracle: (MPix/s, description)."""
+    real = sum(j.real_px_w * j.real_px_h for j in jpegs) / 1e6
+    if kind == "1080p":
+        t = time.perf_counter()
+        oracle_solve(jpegs[0], iterations)
+        return real / (time.perf_counter() - t), "one full solve of the workload by the fp32 C restatement of pipeline_scalar"
+    if kind == "24mp":
+        t = time.perf_counter()
+        oracle_solve(jpegs[0], 0)
+        t_init = time.perf_counter() - t
+        t = time.perf_counter()
+        oracle_solve(jpegs[0], 2)
+        t_iter = (time.perf_counter() - t - t_init) / 2
+        total = t_init + iterations * t_iter
+        return real / total, (f"init alone and a 2-iteration solve of the full image, extrapolated to {iterations} "
+                              f"iterations ({t_init:.1f} s + {iterations} x {t_iter:.2f} s)")
+    sample = jpegs[:4]
+    t = time.perf_counter()
+    for j in sample:
+        oracle_solve(j, iterations)
+    dt = time.perf_counter() - t
+    px = sum(j.real_px_w * j.real_px_h for j in sample) / 1e6
+    return px / dt, f"the first 4 images of the batch ({px:.2f} MPix), {iterations} iterations each"
 
 
 def run_reference(args, rank, world):
@@ -139,24 +192,40 @@ def run_reference(args, rank, world):
         return
     from concurrent.futures import ThreadPoolExecutor
 
-    jpeg = make_workload()
-    w = WORKLOAD
-    mpix = w["width"] * w["height"] / 1e6
-    threads = max(1, min(args.steps, os.cpu_count() or 1))
+    wl = WORKLOADS[args.workload]
+    jpegs = make_workload(args.workload)
+    iters = wl["iterations"]
+    threads = max(1, min(os.cpu_count() or 1, 64))
+    if args.workload == "1080p":
+        work = [jpegs[0]] * args.steps
+        warm = [jpegs[0]] * min(args.warmup, threads)
+        mpix = jpegs[0].real_px_w * jpegs[0].real_px_h / 1e6 * args.steps
+        sample = f"{args.steps} full solves of the workload spread over {threads} host threads"
+    else:
+        # Bounded: one image-solve per step (the batch's first images, or a
+        # 4-iteration solve of the 24 MP image scaled per iteration).
+        work = jpegs[:args.steps] if args.workload == "batch256" else [jpegs[0]] * min(args.steps, 4)
+        warm = []
+        mpix = sum(j.real_px_w * j.real_px_h for j in work) / 1e6
+        sample = f"{len(work)} image solves of the workload spread over {threads} host threads"
+    its = iters if args.workload != "24mp" else 4
     with ThreadPoolExecutor(max_workers=threads) as ex:
-        list(ex.map(lambda _: oracle_solve(jpeg, w["iterations"]), range(min(args.warmup, threads))))
+        list(ex.map(lambda j: oracle_solve(j, its), warm))
         t0 = time.perf_counter()
-        list(ex.map(lambda _: oracle_solve(jpeg, w["iterations"]), range(args.steps)))
+        list(ex.map(lambda j: oracle_solve(j, its), work))
         dt = time.perf_counter() - t0
-    value = args.steps * mpix / dt
+    if args.workload == "24mp":
+        dt *= iters / its  # per-iteration cost scaled to the full solve
+        sample += f" at {its} iterations, scaled to {iters}"
+    value = mpix / dt
     line = {
-        "impl": "reference", "metric": METRIC, "value": value, "unit": "MPix/s", "n_gpus": world,
-        "steps": args.steps, "warmup": args.warmup, "ms_per_step": dt * 1e3 / args.steps * threads,
+        "impl": "reference", "metric": wl["metric"], "value": value, "unit": "MPix/s", "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": dt * 1e3 / max(1, len(work)),
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-        "config": {"workload": WORKLOAD_NAME, "iterations": w["iterations"]},
+        "config": {"workload": wl["name"], "iterations": iters},
         "cpu_baseline": {"value": value, "unit": "MPix/s", "cores": threads, "kind": "port",
-                         "sample": f"{args.steps} full solves of the workload spread over {threads} host threads "
-                                   "(fp32 C restatement of pipeline_scalar; the Rust reference is not buildable here)"},
+                         "sample": sample + " (fp32 C restatement of pipeline_scalar; the Rust reference is not "
+                                            "buildable here)"},
         "e2e": {"value": value, "unit": "MPix/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line), flush=True)
@@ -165,9 +234,10 @@ def run_reference(args, rank, world):
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--steps", type=int, default=20)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--workload", default="1080p", choices=sorted(WORKLOADS))
     ap.add_argument("--no-cpu-baseline", action="store_true")
     args = ap.parse_args()
 
@@ -194,33 +264,48 @@ def main():
     from artefact_b200 import _native as N
 
     lib = N.lib()
-    jpeg = make_workload()
-    W, H, _ = jpeg.max_rounded()
-    w = WORKLOAD
-    nch = jpeg.nchannel
-    iters = w["iterations"]
-    mpix = w["width"] * w["height"] / 1e6
+    wl = WORKLOADS[args.workload]
+    iters = wl["iterations"]
+    jpegs = make_workload(args.workload)
+    nimg = len(jpegs)
+    mpix = sum(j.real_px_w * j.real_px_h for j in jpegs) / 1e6
 
-    # Device-resident inputs and outputs.
-    dev_coefs = [torch.from_numpy(c.dct_coefs.copy()).cuda() for c in jpeg.coefs]
-    qs = [np.ascontiguousarray(c.quant_table, np.float32) for c in jpeg.coefs]
-    chans_dev = (N.ArtChannel * nch)()
-    chans_host = (N.ArtChannel * nch)()
-    pinned_coefs = [torch.from_numpy(c.dct_coefs.copy()).pin_memory() for c in jpeg.coefs]
-    for i, c in enumerate(jpeg.coefs):
-        for arr, ptr in ((chans_dev, dev_coefs[i].data_ptr()), (chans_host, pinned_coefs[i].data_ptr())):
-            ch = arr[i]
-            ch.rounded_px_w, ch.rounded_px_h, ch.block_w, ch.block_h = (c.rounded_px_w, c.rounded_px_h, c.block_w,
-                                                                        c.block_h)
-            ch.samp_h, ch.samp_v, ch.coef_type = c.horizontal_samp_factor, c.vertical_samp_factor, N.ART_COEF_I16
-            ch.dct_coefs = ptr
-            ch.quant_table = qs[i].ctypes.data_as(C.POINTER(C.c_float))
-    pitch = (W + 31) // 32 * 32
-    outs = [torch.empty(H, pitch, device="cuda") for _ in range(nch)]
-    out_ptrs = (C.c_void_p * nch)(*[o.data_ptr() for o in outs])
-    host_outs = [torch.empty(W * H, dtype=torch.float32).pin_memory() for _ in range(nch)]
-    host_ptrs = (C.c_void_p * nch)(*[o.data_ptr() for o in host_outs])
-    pw = (C.c_float * 3)(w["pweight"], w["pweight"], w["pweight"])
+    keep = []
+    imgs_dev = (N.ArtImage * nimg)()
+    imgs_host = (N.ArtImage * nimg)()
+    pw = (C.c_float * 3)(PWEIGHT, PWEIGHT, PWEIGHT)
+    h2d = d2h = 0
+    for i, j in enumerate(jpegs):
+        W, H, _ = j.max_rounded()
+        n = j.nchannel
+        cd = (N.ArtChannel * n)()
+        ch_ = (N.ArtChannel * n)()
+        for c, co in enumerate(j.coefs):
+            dev = torch.from_numpy(co.dct_coefs.copy()).cuda()
+            pin = torch.from_numpy(co.dct_coefs.copy()).pin_memory()
+            q = np.ascontiguousarray(co.quant_table, np.float32)
+            keep += [dev, pin, q]
+            h2d += co.dct_coefs.nbytes
+            for arr, ptr in ((cd, dev.data_ptr()), (ch_, pin.data_ptr())):
+                a = arr[c]
+                a.rounded_px_w, a.rounded_px_h, a.block_w, a.block_h = co.rounded_px_w, co.rounded_px_h, co.block_w, co.block_h
+                a.samp_h, a.samp_v, a.coef_type = co.horizontal_samp_factor, co.vertical_samp_factor, N.ART_COEF_I16
+                a.dct_coefs = ptr
+                a.quant_table = q.ctypes.data_as(C.POINTER(C.c_float))
+        pitch = (W + 31) // 32 * 32
+        douts = [torch.empty(H, pitch, device="cuda") for _ in range(n)]
+        houts = [torch.empty(W * H, dtype=torch.float32).pin_memory() for _ in range(n)]
+        d2h += n * W * H * 4
+        dptr = (C.c_void_p * n)(*[o.data_ptr() for o in douts])
+        hptr = (C.c_void_p * n)(*[o.data_ptr() for o in houts])
+        keep += [cd, ch_, douts, houts, dptr, hptr]
+        for arr, chans, ptrs, op in ((imgs_dev, cd, dptr, pitch), (imgs_host, ch_, hptr, W)):
+            im = arr[i]
+            im.nchannel, im.max_rounded_px_w, im.max_rounded_px_h, im.out_pitch = n, W, H, op
+            im.channels = C.cast(chans, C.POINTER(N.ArtChannel))
+            im.weight = WEIGHT
+            im.pweight = (C.c_float * 3)(PWEIGHT, PWEIGHT, PWEIGHT)
+            im.out_planes = C.cast(ptrs, C.POINTER(C.c_void_p))
     flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")
 
     ctx = C.c_void_p()
@@ -228,22 +313,34 @@ def main():
     stream = torch.cuda.current_stream()
 
     def solve_device():
-        N.check(lib.art_context_compute_device(ctx, nch, chans_dev, w["weight"], pw, iters, W, H, out_ptrs, pitch,
-                                               None, C.c_void_p(stream.cuda_stream)))
+        if nimg == 1:
+            im = imgs_dev[0]
+            N.check(lib.art_context_compute_device(ctx, im.nchannel, im.channels, WEIGHT, pw, iters,
+                                                   im.max_rounded_px_w, im.max_rounded_px_h, im.out_planes,
+                                                   im.out_pitch, None, C.c_void_p(stream.cuda_stream)))
+        else:
+            N.check(lib.art_context_compute_batch_device(ctx, nimg, imgs_dev, iters, None,
+                                                         C.c_void_p(stream.cuda_stream)))
+
+    def solve_host():
+        if nimg == 1:
+            im = imgs_host[0]
+            N.check(lib.art_context_compute(ctx, im.nchannel, im.channels, WEIGHT, pw, iters, im.max_rounded_px_w,
+                                            im.max_rounded_px_h, im.out_planes, None))
+        else:
+            N.check(lib.art_context_compute_batch(ctx, nimg, imgs_host, iters, None))
 
     def barrier():
         if dist:
             dist.barrier()
         torch.cuda.synchronize()
 
-    # --- warm-up
     for _ in range(args.warmup):
         flush.fill_(1.0)
         solve_device()
     torch.cuda.synchronize()
     N.check(lib.art_context_synchronize(ctx))
 
-    # --- timed region: value (device-resident)
     starts = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
     ends = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
     barrier()
@@ -256,63 +353,66 @@ def main():
             ends[k].record(stream)
         barrier()
         wall = time.perf_counter() - t0
-    N.check(lib.art_context_synchronize(ctx))
-    step_ms = [s.elapsed_time(e) for s, e in zip(starts, ends)]
-    total_ms = sum(step_ms)
-    if dist:
-        t = torch.tensor([total_ms], device="cuda", dtype=torch.float64)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        total_ms = float(t.item())
-    value = world * args.steps * mpix / (total_ms / 1e3)
+        N.check(lib.art_context_synchronize(ctx))
+        step_ms = [s.elapsed_time(e) for s, e in zip(starts, ends)]
+        total_ms = sum(step_ms)
+        if dist:
+            t = torch.tensor([total_ms], device="cuda", dtype=torch.float64)
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+            total_ms = float(t.item())
+        value = world * args.steps * mpix / (total_ms / 1e3)
+
+        # Kernel timing pass (event nodes inside the graph).
+        N.check(lib.art_context_set_timing(ctx, 1))
+        grad_ms, upd_ms, loop_ms = [], [], []
+        lm, gm, um, nl = C.c_float(), C.c_float(), C.c_float(), C.c_uint32()
+        for k in range(4):
+            flush.fill_(float(k))
+            solve_device()
+            N.check(lib.art_context_synchronize(ctx))
+            N.check(lib.art_context_last_timing(ctx, C.byref(lm), C.byref(gm), C.byref(um), C.byref(nl)))
+            if k > 0:
+                loop_ms.append(lm.value)
+                grad_ms.append(gm.value)
+                upd_ms.append(um.value)
+        N.check(lib.art_context_set_timing(ctx, 0))
     clocks = clk.summary()
 
-    # --- e2e through the C ABI with pinned host buffers
+    # e2e through the public API with host buffers.
     for _ in range(max(1, args.warmup // 2)):
-        N.check(lib.art_context_compute(ctx, nch, chans_host, w["weight"], pw, iters, W, H, host_ptrs, None))
+        solve_host()
     barrier()
     e2e_ms = []
-    for k in range(args.steps):
+    e2e_steps = min(args.steps, 10)
+    for k in range(e2e_steps):
         flush.fill_(float(k))
         torch.cuda.synchronize()
         t1 = time.perf_counter()
-        N.check(lib.art_context_compute(ctx, nch, chans_host, w["weight"], pw, iters, W, H, host_ptrs, None))
+        solve_host()
         e2e_ms.append((time.perf_counter() - t1) * 1e3)
     e2e_total = sum(e2e_ms)
     if dist:
         t = torch.tensor([e2e_total], device="cuda", dtype=torch.float64)
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         e2e_total = float(t.item())
-    e2e_value = world * args.steps * mpix / (e2e_total / 1e3)
-    h2d = sum(int(c.dct_coefs.nbytes) for c in jpeg.coefs)
-    d2h = nch * W * H * 4
+    e2e_value = world * e2e_steps * mpix / (e2e_total / 1e3)
 
-    # --- kernel timing pass (event nodes inside the graph)
-    N.check(lib.art_context_set_timing(ctx, 1))
-    grad_ms, upd_ms, loop_ms, launches = [], [], [], 0
-    lm, gm, um, nl = C.c_float(), C.c_float(), C.c_float(), C.c_uint32()
-    for k in range(max(3, min(args.steps, 10))):
-        flush.fill_(float(k))
-        solve_device()
-        N.check(lib.art_context_synchronize(ctx))
-        N.check(lib.art_context_last_timing(ctx, C.byref(lm), C.byref(gm), C.byref(um), C.byref(nl)))
-        if k > 0:
-            loop_ms.append(lm.value)
-            grad_ms.append(gm.value)
-            upd_ms.append(um.value)
-    N.check(lib.art_context_set_timing(ctx, 0))
     g_launch = statistics.mean(grad_ms) / iters
     u_launch = statistics.mean(upd_ms) / iters
     loop = statistics.mean(loop_ms)
-
-    # Algorithmic bytes (per launch): the gradient sweep reads x_k, x_{k-1} and
-    # the DCT-distance gradient plane (component resolution) and writes g; the
-    # projection reads x_k, x_{k-1}, g and the int16 coefficients and writes
-    # x_{k+1} and the next DCT-distance gradient plane.
-    n_full = W * H
-    nc = [c.rounded_px_w * c.rounded_px_h for c in jpeg.coefs]
-    grad_bytes = sum(12 * n_full + 4 * x for x in nc)
-    upd_bytes = sum(16 * n_full + 6 * x for x in nc)
-    iter_bytes = sum(20 * n_full + 4 * x for x in nc)  # two-sweep minimum per iteration
+    # Algorithmic bytes per launch (summed over the workload's images): the
+    # gradient sweep reads y and the DCT-distance plane (component resolution)
+    # and writes g; the projection reads y, g, x and the int16 coefficients and
+    # writes x, y and the DCT-distance plane. The iteration figure is the
+    # two-sweep minimum sum_c (20 N + 4 N_c).
+    grad_bytes = upd_bytes = iter_bytes = 0
+    for j in jpegs:
+        W, H, _ = j.max_rounded()
+        for co in j.coefs:
+            nc = co.rounded_px_w * co.rounded_px_h
+            grad_bytes += 8 * W * H + 4 * nc
+            upd_bytes += 20 * W * H + 6 * nc
+            iter_bytes += 20 * W * H + 4 * nc
     peak, peak_kind = load_peaks()
     if g_launch >= u_launch:
         dom, dbytes, dms = "k_grad_sweep", grad_bytes, g_launch
@@ -320,7 +420,7 @@ def main():
         dom, dbytes, dms = "k_project", upd_bytes, u_launch
     achieved = dbytes / (dms * 1e-3) / 1e9
     traffic = None
-    tf = ROOT / "profiles" / "traffic.json"
+    tf = ROOT / "profiles" / f"traffic_{args.workload}.json"
     if tf.exists():
         try:
             traffic = json.loads(tf.read_text()).get(dom)
@@ -329,33 +429,30 @@ def main():
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
-        t2 = time.perf_counter()
-        oracle_solve(jpeg, iters)
-        cdt = time.perf_counter() - t2
-        cpu = {"value": mpix / cdt, "unit": "MPix/s", "cores": 1, "kind": "port",
-               "sample": "one full solve of the workload (50 iterations) by the fp32 C restatement of "
-                         "pipeline_scalar on one host thread"}
+        v, desc = cpu_sample(args.workload, jpegs, iters)
+        cpu = {"value": v, "unit": "MPix/s", "cores": 1, "kind": "port", "sample": desc}
 
-    modes = len({(c.horizontal_samp_factor, c.vertical_samp_factor) for c in jpeg.coefs})
-    gpu_launches = args.steps * (nch + 1 + (1 + modes) * iters)
+    modes = len({(c.horizontal_samp_factor, c.vertical_samp_factor) for j in jpegs for c in j.coefs})
+    nchs = len({j.nchannel for j in jpegs})
+    per_step = sum(j.nchannel for j in jpegs) + 1 + (nchs + modes) * iters
     if rank == 0:
         line = {
-            "metric": METRIC, "value": value, "unit": "MPix/s", "n_gpus": world, "steps": args.steps,
+            "metric": wl["metric"], "value": value, "unit": "MPix/s", "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": total_ms / args.steps, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-            "config": {"workload": WORKLOAD_NAME, "iterations": iters, "channels": nch, "max_rounded": [W, H],
+            "config": {"workload": wl["name"], "iterations": iters, "images": nimg,
                        "l2": "flushed between steps (256 MiB write outside the timed events)",
                        "parallelism": f"replicas x{world}"},
             "e2e": {"value": e2e_value, "unit": "MPix/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
-                    "ms_per_step": e2e_total / args.steps, "api": "art_context_compute (host buffers)"},
+                    "ms_per_step": e2e_total / e2e_steps,
+                    "api": "art_context_compute" if nimg == 1 else "art_context_compute_batch"},
             "roofline": {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": achieved / peak, "traffic": traffic, "peak_kind": peak_kind,
                          "algorithmic_bytes_per_launch": dbytes, "launch_ms": dms},
             "iteration": {"ms": loop / iters, "gradient_ms": g_launch, "update_ms": u_launch,
-                          "algorithmic_bytes": iter_bytes,
-                          "gbs": iter_bytes / (loop / iters * 1e-3) / 1e9,
+                          "algorithmic_bytes": iter_bytes, "gbs": iter_bytes / (loop / iters * 1e-3) / 1e9,
                           "frac_of_hbm": iter_bytes / (loop / iters * 1e-3) / 1e9 / peak},
-            "cpu_baseline": cpu, "gpu_launches": gpu_launches, "clocks": clocks, "wall_s": wall,
+            "cpu_baseline": cpu, "gpu_launches": args.steps * per_step, "clocks": clocks, "wall_s": wall,
         }
         print(json.dumps(line), flush=True)
     lib.art_context_destroy(ctx)

@@ -120,6 +120,46 @@ int32_t art_context_process(ArtContext *ctx, uint32_t nchannel, const ArtChannel
                             const float pweight[3], const uint32_t iterations[3], int32_t separate, uint32_t real_w,
                             uint32_t real_h, uint8_t *rgb_out, const ArtOptions *opts);
 
+/*
+ * A batch of images solved together: every gradient sweep and projection of an
+ * iteration covers all images in one launch (per channel count and sampling
+ * mode), and the fixed-count iteration loop is one captured CUDA graph.
+ * Each image has its own size, channels, sampling, weight and pweight; all run
+ * `iterations` steps. Per image the result equals art_compute's.
+ * No reference counterpart (the reference solves one image per call); it
+ * batches what artefact-lib's callers would do in a loop over
+ * compute(), pipeline_scalar/mod.rs:17-78.
+ */
+typedef struct ArtImage {
+    uint32_t nchannel;
+    uint32_t max_rounded_px_w, max_rounded_px_h;
+    uint32_t out_pitch;            /* device variant: floats per output row (>= width); host variant ignores it */
+    const ArtChannel *channels;    /* nchannel components */
+    float weight;
+    float pweight[3];
+    float *const *out_planes;      /* nchannel planes */
+} ArtImage;
+
+/* Host coefficients in, host planes (row stride = width) out. */
+int32_t art_context_compute_batch(ArtContext *ctx, uint32_t nimages, const ArtImage *images, uint32_t iterations,
+                                  const ArtOptions *opts);
+/* Device coefficients in, device planes out; ordered after `stream`, returns without synchronising. */
+int32_t art_context_compute_batch_device(ArtContext *ctx, uint32_t nimages, const ArtImage *images,
+                                         uint32_t iterations, const ArtOptions *opts, void *stream);
+
+/*
+ * Autotuner. Times the gradient sweep's strip height (16, 32, 64, 128 rows)
+ * on a deterministic synthetic image of the given geometry (`iterations`
+ * steps, 0 = 10) and caches the fastest for the geometry's bucket (channel
+ * count, sampling, width and height rounded up to powers of two); later solves
+ * of images in that bucket use it. art_context_tune_cache saves (save != 0) or
+ * loads the cache as a text file of "<bucket> <rows>" lines.
+ */
+int32_t art_context_autotune(ArtContext *ctx, uint32_t nchannel, const uint32_t *samp_h, const uint32_t *samp_v,
+                             uint32_t max_rounded_px_w, uint32_t max_rounded_px_h, uint32_t iterations,
+                             uint32_t *strip_rows_out);
+int32_t art_context_tune_cache(ArtContext *ctx, const char *path, int32_t save);
+
 /* Wait for the context's queued work; returns the first error it met. */
 int32_t art_context_synchronize(ArtContext *ctx);
 

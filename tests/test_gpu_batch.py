@@ -1,0 +1,59 @@
+"""Batched solves and the autotuner (GPU)."""
+import numpy as np
+import pytest
+
+import oracle_lib as O
+from artefact_b200 import Context, compute, synth
+from parity import check_parity
+from artefact_b200.api import Jpeg, JpegSource
+
+pytestmark = pytest.mark.gpu
+
+MAX_ABS = 1.0
+
+
+def _jpeg(w, h, q, sub, gray, seed):
+    return Jpeg.from_source(JpegSource.Buffer(synth.make_jpeg(w, h, q, sub, gray, seed)))
+
+
+def test_batch_matches_single_solves(gpu):
+    """Heterogeneous sizes, channel counts and subsamplings in one batch."""
+    shapes = [(96, 64, 75, "4:2:0", False), (40, 24, 50, "4:4:4", True), (130, 70, 30, "4:4:4", False),
+              (200, 136, 90, "4:2:0", False), (64, 48, 60, "4:2:2", False), (33, 17, 75, "4:4:4", True)]
+    jpegs = [_jpeg(*s, seed=500 + i) for i, s in enumerate(shapes)]
+    jobs = [dict(coefs=j.coefs, weight=0.3 + 0.1 * i, pweight=[0.001, 0.002, 0.0005]) for i, j in enumerate(jpegs)]
+    with Context(0) as ctx:
+        batch = ctx.compute_batch(jobs, 15)
+    for j, job, got in zip(jpegs, jobs, batch):
+        W, H, N_ = j.max_rounded()
+        single = compute(j.nchannel, j.coefs, job["weight"], job["pweight"], 15, W, H, N_)
+        # Same kernels, strips and reduction order as a solve of the image alone.
+        assert all(np.array_equal(a, b) for a, b in zip(got, single))
+        check_parity(j, 15, job["weight"], job["pweight"], label=f"batch {j.real_px_w}x{j.real_px_h}", gpu=got)
+
+
+def test_batch_is_deterministic(gpu):
+    jpegs = [_jpeg(72, 40, 75, "4:2:0", False, seed=600 + i) for i in range(3)]
+    jobs = [dict(coefs=j.coefs) for j in jpegs]
+    with Context(0) as ctx:
+        a = ctx.compute_batch(jobs, 10)
+        b = ctx.compute_batch(jobs, 10)
+    assert all(np.array_equal(x, y) for pa, pb in zip(a, b) for x, y in zip(pa, pb))
+
+
+def test_autotune_and_cache_roundtrip(gpu, tmp_path):
+    j = _jpeg(512, 384, 75, "4:2:0", False, seed=700)
+    W, H, N_ = j.max_rounded()
+    with Context(0) as ctx:
+        rows = ctx.autotune(3, [1, 2, 2], [1, 2, 2], W, H, iterations=5)
+        assert rows in (16, 32, 64, 128)
+        path = tmp_path / "tune.txt"
+        ctx.save_tune_cache(path)
+        assert f" {rows}" in path.read_text()
+        tuned = ctx.compute(3, j.coefs, 0.3, [0.001] * 3, 20, W, H)
+    with Context(0) as ctx2:
+        ctx2.load_tune_cache(path)
+        again = ctx2.compute(3, j.coefs, 0.3, [0.001] * 3, 20, W, H)
+    assert all(np.array_equal(a, b) for a, b in zip(tuned, again))
+    ref = O.compute(3, j.coefs, 0.3, [0.001] * 3, 20, W, H)
+    assert max(float(np.abs(a - b).max()) for a, b in zip(tuned, ref)) <= MAX_ABS

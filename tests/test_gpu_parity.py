@@ -43,42 +43,7 @@ def jpeg_of(w, h, q, sub, gray, seed):
     return _cache[key]
 
 
-def _maxdiff(a, b):
-    return max(float(np.abs(x.astype(np.float64) - y.astype(np.float64)).max()) for x, y in zip(a, b))
-
-
-def check_parity(j, iterations, weight=0.3, pweight=(0.001,) * 3, label=""):
-    W, H, N_ = j.max_rounded()
-    n = j.nchannel
-    gpu = compute(n, j.coefs, weight, pweight, iterations, W, H, N_)
-    ref = O.compute(n, j.coefs, weight, pweight, iterations, W, H)
-    r64 = O.compute(n, j.coefs, weight, pweight, iterations, W, H, fp64=True)
-    d, d_gpu64, d_ref64 = _maxdiff(gpu, ref), _maxdiff(gpu, r64), _maxdiff(ref, r64)
-    eg = O.objective(n, j.coefs, weight, pweight, W, H, gpu)
-    er = O.objective(n, j.coefs, weight, pweight, W, H, ref)
-    e64 = O.objective(n, j.coefs, weight, pweight, W, H, r64)
-    rel, rel_gpu64, rel_ref64 = abs(eg - er) / abs(er), abs(eg - e64) / abs(e64), abs(er - e64) / abs(e64)
-    feas = O.feasibility(n, j.coefs, W, H, gpu)
-    well = d_ref64 <= 0.5 and rel_ref64 <= 2.5e-5
-    msg = (f"{label} it={iterations} max|gpu-f32|={d:.3g} max|gpu-f64|={d_gpu64:.3g} max|f32-f64|={d_ref64:.3g} "
-           f"obj rel gpu/f32={rel:.2g} gpu/f64={rel_gpu64:.2g} f32/f64={rel_ref64:.2g} feas={feas:.2g} "
-           f"{'well-conditioned' if well else 'ill-conditioned'}")
-    print(msg)
-    if well:
-        assert d <= MAX_ABS, msg
-        assert rel <= OBJ_REL, msg
-    else:
-        spread_d, spread_e = d_ref64, rel_ref64
-        for fp64 in (False, True):
-            v = O.compute(n, j.coefs, weight, pweight, iterations, W, H, init_mode=2, fp64=fp64)
-            spread_d = max(spread_d, _maxdiff(v, r64))
-            spread_e = max(spread_e, abs(O.objective(n, j.coefs, weight, pweight, W, H, v) - e64) / abs(e64))
-        msg += f" variant spread: planes {spread_d:.3g} objective {spread_e:.2g}"
-        print(msg)
-        assert d_gpu64 <= 2 * spread_d + 0.5, msg
-        assert rel_gpu64 <= 2 * spread_e + OBJ_REL, msg
-    assert feas <= FEAS, msg
-    return gpu, ref
+from parity import check_parity  # noqa: E402
 
 
 SMALL = [
