@@ -94,7 +94,8 @@ EXPORTS = {
     "art_context_compute_batch_device": (C.c_int32, [C.c_void_p, C.c_uint32, C.POINTER(ArtImage), C.c_uint32,
                                                      C.POINTER(ArtOptions), C.c_void_p]),
     "art_context_autotune": (C.c_int32, [C.c_void_p, C.c_uint32, C.POINTER(C.c_uint32), C.POINTER(C.c_uint32),
-                                         C.c_uint32, C.c_uint32, C.c_uint32, C.POINTER(C.c_uint32)]),
+                                         C.c_uint32, C.c_uint32, C.c_uint32, C.POINTER(C.c_uint32),
+                                         C.POINTER(C.c_uint32)]),
     "art_context_tune_cache": (C.c_int32, [C.c_void_p, C.c_char_p, C.c_int32]),
     "art_context_synchronize": (C.c_int32, [C.c_void_p]),
     "art_context_set_timing": (C.c_int32, [C.c_void_p, C.c_int32]),

@@ -358,13 +358,15 @@ class Context:
         return results
 
     def autotune(self, nchannel: int, samp_h: Sequence[int], samp_v: Sequence[int], max_w: int, max_h: int,
-                 iterations: int = 10) -> int:
-        """Time the sweep strip heights for this geometry; returns (and caches) the fastest."""
+                 iterations: int = 10) -> tuple:
+        """Time the sweep variants and strip heights for this geometry; returns (and
+        caches) the fastest as (variant, strip_rows), variant 0 narrow or 1 wide."""
         sh = (C.c_uint32 * 3)(*(list(samp_h) + [1, 1, 1])[:3])
         sv = (C.c_uint32 * 3)(*(list(samp_v) + [1, 1, 1])[:3])
-        out = C.c_uint32()
-        N.check(N.lib().art_context_autotune(self._h, nchannel, sh, sv, max_w, max_h, iterations, C.byref(out)))
-        return out.value
+        kind, rows = C.c_uint32(), C.c_uint32()
+        N.check(N.lib().art_context_autotune(self._h, nchannel, sh, sv, max_w, max_h, iterations, C.byref(kind),
+                                             C.byref(rows)))
+        return kind.value, rows.value
 
     def save_tune_cache(self, path: str) -> None:
         N.check(N.lib().art_context_tune_cache(self._h, str(path).encode(), 1))

@@ -38,12 +38,13 @@ namespace art {
 // Gradient of the objective at the FISTA point y_k (compute_step.rs:8-48) and
 // the per-channel sums of squares reduced to sigma_c = step / ||g_c||
 // (compute_step.rs:52-58). One warp per strip of SWEEP_OUT output columns and
-// strip_rows rows; lane L holds column xs - 2 + L. Lanes 1..30 form the
-// per-pixel terms, lanes 2..29 write g. Rows and columns outside the image are
-// read clamped (replicated edges make the reference's last-row/column forward
-// differences vanish, compute_step_tv.rs:105-120) and their terms are zero,
-// which reproduces the reference's scatter guards. Rows are prefetched two
-// ahead of use.
+// strip_rows rows; lane L holds the column pair xs - 2 + 2L, xs - 1 + 2L as a
+// float2 and the arithmetic runs on packed FP32x2 instructions. Lanes 0..31
+// form the per-pixel terms, lanes 1..30 write g. Rows and columns outside the
+// image are read clamped (replicated edges make the reference's last-row and
+// last-column forward differences vanish, compute_step_tv.rs:105-120) and
+// their terms are zero, which reproduces the reference's scatter guards. Rows
+// are prefetched two ahead of use.
 template <int NCH>
 __global__ void __launch_bounds__(SWEEP_WARPS * 32) k_grad_sweep(const ImgDev *__restrict__ imgs,
                                                                  const int2 *__restrict__ work)
@@ -56,15 +57,238 @@ __global__ void __launch_bounds__(SWEEP_WARPS * 32) k_grad_sweep(const ImgDev *_
     const int2 wk = work[blockIdx.x];
     const ImgDev &im = imgs[wk.x];
     const int W = im.W, H = im.H, pitch = im.pitch, R = im.strip_rows;
-    const long long cs = im.cstride;
     const int strip = wk.y * SWEEP_WARPS + warp;
+    float2 ssq[NCH];
+#pragma unroll
+    for (int c = 0; c < NCH; c++) ssq[c] = make_float2(0.f, 0.f);
+
+    if (strip < im.nstrips) {
+        const int sxi = strip % im.strips_x, syi = strip / im.strips_x;
+        const int xs = sxi * SWEEP_OUT, ys = syi * R;
+        const int ca = xs - 2 + 2 * lane, cb = ca + 1;  // this lane's columns (ca even)
+        const bool ina = ca >= 0 && ca < W, inb = cb >= 0 && cb < W;
+        const bool pair = ca >= 0 && cb < W;            // both columns inside: one 8-byte load
+        const int la = min(max(ca, 0), W - 1), lb = min(max(cb, 0), W - 1);
+        const bool outlane = lane >= 1 && lane <= 30 && ca < W;
+        const bool lft = ca > 0;                        // column a has a left neighbour in the image
+        const int cs = (int)im.cstride;
+        const float *ybase = im.y;
+        float *gout = im.g + (outlane ? ca : 0);
+        const float2 at = make_float2(im.alpha_tv, im.alpha_tv), ag = make_float2(im.alpha_tgv, im.alpha_tgv);
+        const float2 half2 = make_float2(0.5f, 0.5f), two2 = make_float2(2.f, 2.f);
+        // DCT-distance gradient plane of each channel at this lane's columns
+        // (offsets from the first channel's plane), prefetched one row ahead.
+        const float *pbase = im.ch[0].P;
+        int pcol[NCH], psh[NCH], ppitch[NCH];
+        bool pon[NCH], pshare[NCH];
+#pragma unroll
+        for (int c = 0; c < NCH; c++) {
+            const ChanDev &cd = im.ch[c];
+            pon[c] = cd.alpha_p != 0.f;
+            psh[c] = cd.sv - 1;
+            ppitch[c] = cd.ppitch;
+            pshare[c] = cd.sh == 2;  // both columns are one component sample
+            pcol[c] = (int)(cd.P - pbase) + (outlane ? (ca >> (cd.sh - 1)) : 0);
+        }
+        const int Hm1 = H - 1;
+        auto ld = [&](int c, int off) -> float2 {
+            const float *p = ybase + c * cs + off;
+            if (pair) return __ldg(reinterpret_cast<const float2 *>(p + ca));
+            return make_float2(__ldg(p + la), __ldg(p + lb));
+        };
+        auto pld = [&](int c, int row) -> float2 {
+            if (!pon[c]) return make_float2(0.f, 0.f);
+            const float *p = pbase + pcol[c] + (row >> psh[c]) * ppitch[c];
+            if (pshare[c]) {
+                const float v = __ldg(p);
+                return make_float2(v, v);
+            }
+            return __ldg(reinterpret_cast<const float2 *>(p));
+        };
+
+        float2 yv[NCH], dxp[NCH], dyp[NCH], Gm[NCH], G0[NCH], Gp[NCH], q1[NCH], q2[NCH], p1[NCH];
+        {
+            const int o0 = min(max(ys - 2, 0), Hm1) * pitch, o1 = min(max(ys - 1, 0), Hm1) * pitch;
+            const int o2 = min(ys, Hm1) * pitch, o3 = min(ys + 1, Hm1) * pitch;
+#pragma unroll
+            for (int c = 0; c < NCH; c++) {
+                const float2 y0 = ld(c, o0);
+                yv[c] = ld(c, o1);
+                q1[c] = ld(c, o2);
+                q2[c] = ld(c, o3);
+                p1[c] = pld(c, max(ys - 2, 0));  // output row of step ys - 1
+                const float yr = __shfl_down_sync(FULL, y0.x, 1);
+                dxp[c] = f2sub(make_float2(y0.y, yr), y0);
+                dyp[c] = f2sub(yv[c], y0);
+                Gm[c] = G0[c] = Gp[c] = make_float2(0.f, 0.f);
+            }
+        }
+        for (int t = ys - 1; t <= ys + R; t++) {
+            float2 yn[NCH], pr[NCH];
+            {
+                const int o = min(t + 3, Hm1) * pitch;
+                const int prow = min(max(t, 0), Hm1);
+#pragma unroll
+                for (int c = 0; c < NCH; c++) {
+                    yn[c] = q1[c];
+                    q1[c] = q2[c];
+                    q2[c] = ld(c, o);
+                    pr[c] = p1[c];
+                    p1[c] = pld(c, prow);
+                }
+            }
+            const bool rowin = t >= 0 && t < H, ty0 = t > 0;
+            float2 dx[NCH], dy[NCH], gxx[NCH], gyy[NCH], gs[NCH];
+            float2 n1 = make_float2(0.f, 0.f), n2 = make_float2(0.f, 0.f);
+#pragma unroll
+            for (int c = 0; c < NCH; c++) {
+                const float yr = __shfl_down_sync(FULL, yv[c].x, 1);
+                dx[c] = f2sub(make_float2(yv[c].y, yr), yv[c]);
+                dy[c] = f2sub(yn[c], yv[c]);
+                n1 = f2fma(dx[c], dx[c], n1);
+                n1 = f2fma(dy[c], dy[c], n1);
+            }
+#pragma unroll
+            for (int c = 0; c < NCH; c++) {
+                // Backward differences are zero at the left edge and the top row
+                // (compute_step_tv2.rs:53-69): take the neighbour equal to self.
+                const float dxs = __shfl_up_sync(FULL, dx[c].y, 1), dys = __shfl_up_sync(FULL, dy[c].y, 1);
+                const float2 dxl = make_float2(lft ? dxs : dx[c].x, dx[c].x);
+                const float2 dyl = make_float2(lft ? dys : dy[c].x, dy[c].x);
+                const float2 dxu = ty0 ? dxp[c] : dx[c], dyu = ty0 ? dyp[c] : dy[c];
+                const float2 axx = f2sub(dx[c], dxl), ayx = f2sub(dy[c], dyl);
+                const float2 ayy = f2sub(dy[c], dyu), axy = f2sub(dx[c], dxu);
+                const float2 s = f2mul(half2, f2add(axy, ayx));
+                n2 = f2add(n2, f2fma(ayy, ayy, f2fma(two2, f2mul(s, s), f2mul(axx, axx))));
+                gxx[c] = axx;
+                gyy[c] = ayy;
+                gs[c] = s;
+            }
+            float2 inv1, inv2;
+            inv1.x = (rowin && ina && n1.x > 0.f) ? rsqrtf(n1.x) : 0.f;
+            inv1.y = (rowin && inb && n1.y > 0.f) ? rsqrtf(n1.y) : 0.f;
+            inv2.x = (rowin && ina && n2.x > 0.f) ? rsqrtf(n2.x) : 0.f;
+            inv2.y = (rowin && inb && n2.y > 0.f) ? rsqrtf(n2.y) : 0.f;
+            const float2 at1 = f2mul(at, inv1), ag2 = f2mul(ag, inv2);
+#pragma unroll
+            for (int c = 0; c < NCH; c++) {
+                const float2 a = f2mul(at1, dx[c]), b = f2mul(at1, dy[c]);
+                const float2 u = f2mul(ag2, f2add(gs[c], gxx[c]));
+                const float2 v = f2mul(ag2, f2add(gyy[c], gs[c]));
+                const float2 w = f2mul(ag2, gs[c]);
+                const float2 au = f2add(a, u);
+                const float aul = __shfl_up_sync(FULL, au.y, 1);
+                const float ur = __shfl_down_sync(FULL, u.x, 1);
+                const float wr = __shfl_down_sync(FULL, w.x, 1);
+                const float wl = __shfl_up_sync(FULL, w.y, 1);
+                // centre term -(a + b) - 2 (u + v - w), then the neighbours' a + u and u
+                const float2 cen = f2fma(two2, f2sub(f2add(u, v), w), f2add(a, b));
+                G0[c] = f2add(f2sub(G0[c], cen), f2add(make_float2(aul, au.x), make_float2(u.y, ur)));
+                Gp[c] = f2add(Gp[c], f2sub(f2add(b, v), make_float2(w.y, wr)));
+                Gm[c] = f2add(Gm[c], f2sub(v, make_float2(wl, w.x)));
+                dxp[c] = dx[c];
+                dyp[c] = dy[c];
+                yv[c] = yn[c];
+            }
+            const int ro = t - 1;
+            if (outlane && ro >= ys && ro < ys + R && ro < H) {
+                const int go = ro * pitch;
+#pragma unroll
+                for (int c = 0; c < NCH; c++) {
+                    const float2 gv = f2add(Gm[c], pr[c]);
+                    *reinterpret_cast<float2 *>(gout + c * cs + go) = gv;
+                    ssq[c] = f2fma(gv, gv, ssq[c]);
+                }
+            }
+#pragma unroll
+            for (int c = 0; c < NCH; c++) {
+                Gm[c] = G0[c];
+                G0[c] = Gp[c];
+                Gp[c] = make_float2(0.f, 0.f);
+            }
+        }
+    }
+
+    // Fixed-order reduction: warp tree, then warps in order, then blocks in order.
+#pragma unroll
+    for (int c = 0; c < NCH; c++) {
+        float s = ssq[c].x + ssq[c].y;
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(FULL, s, o);
+        if (lane == 0) s_red[warp][c] = s;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+#pragma unroll
+        for (int c = 0; c < NCH; c++) {
+            float s = 0.f;
+            for (int w = 0; w < SWEEP_WARPS; w++) s += s_red[w][c];
+            im.partial[wk.y * 4 + c] = s;
+        }
+        __threadfence();
+        const unsigned done = atomicAdd(im.counter, 1u);
+        s_last = done == (unsigned)(im.ncta - 1);
+    }
+    __syncthreads();
+    if (s_last) {
+        __threadfence();
+        double acc[NCH];
+#pragma unroll
+        for (int c = 0; c < NCH; c++) acc[c] = 0.0;
+        for (int t = threadIdx.x; t < im.ncta; t += SWEEP_WARPS * 32) {
+#pragma unroll
+            for (int c = 0; c < NCH; c++) acc[c] += (double)__ldcg(im.partial + t * 4 + c);
+        }
+#pragma unroll
+        for (int c = 0; c < NCH; c++) {
+            double s = acc[c];
+#pragma unroll
+            for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(FULL, s, o);
+            if (lane == 0) s_dred[warp][c] = s;
+        }
+        __syncthreads();
+        if (threadIdx.x == 0) {
+#pragma unroll
+            for (int c = 0; c < NCH; c++) {
+                double s = 0.0;
+                for (int w = 0; w < SWEEP_WARPS; w++) s += s_dred[w][c];
+                const double nrm = sqrt(s);
+                im.sigma[c] = nrm > 0.0 ? (float)((double)im.step / nrm) : 0.f;
+            }
+            atomicExch(im.counter, 0u);
+        }
+    }
+}
+
+// Narrow variant of the gradient sweep: the same terms with one column per lane
+// and scalar arithmetic, so more warps cover an image and small images fill
+// the GPU better. One warp per strip of SWEEP_OUT_N output columns and
+// strip_rows rows; lane L holds column xs - 2 + L. Lanes 1..30 form the
+// per-pixel terms, lanes 2..29 write g. Rows and columns outside the image are
+// read clamped (replicated edges make the reference's last-row/column forward
+// differences vanish, compute_step_tv.rs:105-120) and their terms are zero,
+// which reproduces the reference's scatter guards. Rows are prefetched two
+// ahead of use.
+template <int NCH>
+__global__ void __launch_bounds__(SWEEP_WARPS_N * 32) k_grad_sweep_n(const ImgDev *__restrict__ imgs,
+                                                                 const int2 *__restrict__ work)
+{
+    __shared__ float s_red[SWEEP_WARPS_N][NCH];
+    __shared__ double s_dred[SWEEP_WARPS_N][NCH];
+    __shared__ int s_last;
+    const unsigned FULL = 0xffffffffu;
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int2 wk = work[blockIdx.x];
+    const ImgDev &im = imgs[wk.x];
+    const int W = im.W, H = im.H, pitch = im.pitch, R = im.strip_rows;
+    const int strip = wk.y * SWEEP_WARPS_N + warp;
     float ssq[NCH];
 #pragma unroll
     for (int c = 0; c < NCH; c++) ssq[c] = 0.f;
 
     if (strip < im.nstrips) {
         const int sxi = strip % im.strips_x, syi = strip / im.strips_x;
-        const int xs = sxi * SWEEP_OUT, ys = syi * R;
+        const int xs = sxi * SWEEP_OUT_N, ys = syi * R;
         const int gx = xs - 2 + lane;
         const int cx = min(max(gx, 0), W - 1);
         const bool colin = gx >= 0 && gx < W;
@@ -197,7 +421,7 @@ __global__ void __launch_bounds__(SWEEP_WARPS * 32) k_grad_sweep(const ImgDev *_
 #pragma unroll
         for (int c = 0; c < NCH; c++) {
             float s = 0.f;
-            for (int w = 0; w < SWEEP_WARPS; w++) s += s_red[w][c];
+            for (int w = 0; w < SWEEP_WARPS_N; w++) s += s_red[w][c];
             im.partial[wk.y * 4 + c] = s;
         }
         __threadfence();
@@ -210,7 +434,7 @@ __global__ void __launch_bounds__(SWEEP_WARPS * 32) k_grad_sweep(const ImgDev *_
         double acc[NCH];
 #pragma unroll
         for (int c = 0; c < NCH; c++) acc[c] = 0.0;
-        for (int t = threadIdx.x; t < im.ncta; t += SWEEP_WARPS * 32) {
+        for (int t = threadIdx.x; t < im.ncta; t += SWEEP_WARPS_N * 32) {
 #pragma unroll
             for (int c = 0; c < NCH; c++) acc[c] += (double)__ldcg(im.partial + t * 4 + c);
         }
@@ -226,7 +450,7 @@ __global__ void __launch_bounds__(SWEEP_WARPS * 32) k_grad_sweep(const ImgDev *_
 #pragma unroll
             for (int c = 0; c < NCH; c++) {
                 double s = 0.0;
-                for (int w = 0; w < SWEEP_WARPS; w++) s += s_dred[w][c];
+                for (int w = 0; w < SWEEP_WARPS_N; w++) s += s_dred[w][c];
                 const double nrm = sqrt(s);
                 im.sigma[c] = nrm > 0.0 ? (float)((double)im.step / nrm) : 0.f;
             }
@@ -599,7 +823,7 @@ std::vector<float> fista_factors(uint32_t iterations)
 }
 
 struct GraphKey {
-    int nimg = 0, wcount[4] = {0, 0, 0, 0};
+    int nimg = 0, wcount[8] = {0, 0, 0, 0, 0, 0, 0, 0};
     int mode_off[5] = {0, 0, 0, 0, 0};
     uint32_t iterations = 0;
     bool timing = false;
@@ -607,7 +831,7 @@ struct GraphKey {
     bool operator==(const GraphKey &o) const
     {
         return nimg == o.nimg && iterations == o.iterations && timing == o.timing && desc == o.desc &&
-               work == o.work && tasks == o.tasks && std::equal(wcount, wcount + 4, o.wcount) &&
+               work == o.work && tasks == o.tasks && std::equal(wcount, wcount + 8, o.wcount) &&
                std::equal(mode_off, mode_off + 5, o.mode_off);
     }
 };
@@ -631,8 +855,8 @@ struct ArtContext {
     cudaStream_t stream = nullptr;
     art::DevBuf xbuf, pbuf, coefimg, stage, misc, desc, work, tasks, compat, sepplanes, rgb;
     std::vector<art::ImgDev> h_desc;  // per image (pageable: copies of it are staged)
-    std::vector<int2> h_work;         // sweep blocks {image, block in image}, grouped by channel count 3, 2, 1
-    int wstart[4] = {0, 0, 0, 0}, wcount[4] = {0, 0, 0, 0};  // by channel count
+    std::vector<int2> h_work;         // sweep blocks {image, block in image}, grouped by variant and channel count
+    int wstart[2][4] = {}, wcount[2][4] = {};  // by sweep variant (0 narrow, 1 wide) and channel count
     std::vector<int4> h_tasks;        // block warps {image, channel, block row, first block}
     int mode_off[5] = {0, 0, 0, 0, 0};  // h_tasks grouped by sampling mode (1x1, 2x2, 2x1, 1x2)
     unsigned *errflag = nullptr;
@@ -642,7 +866,8 @@ struct ArtContext {
     std::vector<cudaEvent_t> events;  // [0,1] loop; then 4 per iteration
     uint32_t timed_iterations = 0;
     int strip_rows_override = 0;      // 0 = tuning cache, else size heuristic
-    std::map<std::string, int> tune;  // autotuned strip rows by geometry bucket
+    int sweep_kind_override = 0;
+    std::map<std::string, std::pair<int, int>> tune;  // autotuned (sweep variant, strip rows) by geometry bucket
 };
 
 namespace art {
@@ -665,15 +890,18 @@ std::string tune_key(uint32_t nch, const uint32_t *sh, const uint32_t *sv, uint3
     return k;
 }
 
-// Rows per gradient-sweep strip for one image: the autotuner's choice for its
-// bucket, else enough strips (over the whole batch) to fill every SM several
-// times over with strips as long as that allows, so the 3 extra rows a strip
-// reads stay small.
-int pick_strip_rows(const ArtContext *ctx, const ImageSpec &sp, long long batch_px)
+// Gradient-sweep variant and strip height for one image: the autotuner's
+// choice for its bucket, else by size -- the wide packed sweep once the batch
+// has enough pixels to fill every SM with its fewer, wider strips, and strips
+// as tall as that allows (the 3 extra rows a strip reads stay small).
+std::pair<int, int> pick_sweep(const ArtContext *ctx, const ImageSpec &sp, long long batch_px)
 {
-    if (ctx->strip_rows_override > 0) return ctx->strip_rows_override;
-    const char *env = getenv("ART_STRIP_ROWS");
-    if (env && atoi(env) > 0) return atoi(env);
+    const char *ek = getenv("ART_SWEEP_KIND");
+    const char *er = getenv("ART_STRIP_ROWS");
+    int kind = batch_px >= 8LL * 1024 * 1024 ? 1 : 0;
+    if (ctx->strip_rows_override > 0) return {ctx->sweep_kind_override, ctx->strip_rows_override};
+    if (ek && (atoi(ek) == 0 || atoi(ek) == 1)) kind = atoi(ek);
+    if (er && atoi(er) > 0) return {kind, atoi(er)};
     uint32_t sh[3], sv[3];
     for (uint32_t c = 0; c < sp.nch; c++) {
         sh[c] = sp.ch[c].samp_h;
@@ -681,9 +909,10 @@ int pick_strip_rows(const ArtContext *ctx, const ImageSpec &sp, long long batch_
     }
     auto it = ctx->tune.find(tune_key(sp.nch, sh, sv, sp.W, sp.H));
     if (it != ctx->tune.end()) return it->second;
+    const long long cols = kind ? SWEEP_OUT : SWEEP_OUT_N;
     int R = 128;
-    while (R > 32 && batch_px / ((long long)SWEEP_OUT * R) < 148LL * 16) R /= 2;
-    return R;
+    while (R > 16 && batch_px / (cols * R) < 148LL * 12) R /= 2;
+    return {kind, R};
 }
 
 template <int SH, int SV>
@@ -788,16 +1017,19 @@ static int prepare_batch(ArtContext *ctx, const std::vector<ImageSpec> &specs, u
         memset(&d, 0, sizeof(d));
         const int pitch = (int)align_up(sp.W, 32);
         const long long cstride = (long long)pitch * (long long)align_up(sp.H, 32);
-        const int R = pick_strip_rows(ctx, sp, batch_px);
+        const std::pair<int, int> sw = pick_sweep(ctx, sp, batch_px);
+        const int R = sw.second, out_cols = sw.first ? SWEEP_OUT : SWEEP_OUT_N;
+        const int warps = sw.first ? SWEEP_WARPS : SWEEP_WARPS_N;
         d.nch = (int)sp.nch;
         d.W = (int)sp.W;
         d.H = (int)sp.H;
         d.pitch = pitch;
+        d.sweep_kind = sw.first;
         d.strip_rows = R;
-        d.strips_x = (int)((sp.W + SWEEP_OUT - 1) / SWEEP_OUT);
+        d.strips_x = (int)((sp.W + out_cols - 1) / out_cols);
         d.strips_y = (int)((sp.H + R - 1) / R);
         d.nstrips = d.strips_x * d.strips_y;
-        d.ncta = (d.nstrips + SWEEP_WARPS - 1) / SWEEP_WARPS;
+        d.ncta = (d.nstrips + warps - 1) / warps;
         d.cstride = cstride;
         // compute_step_tv.rs:130 and compute_step_tv2.rs:88-89, compute_step.rs:47.
         d.alpha_tv = 1.0f / sqrtf((float)sp.nch);
@@ -837,7 +1069,7 @@ static int prepare_batch(ArtContext *ctx, const std::vector<ImageSpec> &specs, u
     float *xb = static_cast<float *>(ctx->xbuf.p);
     char *misc = static_cast<char *>(ctx->misc.p);
     ctx->errflag = reinterpret_cast<unsigned *>(misc);
-    std::vector<int2> wk[4];
+    std::vector<int2> wk[2][4];
     std::vector<int4> per_mode[4];
     for (int i = 0; i < nimg; i++) {
         ImgDev &d = ctx->h_desc[i];
@@ -851,15 +1083,16 @@ static int prepare_batch(ArtContext *ctx, const std::vector<ImageSpec> &specs, u
             d.ch[c].coef = reinterpret_cast<const int16_t *>(static_cast<char *>(ctx->coefimg.p) + o_coef[i][c]);
             d.ch[c].P = static_cast<float *>(ctx->pbuf.p) + o_p[i][c];
         }
-        for (int b = 0; b < d.ncta; b++) wk[d.nch].push_back(make_int2(i, b));
+        for (int b = 0; b < d.ncta; b++) wk[d.sweep_kind][d.nch].push_back(make_int2(i, b));
         build_tasks(d, i, per_mode);
     }
     ctx->h_work.clear();
-    for (int n = 3; n >= 1; n--) {
-        ctx->wstart[n] = (int)ctx->h_work.size();
-        ctx->wcount[n] = (int)wk[n].size();
-        ctx->h_work.insert(ctx->h_work.end(), wk[n].begin(), wk[n].end());
-    }
+    for (int kd = 0; kd < 2; kd++)
+        for (int n = 3; n >= 1; n--) {
+            ctx->wstart[kd][n] = (int)ctx->h_work.size();
+            ctx->wcount[kd][n] = (int)wk[kd][n].size();
+            ctx->h_work.insert(ctx->h_work.end(), wk[kd][n].begin(), wk[kd][n].end());
+        }
     ctx->h_tasks.clear();
     for (int m = 0; m < 4; m++) {
         ctx->mode_off[m] = (int)ctx->h_tasks.size();
@@ -924,12 +1157,18 @@ static void launch_iteration(ArtContext *ctx, int it, float fnext)
     cudaStream_t s = ctx->stream;
     const bool tm = ctx->timing;
     if (tm) cudaEventRecordWithFlags(ctx->events[2 + 4 * it], s, cudaEventRecordExternal);
-    if (ctx->wcount[3])
-        k_grad_sweep<3><<<ctx->wcount[3], SWEEP_WARPS * 32, 0, s>>>(ddesc, work + ctx->wstart[3]);
-    if (ctx->wcount[2])
-        k_grad_sweep<2><<<ctx->wcount[2], SWEEP_WARPS * 32, 0, s>>>(ddesc, work + ctx->wstart[2]);
-    if (ctx->wcount[1])
-        k_grad_sweep<1><<<ctx->wcount[1], SWEEP_WARPS * 32, 0, s>>>(ddesc, work + ctx->wstart[1]);
+    if (ctx->wcount[1][3])
+        k_grad_sweep<3><<<ctx->wcount[1][3], SWEEP_WARPS * 32, 0, s>>>(ddesc, work + ctx->wstart[1][3]);
+    if (ctx->wcount[1][2])
+        k_grad_sweep<2><<<ctx->wcount[1][2], SWEEP_WARPS * 32, 0, s>>>(ddesc, work + ctx->wstart[1][2]);
+    if (ctx->wcount[1][1])
+        k_grad_sweep<1><<<ctx->wcount[1][1], SWEEP_WARPS * 32, 0, s>>>(ddesc, work + ctx->wstart[1][1]);
+    if (ctx->wcount[0][3])
+        k_grad_sweep_n<3><<<ctx->wcount[0][3], SWEEP_WARPS_N * 32, 0, s>>>(ddesc, work + ctx->wstart[0][3]);
+    if (ctx->wcount[0][2])
+        k_grad_sweep_n<2><<<ctx->wcount[0][2], SWEEP_WARPS_N * 32, 0, s>>>(ddesc, work + ctx->wstart[0][2]);
+    if (ctx->wcount[0][1])
+        k_grad_sweep_n<1><<<ctx->wcount[0][1], SWEEP_WARPS_N * 32, 0, s>>>(ddesc, work + ctx->wstart[0][1]);
     if (tm) cudaEventRecordWithFlags(ctx->events[3 + 4 * it], s, cudaEventRecordExternal);
     if (tm) cudaEventRecordWithFlags(ctx->events[4 + 4 * it], s, cudaEventRecordExternal);
     for (int m = 3; m >= 0; m--) {
@@ -964,7 +1203,7 @@ static int run_iterations(ArtContext *ctx, uint32_t iterations)
     }
     GraphKey key;
     key.nimg = (int)ctx->h_desc.size();
-    std::copy(ctx->wcount, ctx->wcount + 4, key.wcount);
+    std::copy(&ctx->wcount[0][0], &ctx->wcount[0][0] + 8, key.wcount);
     std::copy(ctx->mode_off, ctx->mode_off + 5, key.mode_off);
     key.iterations = iterations;
     key.timing = ctx->timing;
@@ -1406,7 +1645,8 @@ int32_t art_context_compute_batch_device(ArtContext *ctx, uint32_t nimages, cons
 // -------------------------------------------------------------- autotuner --
 
 int32_t art_context_autotune(ArtContext *ctx, uint32_t nchannel, const uint32_t *samp_h, const uint32_t *samp_v,
-                             uint32_t max_w, uint32_t max_h, uint32_t iterations, uint32_t *strip_rows_out)
+                             uint32_t max_w, uint32_t max_h, uint32_t iterations, uint32_t *variant_out,
+                             uint32_t *strip_rows_out)
 {
     if (!ctx || !samp_h || !samp_v || nchannel < 1 || nchannel > 3)
         return fail(ART_ERR_INVALID_ARGUMENT, "bad autotune arguments");
@@ -1455,11 +1695,13 @@ int32_t art_context_autotune(ArtContext *ctx, uint32_t nchannel, const uint32_t 
     ART_CUDA(cudaEventCreate(&e1));
     const bool timing = ctx->timing;
     ctx->timing = false;
-    int best = 0;
+    int best = 0, best_kind = 0;
     float best_ms = 0.f;
-    const int candidates[4] = {16, 32, 64, 128};
-    for (int R : candidates) {
+    const int candidates[8][2] = {{0, 16}, {0, 32}, {0, 64}, {0, 128}, {1, 16}, {1, 32}, {1, 64}, {1, 128}};
+    for (const auto &cand : candidates) {
+        const int R = cand[1];
         if ((int)max_h < R && R > 16) continue;
+        ctx->sweep_kind_override = cand[0];
         ctx->strip_rows_override = R;
         rc = prepare_batch(ctx, {sp}, iterations, ART_INIT_DECODED);
         if (!rc) rc = run_iterations(ctx, iterations);  // captures and warms up
@@ -1476,16 +1718,19 @@ int32_t art_context_autotune(ArtContext *ctx, uint32_t nchannel, const uint32_t 
         if (rc) break;
         if (!best || ms < best_ms) {
             best = R;
+            best_kind = cand[0];
             best_ms = ms;
         }
     }
     ctx->strip_rows_override = 0;
+    ctx->sweep_kind_override = 0;
     ctx->timing = timing;
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);
     if (rc) return rc;
     ART_CUDA(cudaStreamSynchronize(ctx->stream));
-    ctx->tune[tune_key(nchannel, samp_h, samp_v, max_w, max_h)] = best;
+    ctx->tune[tune_key(nchannel, samp_h, samp_v, max_w, max_h)] = {best_kind, best};
+    if (variant_out) *variant_out = (uint32_t)best_kind;
     if (strip_rows_out) *strip_rows_out = (uint32_t)best;
     return ART_OK;
 }
@@ -1496,8 +1741,8 @@ int32_t art_context_tune_cache(ArtContext *ctx, const char *path, int32_t save)
     if (save) {
         std::ofstream f(path);
         if (!f) return fail(ART_ERR_INVALID_ARGUMENT, std::string("cannot write ") + path);
-        f << "# artefact_b200 autotune cache: <geometry bucket> <gradient-sweep strip rows>\n";
-        for (const auto &kv : ctx->tune) f << kv.first << " " << kv.second << "\n";
+        f << "# artefact_b200 autotune cache: <geometry bucket> <sweep variant 0|1> <strip rows>\n";
+        for (const auto &kv : ctx->tune) f << kv.first << " " << kv.second.first << " " << kv.second.second << "\n";
         return f.good() ? ART_OK : fail(ART_ERR_INVALID_ARGUMENT, std::string("cannot write ") + path);
     }
     std::ifstream f(path);
@@ -1507,10 +1752,11 @@ int32_t art_context_tune_cache(ArtContext *ctx, const char *path, int32_t save)
         if (line.empty() || line[0] == '#') continue;
         std::istringstream ls(line);
         std::string key;
-        int rows = 0;
-        if (!(ls >> key >> rows) || (rows != 16 && rows != 32 && rows != 64 && rows != 128))
+        int kind = -1, rows = 0;
+        if (!(ls >> key >> kind >> rows) || (kind != 0 && kind != 1) ||
+            (rows != 16 && rows != 32 && rows != 64 && rows != 128))
             return fail(ART_ERR_INVALID_ARGUMENT, "malformed tune cache line: " + line);
-        ctx->tune[key] = rows;
+        ctx->tune[key] = {kind, rows};
     }
     return ART_OK;
 }
@@ -1650,8 +1896,8 @@ extern "C" int32_t art_solve_noalloc(uint32_t nchannel, const ArtChannel *coefs,
     if (3 * cstride >= (1LL << 31))
         return fail(ART_ERR_INVALID_ARGUMENT, "image too large: three padded planes must stay below 2^31 floats");
     const int R = 32;
-    const int strips_x = (int)((W + SWEEP_OUT - 1) / SWEEP_OUT), strips_y = (int)((H + R - 1) / R);
-    const int nstrips = strips_x * strips_y, ncta = (nstrips + SWEEP_WARPS - 1) / SWEEP_WARPS;
+    const int strips_x = (int)((W + SWEEP_OUT_N - 1) / SWEEP_OUT_N), strips_y = (int)((H + R - 1) / R);
+    const int nstrips = strips_x * strips_y, ncta = (nstrips + SWEEP_WARPS_N - 1) / SWEEP_WARPS_N;
     size_t off = 0;
     auto take = [&](size_t bytes) {
         const size_t o = off;
@@ -1762,11 +2008,11 @@ extern "C" int32_t art_solve_noalloc(uint32_t nchannel, const ArtChannel *coefs,
     for (uint32_t it = 0; it < iterations; it++) {
         const float fnext = it + 1 < iterations ? next_factor() : 0.0f;
         if (nch == 3)
-            k_grad_sweep<3><<<ncta, SWEEP_WARPS * 32, 0, s>>>(ddesc, work);
+            k_grad_sweep_n<3><<<ncta, SWEEP_WARPS_N * 32, 0, s>>>(ddesc, work);
         else if (nch == 2)
-            k_grad_sweep<2><<<ncta, SWEEP_WARPS * 32, 0, s>>>(ddesc, work);
+            k_grad_sweep_n<2><<<ncta, SWEEP_WARPS_N * 32, 0, s>>>(ddesc, work);
         else
-            k_grad_sweep<1><<<ncta, SWEEP_WARPS * 32, 0, s>>>(ddesc, work);
+            k_grad_sweep_n<1><<<ncta, SWEEP_WARPS_N * 32, 0, s>>>(ddesc, work);
         for (int m = 3; m >= 0; m--) {
             const int n = mode_off[m + 1] - mode_off[m];
             if (n == 0) continue;

@@ -42,9 +42,9 @@ struct ChanDev {
 
 struct ImgDev {
     int nch, W, H, pitch;  // full-resolution plane size; pitch in floats
-    int strips_x, strips_y, nstrips, strip_rows;  // gradient sweep strips (28 columns x strip_rows)
+    int strips_x, strips_y, nstrips, strip_rows;  // gradient sweep strips (28 or 60 columns x strip_rows)
     int ncta;              // gradient-sweep blocks of this image
-    int pad0;
+    int sweep_kind;        // 0 = narrow sweep (one column per lane), 1 = wide (two, packed FP32x2)
     long long cstride;     // floats between channel planes
     float *x;              // iterate x_k; channel c at x + c * cstride
     float *y;              // FISTA point y_k = x_k + f_k (x_k - x_{k-1})
@@ -58,8 +58,10 @@ struct ImgDev {
     float invq2[3][64];
 };
 
-constexpr int SWEEP_OUT = 28;   // output columns per warp strip
-constexpr int SWEEP_WARPS = 8;  // warps (strips) per sweep block
+constexpr int SWEEP_OUT = 60;     // wide sweep: output columns per warp strip (32 lanes x 2 columns, 2 of halo each side)
+constexpr int SWEEP_WARPS = 4;    // wide sweep: warps (strips) per block
+constexpr int SWEEP_OUT_N = 28;   // narrow sweep: 32 lanes x 1 column, 2 of halo each side
+constexpr int SWEEP_WARPS_N = 8;  // narrow sweep: warps per block
 constexpr int PROJ_WARPS = 4;   // warps per projection block (4 coefficient blocks per warp)
 
 // ---------------------------------------------------------------- transforms
@@ -176,6 +178,19 @@ __device__ __forceinline__ void idct8x8_regs(float *a)
     }
 #pragma unroll
     for (int j = 0; j < 8; j++) idct8(a + j * 8);
+}
+
+// Packed FP32x2 arithmetic (one instruction for two lanes' worth of work).
+__device__ __forceinline__ float2 f2add(float2 a, float2 b) { return __fadd2_rn(a, b); }
+__device__ __forceinline__ float2 f2mul(float2 a, float2 b) { return __fmul2_rn(a, b); }
+__device__ __forceinline__ float2 f2fma(float2 a, float2 b, float2 c) { return __ffma2_rn(a, b, c); }
+__device__ __forceinline__ float2 f2sub(float2 a, float2 b)
+{
+    unsigned long long ua, ub, r;
+    ua = (unsigned long long)__float_as_uint(a.x) | ((unsigned long long)__float_as_uint(a.y) << 32);
+    ub = (unsigned long long)__float_as_uint(b.x) | ((unsigned long long)__float_as_uint(b.y) << 32);
+    asm("sub.rn.f32x2 %0, %1, %2;" : "=l"(r) : "l"(ua), "l"(ub));
+    return make_float2(__uint_as_float((unsigned)r), __uint_as_float((unsigned)(r >> 32)));
 }
 
 // 8x8 transpose among the 8 lanes (r = lane & 7) of a lane group through a

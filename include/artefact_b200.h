@@ -148,16 +148,20 @@ int32_t art_context_compute_batch_device(ArtContext *ctx, uint32_t nimages, cons
                                          uint32_t iterations, const ArtOptions *opts, void *stream);
 
 /*
- * Autotuner. Times the gradient sweep's strip height (16, 32, 64, 128 rows)
- * on a deterministic synthetic image of the given geometry (`iterations`
- * steps, 0 = 10) and caches the fastest for the geometry's bucket (channel
- * count, sampling, width and height rounded up to powers of two); later solves
- * of images in that bucket use it. art_context_tune_cache saves (save != 0) or
- * loads the cache as a text file of "<bucket> <rows>" lines.
+ * Autotuner. Times both gradient-sweep variants (0 = narrow, one column per
+ * lane; 1 = wide, two columns per lane on packed FP32x2 arithmetic) at each
+ * strip height (16, 32, 64, 128 rows) on a deterministic synthetic image of
+ * the given geometry (`iterations` steps, 0 = 10) and caches the fastest pair
+ * for the geometry's bucket (channel count, sampling, width and height rounded
+ * up to powers of two); later solves of images in that bucket use it. The two
+ * variants sum the same terms in a different order (results agree to fp32
+ * rounding), and each is deterministic. art_context_tune_cache saves
+ * (save != 0) or loads the cache as a text file of
+ * "<bucket> <variant> <rows>" lines. Either output pointer may be NULL.
  */
 int32_t art_context_autotune(ArtContext *ctx, uint32_t nchannel, const uint32_t *samp_h, const uint32_t *samp_v,
                              uint32_t max_rounded_px_w, uint32_t max_rounded_px_h, uint32_t iterations,
-                             uint32_t *strip_rows_out);
+                             uint32_t *variant_out, uint32_t *strip_rows_out);
 int32_t art_context_tune_cache(ArtContext *ctx, const char *path, int32_t save);
 
 /* Wait for the context's queued work; returns the first error it met. */

@@ -45,11 +45,11 @@ def test_autotune_and_cache_roundtrip(gpu, tmp_path):
     j = _jpeg(512, 384, 75, "4:2:0", False, seed=700)
     W, H, N_ = j.max_rounded()
     with Context(0) as ctx:
-        rows = ctx.autotune(3, [1, 2, 2], [1, 2, 2], W, H, iterations=5)
-        assert rows in (16, 32, 64, 128)
+        kind, rows = ctx.autotune(3, [1, 2, 2], [1, 2, 2], W, H, iterations=5)
+        assert kind in (0, 1) and rows in (16, 32, 64, 128)
         path = tmp_path / "tune.txt"
         ctx.save_tune_cache(path)
-        assert f" {rows}" in path.read_text()
+        assert f" {kind} {rows}\n" in path.read_text()
         tuned = ctx.compute(3, j.coefs, 0.3, [0.001] * 3, 20, W, H)
     with Context(0) as ctx2:
         ctx2.load_tune_cache(path)
@@ -57,3 +57,22 @@ def test_autotune_and_cache_roundtrip(gpu, tmp_path):
     assert all(np.array_equal(a, b) for a, b in zip(tuned, again))
     ref = O.compute(3, j.coefs, 0.3, [0.001] * 3, 20, W, H)
     assert max(float(np.abs(a - b).max()) for a, b in zip(tuned, ref)) <= MAX_ABS
+
+
+@pytest.mark.parametrize("shape", [(72, 40, "4:2:0", False), (200, 136, "4:4:4", False), (128, 96, "4:2:2", False),
+                                   (96, 64, "4:4:4", True)])
+def test_sweep_variants_agree(gpu, monkeypatch, shape):
+    """The narrow and the wide gradient sweep at every strip height match the
+    oracle, and each (variant, height) is deterministic."""
+    w, h, sub, gray = shape
+    j = _jpeg(w, h, 80, sub, gray, seed=900 + w)
+    W, H, N_ = j.max_rounded()
+    for kind in (0, 1):
+        for rows in (16, 32, 64, 128):
+            monkeypatch.setenv("ART_SWEEP_KIND", str(kind))
+            monkeypatch.setenv("ART_STRIP_ROWS", str(rows))
+            with Context(0) as ctx:
+                a = ctx.compute(j.nchannel, j.coefs, 0.3, [0.001] * 3, 30, W, H)
+                b = ctx.compute(j.nchannel, j.coefs, 0.3, [0.001] * 3, 30, W, H)
+            assert all(np.array_equal(x, y) for x, y in zip(a, b))
+            check_parity(j, 30, label=f"sweep variant {kind} rows {rows}", gpu=a)
