@@ -60,6 +60,27 @@ class ArtImage(C.Structure):
     ]
 
 
+class ArtCnnConv(C.Structure):
+    _fields_ = [
+        ("B", C.c_int32), ("H", C.c_int32), ("W", C.c_int32),
+        ("cin", C.c_int32), ("ck", C.c_int32), ("n", C.c_int32), ("n_store", C.c_int32),
+        ("x", C.c_void_p), ("wpack", C.c_void_p), ("bias", C.c_void_p),
+        ("out", C.c_void_p), ("out_cstride", C.c_int32), ("out_coff", C.c_int32),
+        ("out_f32", C.c_void_p), ("f32_cstride", C.c_int32),
+        ("mask", C.c_void_p), ("mask_cstride", C.c_int32),
+        ("relu", C.c_int32), ("accumulate", C.c_int32),
+        ("err", C.c_void_p),
+    ]
+
+
+class ArtCnnWgrad(C.Structure):
+    _fields_ = [
+        ("B", C.c_int32), ("H", C.c_int32), ("W", C.c_int32), ("cout", C.c_int32), ("cin", C.c_int32),
+        ("dy", C.c_void_p), ("x", C.c_void_p), ("dw", C.c_void_p), ("accumulate", C.c_int32),
+        ("workspace", C.c_void_p), ("workspace_bytes", C.c_int64), ("err", C.c_void_p),
+    ]
+
+
 class ArtError(RuntimeError):
     """Raised when a C ABI call returns a negative status."""
 
@@ -106,6 +127,36 @@ EXPORTS = {
     "art_jpeg_info": (C.c_int32, [C.c_void_p, C.POINTER(C.c_uint32), C.POINTER(C.c_uint32),
                                   C.POINTER(C.c_uint32)]),
     "art_jpeg_channel": (C.c_int32, [C.c_void_p, C.c_uint32, C.POINTER(ArtChannel)]),
+    "art_net_num_params": (C.c_int64, []),
+    "art_net_create": (C.c_int32, [C.c_int32, C.c_void_p, C.c_int64, C.POINTER(C.c_void_p)]),
+    "art_net_destroy": (None, [C.c_void_p]),
+    "art_net_params": (C.c_int32, [C.c_void_p, C.c_void_p, C.c_int64]),
+    "art_net_gradients": (C.c_int32, [C.c_void_p, C.c_void_p, C.c_int64]),
+    "art_net_predict": (C.c_int32, [C.c_void_p, C.c_void_p, C.c_int32, C.c_int64, C.c_void_p, C.c_int32, C.c_int32,
+                                    C.c_int32, C.c_void_p, C.c_void_p]),
+    "art_net_train_step": (C.c_int32, [C.c_void_p, C.c_void_p, C.c_int32, C.c_int64, C.c_void_p, C.c_void_p,
+                                       C.c_int32, C.c_int32, C.c_int32, C.c_float, C.POINTER(C.c_float),
+                                       C.c_void_p]),
+    "art_cnn_conv3x3": (C.c_int32, [C.POINTER(ArtCnnConv), C.c_void_p]),
+    "art_cnn_wgrad3x3": (C.c_int32, [C.POINTER(ArtCnnWgrad), C.c_void_p]),
+    "art_cnn_pack_weights": (C.c_int32, [C.c_void_p, C.c_int32, C.c_int32, C.c_int32, C.c_int32, C.c_int32,
+                                         C.c_int32, C.c_void_p, C.c_void_p]),
+    "art_cnn_pool2": (C.c_int32, [C.c_void_p, C.c_int32, C.c_int32, C.c_int32, C.c_int32, C.c_int32, C.c_int32,
+                                  C.c_void_p, C.c_void_p]),
+    "art_cnn_upsample2": (C.c_int32, [C.c_void_p, C.c_int32, C.c_int32, C.c_int32, C.c_int32, C.c_void_p,
+                                      C.c_int32, C.c_int32, C.c_void_p]),
+    "art_cnn_downsum2_mask": (C.c_int32, [C.c_void_p, C.c_int32, C.c_int32, C.c_int32, C.c_int32, C.c_void_p,
+                                          C.c_void_p, C.c_void_p]),
+    "art_cnn_unpool_add_mask": (C.c_int32, [C.c_void_p, C.c_void_p, C.c_int32, C.c_int32, C.c_int32, C.c_int32,
+                                            C.c_void_p, C.c_int32, C.c_int32, C.c_void_p]),
+    "art_cnn_bias_grad": (C.c_int32, [C.c_void_p, C.c_int64, C.c_int32, C.c_void_p, C.c_int64, C.c_void_p,
+                                      C.c_int32, C.c_void_p]),
+    "art_cnn_features": (C.c_int32, [C.c_void_p, C.c_int32, C.c_int64, C.c_void_p, C.c_int32, C.c_int32,
+                                     C.c_int32, C.c_void_p, C.c_void_p, C.c_void_p]),
+    "art_cnn_residual": (C.c_int32, [C.c_void_p, C.c_int32, C.c_void_p, C.c_void_p, C.c_int64, C.c_void_p,
+                                     C.c_void_p, C.c_void_p, C.c_int32, C.c_void_p]),
+    "art_cnn_adam": (C.c_int32, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_int64, C.c_float, C.c_float,
+                                 C.c_float, C.c_float, C.c_int32, C.c_void_p]),
 }
 
 _lib = None

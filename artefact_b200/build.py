@@ -18,7 +18,7 @@ CSRC = PKG / "csrc"
 INCLUDE = PKG.parent / "include"
 LIB = PKG / "libartefact_b200.so"
 
-SOURCES = ["solver.cu", "capi_host.cpp", "jpeg_decode.cpp"]
+SOURCES = ["solver.cu", "cnn.cu", "capi_host.cpp", "jpeg_decode.cpp"]
 GENCODE = ["-gencode", "arch=compute_100a,code=sm_100a"]
 
 

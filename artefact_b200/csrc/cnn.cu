@@ -1,0 +1,1406 @@
+// Warm-start network of the restoration solver: BF16 tensor-core kernels for
+// sm_100a (tcgen05 MMA with TMEM accumulators, TMA-staged operands) and the
+// memory-bound glue around them. The network has no counterpart in the
+// reference; it only chooses where the reference's iteration starts.
+//
+// Tensors are NHWC bf16: element (b, y, x, c) at ((b * H + y) * W + x) * C + c.
+//
+// k_conv3x3   3x3 convolution, stride 1, zero padding 1, as an implicit GEMM:
+//             D[pixel][n] = sum_{tap, c} X[pixel + d(tap)][c] * Wt[n][tap][c].
+//             A tile is 2 output rows x 128 pixels. TMA loads the input halo
+//             (4 rows x 130 pixels, 8 channels per box, zero fill outside the
+//             image) so that, with pixels stored 16 bytes apart, the A
+//             operand of every tap is the same shared-memory matrix started
+//             (dy + 1) * 130 + dx + 1 rows further on. The weights of one
+//             channel chunk for all 9 taps come in by one bulk copy. Warp 0
+//             issues the loads, warp 1 the MMAs (accumulators in TMEM, two
+//             tiles in flight), warps 2-5 the epilogue (bias, ReLU, ReLU-mask,
+//             accumulate, bf16 or fp32 store). Backward-data is the same kernel
+//             on the output gradient with the weights flipped and transposed.
+// k_wgrad3x3  weight gradient dW[n][tap][c] = sum_pixel dY[pixel][n] *
+//             X[pixel + d(tap)][c]: both operands MN-major from the same kind
+//             of TMA tiles; 9 tap accumulators in TMEM; one partial per band
+//             of tiles, reduced in a fixed order by k_wgrad_reduce.
+#include <cuda.h>
+#include <cuda_bf16.h>
+#include <cuda_runtime.h>
+#include <cudaTypedefs.h>
+
+#include <cmath>
+#include <cstdint>
+#include <mutex>
+#include <string>
+
+#include "art_internal.h"
+#include "artefact_b200.h"
+#include "solver_kernels.cuh"
+#include "tc_ptx.cuh"
+
+namespace art {
+namespace cnn {
+
+using bf16 = __nv_bfloat16;
+
+constexpr int TPX = 128;                    // output pixels per tile row (MMA M)
+constexpr int TROWS = 2;                    // output rows per tile
+constexpr int HPX = TPX + 2;                // halo tile width
+constexpr int HROWS = TROWS + 2;            // halo tile height
+constexpr uint32_t KCOL = HROWS * HPX * 16; // bytes of one 8-channel column of a halo tile (8320)
+constexpr uint32_t DYREG = TROWS * TPX * 16;// bytes of one 8-channel region of a gradient tile (4096)
+constexpr int THREADS = 192;                // warp 0 loads, warp 1 MMA, warps 2-5 epilogue
+constexpr uint32_t SMEM_BUDGET = 220 * 1024;  // pipeline stages; 1 KB more is requested for alignment
+constexpr int MAX_STAGES = 4;
+
+struct ConvArgs {
+    int B, H, W;
+    int cin, ck;      // input channels (multiple of ck), channels per pipeline stage (16 or 32)
+    int n, n_store;   // MMA N (multiple of 16, <= 128), channels stored (multiple of 16, <= n)
+    const bf16 *wpack;  // [cin/ck][9][ck/8][n][8]
+    const float *bias;  // [n] or null
+    bf16 *out;
+    int out_cstride, out_coff;
+    float *out_f32;
+    int f32_cstride;
+    const bf16 *mask;   // optional: zero where mask <= 0 (ReLU backward)
+    int mask_cstride;
+    int relu, accumulate;
+    int stages;
+    uint32_t stage_bytes, halo_bytes;
+    int *err;
+};
+
+struct WgradArgs {
+    int B, H, W;
+    int cout, cin, nci;  // gradient channels (<= 128), input channels, input channels per CTA (16 or 32)
+    int tiles_per_band;
+    float *partial;      // [bands][cin/nci][9][cout][nci]
+    int stages;
+    uint32_t stage_bytes;
+    int *err;
+};
+
+__device__ __forceinline__ void tile_coords(int tile, int tiles_x, int tiles_y, int &b, int &y0, int &x0)
+{
+    const int per = tiles_x * tiles_y;
+    b = tile / per;
+    const int r = tile - b * per;
+    y0 = (r / tiles_x) * TROWS;
+    x0 = (r % tiles_x) * TPX;
+}
+
+// Waits without honouring the abort flag (used to drain in-flight work
+// before TMEM is freed), still bounded.
+__device__ __forceinline__ bool drain_wait(uint64_t *bar, uint32_t parity)
+{
+    int dummy = 0;
+    return tc::mbar_wait(bar, parity, &dummy);
+}
+
+__device__ __forceinline__ unsigned char *aligned_smem(unsigned char *p)
+{
+    const uint32_t a = tc::smem_u32(p);
+    return p + ((1024 - (a & 1023)) & 1023);
+}
+
+__global__ void __launch_bounds__(THREADS, 1) k_conv3x3(const __grid_constant__ CUtensorMap xmap, const ConvArgs a)
+{
+    extern __shared__ __align__(1024) unsigned char smem_raw[];
+    unsigned char *smem = aligned_smem(smem_raw);
+    __shared__ __align__(8) uint64_t full_bar[MAX_STAGES], empty_bar[MAX_STAGES], accf_bar[2], acce_bar[2],
+        done_bar;
+    __shared__ uint32_t tmem_base;
+    __shared__ int abort_s;
+    volatile int *abort_p = &abort_s;
+
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int tiles_x = (a.W + TPX - 1) / TPX, tiles_y = (a.H + TROWS - 1) / TROWS;
+    const int ntiles = a.B * tiles_x * tiles_y;
+    const int nchunks = a.cin / a.ck;
+    const int S = a.stages;
+
+    if (threadIdx.x == 0) {
+        abort_s = 0;
+        for (int s = 0; s < S; s++) {
+            tc::mbar_init(&full_bar[s], 1);
+            tc::mbar_init(&empty_bar[s], 1);
+        }
+        for (int b = 0; b < 2; b++) {
+            tc::mbar_init(&accf_bar[b], 1);
+            tc::mbar_init(&acce_bar[b], 128);
+        }
+        tc::mbar_init(&done_bar, 1);
+        tc::fence_barrier_init();
+    }
+    if (warp == 1) tc::tmem_alloc(&tmem_base, 512);
+    tc::tc_fence_before();
+    __syncthreads();
+    tc::tc_fence_after();
+    const uint32_t tbase = tmem_base;
+
+    if (warp == 0) {
+        if (lane == 0) {
+            uint32_t it = 0;
+            bool ok = true;
+            for (int tile = blockIdx.x; tile < ntiles && ok; tile += gridDim.x) {
+                int b, y0, x0;
+                tile_coords(tile, tiles_x, tiles_y, b, y0, x0);
+                for (int c = 0; c < nchunks; c++, it++) {
+                    const int s = it % S;
+                    const uint32_t use = it / S;
+                    if (use > 0 && !tc::mbar_wait(&empty_bar[s], (use - 1) & 1, abort_p)) {
+                        ok = false;
+                        break;
+                    }
+                    unsigned char *st = smem + (size_t)s * a.stage_bytes;
+                    tc::mbar_arrive_expect_tx(&full_bar[s], a.stage_bytes);
+                    for (int j = 0; j < a.ck / 8; j++)
+                        tc::tma_load_4d(st + j * KCOL, &xmap, c * a.ck + 8 * j, x0 - 1, y0 - 1, b, &full_bar[s]);
+                    tc::bulk_load(st + a.halo_bytes, a.wpack + (size_t)c * 9 * a.ck * a.n, 18u * a.ck * a.n,
+                                  &full_bar[s]);
+                }
+            }
+            // Let the copies still in flight land before the block can exit.
+            const uint32_t last = it;
+            for (uint32_t k = (last > (uint32_t)S ? last - S : 0); k < last; k++)
+                drain_wait(&full_bar[k % S], (k / S) & 1);
+        }
+        __syncwarp();
+    } else if (warp == 1) {
+        if (lane == 0) {
+            const uint32_t idesc = tc::idesc_bf16(128, a.n, 0, 0);
+            uint32_t it = 0, tcount = 0;
+            bool ok = true;
+            for (int tile = blockIdx.x; tile < ntiles && ok; tile += gridDim.x, tcount++) {
+                const int ab = tcount & 1;
+                const uint32_t ause = tcount >> 1;
+                if (ause > 0 && !tc::mbar_wait(&acce_bar[ab], (ause - 1) & 1, abort_p)) break;
+                tc::tc_fence_after();
+                for (int c = 0; c < nchunks; c++, it++) {
+                    const int s = it % S;
+                    if (!tc::mbar_wait(&full_bar[s], (it / S) & 1, abort_p)) {
+                        ok = false;
+                        break;
+                    }
+                    tc::tc_fence_after();
+                    const uint32_t st = tc::smem_u32(smem + (size_t)s * a.stage_bytes);
+                    const uint32_t wst = st + a.halo_bytes;
+                    for (int tap = 0; tap < 9; tap++) {
+                        const int ty = tap / 3, tx = tap % 3;
+                        for (int kk = 0; kk < a.ck / 16; kk++) {
+                            const uint64_t bdesc =
+                                tc::smem_desc(wst + (uint32_t)((tap * (a.ck / 8) + 2 * kk) * a.n * 16), a.n * 16, 128);
+#pragma unroll
+                            for (int t = 0; t < TROWS; t++) {
+                                const uint64_t adesc = tc::smem_desc(
+                                    st + 2 * kk * KCOL + (uint32_t)(((t + ty) * HPX + tx) * 16), KCOL, 128);
+                                tc::mma_bf16(tbase + (uint32_t)((ab * TROWS + t) * 128), adesc, bdesc, idesc,
+                                             (c | tap | kk) != 0);
+                            }
+                        }
+                    }
+                    tc::mma_commit(&empty_bar[s]);
+                }
+                if (ok) tc::mma_commit(&accf_bar[ab]);
+            }
+            tc::mma_commit(&done_bar);
+            drain_wait(&done_bar, 0);
+        }
+        __syncwarp();
+    } else {
+        const int q = warp & 3;  // TMEM lanes 32q..32q+31 belong to this warp
+        const int px = q * 32 + lane;
+        uint32_t tcount = 0;
+        for (int tile = blockIdx.x; tile < ntiles; tile += gridDim.x, tcount++) {
+            const int ab = tcount & 1;
+            // One lane waits and the warp follows its verdict, so the warp-wide
+            // TMEM loads below never run with part of the warp gone.
+            int ok = lane == 0 ? (int)tc::mbar_wait(&accf_bar[ab], (tcount >> 1) & 1, abort_p) : 0;
+            ok = __shfl_sync(0xffffffffu, ok, 0);
+            if (!ok) break;
+            tc::mbar_wait(&accf_bar[ab], (tcount >> 1) & 1, abort_p);  // completes at once: every lane observes the phase
+            tc::tc_fence_after();
+            int b, y0, x0;
+            tile_coords(tile, tiles_x, tiles_y, b, y0, x0);
+#pragma unroll 1
+            for (int t = 0; t < TROWS; t++) {
+                const int y = y0 + t, x = x0 + px;
+                const bool in = y < a.H && x < a.W;
+                const size_t pix = ((size_t)b * a.H + (in ? y : 0)) * a.W + (in ? x : 0);
+#pragma unroll 1
+                for (int c0 = 0; c0 < a.n; c0 += 16) {
+                    float v[16];
+                    tc::tmem_ld16(tbase + ((uint32_t)(q * 32) << 16) + (uint32_t)((ab * TROWS + t) * 128 + c0), v);
+                    if (!in || c0 >= a.n_store) continue;
+                    if (a.bias) {
+#pragma unroll
+                        for (int i = 0; i < 16; i++) v[i] += __ldg(a.bias + c0 + i);
+                    }
+                    if (a.relu) {
+#pragma unroll
+                        for (int i = 0; i < 16; i++) v[i] = fmaxf(v[i], 0.f);
+                    }
+                    if (a.mask) {
+                        const uint4 *mp = reinterpret_cast<const uint4 *>(a.mask + pix * a.mask_cstride + c0);
+                        const uint4 m2[2] = {__ldg(mp), __ldg(mp + 1)};
+                        const bf16 *m = reinterpret_cast<const bf16 *>(m2);
+#pragma unroll
+                        for (int i = 0; i < 16; i++) v[i] = __bfloat162float(m[i]) > 0.f ? v[i] : 0.f;
+                    }
+                    if (a.out_f32) {
+                        float4 *o = reinterpret_cast<float4 *>(a.out_f32 + pix * a.f32_cstride + c0);
+#pragma unroll
+                        for (int i = 0; i < 4; i++) o[i] = make_float4(v[4 * i], v[4 * i + 1], v[4 * i + 2], v[4 * i + 3]);
+                    }
+                    if (a.out) {
+                        uint4 *o = reinterpret_cast<uint4 *>(a.out + pix * a.out_cstride + a.out_coff + c0);
+                        if (a.accumulate) {
+                            const uint4 p2[2] = {o[0], o[1]};
+                            const bf16 *p = reinterpret_cast<const bf16 *>(p2);
+#pragma unroll
+                            for (int i = 0; i < 16; i++) v[i] += __bfloat162float(p[i]);
+                        }
+                        uint4 w2[2];
+                        __nv_bfloat162 *w = reinterpret_cast<__nv_bfloat162 *>(w2);
+#pragma unroll
+                        for (int i = 0; i < 8; i++) w[i] = __floats2bfloat162_rn(v[2 * i], v[2 * i + 1]);
+                        o[0] = w2[0];
+                        o[1] = w2[1];
+                    }
+                }
+            }
+            tc::tc_fence_before();
+            tc::mbar_arrive(&acce_bar[ab]);
+        }
+    }
+
+    tc::tc_fence_before();
+    __syncthreads();
+    if (warp == 1) {
+        tc::tc_fence_after();
+        tc::tmem_dealloc(tbase, 512);
+    }
+    if (threadIdx.x == 0 && abort_s) atomicExch(a.err, 1);
+}
+
+__global__ void __launch_bounds__(THREADS, 1) k_wgrad3x3(const __grid_constant__ CUtensorMap dymap,
+                                                         const __grid_constant__ CUtensorMap xmap, const WgradArgs a)
+{
+    extern __shared__ __align__(1024) unsigned char smem_raw[];
+    unsigned char *smem = aligned_smem(smem_raw);
+    __shared__ __align__(8) uint64_t full_bar[MAX_STAGES], empty_bar[MAX_STAGES], accf_bar, done_bar;
+    __shared__ uint32_t tmem_base;
+    __shared__ int abort_s;
+    volatile int *abort_p = &abort_s;
+
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int tiles_x = (a.W + TPX - 1) / TPX, tiles_y = (a.H + TROWS - 1) / TROWS;
+    const int ntiles = a.B * tiles_x * tiles_y;
+    const int band = blockIdx.x, chunk = blockIdx.y, nchunk = gridDim.y;
+    const int t_begin = band * a.tiles_per_band, t_end = min(ntiles, t_begin + a.tiles_per_band);
+    const int S = a.stages;
+    const uint32_t dy_bytes = 16 * DYREG;  // M = 128 gradient channels: 16 regions (unused ones are never read back)
+
+    if (threadIdx.x == 0) {
+        abort_s = 0;
+        for (int s = 0; s < S; s++) {
+            tc::mbar_init(&full_bar[s], 1);
+            tc::mbar_init(&empty_bar[s], 1);
+        }
+        tc::mbar_init(&accf_bar, 1);
+        tc::mbar_init(&done_bar, 1);
+        tc::fence_barrier_init();
+    }
+    if (warp == 1) tc::tmem_alloc(&tmem_base, 512);
+    tc::tc_fence_before();
+    __syncthreads();
+    tc::tc_fence_after();
+    const uint32_t tbase = tmem_base;
+
+    if (warp == 0) {
+        if (lane == 0) {
+            const uint32_t tx_bytes = (uint32_t)(a.cout / 8) * DYREG + (uint32_t)(a.nci / 8) * KCOL;
+            uint32_t it = 0;
+            for (int tile = t_begin; tile < t_end; tile++, it++) {
+                const int s = it % S;
+                const uint32_t use = it / S;
+                if (use > 0 && !tc::mbar_wait(&empty_bar[s], (use - 1) & 1, abort_p)) break;
+                int b, y0, x0;
+                tile_coords(tile, tiles_x, tiles_y, b, y0, x0);
+                unsigned char *st = smem + (size_t)s * a.stage_bytes;
+                tc::mbar_arrive_expect_tx(&full_bar[s], tx_bytes);
+                for (int g = 0; g < a.cout / 8; g++)
+                    tc::tma_load_4d(st + g * DYREG, &dymap, 8 * g, x0, y0, b, &full_bar[s]);
+                for (int j = 0; j < a.nci / 8; j++)
+                    tc::tma_load_4d(st + dy_bytes + j * KCOL, &xmap, chunk * a.nci + 8 * j, x0 - 1, y0 - 1, b,
+                                    &full_bar[s]);
+            }
+            const uint32_t last = it;
+            for (uint32_t k = (last > (uint32_t)S ? last - S : 0); k < last; k++)
+                drain_wait(&full_bar[k % S], (k / S) & 1);
+        }
+        __syncwarp();
+    } else if (warp == 1) {
+        if (lane == 0) {
+            const uint32_t idesc = tc::idesc_bf16(128, a.nci, 1, 1);
+            uint32_t it = 0;
+            bool ok = true;
+            for (int tile = t_begin; tile < t_end; tile++, it++) {
+                const int s = it % S;
+                if (!tc::mbar_wait(&full_bar[s], (it / S) & 1, abort_p)) {
+                    ok = false;
+                    break;
+                }
+                tc::tc_fence_after();
+                const uint32_t st = tc::smem_u32(smem + (size_t)s * a.stage_bytes);
+                const uint32_t xs = st + dy_bytes;
+                for (int tap = 0; tap < 9; tap++) {
+                    const int ty = tap / 3, tx = tap % 3;
+#pragma unroll
+                    for (int r = 0; r < TROWS; r++)
+#pragma unroll
+                        for (int k0 = 0; k0 < TPX; k0 += 16) {
+                            const uint64_t adesc = tc::smem_desc(st + (uint32_t)((r * TPX + k0) * 16), 128, DYREG);
+                            const uint64_t bdesc =
+                                tc::smem_desc(xs + (uint32_t)(((r + ty) * HPX + k0 + tx) * 16), 128, KCOL);
+                            tc::mma_bf16(tbase + (uint32_t)(tap * a.nci), adesc, bdesc, idesc,
+                                         (it | r | k0) != 0);
+                        }
+                }
+                tc::mma_commit(&empty_bar[s]);
+            }
+            if (ok) tc::mma_commit(&accf_bar);
+            tc::mma_commit(&done_bar);
+            drain_wait(&done_bar, 0);
+        }
+        __syncwarp();
+    } else {
+        const int q = warp & 3;
+        const int co = q * 32 + lane;
+        int ok = lane == 0 ? (int)tc::mbar_wait(&accf_bar, 0, abort_p) : 0;
+        ok = __shfl_sync(0xffffffffu, ok, 0);
+        if (ok) tc::mbar_wait(&accf_bar, 0, abort_p);
+        if (ok) {
+            tc::tc_fence_after();
+            float *dst = a.partial + ((size_t)(band * nchunk + chunk) * 9) * a.cout * a.nci;
+#pragma unroll 1
+            for (int tap = 0; tap < 9; tap++)
+#pragma unroll 1
+                for (int c0 = 0; c0 < a.nci; c0 += 16) {
+                    float v[16];
+                    tc::tmem_ld16(tbase + ((uint32_t)(q * 32) << 16) + (uint32_t)(tap * a.nci + c0), v);
+                    if (co < a.cout) {
+                        float4 *o = reinterpret_cast<float4 *>(dst + ((size_t)tap * a.cout + co) * a.nci + c0);
+#pragma unroll
+                        for (int i = 0; i < 4; i++)
+                            o[i] = make_float4(v[4 * i], v[4 * i + 1], v[4 * i + 2], v[4 * i + 3]);
+                    }
+                }
+        }
+    }
+
+    tc::tc_fence_before();
+    __syncthreads();
+    if (warp == 1) {
+        tc::tc_fence_after();
+        tc::tmem_dealloc(tbase, 512);
+    }
+    if (threadIdx.x == 0 && abort_s) atomicExch(a.err, 1);
+}
+
+// dW[n][tap][c] (+)= sum over bands of the partials, in band order.
+__global__ void k_wgrad_reduce(const float *__restrict__ partial, int bands, int cout, int cin, int nci,
+                               float *__restrict__ dw, int accumulate)
+{
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    const int total = cout * 9 * cin;
+    if (i >= total) return;
+    const int c = i % cin, tap = (i / cin) % 9, n = i / (9 * cin);
+    const int chunk = c / nci, cc = c % nci, nchunk = cin / nci;
+    float s = 0.f;
+    for (int b = 0; b < bands; b++)
+        s += partial[(((size_t)(b * nchunk + chunk) * 9 + tap) * cout + n) * nci + cc];
+    dw[i] = accumulate ? dw[i] + s : s;
+}
+
+// Packs fp32 master weights W[cout][9][cin] into the bf16 layout a conv stage
+// copies in one piece: [chunk][tap][ck/8][n][8]. Forward: n = output channel,
+// k = input channel. Transposed (backward-data): n = input channel ci0 + n,
+// k = output channel, taps mirrored.
+__global__ void k_pack(const float *__restrict__ w, int cout, int cin, int transpose, int ci0, int n_out, int ck,
+                       bf16 *__restrict__ out)
+{
+    const int K = transpose ? cout : cin;
+    const int total = n_out * 9 * K;
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= total) return;
+    const int e = i % 8;
+    const int n = (i / 8) % n_out;
+    const int rest = i / (8 * n_out);  // (chunk * 9 + tap) * (ck/8) + kcol
+    const int kcol = rest % (ck / 8);
+    const int tap = (rest / (ck / 8)) % 9;
+    const int chunk = rest / ((ck / 8) * 9);
+    const int k = chunk * ck + kcol * 8 + e;
+    float v;
+    if (!transpose)
+        v = (n < cout && k < cin) ? w[((size_t)n * 9 + tap) * cin + k] : 0.f;
+    else
+        v = (k < cout && ci0 + n < cin) ? w[((size_t)k * 9 + (8 - tap)) * cin + ci0 + n] : 0.f;
+    out[i] = __float2bfloat16_rn(v);
+}
+
+// 2x2 average pooling (NHWC, 8 channels per thread) of channels
+// [in_coff, in_coff + C) of a tensor with in_cstride channels.
+__global__ void k_pool2(const bf16 *__restrict__ in, int B, int H, int W, int C, int in_cstride, int in_coff,
+                        bf16 *__restrict__ out)
+{
+    const int Ho = H / 2, Wo = W / 2, cg = C / 8;
+    const long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    const long long total = (long long)B * Ho * Wo * cg;
+    if (i >= total) return;
+    const int g = (int)(i % cg);
+    const long long p = i / cg;
+    const int x = (int)(p % Wo), y = (int)((p / Wo) % Ho), b = (int)(p / ((long long)Wo * Ho));
+    float acc[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+#pragma unroll
+    for (int dy = 0; dy < 2; dy++)
+#pragma unroll
+        for (int dx = 0; dx < 2; dx++) {
+            const uint4 r =
+                __ldg(reinterpret_cast<const uint4 *>(in + (((size_t)b * H + 2 * y + dy) * W + 2 * x + dx) * in_cstride +
+                                                      in_coff + 8 * g));
+            const bf16 *v = reinterpret_cast<const bf16 *>(&r);
+#pragma unroll
+            for (int k = 0; k < 8; k++) acc[k] += __bfloat162float(v[k]);
+        }
+    uint4 o;
+    __nv_bfloat162 *w = reinterpret_cast<__nv_bfloat162 *>(&o);
+#pragma unroll
+    for (int k = 0; k < 4; k++) w[k] = __floats2bfloat162_rn(0.25f * acc[2 * k], 0.25f * acc[2 * k + 1]);
+    *reinterpret_cast<uint4 *>(out + (((size_t)b * Ho + y) * Wo + x) * C + 8 * g) = o;
+}
+
+// Nearest 2x upsampling of in[B][H/2][W/2][C] into channels [coff, coff + C)
+// of out[B][H][W][Cs].
+__global__ void k_upsample2(const bf16 *__restrict__ in, int B, int H, int W, int C, bf16 *__restrict__ out,
+                            int Cs, int coff)
+{
+    const int cg = C / 8;
+    const long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    const long long total = (long long)B * H * W * cg;
+    if (i >= total) return;
+    const int g = (int)(i % cg);
+    const long long p = i / cg;
+    const int x = (int)(p % W), y = (int)((p / W) % H), b = (int)(p / ((long long)W * H));
+    const uint4 r = __ldg(
+        reinterpret_cast<const uint4 *>(in + (((size_t)b * (H / 2) + y / 2) * (W / 2) + x / 2) * C + 8 * g));
+    *reinterpret_cast<uint4 *>(out + (((size_t)b * H + y) * W + x) * Cs + coff + 8 * g) = r;
+}
+
+// Backward of nearest upsampling followed by the ReLU mask of the upsampled
+// activation: out[b][y][x][c] = (sum of the 2x2 cell of g) * (act > 0).
+__global__ void k_downsum2_mask(const bf16 *__restrict__ g, int B, int H, int W, int C, const bf16 *__restrict__ act,
+                                bf16 *__restrict__ out)
+{
+    const int Ho = H / 2, Wo = W / 2, cg = C / 8;
+    const long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    const long long total = (long long)B * Ho * Wo * cg;
+    if (i >= total) return;
+    const int k8 = (int)(i % cg);
+    const long long p = i / cg;
+    const int x = (int)(p % Wo), y = (int)((p / Wo) % Ho), b = (int)(p / ((long long)Wo * Ho));
+    float acc[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+#pragma unroll
+    for (int dy = 0; dy < 2; dy++)
+#pragma unroll
+        for (int dx = 0; dx < 2; dx++) {
+            const uint4 r =
+                __ldg(reinterpret_cast<const uint4 *>(g + (((size_t)b * H + 2 * y + dy) * W + 2 * x + dx) * C + 8 * k8));
+            const bf16 *v = reinterpret_cast<const bf16 *>(&r);
+#pragma unroll
+            for (int k = 0; k < 8; k++) acc[k] += __bfloat162float(v[k]);
+        }
+    const size_t o = (((size_t)b * Ho + y) * Wo + x) * C + 8 * k8;
+    const uint4 ra = __ldg(reinterpret_cast<const uint4 *>(act + o));
+    const bf16 *av = reinterpret_cast<const bf16 *>(&ra);
+    uint4 res;
+    __nv_bfloat162 *w = reinterpret_cast<__nv_bfloat162 *>(&res);
+#pragma unroll
+    for (int k = 0; k < 4; k++)
+        w[k] = __floats2bfloat162_rn(__bfloat162float(av[2 * k]) > 0.f ? acc[2 * k] : 0.f,
+                                     __bfloat162float(av[2 * k + 1]) > 0.f ? acc[2 * k + 1] : 0.f);
+    *reinterpret_cast<uint4 *>(out + o) = res;
+}
+
+// Gradient of an encoder activation used both as a skip connection (gradient
+// already in g) and through 2x2 average pooling (gradient gp at half
+// resolution, may be null), then its ReLU mask, in place:
+// g = (g + gp[up] / 4) * (act > 0); act = channels [act_coff, act_coff + C)
+// of a tensor with act_cstride channels.
+__global__ void k_unpool_add_mask(bf16 *__restrict__ g, const bf16 *__restrict__ gp, int B, int H, int W, int C,
+                                  const bf16 *__restrict__ act, int act_cstride, int act_coff)
+{
+    const int cg = C / 8;
+    const long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    const long long total = (long long)B * H * W * cg;
+    if (i >= total) return;
+    const int k8 = (int)(i % cg);
+    const long long p = i / cg;
+    const int x = (int)(p % W), y = (int)((p / W) % H), b = (int)(p / ((long long)W * H));
+    const size_t o = (size_t)p * C + 8 * k8;
+    uint4 rg = *reinterpret_cast<const uint4 *>(g + o);
+    const uint4 ra = __ldg(reinterpret_cast<const uint4 *>(act + (size_t)p * act_cstride + act_coff + 8 * k8));
+    uint4 rp = make_uint4(0, 0, 0, 0);
+    if (gp) rp = __ldg(reinterpret_cast<const uint4 *>(gp + (((size_t)b * (H / 2) + y / 2) * (W / 2) + x / 2) * C + 8 * k8));
+    const bf16 *gv = reinterpret_cast<const bf16 *>(&rg), *av = reinterpret_cast<const bf16 *>(&ra),
+               *pv = reinterpret_cast<const bf16 *>(&rp);
+    uint4 res;
+    __nv_bfloat162 *w = reinterpret_cast<__nv_bfloat162 *>(&res);
+#pragma unroll
+    for (int k = 0; k < 4; k++) {
+        float v0 = __bfloat162float(gv[2 * k]) + 0.25f * __bfloat162float(pv[2 * k]);
+        float v1 = __bfloat162float(gv[2 * k + 1]) + 0.25f * __bfloat162float(pv[2 * k + 1]);
+        v0 = __bfloat162float(av[2 * k]) > 0.f ? v0 : 0.f;
+        v1 = __bfloat162float(av[2 * k + 1]) > 0.f ? v1 : 0.f;
+        w[k] = __floats2bfloat162_rn(v0, v1);
+    }
+    *reinterpret_cast<uint4 *>(g + o) = res;
+}
+
+// Per-channel sums over all pixels of g[npix][C] (bias gradient), two passes
+// with a fixed order: blocks write partials, one block adds them.
+__global__ void k_colsum_partial(const bf16 *__restrict__ g, long long npix, int C, float *__restrict__ partial)
+{
+    __shared__ float s[256];
+    const int per_row = 256 / C;  // pixels handled per step by the block
+    const int c = threadIdx.x % C, r = threadIdx.x / C;
+    float acc = 0.f;
+    if (r < per_row)
+        for (long long p = (long long)blockIdx.x * per_row + r; p < npix; p += (long long)gridDim.x * per_row)
+            acc += __bfloat162float(g[p * C + c]);
+    s[threadIdx.x] = acc;
+    __syncthreads();
+    if (threadIdx.x < C) {
+        float t = 0.f;
+        for (int k = 0; k < per_row; k++) t += s[k * C + threadIdx.x];
+        partial[(size_t)blockIdx.x * C + threadIdx.x] = t;
+    }
+}
+
+__global__ void k_colsum_final(const float *__restrict__ partial, int nblk, int C, float *__restrict__ out,
+                               int accumulate)
+{
+    const int c = threadIdx.x;
+    if (c >= C) return;
+    float t = 0.f;
+    for (int b = 0; b < nblk; b++) t += partial[(size_t)b * C + c];
+    out[c] = accumulate ? out[c] + t : t;
+}
+
+// Network input from a coefficient image: per 8x8 block the decoded samples
+// IDCT(c * q) (level-shifted, as the solver's start) into dec (fp32) and the
+// feature tensor F[B][H][W][16] (bf16): channel 0 = decoded / 128, channel 1
+// = the block's quantisation step of the sample's frequency position / 64,
+// channels 2-15 = 0.
+__global__ void k_features(const int16_t *__restrict__ coef, int cpitch, long long img_stride, const float *__restrict__ q,
+                           int B, int H, int W, float *__restrict__ dec, bf16 *__restrict__ feat)
+{
+    const int bw = W / 8, bh = H / 8;
+    const long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    if (i >= (long long)B * bw * bh) return;
+    const int bx = (int)(i % bw), by = (int)((i / bw) % bh), b = (int)(i / ((long long)bw * bh));
+    const float *qt = q + (size_t)b * 64;
+    float a[64];
+    for (int r = 0; r < 8; r++) {
+        float c8[8];
+        load_coef_row(coef + b * img_stride + (size_t)(by * 8 + r) * cpitch + bx * 8, c8);
+#pragma unroll
+        for (int u = 0; u < 8; u++) a[r * 8 + u] = c8[u] * __ldg(qt + r * 8 + u);
+    }
+    idct8x8_regs(a);
+    for (int r = 0; r < 8; r++) {
+        const size_t p0 = ((size_t)b * H + by * 8 + r) * W + bx * 8;
+#pragma unroll
+        for (int u = 0; u < 8; u++) {
+            dec[p0 + u] = a[r * 8 + u];
+            uint4 o[2] = {make_uint4(0, 0, 0, 0), make_uint4(0, 0, 0, 0)};
+            __nv_bfloat162 *w = reinterpret_cast<__nv_bfloat162 *>(o);
+            w[0] = __floats2bfloat162_rn(a[r * 8 + u] * (1.f / 128.f), __ldg(qt + r * 8 + u) * (1.f / 64.f));
+            uint4 *f = reinterpret_cast<uint4 *>(feat + (p0 + u) * 16);
+            f[0] = o[0];
+            f[1] = o[1];
+        }
+    }
+}
+
+// Residual head output r (fp32, channel 0 of rows of `rstride`) -> prediction
+// x = dec + 16 r; with a target: gradient of the mean squared error in
+// units of 16 levels into grad[p][16] (channel 0, others zero) and per-block
+// partial sums of the squared error.
+__global__ void k_residual(const float *__restrict__ r, int rstride, const float *__restrict__ dec,
+                           const float *__restrict__ target, long long npix, float inv_count, float *__restrict__ pred,
+                           bf16 *__restrict__ grad, float *__restrict__ loss_partial)
+{
+    __shared__ float s[256];
+    float acc = 0.f;
+    for (long long p = blockIdx.x * (long long)blockDim.x + threadIdx.x; p < npix; p += (long long)gridDim.x * blockDim.x) {
+        const float rv = r[p * rstride];
+        const float d = dec[p];
+        if (pred) pred[p] = d + 16.f * rv;
+        if (target) {
+            const float e = rv - (target[p] - d) * (1.f / 16.f);
+            acc += e * e;
+            uint4 o[2] = {make_uint4(0, 0, 0, 0), make_uint4(0, 0, 0, 0)};
+            reinterpret_cast<bf16 *>(o)[0] = __float2bfloat16_rn(2.f * e * inv_count);
+            uint4 *g = reinterpret_cast<uint4 *>(grad + p * 16);
+            g[0] = o[0];
+            g[1] = o[1];
+        }
+    }
+    s[threadIdx.x] = acc;
+    __syncthreads();
+    for (int k = 128; k > 0; k >>= 1) {
+        if (threadIdx.x < k) s[threadIdx.x] += s[threadIdx.x + k];
+        __syncthreads();
+    }
+    if (threadIdx.x == 0 && loss_partial) loss_partial[blockIdx.x] = s[0];
+}
+
+// Adam on flat fp32 parameters (decoupled from the bf16 copies the convs read).
+__global__ void k_adam(float *__restrict__ w, const float *__restrict__ g, float *__restrict__ m, float *__restrict__ v,
+                       long long n, float lr, float b1, float b2, float eps, float c1, float c2)
+{
+    const long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const float gi = g[i];
+    const float mi = b1 * m[i] + (1.f - b1) * gi;
+    const float vi = b2 * v[i] + (1.f - b2) * gi * gi;
+    m[i] = mi;
+    v[i] = vi;
+    w[i] -= lr * (mi * c1) / (sqrtf(vi * c2) + eps);
+}
+
+// ---------------------------------------------------------------------------
+// Host side.
+
+PFN_cuTensorMapEncodeTiled_v12000 encode_fn()
+{
+    static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
+    static std::once_flag once;
+    std::call_once(once, [] {
+        void *p = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) == cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            fn = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(p);
+    });
+    return fn;
+}
+
+// Tensor map over an NHWC bf16 tensor [B][H][W][C] with box {8, bw, bh, 1}.
+bool make_map(CUtensorMap *m, const void *base, int B, int H, int W, int C, int bw, int bh, std::string &err)
+{
+    auto fn = encode_fn();
+    if (!fn) {
+        err = "cuTensorMapEncodeTiled is unavailable";
+        return false;
+    }
+    if ((reinterpret_cast<uintptr_t>(base) & 15) || C % 8) {
+        err = "tensor base must be 16-byte aligned and channels a multiple of 8";
+        return false;
+    }
+    cuuint64_t dims[4] = {(cuuint64_t)C, (cuuint64_t)W, (cuuint64_t)H, (cuuint64_t)B};
+    cuuint64_t strides[3] = {(cuuint64_t)C * 2, (cuuint64_t)W * C * 2, (cuuint64_t)H * W * C * 2};
+    cuuint32_t box[4] = {8, (cuuint32_t)bw, (cuuint32_t)bh, 1};
+    cuuint32_t es[4] = {1, 1, 1, 1};
+    const CUresult r = fn(m, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 4, const_cast<void *>(base), dims, strides, box, es,
+                          CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
+                          CU_TENSOR_MAP_L2_PROMOTION_L2_128B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    if (r != CUDA_SUCCESS) {
+        err = "cuTensorMapEncodeTiled failed (" + std::to_string((int)r) + ")";
+        return false;
+    }
+    return true;
+}
+
+int num_sms()
+{
+    static int n = 0;
+    if (!n) {
+        int dev = 0;
+        cudaGetDevice(&dev);
+        cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev);
+        if (n <= 0) n = 148;
+    }
+    return n;
+}
+
+int32_t fail(int32_t code, const std::string &msg)
+{
+    set_error(msg);
+    return code;
+}
+
+int32_t check_launch(const char *what)
+{
+    const cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return fail(ART_ERR_CUDA, std::string(what) + ": " + cudaGetErrorString(e));
+    return ART_OK;
+}
+
+int32_t conv3x3(const ArtCnnConv *d, cudaStream_t s)
+{
+    if (!d || !d->x || !d->wpack || !d->err) return fail(ART_ERR_INVALID_ARGUMENT, "conv: null pointer");
+    if (d->B < 1 || d->H < 1 || d->W < 1) return fail(ART_ERR_INVALID_ARGUMENT, "conv: empty tensor");
+    if (d->ck != 16 && d->ck != 32) return fail(ART_ERR_INVALID_ARGUMENT, "conv: ck must be 16 or 32");
+    if (d->cin < d->ck || d->cin % d->ck) return fail(ART_ERR_INVALID_ARGUMENT, "conv: cin must be a multiple of ck");
+    if (d->n < 16 || d->n > 128 || d->n % 16) return fail(ART_ERR_INVALID_ARGUMENT, "conv: n must be 16..128, multiple of 16");
+    if (d->n_store < 16 || d->n_store > d->n || d->n_store % 16)
+        return fail(ART_ERR_INVALID_ARGUMENT, "conv: n_store must be a multiple of 16 and at most n");
+    if (!d->out && !d->out_f32) return fail(ART_ERR_INVALID_ARGUMENT, "conv: no output");
+    if (d->out && (d->out_cstride % 8 || d->out_coff % 8 || d->out_coff + d->n_store > d->out_cstride))
+        return fail(ART_ERR_INVALID_ARGUMENT, "conv: bad output channel stride/offset");
+    if (d->out_f32 && (d->f32_cstride % 4 || d->f32_cstride < d->n_store))
+        return fail(ART_ERR_INVALID_ARGUMENT, "conv: bad fp32 output stride");
+    if (d->mask && (d->mask_cstride % 8 || d->mask_cstride < d->n_store))
+        return fail(ART_ERR_INVALID_ARGUMENT, "conv: bad mask stride");
+    if ((long long)d->B * d->H * d->W * (long long)d->cin >= (1LL << 40))
+        return fail(ART_ERR_INVALID_ARGUMENT, "conv: tensor too large");
+    CUtensorMap map;
+    std::string err;
+    if (!make_map(&map, d->x, d->B, d->H, d->W, d->cin, HPX, HROWS, err)) return fail(ART_ERR_CUDA, "conv: " + err);
+    ConvArgs a{};
+    a.B = d->B;
+    a.H = d->H;
+    a.W = d->W;
+    a.cin = d->cin;
+    a.ck = d->ck;
+    a.n = d->n;
+    a.n_store = d->n_store;
+    a.wpack = static_cast<const bf16 *>(d->wpack);
+    a.bias = d->bias;
+    a.out = static_cast<bf16 *>(d->out);
+    a.out_cstride = d->out_cstride;
+    a.out_coff = d->out_coff;
+    a.out_f32 = d->out_f32;
+    a.f32_cstride = d->f32_cstride;
+    a.mask = static_cast<const bf16 *>(d->mask);
+    a.mask_cstride = d->mask_cstride;
+    a.relu = d->relu;
+    a.accumulate = d->accumulate;
+    a.halo_bytes = (uint32_t)(d->ck / 8) * KCOL;
+    a.stage_bytes = a.halo_bytes + 18u * d->ck * d->n;
+    a.stages = (int)std::min<uint32_t>(MAX_STAGES, SMEM_BUDGET / a.stage_bytes);
+    a.err = d->err;
+    if (a.stages < 2) return fail(ART_ERR_INVALID_ARGUMENT, "conv: stage does not fit shared memory");
+    const uint32_t smem = a.stages * a.stage_bytes + 1024;
+    cudaFuncSetAttribute(k_conv3x3, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)(SMEM_BUDGET + 1024));
+    const long long ntiles = (long long)d->B * ((d->H + TROWS - 1) / TROWS) * ((d->W + TPX - 1) / TPX);
+    const int grid = (int)std::min<long long>(ntiles, num_sms());
+    k_conv3x3<<<grid, THREADS, smem, s>>>(map, a);
+    return check_launch("k_conv3x3");
+}
+
+int32_t wgrad3x3(const ArtCnnWgrad *d, cudaStream_t s)
+{
+    if (!d || !d->x || !d->dy || !d->dw || !d->workspace || !d->err)
+        return fail(ART_ERR_INVALID_ARGUMENT, "wgrad: null pointer");
+    if (d->B < 1 || d->H < 1 || d->W < 1) return fail(ART_ERR_INVALID_ARGUMENT, "wgrad: empty tensor");
+    if (d->cout < 8 || d->cout > 128 || d->cout % 8) return fail(ART_ERR_INVALID_ARGUMENT, "wgrad: cout must be 8..128, multiple of 8");
+    const int nci = d->cin % 32 == 0 ? 32 : 16;
+    if (d->cin < 16 || d->cin % 16) return fail(ART_ERR_INVALID_ARGUMENT, "wgrad: cin must be a multiple of 16");
+    const long long ntiles = (long long)d->B * ((d->H + TROWS - 1) / TROWS) * ((d->W + TPX - 1) / TPX);
+    const int nchunk = d->cin / nci;
+    int bands = (int)std::max<long long>(1, std::min<long long>(ntiles, (2LL * num_sms() + nchunk - 1) / nchunk));
+    const long long per_band_bytes = (long long)nchunk * 9 * d->cout * nci * 4;
+    bands = (int)std::min<long long>(bands, std::max<long long>(1, (long long)d->workspace_bytes / per_band_bytes));
+    if (per_band_bytes > (long long)d->workspace_bytes) return fail(ART_ERR_INVALID_ARGUMENT, "wgrad: workspace too small");
+    const int tpb = (int)((ntiles + bands - 1) / bands);
+    bands = (int)((ntiles + tpb - 1) / tpb);
+    CUtensorMap dymap, xmap;
+    std::string err;
+    if (!make_map(&dymap, d->dy, d->B, d->H, d->W, d->cout, TPX, TROWS, err)) return fail(ART_ERR_CUDA, "wgrad: " + err);
+    if (!make_map(&xmap, d->x, d->B, d->H, d->W, d->cin, HPX, HROWS, err)) return fail(ART_ERR_CUDA, "wgrad: " + err);
+    WgradArgs a{};
+    a.B = d->B;
+    a.H = d->H;
+    a.W = d->W;
+    a.cout = d->cout;
+    a.cin = d->cin;
+    a.nci = nci;
+    a.tiles_per_band = tpb;
+    a.partial = static_cast<float *>(d->workspace);
+    a.stage_bytes = 16 * DYREG + (uint32_t)(nci / 8) * KCOL;
+    a.stages = (int)std::min<uint32_t>(MAX_STAGES, SMEM_BUDGET / a.stage_bytes);
+    a.err = d->err;
+    cudaFuncSetAttribute(k_wgrad3x3, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)(SMEM_BUDGET + 1024));
+    k_wgrad3x3<<<dim3(bands, nchunk), THREADS, a.stages * a.stage_bytes + 1024, s>>>(dymap, xmap, a);
+    int32_t rc = check_launch("k_wgrad3x3");
+    if (rc) return rc;
+    const int total = d->cout * 9 * d->cin;
+    k_wgrad_reduce<<<(total + 255) / 256, 256, 0, s>>>(a.partial, bands, d->cout, d->cin, nci, d->dw, d->accumulate);
+    return check_launch("k_wgrad_reduce");
+}
+
+inline unsigned blocks_for(long long n, int t = 256) { return (unsigned)((n + t - 1) / t); }
+
+}  // namespace cnn
+}  // namespace art
+
+using namespace art::cnn;
+
+extern "C" {
+
+int32_t art_cnn_conv3x3(const ArtCnnConv *desc, void *stream)
+{
+    return conv3x3(desc, static_cast<cudaStream_t>(stream));
+}
+
+int32_t art_cnn_wgrad3x3(const ArtCnnWgrad *desc, void *stream)
+{
+    return wgrad3x3(desc, static_cast<cudaStream_t>(stream));
+}
+
+int32_t art_cnn_pack_weights(const float *w, int32_t cout, int32_t cin, int32_t transpose, int32_t ci0, int32_t n,
+                             int32_t ck, void *out, void *stream)
+{
+    if (!w || !out || cout < 1 || cin < 1 || n < 16 || n % 16 || (ck != 16 && ck != 32))
+        return fail(ART_ERR_INVALID_ARGUMENT, "pack_weights: bad arguments");
+    const int K = transpose ? cout : cin;
+    if (K % ck) return fail(ART_ERR_INVALID_ARGUMENT, "pack_weights: reduction size must be a multiple of ck");
+    const int total = n * 9 * K;
+    k_pack<<<blocks_for(total), 256, 0, static_cast<cudaStream_t>(stream)>>>(w, cout, cin, transpose, ci0, n, ck,
+                                                                             static_cast<bf16 *>(out));
+    return check_launch("k_pack");
+}
+
+int32_t art_cnn_pool2(const void *in, int32_t B, int32_t H, int32_t W, int32_t C, int32_t in_cstride,
+                      int32_t in_coff, void *out, void *stream)
+{
+    if (!in || !out || H % 2 || W % 2 || C % 8 || in_cstride % 8 || in_coff % 8 || in_coff + C > in_cstride)
+        return fail(ART_ERR_INVALID_ARGUMENT, "pool2: bad arguments");
+    const long long n = (long long)B * (H / 2) * (W / 2) * (C / 8);
+    k_pool2<<<blocks_for(n), 256, 0, static_cast<cudaStream_t>(stream)>>>(static_cast<const bf16 *>(in), B, H, W, C,
+                                                                          in_cstride, in_coff, static_cast<bf16 *>(out));
+    return check_launch("k_pool2");
+}
+
+int32_t art_cnn_upsample2(const void *in, int32_t B, int32_t H, int32_t W, int32_t C, void *out, int32_t out_cstride,
+                          int32_t out_coff, void *stream)
+{
+    if (!in || !out || H % 2 || W % 2 || C % 8 || out_cstride % 8 || out_coff % 8 || out_coff + C > out_cstride)
+        return fail(ART_ERR_INVALID_ARGUMENT, "upsample2: bad arguments");
+    const long long n = (long long)B * H * W * (C / 8);
+    k_upsample2<<<blocks_for(n), 256, 0, static_cast<cudaStream_t>(stream)>>>(
+        static_cast<const bf16 *>(in), B, H, W, C, static_cast<bf16 *>(out), out_cstride, out_coff);
+    return check_launch("k_upsample2");
+}
+
+int32_t art_cnn_downsum2_mask(const void *g, int32_t B, int32_t H, int32_t W, int32_t C, const void *act, void *out,
+                              void *stream)
+{
+    if (!g || !act || !out || H % 2 || W % 2 || C % 8) return fail(ART_ERR_INVALID_ARGUMENT, "downsum2_mask: bad arguments");
+    const long long n = (long long)B * (H / 2) * (W / 2) * (C / 8);
+    k_downsum2_mask<<<blocks_for(n), 256, 0, static_cast<cudaStream_t>(stream)>>>(
+        static_cast<const bf16 *>(g), B, H, W, C, static_cast<const bf16 *>(act), static_cast<bf16 *>(out));
+    return check_launch("k_downsum2_mask");
+}
+
+int32_t art_cnn_unpool_add_mask(void *g, const void *gp, int32_t B, int32_t H, int32_t W, int32_t C, const void *act,
+                                int32_t act_cstride, int32_t act_coff, void *stream)
+{
+    if (!g || !act || H % 2 || W % 2 || C % 8 || act_cstride % 8 || act_coff % 8 || act_coff + C > act_cstride)
+        return fail(ART_ERR_INVALID_ARGUMENT, "unpool_add_mask: bad arguments");
+    const long long n = (long long)B * H * W * (C / 8);
+    k_unpool_add_mask<<<blocks_for(n), 256, 0, static_cast<cudaStream_t>(stream)>>>(
+        static_cast<bf16 *>(g), static_cast<const bf16 *>(gp), B, H, W, C, static_cast<const bf16 *>(act), act_cstride,
+        act_coff);
+    return check_launch("k_unpool_add_mask");
+}
+
+int32_t art_cnn_bias_grad(const void *g, int64_t npix, int32_t C, float *workspace, int64_t workspace_bytes,
+                          float *out, int32_t accumulate, void *stream)
+{
+    if (!g || !workspace || !out || C < 1 || C > 256) return fail(ART_ERR_INVALID_ARGUMENT, "bias_grad: bad arguments");
+    int nblk = (int)std::min<long long>(2 * num_sms(), workspace_bytes / (4LL * C));
+    if (nblk < 1) return fail(ART_ERR_INVALID_ARGUMENT, "bias_grad: workspace too small");
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    k_colsum_partial<<<nblk, 256, 0, s>>>(static_cast<const bf16 *>(g), npix, C, workspace);
+    int32_t rc = check_launch("k_colsum_partial");
+    if (rc) return rc;
+    k_colsum_final<<<1, 256, 0, s>>>(workspace, nblk, C, out, accumulate);
+    return check_launch("k_colsum_final");
+}
+
+int32_t art_cnn_features(const int16_t *coef, int32_t cpitch, int64_t img_stride, const float *q, int32_t B,
+                         int32_t H, int32_t W, float *dec, void *feat, void *stream)
+{
+    if (!coef || !q || !dec || !feat || H % 8 || W % 8 || cpitch < W || cpitch % 8)
+        return fail(ART_ERR_INVALID_ARGUMENT, "features: bad arguments");
+    const long long n = (long long)B * (H / 8) * (W / 8);
+    k_features<<<blocks_for(n, 128), 128, 0, static_cast<cudaStream_t>(stream)>>>(coef, cpitch, img_stride, q, B, H, W,
+                                                                                dec, static_cast<bf16 *>(feat));
+    return check_launch("k_features");
+}
+
+int32_t art_cnn_residual(const float *r, int32_t rstride, const float *dec, const float *target, int64_t npix,
+                         float *pred, void *grad, float *loss_partial, int32_t loss_blocks, void *stream)
+{
+    if (!r || !dec || (target && (!grad || !loss_partial)) || loss_blocks < 1)
+        return fail(ART_ERR_INVALID_ARGUMENT, "residual: bad arguments");
+    k_residual<<<loss_blocks, 256, 0, static_cast<cudaStream_t>(stream)>>>(
+        r, rstride, dec, target, npix, npix > 0 ? 1.f / (float)npix : 0.f, pred, static_cast<bf16 *>(grad),
+        loss_partial);
+    return check_launch("k_residual");
+}
+
+int32_t art_cnn_adam(float *w, const float *g, float *m, float *v, int64_t n, float lr, float beta1, float beta2,
+                     float eps, int32_t step, void *stream)
+{
+    if (!w || !g || !m || !v || n < 0 || step < 1) return fail(ART_ERR_INVALID_ARGUMENT, "adam: bad arguments");
+    const float c1 = 1.f / (1.f - std::pow(beta1, (float)step)), c2 = 1.f / (1.f - std::pow(beta2, (float)step));
+    k_adam<<<blocks_for(n), 256, 0, static_cast<cudaStream_t>(stream)>>>(w, g, m, v, n, lr, beta1, beta2, eps, c1, c2);
+    return check_launch("k_adam");
+}
+
+}  // extern "C"
+
+// ---------------------------------------------------------------------------
+// The network: a 4-level encoder-decoder, one 3x3 convolution per level and
+// direction. Level l has H >> l rows. Encoder activations are written into
+// the first channels of the decoder's concatenation buffers (skip | upsampled):
+//   e1 = relu(conv(F, 16 -> 32))            -> cat1[0:32]     level 0
+//   e2 = relu(conv(pool(e1), 32 -> 64))     -> cat2[0:64]     level 1
+//   e3 = relu(conv(pool(e2), 64 -> 96))     -> cat3[0:96]     level 2
+//   e4 = relu(conv(pool(e3), 96 -> 128))                      level 3
+//   d3 = relu(conv(cat3 = [e3 | up(e4)], 224 -> 96))          level 2
+//   d2 = relu(conv(cat2 = [e2 | up(d3)], 160 -> 64))          level 1
+//   d1 = relu(conv(cat1 = [e1 | up(d2)], 96 -> 32))           level 0
+//   r  = conv(d1, 32 -> 16), channel 0 used; prediction = decoded + 16 r.
+namespace art {
+namespace cnn {
+
+struct LayerDef {
+    int cin, cout, level, relu, skip;  // skip: channels of cin that come from the encoder (decoder layers)
+};
+constexpr int NLAYER = 8;
+constexpr LayerDef LAYERS[NLAYER] = {
+    {16, 32, 0, 1, 0},   {32, 64, 1, 1, 0},  {64, 96, 2, 1, 0},  {96, 128, 3, 1, 0},
+    {224, 96, 2, 1, 96}, {160, 64, 1, 1, 64}, {96, 32, 0, 1, 32}, {32, 16, 0, 0, 0},
+};
+enum { E1, E2, E3, E4, D3, D2, D1, HEAD };
+
+inline int ck_for(int k) { return k % 32 == 0 ? 32 : 16; }
+
+long long param_count()
+{
+    long long n = 0;
+    for (const auto &l : LAYERS) n += (long long)l.cout * 9 * l.cin + l.cout;
+    return n;
+}
+
+struct Buf {
+    void *p = nullptr;
+    size_t n = 0;
+    bool ensure(size_t bytes)
+    {
+        if (bytes <= n) return true;
+        if (p) cudaFree(p);
+        p = nullptr;
+        n = 0;
+        if (cudaMalloc(&p, bytes) != cudaSuccess) {
+            p = nullptr;
+            return false;
+        }
+        n = bytes;
+        return true;
+    }
+    void release()
+    {
+        if (p) cudaFree(p);
+        p = nullptr;
+        n = 0;
+    }
+    template <class T>
+    T *as() const
+    {
+        return static_cast<T *>(p);
+    }
+};
+
+}  // namespace cnn
+}  // namespace art
+
+struct ArtNet {
+    int device = 0;
+    long long nparam = 0;
+    int step = 0;
+    size_t w_off[art::cnn::NLAYER], b_off[art::cnn::NLAYER];
+    art::cnn::Buf params, grads, adam_m, adam_v, errflag, workspace, loss_partial;
+    art::cnn::Buf wf[art::cnn::NLAYER];     // forward packs
+    art::cnn::Buf wb[art::cnn::NLAYER][2];  // backward-data packs (skip part, upsampled part or whole input)
+    bool packed = false;
+    // activations (forward) and gradients (training)
+    art::cnn::Buf feat, dec, cat1, cat2, cat3, p1, p2, p3, e4, d3, d2, d1, r, pred;
+    art::cnn::Buf dr, gd1, ge1, gup1, gd2, ge2, gup2, gd3, ge3, gup3, ge4, gp3, gp2, gp1;
+    long long cap_px = 0;  // level-0 pixels the buffers hold
+    bool cap_train = false;
+};
+
+namespace art {
+namespace cnn {
+
+constexpr int LOSS_BLOCKS = 296;
+constexpr size_t WORKSPACE_BYTES = 64ull << 20;
+
+int32_t net_alloc(ArtNet *net, long long px, bool train)
+{
+    if (px <= net->cap_px && (!train || net->cap_train)) return ART_OK;
+    px = std::max(px, net->cap_px);
+    train = train || net->cap_train;
+    const size_t P0 = (size_t)px, P1 = P0 / 4 + 64, P2 = P0 / 16 + 64, P3 = P0 / 64 + 64;
+    struct Req {
+        Buf *b;
+        size_t bytes;
+    };
+    std::vector<Req> req = {
+        {&net->feat, P0 * 16 * 2}, {&net->dec, P0 * 4},       {&net->cat1, P0 * 96 * 2}, {&net->cat2, P1 * 160 * 2},
+        {&net->cat3, P2 * 224 * 2}, {&net->p1, P1 * 32 * 2},   {&net->p2, P2 * 64 * 2},   {&net->p3, P3 * 96 * 2},
+        {&net->e4, P3 * 128 * 2},  {&net->d3, P2 * 96 * 2},   {&net->d2, P1 * 64 * 2},   {&net->d1, P0 * 32 * 2},
+        {&net->r, P0 * 16 * 4},    {&net->pred, P0 * 4},
+    };
+    if (train) {
+        std::vector<Req> t = {
+            {&net->dr, P0 * 16 * 2},  {&net->gd1, P0 * 32 * 2}, {&net->ge1, P0 * 32 * 2},  {&net->gup1, P0 * 64 * 2},
+            {&net->gd2, P1 * 64 * 2}, {&net->ge2, P1 * 64 * 2}, {&net->gup2, P1 * 96 * 2}, {&net->gd3, P2 * 96 * 2},
+            {&net->ge3, P2 * 96 * 2}, {&net->gup3, P2 * 128 * 2}, {&net->ge4, P3 * 128 * 2}, {&net->gp3, P3 * 96 * 2},
+            {&net->gp2, P2 * 64 * 2}, {&net->gp1, P1 * 32 * 2},
+        };
+        req.insert(req.end(), t.begin(), t.end());
+    }
+    for (auto &q : req)
+        if (!q.b->ensure(q.bytes)) return fail(ART_ERR_CUDA, "network buffers: cudaMalloc failed");
+    net->cap_px = px;
+    net->cap_train = train;
+    return ART_OK;
+}
+
+int32_t net_pack(ArtNet *net, bool backward, cudaStream_t s)
+{
+    const float *w = net->params.as<float>();
+    for (int i = 0; i < NLAYER; i++) {
+        const LayerDef &L = LAYERS[i];
+        const size_t fbytes = (size_t)L.cout * 9 * L.cin * 2;
+        if (!net->wf[i].ensure(fbytes)) return fail(ART_ERR_CUDA, "weight packs: cudaMalloc failed");
+        int32_t rc = art_cnn_pack_weights(w + net->w_off[i], L.cout, L.cin, 0, 0, L.cout, ck_for(L.cin), net->wf[i].p, s);
+        if (rc) return rc;
+        if (!backward || i == E1) continue;
+        // Backward-data packs: decoder layers in two parts (skip, upsampled), others whole.
+        const int parts = L.skip ? 2 : 1;
+        for (int k = 0; k < parts; k++) {
+            const int ci0 = k == 0 ? 0 : L.skip, n = L.skip ? (k == 0 ? L.skip : L.cin - L.skip) : L.cin;
+            if (!net->wb[i][k].ensure((size_t)n * 9 * L.cout * 2)) return fail(ART_ERR_CUDA, "weight packs: cudaMalloc failed");
+            rc = art_cnn_pack_weights(w + net->w_off[i], L.cout, L.cin, 1, ci0, n, ck_for(L.cout), net->wb[i][k].p, s);
+            if (rc) return rc;
+        }
+    }
+    net->packed = true;
+    return ART_OK;
+}
+
+int32_t conv(ArtNet *net, int layer, const void *x, int B, int H, int W, void *out, int cstride, int coff,
+             float *out_f32, cudaStream_t s)
+{
+    const LayerDef &L = LAYERS[layer];
+    ArtCnnConv d{};
+    d.B = B;
+    d.H = H;
+    d.W = W;
+    d.cin = L.cin;
+    d.ck = ck_for(L.cin);
+    d.n = L.cout;
+    d.n_store = L.cout;
+    d.x = x;
+    d.wpack = net->wf[layer].p;
+    d.bias = net->params.as<float>() + net->b_off[layer];
+    d.out = out;
+    d.out_cstride = cstride;
+    d.out_coff = coff;
+    d.out_f32 = out_f32;
+    d.f32_cstride = L.cout;
+    d.relu = L.relu;
+    d.err = net->errflag.as<int>();
+    return conv3x3(&d, s);
+}
+
+// Backward-data of `layer` (part k) from the gradient g of its
+// pre-activation output; writes n channels dense into out.
+int32_t dgrad(ArtNet *net, int layer, int k, const void *g, int B, int H, int W, void *out, const void *mask,
+              int mask_cstride, cudaStream_t s)
+{
+    const LayerDef &L = LAYERS[layer];
+    const int n = L.skip ? (k == 0 ? L.skip : L.cin - L.skip) : L.cin;
+    ArtCnnConv d{};
+    d.B = B;
+    d.H = H;
+    d.W = W;
+    d.cin = L.cout;
+    d.ck = ck_for(L.cout);
+    d.n = n;
+    d.n_store = n;
+    d.x = g;
+    d.wpack = net->wb[layer][k].p;
+    d.out = out;
+    d.out_cstride = n;
+    d.out_coff = 0;
+    d.mask = mask;
+    d.mask_cstride = mask_cstride;
+    d.err = net->errflag.as<int>();
+    return conv3x3(&d, s);
+}
+
+int32_t wgrad(ArtNet *net, int layer, const void *x, const void *g, int B, int H, int W, cudaStream_t s)
+{
+    const LayerDef &L = LAYERS[layer];
+    ArtCnnWgrad d{};
+    d.B = B;
+    d.H = H;
+    d.W = W;
+    d.cout = L.cout;
+    d.cin = L.cin;
+    d.dy = g;
+    d.x = x;
+    d.dw = net->grads.as<float>() + net->w_off[layer];
+    d.workspace = net->workspace.p;
+    d.workspace_bytes = (int64_t)net->workspace.n;
+    d.err = net->errflag.as<int>();
+    int32_t rc = wgrad3x3(&d, s);
+    if (rc) return rc;
+    return art_cnn_bias_grad(g, (int64_t)B * H * W, L.cout, net->workspace.as<float>(), (int64_t)net->workspace.n,
+                             net->grads.as<float>() + net->b_off[layer], 0, s);
+}
+
+#define NET_TRY(x)                \
+    do {                          \
+        const int32_t rc_ = (x);  \
+        if (rc_) return rc_;      \
+    } while (0)
+
+int32_t net_forward(ArtNet *net, int B, int H, int W, cudaStream_t s)
+{
+    const int H1 = H / 2, W1 = W / 2, H2 = H / 4, W2 = W / 4, H3 = H / 8, W3 = W / 8;
+    NET_TRY(conv(net, E1, net->feat.p, B, H, W, net->cat1.p, 96, 0, nullptr, s));
+    NET_TRY(art_cnn_pool2(net->cat1.p, B, H, W, 32, 96, 0, net->p1.p, s));
+    NET_TRY(conv(net, E2, net->p1.p, B, H1, W1, net->cat2.p, 160, 0, nullptr, s));
+    NET_TRY(art_cnn_pool2(net->cat2.p, B, H1, W1, 64, 160, 0, net->p2.p, s));
+    NET_TRY(conv(net, E3, net->p2.p, B, H2, W2, net->cat3.p, 224, 0, nullptr, s));
+    NET_TRY(art_cnn_pool2(net->cat3.p, B, H2, W2, 96, 224, 0, net->p3.p, s));
+    NET_TRY(conv(net, E4, net->p3.p, B, H3, W3, net->e4.p, 128, 0, nullptr, s));
+    NET_TRY(art_cnn_upsample2(net->e4.p, B, H2, W2, 128, net->cat3.p, 224, 96, s));
+    NET_TRY(conv(net, D3, net->cat3.p, B, H2, W2, net->d3.p, 96, 0, nullptr, s));
+    NET_TRY(art_cnn_upsample2(net->d3.p, B, H1, W1, 96, net->cat2.p, 160, 64, s));
+    NET_TRY(conv(net, D2, net->cat2.p, B, H1, W1, net->d2.p, 64, 0, nullptr, s));
+    NET_TRY(art_cnn_upsample2(net->d2.p, B, H, W, 64, net->cat1.p, 96, 32, s));
+    NET_TRY(conv(net, D1, net->cat1.p, B, H, W, net->d1.p, 32, 0, nullptr, s));
+    NET_TRY(conv(net, HEAD, net->d1.p, B, H, W, nullptr, 0, 0, net->r.as<float>(), s));
+    return ART_OK;
+}
+
+int32_t net_backward(ArtNet *net, int B, int H, int W, cudaStream_t s)
+{
+    const int H1 = H / 2, W1 = W / 2, H2 = H / 4, W2 = W / 4, H3 = H / 8, W3 = W / 8;
+    // head
+    NET_TRY(wgrad(net, HEAD, net->d1.p, net->dr.p, B, H, W, s));
+    NET_TRY(dgrad(net, HEAD, 0, net->dr.p, B, H, W, net->gd1.p, net->d1.p, 32, s));
+    // d1 (level 0): input cat1 = [e1 | up(d2)]
+    NET_TRY(wgrad(net, D1, net->cat1.p, net->gd1.p, B, H, W, s));
+    NET_TRY(dgrad(net, D1, 0, net->gd1.p, B, H, W, net->ge1.p, nullptr, 0, s));
+    NET_TRY(dgrad(net, D1, 1, net->gd1.p, B, H, W, net->gup1.p, nullptr, 0, s));
+    NET_TRY(art_cnn_downsum2_mask(net->gup1.p, B, H, W, 64, net->d2.p, net->gd2.p, s));
+    // d2 (level 1): input cat2 = [e2 | up(d3)]
+    NET_TRY(wgrad(net, D2, net->cat2.p, net->gd2.p, B, H1, W1, s));
+    NET_TRY(dgrad(net, D2, 0, net->gd2.p, B, H1, W1, net->ge2.p, nullptr, 0, s));
+    NET_TRY(dgrad(net, D2, 1, net->gd2.p, B, H1, W1, net->gup2.p, nullptr, 0, s));
+    NET_TRY(art_cnn_downsum2_mask(net->gup2.p, B, H1, W1, 96, net->d3.p, net->gd3.p, s));
+    // d3 (level 2): input cat3 = [e3 | up(e4)]
+    NET_TRY(wgrad(net, D3, net->cat3.p, net->gd3.p, B, H2, W2, s));
+    NET_TRY(dgrad(net, D3, 0, net->gd3.p, B, H2, W2, net->ge3.p, nullptr, 0, s));
+    NET_TRY(dgrad(net, D3, 1, net->gd3.p, B, H2, W2, net->gup3.p, nullptr, 0, s));
+    NET_TRY(art_cnn_downsum2_mask(net->gup3.p, B, H2, W2, 128, net->e4.p, net->ge4.p, s));
+    // e4 (level 3)
+    NET_TRY(wgrad(net, E4, net->p3.p, net->ge4.p, B, H3, W3, s));
+    NET_TRY(dgrad(net, E4, 0, net->ge4.p, B, H3, W3, net->gp3.p, nullptr, 0, s));
+    NET_TRY(art_cnn_unpool_add_mask(net->ge3.p, net->gp3.p, B, H2, W2, 96, net->cat3.p, 224, 0, s));
+    // e3 (level 2)
+    NET_TRY(wgrad(net, E3, net->p2.p, net->ge3.p, B, H2, W2, s));
+    NET_TRY(dgrad(net, E3, 0, net->ge3.p, B, H2, W2, net->gp2.p, nullptr, 0, s));
+    NET_TRY(art_cnn_unpool_add_mask(net->ge2.p, net->gp2.p, B, H1, W1, 64, net->cat2.p, 160, 0, s));
+    // e2 (level 1)
+    NET_TRY(wgrad(net, E2, net->p1.p, net->ge2.p, B, H1, W1, s));
+    NET_TRY(dgrad(net, E2, 0, net->ge2.p, B, H1, W1, net->gp1.p, nullptr, 0, s));
+    NET_TRY(art_cnn_unpool_add_mask(net->ge1.p, net->gp1.p, B, H, W, 32, net->cat1.p, 96, 0, s));
+    // e1 (level 0)
+    NET_TRY(wgrad(net, E1, net->feat.p, net->ge1.p, B, H, W, s));
+    return ART_OK;
+}
+
+int32_t check_geometry(int B, int H, int W)
+{
+    if (B < 1 || H < 8 || W < 8 || H % 8 || W % 8)
+        return fail(ART_ERR_INVALID_ARGUMENT, "network input must be at least 8x8 and a multiple of 8 on each side");
+    if ((long long)B * H * W > (1LL << 28)) return fail(ART_ERR_INVALID_ARGUMENT, "network input too large");
+    return ART_OK;
+}
+
+int32_t read_err(ArtNet *net, cudaStream_t s)
+{
+    int h = 0;
+    if (cudaMemcpyAsync(&h, net->errflag.p, sizeof(int), cudaMemcpyDeviceToHost, s) != cudaSuccess ||
+        cudaStreamSynchronize(s) != cudaSuccess)
+        return fail(ART_ERR_CUDA, std::string("network: ") + cudaGetErrorString(cudaGetLastError()));
+    if (h) return fail(ART_ERR_CUDA, "network: a tensor-core pipeline wait timed out");
+    return ART_OK;
+}
+
+// Features + forward for B coefficient images; prediction into pred (or the
+// net's own buffer when pred is null).
+int32_t net_predict(ArtNet *net, const int16_t *coef, int cpitch, long long img_stride, const float *q, int B, int H,
+                    int W, float *pred, cudaStream_t s)
+{
+    NET_TRY(check_geometry(B, H, W));
+    NET_TRY(net_alloc(net, (long long)B * H * W, false));
+    if (!net->packed) NET_TRY(net_pack(net, false, s));
+    NET_TRY(art_cnn_features(coef, cpitch, img_stride, q, B, H, W, net->dec.as<float>(), net->feat.p, s));
+    NET_TRY(net_forward(net, B, H, W, s));
+    return art_cnn_residual(net->r.as<float>(), 16, net->dec.as<float>(), nullptr, (int64_t)B * H * W,
+                            pred ? pred : net->pred.as<float>(), nullptr, nullptr, 1, s);
+}
+
+}  // namespace cnn
+}  // namespace art
+
+extern "C" {
+
+int64_t art_net_num_params(void) { return art::cnn::param_count(); }
+
+int32_t art_net_create(int32_t device, const float *params, int64_t nparams, ArtNet **out)
+{
+    using namespace art::cnn;
+    if (!out || !params) return fail(ART_ERR_INVALID_ARGUMENT, "net_create: null pointer");
+    *out = nullptr;
+    if (nparams != param_count()) return fail(ART_ERR_INVALID_ARGUMENT, "net_create: wrong parameter count");
+    for (int64_t i = 0; i < nparams; i++)
+        if (!std::isfinite(params[i])) return fail(ART_ERR_INVALID_DATA, "net_create: non-finite parameter");
+    if (device < 0 && cudaGetDevice(&device) != cudaSuccess) return fail(ART_ERR_CUDA, "net_create: no device");
+    if (cudaSetDevice(device) != cudaSuccess) return fail(ART_ERR_CUDA, "net_create: cudaSetDevice failed");
+    ArtNet *net = new ArtNet();
+    net->device = device;
+    net->nparam = nparams;
+    size_t off = 0;
+    for (int i = 0; i < NLAYER; i++) {
+        net->w_off[i] = off;
+        off += (size_t)LAYERS[i].cout * 9 * LAYERS[i].cin;
+        net->b_off[i] = off;
+        off += LAYERS[i].cout;
+    }
+    const size_t pb = (size_t)nparams * 4;
+    if (!net->params.ensure(pb) || !net->errflag.ensure(64) || !net->workspace.ensure(WORKSPACE_BYTES) ||
+        !net->loss_partial.ensure(LOSS_BLOCKS * 4) ||
+        cudaMemcpy(net->params.p, params, pb, cudaMemcpyHostToDevice) != cudaSuccess ||
+        cudaMemset(net->errflag.p, 0, 64) != cudaSuccess) {
+        art_net_destroy(net);
+        return fail(ART_ERR_CUDA, "net_create: device allocation failed");
+    }
+    *out = net;
+    return ART_OK;
+}
+
+void art_net_destroy(ArtNet *net)
+{
+    if (!net) return;
+    cudaSetDevice(net->device);
+    art::cnn::Buf *all[] = {&net->params, &net->grads, &net->adam_m, &net->adam_v, &net->errflag, &net->workspace,
+                            &net->loss_partial, &net->feat, &net->dec, &net->cat1, &net->cat2, &net->cat3, &net->p1,
+                            &net->p2, &net->p3, &net->e4, &net->d3, &net->d2, &net->d1, &net->r, &net->pred,
+                            &net->dr, &net->gd1, &net->ge1, &net->gup1, &net->gd2, &net->ge2, &net->gup2, &net->gd3,
+                            &net->ge3, &net->gup3, &net->ge4, &net->gp3, &net->gp2, &net->gp1};
+    for (auto *b : all) b->release();
+    for (int i = 0; i < art::cnn::NLAYER; i++) {
+        net->wf[i].release();
+        net->wb[i][0].release();
+        net->wb[i][1].release();
+    }
+    delete net;
+}
+
+int32_t art_net_params(ArtNet *net, float *host, int64_t n)
+{
+    if (!net || !host || n != net->nparam) return fail(ART_ERR_INVALID_ARGUMENT, "net_params: bad arguments");
+    cudaSetDevice(net->device);
+    if (cudaMemcpy(host, net->params.p, (size_t)n * 4, cudaMemcpyDeviceToHost) != cudaSuccess)
+        return fail(ART_ERR_CUDA, "net_params: copy failed");
+    return ART_OK;
+}
+
+int32_t art_net_gradients(ArtNet *net, float *host, int64_t n)
+{
+    if (!net || !host || n != net->nparam || !net->grads.p)
+        return fail(ART_ERR_INVALID_ARGUMENT, "net_gradients: no gradients yet");
+    cudaSetDevice(net->device);
+    if (cudaMemcpy(host, net->grads.p, (size_t)n * 4, cudaMemcpyDeviceToHost) != cudaSuccess)
+        return fail(ART_ERR_CUDA, "net_gradients: copy failed");
+    return ART_OK;
+}
+
+int32_t art_net_predict(ArtNet *net, const int16_t *coef, int32_t cpitch, int64_t img_stride, const float *q,
+                        int32_t B, int32_t H, int32_t W, float *pred, void *stream)
+{
+    using namespace art::cnn;
+    if (!net || !coef || !q || !pred) return fail(ART_ERR_INVALID_ARGUMENT, "net_predict: null pointer");
+    cudaSetDevice(net->device);
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    NET_TRY(net_predict(net, coef, cpitch, img_stride, q, B, H, W, pred, s));
+    return read_err(net, s);
+}
+
+int32_t art_net_train_step(ArtNet *net, const int16_t *coef, int32_t cpitch, int64_t img_stride, const float *q,
+                           const float *target, int32_t B, int32_t H, int32_t W, float lr, float *loss, void *stream)
+{
+    using namespace art::cnn;
+    if (!net || !coef || !q || !target) return fail(ART_ERR_INVALID_ARGUMENT, "net_train_step: null pointer");
+    cudaSetDevice(net->device);
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    NET_TRY(check_geometry(B, H, W));
+    NET_TRY(net_alloc(net, (long long)B * H * W, true));
+    const size_t pb = (size_t)net->nparam * 4;
+    if (!net->grads.p) {
+        if (!net->grads.ensure(pb) || !net->adam_m.ensure(pb) || !net->adam_v.ensure(pb) ||
+            cudaMemsetAsync(net->adam_m.p, 0, pb, s) != cudaSuccess || cudaMemsetAsync(net->adam_v.p, 0, pb, s) != cudaSuccess)
+            return fail(ART_ERR_CUDA, "net_train_step: allocation failed");
+    }
+    NET_TRY(net_pack(net, true, s));
+    NET_TRY(art_cnn_features(coef, cpitch, img_stride, q, B, H, W, net->dec.as<float>(), net->feat.p, s));
+    NET_TRY(net_forward(net, B, H, W, s));
+    const long long npix = (long long)B * H * W;
+    NET_TRY(art_cnn_residual(net->r.as<float>(), 16, net->dec.as<float>(), target, npix, net->pred.as<float>(),
+                             net->dr.p, net->loss_partial.as<float>(), LOSS_BLOCKS, s));
+    NET_TRY(net_backward(net, B, H, W, s));
+    if (lr > 0.f) {
+        net->step++;
+        NET_TRY(art_cnn_adam(net->params.as<float>(), net->grads.as<float>(), net->adam_m.as<float>(),
+                             net->adam_v.as<float>(), net->nparam, lr, 0.9f, 0.999f, 1e-8f, net->step, s));
+        net->packed = false;
+    }
+    if (loss) {
+        float h[LOSS_BLOCKS];
+        if (cudaMemcpyAsync(h, net->loss_partial.p, sizeof(h), cudaMemcpyDeviceToHost, s) != cudaSuccess)
+            return fail(ART_ERR_CUDA, "net_train_step: loss copy failed");
+        NET_TRY(read_err(net, s));
+        double t = 0;
+        for (int i = 0; i < LOSS_BLOCKS; i++) t += h[i];
+        *loss = (float)(t / (double)npix);
+        return ART_OK;
+    }
+    return read_err(net, s);
+}
+
+}  // extern "C"

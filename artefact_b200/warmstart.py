@@ -1,0 +1,156 @@
+"""Learned warm start for the restoration solver.
+
+A 4-level encoder-decoder CNN predicts, per channel, the converged solver
+output from the decoded channel and its quantisation table. Its forward and
+backward passes are the library's own sm_100a kernels (``art_net_*`` /
+``art_cnn_*`` in libartefact_b200.so: tcgen05 MMAs with TMEM accumulators,
+TMA-staged tiles); PyTorch only provides device memory and streams here.
+
+The solver uses a prediction as its starting point (``ART_INIT_LEARNED``):
+the prediction is projected onto the quantisation constraint set and refined
+by plain iterations, so the constraint and the objective stay the
+reference's. Training pairs come from the plain solver itself (targets: long
+plain runs of the same synthetic JPEGs).
+
+Weights file: 8-byte magic ``ARTWS001``, int64 parameter count, then that
+many little-endian float32 values (per layer e1, e2, e3, e4, d3, d2, d1,
+head: weights [cout][9][cin], then bias [cout]).
+"""
+from __future__ import annotations
+
+import ctypes as C
+from pathlib import Path
+from typing import Optional
+
+import numpy as np
+
+from . import _native as N
+
+MAGIC = b"ARTWS001"
+DEFAULT_WEIGHTS = Path(__file__).resolve().parent / "weights" / "warmstart.bin"
+LAYERS = [("e1", 16, 32), ("e2", 32, 64), ("e3", 64, 96), ("e4", 96, 128), ("d3", 224, 96), ("d2", 160, 64),
+          ("d1", 96, 32), ("head", 32, 16)]
+
+
+def num_params() -> int:
+    return int(N.lib().art_net_num_params())
+
+
+def init_params(seed: int = 0) -> np.ndarray:
+    """He-normal weights, zero biases; the head starts near zero (prediction =
+    decoded image) and only its first output channel is ever non-zero."""
+    rng = np.random.default_rng(seed)
+    out = []
+    for name, cin, cout in LAYERS:
+        std = np.sqrt(2.0 / (9 * cin))
+        w = rng.standard_normal((cout, 9, cin)) * std
+        if name == "head":
+            w[1:] = 0.0
+            w[0] *= 0.01
+        out += [w.ravel(), np.zeros(cout)]
+    p = np.concatenate(out).astype(np.float32)
+    assert p.size == num_params()
+    return p
+
+
+def save_params(path, params: np.ndarray) -> None:
+    path = Path(path)
+    path.parent.mkdir(parents=True, exist_ok=True)
+    p = np.ascontiguousarray(params, dtype="<f4")
+    with open(path, "wb") as f:
+        f.write(MAGIC)
+        f.write(np.int64(p.size).tobytes())
+        f.write(p.tobytes())
+
+
+def load_params(path=DEFAULT_WEIGHTS) -> np.ndarray:
+    data = Path(path).read_bytes()
+    if data[:8] != MAGIC:
+        raise ValueError(f"{path}: not a warm-start weights file")
+    n = int(np.frombuffer(data[8:16], "<i8")[0])
+    if n != num_params() or len(data) != 16 + 4 * n:
+        raise ValueError(f"{path}: expected {num_params()} parameters")
+    return np.frombuffer(data[16:], "<f4").copy()
+
+
+def coef_image(coef) -> np.ndarray:
+    """Block-raster coefficients of one component -> int16 coefficient image
+    (coefficient (v,u) of block (bx,by) at row 8by+v, column 8bx+u)."""
+    c = np.asarray(coef.dct_coefs)
+    if c.dtype != np.int16:
+        if not np.all(np.isfinite(c)) or np.any(c != np.rint(c)) or np.abs(c).max(initial=0) > 32767:
+            raise ValueError("coefficients must be integers in [-32768, 32767]")
+        c = c.astype(np.int16)
+    bh, bw = coef.block_h, coef.block_w
+    return np.ascontiguousarray(c.reshape(bh, bw, 8, 8).transpose(0, 2, 1, 3).reshape(bh * 8, bw * 8))
+
+
+def _ptr(t) -> C.c_void_p:
+    return C.c_void_p(t.data_ptr())
+
+
+def _stream(stream) -> C.c_void_p:
+    return C.c_void_p(stream.cuda_stream if stream is not None else 0)
+
+
+class WarmStartNet:
+    """The network on one GPU (``art_net_*``)."""
+
+    def __init__(self, params: Optional[np.ndarray] = None, device: int = 0):
+        p = init_params() if params is None else np.ascontiguousarray(params, dtype=np.float32)
+        h = C.c_void_p()
+        N.check(N.lib().art_net_create(device, p.ctypes.data, p.size, C.byref(h)))
+        self._h = h
+        self.device = device
+
+    @classmethod
+    def load(cls, path=DEFAULT_WEIGHTS, device: int = 0) -> "WarmStartNet":
+        return cls(load_params(path), device)
+
+    @property
+    def handle(self) -> C.c_void_p:
+        return self._h
+
+    def close(self) -> None:
+        if self._h:
+            N.lib().art_net_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def params(self) -> np.ndarray:
+        out = np.empty(num_params(), np.float32)
+        N.check(N.lib().art_net_params(self._h, out.ctypes.data, out.size))
+        return out
+
+    def gradients(self) -> np.ndarray:
+        out = np.empty(num_params(), np.float32)
+        N.check(N.lib().art_net_gradients(self._h, out.ctypes.data, out.size))
+        return out
+
+    def save(self, path) -> None:
+        save_params(path, self.params())
+
+    def train_step(self, coef, q, target, lr: float, stream=None) -> float:
+        """One step on a batch: coef int16 [B][H][W], q float32 [B][64] and
+        target float32 [B][H][W] CUDA tensors. Returns the mean loss."""
+        B, H, W = coef.shape
+        loss = C.c_float()
+        N.check(N.lib().art_net_train_step(self._h, _ptr(coef), W, H * W, _ptr(q), _ptr(target), B, H, W,
+                                           float(lr), C.byref(loss), _stream(stream)))
+        return float(loss.value)
+
+    def predict(self, coef, q, out=None, stream=None):
+        """Prediction float32 [B][H][W] (a CUDA tensor) for coef int16 [B][H][W]."""
+        import torch
+
+        B, H, W = coef.shape
+        if out is None:
+            out = torch.empty((B, H, W), dtype=torch.float32, device=coef.device)
+        N.check(N.lib().art_net_predict(self._h, _ptr(coef), W, H * W, _ptr(q), B, H, W, _ptr(out),
+                                        _stream(stream)))
+        return out

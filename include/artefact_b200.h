@@ -210,6 +210,117 @@ int32_t art_jpeg_info(const ArtJpeg *jpeg, uint32_t *nchannel, uint32_t *real_px
 /* Fill `out` with component c; pointers stay valid until art_jpeg_free. coef_type is ART_COEF_I16. */
 int32_t art_jpeg_channel(const ArtJpeg *jpeg, uint32_t c, ArtChannel *out);
 
+
+/* ------------------------------------------------------------------------
+ * Warm-start network kernels (no counterpart in the reference: the network
+ * only chooses the solver's starting point). All pointers are device
+ * pointers; tensors are NHWC bf16 ([B][H][W][C], channels innermost) unless
+ * stated; `stream` is a cudaStream_t (NULL = legacy default stream). `err`
+ * is a device int that a kernel sets to 1 if one of its bounded waits gave up.
+ * ------------------------------------------------------------------------ */
+
+/* 3x3 convolution, stride 1, zero padding 1, BF16 x BF16 -> FP32 on the
+ * tensor cores: out[p][n] = sum_{tap, c} x[p + d(tap)][c] * W[n][tap][c]
+ * (+ bias, ReLU, zeroed where mask <= 0, + the previous output when
+ * accumulate), stored as bf16 into channels [out_coff, out_coff + n_store) of
+ * a tensor with out_cstride channels and/or as fp32 with f32_cstride.
+ * wpack holds the weights as art_cnn_pack_weights lays them out for this ck
+ * and n. cin is a multiple of ck (16 or 32); n, n_store multiples of 16,
+ * n <= 128. */
+typedef struct ArtCnnConv {
+    int32_t B, H, W;
+    int32_t cin, ck, n, n_store;
+    const void *x;
+    const void *wpack;
+    const float *bias;
+    void *out;
+    int32_t out_cstride, out_coff;
+    float *out_f32;
+    int32_t f32_cstride;
+    const void *mask;
+    int32_t mask_cstride;
+    int32_t relu, accumulate;
+    int32_t *err;
+} ArtCnnConv;
+int32_t art_cnn_conv3x3(const ArtCnnConv *desc, void *stream);
+
+/* Weight gradient of a 3x3 convolution: dw[n][tap][c] (+)= sum_p dy[p][n] *
+ * x[p + d(tap)][c], fp32 [cout][9][cin]. cout a multiple of 8 up to 128, cin
+ * a multiple of 16. `workspace` holds per-band partial sums (reduced in a
+ * fixed order, so results are deterministic); a few MB suffice. */
+typedef struct ArtCnnWgrad {
+    int32_t B, H, W, cout, cin;
+    const void *dy;
+    const void *x;
+    float *dw;
+    int32_t accumulate;
+    void *workspace;
+    int64_t workspace_bytes;
+    int32_t *err;
+} ArtCnnWgrad;
+int32_t art_cnn_wgrad3x3(const ArtCnnWgrad *desc, void *stream);
+
+/* Pack fp32 weights w[cout][9][cin] into the bf16 stage layout of
+ * art_cnn_conv3x3 ([cin/ck][9][ck/8][n][8]). transpose != 0 packs the
+ * backward-data weights of input channels [ci0, ci0 + n) (taps mirrored,
+ * reduction over cout). */
+int32_t art_cnn_pack_weights(const float *w, int32_t cout, int32_t cin, int32_t transpose, int32_t ci0, int32_t n,
+                             int32_t ck, void *out, void *stream);
+/* 2x2 average pooling of channels [in_coff, in_coff + C) of [B][H][W][in_cstride] -> [B][H/2][W/2][C]. */
+int32_t art_cnn_pool2(const void *in, int32_t B, int32_t H, int32_t W, int32_t C, int32_t in_cstride,
+                      int32_t in_coff, void *out, void *stream);
+/* Nearest 2x upsampling of [B][H/2][W/2][C] into channels [out_coff, +C) of [B][H][W][out_cstride]. */
+int32_t art_cnn_upsample2(const void *in, int32_t B, int32_t H, int32_t W, int32_t C, void *out, int32_t out_cstride,
+                          int32_t out_coff, void *stream);
+/* out[B][H/2][W/2][C] = (2x2 sums of g[B][H][W][C]) * (act > 0). */
+int32_t art_cnn_downsum2_mask(const void *g, int32_t B, int32_t H, int32_t W, int32_t C, const void *act, void *out,
+                              void *stream);
+/* In place: g = (g + gp[upsampled] / 4) * (act > 0); gp ([B][H/2][W/2][C]) may be NULL; act is channels
+ * [act_coff, act_coff + C) of a tensor with act_cstride channels. */
+int32_t art_cnn_unpool_add_mask(void *g, const void *gp, int32_t B, int32_t H, int32_t W, int32_t C, const void *act,
+                                int32_t act_cstride, int32_t act_coff, void *stream);
+/* out[c] (+)= sum over npix pixels of g[p][c] (bf16), fixed reduction order. */
+int32_t art_cnn_bias_grad(const void *g, int64_t npix, int32_t C, float *workspace, int64_t workspace_bytes,
+                          float *out, int32_t accumulate, void *stream);
+/* Network input from B int16 coefficient images (rows of cpitch, images
+ * img_stride elements apart, coefficient (v,u) of block (bx,by) at
+ * (8by+v, 8bx+u)) and B quantisation tables q[B][64]: dec = IDCT(c q) per
+ * block (fp32 [B][H][W]) and feat[B][H][W][16] = (dec / 128, q / 64, 0...). */
+int32_t art_cnn_features(const int16_t *coef, int32_t cpitch, int64_t img_stride, const float *q, int32_t B,
+                         int32_t H, int32_t W, float *dec, void *feat, void *stream);
+/* Prediction pred = dec + 16 r (r = channel 0 of rows of rstride floats);
+ * with a target, the mean-squared-error gradient into grad[p][16] (channel 0)
+ * and loss_blocks partial sums of the squared error in units of 16 levels. */
+int32_t art_cnn_residual(const float *r, int32_t rstride, const float *dec, const float *target, int64_t npix,
+                         float *pred, void *grad, float *loss_partial, int32_t loss_blocks, void *stream);
+/* One Adam step on n fp32 parameters (step counts from 1). */
+int32_t art_cnn_adam(float *w, const float *g, float *m, float *v, int64_t n, float lr, float beta1, float beta2,
+                     float eps, int32_t step, void *stream);
+
+
+/* The warm-start network as a whole (4-level encoder-decoder, 3x3 convs,
+ * 32/64/96/128 channels, BF16 weights and activations, FP32 accumulation and
+ * master weights). Parameters are one fp32 array of art_net_num_params()
+ * values: per layer (e1, e2, e3, e4, d3, d2, d1, head) the weights
+ * [cout][9][cin] then the bias [cout]. Inputs are B int16 coefficient images
+ * of H x W (multiples of 8; rows of cpitch elements, images img_stride
+ * elements apart) with their quantisation tables q[B][64], all on the device. */
+typedef struct ArtNet ArtNet;
+int64_t art_net_num_params(void);
+int32_t art_net_create(int32_t device, const float *params_host, int64_t nparams, ArtNet **out);
+void art_net_destroy(ArtNet *net);
+/* Copy the current parameters / the last step's gradients to the host. */
+int32_t art_net_params(ArtNet *net, float *host, int64_t n);
+int32_t art_net_gradients(ArtNet *net, float *host, int64_t n);
+/* Warm start: pred[B][H][W] (fp32, level-shifted samples) = decoded + 16 * residual. */
+int32_t art_net_predict(ArtNet *net, const int16_t *coef, int32_t cpitch, int64_t img_stride, const float *q,
+                        int32_t B, int32_t H, int32_t W, float *pred, void *stream);
+/* One training step on the mean squared error against target[B][H][W]
+ * (in units of 16 levels): forward, backward, then Adam with learning rate
+ * lr (lr <= 0: gradients only). *loss (may be NULL) receives the mean loss. */
+int32_t art_net_train_step(ArtNet *net, const int16_t *coef, int32_t cpitch, int64_t img_stride, const float *q,
+                           const float *target, int32_t B, int32_t H, int32_t W, float lr, float *loss, void *stream);
+
 #ifdef __cplusplus
 }
 #endif

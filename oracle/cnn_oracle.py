@@ -1,0 +1,209 @@
+"""CPU FP64 oracle of the warm-start network (test infrastructure only).
+
+The network has no counterpart in the reference (it only chooses where the
+solver starts); this module is the checker for the project's tensor-core
+forward and backward kernels. Only tests import it.
+
+It restates the network independently of the CUDA code:
+
+  e1 = relu(conv(F, 16 -> 32))                       level 0
+  e2 = relu(conv(pool(e1), 32 -> 64))                level 1
+  e3 = relu(conv(pool(e2), 64 -> 96))                level 2
+  e4 = relu(conv(pool(e3), 96 -> 128))               level 3
+  d3 = relu(conv([e3 | up(e4)], 224 -> 96))         level 2
+  d2 = relu(conv([e2 | up(d3)], 160 -> 64))         level 1
+  d1 = relu(conv([e1 | up(d2)], 96 -> 32))          level 0
+  r  = conv(d1, 32 -> 16)[..., 0]
+  prediction = decoded + 16 r, loss = mean((r - (target - decoded) / 16)^2)
+
+conv = 3x3, stride 1, zero padding 1, weights W[cout][tap = 3 (dy+1) + (dx+1)][cin];
+pool = 2x2 mean; up = nearest 2x. F = (decoded / 128, q / 64, 0 x 14) with q
+the quantisation step of each sample's frequency position.
+
+With ``bf16=True`` every tensor the GPU stores in bf16 is rounded to bf16
+(round to nearest even) at the same point, so the only remaining difference
+from the GPU is the order of its fp32 accumulations.
+"""
+from __future__ import annotations
+
+import numpy as np
+
+LAYERS = [  # name, cin, cout, relu, skip channels
+    ("e1", 16, 32, True, 0), ("e2", 32, 64, True, 0), ("e3", 64, 96, True, 0), ("e4", 96, 128, True, 0),
+    ("d3", 224, 96, True, 96), ("d2", 160, 64, True, 64), ("d1", 96, 32, True, 32), ("head", 32, 16, False, 0),
+]
+
+
+def offsets():
+    """(name -> (weight offset, bias offset)) in the flat parameter array."""
+    off, out = 0, {}
+    for name, cin, cout, _, _ in LAYERS:
+        out[name] = (off, off + cout * 9 * cin)
+        off += cout * 9 * cin + cout
+    return out, off
+
+
+def unpack(params):
+    offs, total = offsets()
+    assert params.size == total
+    res = {}
+    for name, cin, cout, _, _ in LAYERS:
+        wo, bo = offs[name]
+        res[name] = (params[wo:wo + cout * 9 * cin].reshape(cout, 9, cin).astype(np.float64),
+                     params[bo:bo + cout].astype(np.float64))
+    return res
+
+
+def bf16(x):
+    """Round to bfloat16 (nearest even) and return as float64."""
+    f = np.ascontiguousarray(x, dtype=np.float32)
+    u = f.view(np.uint32).astype(np.uint64)
+    u = ((u + ((u >> 16) & 1) + 0x7FFF) >> 16) << 16
+    return u.astype(np.uint32).view(np.float32).astype(np.float64)
+
+
+def _shifted(x, dy, dx):
+    """x[b, y + dy, x + dx, c] with zeros outside."""
+    B, H, W, C = x.shape
+    p = np.zeros((B, H + 2, W + 2, C), np.float64)
+    p[:, 1:H + 1, 1:W + 1] = x
+    return p[:, 1 + dy:1 + dy + H, 1 + dx:1 + dx + W]
+
+
+def conv(x, w, b=None):
+    out = 0.0
+    for tap in range(9):
+        out = out + np.einsum("bhwc,oc->bhwo", _shifted(x, tap // 3 - 1, tap % 3 - 1), w[:, tap, :], optimize=True)
+    return out if b is None else out + b
+
+
+def conv_dgrad(g, w):
+    """Gradient with respect to the input of conv(x, w) given the output gradient g."""
+    wt = np.transpose(w[:, ::-1, :], (2, 1, 0))  # [cin][tap'][cout] = w[cout][8 - tap'][cin]
+    return conv(g, wt)
+
+
+def conv_wgrad(x, g):
+    cout, cin = g.shape[-1], x.shape[-1]
+    dw = np.zeros((cout, 9, cin))
+    for tap in range(9):
+        dw[:, tap, :] = np.einsum("bhwo,bhwc->oc", g, _shifted(x, tap // 3 - 1, tap % 3 - 1), optimize=True)
+    return dw
+
+
+def pool(x):
+    B, H, W, C = x.shape
+    return x.reshape(B, H // 2, 2, W // 2, 2, C).mean(axis=(2, 4))
+
+
+def up(x):
+    return x.repeat(2, axis=1).repeat(2, axis=2)
+
+
+def downsum(g):
+    B, H, W, C = g.shape
+    return g.reshape(B, H // 2, 2, W // 2, 2, C).sum(axis=(2, 4))
+
+
+def _dct_matrix():
+    k = np.arange(8)
+    m = np.sqrt(2 / 8) * np.cos(np.pi * (2 * k[None, :] + 1) * k[:, None] / 16)
+    m[0] /= np.sqrt(2)
+    return m  # m[u][x]
+
+
+def features(coef_img, q):
+    """coef_img [B][H][W] (coefficient (v,u) of block (bx,by) at (8by+v, 8bx+u)), q [B][64].
+    Returns decoded [B][H][W] (fp64) and F [B][H][W][16]."""
+    m = _dct_matrix()
+    B, H, W = coef_img.shape
+    c = coef_img.reshape(B, H // 8, 8, W // 8, 8).transpose(0, 1, 3, 2, 4).astype(np.float64)
+    qq = q.reshape(B, 1, 1, 8, 8).astype(np.float64)
+    blocks = np.einsum("vy,bijvu,ux->bijyx", m, c * qq, m)
+    dec = blocks.transpose(0, 1, 3, 2, 4).reshape(B, H, W)
+    qt = np.tile(q.reshape(B, 8, 8), (1, H // 8, W // 8)).astype(np.float64)
+    F = np.zeros((B, H, W, 16))
+    F[..., 0] = dec / 128.0
+    F[..., 1] = qt / 64.0
+    return dec, F
+
+
+def forward(params, F, dec, target=None, bf=True):
+    """Activations (dict), prediction and, with a target, the loss."""
+    rnd = bf16 if bf else (lambda a: np.asarray(a, np.float64))
+    P = unpack(params)
+    Wq = {k: (rnd(w), b) for k, (w, b) in P.items()}
+    a = {"F": rnd(F)}
+    relu = lambda v: np.maximum(v, 0.0)
+    a["e1"] = rnd(relu(conv(a["F"], *Wq["e1"])))
+    a["p1"] = rnd(pool(a["e1"]))
+    a["e2"] = rnd(relu(conv(a["p1"], *Wq["e2"])))
+    a["p2"] = rnd(pool(a["e2"]))
+    a["e3"] = rnd(relu(conv(a["p2"], *Wq["e3"])))
+    a["p3"] = rnd(pool(a["e3"]))
+    a["e4"] = rnd(relu(conv(a["p3"], *Wq["e4"])))
+    a["cat3"] = np.concatenate([a["e3"], up(a["e4"])], axis=-1)
+    a["d3"] = rnd(relu(conv(a["cat3"], *Wq["d3"])))
+    a["cat2"] = np.concatenate([a["e2"], up(a["d3"])], axis=-1)
+    a["d2"] = rnd(relu(conv(a["cat2"], *Wq["d2"])))
+    a["cat1"] = np.concatenate([a["e1"], up(a["d2"])], axis=-1)
+    a["d1"] = rnd(relu(conv(a["cat1"], *Wq["d1"])))
+    r = conv(a["d1"], *Wq["head"])
+    if bf:
+        r = r.astype(np.float32).astype(np.float64)
+    a["r"] = r
+    pred = dec + 16.0 * r[..., 0]
+    loss = None
+    if target is not None:
+        e = r[..., 0] - (target - dec) / 16.0
+        loss = float(np.mean(e * e))
+        a["e"] = e
+    return a, pred, loss, Wq
+
+
+def gradients(params, F, dec, target, bf=True):
+    """Loss and d loss / d params (flat, same layout as params)."""
+    rnd = bf16 if bf else (lambda v: np.asarray(v, np.float64))
+    a, _, loss, Wq = forward(params, F, dec, target, bf)
+    npix = dec.size
+    mask = lambda g, act: g * (act > 0)
+    dr = np.zeros(a["r"].shape)
+    dr[..., 0] = 2.0 * a["e"] / npix
+    if bf:
+        dr[..., 0] = bf16(dr[..., 0].astype(np.float32))
+    grads = {}
+
+    def wb(name, x, g):
+        grads[name] = (conv_wgrad(x, g), g.sum(axis=(0, 1, 2)))
+
+    wb("head", a["d1"], dr)
+    gd1 = rnd(mask(conv_dgrad(dr, Wq["head"][0]), a["d1"]))
+    wb("d1", a["cat1"], gd1)
+    w = Wq["d1"][0]
+    ge1 = rnd(conv_dgrad(gd1, w[:, :, :32]))
+    gd2 = rnd(mask(downsum(rnd(conv_dgrad(gd1, w[:, :, 32:]))), a["d2"]))
+    wb("d2", a["cat2"], gd2)
+    w = Wq["d2"][0]
+    ge2 = rnd(conv_dgrad(gd2, w[:, :, :64]))
+    gd3 = rnd(mask(downsum(rnd(conv_dgrad(gd2, w[:, :, 64:]))), a["d3"]))
+    wb("d3", a["cat3"], gd3)
+    w = Wq["d3"][0]
+    ge3 = rnd(conv_dgrad(gd3, w[:, :, :96]))
+    ge4 = rnd(mask(downsum(rnd(conv_dgrad(gd3, w[:, :, 96:]))), a["e4"]))
+    wb("e4", a["p3"], ge4)
+    gp3 = rnd(conv_dgrad(ge4, Wq["e4"][0]))
+    ge3 = rnd(mask(ge3 + 0.25 * up(gp3), a["e3"]))
+    wb("e3", a["p2"], ge3)
+    gp2 = rnd(conv_dgrad(ge3, Wq["e3"][0]))
+    ge2 = rnd(mask(ge2 + 0.25 * up(gp2), a["e2"]))
+    wb("e2", a["p1"], ge2)
+    gp1 = rnd(conv_dgrad(ge2, Wq["e2"][0]))
+    ge1 = rnd(mask(ge1 + 0.25 * up(gp1), a["e1"]))
+    wb("e1", a["F"], ge1)
+    offs, total = offsets()
+    flat = np.zeros(total)
+    for name, cin, cout, _, _ in LAYERS:
+        wo, bo = offs[name]
+        flat[wo:wo + cout * 9 * cin] = grads[name][0].ravel()
+        flat[bo:bo + cout] = grads[name][1]
+    return loss, flat

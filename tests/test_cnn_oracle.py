@@ -1,0 +1,71 @@
+"""The warm-start network's CPU FP64 oracle against finite differences (CPU)."""
+import sys
+from pathlib import Path
+
+import numpy as np
+
+sys.path.insert(0, str(Path(__file__).resolve().parent.parent / "oracle"))
+import cnn_oracle as O  # noqa: E402
+
+
+def _case(seed, B=1, H=16, W=16):
+    rng = np.random.default_rng(seed)
+    _, total = O.offsets()
+    params = np.zeros(total)
+    offs, _ = O.offsets()
+    for name, cin, cout, _, _ in O.LAYERS:
+        wo, bo = offs[name]
+        params[wo:wo + cout * 9 * cin] = rng.standard_normal(cout * 9 * cin) * np.sqrt(2.0 / (9 * cin))
+        params[bo:bo + cout] = rng.standard_normal(cout) * 0.05
+    coef = rng.integers(-20, 20, size=(B, H, W)).astype(np.int16)
+    q = rng.integers(2, 40, size=(B, 64)).astype(np.float64)
+    dec, F = O.features(coef, q)
+    target = dec + rng.standard_normal(dec.shape) * 4.0
+    return params, F, dec, target
+
+
+def test_features_decode_dc_block():
+    coef = np.zeros((1, 8, 8), np.int16)
+    coef[0, 0, 0] = 4
+    q = np.full((1, 64), 2.0)
+    dec, F = O.features(coef, q)
+    np.testing.assert_allclose(dec, 1.0, atol=1e-12)  # DC 8 / 8 (orthonormal 2-D DCT)
+    np.testing.assert_allclose(F[..., 1], 2.0 / 64.0)
+    assert np.all(F[..., 2:] == 0)
+
+
+def test_gradients_match_finite_differences():
+    """Central differences with a step small enough that no ReLU changes side."""
+    params, F, dec, target = _case(1)
+    loss, g = O.gradients(params, F, dec, target, bf=False)
+    rng = np.random.default_rng(7)
+    for _ in range(3):
+        v = rng.standard_normal(params.size)
+        eps = 1e-8
+        lp = O.forward(params + eps * v, F, dec, target, bf=False)[2]
+        lm = O.forward(params - eps * v, F, dec, target, bf=False)[2]
+        fd = (lp - lm) / (2 * eps)
+        assert abs(fd - g @ v) <= 1e-5 * max(1.0, abs(fd)), (fd, g @ v)
+
+
+def test_layer_gradients_match_finite_differences():
+    """Per layer, so that a wrong slice (skip vs upsampled channels) cannot hide."""
+    params, F, dec, target = _case(2, H=24, W=16)
+    _, g = O.gradients(params, F, dec, target, bf=False)
+    offs, _ = O.offsets()
+    rng = np.random.default_rng(3)
+    for name, cin, cout, _, _ in O.LAYERS:
+        wo, bo = offs[name]
+        for lo, hi in ((wo, wo + cout * 9 * cin), (bo, bo + cout)):
+            v = np.zeros(params.size)
+            v[lo:hi] = rng.standard_normal(hi - lo)
+            eps = 1e-8
+            fd = (O.forward(params + eps * v, F, dec, target, bf=False)[2] -
+                  O.forward(params - eps * v, F, dec, target, bf=False)[2]) / (2 * eps)
+            assert abs(fd - g @ v) <= 1e-5 * max(1e-3, abs(fd)), (name, fd, g @ v)
+
+
+def test_bf16_rounding_is_nearest_even():
+    x = np.array([1.0, 1.0 + 2 ** -8, 1.0 + 3 * 2 ** -8, -2.5, 0.0], np.float64)
+    r = O.bf16(x)
+    assert r[0] == 1.0 and r[1] == 1.0 and r[2] == 1.0 + 2 ** -6 and r[3] == -2.5 and r[4] == 0.0

@@ -1,0 +1,245 @@
+"""Tensor-core kernels of the warm-start network against the CPU FP64 oracle (GPU).
+
+The oracle rounds to bf16 wherever the GPU stores bf16, so forward values
+agree up to the GPU's fp32 accumulation order (a rare flip of one bf16 ulp,
+2^-8 relative); weight gradients are fp32 sums of exact bf16 products.
+"""
+import ctypes as C
+import sys
+from pathlib import Path
+
+import numpy as np
+import pytest
+
+sys.path.insert(0, str(Path(__file__).resolve().parent.parent / "oracle"))
+import cnn_oracle as O  # noqa: E402
+
+from artefact_b200 import _native as N  # noqa: E402
+from artefact_b200 import warmstart as WS  # noqa: E402
+
+pytestmark = pytest.mark.gpu
+
+
+def _torch():
+    import torch
+
+    return torch
+
+
+def _bf(a):
+    torch = _torch()
+    return torch.from_numpy(np.ascontiguousarray(a, np.float32)).to(torch.bfloat16).cuda()
+
+
+def _f32(a):
+    torch = _torch()
+    return torch.from_numpy(np.ascontiguousarray(a, np.float32)).cuda()
+
+
+def _np(t):
+    return t.float().cpu().numpy().astype(np.float64)
+
+
+def _ptr(t):
+    return C.c_void_p(t.data_ptr()) if t is not None else None
+
+
+def _pack(w, transpose=0, ci0=0, n=None, ck=32):
+    torch = _torch()
+    cout, _, cin = w.shape
+    n = n if n is not None else (cin if transpose else cout)
+    K = cout if transpose else cin
+    out = torch.empty(n * 9 * K, dtype=torch.bfloat16, device="cuda")
+    wt = _f32(w)
+    N.check(N.lib().art_cnn_pack_weights(_ptr(wt), cout, cin, transpose, ci0, n, ck, _ptr(out), None))
+    return out
+
+
+def _conv(x, wpack, cin, ck, n, bias=None, relu=0, mask=None, out=None, out_cstride=None, out_coff=0, f32=None,
+          accumulate=0):
+    torch = _torch()
+    B, H, W, _ = x.shape
+    err = torch.zeros(1, dtype=torch.int32, device="cuda")
+    if out is None and f32 is None:
+        out = torch.zeros((B, H, W, n), dtype=torch.bfloat16, device="cuda")
+    d = N.ArtCnnConv()
+    d.B, d.H, d.W, d.cin, d.ck, d.n, d.n_store = B, H, W, cin, ck, n, n
+    d.x, d.wpack = x.data_ptr(), wpack.data_ptr()
+    d.bias = bias.data_ptr() if bias is not None else None
+    d.out = out.data_ptr() if out is not None else None
+    d.out_cstride = out_cstride if out_cstride is not None else n
+    d.out_coff = out_coff
+    d.out_f32 = f32.data_ptr() if f32 is not None else None
+    d.f32_cstride = n
+    d.mask = mask.data_ptr() if mask is not None else None
+    d.mask_cstride = mask.shape[-1] if mask is not None else 0
+    d.relu, d.accumulate = relu, accumulate
+    d.err = err.data_ptr()
+    N.check(N.lib().art_cnn_conv3x3(C.byref(d), None))
+    torch.cuda.synchronize()
+    assert int(err.item()) == 0, "a pipeline wait timed out"
+    return out
+
+
+def _close(got, ref, rel=1.2e-2):
+    scale = max(float(np.abs(ref).max()), 1e-6)
+    err = float(np.abs(got - ref).max())
+    assert err <= rel * scale, f"max err {err:.3g} vs scale {scale:.3g}"
+    # Mean error well below one bf16 ulp: only rare rounding flips.
+    assert float(np.abs(got - ref).mean()) <= 1e-3 * scale
+
+
+@pytest.mark.parametrize("B,H,W,cin,cout", [(1, 8, 128, 16, 16), (2, 10, 200, 32, 64), (1, 6, 40, 64, 96),
+                                            (1, 4, 260, 224, 96), (2, 16, 96, 96, 128), (1, 3, 130, 160, 32)])
+def test_conv_forward(gpu, B, H, W, cin, cout):
+    rng = np.random.default_rng(cin * 7 + cout)
+    x = O.bf16(rng.standard_normal((B, H, W, cin)))
+    w = O.bf16(rng.standard_normal((cout, 9, cin)) * np.sqrt(2 / (9 * cin)))
+    b = rng.standard_normal(cout) * 0.1
+    ck = 32 if cin % 32 == 0 else 16
+    got = _np(_conv(_bf(x), _pack(w, ck=ck), cin, ck, cout, bias=_f32(b), relu=1))
+    ref = O.bf16(np.maximum(O.conv(x, w, b), 0))
+    _close(got, ref)
+
+
+def test_conv_channel_offset_accumulate_and_f32(gpu):
+    torch = _torch()
+    rng = np.random.default_rng(5)
+    B, H, W, cin, cout = 1, 6, 150, 32, 32
+    x = O.bf16(rng.standard_normal((B, H, W, cin)))
+    w = O.bf16(rng.standard_normal((cout, 9, cin)) * 0.1)
+    wp = _pack(w)
+    base = O.bf16(rng.standard_normal((B, H, W, 96)))
+    out = _bf(base)
+    _conv(_bf(x), wp, cin, 32, cout, out=out, out_cstride=96, out_coff=32, accumulate=1)
+    got = _np(out)
+    ref = base.copy()
+    ref[..., 32:64] = O.bf16(base[..., 32:64] + O.conv(x, w))
+    assert np.array_equal(got[..., :32], base[..., :32]) and np.array_equal(got[..., 64:], base[..., 64:])
+    _close(got[..., 32:64], ref[..., 32:64])
+    f = torch.zeros((B, H, W, cout), dtype=torch.float32, device="cuda")
+    _conv(_bf(x), wp, cin, 32, cout, f32=f)
+    np.testing.assert_allclose(_np(f), O.conv(x, w), rtol=1e-4, atol=1e-4 * float(np.abs(O.conv(x, w)).max()))
+
+
+def test_conv_backward_data_with_mask(gpu):
+    rng = np.random.default_rng(9)
+    B, H, W, cin, cout = 2, 8, 136, 96, 64
+    g = O.bf16(rng.standard_normal((B, H, W, cout)))
+    w = O.bf16(rng.standard_normal((cout, 9, cin)) * 0.1)
+    act = O.bf16(rng.standard_normal((B, H, W, 32)))
+    # Input channels 64..95 only, masked by act > 0.
+    got = _np(_conv(_bf(g), _pack(w, transpose=1, ci0=64, n=32), cout, 32, 32, mask=_bf(act)))
+    ref = O.bf16(O.conv_dgrad(g, w)[..., 64:96] * (act > 0))
+    _close(got, ref)
+
+
+@pytest.mark.parametrize("B,H,W,cin,cout", [(1, 8, 128, 16, 32), (2, 6, 70, 224, 96), (1, 10, 300, 32, 128),
+                                            (3, 4, 40, 64, 16)])
+def test_conv_weight_gradient(gpu, B, H, W, cin, cout):
+    torch = _torch()
+    rng = np.random.default_rng(cin + 3 * cout)
+    x = O.bf16(rng.standard_normal((B, H, W, cin)))
+    g = O.bf16(rng.standard_normal((B, H, W, cout)))
+    dw = torch.zeros(cout * 9 * cin, dtype=torch.float32, device="cuda")
+    ws = torch.empty(64 << 20, dtype=torch.uint8, device="cuda")
+    err = torch.zeros(1, dtype=torch.int32, device="cuda")
+    d = N.ArtCnnWgrad()
+    d.B, d.H, d.W, d.cout, d.cin = B, H, W, cout, cin
+    xt, gt = _bf(x), _bf(g)
+    d.dy, d.x, d.dw, d.accumulate = gt.data_ptr(), xt.data_ptr(), dw.data_ptr(), 0
+    d.workspace, d.workspace_bytes, d.err = ws.data_ptr(), ws.numel(), err.data_ptr()
+    N.check(N.lib().art_cnn_wgrad3x3(C.byref(d), None))
+    torch.cuda.synchronize()
+    assert int(err.item()) == 0
+    ref = O.conv_wgrad(x, g)
+    got = dw.cpu().numpy().astype(np.float64).reshape(cout, 9, cin)
+    np.testing.assert_allclose(got, ref, rtol=0, atol=2e-5 * float(np.abs(ref).max()) + 1e-5)
+
+
+def test_memory_kernels(gpu):
+    torch = _torch()
+    rng = np.random.default_rng(11)
+    B, H, W, C = 2, 8, 12, 16
+    a = O.bf16(rng.standard_normal((B, H, W, 48)))
+    out = torch.empty((B, H // 2, W // 2, C), dtype=torch.bfloat16, device="cuda")
+    N.check(N.lib().art_cnn_pool2(_ptr(_bf(a)), B, H, W, C, 48, 16, _ptr(out), None))
+    np.testing.assert_array_equal(_np(out), O.bf16(O.pool(a[..., 16:32])))
+    lo = O.bf16(rng.standard_normal((B, H // 2, W // 2, C)))
+    cat = _bf(np.zeros((B, H, W, 32)))
+    N.check(N.lib().art_cnn_upsample2(_ptr(_bf(lo)), B, H, W, C, _ptr(cat), 32, 16, None))
+    np.testing.assert_array_equal(_np(cat)[..., 16:], O.up(lo))
+    g = O.bf16(rng.standard_normal((B, H, W, C)))
+    act = O.bf16(rng.standard_normal((B, H // 2, W // 2, C)))
+    ds = torch.empty((B, H // 2, W // 2, C), dtype=torch.bfloat16, device="cuda")
+    N.check(N.lib().art_cnn_downsum2_mask(_ptr(_bf(g)), B, H, W, C, _ptr(_bf(act)), _ptr(ds), None))
+    np.testing.assert_array_equal(_np(ds), O.bf16(O.downsum(g) * (act > 0)))
+    gs = O.bf16(rng.standard_normal((B, H, W, C)))
+    gp = O.bf16(rng.standard_normal((B, H // 2, W // 2, C)))
+    act2 = O.bf16(rng.standard_normal((B, H, W, 48)))
+    gt = _bf(gs)
+    N.check(N.lib().art_cnn_unpool_add_mask(_ptr(gt), _ptr(_bf(gp)), B, H, W, C, _ptr(_bf(act2)), 48, 32, None))
+    np.testing.assert_array_equal(_np(gt), O.bf16((gs + 0.25 * O.up(gp)) * (act2[..., 32:48] > 0)))
+
+
+def _batch(seed, B=2, H=64, W=48):
+    rng = np.random.default_rng(seed)
+    coef = np.zeros((B, H, W), np.int16)
+    for b in range(B):  # sparse low-frequency coefficients like a real JPEG
+        blk = coef[b].reshape(H // 8, 8, W // 8, 8)
+        blk[:, 0, :, 0] = rng.integers(-60, 60, size=(H // 8, W // 8))
+        blk[:, :3, :, :3] += rng.integers(-3, 4, size=(H // 8, 3, W // 8, 3)).astype(np.int16)
+    q = rng.integers(4, 40, size=(B, 64)).astype(np.float32)
+    dec, _ = O.features(coef, q)
+    target = (dec + rng.standard_normal(dec.shape) * 3.0).astype(np.float32)
+    return coef, q, target
+
+
+def test_features_and_prediction(gpu):
+    torch = _torch()
+    coef, q, _ = _batch(1)
+    params = WS.init_params(3)
+    net = WS.WarmStartNet(params)
+    pred = net.predict(torch.from_numpy(coef).cuda(), _f32(q)).cpu().numpy().astype(np.float64)
+    dec, F = O.features(coef, q)
+    a, ref, _, _ = O.forward(params.astype(np.float64), F, dec)
+    np.testing.assert_allclose(pred, ref, rtol=0, atol=2e-3 * max(1.0, float(np.abs(ref - dec).max())) + 1e-3)
+
+
+def test_network_gradients_match_oracle(gpu):
+    """The full forward + backward on the GPU against the oracle's FP64 backward
+    (bf16 storage emulated): per layer, cosine >= 0.999 and relative error <= 3e-2."""
+    torch = _torch()
+    coef, q, target = _batch(2)
+    params = WS.init_params(4)
+    rng = np.random.default_rng(4)
+    offs, _ = O.offsets()
+    wo, bo = offs["head"]
+    params[wo:bo] = (rng.standard_normal(bo - wo) * 0.05).astype(np.float32)  # a head that passes gradient
+    params[wo + 32 * 9:bo] = 0.0
+    net = WS.WarmStartNet(params)
+    loss = net.train_step(torch.from_numpy(coef).cuda(), _f32(q), _f32(target), lr=0.0)
+    g = net.gradients().astype(np.float64)
+    dec, F = O.features(coef, q)
+    ref_loss, ref = O.gradients(params.astype(np.float64), F, dec, target.astype(np.float64))
+    assert abs(loss - ref_loss) <= 1e-3 * ref_loss, (loss, ref_loss)
+    for name, cin, cout, _, _ in O.LAYERS:
+        for lo, hi in ((offs[name][0], offs[name][1]), (offs[name][1], offs[name][1] + cout)):
+            a, b = g[lo:hi], ref[lo:hi]
+            nb = float(np.linalg.norm(b))
+            if nb == 0:
+                assert float(np.abs(a).max()) == 0
+                continue
+            cos = float(a @ b) / (float(np.linalg.norm(a)) * nb)
+            rel = float(np.linalg.norm(a - b)) / nb
+            assert cos >= 0.999 and rel <= 3e-2, (name, cos, rel)
+
+
+def test_training_reduces_loss(gpu):
+    torch = _torch()
+    coef, q, target = _batch(3, B=4, H=64, W=64)
+    net = WS.WarmStartNet(WS.init_params(5))
+    c, qq, t = torch.from_numpy(coef).cuda(), _f32(q), _f32(target)
+    losses = [net.train_step(c, qq, t, lr=2e-3) for _ in range(30)]
+    assert losses[-1] < 0.7 * losses[0], losses
+    assert all(np.isfinite(losses))
