@@ -72,6 +72,19 @@ def load_peaks():
     return 6650.0, "fallback"
 
 
+def read_traffic(workload, kernel):
+    """DRAM bytes per launch of `kernel` on `workload` from the ncu captures
+    summarised in profiles/traffic.txt ("workload kernel bytes" lines), or None."""
+    p = ROOT / "profiles" / "traffic.txt"
+    if not p.exists():
+        return None
+    for line in p.read_text().splitlines():
+        parts = line.split()
+        if len(parts) == 3 and not line.startswith("#") and parts[0] == workload and parts[1] == kernel:
+            return float(parts[2])
+    return None
+
+
 def make_workload(kind):
     """List of decoded Jpeg objects for the workload."""
     from artefact_b200 import synth
@@ -456,13 +469,7 @@ def main():
     else:
         dom, dbytes, dms = "k_project", upd_bytes, u_launch
     achieved = dbytes / (dms * 1e-3) / 1e9
-    traffic = None
-    tf = ROOT / "profiles" / f"traffic_{args.workload}.json"
-    if tf.exists():
-        try:
-            traffic = json.loads(tf.read_text()).get(dom)
-        except Exception:
-            traffic = None
+    traffic = read_traffic(args.workload, dom)
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
