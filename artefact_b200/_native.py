@@ -22,6 +22,7 @@ ART_COEF_F32 = 0
 ART_COEF_I16 = 1
 ART_INIT_DECODED = 0
 ART_INIT_SCALAR_COMPAT = 1
+ART_INIT_LEARNED = 2
 
 
 class ArtChannel(C.Structure):
@@ -43,7 +44,8 @@ class ArtOptions(C.Structure):
     _fields_ = [
         ("init_mode", C.c_uint32),
         ("device", C.c_int32),
-        ("reserved", C.c_uint32 * 6),
+        ("step_iterations", C.c_uint32),
+        ("reserved", C.c_uint32 * 5),
     ]
 
 
@@ -119,6 +121,8 @@ EXPORTS = {
                                          C.POINTER(C.c_uint32)]),
     "art_context_tune_cache": (C.c_int32, [C.c_void_p, C.c_char_p, C.c_int32]),
     "art_context_synchronize": (C.c_int32, [C.c_void_p]),
+    "art_context_set_warm_start": (C.c_int32, [C.c_void_p, C.c_void_p]),
+    "art_context_evaluate": (C.c_int32, [C.c_void_p, C.c_uint32, C.POINTER(C.c_double)]),
     "art_context_set_timing": (C.c_int32, [C.c_void_p, C.c_int32]),
     "art_context_last_timing": (C.c_int32, [C.c_void_p, C.POINTER(C.c_float), C.POINTER(C.c_float),
                                             C.POINTER(C.c_float), C.POINTER(C.c_uint32)]),

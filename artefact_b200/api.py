@@ -135,10 +135,11 @@ class ArtefactError(RuntimeError):
     """Error of :meth:`Artefact.process` (the reference's ``Err(String)``)."""
 
 
-def _options(init_mode: int, device: int) -> N.ArtOptions:
+def _options(init_mode: int, device: int, step_iterations: int = 0) -> N.ArtOptions:
     o = N.ArtOptions()
     o.init_mode = init_mode
     o.device = device
+    o.step_iterations = int(step_iterations)
     return o
 
 
@@ -315,20 +316,34 @@ class Context:
     def handle(self) -> C.c_void_p:
         return self._h
 
+    def set_warm_start(self, net) -> None:
+        """Attach a :class:`artefact_b200.warmstart.WarmStartNet` (or None) for
+        ``init_mode=ART_INIT_LEARNED`` solves; the context does not own it."""
+        self._net = net
+        N.check(N.lib().art_context_set_warm_start(self._h, net.handle if net is not None else None))
+
+    def evaluate(self, image: int = 0) -> dict:
+        """Objective and feasibility of the last solve's result for `image`
+        (``art_context_evaluate``, fp64 on the GPU): keys E, tv, tgv, prob, infeasibility."""
+        out = (C.c_double * 5)()
+        N.check(N.lib().art_context_evaluate(self._h, int(image), out))
+        return dict(E=out[0], tv=out[1], tgv=out[2], prob=out[3], infeasibility=out[4])
+
     def compute(self, nchannel: int, coefs: Sequence[Coefficient], weight: float, pweight: Sequence[float],
                 iterations: int, max_rounded_px_w: int, max_rounded_px_h: int,
-                init_mode: int = N.ART_INIT_DECODED) -> List[np.ndarray]:
+                init_mode: int = N.ART_INIT_DECODED, step_iterations: int = 0) -> List[np.ndarray]:
         keep: list = []
         chans = (N.ArtChannel * nchannel)(*[coefs[c].as_c(keep) for c in range(nchannel)])
         pw = (C.c_float * 3)(*[float(v) for v in list(pweight)[:3]])
         outs = [np.empty(max_rounded_px_w * max_rounded_px_h, np.float32) for _ in range(nchannel)]
         ptrs = (C.c_void_p * nchannel)(*[o.ctypes.data for o in outs])
         N.check(N.lib().art_context_compute(self._h, nchannel, chans, float(weight), pw, int(iterations),
-                                            max_rounded_px_w, max_rounded_px_h, ptrs, C.byref(_options(init_mode, -1))))
+                                            max_rounded_px_w, max_rounded_px_h, ptrs,
+                                            C.byref(_options(init_mode, -1, step_iterations))))
         return outs
 
-    def compute_batch(self, jobs: Sequence[dict], iterations: int,
-                      init_mode: int = N.ART_INIT_DECODED) -> List[List[np.ndarray]]:
+    def compute_batch(self, jobs: Sequence[dict], iterations: int, init_mode: int = N.ART_INIT_DECODED,
+                      step_iterations: int = 0) -> List[List[np.ndarray]]:
         """Solve many images together (one launch per kernel and iteration over
         all of them, the loop in one CUDA graph). Each job is a dict with keys
         ``coefs`` (list of :class:`Coefficient`), ``weight``, ``pweight`` and
@@ -354,7 +369,7 @@ class Context:
             im.out_planes = C.cast(ptrs, C.POINTER(C.c_void_p))
             results.append(outs)
         N.check(N.lib().art_context_compute_batch(self._h, len(jobs), imgs, int(iterations),
-                                                  C.byref(_options(init_mode, -1))))
+                                                  C.byref(_options(init_mode, -1, step_iterations))))
         return results
 
     def autotune(self, nchannel: int, samp_h: Sequence[int], samp_v: Sequence[int], max_w: int, max_h: int,

@@ -5,6 +5,8 @@
 #include <string>
 #include <vector>
 
+struct ArtNet;
+
 namespace art {
 
 struct JpegChannel {
@@ -23,5 +25,17 @@ bool decode_jpeg(const uint8_t *data, size_t len, JpegImage &out, std::string &e
 
 // Thread-local error message for art_last_error().
 void set_error(const std::string &msg);
+
+namespace cnn {
+// Warm-start prediction for the solver: features + forward + residual of B
+// coefficient images into pred (dense [B][H][W] floats), queued on `stream`
+// (a cudaStream_t) without waiting for it.
+int32_t net_predict_async(ArtNet *net, const int16_t *coef, int cpitch, long long img_stride, const float *q, int B,
+                          int H, int W, float *pred, void *stream);
+int net_device(const ArtNet *net);
+// Reads the network's device error flag (synchronous): ART_OK, or an error if
+// one of its bounded tensor-core waits gave up.
+int32_t net_error(ArtNet *net);
+}  // namespace cnn
 
 }  // namespace art

@@ -1275,6 +1275,23 @@ int32_t net_predict(ArtNet *net, const int16_t *coef, int cpitch, long long img_
                             pred ? pred : net->pred.as<float>(), nullptr, nullptr, 1, s);
 }
 
+int32_t net_predict_async(ArtNet *net, const int16_t *coef, int cpitch, long long img_stride, const float *q, int B,
+                          int H, int W, float *pred, void *stream)
+{
+    return net_predict(net, coef, cpitch, img_stride, q, B, H, W, pred, static_cast<cudaStream_t>(stream));
+}
+
+int net_device(const ArtNet *net) { return net->device; }
+
+int32_t net_error(ArtNet *net)
+{
+    int h = 0;
+    if (cudaMemcpy(&h, net->errflag.p, sizeof(int), cudaMemcpyDeviceToHost) != cudaSuccess)
+        return fail(ART_ERR_CUDA, std::string("network: ") + cudaGetErrorString(cudaGetLastError()));
+    if (h) return fail(ART_ERR_CUDA, "network: a tensor-core pipeline wait timed out");
+    return ART_OK;
+}
+
 }  // namespace cnn
 }  // namespace art
 

@@ -712,6 +712,134 @@ __global__ void k_compat_step(const float *__restrict__ a, float *__restrict__ b
     b[(by * 8 + (k >> 3)) * cd.cw + bx * 8 + (k & 7)] = val;
 }
 
+// ---------------------------------------------------------- evaluation ----
+// Objective and feasibility of an iterate in fp64 (not on the solve path).
+// The objective is the function whose gradient the iteration follows: the
+// coupled TV and TGV norms of compute_step_tv.rs:63-71 and
+// compute_step_tv2.rs:76-90 summed over pixels, plus for each component
+// (alpha_p sh sv / 2) sum ((X - c q) / q)^2 over its blocks, X the DCT of the
+// (cell-averaged) plane; the sh sv factor makes the gradient of that term the
+// reference's unscaled replication to subsampled pixels
+// (compute_step_prob.rs:43-55).
+
+__constant__ double c_dct_matrix[64];  // orthonormal DCT-II, row u: s(u) cos((2y + 1) u pi / 16)
+
+constexpr int EVAL_THREADS = 256;
+constexpr int EVAL_BLOCKS = 592;
+
+__device__ __forceinline__ double block_sum(double v, double *sh)
+{
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    if (lane == 0) sh[warp] = v;
+    __syncthreads();
+    double t = 0;
+    if (threadIdx.x == 0)
+        for (int w = 0; w < EVAL_THREADS / 32; w++) t += sh[w];
+    __syncthreads();
+    return t;
+}
+
+// Per block: sum over its pixels of n1 = sqrt(sum_c dx^2 + dy^2) and
+// n2 = sqrt(sum_c gyy^2 + 2 s^2 + gxx^2), into partial[2 b], partial[2 b + 1].
+__global__ void __launch_bounds__(EVAL_THREADS) k_eval_pixels(const ImgDev *__restrict__ imgs, int img,
+                                                              double *__restrict__ partial)
+{
+    __shared__ double sh[EVAL_THREADS / 32];
+    const ImgDev &im = imgs[img];
+    const int W = im.W, H = im.H;
+    double s1 = 0, s2 = 0;
+    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < (long long)W * H;
+         i += (long long)gridDim.x * blockDim.x) {
+        const int x = (int)(i % W), y = (int)(i / W);
+        double n1 = 0, n2 = 0;
+        for (int c = 0; c < im.nch; c++) {
+            const float *f = im.x + c * im.cstride;
+            auto F = [&](int xx, int yy) { return (double)f[(long long)yy * im.pitch + xx]; };
+            auto DX = [&](int xx, int yy) { return xx < W - 1 ? F(xx + 1, yy) - F(xx, yy) : 0.0; };
+            auto DY = [&](int xx, int yy) { return yy < H - 1 ? F(xx, yy + 1) - F(xx, yy) : 0.0; };
+            const double dx = DX(x, y), dy = DY(x, y);
+            n1 += dx * dx + dy * dy;
+            double gxx = 0, gyx = 0, gyy = 0, gxy = 0;
+            if (x > 0) {
+                gxx = dx - DX(x - 1, y);
+                gyx = dy - DY(x - 1, y);
+            }
+            if (y > 0) {
+                gyy = dy - DY(x, y - 1);
+                gxy = dx - DX(x, y - 1);
+            }
+            const double sm = 0.5 * (gxy + gyx);
+            n2 += gyy * gyy + 2.0 * sm * sm + gxx * gxx;
+        }
+        s1 += sqrt(n1);
+        s2 += sqrt(n2);
+    }
+    s1 = block_sum(s1, sh);
+    s2 = block_sum(s2, sh);
+    if (threadIdx.x == 0) {
+        partial[2 * blockIdx.x] = s1;
+        partial[2 * blockIdx.x + 1] = s2;
+    }
+}
+
+// Per block: for channel c, sum over its 8x8 coefficient blocks of
+// ((X - c q) / q)^2 and the largest distance of X outside [(c - 1/2) q, (c + 1/2) q]
+// (X in fp64 from the cell-averaged plane, compute_projection.rs:18-32 and :72-79).
+__global__ void __launch_bounds__(EVAL_THREADS) k_eval_blocks(const ImgDev *__restrict__ imgs, int img, int c,
+                                                              double *__restrict__ partial)
+{
+    __shared__ double sh[EVAL_THREADS / 32];
+    __shared__ double sm_max[EVAL_THREADS];
+    const ImgDev &im = imgs[img];
+    const ChanDev &cd = im.ch[c];
+    const int bw = cd.cw / 8, nb = bw * (cd.chh / 8);
+    const float *f = im.x + c * im.cstride;
+    const double inv_cell = 1.0 / (double)(cd.sh * cd.sv);
+    double acc = 0, worst = 0;
+    for (int b = blockIdx.x * blockDim.x + threadIdx.x; b < nb; b += gridDim.x * blockDim.x) {
+        const int bx = b % bw, by = b / bw;
+        double blk[64], t[64];
+        for (int r = 0; r < 8; r++)
+            for (int u = 0; u < 8; u++) {
+                double m = 0;
+                for (int sy = 0; sy < cd.sv; sy++)
+                    for (int sx = 0; sx < cd.sh; sx++)
+                        m += (double)f[(long long)((by * 8 + r) * cd.sv + sy) * im.pitch + (bx * 8 + u) * cd.sh + sx];
+                blk[r * 8 + u] = m * inv_cell;
+            }
+        for (int v = 0; v < 8; v++)  // t = C * blk (columns)
+            for (int u = 0; u < 8; u++) {
+                double a = 0;
+                for (int r = 0; r < 8; r++) a += c_dct_matrix[v * 8 + r] * blk[r * 8 + u];
+                t[v * 8 + u] = a;
+            }
+        for (int v = 0; v < 8; v++)  // X = t * C^T (rows)
+            for (int u = 0; u < 8; u++) {
+                double X = 0;
+                for (int k = 0; k < 8; k++) X += t[v * 8 + k] * c_dct_matrix[u * 8 + k];
+                const double q = im.q[c][v * 8 + u];
+                const double cc = (double)cd.coef[(long long)(by * 8 + v) * cd.cpitch + bx * 8 + u];
+                const double d = (X - cc * q) / q;
+                acc += d * d;
+                const double lo = (cc - 0.5) * q, hi = (cc + 0.5) * q;
+                const double viol = X < lo ? lo - X : (X > hi ? X - hi : 0.0);
+                worst = fmax(worst, viol);
+            }
+    }
+    acc = block_sum(acc, sh);
+    sm_max[threadIdx.x] = worst;
+    __syncthreads();
+    for (int k = EVAL_THREADS / 2; k > 0; k >>= 1) {
+        if (threadIdx.x < k) sm_max[threadIdx.x] = fmax(sm_max[threadIdx.x], sm_max[threadIdx.x + k]);
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) {
+        partial[2 * blockIdx.x] = acc;
+        partial[2 * blockIdx.x + 1] = sm_max[0];
+    }
+}
+
 // Nearest upsampling of a component image to both state buffers (coef.rs:69-92).
 __global__ void k_upsample(const float *__restrict__ img, const ImgDev *__restrict__ imgs, int c)
 {
@@ -853,8 +981,12 @@ struct ImageSpec {
 struct ArtContext {
     int device = 0;
     cudaStream_t stream = nullptr;
-    art::DevBuf xbuf, pbuf, coefimg, stage, misc, desc, work, tasks, compat, sepplanes, rgb;
+    art::DevBuf xbuf, pbuf, coefimg, stage, misc, desc, work, tasks, compat, sepplanes, rgb, pred;
+    ArtNet *net = nullptr;            // warm-start network for ART_INIT_LEARNED (not owned)
+    bool net_used = false;            // the last solve ran the network (its error flag is checked)
     std::vector<art::ImgDev> h_desc;  // per image (pageable: copies of it are staged)
+    std::vector<std::array<float, 4>> h_weights;  // per image: weight, pweight[3]
+    art::DevBuf evalbuf;              // partial sums of art_context_evaluate
     std::vector<int2> h_work;         // sweep blocks {image, block in image}, grouped by variant and channel count
     int wstart[2][4] = {}, wcount[2][4] = {};  // by sweep variant (0 narrow, 1 wide) and channel count
     std::vector<int4> h_tasks;        // block warps {image, channel, block row, first block}
@@ -999,10 +1131,35 @@ static void build_tasks(const ImgDev &d, int img, std::vector<int4> per_mode[4])
     for (const Key &k : keys) per_mode[k.mode].push_back(make_int4(img, k.c, k.by, k.bx0));
 }
 
+// Step + projection of every image, one launch per sampling mode present.
+static void launch_projections(ArtContext *ctx, float fnext)
+{
+    const ImgDev *ddesc = static_cast<const ImgDev *>(ctx->desc.p);
+    const int4 *tasks = static_cast<const int4 *>(ctx->tasks.p);
+    cudaStream_t s = ctx->stream;
+    for (int m = 3; m >= 0; m--) {
+        const int n = ctx->mode_off[m + 1] - ctx->mode_off[m];
+        if (n == 0) continue;
+        const int4 *tk = tasks + ctx->mode_off[m];
+        const int grid = (n + PROJ_WARPS - 1) / PROJ_WARPS;
+        if (m == 0)
+            k_project<1, 1><<<grid, PROJ_WARPS * 32, proj_smem<1, 1>(), s>>>(ddesc, tk, n, fnext);
+        else if (m == 1)
+            k_project<2, 2><<<grid, PROJ_WARPS * 32, proj_smem<2, 2>(), s>>>(ddesc, tk, n, fnext);
+        else if (m == 2)
+            k_project<2, 1><<<grid, PROJ_WARPS * 32, proj_smem<2, 1>(), s>>>(ddesc, tk, n, fnext);
+        else
+            k_project<1, 2><<<grid, PROJ_WARPS * 32, proj_smem<1, 2>(), s>>>(ddesc, tk, n, fnext);
+    }
+}
+
 // Lays out the buffers of a batch of images, uploads descriptors and work
 // lists, ingests coefficients and queues the initialisation.
-static int prepare_batch(ArtContext *ctx, const std::vector<ImageSpec> &specs, uint32_t iterations, int init_mode)
+static int prepare_batch(ArtContext *ctx, const std::vector<ImageSpec> &specs, uint32_t iterations, int init_mode,
+                         uint32_t step_iterations)
 {
+    if (init_mode == ART_INIT_LEARNED && !ctx->net) return fail(ART_ERR_INVALID_ARGUMENT, "learned start: no network attached");
+    const uint32_t step_its = step_iterations ? step_iterations : iterations;
     int rc;
     const int nimg = (int)specs.size();
     long long batch_px = 0;
@@ -1011,10 +1168,12 @@ static int prepare_batch(ArtContext *ctx, const std::vector<ImageSpec> &specs, u
     std::vector<std::array<size_t, 3>> o_coef(nimg), o_p(nimg);
     size_t x_floats = 0, coef_bytes = 0, p_floats = 0, misc_bytes = 256;  // misc starts with the error flag
     ctx->h_desc.assign(nimg, ImgDev());
+    ctx->h_weights.assign(nimg, std::array<float, 4>{});
     for (int i = 0; i < nimg; i++) {
         const ImageSpec &sp = specs[i];
         ImgDev &d = ctx->h_desc[i];
         memset(&d, 0, sizeof(d));
+        ctx->h_weights[i] = {sp.weight, sp.pweight[0], sp.pweight[1], sp.pweight[2]};
         const int pitch = (int)align_up(sp.W, 32);
         const long long cstride = (long long)pitch * (long long)align_up(sp.H, 32);
         const std::pair<int, int> sw = pick_sweep(ctx, sp, batch_px);
@@ -1035,7 +1194,7 @@ static int prepare_batch(ArtContext *ctx, const std::vector<ImageSpec> &specs, u
         d.alpha_tv = 1.0f / sqrtf((float)sp.nch);
         d.alpha_tgv = (sp.weight / sqrtf(2.0f)) / sqrtf((float)sp.nch);
         // mod.rs:45 and :71.
-        d.step = (sqrtf((float)((uint64_t)sp.W * sp.H)) / 2.0f) / sqrtf(1.0f + (float)iterations);
+        d.step = (sqrtf((float)((uint64_t)sp.W * sp.H)) / 2.0f) / sqrtf(1.0f + (float)step_its);
         o_x[i] = x_floats;
         x_floats += align_up((size_t)3 * sp.nch * cstride, 64);
         o_misc[i] = misc_bytes;
@@ -1141,6 +1300,30 @@ static int prepare_batch(ArtContext *ctx, const std::vector<ImageSpec> &specs, u
                 k_upsample<<<(int)(((long long)sp.W * sp.H + 255) / 256), 256, 0, s>>>(a, ddesc + i, (int)c);
             }
         }
+    } else if (init_mode == ART_INIT_LEARNED) {
+        // Prediction per component at its own resolution, repeated to full
+        // resolution into x and y, then one projection with a zero step
+        // (g = 0, sigma = 0): x_0 = y_0 = P(prediction), and the DCT-distance
+        // plane of the projected prediction for the first gradient.
+        size_t need = 0;
+        for (const auto &sp : specs)
+            for (uint32_t c = 0; c < sp.nch; c++)
+                need = std::max(need, (size_t)sp.ch[c].rounded_px_w * sp.ch[c].rounded_px_h);
+        if ((rc = ctx->pred.ensure(need * sizeof(float)))) return rc;
+        float *pred = static_cast<float *>(ctx->pred.p);
+        for (int i = 0; i < nimg; i++) {
+            const ImgDev &d = ctx->h_desc[i];
+            for (int c = 0; c < d.nch; c++) {
+                const ChanDev &cd = d.ch[c];
+                rc = cnn::net_predict_async(ctx->net, cd.coef, cd.cpitch, 0, &ddesc[i].q[c][0], 1, cd.chh, cd.cw,
+                                            pred, s);
+                if (rc) return rc;
+                k_upsample<<<(int)(((long long)d.W * d.H + 255) / 256), 256, 0, s>>>(pred, ddesc + i, c);
+            }
+            ART_CUDA(cudaMemsetAsync(d.g, 0, (size_t)d.nch * d.cstride * sizeof(float), s));
+        }
+        launch_projections(ctx, 0.0f);
+        ctx->net_used = true;
     } else {
         k_init<<<(ntasks + PROJ_WARPS - 1) / PROJ_WARPS, PROJ_WARPS * 32, 0, s>>>(
             ddesc, static_cast<const int4 *>(ctx->tasks.p), ntasks);
@@ -1153,7 +1336,6 @@ static void launch_iteration(ArtContext *ctx, int it, float fnext)
 {
     const ImgDev *ddesc = static_cast<const ImgDev *>(ctx->desc.p);
     const int2 *work = static_cast<const int2 *>(ctx->work.p);
-    const int4 *tasks = static_cast<const int4 *>(ctx->tasks.p);
     cudaStream_t s = ctx->stream;
     const bool tm = ctx->timing;
     if (tm) cudaEventRecordWithFlags(ctx->events[2 + 4 * it], s, cudaEventRecordExternal);
@@ -1171,20 +1353,7 @@ static void launch_iteration(ArtContext *ctx, int it, float fnext)
         k_grad_sweep_n<1><<<ctx->wcount[0][1], SWEEP_WARPS_N * 32, 0, s>>>(ddesc, work + ctx->wstart[0][1]);
     if (tm) cudaEventRecordWithFlags(ctx->events[3 + 4 * it], s, cudaEventRecordExternal);
     if (tm) cudaEventRecordWithFlags(ctx->events[4 + 4 * it], s, cudaEventRecordExternal);
-    for (int m = 3; m >= 0; m--) {
-        const int n = ctx->mode_off[m + 1] - ctx->mode_off[m];
-        if (n == 0) continue;
-        const int4 *tk = tasks + ctx->mode_off[m];
-        const int grid = (n + PROJ_WARPS - 1) / PROJ_WARPS;
-        if (m == 0)
-            k_project<1, 1><<<grid, PROJ_WARPS * 32, proj_smem<1, 1>(), s>>>(ddesc, tk, n, fnext);
-        else if (m == 1)
-            k_project<2, 2><<<grid, PROJ_WARPS * 32, proj_smem<2, 2>(), s>>>(ddesc, tk, n, fnext);
-        else if (m == 2)
-            k_project<2, 1><<<grid, PROJ_WARPS * 32, proj_smem<2, 1>(), s>>>(ddesc, tk, n, fnext);
-        else
-            k_project<1, 2><<<grid, PROJ_WARPS * 32, proj_smem<1, 2>(), s>>>(ddesc, tk, n, fnext);
-    }
+    launch_projections(ctx, fnext);
     if (tm) cudaEventRecordWithFlags(ctx->events[5 + 4 * it], s, cudaEventRecordExternal);
 }
 
@@ -1254,6 +1423,24 @@ static int check_errflag(ArtContext *ctx)
     unsigned flag = 0;
     ART_CUDA(cudaMemcpy(&flag, ctx->errflag, sizeof(unsigned), cudaMemcpyDeviceToHost));
     if (flag) return fail(ART_ERR_INVALID_DATA, "coefficients must be integers in [-32768, 32767]");
+    if (ctx->net_used && ctx->net) return cnn::net_error(ctx->net);
+    return ART_OK;
+}
+
+// Start mode and step schedule of a solve.
+struct InitSpec {
+    int mode = ART_INIT_DECODED;
+    uint32_t step_iterations = 0;
+};
+
+static int init_spec(const ArtContext *ctx, const ArtOptions *opts, InitSpec *out)
+{
+    out->mode = opts ? (int)opts->init_mode : ART_INIT_DECODED;
+    out->step_iterations = opts ? opts->step_iterations : 0;
+    if (out->mode != ART_INIT_DECODED && out->mode != ART_INIT_SCALAR_COMPAT && out->mode != ART_INIT_LEARNED)
+        return fail(ART_ERR_INVALID_ARGUMENT, "unknown init mode");
+    if (out->mode == ART_INIT_LEARNED && !ctx->net)
+        return fail(ART_ERR_INVALID_ARGUMENT, "learned start: no network attached (art_context_set_warm_start)");
     return ART_OK;
 }
 
@@ -1351,10 +1538,10 @@ int32_t art_context_compute_device(ArtContext *ctx, uint32_t nchannel, const Art
     if (!out_planes_device || out_pitch < max_w) return fail(ART_ERR_INVALID_ARGUMENT, "bad output planes");
     for (uint32_t c = 0; c < nchannel; c++)
         if (!out_planes_device[c]) return fail(ART_ERR_INVALID_ARGUMENT, "null output plane");
-    const int init_mode = opts ? (int)opts->init_mode : ART_INIT_DECODED;
-    if (init_mode != ART_INIT_DECODED && init_mode != ART_INIT_SCALAR_COMPAT)
-        return fail(ART_ERR_INVALID_ARGUMENT, "unknown init mode");
+    InitSpec ini;
+    if ((rc = init_spec(ctx, opts, &ini))) return rc;
     ART_CUDA(cudaSetDevice(ctx->device));
+    ctx->net_used = false;
     // `stream` NULL is the legacy default stream, as everywhere in CUDA.
     cudaStream_t user = static_cast<cudaStream_t>(stream);
     cudaEvent_t join = nullptr;
@@ -1367,7 +1554,7 @@ int32_t art_context_compute_device(ArtContext *ctx, uint32_t nchannel, const Art
     ImageSpec sp{nchannel, coefs, {nullptr, nullptr, nullptr}, weight, {pweight[0], pweight[1], pweight[2]}, max_w,
                  max_h};
     for (uint32_t c = 0; c < nchannel; c++) sp.src[c] = coefs[c].dct_coefs;
-    rc = prepare_batch(ctx, {sp}, iterations, init_mode);
+    rc = prepare_batch(ctx, {sp}, iterations, ini.mode, ini.step_iterations);
     if (!rc) rc = run_iterations(ctx, iterations);
     if (!rc) {
         const float *fb;
@@ -1391,6 +1578,70 @@ int32_t art_context_compute_device(ArtContext *ctx, uint32_t nchannel, const Art
     return rc;
 }
 
+int32_t art_context_evaluate(ArtContext *ctx, uint32_t image, double out[5])
+{
+    if (!ctx || !out) return fail(ART_ERR_INVALID_ARGUMENT, "null argument");
+    if (image >= ctx->h_desc.size()) return fail(ART_ERR_INVALID_ARGUMENT, "no such image in the last solve");
+    ART_CUDA(cudaSetDevice(ctx->device));
+    static std::once_flag once;
+    static double mat[64];
+    std::call_once(once, [] {
+        const double pi = 3.14159265358979323846;
+        for (int u = 0; u < 8; u++)
+            for (int y = 0; y < 8; y++)
+                mat[u * 8 + y] = (u == 0 ? std::sqrt(1.0 / 8.0) : std::sqrt(2.0 / 8.0)) * std::cos((2 * y + 1) * u * pi / 16.0);
+    });
+    ART_CUDA(cudaMemcpyToSymbolAsync(c_dct_matrix, mat, sizeof(mat), 0, cudaMemcpyHostToDevice, ctx->stream));
+    const ImgDev &d = ctx->h_desc[image];
+    const int nparts = 2 * EVAL_BLOCKS * (1 + d.nch);
+    int rc;
+    if ((rc = ctx->evalbuf.ensure(nparts * sizeof(double)))) return rc;
+    double *part = static_cast<double *>(ctx->evalbuf.p);
+    const ImgDev *ddesc = static_cast<const ImgDev *>(ctx->desc.p);
+    k_eval_pixels<<<EVAL_BLOCKS, EVAL_THREADS, 0, ctx->stream>>>(ddesc, (int)image, part);
+    for (int c = 0; c < d.nch; c++)
+        k_eval_blocks<<<EVAL_BLOCKS, EVAL_THREADS, 0, ctx->stream>>>(ddesc, (int)image, c,
+                                                                      part + 2 * EVAL_BLOCKS * (1 + c));
+    ART_CUDA(cudaGetLastError());
+    std::vector<double> h(nparts);
+    ART_CUDA(cudaMemcpyAsync(h.data(), part, nparts * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
+    ART_CUDA(cudaStreamSynchronize(ctx->stream));
+    const std::array<float, 4> &wt = ctx->h_weights[image];
+    const double nch = (double)d.nch;
+    double s1 = 0, s2 = 0;
+    for (int b = 0; b < EVAL_BLOCKS; b++) {
+        s1 += h[2 * b];
+        s2 += h[2 * b + 1];
+    }
+    const double tv = s1 / std::sqrt(nch), tgv = s2 * (((double)wt[0] / std::sqrt(2.0)) / std::sqrt(nch));
+    double prob = 0, worst = 0;
+    for (int c = 0; c < d.nch; c++) {
+        double acc = 0;
+        for (int b = 0; b < EVAL_BLOCKS; b++) {
+            acc += h[2 * EVAL_BLOCKS * (1 + c) + 2 * b];
+            worst = std::max(worst, h[2 * EVAL_BLOCKS * (1 + c) + 2 * b + 1]);
+        }
+        if (wt[1 + c] != 0.0f)
+            prob += 0.5 * ((double)wt[1 + c] * 2.0 * 255.0 * std::sqrt(2.0) * (double)(d.ch[c].sh * d.ch[c].sv)) * acc;
+    }
+    out[0] = tv + tgv + prob;
+    out[1] = tv;
+    out[2] = tgv;
+    out[3] = prob;
+    out[4] = worst;
+    return ART_OK;
+}
+
+int32_t art_context_set_warm_start(ArtContext *ctx, ArtNet *net)
+{
+    if (!ctx) return fail(ART_ERR_INVALID_ARGUMENT, "null context");
+    if (net && cnn::net_device(net) != ctx->device)
+        return fail(ART_ERR_INVALID_ARGUMENT, "warm-start network lives on another device than the context");
+    ctx->net = net;
+    ctx->net_used = false;
+    return ART_OK;
+}
+
 int32_t art_context_synchronize(ArtContext *ctx)
 {
     if (!ctx) return fail(ART_ERR_INVALID_ARGUMENT, "null context");
@@ -1400,12 +1651,14 @@ int32_t art_context_synchronize(ArtContext *ctx)
 }
 
 static int solve_host(ArtContext *ctx, uint32_t nchannel, const ArtChannel *coefs, float weight,
-                      const float pweight[3], uint32_t iterations, uint32_t max_w, uint32_t max_h, int init_mode)
+                      const float pweight[3], uint32_t iterations, uint32_t max_w, uint32_t max_h,
+                      const ArtOptions *opts)
 {
     int rc = validate(nchannel, coefs, weight, pweight, max_w, max_h);
     if (rc) return rc;
-    if (init_mode != ART_INIT_DECODED && init_mode != ART_INIT_SCALAR_COMPAT)
-        return fail(ART_ERR_INVALID_ARGUMENT, "unknown init mode");
+    InitSpec ini;
+    if ((rc = init_spec(ctx, opts, &ini))) return rc;
+    ctx->net_used = false;
     // Host coefficients go through a device staging buffer.
     size_t off[3], total = 0;
     for (uint32_t c = 0; c < nchannel; c++) {
@@ -1423,7 +1676,7 @@ static int solve_host(ArtContext *ctx, uint32_t nchannel, const ArtChannel *coef
                                  cudaMemcpyHostToDevice, ctx->stream));
         sp.src[c] = dst;
     }
-    rc = prepare_batch(ctx, {sp}, iterations, init_mode);
+    rc = prepare_batch(ctx, {sp}, iterations, ini.mode, ini.step_iterations);
     if (!rc) rc = run_iterations(ctx, iterations);
     return rc;
 }
@@ -1437,8 +1690,7 @@ int32_t art_context_compute(ArtContext *ctx, uint32_t nchannel, const ArtChannel
     for (uint32_t c = 0; c < nchannel && c < 3; c++)
         if (!out_planes[c]) return fail(ART_ERR_INVALID_ARGUMENT, "null output plane");
     ART_CUDA(cudaSetDevice(ctx->device));
-    const int init_mode = opts ? (int)opts->init_mode : ART_INIT_DECODED;
-    int rc = solve_host(ctx, nchannel, coefs, weight, pweight, iterations, max_w, max_h, init_mode);
+    int rc = solve_host(ctx, nchannel, coefs, weight, pweight, iterations, max_w, max_h, opts);
     if (rc) {
         cudaStreamSynchronize(ctx->stream);
         return rc;
@@ -1463,7 +1715,6 @@ int32_t art_context_process(ArtContext *ctx, uint32_t nchannel, const ArtChannel
     if (!coefs || !weight || !pweight || !iterations) return fail(ART_ERR_INVALID_ARGUMENT, "null argument");
     if (nchannel < 1 || nchannel > 4) return fail(ART_ERR_INVALID_ARGUMENT, "nchannel must be 1 to 4");
     ART_CUDA(cudaSetDevice(ctx->device));
-    const int init_mode = opts ? (int)opts->init_mode : ART_INIT_DECODED;
     // lib.rs:108-116: max rounded size over components.
     uint32_t W = 0, H = 0;
     for (uint32_t c = 0; c < nchannel; c++) {
@@ -1478,7 +1729,7 @@ int32_t art_context_process(ArtContext *ctx, uint32_t nchannel, const ArtChannel
     int rc;
     if (nchannel == 3 && !separate) {
         // lib.rs:122-132: joint solve with weight[0], pweight, iterations[0].
-        rc = solve_host(ctx, 3, coefs, weight[0], pweight, iterations[0], W, H, init_mode);
+        rc = solve_host(ctx, 3, coefs, weight[0], pweight, iterations[0], W, H, opts);
         if (rc) {
             cudaStreamSynchronize(ctx->stream);
             return rc;
@@ -1497,7 +1748,7 @@ int32_t art_context_process(ArtContext *ctx, uint32_t nchannel, const ArtChannel
         for (uint32_t c = 0; c < nchannel; c++) {
             const float w = weight[c < 3 ? c : 2];
             const uint32_t its = iterations[c < 3 ? c : 2];
-            rc = solve_host(ctx, 1, &coefs[c], w, pweight, its, W, H, init_mode);
+            rc = solve_host(ctx, 1, &coefs[c], w, pweight, its, W, H, opts);
             if (rc) {
                 cudaStreamSynchronize(ctx->stream);
                 return rc;
@@ -1557,9 +1808,12 @@ int32_t art_context_compute_batch(ArtContext *ctx, uint32_t nimages, const ArtIm
 {
     if (!ctx || !images || nimages == 0) return fail(ART_ERR_INVALID_ARGUMENT, "null context or empty batch");
     ART_CUDA(cudaSetDevice(ctx->device));
-    const int init_mode = opts ? (int)opts->init_mode : ART_INIT_DECODED;
+    InitSpec ini;
+    int rc = init_spec(ctx, opts, &ini);
+    if (rc) return rc;
+    ctx->net_used = false;
     std::vector<ImageSpec> specs;
-    int rc = batch_specs(images, nimages, specs);
+    rc = batch_specs(images, nimages, specs);
     if (rc) return rc;
     // Host coefficients of every image through one device staging buffer.
     size_t total = 0;
@@ -1577,7 +1831,7 @@ int32_t art_context_compute_batch(ArtContext *ctx, uint32_t nimages, const ArtIm
             sp.src[c] = dst;
             off += align_up(n, 256);
         }
-    rc = prepare_batch(ctx, specs, iterations, init_mode);
+    rc = prepare_batch(ctx, specs, iterations, ini.mode, ini.step_iterations);
     if (!rc) rc = run_iterations(ctx, iterations);
     if (rc) {
         cudaStreamSynchronize(ctx->stream);
@@ -1603,9 +1857,12 @@ int32_t art_context_compute_batch_device(ArtContext *ctx, uint32_t nimages, cons
 {
     if (!ctx || !images || nimages == 0) return fail(ART_ERR_INVALID_ARGUMENT, "null context or empty batch");
     ART_CUDA(cudaSetDevice(ctx->device));
-    const int init_mode = opts ? (int)opts->init_mode : ART_INIT_DECODED;
+    InitSpec ini;
+    int rc = init_spec(ctx, opts, &ini);
+    if (rc) return rc;
+    ctx->net_used = false;
     std::vector<ImageSpec> specs;
-    int rc = batch_specs(images, nimages, specs);
+    rc = batch_specs(images, nimages, specs);
     if (rc) return rc;
     for (uint32_t i = 0; i < nimages; i++)
         if (images[i].out_pitch < images[i].max_rounded_px_w)
@@ -1617,7 +1874,7 @@ int32_t art_context_compute_batch_device(ArtContext *ctx, uint32_t nimages, cons
         ART_CUDA(cudaEventRecord(join, user));
         ART_CUDA(cudaStreamWaitEvent(ctx->stream, join, 0));
     }
-    rc = prepare_batch(ctx, specs, iterations, init_mode);
+    rc = prepare_batch(ctx, specs, iterations, ini.mode, ini.step_iterations);
     if (!rc) rc = run_iterations(ctx, iterations);
     for (uint32_t i = 0; !rc && i < nimages; i++) {
         const float *fb;
@@ -1703,7 +1960,7 @@ int32_t art_context_autotune(ArtContext *ctx, uint32_t nchannel, const uint32_t 
         if ((int)max_h < R && R > 16) continue;
         ctx->sweep_kind_override = cand[0];
         ctx->strip_rows_override = R;
-        rc = prepare_batch(ctx, {sp}, iterations, ART_INIT_DECODED);
+        rc = prepare_batch(ctx, {sp}, iterations, ART_INIT_DECODED, 0);
         if (!rc) rc = run_iterations(ctx, iterations);  // captures and warms up
         float ms = 1e30f;
         for (int rep = 0; rep < 3 && !rc; rep++) {

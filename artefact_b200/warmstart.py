@@ -154,3 +154,15 @@ class WarmStartNet:
         N.check(N.lib().art_net_predict(self._h, _ptr(coef), W, H * W, _ptr(q), B, H, W, _ptr(out),
                                         _stream(stream)))
         return out
+
+    def predict_decoded(self, coef, q, stream=None):
+        """The decoded start IDCT(c q) per block, float32 [B][H][W] (the
+        network's input before its residual; what the plain solver starts from)."""
+        import torch
+
+        B, H, W = coef.shape
+        dec = torch.empty((B, H, W), dtype=torch.float32, device=coef.device)
+        feat = torch.empty((B, H, W, 16), dtype=torch.bfloat16, device=coef.device)
+        N.check(N.lib().art_cnn_features(_ptr(coef), W, H * W, _ptr(q), B, H, W, _ptr(dec), _ptr(feat),
+                                         _stream(stream)))
+        return dec

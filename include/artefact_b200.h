@@ -34,6 +34,11 @@ extern "C" {
 
 #define ART_INIT_DECODED 0       /* x0 = block IDCT of c*q, unboxed once (pipeline_simd_adaptive/coef.rs:69-95) */
 #define ART_INIT_SCALAR_COMPAT 1 /* x0 as pipeline_scalar/coef.rs:29-50 builds it (per-block whole-plane unboxing) */
+#define ART_INIT_LEARNED 2       /* x0 = projection of the warm-start network's prediction (art_context_set_warm_start);
+                                    no reference counterpart: only the starting point changes, the iteration is the
+                                    reference's */
+
+typedef struct ArtNet ArtNet; /* warm-start network, declared with its functions at the end of this file */
 
 /*
  * One JPEG component as the solver receives it.
@@ -53,9 +58,12 @@ typedef struct ArtChannel {
 } ArtChannel;
 
 typedef struct ArtOptions {
-    uint32_t init_mode; /* ART_INIT_DECODED (default) or ART_INIT_SCALAR_COMPAT */
-    int32_t device;     /* CUDA device ordinal, -1 = current device */
-    uint32_t reserved[6];
+    uint32_t init_mode;       /* ART_INIT_DECODED (default), ART_INIT_SCALAR_COMPAT or ART_INIT_LEARNED */
+    int32_t device;           /* CUDA device ordinal, -1 = current device */
+    uint32_t step_iterations; /* 0: step size radius / sqrt(1 + iterations) as mod.rs:71 forms it; otherwise
+                                 radius / sqrt(1 + step_iterations), the step of a run of that many iterations
+                                 (a refinement after a learned start can take a long run's step) */
+    uint32_t reserved[5];
 } ArtOptions;
 
 typedef struct ArtContext ArtContext;
@@ -163,6 +171,30 @@ int32_t art_context_autotune(ArtContext *ctx, uint32_t nchannel, const uint32_t 
                              uint32_t max_rounded_px_w, uint32_t max_rounded_px_h, uint32_t iterations,
                              uint32_t *variant_out, uint32_t *strip_rows_out);
 int32_t art_context_tune_cache(ArtContext *ctx, const char *path, int32_t save);
+
+/*
+ * Attach the warm-start network used by ART_INIT_LEARNED solves on this
+ * context (NULL detaches). The network must live on the context's device and
+ * outlive its use; it is not owned by the context. With a learned start, each
+ * component's prediction (art_net_predict at the component's resolution) is
+ * repeated to full resolution like the decoded start, projected onto the
+ * quantisation box, and the solve's `iterations` plain iterations refine it
+ * with the FISTA sequence restarted. No reference counterpart.
+ */
+int32_t art_context_set_warm_start(ArtContext *ctx, ArtNet *net);
+
+/*
+ * Objective and feasibility of image `image`'s result of the context's last
+ * solve, in fp64 on the GPU (waits for the solve). out[0] = objective E,
+ * out[1..3] = its TV, TGV and DCT-distance terms, out[4] = the largest
+ * distance (coefficient units) by which a DCT coefficient of a result block
+ * (cell-averaged for subsampled components) lies outside its quantisation
+ * interval, 0 when all are inside. E is the function whose gradient the
+ * reference follows (compute_step_tv.rs:63-71, compute_step_tv2.rs:76-90,
+ * compute_step_prob.rs:24-55); the reference itself never evaluates it
+ * (compute_step.rs:39-48 discards the TV value).
+ */
+int32_t art_context_evaluate(ArtContext *ctx, uint32_t image, double out[5]);
 
 /* Wait for the context's queued work; returns the first error it met. */
 int32_t art_context_synchronize(ArtContext *ctx);
@@ -305,7 +337,6 @@ int32_t art_cnn_adam(float *w, const float *g, float *m, float *v, int64_t n, fl
  * [cout][9][cin] then the bias [cout]. Inputs are B int16 coefficient images
  * of H x W (multiples of 8; rows of cpitch elements, images img_stride
  * elements apart) with their quantisation tables q[B][64], all on the device. */
-typedef struct ArtNet ArtNet;
 int64_t art_net_num_params(void);
 int32_t art_net_create(int32_t device, const float *params_host, int64_t nparams, ArtNet **out);
 void art_net_destroy(ArtNet *net);

@@ -161,24 +161,30 @@ def test_memory_kernels(gpu):
     torch = _torch()
     rng = np.random.default_rng(11)
     B, H, W, C = 2, 8, 12, 16
+    # Every device input is held in a variable for the duration of its call:
+    # a temporary would go back to torch's caching allocator as soon as its
+    # pointer is taken, and the next input could be placed in the same memory.
     a = O.bf16(rng.standard_normal((B, H, W, 48)))
+    a_d = _bf(a)
     out = torch.empty((B, H // 2, W // 2, C), dtype=torch.bfloat16, device="cuda")
-    N.check(N.lib().art_cnn_pool2(_ptr(_bf(a)), B, H, W, C, 48, 16, _ptr(out), None))
+    N.check(N.lib().art_cnn_pool2(_ptr(a_d), B, H, W, C, 48, 16, _ptr(out), None))
     np.testing.assert_array_equal(_np(out), O.bf16(O.pool(a[..., 16:32])))
     lo = O.bf16(rng.standard_normal((B, H // 2, W // 2, C)))
+    lo_d = _bf(lo)
     cat = _bf(np.zeros((B, H, W, 32)))
-    N.check(N.lib().art_cnn_upsample2(_ptr(_bf(lo)), B, H, W, C, _ptr(cat), 32, 16, None))
+    N.check(N.lib().art_cnn_upsample2(_ptr(lo_d), B, H, W, C, _ptr(cat), 32, 16, None))
     np.testing.assert_array_equal(_np(cat)[..., 16:], O.up(lo))
     g = O.bf16(rng.standard_normal((B, H, W, C)))
     act = O.bf16(rng.standard_normal((B, H // 2, W // 2, C)))
+    g_d, act_d = _bf(g), _bf(act)
     ds = torch.empty((B, H // 2, W // 2, C), dtype=torch.bfloat16, device="cuda")
-    N.check(N.lib().art_cnn_downsum2_mask(_ptr(_bf(g)), B, H, W, C, _ptr(_bf(act)), _ptr(ds), None))
+    N.check(N.lib().art_cnn_downsum2_mask(_ptr(g_d), B, H, W, C, _ptr(act_d), _ptr(ds), None))
     np.testing.assert_array_equal(_np(ds), O.bf16(O.downsum(g) * (act > 0)))
     gs = O.bf16(rng.standard_normal((B, H, W, C)))
     gp = O.bf16(rng.standard_normal((B, H // 2, W // 2, C)))
     act2 = O.bf16(rng.standard_normal((B, H, W, 48)))
-    gt = _bf(gs)
-    N.check(N.lib().art_cnn_unpool_add_mask(_ptr(gt), _ptr(_bf(gp)), B, H, W, C, _ptr(_bf(act2)), 48, 32, None))
+    gt, gp_d, act2_d = _bf(gs), _bf(gp), _bf(act2)
+    N.check(N.lib().art_cnn_unpool_add_mask(_ptr(gt), _ptr(gp_d), B, H, W, C, _ptr(act2_d), 48, 32, None))
     np.testing.assert_array_equal(_np(gt), O.bf16((gs + 0.25 * O.up(gp)) * (act2[..., 32:48] > 0)))
 
 

@@ -1,0 +1,170 @@
+"""The GPU objective evaluator and the learned (warm) start, against the oracle (GPU).
+
+* ``art_context_evaluate`` (fp64 objective and feasibility on the GPU) against
+  the oracle's fp64 objective and feasibility of the same planes.
+* ``ART_INIT_LEARNED``: the solver's projection of the network's prediction
+  and the plain iterations after it, against the oracle's iteration from the
+  same start planes (``oracle_*_compute_from``), with the plain solver's
+  parity bar (max |GPU - oracle| <= 1.0 in 0..255 units, objective within
+  1e-4 relative, feasibility <= 1e-3 coefficient units).
+* The trained network's gain: from its start, a few plain iterations reach a
+  lower objective than the same iterations from the decoded start.
+"""
+import numpy as np
+import pytest
+
+import oracle_lib as O
+from artefact_b200 import _native as N
+from artefact_b200 import synth
+from artefact_b200 import warmstart as WS
+from artefact_b200.api import Context, Jpeg, JpegSource
+
+pytestmark = pytest.mark.gpu
+
+WEIGHT, PW = 0.3, [0.001] * 3
+CASES = [(40, 24, 50, "4:4:4", True), (72, 40, 75, "4:2:0", False), (48, 32, 30, "4:4:4", False),
+         (200, 136, 75, "4:2:0", False), (50, 30, 75, "4:2:2", False)]
+IDS = [f"{c[0]}x{c[1]}_q{c[2]}_{c[3]}{'_gray' if c[4] else ''}" for c in CASES]
+
+
+def jpeg_of(w, h, q, sub, gray, seed=21):
+    return Jpeg.from_source(JpegSource.Buffer(synth.make_jpeg(w, h, q, sub, gray, seed)))
+
+
+@pytest.fixture(scope="module")
+def ctx():
+    c = Context(0)
+    yield c
+    c.close()
+
+
+@pytest.mark.parametrize("shape", CASES, ids=IDS)
+@pytest.mark.parametrize("iterations", [0, 10])
+def test_evaluate_matches_oracle(gpu, ctx, shape, iterations):
+    j = jpeg_of(*shape)
+    W, H, _ = j.max_rounded()
+    n = j.nchannel
+    planes = ctx.compute(n, j.coefs, WEIGHT, PW, iterations, W, H)
+    ev = ctx.evaluate()
+    e, terms = O.objective(n, j.coefs, WEIGHT, PW, W, H, planes, terms=True)
+    assert abs(ev["E"] - e) <= 1e-9 * abs(e), (ev, e)
+    for got, ref in zip((ev["tv"], ev["tgv"], ev["prob"]), terms):
+        assert abs(got - ref) <= 1e-9 * abs(e), (ev, terms)
+    feas = O.feasibility(n, j.coefs, W, H, planes)
+    assert abs(ev["infeasibility"] - feas) <= 1e-6, (ev["infeasibility"], feas)
+    assert ev["infeasibility"] <= 1e-3
+
+
+def _strong_params(seed):
+    """Untrained weights whose head is large enough that the prediction moves
+    visibly away from the decoded start (the trained head is not near zero)."""
+    p = WS.init_params(seed)
+    rng = np.random.default_rng(seed)
+    offs = {}
+    o = 0
+    for name, cin, cout in WS.LAYERS:
+        offs[name] = (o, o + cout * 9 * cin)
+        o += cout * 9 * cin + cout
+    lo, hi = offs["head"]
+    p[lo:lo + 9 * 32] = (rng.standard_normal(9 * 32) * 0.05).astype(np.float32)
+    return p
+
+
+def _upsampled_prediction(net, j):
+    """Per component: the network's prediction at the component's resolution,
+    repeated to full resolution (as the solver places it)."""
+    import torch
+
+    W, H, _ = j.max_rounded()
+    out = []
+    for co in j.coefs:
+        ci = torch.from_numpy(WS.coef_image(co)[None]).cuda()
+        q = torch.from_numpy(np.asarray(co.quant_table, np.float32)[None].copy()).cuda()
+        p = net.predict(ci, q)[0].cpu().numpy()
+        out.append(np.repeat(np.repeat(p, co.vertical_samp_factor, 0), co.horizontal_samp_factor, 1)
+                   .reshape(H, W))
+    return out
+
+
+@pytest.mark.parametrize("shape", CASES, ids=IDS)
+@pytest.mark.parametrize("iterations,step_iterations", [(0, 0), (1, 0), (8, 0), (8, 50)])
+def test_learned_start_matches_oracle(gpu, ctx, shape, iterations, step_iterations):
+    j = jpeg_of(*shape)
+    W, H, _ = j.max_rounded()
+    n = j.nchannel
+    net = WS.WarmStartNet(_strong_params(7))
+    ctx.set_warm_start(net)
+    try:
+        gpu_planes = ctx.compute(n, j.coefs, WEIGHT, PW, iterations, W, H, init_mode=N.ART_INIT_LEARNED,
+                                 step_iterations=step_iterations)
+        ev = ctx.evaluate()
+    finally:
+        ctx.set_warm_start(None)
+    start = _upsampled_prediction(net, j)
+    ref = O.compute_from(n, j.coefs, WEIGHT, PW, iterations, W, H, start, step_iterations)
+    r64 = O.compute_from(n, j.coefs, WEIGHT, PW, iterations, W, H, start, step_iterations, fp64=True)
+    d = max(float(np.abs(a.astype(np.float64) - b).max()) for a, b in zip(gpu_planes, ref))
+    d64 = max(float(np.abs(a.astype(np.float64) - b).max()) for a, b in zip(gpu_planes, r64))
+    moved = max(float(np.abs(s.ravel() - a).max()) for s, a in zip(start, ref))
+    er = O.objective(n, j.coefs, WEIGHT, PW, W, H, ref)
+    print(f"{shape} it={iterations} step_it={step_iterations} max|gpu-f32|={d:.3g} max|gpu-f64|={d64:.3g} "
+          f"start moved by {moved:.3g} objective gpu {ev['E']:.9g} oracle {er:.9g}")
+    assert d <= 1.0
+    assert abs(ev["E"] - er) <= 1e-4 * abs(er)
+    assert ev["infeasibility"] <= 1e-3
+
+
+@pytest.mark.parametrize("shape", CASES[:3], ids=IDS[:3])
+def test_zero_residual_start_equals_decoded_start(gpu, ctx, shape):
+    """With a zero head the prediction is the decoded image, whose projection
+    is itself; the learned path then follows the plain solver."""
+    j = jpeg_of(*shape)
+    W, H, _ = j.max_rounded()
+    n = j.nchannel
+    p = WS.init_params(3)
+    offs = 0
+    for name, cin, cout in WS.LAYERS:
+        if name == "head":
+            p[offs:offs + cout * 9 * cin + cout] = 0.0
+        offs += cout * 9 * cin + cout
+    net = WS.WarmStartNet(p)
+    ctx.set_warm_start(net)
+    try:
+        a = ctx.compute(n, j.coefs, WEIGHT, PW, 10, W, H, init_mode=N.ART_INIT_LEARNED)
+    finally:
+        ctx.set_warm_start(None)
+    b = ctx.compute(n, j.coefs, WEIGHT, PW, 10, W, H)
+    d = max(float(np.abs(x - y).max()) for x, y in zip(a, b))
+    assert d <= 1e-2, d
+
+
+def test_learned_start_needs_a_network(gpu, ctx):
+    j = jpeg_of(*CASES[0])
+    W, H, _ = j.max_rounded()
+    with pytest.raises(N.ArtError, match="no network attached"):
+        ctx.compute(j.nchannel, j.coefs, WEIGHT, PW, 2, W, H, init_mode=N.ART_INIT_LEARNED)
+
+
+@pytest.mark.skipif(not WS.DEFAULT_WEIGHTS.exists(), reason="no trained weights in the package")
+@pytest.mark.parametrize("quality", [30, 50, 75])
+def test_trained_network_gain(gpu, ctx, quality):
+    """The trained network's start against the decoded start on an image it
+    was not trained on (seed outside the training range), at equal iterations:
+    after 8 plain iterations (their step the 50-iteration run's), the learned
+    path's objective is below the decoded path's, and both stay feasible."""
+    j = jpeg_of(512, 384, quality, "4:2:0", False, seed=7000 + quality)
+    W, H, _ = j.max_rounded()
+    net = WS.WarmStartNet.load()
+    ctx.set_warm_start(net)
+    try:
+        ctx.compute(3, j.coefs, WEIGHT, PW, 8, W, H, init_mode=N.ART_INIT_LEARNED, step_iterations=50)
+        el = ctx.evaluate()
+    finally:
+        ctx.set_warm_start(None)
+    ctx.compute(3, j.coefs, WEIGHT, PW, 8, W, H, step_iterations=50)
+    ed = ctx.evaluate()
+    ctx.compute(3, j.coefs, WEIGHT, PW, 50, W, H)
+    e50 = ctx.evaluate()
+    print(f"q{quality}: E learned+8 {el['E']:.6g}  decoded+8 {ed['E']:.6g}  plain 50 {e50['E']:.6g}")
+    assert el["E"] < ed["E"]
+    assert el["infeasibility"] <= 1e-3 and ed["infeasibility"] <= 1e-3
