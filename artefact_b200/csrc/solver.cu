@@ -981,6 +981,8 @@ struct ImageSpec {
 struct ArtContext {
     int device = 0;
     cudaStream_t stream = nullptr;
+    cudaStream_t side = nullptr;      // second stream: projections of different sampling modes run side by side
+    cudaEvent_t fork = nullptr, join = nullptr;
     art::DevBuf xbuf, pbuf, coefimg, stage, misc, desc, work, tasks, compat, sepplanes, rgb, pred;
     ArtNet *net = nullptr;            // warm-start network for ART_INIT_LEARNED (not owned)
     bool net_used = false;            // the last solve ran the network (its error flag is checked)
@@ -1132,14 +1134,24 @@ static void build_tasks(const ImgDev &d, int img, std::vector<int4> per_mode[4])
 }
 
 // Step + projection of every image, one launch per sampling mode present.
+// The launches touch disjoint channels, so with more than one mode the
+// subsampled modes run on the side stream, concurrently with the full-
+// resolution one (a fork and join inside the captured graph).
 static void launch_projections(ArtContext *ctx, float fnext)
 {
     const ImgDev *ddesc = static_cast<const ImgDev *>(ctx->desc.p);
     const int4 *tasks = static_cast<const int4 *>(ctx->tasks.p);
-    cudaStream_t s = ctx->stream;
+    int modes = 0;
+    for (int m = 0; m < 4; m++) modes += ctx->mode_off[m + 1] > ctx->mode_off[m];
+    const bool split = modes > 1 && ctx->mode_off[1] > ctx->mode_off[0];
+    if (split) {
+        cudaEventRecord(ctx->fork, ctx->stream);
+        cudaStreamWaitEvent(ctx->side, ctx->fork, 0);
+    }
     for (int m = 3; m >= 0; m--) {
         const int n = ctx->mode_off[m + 1] - ctx->mode_off[m];
         if (n == 0) continue;
+        cudaStream_t s = split && m > 0 ? ctx->side : ctx->stream;
         const int4 *tk = tasks + ctx->mode_off[m];
         const int grid = (n + PROJ_WARPS - 1) / PROJ_WARPS;
         if (m == 0)
@@ -1150,6 +1162,10 @@ static void launch_projections(ArtContext *ctx, float fnext)
             k_project<2, 1><<<grid, PROJ_WARPS * 32, proj_smem<2, 1>(), s>>>(ddesc, tk, n, fnext);
         else
             k_project<1, 2><<<grid, PROJ_WARPS * 32, proj_smem<1, 2>(), s>>>(ddesc, tk, n, fnext);
+    }
+    if (split) {
+        cudaEventRecord(ctx->join, ctx->side);
+        cudaStreamWaitEvent(ctx->stream, ctx->join, 0);
     }
 }
 
@@ -1472,6 +1488,9 @@ int32_t art_context_create(int32_t device, ArtContext **out)
     std::unique_ptr<ArtContext> ctx(new ArtContext());
     ctx->device = device;
     ART_CUDA(cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking));
+    ART_CUDA(cudaStreamCreateWithFlags(&ctx->side, cudaStreamNonBlocking));
+    ART_CUDA(cudaEventCreateWithFlags(&ctx->fork, cudaEventDisableTiming));
+    ART_CUDA(cudaEventCreateWithFlags(&ctx->join, cudaEventDisableTiming));
     *out = ctx.release();
     return ART_OK;
 }
@@ -1494,6 +1513,11 @@ void art_context_destroy(ArtContext *ctx)
     ctx->compat.release();
     ctx->sepplanes.release();
     ctx->rgb.release();
+    ctx->pred.release();
+    ctx->evalbuf.release();
+    if (ctx->fork) cudaEventDestroy(ctx->fork);
+    if (ctx->join) cudaEventDestroy(ctx->join);
+    if (ctx->side) cudaStreamDestroy(ctx->side);
     if (ctx->stream) cudaStreamDestroy(ctx->stream);
     delete ctx;
 }

@@ -56,7 +56,14 @@ WORKLOADS = {
                  metric="MPix/s (plain 100-iteration solve, 6000x4000 4:4:4 q30)", iterations=100),
     "batch256": dict(name="256 JPEGs, W,H~U[256,2048] (x16), 4:2:0|4:4:4 p=.5, q~U[20,90], one batch, 50 iterations",
                      metric="MPix/s (plain 50-iteration batched solve, 256 images)", iterations=50),
+    "learned": dict(name="1920x1080 YCbCr 4:2:0 baseline JPEGs at q30/50/75: learned warm start + 8 plain "
+                         "iterations against the plain 50-iteration solve",
+                    metric="MPix/s to the plain 50-iteration objective (learned warm start + 8 iterations, "
+                           "1080p 4:2:0 q30/50/75)", iterations=8),
 }
+LEARNED_QUALITIES = (30, 50, 75)
+REFINE_ITERATIONS = 8
+REFINE_STEP_ITERATIONS = 50  # refinement steps of the 50-iteration run's size
 WEIGHT, PWEIGHT = 0.3, 0.001
 
 
@@ -210,6 +217,221 @@ def oracle_solve(jpeg, iterations):
     return oracle_lib.compute(jpeg.nchannel, jpeg.coefs, WEIGHT, [PWEIGHT] * 3, iterations, W, H)
 
 
+class DeviceImage:
+    """One decoded JPEG with its coefficients and result planes in HBM."""
+
+    def __init__(self, jpeg):
+        import torch
+
+        from artefact_b200 import _native as N
+
+        self.jpeg = jpeg
+        self.W, self.H, _ = jpeg.max_rounded()
+        self.n = jpeg.nchannel
+        self.keep = []
+        self.ch = (N.ArtChannel * self.n)()
+        for c, co in enumerate(jpeg.coefs):
+            dev = torch.from_numpy(co.dct_coefs.copy()).cuda()
+            q = np.ascontiguousarray(co.quant_table, np.float32)
+            self.keep += [dev, q]
+            a = self.ch[c]
+            a.rounded_px_w, a.rounded_px_h, a.block_w, a.block_h = co.rounded_px_w, co.rounded_px_h, co.block_w, co.block_h
+            a.samp_h, a.samp_v, a.coef_type = co.horizontal_samp_factor, co.vertical_samp_factor, N.ART_COEF_I16
+            a.dct_coefs = dev.data_ptr()
+            a.quant_table = q.ctypes.data_as(C.POINTER(C.c_float))
+        self.pitch = (self.W + 31) // 32 * 32
+        self.outs = [torch.empty(self.H, self.pitch, device="cuda") for _ in range(self.n)]
+        self.ptrs = (C.c_void_p * self.n)(*[o.data_ptr() for o in self.outs])
+
+    def solve(self, lib, ctx, iterations, init_mode, step_iterations, stream):
+        from artefact_b200 import _native as N
+
+        opts = N.ArtOptions()
+        opts.init_mode, opts.device, opts.step_iterations = init_mode, -1, step_iterations
+        pw = (C.c_float * 3)(PWEIGHT, PWEIGHT, PWEIGHT)
+        N.check(lib.art_context_compute_device(ctx, self.n, self.ch, WEIGHT, pw, iterations, self.W, self.H,
+                                               self.ptrs, self.pitch, C.byref(opts), C.c_void_p(stream.cuda_stream)))
+
+
+def learned_comparison(lib, device, steps, warmup, refine=REFINE_ITERATIONS, step_iterations=REFINE_STEP_ITERATIONS,
+                       qualities=LEARNED_QUALITIES):
+    """Learned warm start + `refine` plain iterations against the plain
+    50-iteration solve, per quality, on seeded 1920x1080 4:2:0 JPEGs (seeds
+    5000 + quality, outside the network's training seeds). Each path is timed
+    from device-resident coefficients to device-resident planes (CUDA events,
+    L2 flushed between steps); its objective and feasibility come from
+    art_context_evaluate. Also reports the fewest refinement iterations (of a
+    fixed ladder) whose objective reaches the plain 50-iteration one within
+    1e-4 relative. None when the package holds no trained weights."""
+    import torch
+
+    from artefact_b200 import _native as N
+    from artefact_b200 import synth
+    from artefact_b200 import warmstart as WS
+    from artefact_b200.api import Jpeg, JpegSource
+
+    if not WS.DEFAULT_WEIGHTS.exists():
+        return None
+    net = WS.WarmStartNet.load(device=device)
+    ctx = C.c_void_p()
+    N.check(lib.art_context_create(device, C.byref(ctx)))
+    N.check(lib.art_context_set_warm_start(ctx, net.handle))
+    stream = torch.cuda.current_stream()
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")
+
+    def evaluate():
+        out = (C.c_double * 5)()
+        N.check(lib.art_context_evaluate(ctx, 0, out))
+        return out[0], out[4]
+
+    def timed(img, its, mode, step_its):
+        for _ in range(warmup):
+            flush.fill_(1.0)
+            img.solve(lib, ctx, its, mode, step_its, stream)
+        torch.cuda.synchronize()
+        ms = []
+        for k in range(steps):
+            flush.fill_(float(k))
+            a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            a.record(stream)
+            img.solve(lib, ctx, its, mode, step_its, stream)
+            b.record(stream)
+            b.synchronize()
+            ms.append(a.elapsed_time(b))
+        N.check(lib.art_context_synchronize(ctx))
+        return statistics.median(ms)
+
+    rows = []
+    ladder = (2, 4, 6, 8, 12, 16, 24, 32, 48)
+    for q in qualities:
+        j = Jpeg.from_source(JpegSource.Buffer(synth.make_jpeg(1920, 1080, q, "4:2:0", False, seed=5000 + q)))
+        img = DeviceImage(j)
+        mpix = j.real_px_w * j.real_px_h / 1e6
+        plain_ms = timed(img, 50, N.ART_INIT_DECODED, 0)
+        e50, f50 = evaluate()
+        learned_ms = timed(img, refine, N.ART_INIT_LEARNED, step_iterations)
+        el, fl = evaluate()
+        img.solve(lib, ctx, refine, N.ART_INIT_DECODED, step_iterations, stream)
+        ed, _ = evaluate()
+        kmin = None
+        for k in ladder:
+            img.solve(lib, ctx, k, N.ART_INIT_LEARNED, step_iterations, stream)
+            ek, fk = evaluate()
+            if ek <= e50 * (1 + 1e-4) and fk <= 1e-3:
+                kmin = k
+                break
+        kmin_ms = timed(img, kmin, N.ART_INIT_LEARNED, step_iterations) if kmin else None
+        rows.append(dict(quality=q, plain50_ms=plain_ms, plain50_mpix_s=mpix / plain_ms * 1e3,
+                         learned_ms=learned_ms, learned_mpix_s=mpix / learned_ms * 1e3,
+                         speedup=plain_ms / learned_ms, E_plain50=e50, E_learned=el,
+                         E_learned_rel=(el - e50) / e50, E_decoded_same_iterations=ed,
+                         infeasibility_learned=fl, infeasibility_plain=f50,
+                         reaches_plain50=bool(el <= e50 * (1 + 1e-4) and fl <= 1e-3),
+                         min_refine_to_reach=kmin,
+                         min_refine_ms=kmin_ms, min_refine_speedup=(plain_ms / kmin_ms) if kmin_ms else None))
+        log(f"learned q{q}: plain50 {plain_ms:.3f} ms E {e50:.7g}; learned+{refine} {learned_ms:.3f} ms "
+            f"E {el:.7g} ({(el - e50) / e50:+.2e}); decoded+{refine} E {ed:.7g}; reach at K={kmin}")
+    lib.art_context_set_warm_start(ctx, None)
+    lib.art_context_destroy(ctx)
+    net.close()
+    mp_total = sum(1920 * 1080 / 1e6 for _ in rows)
+    return dict(refine_iterations=refine, refine_step_iterations=step_iterations, images=rows,
+                plain50_mpix_s=mp_total / sum(r["plain50_ms"] for r in rows) * 1e3,
+                learned_mpix_s=mp_total / sum(r["learned_ms"] for r in rows) * 1e3,
+                all_reach_plain50=all(r["reaches_plain50"] for r in rows))
+
+
+def network_flops(H, W):
+    """Multiply-add FLOPs (x2) of one forward pass of the warm-start network
+    on an H x W component, as executed (input features padded to 16 channels,
+    head to 16 outputs)."""
+    P0, P1, P2, P3 = H * W, (H // 2) * (W // 2), (H // 4) * (W // 4), (H // 8) * (W // 8)
+    macs = 9 * (16 * 32 * P0 + 32 * 64 * P1 + 64 * 96 * P2 + 96 * 128 * P3 + 224 * 96 * P2 + 160 * 64 * P1
+                + 96 * 32 * P0 + 32 * 16 * P0)
+    return 2 * macs
+
+
+def time_network(device, steps, warmup):
+    """The network's forward pass on one 1080p 4:2:0 image (luma 1920x1088,
+    then both chroma planes of 960x544 as a batch of two), CUDA events:
+    (ms, TFLOP/s)."""
+    import torch
+
+    from artefact_b200 import synth
+    from artefact_b200 import warmstart as WS
+    from artefact_b200.api import Jpeg, JpegSource
+
+    j = Jpeg.from_source(JpegSource.Buffer(synth.make_jpeg(1920, 1080, 50, "4:2:0", False, seed=5050)))
+    net = WS.WarmStartNet.load(device=device) if WS.DEFAULT_WEIGHTS.exists() else WS.WarmStartNet(device=device)
+    groups = [[j.coefs[0]], j.coefs[1:]]
+    inputs = []
+    flops = 0
+    for g in groups:
+        c = torch.from_numpy(np.stack([WS.coef_image(co) for co in g])).cuda()
+        q = torch.from_numpy(np.stack([np.asarray(co.quant_table, np.float32) for co in g])).cuda()
+        inputs.append((c, q))
+        flops += len(g) * network_flops(c.shape[1], c.shape[2])
+    outs = [net.predict(c, q) for c, q in inputs]
+    for _ in range(warmup):
+        for (c, q), o in zip(inputs, outs):
+            net.predict(c, q, out=o)
+    torch.cuda.synchronize()
+    ms = []
+    for _ in range(steps):
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record()
+        for (c, q), o in zip(inputs, outs):
+            net.predict(c, q, out=o)
+        b.record()
+        b.synchronize()
+        ms.append(a.elapsed_time(b))
+    net.close()
+    t = statistics.median(ms)
+    return t, flops / (t * 1e-3) / 1e12, flops
+
+
+def run_learned(args, lib, local, rank, world, dist):
+    """Config 5: learned warm start + 8 plain iterations vs the plain 50-iteration solve."""
+    import torch
+
+    wl = WORKLOADS["learned"]
+    with Clocks(local) as clk:
+        res = learned_comparison(lib, local, args.steps, args.warmup)
+    if res is None:
+        if rank == 0:
+            print(json.dumps({"metric": wl["metric"], "unavailable": "no trained warm-start weights in the package"}))
+        return
+    net_ms, net_tflops, net_flops = time_network(local, args.steps, args.warmup)
+    peaks = json.loads((ROOT / "MEASURED_PEAKS.json").read_text()) if (ROOT / "MEASURED_PEAKS.json").exists() else {}
+    tc_peak = float(peaks.get("bf16_tflops", 1590.0))
+    value = res["learned_mpix_s"]
+    total_ms = sum(r["learned_ms"] for r in res["images"])
+    if dist:
+        t = torch.tensor([total_ms], device="cuda", dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        total_ms = float(t.item())
+        value = world * len(res["images"]) * 1920 * 1080 / 1e6 / (total_ms * 1e-3)
+    if rank == 0:
+        line = {
+            "metric": wl["metric"], "value": value, "unit": "MPix/s", "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": total_ms / len(res["images"]), "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32 solver, bf16 network (fp32 accumulation)",
+            "data": "synthetic",
+            "config": {"workload": wl["name"], "refine_iterations": res["refine_iterations"],
+                       "refine_step_iterations": res["refine_step_iterations"],
+                       "l2": "flushed between steps (256 MiB write outside the timed events)",
+                       "parallelism": f"replicas x{world}"},
+            "plain50_mpix_s": res["plain50_mpix_s"], "speedup_vs_plain50": value / res["plain50_mpix_s"],
+            "all_reach_plain50": res["all_reach_plain50"], "images": res["images"],
+            "roofline": {"bound": "tensor", "kernel": "warm-start network forward (k_conv3x3 and glue)",
+                         "achieved": net_tflops, "peak": tc_peak, "unit": "TFLOP/s", "frac": net_tflops / tc_peak,
+                         "traffic": None, "peak_kind": "measured" if peaks else "fallback",
+                         "algorithmic_flops_per_launch": net_flops, "launch_ms": net_ms},
+            "e2e": None, "cpu_baseline": None, "clocks": clk.summary(),
+        }
+        print(json.dumps(line), flush=True)
+
+
 def cpu_sample(kind, jpegs, iterations):
     """Bounded CPU measurement of the oracle: (MPix/s, description)."""
     real = sum(j.real_px_w * j.real_px_h for j in jpegs) / 1e6
@@ -315,6 +537,9 @@ def main():
 
     lib = N.lib()
     wl = WORKLOADS[args.workload]
+    if args.workload == "learned":
+        run_learned(args, lib, local, rank, world, dist)
+        return
     iters = wl["iterations"]
     jpegs = make_workload(args.workload)
     nimg = len(jpegs)

@@ -242,10 +242,16 @@ def test_network_gradients_match_oracle(gpu):
 
 
 def test_training_reduces_loss(gpu):
+    """A residual the network can represent -- the decoded image smoothed by a
+    3x3 box filter, minus itself -- is learned: the loss falls well below its
+    starting value (where the prediction is about the decoded image)."""
     torch = _torch()
-    coef, q, target = _batch(3, B=4, H=64, W=64)
+    coef, q, _ = _batch(3, B=4, H=64, W=64)
+    dec, _ = O.features(coef, q)
+    pad = np.pad(dec, ((0, 0), (1, 1), (1, 1)), mode="edge")
+    target = sum(pad[:, 1 + dy:1 + dy + 64, 1 + dx:1 + dx + 64] for dy in (-1, 0, 1) for dx in (-1, 0, 1)) / 9.0
     net = WS.WarmStartNet(WS.init_params(5))
-    c, qq, t = torch.from_numpy(coef).cuda(), _f32(q), _f32(target)
-    losses = [net.train_step(c, qq, t, lr=2e-3) for _ in range(30)]
-    assert losses[-1] < 0.7 * losses[0], losses
+    c, qq, t = torch.from_numpy(coef).cuda(), _f32(q), _f32(target.astype(np.float32))
+    losses = [net.train_step(c, qq, t, lr=2e-3) for _ in range(100)]
     assert all(np.isfinite(losses))
+    assert losses[-1] < 0.5 * losses[0], losses[::10]
