@@ -597,60 +597,91 @@ __global__ void k_colsum_final(const float *__restrict__ partial, int nblk, int 
 }
 
 // Network input from a coefficient image: per 8x8 block the decoded samples
-// IDCT(c * q) (level-shifted, as the solver's start) into dec (fp32) and the
-// feature tensor F[B][H][W][16] (bf16): channel 0 = decoded / 128, channel 1
-// = the block's quantisation step of the sample's frequency position / 64,
-// channels 2-15 = 0.
+// IDCT(c * q) (level-shifted, as the solver's start) into dec (fp32
+// [B][H][W]) and the feature tensor F[B][H0][W0][16] (bf16) on the network's
+// half-resolution grid (H0 = ceil(H / 16) * 8, W0 likewise): level-0 pixel
+// (y, x) holds the 2x2 cell of samples (2y + dy, 2x + dx) -- channel 2 dy + dx
+// = decoded / 128, channel 4 + 2 dy + dx = the quantisation step of that
+// sample's frequency position / 64, channels 8-15 = 0; cells outside the
+// component are zero. One thread per 8x8 block of the padded block grid
+// (4x4 level-0 pixels).
 __global__ void k_features(const int16_t *__restrict__ coef, int cpitch, long long img_stride, const float *__restrict__ q,
                            int B, int H, int W, float *__restrict__ dec, bf16 *__restrict__ feat)
 {
     const int bw = W / 8, bh = H / 8;
+    const int W0 = (W + 15) / 16 * 8, H0 = (H + 15) / 16 * 8;
+    const int pbw = W0 / 4, pbh = H0 / 4;  // padded block grid
     const long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
-    if (i >= (long long)B * bw * bh) return;
-    const int bx = (int)(i % bw), by = (int)((i / bw) % bh), b = (int)(i / ((long long)bw * bh));
+    if (i >= (long long)B * pbw * pbh) return;
+    const int bx = (int)(i % pbw), by = (int)((i / pbw) % pbh), b = (int)(i / ((long long)pbw * pbh));
+    const bool real = bx < bw && by < bh;
     const float *qt = q + (size_t)b * 64;
     float a[64];
-    for (int r = 0; r < 8; r++) {
-        float c8[8];
-        load_coef_row(coef + b * img_stride + (size_t)(by * 8 + r) * cpitch + bx * 8, c8);
+    if (real) {
+        for (int r = 0; r < 8; r++) {
+            float c8[8];
+            load_coef_row(coef + b * img_stride + (size_t)(by * 8 + r) * cpitch + bx * 8, c8);
 #pragma unroll
-        for (int u = 0; u < 8; u++) a[r * 8 + u] = c8[u] * __ldg(qt + r * 8 + u);
+            for (int u = 0; u < 8; u++) a[r * 8 + u] = c8[u] * __ldg(qt + r * 8 + u);
+        }
+        idct8x8_regs(a);
+        for (int r = 0; r < 8; r++) {
+            const size_t p0 = ((size_t)b * H + by * 8 + r) * W + bx * 8;
+#pragma unroll
+            for (int u = 0; u < 8; u++) dec[p0 + u] = a[r * 8 + u];
+        }
     }
-    idct8x8_regs(a);
-    for (int r = 0; r < 8; r++) {
-        const size_t p0 = ((size_t)b * H + by * 8 + r) * W + bx * 8;
-#pragma unroll
-        for (int u = 0; u < 8; u++) {
-            dec[p0 + u] = a[r * 8 + u];
+    for (int yy = 0; yy < 4; yy++)
+        for (int xx = 0; xx < 4; xx++) {
             uint4 o[2] = {make_uint4(0, 0, 0, 0), make_uint4(0, 0, 0, 0)};
-            __nv_bfloat162 *w = reinterpret_cast<__nv_bfloat162 *>(o);
-            w[0] = __floats2bfloat162_rn(a[r * 8 + u] * (1.f / 128.f), __ldg(qt + r * 8 + u) * (1.f / 64.f));
-            uint4 *f = reinterpret_cast<uint4 *>(feat + (p0 + u) * 16);
+            if (real) {
+                bf16 *w = reinterpret_cast<bf16 *>(o);
+#pragma unroll
+                for (int k = 0; k < 4; k++) {
+                    const int r = 2 * yy + (k >> 1), u = 2 * xx + (k & 1);
+                    w[k] = __float2bfloat16_rn(a[r * 8 + u] * (1.f / 128.f));
+                    w[4 + k] = __float2bfloat16_rn(__ldg(qt + r * 8 + u) * (1.f / 64.f));
+                }
+            }
+            uint4 *f = reinterpret_cast<uint4 *>(feat + (((size_t)b * H0 + by * 4 + yy) * W0 + bx * 4 + xx) * 16);
             f[0] = o[0];
             f[1] = o[1];
         }
-    }
 }
 
-// Residual head output r (fp32, channel 0 of rows of `rstride`) -> prediction
-// x = dec + 16 r; with a target: gradient of the mean squared error in
-// units of 16 levels into grad[p][16] (channel 0, others zero) and per-block
-// partial sums of the squared error.
+// Residual head output r (fp32 [B][H0][W0][rstride], channels 0-3 = the 2x2
+// cell of a level-0 pixel, channel 2 dy + dx) -> prediction x = dec + 16 r at
+// full resolution [B][H][W]; with a target: gradient of the mean squared error
+// over the B H W samples (in units of 16 levels) into grad[B][H0][W0][16]
+// (channels 0-3; the rest and cells outside the component zero) and per-block
+// partial sums of the squared error. One thread per level-0 pixel.
 __global__ void k_residual(const float *__restrict__ r, int rstride, const float *__restrict__ dec,
-                           const float *__restrict__ target, long long npix, float inv_count, float *__restrict__ pred,
-                           bf16 *__restrict__ grad, float *__restrict__ loss_partial)
+                           const float *__restrict__ target, int B, int H, int W, float inv_count,
+                           float *__restrict__ pred, bf16 *__restrict__ grad, float *__restrict__ loss_partial)
 {
     __shared__ float s[256];
+    const int W0 = (W + 15) / 16 * 8, H0 = (H + 15) / 16 * 8;
+    const long long n0 = (long long)B * H0 * W0;
     float acc = 0.f;
-    for (long long p = blockIdx.x * (long long)blockDim.x + threadIdx.x; p < npix; p += (long long)gridDim.x * blockDim.x) {
-        const float rv = r[p * rstride];
-        const float d = dec[p];
-        if (pred) pred[p] = d + 16.f * rv;
+    for (long long p = blockIdx.x * (long long)blockDim.x + threadIdx.x; p < n0; p += (long long)gridDim.x * blockDim.x) {
+        const int x = (int)(p % W0), y = (int)((p / W0) % H0), b = (int)(p / ((long long)W0 * H0));
+        uint4 o[2] = {make_uint4(0, 0, 0, 0), make_uint4(0, 0, 0, 0)};
+        bf16 *gv = reinterpret_cast<bf16 *>(o);
+#pragma unroll
+        for (int k = 0; k < 4; k++) {
+            const int Y = 2 * y + (k >> 1), X = 2 * x + (k & 1);
+            if (Y >= H || X >= W) continue;
+            const size_t q = ((size_t)b * H + Y) * W + X;
+            const float rv = r[p * rstride + k];
+            const float d = dec[q];
+            if (pred) pred[q] = d + 16.f * rv;
+            if (target) {
+                const float e = rv - (target[q] - d) * (1.f / 16.f);
+                acc += e * e;
+                gv[k] = __float2bfloat16_rn(2.f * e * inv_count);
+            }
+        }
         if (target) {
-            const float e = rv - (target[p] - d) * (1.f / 16.f);
-            acc += e * e;
-            uint4 o[2] = {make_uint4(0, 0, 0, 0), make_uint4(0, 0, 0, 0)};
-            reinterpret_cast<bf16 *>(o)[0] = __float2bfloat16_rn(2.f * e * inv_count);
             uint4 *g = reinterpret_cast<uint4 *>(grad + p * 16);
             g[0] = o[0];
             g[1] = o[1];
@@ -936,20 +967,22 @@ int32_t art_cnn_features(const int16_t *coef, int32_t cpitch, int64_t img_stride
 {
     if (!coef || !q || !dec || !feat || H % 8 || W % 8 || cpitch < W || cpitch % 8)
         return fail(ART_ERR_INVALID_ARGUMENT, "features: bad arguments");
-    const long long n = (long long)B * (H / 8) * (W / 8);
+    const long long n = (long long)B * ((H + 15) / 16 * 2) * ((W + 15) / 16 * 2);
     k_features<<<blocks_for(n, 128), 128, 0, static_cast<cudaStream_t>(stream)>>>(coef, cpitch, img_stride, q, B, H, W,
                                                                                 dec, static_cast<bf16 *>(feat));
     return check_launch("k_features");
 }
 
-int32_t art_cnn_residual(const float *r, int32_t rstride, const float *dec, const float *target, int64_t npix,
-                         float *pred, void *grad, float *loss_partial, int32_t loss_blocks, void *stream)
+int32_t art_cnn_residual(const float *r, int32_t rstride, const float *dec, const float *target, int32_t B,
+                         int32_t H, int32_t W, float *pred, void *grad, float *loss_partial, int32_t loss_blocks,
+                         void *stream)
 {
-    if (!r || !dec || (target && (!grad || !loss_partial)) || loss_blocks < 1)
+    if (!r || !dec || (target && (!grad || !loss_partial)) || loss_blocks < 1 || rstride < 4 || B < 1 || H < 1 ||
+        W < 1)
         return fail(ART_ERR_INVALID_ARGUMENT, "residual: bad arguments");
+    const long long npix = (long long)B * H * W;
     k_residual<<<loss_blocks, 256, 0, static_cast<cudaStream_t>(stream)>>>(
-        r, rstride, dec, target, npix, npix > 0 ? 1.f / (float)npix : 0.f, pred, static_cast<bf16 *>(grad),
-        loss_partial);
+        r, rstride, dec, target, B, H, W, 1.f / (float)npix, pred, static_cast<bf16 *>(grad), loss_partial);
     return check_launch("k_residual");
 }
 
@@ -1042,7 +1075,8 @@ struct ArtNet {
     // activations (forward) and gradients (training)
     art::cnn::Buf feat, dec, cat1, cat2, cat3, p1, p2, p3, e4, d3, d2, d1, r, pred;
     art::cnn::Buf dr, gd1, ge1, gup1, gd2, ge2, gup2, gd3, ge3, gup3, ge4, gp3, gp2, gp1;
-    long long cap_px = 0;  // level-0 pixels the buffers hold
+    long long cap_px = 0;    // level-0 pixels the activation buffers hold
+    long long cap_full = 0;  // full-resolution samples the decoded/prediction buffers hold
     bool cap_train = false;
 };
 
@@ -1052,21 +1086,24 @@ namespace cnn {
 constexpr int LOSS_BLOCKS = 296;
 constexpr size_t WORKSPACE_BYTES = 64ull << 20;
 
-int32_t net_alloc(ArtNet *net, long long px, bool train)
+// Buffers for px level-0 pixels (activations) and full full-resolution
+// samples (decoded image, prediction).
+int32_t net_alloc(ArtNet *net, long long px, long long full, bool train)
 {
-    if (px <= net->cap_px && (!train || net->cap_train)) return ART_OK;
+    if (px <= net->cap_px && full <= net->cap_full && (!train || net->cap_train)) return ART_OK;
     px = std::max(px, net->cap_px);
+    full = std::max(full, net->cap_full);
     train = train || net->cap_train;
-    const size_t P0 = (size_t)px, P1 = P0 / 4 + 64, P2 = P0 / 16 + 64, P3 = P0 / 64 + 64;
+    const size_t P0 = (size_t)px, P1 = P0 / 4 + 64, P2 = P0 / 16 + 64, P3 = P0 / 64 + 64, PF = (size_t)full;
     struct Req {
         Buf *b;
         size_t bytes;
     };
     std::vector<Req> req = {
-        {&net->feat, P0 * 16 * 2}, {&net->dec, P0 * 4},       {&net->cat1, P0 * 96 * 2}, {&net->cat2, P1 * 160 * 2},
+        {&net->feat, P0 * 16 * 2}, {&net->dec, PF * 4},       {&net->cat1, P0 * 96 * 2}, {&net->cat2, P1 * 160 * 2},
         {&net->cat3, P2 * 224 * 2}, {&net->p1, P1 * 32 * 2},   {&net->p2, P2 * 64 * 2},   {&net->p3, P3 * 96 * 2},
         {&net->e4, P3 * 128 * 2},  {&net->d3, P2 * 96 * 2},   {&net->d2, P1 * 64 * 2},   {&net->d1, P0 * 32 * 2},
-        {&net->r, P0 * 16 * 4},    {&net->pred, P0 * 4},
+        {&net->r, P0 * 16 * 4},    {&net->pred, PF * 4},
     };
     if (train) {
         std::vector<Req> t = {
@@ -1080,6 +1117,7 @@ int32_t net_alloc(ArtNet *net, long long px, bool train)
     for (auto &q : req)
         if (!q.b->ensure(q.bytes)) return fail(ART_ERR_CUDA, "network buffers: cudaMalloc failed");
     net->cap_px = px;
+    net->cap_full = full;
     net->cap_train = train;
     return ART_OK;
 }
@@ -1243,6 +1281,10 @@ int32_t net_backward(ArtNet *net, int B, int H, int W, cudaStream_t s)
     return ART_OK;
 }
 
+// Side of the network's first (half-resolution) level for a component side n:
+// n padded to a multiple of 16, halved, so that three 2x2 poolings divide it.
+int level0(int n) { return (n + 15) / 16 * 8; }
+
 int32_t check_geometry(int B, int H, int W)
 {
     if (B < 1 || H < 8 || W < 8 || H % 8 || W % 8)
@@ -1267,12 +1309,13 @@ int32_t net_predict(ArtNet *net, const int16_t *coef, int cpitch, long long img_
                     int W, float *pred, cudaStream_t s)
 {
     NET_TRY(check_geometry(B, H, W));
-    NET_TRY(net_alloc(net, (long long)B * H * W, false));
+    const int H0 = level0(H), W0 = level0(W);
+    NET_TRY(net_alloc(net, (long long)B * H0 * W0, (long long)B * H * W, false));
     if (!net->packed) NET_TRY(net_pack(net, false, s));
     NET_TRY(art_cnn_features(coef, cpitch, img_stride, q, B, H, W, net->dec.as<float>(), net->feat.p, s));
-    NET_TRY(net_forward(net, B, H, W, s));
-    return art_cnn_residual(net->r.as<float>(), 16, net->dec.as<float>(), nullptr, (int64_t)B * H * W,
-                            pred ? pred : net->pred.as<float>(), nullptr, nullptr, 1, s);
+    NET_TRY(net_forward(net, B, H0, W0, s));
+    return art_cnn_residual(net->r.as<float>(), 16, net->dec.as<float>(), nullptr, B, H, W,
+                            pred ? pred : net->pred.as<float>(), nullptr, nullptr, 148, s);
 }
 
 int32_t net_predict_async(ArtNet *net, const int16_t *coef, int cpitch, long long img_stride, const float *q, int B,
@@ -1387,7 +1430,8 @@ int32_t art_net_train_step(ArtNet *net, const int16_t *coef, int32_t cpitch, int
     cudaSetDevice(net->device);
     cudaStream_t s = static_cast<cudaStream_t>(stream);
     NET_TRY(check_geometry(B, H, W));
-    NET_TRY(net_alloc(net, (long long)B * H * W, true));
+    const int H0 = level0(H), W0 = level0(W);
+    NET_TRY(net_alloc(net, (long long)B * H0 * W0, (long long)B * H * W, true));
     const size_t pb = (size_t)net->nparam * 4;
     if (!net->grads.p) {
         if (!net->grads.ensure(pb) || !net->adam_m.ensure(pb) || !net->adam_v.ensure(pb) ||
@@ -1396,11 +1440,11 @@ int32_t art_net_train_step(ArtNet *net, const int16_t *coef, int32_t cpitch, int
     }
     NET_TRY(net_pack(net, true, s));
     NET_TRY(art_cnn_features(coef, cpitch, img_stride, q, B, H, W, net->dec.as<float>(), net->feat.p, s));
-    NET_TRY(net_forward(net, B, H, W, s));
+    NET_TRY(net_forward(net, B, H0, W0, s));
     const long long npix = (long long)B * H * W;
-    NET_TRY(art_cnn_residual(net->r.as<float>(), 16, net->dec.as<float>(), target, npix, net->pred.as<float>(),
+    NET_TRY(art_cnn_residual(net->r.as<float>(), 16, net->dec.as<float>(), target, B, H, W, net->pred.as<float>(),
                              net->dr.p, net->loss_partial.as<float>(), LOSS_BLOCKS, s));
-    NET_TRY(net_backward(net, B, H, W, s));
+    NET_TRY(net_backward(net, B, H0, W0, s));
     if (lr > 0.f) {
         net->step++;
         NET_TRY(art_cnn_adam(net->params.as<float>(), net->grads.as<float>(), net->adam_m.as<float>(),

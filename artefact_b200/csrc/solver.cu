@@ -106,17 +106,20 @@ __global__ void __launch_bounds__(SWEEP_WARPS * 32) k_grad_sweep(const ImgDev *_
             return __ldg(reinterpret_cast<const float2 *>(p));
         };
 
-        float2 yv[NCH], dxp[NCH], dyp[NCH], Gm[NCH], G0[NCH], Gp[NCH], q1[NCH], q2[NCH], p1[NCH];
+        // Rows in flight: ring[c][k] holds y row t + 1 + k at step t (SWEEP_PF rows
+        // ahead of use), pring[c][k] the DCT-distance row t - 1 + k (the output row
+        // of step t and SWEEP_PPF - 1 more).
+        float2 yv[NCH], dxp[NCH], dyp[NCH], Gm[NCH], G0[NCH], Gp[NCH], ring[NCH][SWEEP_PF], pring[NCH][SWEEP_PPF];
         {
             const int o0 = min(max(ys - 2, 0), Hm1) * pitch, o1 = min(max(ys - 1, 0), Hm1) * pitch;
-            const int o2 = min(ys, Hm1) * pitch, o3 = min(ys + 1, Hm1) * pitch;
 #pragma unroll
             for (int c = 0; c < NCH; c++) {
                 const float2 y0 = ld(c, o0);
                 yv[c] = ld(c, o1);
-                q1[c] = ld(c, o2);
-                q2[c] = ld(c, o3);
-                p1[c] = pld(c, max(ys - 2, 0));  // output row of step ys - 1
+#pragma unroll
+                for (int k = 0; k < SWEEP_PF; k++) ring[c][k] = ld(c, min(ys + k, Hm1) * pitch);
+#pragma unroll
+                for (int k = 0; k < SWEEP_PPF; k++) pring[c][k] = pld(c, min(max(ys - 2 + k, 0), Hm1));
                 const float yr = __shfl_down_sync(FULL, y0.x, 1);
                 dxp[c] = f2sub(make_float2(y0.y, yr), y0);
                 dyp[c] = f2sub(yv[c], y0);
@@ -126,15 +129,18 @@ __global__ void __launch_bounds__(SWEEP_WARPS * 32) k_grad_sweep(const ImgDev *_
         for (int t = ys - 1; t <= ys + R; t++) {
             float2 yn[NCH], pr[NCH];
             {
-                const int o = min(t + 3, Hm1) * pitch;
-                const int prow = min(max(t, 0), Hm1);
+                const int o = min(t + 1 + SWEEP_PF, Hm1) * pitch;
+                const int prow = min(max(t - 1 + SWEEP_PPF, 0), Hm1);
 #pragma unroll
                 for (int c = 0; c < NCH; c++) {
-                    yn[c] = q1[c];
-                    q1[c] = q2[c];
-                    q2[c] = ld(c, o);
-                    pr[c] = p1[c];
-                    p1[c] = pld(c, prow);
+                    yn[c] = ring[c][0];
+#pragma unroll
+                    for (int k = 0; k + 1 < SWEEP_PF; k++) ring[c][k] = ring[c][k + 1];
+                    ring[c][SWEEP_PF - 1] = ld(c, o);
+                    pr[c] = pring[c][0];
+#pragma unroll
+                    for (int k = 0; k + 1 < SWEEP_PPF; k++) pring[c][k] = pring[c][k + 1];
+                    pring[c][SWEEP_PPF - 1] = pld(c, prow);
                 }
             }
             const bool rowin = t >= 0 && t < H, ty0 = t > 0;
@@ -313,17 +319,22 @@ __global__ void __launch_bounds__(SWEEP_WARPS_N * 32) k_grad_sweep_n(const ImgDe
         const int Hm1 = H - 1;
         auto yrow = [&](int row) -> int { return min(max(row, 0), Hm1) * pitch; };
 
-        float yv[NCH], dxp[NCH], dyp[NCH], Gm[NCH], G0[NCH], Gp[NCH], q1[NCH], q2[NCH], p1[NCH];
+        // Rows in flight, as in the wide variant: ring[c][k] = y row t + 1 + k,
+        // pring[c][k] = DCT-distance row t - 1 + k at step t.
+        float yv[NCH], dxp[NCH], dyp[NCH], Gm[NCH], G0[NCH], Gp[NCH], ring[NCH][SWEEP_PF_N], pring[NCH][SWEEP_PPF_N];
         {
-            const int o0 = yrow(ys - 2), o1 = yrow(ys - 1), o2 = yrow(ys), o3 = yrow(ys + 1);
-            const int r0 = max(ys - 2, 0);
+            const int o0 = yrow(ys - 2), o1 = yrow(ys - 1);
 #pragma unroll
             for (int c = 0; c < NCH; c++) {
                 const float y0 = __ldg(yp + c * cs + o0);
                 yv[c] = __ldg(yp + c * cs + o1);
-                q1[c] = __ldg(yp + c * cs + o2);
-                q2[c] = __ldg(yp + c * cs + o3);
-                p1[c] = pon[c] ? __ldg(pbase + pcol[c] + (r0 >> psh[c]) * ppitch[c]) : 0.f;  // output row of step ys - 1
+#pragma unroll
+                for (int k = 0; k < SWEEP_PF_N; k++) ring[c][k] = __ldg(yp + c * cs + yrow(ys + k));
+#pragma unroll
+                for (int k = 0; k < SWEEP_PPF_N; k++) {
+                    const int r = min(max(ys - 2 + k, 0), Hm1);
+                    pring[c][k] = pon[c] ? __ldg(pbase + pcol[c] + (r >> psh[c]) * ppitch[c]) : 0.f;
+                }
                 dxp[c] = __shfl_down_sync(FULL, y0, 1) - y0;
                 dyp[c] = yv[c] - y0;
                 Gm[c] = G0[c] = Gp[c] = 0.f;
@@ -332,15 +343,18 @@ __global__ void __launch_bounds__(SWEEP_WARPS_N * 32) k_grad_sweep_n(const ImgDe
         for (int t = ys - 1; t <= ys + R; t++) {
             float yn[NCH], pr[NCH];
             {
-                const int o = min(t + 3, Hm1) * pitch;
-                const int pr1 = min(max(t, 0), Hm1);
+                const int o = min(t + 1 + SWEEP_PF_N, Hm1) * pitch;
+                const int pr1 = min(max(t - 1 + SWEEP_PPF_N, 0), Hm1);
 #pragma unroll
                 for (int c = 0; c < NCH; c++) {
-                    yn[c] = q1[c];
-                    q1[c] = q2[c];
-                    q2[c] = __ldg(yp + c * cs + o);
-                    pr[c] = p1[c];
-                    p1[c] = pon[c] ? __ldg(pbase + pcol[c] + (pr1 >> psh[c]) * ppitch[c]) : 0.f;
+                    yn[c] = ring[c][0];
+#pragma unroll
+                    for (int k = 0; k + 1 < SWEEP_PF_N; k++) ring[c][k] = ring[c][k + 1];
+                    ring[c][SWEEP_PF_N - 1] = __ldg(yp + c * cs + o);
+                    pr[c] = pring[c][0];
+#pragma unroll
+                    for (int k = 0; k + 1 < SWEEP_PPF_N; k++) pring[c][k] = pring[c][k + 1];
+                    pring[c][SWEEP_PPF_N - 1] = pon[c] ? __ldg(pbase + pcol[c] + (pr1 >> psh[c]) * ppitch[c]) : 0.f;
                 }
             }
             const bool inside = colin && t >= 0 && t < H;

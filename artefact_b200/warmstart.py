@@ -1,7 +1,10 @@
 """Learned warm start for the restoration solver.
 
 A 4-level encoder-decoder CNN predicts, per channel, the converged solver
-output from the decoded channel and its quantisation table. Its forward and
+output from the decoded channel and its quantisation table. It runs at half
+the component's resolution: each first-level pixel carries a 2x2 cell of
+samples (space to depth), and the head's first four outputs are the cell's
+residuals. Its forward and
 backward passes are the library's own sm_100a kernels (``art_net_*`` /
 ``art_cnn_*`` in libartefact_b200.so: tcgen05 MMAs with TMEM accumulators,
 TMA-staged tiles); PyTorch only provides device memory and streams here.
@@ -32,21 +35,29 @@ LAYERS = [("e1", 16, 32), ("e2", 32, 64), ("e3", 64, 96), ("e4", 96, 128), ("d3"
           ("d1", 96, 32), ("head", 32, 16)]
 
 
+def level0(n: int) -> int:
+    """Side of the network's first level for a component side n (multiple of
+    8): n padded to a multiple of 16, halved; each level-0 pixel carries a 2x2
+    cell of samples."""
+    return (n + 15) // 16 * 8
+
+
 def num_params() -> int:
     return int(N.lib().art_net_num_params())
 
 
 def init_params(seed: int = 0) -> np.ndarray:
     """He-normal weights, zero biases; the head starts near zero (prediction =
-    decoded image) and only its first output channel is ever non-zero."""
+    decoded image) and only its first four output channels (the 2x2 cell of a
+    level-0 pixel) are ever non-zero."""
     rng = np.random.default_rng(seed)
     out = []
     for name, cin, cout in LAYERS:
         std = np.sqrt(2.0 / (9 * cin))
         w = rng.standard_normal((cout, 9, cin)) * std
         if name == "head":
-            w[1:] = 0.0
-            w[0] *= 0.01
+            w[4:] = 0.0
+            w[:4] *= 0.01
         out += [w.ravel(), np.zeros(cout)]
     p = np.concatenate(out).astype(np.float32)
     assert p.size == num_params()
@@ -162,7 +173,7 @@ class WarmStartNet:
 
         B, H, W = coef.shape
         dec = torch.empty((B, H, W), dtype=torch.float32, device=coef.device)
-        feat = torch.empty((B, H, W, 16), dtype=torch.bfloat16, device=coef.device)
+        feat = torch.empty((B, level0(H), level0(W), 16), dtype=torch.bfloat16, device=coef.device)
         N.check(N.lib().art_cnn_features(_ptr(coef), W, H * W, _ptr(q), B, H, W, _ptr(dec), _ptr(feat),
                                          _stream(stream)))
         return dec

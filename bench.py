@@ -61,6 +61,9 @@ WORKLOADS = {
                     metric="MPix/s to the plain 50-iteration objective (learned warm start + 8 iterations, "
                            "1080p 4:2:0 q30/50/75)", iterations=8),
 }
+WORKLOADS["network"] = dict(
+    name="warm-start network forward on one 1920x1080 4:2:0 JPEG (luma 1920x1088, chroma 2 x 960x544)",
+    metric="TFLOP/s (warm-start network forward, 1080p 4:2:0)", iterations=0)
 LEARNED_QUALITIES = (30, 50, 75)
 REFINE_ITERATIONS = 8
 REFINE_STEP_ITERATIONS = 50  # refinement steps of the 50-iteration run's size
@@ -321,6 +324,12 @@ def learned_comparison(lib, device, steps, warmup, refine=REFINE_ITERATIONS, ste
                 kmin = k
                 break
         kmin_ms = timed(img, kmin, N.ART_INIT_LEARNED, step_iterations) if kmin else None
+        sweep = {}
+        for si in (8, 16, 30, 50, 100, 300):
+            img.solve(lib, ctx, refine, N.ART_INIT_LEARNED, si, stream)
+            sweep[si] = (evaluate()[0] - e50) / e50
+        img.solve(lib, ctx, 0, N.ART_INIT_LEARNED, 0, stream)
+        e_start = (evaluate()[0] - e50) / e50
         rows.append(dict(quality=q, plain50_ms=plain_ms, plain50_mpix_s=mpix / plain_ms * 1e3,
                          learned_ms=learned_ms, learned_mpix_s=mpix / learned_ms * 1e3,
                          speedup=plain_ms / learned_ms, E_plain50=e50, E_learned=el,
@@ -328,7 +337,8 @@ def learned_comparison(lib, device, steps, warmup, refine=REFINE_ITERATIONS, ste
                          infeasibility_learned=fl, infeasibility_plain=f50,
                          reaches_plain50=bool(el <= e50 * (1 + 1e-4) and fl <= 1e-3),
                          min_refine_to_reach=kmin,
-                         min_refine_ms=kmin_ms, min_refine_speedup=(plain_ms / kmin_ms) if kmin_ms else None))
+                         min_refine_ms=kmin_ms, min_refine_speedup=(plain_ms / kmin_ms) if kmin_ms else None,
+                         E_rel_after_projection_only=e_start, E_rel_by_refine_step_iterations=sweep))
         log(f"learned q{q}: plain50 {plain_ms:.3f} ms E {e50:.7g}; learned+{refine} {learned_ms:.3f} ms "
             f"E {el:.7g} ({(el - e50) / e50:+.2e}); decoded+{refine} E {ed:.7g}; reach at K={kmin}")
     lib.art_context_set_warm_start(ctx, None)
@@ -343,9 +353,11 @@ def learned_comparison(lib, device, steps, warmup, refine=REFINE_ITERATIONS, ste
 
 def network_flops(H, W):
     """Multiply-add FLOPs (x2) of one forward pass of the warm-start network
-    on an H x W component, as executed (input features padded to 16 channels,
-    head to 16 outputs)."""
-    P0, P1, P2, P3 = H * W, (H // 2) * (W // 2), (H // 4) * (W // 4), (H // 8) * (W // 8)
+    on an H x W component, as executed: its first level is H0 x W0 =
+    ceil(H / 16) * 8 x ceil(W / 16) * 8 (2x2 cells of samples per pixel), input
+    features padded to 16 channels, head to 16 outputs."""
+    H0, W0 = (H + 15) // 16 * 8, (W + 15) // 16 * 8
+    P0, P1, P2, P3 = H0 * W0, (H0 // 2) * (W0 // 2), (H0 // 4) * (W0 // 4), (H0 // 8) * (W0 // 8)
     macs = 9 * (16 * 32 * P0 + 32 * 64 * P1 + 64 * 96 * P2 + 96 * 128 * P3 + 224 * 96 * P2 + 160 * 64 * P1
                 + 96 * 32 * P0 + 32 * 16 * P0)
     return 2 * macs
@@ -539,6 +551,20 @@ def main():
     wl = WORKLOADS[args.workload]
     if args.workload == "learned":
         run_learned(args, lib, local, rank, world, dist)
+        return
+    if args.workload == "network":
+        ms, tflops, flops = time_network(local, args.steps, args.warmup)
+        if rank == 0:
+            peaks = json.loads((ROOT / "MEASURED_PEAKS.json").read_text()) if (ROOT / "MEASURED_PEAKS.json").exists() else {}
+            peak = float(peaks.get("bf16_tflops", 1590.0))
+            print(json.dumps({"metric": wl["metric"], "value": tflops, "unit": "TFLOP/s", "n_gpus": world,
+                              "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True,
+                              "scaling": "weak", "vs_baseline": None, "dtype": "bf16 (fp32 accumulation)",
+                              "data": "synthetic", "config": {"workload": wl["name"]},
+                              "roofline": {"bound": "tensor", "achieved": tflops, "peak": peak, "unit": "TFLOP/s",
+                                           "frac": tflops / peak, "traffic": None,
+                                           "peak_kind": "measured" if peaks else "fallback",
+                                           "algorithmic_flops_per_launch": flops, "launch_ms": ms}}), flush=True)
         return
     iters = wl["iterations"]
     jpegs = make_workload(args.workload)

@@ -317,14 +317,21 @@ int32_t art_cnn_bias_grad(const void *g, int64_t npix, int32_t C, float *workspa
 /* Network input from B int16 coefficient images (rows of cpitch, images
  * img_stride elements apart, coefficient (v,u) of block (bx,by) at
  * (8by+v, 8bx+u)) and B quantisation tables q[B][64]: dec = IDCT(c q) per
- * block (fp32 [B][H][W]) and feat[B][H][W][16] = (dec / 128, q / 64, 0...). */
+ * block (fp32 [B][H][W]) and feat[B][H0][W0][16] on the network's first
+ * level, H0 = ceil(H / 16) * 8, W0 = ceil(W / 16) * 8 (space to depth):
+ * level-0 pixel (y, x) holds samples (2y + dy, 2x + dx) as channels
+ * 2 dy + dx = dec / 128 and 4 + 2 dy + dx = q / 64 (zero outside the image;
+ * channels 8-15 zero). */
 int32_t art_cnn_features(const int16_t *coef, int32_t cpitch, int64_t img_stride, const float *q, int32_t B,
                          int32_t H, int32_t W, float *dec, void *feat, void *stream);
-/* Prediction pred = dec + 16 r (r = channel 0 of rows of rstride floats);
- * with a target, the mean-squared-error gradient into grad[p][16] (channel 0)
- * and loss_blocks partial sums of the squared error in units of 16 levels. */
-int32_t art_cnn_residual(const float *r, int32_t rstride, const float *dec, const float *target, int64_t npix,
-                         float *pred, void *grad, float *loss_partial, int32_t loss_blocks, void *stream);
+/* Prediction pred[B][H][W] = dec + 16 r, r the depth-to-space of channels
+ * 0-3 of the level-0 head output r[B][H0][W0][rstride] (inverse of the
+ * features' layout); with a target [B][H][W], the gradient of the mean
+ * squared error over the B H W samples into grad[B][H0][W0][16] (channels
+ * 0-3) and loss_blocks partial sums of the squared error in units of 16 levels. */
+int32_t art_cnn_residual(const float *r, int32_t rstride, const float *dec, const float *target, int32_t B,
+                         int32_t H, int32_t W, float *pred, void *grad, float *loss_partial, int32_t loss_blocks,
+                         void *stream);
 /* One Adam step on n fp32 parameters (step counts from 1). */
 int32_t art_cnn_adam(float *w, const float *g, float *m, float *v, int64_t n, float lr, float beta1, float beta2,
                      float eps, int32_t step, void *stream);
@@ -332,7 +339,9 @@ int32_t art_cnn_adam(float *w, const float *g, float *m, float *v, int64_t n, fl
 
 /* The warm-start network as a whole (4-level encoder-decoder, 3x3 convs,
  * 32/64/96/128 channels, BF16 weights and activations, FP32 accumulation and
- * master weights). Parameters are one fp32 array of art_net_num_params()
+ * master weights). Its first level is the component at half resolution, each
+ * pixel carrying a 2x2 cell of samples (art_cnn_features), so the levels are
+ * 1/2, 1/4, 1/8 and 1/16 of the component's size. Parameters are one fp32 array of art_net_num_params()
  * values: per layer (e1, e2, e3, e4, d3, d2, d1, head) the weights
  * [cout][9][cin] then the bias [cout]. Inputs are B int16 coefficient images
  * of H x W (multiples of 8; rows of cpitch elements, images img_stride

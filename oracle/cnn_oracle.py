@@ -4,7 +4,9 @@ The network has no counterpart in the reference (it only chooses where the
 solver starts); this module is the checker for the project's tensor-core
 forward and backward kernels. Only tests import it.
 
-It restates the network independently of the CUDA code:
+It restates the network independently of the CUDA code. The network runs on
+a half-resolution grid ("level 0", H0 x W0 = ceil(H / 16) * 8 x ceil(W / 16) * 8):
+each level-0 pixel carries a 2x2 cell of the component (space to depth).
 
   e1 = relu(conv(F, 16 -> 32))                       level 0
   e2 = relu(conv(pool(e1), 32 -> 64))                level 1
@@ -13,12 +15,14 @@ It restates the network independently of the CUDA code:
   d3 = relu(conv([e3 | up(e4)], 224 -> 96))         level 2
   d2 = relu(conv([e2 | up(d3)], 160 -> 64))         level 1
   d1 = relu(conv([e1 | up(d2)], 96 -> 32))          level 0
-  r  = conv(d1, 32 -> 16)[..., 0]
+  r  = depth_to_space(conv(d1, 32 -> 16)[..., 0:4]) cropped to H x W
   prediction = decoded + 16 r, loss = mean((r - (target - decoded) / 16)^2)
 
 conv = 3x3, stride 1, zero padding 1, weights W[cout][tap = 3 (dy+1) + (dx+1)][cin];
-pool = 2x2 mean; up = nearest 2x. F = (decoded / 128, q / 64, 0 x 14) with q
-the quantisation step of each sample's frequency position.
+pool = 2x2 mean; up = nearest 2x. F = (space_to_depth(decoded) / 128,
+space_to_depth(q) / 64, 0 x 8) with q the quantisation step of each sample's
+frequency position; channel 2 dy + dx of a level-0 pixel (y, x) is sample
+(2y + dy, 2x + dx), zero outside the component.
 
 With ``bf16=True`` every tensor the GPU stores in bf16 is rounded to bf16
 (round to nearest even) at the same point, so the only remaining difference
@@ -112,9 +116,28 @@ def _dct_matrix():
     return m  # m[u][x]
 
 
+def level0(H, W):
+    """Size of the network's first level for an H x W component."""
+    return (H + 15) // 16 * 8, (W + 15) // 16 * 8
+
+
+def space_to_depth(a, H0, W0):
+    """[B][H][W] -> [B][H0][W0][4], zero-padded to 2 H0 x 2 W0; channel 2 dy + dx."""
+    B, H, W = a.shape
+    p = np.zeros((B, 2 * H0, 2 * W0))
+    p[:, :H, :W] = a
+    return p.reshape(B, H0, 2, W0, 2).transpose(0, 1, 3, 2, 4).reshape(B, H0, W0, 4)
+
+
+def depth_to_space(r, H, W):
+    """[B][H0][W0][4] -> [B][H][W] (inverse of space_to_depth, cropped)."""
+    B, H0, W0, _ = r.shape
+    return r.reshape(B, H0, W0, 2, 2).transpose(0, 1, 3, 2, 4).reshape(B, 2 * H0, 2 * W0)[:, :H, :W]
+
+
 def features(coef_img, q):
     """coef_img [B][H][W] (coefficient (v,u) of block (bx,by) at (8by+v, 8bx+u)), q [B][64].
-    Returns decoded [B][H][W] (fp64) and F [B][H][W][16]."""
+    Returns decoded [B][H][W] (fp64) and F [B][H0][W0][16]."""
     m = _dct_matrix()
     B, H, W = coef_img.shape
     c = coef_img.reshape(B, H // 8, 8, W // 8, 8).transpose(0, 1, 3, 2, 4).astype(np.float64)
@@ -122,9 +145,10 @@ def features(coef_img, q):
     blocks = np.einsum("vy,bijvu,ux->bijyx", m, c * qq, m)
     dec = blocks.transpose(0, 1, 3, 2, 4).reshape(B, H, W)
     qt = np.tile(q.reshape(B, 8, 8), (1, H // 8, W // 8)).astype(np.float64)
-    F = np.zeros((B, H, W, 16))
-    F[..., 0] = dec / 128.0
-    F[..., 1] = qt / 64.0
+    H0, W0 = level0(H, W)
+    F = np.zeros((B, H0, W0, 16))
+    F[..., 0:4] = space_to_depth(dec, H0, W0) / 128.0
+    F[..., 4:8] = space_to_depth(qt, H0, W0) / 64.0
     return dec, F
 
 
@@ -152,10 +176,12 @@ def forward(params, F, dec, target=None, bf=True):
     if bf:
         r = r.astype(np.float32).astype(np.float64)
     a["r"] = r
-    pred = dec + 16.0 * r[..., 0]
+    H, W = dec.shape[1:]
+    rf = depth_to_space(r[..., 0:4], H, W)
+    pred = dec + 16.0 * rf
     loss = None
     if target is not None:
-        e = r[..., 0] - (target - dec) / 16.0
+        e = rf - (target - dec) / 16.0
         loss = float(np.mean(e * e))
         a["e"] = e
     return a, pred, loss, Wq
@@ -168,9 +194,9 @@ def gradients(params, F, dec, target, bf=True):
     npix = dec.size
     mask = lambda g, act: g * (act > 0)
     dr = np.zeros(a["r"].shape)
-    dr[..., 0] = 2.0 * a["e"] / npix
+    dr[..., 0:4] = space_to_depth(2.0 * a["e"] / npix, *a["r"].shape[1:3])
     if bf:
-        dr[..., 0] = bf16(dr[..., 0].astype(np.float32))
+        dr[..., 0:4] = bf16(dr[..., 0:4].astype(np.float32))
     grads = {}
 
     def wb(name, x, g):

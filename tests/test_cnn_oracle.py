@@ -30,8 +30,21 @@ def test_features_decode_dc_block():
     q = np.full((1, 64), 2.0)
     dec, F = O.features(coef, q)
     np.testing.assert_allclose(dec, 1.0, atol=1e-12)  # DC 8 / 8 (orthonormal 2-D DCT)
-    np.testing.assert_allclose(F[..., 1], 2.0 / 64.0)
-    assert np.all(F[..., 2:] == 0)
+    assert F.shape == (1, 8, 8, 16)  # level 0 of an 8x8 component: padded to 16x16, halved
+    np.testing.assert_allclose(F[0, :4, :4, 0:4], 1.0 / 128.0, atol=1e-12)
+    np.testing.assert_allclose(F[0, :4, :4, 4:8], 2.0 / 64.0)
+    assert np.all(F[0, 4:] == 0) and np.all(F[0, :, 4:] == 0)  # padding
+    assert np.all(F[..., 8:] == 0)
+
+
+def test_space_to_depth_round_trip():
+    rng = np.random.default_rng(4)
+    a = rng.standard_normal((2, 24, 40))
+    H0, W0 = O.level0(24, 40)
+    assert (H0, W0) == (16, 24)
+    s = O.space_to_depth(a, H0, W0)
+    assert s[1, 3, 5, 2] == a[1, 7, 10] and s[1, 3, 5, 1] == a[1, 6, 11]
+    np.testing.assert_array_equal(O.depth_to_space(s, 24, 40), a)
 
 
 def test_gradients_match_finite_differences():
@@ -50,7 +63,7 @@ def test_gradients_match_finite_differences():
 
 def test_layer_gradients_match_finite_differences():
     """Per layer, so that a wrong slice (skip vs upsampled channels) cannot hide."""
-    params, F, dec, target = _case(2, H=24, W=16)
+    params, F, dec, target = _case(2, H=24, W=40)
     _, g = O.gradients(params, F, dec, target, bf=False)
     offs, _ = O.offsets()
     rng = np.random.default_rng(3)

@@ -222,7 +222,7 @@ def test_network_gradients_match_oracle(gpu):
     offs, _ = O.offsets()
     wo, bo = offs["head"]
     params[wo:bo] = (rng.standard_normal(bo - wo) * 0.05).astype(np.float32)  # a head that passes gradient
-    params[wo + 32 * 9:bo] = 0.0
+    params[wo + 4 * 32 * 9:bo] = 0.0  # outputs 4-15 are unused (outputs 0-3: the 2x2 cell)
     net = WS.WarmStartNet(params)
     loss = net.train_step(torch.from_numpy(coef).cuda(), _f32(q), _f32(target), lr=0.0)
     g = net.gradients().astype(np.float64)

@@ -66,7 +66,7 @@ def _strong_params(seed):
         offs[name] = (o, o + cout * 9 * cin)
         o += cout * 9 * cin + cout
     lo, hi = offs["head"]
-    p[lo:lo + 9 * 32] = (rng.standard_normal(9 * 32) * 0.05).astype(np.float32)
+    p[lo:lo + 4 * 9 * 32] = (rng.standard_normal(4 * 9 * 32) * 0.05).astype(np.float32)
     return p
 
 
