@@ -159,6 +159,7 @@ EXPORTS = {
                                      C.c_int32, C.c_void_p, C.c_void_p, C.c_void_p]),
     "art_cnn_residual": (C.c_int32, [C.c_void_p, C.c_int32, C.c_void_p, C.c_void_p, C.c_int32, C.c_int32,
                                      C.c_int32, C.c_void_p, C.c_void_p, C.c_void_p, C.c_int32, C.c_void_p]),
+    "art_cnn_wait_selftest": (C.c_int32, [C.c_void_p, C.c_int64, C.c_void_p]),
     "art_cnn_adam": (C.c_int32, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_int64, C.c_float, C.c_float,
                                  C.c_float, C.c_float, C.c_int32, C.c_void_p]),
 }

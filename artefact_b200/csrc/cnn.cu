@@ -42,10 +42,11 @@ namespace cnn {
 using bf16 = __nv_bfloat16;
 
 constexpr int TPX = 128;                    // output pixels per tile row (MMA M)
-constexpr int TROWS = 2;                    // output rows per tile
+constexpr int TROWS = 2;                    // weight gradient: output rows per tile
+constexpr int MAX_TROWS = 8;                // convolution: output rows per tile, chosen per launch (1..8)
 constexpr int HPX = TPX + 2;                // halo tile width
-constexpr int HROWS = TROWS + 2;            // halo tile height
-constexpr uint32_t KCOL = HROWS * HPX * 16; // bytes of one 8-channel column of a halo tile (8320)
+constexpr int HROWS = TROWS + 2;            // weight gradient: halo tile height
+constexpr uint32_t KCOL = HROWS * HPX * 16; // weight gradient: bytes of one 8-channel column of a halo tile (8320)
 constexpr uint32_t DYREG = TROWS * TPX * 16;// bytes of one 8-channel region of a gradient tile (4096)
 constexpr int THREADS = 192;                // warp 0 loads, warp 1 MMA, warps 2-5 epilogue
 constexpr uint32_t SMEM_BUDGET = 220 * 1024;  // pipeline stages; 1 KB more is requested for alignment
@@ -65,6 +66,10 @@ struct ConvArgs {
     int mask_cstride;
     int relu, accumulate;
     int stages;
+    int trows;          // output rows per tile; accumulators of 2 * trows rows x n columns fit TMEM's 512
+    uint32_t kcol;      // shared-memory stride of the 8-channel columns of a halo tile: (trows + 2) * HPX * 16
+                        // bytes rounded up to 128 (TMA destinations stay 128-byte aligned)
+    uint32_t tx_bytes;  // bytes the TMA and bulk copies of one stage deliver
     uint32_t stage_bytes, halo_bytes;
     int *err;
 };
@@ -79,12 +84,12 @@ struct WgradArgs {
     int *err;
 };
 
-__device__ __forceinline__ void tile_coords(int tile, int tiles_x, int tiles_y, int &b, int &y0, int &x0)
+__device__ __forceinline__ void tile_coords(int tile, int tiles_x, int tiles_y, int trows, int &b, int &y0, int &x0)
 {
     const int per = tiles_x * tiles_y;
     b = tile / per;
     const int r = tile - b * per;
-    y0 = (r / tiles_x) * TROWS;
+    y0 = (r / tiles_x) * trows;
     x0 = (r % tiles_x) * TPX;
 }
 
@@ -113,7 +118,9 @@ __global__ void __launch_bounds__(THREADS, 1) k_conv3x3(const __grid_constant__ 
     volatile int *abort_p = &abort_s;
 
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const int tiles_x = (a.W + TPX - 1) / TPX, tiles_y = (a.H + TROWS - 1) / TROWS;
+    const int TR = a.trows;
+    const uint32_t kcol = a.kcol;
+    const int tiles_x = (a.W + TPX - 1) / TPX, tiles_y = (a.H + TR - 1) / TR;
     const int ntiles = a.B * tiles_x * tiles_y;
     const int nchunks = a.cin / a.ck;
     const int S = a.stages;
@@ -143,7 +150,7 @@ __global__ void __launch_bounds__(THREADS, 1) k_conv3x3(const __grid_constant__ 
             bool ok = true;
             for (int tile = blockIdx.x; tile < ntiles && ok; tile += gridDim.x) {
                 int b, y0, x0;
-                tile_coords(tile, tiles_x, tiles_y, b, y0, x0);
+                tile_coords(tile, tiles_x, tiles_y, TR, b, y0, x0);
                 for (int c = 0; c < nchunks; c++, it++) {
                     const int s = it % S;
                     const uint32_t use = it / S;
@@ -152,9 +159,9 @@ __global__ void __launch_bounds__(THREADS, 1) k_conv3x3(const __grid_constant__ 
                         break;
                     }
                     unsigned char *st = smem + (size_t)s * a.stage_bytes;
-                    tc::mbar_arrive_expect_tx(&full_bar[s], a.stage_bytes);
+                    tc::mbar_arrive_expect_tx(&full_bar[s], a.tx_bytes);
                     for (int j = 0; j < a.ck / 8; j++)
-                        tc::tma_load_4d(st + j * KCOL, &xmap, c * a.ck + 8 * j, x0 - 1, y0 - 1, b, &full_bar[s]);
+                        tc::tma_load_4d(st + j * kcol, &xmap, c * a.ck + 8 * j, x0 - 1, y0 - 1, b, &full_bar[s]);
                     tc::bulk_load(st + a.halo_bytes, a.wpack + (size_t)c * 9 * a.ck * a.n, 18u * a.ck * a.n,
                                   &full_bar[s]);
                 }
@@ -189,11 +196,11 @@ __global__ void __launch_bounds__(THREADS, 1) k_conv3x3(const __grid_constant__ 
                         for (int kk = 0; kk < a.ck / 16; kk++) {
                             const uint64_t bdesc =
                                 tc::smem_desc(wst + (uint32_t)((tap * (a.ck / 8) + 2 * kk) * a.n * 16), a.n * 16, 128);
-#pragma unroll
-                            for (int t = 0; t < TROWS; t++) {
+#pragma unroll 1
+                            for (int t = 0; t < TR; t++) {
                                 const uint64_t adesc = tc::smem_desc(
-                                    st + 2 * kk * KCOL + (uint32_t)(((t + ty) * HPX + tx) * 16), KCOL, 128);
-                                tc::mma_bf16(tbase + (uint32_t)((ab * TROWS + t) * 128), adesc, bdesc, idesc,
+                                    st + 2 * kk * kcol + (uint32_t)(((t + ty) * HPX + tx) * 16), kcol, 128);
+                                tc::mma_bf16(tbase + (uint32_t)((ab * TR + t) * a.n), adesc, bdesc, idesc,
                                              (c | tap | kk) != 0);
                             }
                         }
@@ -220,16 +227,16 @@ __global__ void __launch_bounds__(THREADS, 1) k_conv3x3(const __grid_constant__ 
             tc::mbar_wait(&accf_bar[ab], (tcount >> 1) & 1, abort_p);  // completes at once: every lane observes the phase
             tc::tc_fence_after();
             int b, y0, x0;
-            tile_coords(tile, tiles_x, tiles_y, b, y0, x0);
+            tile_coords(tile, tiles_x, tiles_y, TR, b, y0, x0);
 #pragma unroll 1
-            for (int t = 0; t < TROWS; t++) {
+            for (int t = 0; t < TR; t++) {
                 const int y = y0 + t, x = x0 + px;
                 const bool in = y < a.H && x < a.W;
                 const size_t pix = ((size_t)b * a.H + (in ? y : 0)) * a.W + (in ? x : 0);
 #pragma unroll 1
                 for (int c0 = 0; c0 < a.n; c0 += 16) {
                     float v[16];
-                    tc::tmem_ld16(tbase + ((uint32_t)(q * 32) << 16) + (uint32_t)((ab * TROWS + t) * 128 + c0), v);
+                    tc::tmem_ld16(tbase + ((uint32_t)(q * 32) << 16) + (uint32_t)((ab * TR + t) * a.n + c0), v);
                     if (!in || c0 >= a.n_store) continue;
                     if (a.bias) {
 #pragma unroll
@@ -325,7 +332,7 @@ __global__ void __launch_bounds__(THREADS, 1) k_wgrad3x3(const __grid_constant__
                 const uint32_t use = it / S;
                 if (use > 0 && !tc::mbar_wait(&empty_bar[s], (use - 1) & 1, abort_p)) break;
                 int b, y0, x0;
-                tile_coords(tile, tiles_x, tiles_y, b, y0, x0);
+                tile_coords(tile, tiles_x, tiles_y, TROWS, b, y0, x0);
                 unsigned char *st = smem + (size_t)s * a.stage_bytes;
                 tc::mbar_arrive_expect_tx(&full_bar[s], tx_bytes);
                 for (int g = 0; g < a.cout / 8; g++)
@@ -696,6 +703,28 @@ __global__ void k_residual(const float *__restrict__ r, int rstride, const float
     if (threadIdx.x == 0 && loss_partial) loss_partial[blockIdx.x] = s[0];
 }
 
+// Self-test of the bounded wait every tensor-core pipeline uses: thread 0
+// waits on an mbarrier phase that nothing completes. After `limit` clock
+// cycles the wait gives up and raises the abort flag, and the kernel writes
+// 1 to *err and returns -- what the pipelines do when a partner role stalls,
+// leaving the context usable. 0 would mean the phase completed (impossible here).
+__global__ void k_wait_selftest(int *err, long long limit)
+{
+    __shared__ __align__(8) uint64_t bar;
+    __shared__ int abort_s;
+    if (threadIdx.x == 0) {
+        abort_s = 0;
+        tc::mbar_init(&bar, 1);
+        tc::fence_barrier_init();
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        volatile int *ab = &abort_s;
+        const bool ok = tc::mbar_wait_limit(&bar, 0, ab, limit);
+        *err = ok ? 0 : 1;
+    }
+}
+
 // Adam on flat fp32 parameters (decoupled from the bf16 copies the convs read).
 __global__ void k_adam(float *__restrict__ w, const float *__restrict__ g, float *__restrict__ m, float *__restrict__ v,
                        long long n, float lr, float b1, float b2, float eps, float c1, float c2)
@@ -796,10 +825,29 @@ int32_t conv3x3(const ArtCnnConv *d, cudaStream_t s)
         return fail(ART_ERR_INVALID_ARGUMENT, "conv: bad mask stride");
     if ((long long)d->B * d->H * d->W * (long long)d->cin >= (1LL << 40))
         return fail(ART_ERR_INVALID_ARGUMENT, "conv: tensor too large");
+    // Output rows per tile: as many as TMEM (2 tiles in flight x trows
+    // accumulators of n columns <= 512) and three pipeline stages allow, but
+    // no more than leaves every SM a tile; taller tiles re-read less halo and
+    // reload the weights less often.
+    const int tiles_x = (d->W + TPX - 1) / TPX;
+    int trows = 0;
+    auto col_stride = [](int t) { return ((uint32_t)((t + 2) * HPX * 16) + 127u) / 128u * 128u; };
+    for (int want = 3; want >= 2 && !trows; want--)
+        for (int t = MAX_TROWS; t >= 1; t--) {
+            const uint32_t sb = (uint32_t)(d->ck / 8) * col_stride(t) + 18u * d->ck * d->n;
+            const long long tiles = (long long)d->B * tiles_x * ((d->H + t - 1) / t);
+            if (2 * t * d->n <= 512 && SMEM_BUDGET / sb >= (uint32_t)want && (tiles >= num_sms() || t == 1)) {
+                trows = t;
+                break;
+            }
+        }
+    if (!trows) return fail(ART_ERR_INVALID_ARGUMENT, "conv: stage does not fit shared memory");
     CUtensorMap map;
     std::string err;
-    if (!make_map(&map, d->x, d->B, d->H, d->W, d->cin, HPX, HROWS, err)) return fail(ART_ERR_CUDA, "conv: " + err);
+    if (!make_map(&map, d->x, d->B, d->H, d->W, d->cin, HPX, trows + 2, err)) return fail(ART_ERR_CUDA, "conv: " + err);
     ConvArgs a{};
+    a.trows = trows;
+    a.kcol = col_stride(trows);
     a.B = d->B;
     a.H = d->H;
     a.W = d->W;
@@ -818,14 +866,15 @@ int32_t conv3x3(const ArtCnnConv *d, cudaStream_t s)
     a.mask_cstride = d->mask_cstride;
     a.relu = d->relu;
     a.accumulate = d->accumulate;
-    a.halo_bytes = (uint32_t)(d->ck / 8) * KCOL;
+    a.halo_bytes = (uint32_t)(d->ck / 8) * a.kcol;
     a.stage_bytes = a.halo_bytes + 18u * d->ck * d->n;
+    a.tx_bytes = (uint32_t)(d->ck / 8) * (uint32_t)((trows + 2) * HPX * 16) + 18u * d->ck * d->n;
     a.stages = (int)std::min<uint32_t>(MAX_STAGES, SMEM_BUDGET / a.stage_bytes);
     a.err = d->err;
     if (a.stages < 2) return fail(ART_ERR_INVALID_ARGUMENT, "conv: stage does not fit shared memory");
     const uint32_t smem = a.stages * a.stage_bytes + 1024;
     cudaFuncSetAttribute(k_conv3x3, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)(SMEM_BUDGET + 1024));
-    const long long ntiles = (long long)d->B * ((d->H + TROWS - 1) / TROWS) * ((d->W + TPX - 1) / TPX);
+    const long long ntiles = (long long)d->B * ((d->H + trows - 1) / trows) * tiles_x;
     const int grid = (int)std::min<long long>(ntiles, num_sms());
     k_conv3x3<<<grid, THREADS, smem, s>>>(map, a);
     return check_launch("k_conv3x3");
@@ -984,6 +1033,14 @@ int32_t art_cnn_residual(const float *r, int32_t rstride, const float *dec, cons
     k_residual<<<loss_blocks, 256, 0, static_cast<cudaStream_t>(stream)>>>(
         r, rstride, dec, target, B, H, W, 1.f / (float)npix, pred, static_cast<bf16 *>(grad), loss_partial);
     return check_launch("k_residual");
+}
+
+int32_t art_cnn_wait_selftest(int32_t *err, int64_t limit_cycles, void *stream)
+{
+    if (!err || limit_cycles < 1 || limit_cycles > 8000000000LL)
+        return fail(ART_ERR_INVALID_ARGUMENT, "wait_selftest: bad arguments");
+    k_wait_selftest<<<1, 32, 0, static_cast<cudaStream_t>(stream)>>>(err, (long long)limit_cycles);
+    return check_launch("k_wait_selftest");
 }
 
 int32_t art_cnn_adam(float *w, const float *g, float *m, float *v, int64_t n, float lr, float beta1, float beta2,

@@ -56,19 +56,25 @@ __device__ __forceinline__ bool mbar_try_wait(uint64_t *bar, uint32_t parity)
 }
 
 // Waits for the phase of `bar` with the given parity to complete. Gives up
-// after about two seconds (or at once when another role already gave up):
+// after `limit` clock cycles (or at once when another role already gave up):
 // raises *abort and returns false.
-__device__ __forceinline__ bool mbar_wait(uint64_t *bar, uint32_t parity, volatile int *abort)
+__device__ __forceinline__ bool mbar_wait_limit(uint64_t *bar, uint32_t parity, volatile int *abort, long long limit)
 {
     const long long t0 = clock64();
     while (!mbar_try_wait(bar, parity)) {
         if (*abort) return false;
-        if (clock64() - t0 > 4000000000LL) {
+        if (clock64() - t0 > limit) {
             *abort = 1;
             return false;
         }
     }
     return true;
+}
+
+// The pipelines' wait: gives up after about two seconds.
+__device__ __forceinline__ bool mbar_wait(uint64_t *bar, uint32_t parity, volatile int *abort)
+{
+    return mbar_wait_limit(bar, parity, abort, 4000000000LL);
 }
 
 // 4-D tiled TMA load (no multicast) of one box into shared memory, completing

@@ -332,6 +332,12 @@ int32_t art_cnn_features(const int16_t *coef, int32_t cpitch, int64_t img_stride
 int32_t art_cnn_residual(const float *r, int32_t rstride, const float *dec, const float *target, int32_t B,
                          int32_t H, int32_t W, float *pred, void *grad, float *loss_partial, int32_t loss_blocks,
                          void *stream);
+/* Self-test of the bounded waits of the tensor-core pipelines: one thread
+ * waits on an mbarrier phase that nothing completes, gives up after
+ * limit_cycles clock cycles (1 .. 8e9) and writes 1 to the device int *err;
+ * the kernel then returns normally. The pipelines' own waits give up after
+ * about 4e9 cycles and report through their err flag the same way. */
+int32_t art_cnn_wait_selftest(int32_t *err, int64_t limit_cycles, void *stream);
 /* One Adam step on n fp32 parameters (step counts from 1). */
 int32_t art_cnn_adam(float *w, const float *g, float *m, float *v, int64_t n, float lr, float beta1, float beta2,
                      float eps, int32_t step, void *stream);

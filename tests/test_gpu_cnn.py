@@ -255,3 +255,23 @@ def test_training_reduces_loss(gpu):
     losses = [net.train_step(c, qq, t, lr=2e-3) for _ in range(100)]
     assert all(np.isfinite(losses))
     assert losses[-1] < 0.5 * losses[0], losses[::10]
+
+
+def test_bounded_wait_gives_up_and_reports(gpu):
+    """A pipeline wait on a phase that never completes gives up after its
+    limit and reports through the error flag; the context stays usable (a
+    convolution right after it is still correct)."""
+    import time
+
+    torch = _torch()
+    err = torch.full((1,), -1, dtype=torch.int32, device="cuda")
+    t0 = time.perf_counter()
+    N.check(N.lib().art_cnn_wait_selftest(_ptr(err), 20_000_000, None))
+    torch.cuda.synchronize()
+    assert int(err.item()) == 1
+    assert time.perf_counter() - t0 < 10.0
+    rng = np.random.default_rng(12)
+    x = O.bf16(rng.standard_normal((1, 4, 64, 16)))
+    w = O.bf16(rng.standard_normal((16, 9, 16)) * 0.2)
+    got = _np(_conv(_bf(x), _pack(w, ck=16), 16, 16, 16))
+    _close(got, O.bf16(O.conv(x, w)))
