@@ -45,7 +45,9 @@ class ArtOptions(C.Structure):
         ("init_mode", C.c_uint32),
         ("device", C.c_int32),
         ("step_iterations", C.c_uint32),
-        ("reserved", C.c_uint32 * 5),
+        ("tail_iterations", C.c_uint32),
+        ("tail_step_iterations", C.c_uint32),
+        ("reserved", C.c_uint32 * 3),
     ]
 
 

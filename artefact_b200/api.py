@@ -135,11 +135,14 @@ class ArtefactError(RuntimeError):
     """Error of :meth:`Artefact.process` (the reference's ``Err(String)``)."""
 
 
-def _options(init_mode: int, device: int, step_iterations: int = 0) -> N.ArtOptions:
+def _options(init_mode: int, device: int, step_iterations: int = 0, tail_iterations: int = 0,
+             tail_step_iterations: int = 0) -> N.ArtOptions:
     o = N.ArtOptions()
     o.init_mode = init_mode
     o.device = device
     o.step_iterations = int(step_iterations)
+    o.tail_iterations = int(tail_iterations)
+    o.tail_step_iterations = int(tail_step_iterations)
     return o
 
 
@@ -331,7 +334,8 @@ class Context:
 
     def compute(self, nchannel: int, coefs: Sequence[Coefficient], weight: float, pweight: Sequence[float],
                 iterations: int, max_rounded_px_w: int, max_rounded_px_h: int,
-                init_mode: int = N.ART_INIT_DECODED, step_iterations: int = 0) -> List[np.ndarray]:
+                init_mode: int = N.ART_INIT_DECODED, step_iterations: int = 0, tail_iterations: int = 0,
+                tail_step_iterations: int = 0) -> List[np.ndarray]:
         keep: list = []
         chans = (N.ArtChannel * nchannel)(*[coefs[c].as_c(keep) for c in range(nchannel)])
         pw = (C.c_float * 3)(*[float(v) for v in list(pweight)[:3]])
@@ -339,7 +343,8 @@ class Context:
         ptrs = (C.c_void_p * nchannel)(*[o.ctypes.data for o in outs])
         N.check(N.lib().art_context_compute(self._h, nchannel, chans, float(weight), pw, int(iterations),
                                             max_rounded_px_w, max_rounded_px_h, ptrs,
-                                            C.byref(_options(init_mode, -1, step_iterations))))
+                                            C.byref(_options(init_mode, -1, step_iterations, tail_iterations,
+                                                             tail_step_iterations))))
         return outs
 
     def compute_batch(self, jobs: Sequence[dict], iterations: int, init_mode: int = N.ART_INIT_DECODED,

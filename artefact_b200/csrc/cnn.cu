@@ -43,7 +43,8 @@ using bf16 = __nv_bfloat16;
 
 constexpr int TPX = 128;                    // output pixels per tile row (MMA M)
 constexpr int TROWS = 2;                    // weight gradient: output rows per tile
-constexpr int MAX_TROWS = 8;                // convolution: output rows per tile, chosen per launch (1..8)
+constexpr int MAX_TROWS = 2;                // convolution: output rows per tile, chosen per launch (1..MAX_TROWS;
+                                            // taller tiles measured slower: fewer tiles balance worse over the SMs)
 constexpr int HPX = TPX + 2;                // halo tile width
 constexpr int HROWS = TROWS + 2;            // weight gradient: halo tile height
 constexpr uint32_t KCOL = HROWS * HPX * 16; // weight gradient: bytes of one 8-channel column of a halo tile (8320)
@@ -826,17 +827,15 @@ int32_t conv3x3(const ArtCnnConv *d, cudaStream_t s)
     if ((long long)d->B * d->H * d->W * (long long)d->cin >= (1LL << 40))
         return fail(ART_ERR_INVALID_ARGUMENT, "conv: tensor too large");
     // Output rows per tile: as many as TMEM (2 tiles in flight x trows
-    // accumulators of n columns <= 512) and three pipeline stages allow, but
-    // no more than leaves every SM a tile; taller tiles re-read less halo and
-    // reload the weights less often.
+    // accumulators of n columns <= 512) and three pipeline stages (else two)
+    // allow, up to MAX_TROWS.
     const int tiles_x = (d->W + TPX - 1) / TPX;
     int trows = 0;
     auto col_stride = [](int t) { return ((uint32_t)((t + 2) * HPX * 16) + 127u) / 128u * 128u; };
     for (int want = 3; want >= 2 && !trows; want--)
         for (int t = MAX_TROWS; t >= 1; t--) {
             const uint32_t sb = (uint32_t)(d->ck / 8) * col_stride(t) + 18u * d->ck * d->n;
-            const long long tiles = (long long)d->B * tiles_x * ((d->H + t - 1) / t);
-            if (2 * t * d->n <= 512 && SMEM_BUDGET / sb >= (uint32_t)want && (tiles >= num_sms() || t == 1)) {
+            if (2 * t * d->n <= 512 && SMEM_BUDGET / sb >= (uint32_t)want) {
                 trows = t;
                 break;
             }

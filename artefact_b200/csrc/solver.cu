@@ -46,8 +46,8 @@ namespace art {
 // their terms are zero, which reproduces the reference's scatter guards. Rows
 // are prefetched two ahead of use.
 template <int NCH>
-__global__ void __launch_bounds__(SWEEP_WARPS * 32) k_grad_sweep(const ImgDev *__restrict__ imgs,
-                                                                 const int2 *__restrict__ work)
+__global__ void __launch_bounds__(SWEEP_WARPS * 32, SWEEP_MIN_BLOCKS) k_grad_sweep(const ImgDev *__restrict__ imgs,
+                                                                 const int2 *__restrict__ work, float stepmul)
 {
     __shared__ float s_red[SWEEP_WARPS][NCH];
     __shared__ double s_dred[SWEEP_WARPS][NCH];
@@ -259,7 +259,7 @@ __global__ void __launch_bounds__(SWEEP_WARPS * 32) k_grad_sweep(const ImgDev *_
                 double s = 0.0;
                 for (int w = 0; w < SWEEP_WARPS; w++) s += s_dred[w][c];
                 const double nrm = sqrt(s);
-                im.sigma[c] = nrm > 0.0 ? (float)((double)im.step / nrm) : 0.f;
+                im.sigma[c] = nrm > 0.0 ? (float)((double)(im.step * stepmul) / nrm) : 0.f;
             }
             atomicExch(im.counter, 0u);
         }
@@ -276,8 +276,8 @@ __global__ void __launch_bounds__(SWEEP_WARPS * 32) k_grad_sweep(const ImgDev *_
 // which reproduces the reference's scatter guards. Rows are prefetched two
 // ahead of use.
 template <int NCH>
-__global__ void __launch_bounds__(SWEEP_WARPS_N * 32) k_grad_sweep_n(const ImgDev *__restrict__ imgs,
-                                                                 const int2 *__restrict__ work)
+__global__ void __launch_bounds__(SWEEP_WARPS_N * 32, SWEEP_MIN_BLOCKS_N) k_grad_sweep_n(const ImgDev *__restrict__ imgs,
+                                                                 const int2 *__restrict__ work, float stepmul)
 {
     __shared__ float s_red[SWEEP_WARPS_N][NCH];
     __shared__ double s_dred[SWEEP_WARPS_N][NCH];
@@ -466,7 +466,7 @@ __global__ void __launch_bounds__(SWEEP_WARPS_N * 32) k_grad_sweep_n(const ImgDe
                 double s = 0.0;
                 for (int w = 0; w < SWEEP_WARPS_N; w++) s += s_dred[w][c];
                 const double nrm = sqrt(s);
-                im.sigma[c] = nrm > 0.0 ? (float)((double)im.step / nrm) : 0.f;
+                im.sigma[c] = nrm > 0.0 ? (float)((double)(im.step * stepmul) / nrm) : 0.f;
             }
             atomicExch(im.counter, 0u);
         }
@@ -967,12 +967,14 @@ std::vector<float> fista_factors(uint32_t iterations)
 struct GraphKey {
     int nimg = 0, wcount[8] = {0, 0, 0, 0, 0, 0, 0, 0};
     int mode_off[5] = {0, 0, 0, 0, 0};
-    uint32_t iterations = 0;
+    uint32_t iterations = 0, tail = 0;
+    float tail_stepmul = 1.0f;
     bool timing = false;
     const void *desc = nullptr, *work = nullptr, *tasks = nullptr;
     bool operator==(const GraphKey &o) const
     {
-        return nimg == o.nimg && iterations == o.iterations && timing == o.timing && desc == o.desc &&
+        return nimg == o.nimg && iterations == o.iterations && tail == o.tail && tail_stepmul == o.tail_stepmul &&
+               timing == o.timing && desc == o.desc &&
                work == o.work && tasks == o.tasks && std::equal(wcount, wcount + 8, o.wcount) &&
                std::equal(mode_off, mode_off + 5, o.mode_off);
     }
@@ -1362,7 +1364,9 @@ static int prepare_batch(ArtContext *ctx, const std::vector<ImageSpec> &specs, u
     return ART_OK;
 }
 
-static void launch_iteration(ArtContext *ctx, int it, float fnext)
+// One iteration: the gradient sweeps (sigma = step * stepmul / ||g||) and the
+// projections forming y_{k+1} with FISTA factor fnext.
+static void launch_iteration(ArtContext *ctx, int it, float fnext, float stepmul)
 {
     const ImgDev *ddesc = static_cast<const ImgDev *>(ctx->desc.p);
     const int2 *work = static_cast<const int2 *>(ctx->work.p);
@@ -1370,17 +1374,17 @@ static void launch_iteration(ArtContext *ctx, int it, float fnext)
     const bool tm = ctx->timing;
     if (tm) cudaEventRecordWithFlags(ctx->events[2 + 4 * it], s, cudaEventRecordExternal);
     if (ctx->wcount[1][3])
-        k_grad_sweep<3><<<ctx->wcount[1][3], SWEEP_WARPS * 32, 0, s>>>(ddesc, work + ctx->wstart[1][3]);
+        k_grad_sweep<3><<<ctx->wcount[1][3], SWEEP_WARPS * 32, 0, s>>>(ddesc, work + ctx->wstart[1][3], stepmul);
     if (ctx->wcount[1][2])
-        k_grad_sweep<2><<<ctx->wcount[1][2], SWEEP_WARPS * 32, 0, s>>>(ddesc, work + ctx->wstart[1][2]);
+        k_grad_sweep<2><<<ctx->wcount[1][2], SWEEP_WARPS * 32, 0, s>>>(ddesc, work + ctx->wstart[1][2], stepmul);
     if (ctx->wcount[1][1])
-        k_grad_sweep<1><<<ctx->wcount[1][1], SWEEP_WARPS * 32, 0, s>>>(ddesc, work + ctx->wstart[1][1]);
+        k_grad_sweep<1><<<ctx->wcount[1][1], SWEEP_WARPS * 32, 0, s>>>(ddesc, work + ctx->wstart[1][1], stepmul);
     if (ctx->wcount[0][3])
-        k_grad_sweep_n<3><<<ctx->wcount[0][3], SWEEP_WARPS_N * 32, 0, s>>>(ddesc, work + ctx->wstart[0][3]);
+        k_grad_sweep_n<3><<<ctx->wcount[0][3], SWEEP_WARPS_N * 32, 0, s>>>(ddesc, work + ctx->wstart[0][3], stepmul);
     if (ctx->wcount[0][2])
-        k_grad_sweep_n<2><<<ctx->wcount[0][2], SWEEP_WARPS_N * 32, 0, s>>>(ddesc, work + ctx->wstart[0][2]);
+        k_grad_sweep_n<2><<<ctx->wcount[0][2], SWEEP_WARPS_N * 32, 0, s>>>(ddesc, work + ctx->wstart[0][2], stepmul);
     if (ctx->wcount[0][1])
-        k_grad_sweep_n<1><<<ctx->wcount[0][1], SWEEP_WARPS_N * 32, 0, s>>>(ddesc, work + ctx->wstart[0][1]);
+        k_grad_sweep_n<1><<<ctx->wcount[0][1], SWEEP_WARPS_N * 32, 0, s>>>(ddesc, work + ctx->wstart[0][1], stepmul);
     if (tm) cudaEventRecordWithFlags(ctx->events[3 + 4 * it], s, cudaEventRecordExternal);
     if (tm) cudaEventRecordWithFlags(ctx->events[4 + 4 * it], s, cudaEventRecordExternal);
     launch_projections(ctx, fnext);
@@ -1389,9 +1393,10 @@ static void launch_iteration(ArtContext *ctx, int it, float fnext)
 
 // Replays (capturing first if the work changed shape) the fixed-count
 // iteration loop as one CUDA graph.
-static int run_iterations(ArtContext *ctx, uint32_t iterations)
+static int run_iterations(ArtContext *ctx, uint32_t iterations, uint32_t tail = 0, float tail_stepmul = 1.0f)
 {
     if (iterations == 0) return ART_OK;
+    tail = std::min(tail, iterations);
     if (ctx->timing) {
         const size_t need = 2 + 4 * (size_t)iterations;
         while (ctx->events.size() < need) {
@@ -1405,6 +1410,8 @@ static int run_iterations(ArtContext *ctx, uint32_t iterations)
     std::copy(&ctx->wcount[0][0], &ctx->wcount[0][0] + 8, key.wcount);
     std::copy(ctx->mode_off, ctx->mode_off + 5, key.mode_off);
     key.iterations = iterations;
+    key.tail = tail;
+    key.tail_stepmul = tail_stepmul;
     key.timing = ctx->timing;
     key.desc = ctx->desc.p;
     key.work = ctx->work.p;
@@ -1415,13 +1422,22 @@ static int run_iterations(ArtContext *ctx, uint32_t iterations)
             cudaGraphExecDestroy(ctx->exec);
             ctx->exec = nullptr;
         }
-        const std::vector<float> fs = fista_factors(iterations);
+        // Two phases: iterations - tail steps of the solve's own size, then
+        // `tail` steps of tail_stepmul times that size with the FISTA sequence
+        // restarted (the last step of the first phase forms y = x). Without a
+        // tail this is the reference's loop (mod.rs:49-75).
+        const uint32_t k1 = iterations - tail;
+        const std::vector<float> fs1 = fista_factors(k1), fs2 = fista_factors(tail);
         cudaGraph_t graph;
         ART_CUDA(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
         if (ctx->timing) cudaEventRecordWithFlags(ctx->events[0], s, cudaEventRecordExternal);
         // y_0 = x_0 (f_0 = 0); the projection of iteration k forms y_{k+1} with f_{k+1}.
-        for (uint32_t it = 0; it < iterations; it++)
-            launch_iteration(ctx, (int)it, it + 1 < iterations ? fs[it + 1] : 0.0f);
+        for (uint32_t it = 0; it < iterations; it++) {
+            if (it < k1)
+                launch_iteration(ctx, (int)it, it + 1 < k1 ? fs1[it + 1] : 0.0f, 1.0f);
+            else
+                launch_iteration(ctx, (int)it, it - k1 + 1 < tail ? fs2[it - k1 + 1] : 0.0f, tail_stepmul);
+        }
         if (ctx->timing) cudaEventRecordWithFlags(ctx->events[1], s, cudaEventRecordExternal);
         cudaError_t e = cudaStreamEndCapture(s, &graph);
         if (e != cudaSuccess) return fail(ART_ERR_CUDA, std::string("graph capture: ") + cudaGetErrorString(e));
@@ -1461,12 +1477,22 @@ static int check_errflag(ArtContext *ctx)
 struct InitSpec {
     int mode = ART_INIT_DECODED;
     uint32_t step_iterations = 0;
+    uint32_t tail_iterations = 0, tail_step_iterations = 0;
+    // Step of the tail phase relative to the first phase's, for `iterations` in all.
+    float tail_stepmul(uint32_t iterations) const
+    {
+        if (!tail_iterations || !tail_step_iterations) return 1.0f;
+        const float s1 = (float)(step_iterations ? step_iterations : iterations);
+        return sqrtf(1.0f + s1) / sqrtf(1.0f + (float)tail_step_iterations);
+    }
 };
 
 static int init_spec(const ArtContext *ctx, const ArtOptions *opts, InitSpec *out)
 {
     out->mode = opts ? (int)opts->init_mode : ART_INIT_DECODED;
     out->step_iterations = opts ? opts->step_iterations : 0;
+    out->tail_iterations = opts ? opts->tail_iterations : 0;
+    out->tail_step_iterations = opts ? opts->tail_step_iterations : 0;
     if (out->mode != ART_INIT_DECODED && out->mode != ART_INIT_SCALAR_COMPAT && out->mode != ART_INIT_LEARNED)
         return fail(ART_ERR_INVALID_ARGUMENT, "unknown init mode");
     if (out->mode == ART_INIT_LEARNED && !ctx->net)
@@ -1593,7 +1619,7 @@ int32_t art_context_compute_device(ArtContext *ctx, uint32_t nchannel, const Art
                  max_h};
     for (uint32_t c = 0; c < nchannel; c++) sp.src[c] = coefs[c].dct_coefs;
     rc = prepare_batch(ctx, {sp}, iterations, ini.mode, ini.step_iterations);
-    if (!rc) rc = run_iterations(ctx, iterations);
+    if (!rc) rc = run_iterations(ctx, iterations, ini.tail_iterations, ini.tail_stepmul(iterations));
     if (!rc) {
         const float *fb;
         int fp;
@@ -1715,7 +1741,7 @@ static int solve_host(ArtContext *ctx, uint32_t nchannel, const ArtChannel *coef
         sp.src[c] = dst;
     }
     rc = prepare_batch(ctx, {sp}, iterations, ini.mode, ini.step_iterations);
-    if (!rc) rc = run_iterations(ctx, iterations);
+    if (!rc) rc = run_iterations(ctx, iterations, ini.tail_iterations, ini.tail_stepmul(iterations));
     return rc;
 }
 
@@ -1870,7 +1896,7 @@ int32_t art_context_compute_batch(ArtContext *ctx, uint32_t nimages, const ArtIm
             off += align_up(n, 256);
         }
     rc = prepare_batch(ctx, specs, iterations, ini.mode, ini.step_iterations);
-    if (!rc) rc = run_iterations(ctx, iterations);
+    if (!rc) rc = run_iterations(ctx, iterations, ini.tail_iterations, ini.tail_stepmul(iterations));
     if (rc) {
         cudaStreamSynchronize(ctx->stream);
         return rc;
@@ -1913,7 +1939,7 @@ int32_t art_context_compute_batch_device(ArtContext *ctx, uint32_t nimages, cons
         ART_CUDA(cudaStreamWaitEvent(ctx->stream, join, 0));
     }
     rc = prepare_batch(ctx, specs, iterations, ini.mode, ini.step_iterations);
-    if (!rc) rc = run_iterations(ctx, iterations);
+    if (!rc) rc = run_iterations(ctx, iterations, ini.tail_iterations, ini.tail_stepmul(iterations));
     for (uint32_t i = 0; !rc && i < nimages; i++) {
         const float *fb;
         int fp;
@@ -2303,11 +2329,11 @@ extern "C" int32_t art_solve_noalloc(uint32_t nchannel, const ArtChannel *coefs,
     for (uint32_t it = 0; it < iterations; it++) {
         const float fnext = it + 1 < iterations ? next_factor() : 0.0f;
         if (nch == 3)
-            k_grad_sweep_n<3><<<ncta, SWEEP_WARPS_N * 32, 0, s>>>(ddesc, work);
+            k_grad_sweep_n<3><<<ncta, SWEEP_WARPS_N * 32, 0, s>>>(ddesc, work, 1.0f);
         else if (nch == 2)
-            k_grad_sweep_n<2><<<ncta, SWEEP_WARPS_N * 32, 0, s>>>(ddesc, work);
+            k_grad_sweep_n<2><<<ncta, SWEEP_WARPS_N * 32, 0, s>>>(ddesc, work, 1.0f);
         else
-            k_grad_sweep_n<1><<<ncta, SWEEP_WARPS_N * 32, 0, s>>>(ddesc, work);
+            k_grad_sweep_n<1><<<ncta, SWEEP_WARPS_N * 32, 0, s>>>(ddesc, work, 1.0f);
         for (int m = 3; m >= 0; m--) {
             const int n = mode_off[m + 1] - mode_off[m];
             if (n == 0) continue;

@@ -58,12 +58,17 @@ struct ImgDev {
     float invq2[3][64];
 };
 
+// Resident blocks per SM the sweeps' register counts must allow (wide: 3 x 4
+// warps at <= 168 registers; narrow: 2 x 8 warps). Tighter caps spill and
+// measured slower on 1080p and 24 MP.
+constexpr int SWEEP_MIN_BLOCKS = 3;
+constexpr int SWEEP_MIN_BLOCKS_N = 2;
 constexpr int SWEEP_PF = 4;       // wide sweep: y rows loaded ahead of use
 constexpr int SWEEP_PPF = 3;      // wide sweep: DCT-distance rows loaded ahead of use
 constexpr int SWEEP_OUT = 60;     // wide sweep: output columns per warp strip (32 lanes x 2 columns, 2 of halo each side)
 constexpr int SWEEP_WARPS = 4;    // wide sweep: warps (strips) per block
-constexpr int SWEEP_PF_N = 3;     // narrow sweep: y rows loaded ahead of use
-constexpr int SWEEP_PPF_N = 2;    // narrow sweep: DCT-distance rows loaded ahead of use
+constexpr int SWEEP_PF_N = 2;     // narrow sweep: y rows loaded ahead of use
+constexpr int SWEEP_PPF_N = 1;    // narrow sweep: DCT-distance rows loaded ahead of use
 constexpr int SWEEP_OUT_N = 28;   // narrow sweep: 32 lanes x 1 column, 2 of halo each side
 constexpr int SWEEP_WARPS_N = 8;  // narrow sweep: warps per block
 constexpr int PROJ_WARPS = 4;   // warps per projection block (4 coefficient blocks per warp)

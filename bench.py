@@ -246,11 +246,12 @@ class DeviceImage:
         self.outs = [torch.empty(self.H, self.pitch, device="cuda") for _ in range(self.n)]
         self.ptrs = (C.c_void_p * self.n)(*[o.data_ptr() for o in self.outs])
 
-    def solve(self, lib, ctx, iterations, init_mode, step_iterations, stream):
+    def solve(self, lib, ctx, iterations, init_mode, step_iterations, stream, tail=0, tail_step=0):
         from artefact_b200 import _native as N
 
         opts = N.ArtOptions()
         opts.init_mode, opts.device, opts.step_iterations = init_mode, -1, step_iterations
+        opts.tail_iterations, opts.tail_step_iterations = tail, tail_step
         pw = (C.c_float * 3)(PWEIGHT, PWEIGHT, PWEIGHT)
         N.check(lib.art_context_compute_device(ctx, self.n, self.ch, WEIGHT, pw, iterations, self.W, self.H,
                                                self.ptrs, self.pitch, C.byref(opts), C.c_void_p(stream.cuda_stream)))

@@ -63,7 +63,12 @@ typedef struct ArtOptions {
     uint32_t step_iterations; /* 0: step size radius / sqrt(1 + iterations) as mod.rs:71 forms it; otherwise
                                  radius / sqrt(1 + step_iterations), the step of a run of that many iterations
                                  (a refinement after a learned start can take a long run's step) */
-    uint32_t reserved[5];
+    uint32_t tail_iterations; /* 0: one phase (the reference). Otherwise the last tail_iterations of the
+                                 `iterations` form a second phase: FISTA restarted and steps of
+                                 radius / sqrt(1 + tail_step_iterations) -- large steps first to remove a warm
+                                 start's error, then small ones to settle. No reference counterpart. */
+    uint32_t tail_step_iterations;
+    uint32_t reserved[3];
 } ArtOptions;
 
 typedef struct ArtContext ArtContext;

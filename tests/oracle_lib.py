@@ -50,8 +50,8 @@ def lib() -> C.CDLL:
                           C.POINTER(P)]
             f2 = getattr(h, f"oracle_{prec}_compute_from")
             f2.restype = C.c_int
-            f2.argtypes = [C.c_uint32, CH, C.c_float, FP, C.c_uint32, C.c_uint32, C.c_uint32, C.c_uint32, C.c_int,
-                           C.POINTER(FP), C.POINTER(P)]
+            f2.argtypes = [C.c_uint32, CH, C.c_float, FP, C.c_uint32, C.c_uint32, C.c_uint32, C.c_uint32,
+                           C.c_uint32, C.c_uint32, C.c_int, C.POINTER(FP), C.POINTER(P)]
             g = getattr(h, f"oracle_{prec}_gradient")
             g.restype = C.c_int
             g.argtypes = [C.c_uint32, CH, C.c_float, FP, C.c_uint32, C.c_uint32, C.POINTER(P), C.POINTER(P)]
@@ -107,10 +107,12 @@ def compute(nch: int, coefs, weight: float, pweight, iterations: int, W: int, H:
 
 
 def compute_from(nch: int, coefs, weight: float, pweight, iterations: int, W: int, H: int, start,
-                 step_iterations: int = 0, fp64: bool = False) -> List[np.ndarray]:
+                 step_iterations: int = 0, fp64: bool = False, tail_iterations: int = 0,
+                 tail_step_iterations: int = 0) -> List[np.ndarray]:
     """The oracle's iteration from given full-resolution start planes (a warm
     start): projection of the start, then `iterations` steps of size
-    radius / sqrt(1 + (step_iterations or iterations))."""
+    radius / sqrt(1 + (step_iterations or iterations)); the last
+    `tail_iterations` restart FISTA with steps radius / sqrt(1 + tail_step_iterations)."""
     h = lib()
     chans, keep = _channels(coefs[:nch])
     dt, ct = (np.float64, C.c_double) if fp64 else (np.float32, C.c_float)
@@ -120,7 +122,8 @@ def compute_from(nch: int, coefs, weight: float, pweight, iterations: int, W: in
     outs = [np.empty(W * H, dtype=dt) for _ in range(nch)]
     ptrs = (C.POINTER(ct) * nch)(*[o.ctypes.data_as(C.POINTER(ct)) for o in outs])
     fn = h.oracle_f64_compute_from if fp64 else h.oracle_f32_compute_from
-    rc = fn(nch, chans, float(weight), _pw(pweight), int(iterations), int(step_iterations), W, H, 0, sp, ptrs)
+    rc = fn(nch, chans, float(weight), _pw(pweight), int(iterations), int(step_iterations), int(tail_iterations),
+            int(tail_step_iterations), W, H, 0, sp, ptrs)
     if rc != 0:
         raise ValueError("oracle rejected its input")
     return outs

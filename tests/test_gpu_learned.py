@@ -87,8 +87,9 @@ def _upsampled_prediction(net, j):
 
 
 @pytest.mark.parametrize("shape", CASES, ids=IDS)
-@pytest.mark.parametrize("iterations,step_iterations", [(0, 0), (1, 0), (8, 0), (8, 50)])
-def test_learned_start_matches_oracle(gpu, ctx, shape, iterations, step_iterations):
+@pytest.mark.parametrize("iterations,step_iterations,tail,tail_step",
+                         [(0, 0, 0, 0), (1, 0, 0, 0), (8, 0, 0, 0), (8, 50, 0, 0), (10, 8, 4, 60), (6, 0, 6, 20)])
+def test_learned_start_matches_oracle(gpu, ctx, shape, iterations, step_iterations, tail, tail_step):
     j = jpeg_of(*shape)
     W, H, _ = j.max_rounded()
     n = j.nchannel
@@ -96,13 +97,16 @@ def test_learned_start_matches_oracle(gpu, ctx, shape, iterations, step_iteratio
     ctx.set_warm_start(net)
     try:
         gpu_planes = ctx.compute(n, j.coefs, WEIGHT, PW, iterations, W, H, init_mode=N.ART_INIT_LEARNED,
-                                 step_iterations=step_iterations)
+                                 step_iterations=step_iterations, tail_iterations=tail,
+                                 tail_step_iterations=tail_step)
         ev = ctx.evaluate()
     finally:
         ctx.set_warm_start(None)
     start = _upsampled_prediction(net, j)
-    ref = O.compute_from(n, j.coefs, WEIGHT, PW, iterations, W, H, start, step_iterations)
-    r64 = O.compute_from(n, j.coefs, WEIGHT, PW, iterations, W, H, start, step_iterations, fp64=True)
+    ref = O.compute_from(n, j.coefs, WEIGHT, PW, iterations, W, H, start, step_iterations,
+                         tail_iterations=tail, tail_step_iterations=tail_step)
+    r64 = O.compute_from(n, j.coefs, WEIGHT, PW, iterations, W, H, start, step_iterations, fp64=True,
+                         tail_iterations=tail, tail_step_iterations=tail_step)
     d = max(float(np.abs(a.astype(np.float64) - b).max()) for a, b in zip(gpu_planes, ref))
     d64 = max(float(np.abs(a.astype(np.float64) - b).max()) for a, b in zip(gpu_planes, r64))
     moved = max(float(np.abs(s.ravel() - a).max()) for s, a in zip(start, ref))
