@@ -66,7 +66,8 @@ WORKLOADS["network"] = dict(
     metric="TFLOP/s (warm-start network forward, 1080p 4:2:0)", iterations=0)
 LEARNED_QUALITIES = (30, 50, 75)
 REFINE_ITERATIONS = 8
-REFINE_STEP_ITERATIONS = 50  # refinement steps of the 50-iteration run's size
+REFINE_STEP_ITERATIONS = 4         # first refinement phase: steps of a 4-iteration run
+REFINE_TAIL_STEP_ITERATIONS = 100  # last quarter: steps of a 100-iteration run
 WEIGHT, PWEIGHT = 0.3, 0.001
 
 
@@ -257,16 +258,24 @@ class DeviceImage:
                                                self.ptrs, self.pitch, C.byref(opts), C.c_void_p(stream.cuda_stream)))
 
 
-def learned_comparison(lib, device, steps, warmup, refine=REFINE_ITERATIONS, step_iterations=REFINE_STEP_ITERATIONS,
-                       qualities=LEARNED_QUALITIES):
+def refine_schedule(k):
+    """Refinement after a learned start: k plain iterations, the first k - k/4
+    with the step of a REFINE_STEP_ITERATIONS-iteration run (large: they remove
+    the prediction's error), the last k/4 restarted with the step of a
+    REFINE_TAIL_STEP_ITERATIONS-iteration run (small: they settle)."""
+    return dict(step=REFINE_STEP_ITERATIONS, tail=max(1, k // 4), tail_step=REFINE_TAIL_STEP_ITERATIONS)
+
+
+def learned_comparison(lib, device, steps, warmup, refine=REFINE_ITERATIONS, qualities=LEARNED_QUALITIES):
     """Learned warm start + `refine` plain iterations against the plain
     50-iteration solve, per quality, on seeded 1920x1080 4:2:0 JPEGs (seeds
     5000 + quality, outside the network's training seeds). Each path is timed
     from device-resident coefficients to device-resident planes (CUDA events,
     L2 flushed between steps); its objective and feasibility come from
-    art_context_evaluate. Also reports the fewest refinement iterations (of a
+    art_context_evaluate. Also finds the fewest refinement iterations (of a
     fixed ladder) whose objective reaches the plain 50-iteration one within
-    1e-4 relative. None when the package holds no trained weights."""
+    1e-4 relative, and times that. The decoded start with the same schedule
+    is the control. None when the package holds no trained weights."""
     import torch
 
     from artefact_b200 import _native as N
@@ -288,17 +297,23 @@ def learned_comparison(lib, device, steps, warmup, refine=REFINE_ITERATIONS, ste
         N.check(lib.art_context_evaluate(ctx, 0, out))
         return out[0], out[4]
 
-    def timed(img, its, mode, step_its):
+    def run(img, its, mode, sched):
+        if sched is None:
+            img.solve(lib, ctx, its, mode, 0, stream)
+        else:
+            img.solve(lib, ctx, its, mode, sched["step"], stream, sched["tail"], sched["tail_step"])
+
+    def timed(img, its, mode, sched):
         for _ in range(warmup):
             flush.fill_(1.0)
-            img.solve(lib, ctx, its, mode, step_its, stream)
+            run(img, its, mode, sched)
         torch.cuda.synchronize()
         ms = []
         for k in range(steps):
             flush.fill_(float(k))
             a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
             a.record(stream)
-            img.solve(lib, ctx, its, mode, step_its, stream)
+            run(img, its, mode, sched)
             b.record(stream)
             b.synchronize()
             ms.append(a.elapsed_time(b))
@@ -306,50 +321,59 @@ def learned_comparison(lib, device, steps, warmup, refine=REFINE_ITERATIONS, ste
         return statistics.median(ms)
 
     rows = []
-    ladder = (2, 4, 6, 8, 12, 16, 24, 32, 48)
+    ladder = (8, 12, 16, 20, 24, 28, 32, 40, 48)
     for q in qualities:
         j = Jpeg.from_source(JpegSource.Buffer(synth.make_jpeg(1920, 1080, q, "4:2:0", False, seed=5000 + q)))
         img = DeviceImage(j)
         mpix = j.real_px_w * j.real_px_h / 1e6
-        plain_ms = timed(img, 50, N.ART_INIT_DECODED, 0)
+        plain_ms = timed(img, 50, N.ART_INIT_DECODED, None)
         e50, f50 = evaluate()
-        learned_ms = timed(img, refine, N.ART_INIT_LEARNED, step_iterations)
+        sched = refine_schedule(refine)
+        learned_ms = timed(img, refine, N.ART_INIT_LEARNED, sched)
         el, fl = evaluate()
-        img.solve(lib, ctx, refine, N.ART_INIT_DECODED, step_iterations, stream)
+        run(img, refine, N.ART_INIT_DECODED, sched)
         ed, _ = evaluate()
-        kmin = None
+        run(img, refine, N.ART_INIT_LEARNED, None)
+        el_plain_step = evaluate()[0]
+        run(img, 0, N.ART_INIT_LEARNED, None)
+        e_start = evaluate()[0]
+        kmin, ek_min = None, None
         for k in ladder:
-            img.solve(lib, ctx, k, N.ART_INIT_LEARNED, step_iterations, stream)
+            run(img, k, N.ART_INIT_LEARNED, refine_schedule(k))
             ek, fk = evaluate()
             if ek <= e50 * (1 + 1e-4) and fk <= 1e-3:
-                kmin = k
+                kmin, ek_min = k, ek
                 break
-        kmin_ms = timed(img, kmin, N.ART_INIT_LEARNED, step_iterations) if kmin else None
-        sweep = {}
-        for si in (8, 16, 30, 50, 100, 300):
-            img.solve(lib, ctx, refine, N.ART_INIT_LEARNED, si, stream)
-            sweep[si] = (evaluate()[0] - e50) / e50
-        img.solve(lib, ctx, 0, N.ART_INIT_LEARNED, 0, stream)
-        e_start = (evaluate()[0] - e50) / e50
+        kmin_ms = timed(img, kmin, N.ART_INIT_LEARNED, refine_schedule(kmin)) if kmin else None
+        dk = None
+        if kmin:
+            run(img, kmin, N.ART_INIT_DECODED, refine_schedule(kmin))
+            dk = (evaluate()[0] - e50) / e50
         rows.append(dict(quality=q, plain50_ms=plain_ms, plain50_mpix_s=mpix / plain_ms * 1e3,
                          learned_ms=learned_ms, learned_mpix_s=mpix / learned_ms * 1e3,
                          speedup=plain_ms / learned_ms, E_plain50=e50, E_learned=el,
-                         E_learned_rel=(el - e50) / e50, E_decoded_same_iterations=ed,
+                         E_learned_rel=(el - e50) / e50, E_decoded_same_schedule_rel=(ed - e50) / e50,
+                         E_learned_single_phase_rel=(el_plain_step - e50) / e50,
+                         E_after_projection_only_rel=(e_start - e50) / e50,
                          infeasibility_learned=fl, infeasibility_plain=f50,
                          reaches_plain50=bool(el <= e50 * (1 + 1e-4) and fl <= 1e-3),
                          min_refine_to_reach=kmin,
-                         min_refine_ms=kmin_ms, min_refine_speedup=(plain_ms / kmin_ms) if kmin_ms else None,
-                         E_rel_after_projection_only=e_start, E_rel_by_refine_step_iterations=sweep))
+                         min_refine_E_rel=((ek_min - e50) / e50) if kmin else None,
+                         min_refine_decoded_same_schedule_E_rel=dk,
+                         min_refine_ms=kmin_ms, min_refine_speedup=(plain_ms / kmin_ms) if kmin_ms else None))
         log(f"learned q{q}: plain50 {plain_ms:.3f} ms E {e50:.7g}; learned+{refine} {learned_ms:.3f} ms "
-            f"E {el:.7g} ({(el - e50) / e50:+.2e}); decoded+{refine} E {ed:.7g}; reach at K={kmin}")
+            f"E {(el - e50) / e50:+.2e} (decoded start, same schedule {(ed - e50) / e50:+.2e}); "
+            f"reaches at K={kmin} in {kmin_ms} ms")
     lib.art_context_set_warm_start(ctx, None)
     lib.art_context_destroy(ctx)
     net.close()
     mp_total = sum(1920 * 1080 / 1e6 for _ in rows)
-    return dict(refine_iterations=refine, refine_step_iterations=step_iterations, images=rows,
+    reach = all(r["min_refine_to_reach"] for r in rows)
+    return dict(refine_iterations=refine, schedule=refine_schedule(refine), images=rows,
                 plain50_mpix_s=mp_total / sum(r["plain50_ms"] for r in rows) * 1e3,
                 learned_mpix_s=mp_total / sum(r["learned_ms"] for r in rows) * 1e3,
-                all_reach_plain50=all(r["reaches_plain50"] for r in rows))
+                all_reach_plain50=all(r["reaches_plain50"] for r in rows),
+                reach_mpix_s=(mp_total / sum(r["min_refine_ms"] for r in rows) * 1e3) if reach else None)
 
 
 def network_flops(H, W):
@@ -431,11 +455,14 @@ def run_learned(args, lib, local, rank, world, dist):
             "scaling": "weak", "vs_baseline": None, "dtype": "f32 solver, bf16 network (fp32 accumulation)",
             "data": "synthetic",
             "config": {"workload": wl["name"], "refine_iterations": res["refine_iterations"],
-                       "refine_step_iterations": res["refine_step_iterations"],
+                       "refine_schedule": res["schedule"],
                        "l2": "flushed between steps (256 MiB write outside the timed events)",
                        "parallelism": f"replicas x{world}"},
             "plain50_mpix_s": res["plain50_mpix_s"], "speedup_vs_plain50": value / res["plain50_mpix_s"],
-            "all_reach_plain50": res["all_reach_plain50"], "images": res["images"],
+            "all_reach_plain50": res["all_reach_plain50"],
+            "reach_plain50_mpix_s": res["reach_mpix_s"],
+            "reach_speedup_vs_plain50": (res["reach_mpix_s"] / res["plain50_mpix_s"]) if res["reach_mpix_s"] else None,
+            "images": res["images"],
             "roofline": {"bound": "tensor", "kernel": "warm-start network forward (k_conv3x3 and glue)",
                          "achieved": net_tflops, "peak": tc_peak, "unit": "TFLOP/s", "frac": net_tflops / tc_peak,
                          "traffic": None, "peak_kind": "measured" if peaks else "fallback",

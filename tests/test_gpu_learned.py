@@ -153,22 +153,29 @@ def test_learned_start_needs_a_network(gpu, ctx):
 @pytest.mark.parametrize("quality", [30, 50, 75])
 def test_trained_network_gain(gpu, ctx, quality):
     """The trained network's start against the decoded start on an image it
-    was not trained on (seed outside the training range), at equal iterations:
-    after 8 plain iterations (their step the 50-iteration run's), the learned
-    path's objective is below the decoded path's, and both stay feasible."""
+    was not trained on (seed outside the training range), with the same
+    refinement (8 and 24 iterations: steps of a 4-iteration run, the last
+    quarter restarted with steps of a 100-iteration run): the learned path's
+    objective is below the decoded path's, both stay feasible, and with 24
+    iterations the learned path is within 0.1 % of the plain 50-iteration
+    objective while the decoded path is not closer."""
     j = jpeg_of(512, 384, quality, "4:2:0", False, seed=7000 + quality)
     W, H, _ = j.max_rounded()
     net = WS.WarmStartNet.load()
-    ctx.set_warm_start(net)
-    try:
-        ctx.compute(3, j.coefs, WEIGHT, PW, 8, W, H, init_mode=N.ART_INIT_LEARNED, step_iterations=50)
-        el = ctx.evaluate()
-    finally:
-        ctx.set_warm_start(None)
-    ctx.compute(3, j.coefs, WEIGHT, PW, 8, W, H, step_iterations=50)
-    ed = ctx.evaluate()
     ctx.compute(3, j.coefs, WEIGHT, PW, 50, W, H)
-    e50 = ctx.evaluate()
-    print(f"q{quality}: E learned+8 {el['E']:.6g}  decoded+8 {ed['E']:.6g}  plain 50 {e50['E']:.6g}")
-    assert el["E"] < ed["E"]
-    assert el["infeasibility"] <= 1e-3 and ed["infeasibility"] <= 1e-3
+    e50 = ctx.evaluate()["E"]
+    for k in (8, 24):
+        sched = dict(step_iterations=4, tail_iterations=k // 4, tail_step_iterations=100)
+        ctx.set_warm_start(net)
+        try:
+            ctx.compute(3, j.coefs, WEIGHT, PW, k, W, H, init_mode=N.ART_INIT_LEARNED, **sched)
+            el = ctx.evaluate()
+        finally:
+            ctx.set_warm_start(None)
+        ctx.compute(3, j.coefs, WEIGHT, PW, k, W, H, **sched)
+        ed = ctx.evaluate()
+        print(f"q{quality} K={k}: E rel to plain 50: learned {el['E'] / e50 - 1:+.2e}, decoded {ed['E'] / e50 - 1:+.2e}")
+        assert el["E"] < ed["E"]
+        assert el["infeasibility"] <= 1e-3 and ed["infeasibility"] <= 1e-3
+        if k == 24:
+            assert el["E"] <= e50 * (1 + 1e-3)
