@@ -155,8 +155,8 @@ EXPORTS = {
                                           C.c_void_p, C.c_void_p]),
     "art_cnn_unpool_add_mask": (C.c_int32, [C.c_void_p, C.c_void_p, C.c_int32, C.c_int32, C.c_int32, C.c_int32,
                                             C.c_void_p, C.c_int32, C.c_int32, C.c_void_p]),
-    "art_cnn_bias_grad": (C.c_int32, [C.c_void_p, C.c_int64, C.c_int32, C.c_int32, C.c_void_p, C.c_int64,
-                                      C.c_void_p, C.c_int32, C.c_void_p]),
+    "art_cnn_bias_grad": (C.c_int32, [C.c_void_p, C.c_int64, C.c_int32, C.c_void_p, C.c_int64, C.c_void_p,
+                                      C.c_int32, C.c_void_p]),
     "art_cnn_features": (C.c_int32, [C.c_void_p, C.c_int32, C.c_int64, C.c_void_p, C.c_int32, C.c_int32,
                                      C.c_int32, C.c_void_p, C.c_void_p, C.c_void_p]),
     "art_cnn_residual": (C.c_int32, [C.c_void_p, C.c_int32, C.c_void_p, C.c_void_p, C.c_int32, C.c_int32,

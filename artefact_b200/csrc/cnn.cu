@@ -3,12 +3,7 @@
 // memory-bound glue around them. The network has no counterpart in the
 // reference; it only chooses where the reference's iteration starts.
 //
-// Activation tensors are bf16 in a row-blocked NHWC8 layout: element
-// (b, y, x, c) of a tensor with C channels (a multiple of 8) sits at
-// (((b * H + y) * (C / 8) + c / 8) * W + x) * 8 + c % 8. Each image row holds
-// its 8-channel groups one after another and a group's pixels 16 bytes apart,
-// so the TMA box of one group over a run of pixels is one contiguous span
-// (whole cache lines, not one 16-byte piece per pixel).
+// Tensors are NHWC bf16: element (b, y, x, c) at ((b * H + y) * W + x) * C + c.
 //
 // k_conv3x3   3x3 convolution, stride 1, zero padding 1, as an implicit GEMM:
 //             D[pixel][n] = sum_{tap, c} X[pixel + d(tap)][c] * Wt[n][tap][c].
@@ -90,13 +85,6 @@ struct WgradArgs {
     int *err;
 };
 
-// Element offset of channel group g (8 channels) of pixel (b, y, x) in a
-// row-blocked tensor of H x W pixels and C channels.
-__host__ __device__ __forceinline__ size_t grp_off(int b, int y, int x, int g, int H, int W, int C)
-{
-    return ((((size_t)b * H + y) * (size_t)(C >> 3) + g) * (size_t)W + x) * 8;
-}
-
 __device__ __forceinline__ void tile_coords(int tile, int tiles_x, int tiles_y, int trows, int &b, int &y0, int &x0)
 {
     const int per = tiles_x * tiles_y;
@@ -174,7 +162,7 @@ __global__ void __launch_bounds__(THREADS, 1) k_conv3x3(const __grid_constant__ 
                     unsigned char *st = smem + (size_t)s * a.stage_bytes;
                     tc::mbar_arrive_expect_tx(&full_bar[s], a.tx_bytes);
                     for (int j = 0; j < a.ck / 8; j++)
-                        tc::tma_load_5d(st + j * kcol, &xmap, 0, x0 - 1, (c * a.ck) / 8 + j, y0 - 1, b, &full_bar[s]);
+                        tc::tma_load_4d(st + j * kcol, &xmap, c * a.ck + 8 * j, x0 - 1, y0 - 1, b, &full_bar[s]);
                     tc::bulk_load(st + a.halo_bytes, a.wpack + (size_t)c * 9 * a.ck * a.n, 18u * a.ck * a.n,
                                   &full_bar[s]);
                 }
@@ -245,7 +233,7 @@ __global__ void __launch_bounds__(THREADS, 1) k_conv3x3(const __grid_constant__ 
             for (int t = 0; t < TR; t++) {
                 const int y = y0 + t, x = x0 + px;
                 const bool in = y < a.H && x < a.W;
-                const size_t pix = ((size_t)b * a.H + (in ? y : 0)) * a.W + (in ? x : 0);  // fp32 output (NHWC)
+                const size_t pix = ((size_t)b * a.H + (in ? y : 0)) * a.W + (in ? x : 0);
 #pragma unroll 1
                 for (int c0 = 0; c0 < a.n; c0 += 16) {
                     float v[16];
@@ -260,9 +248,8 @@ __global__ void __launch_bounds__(THREADS, 1) k_conv3x3(const __grid_constant__ 
                         for (int i = 0; i < 16; i++) v[i] = fmaxf(v[i], 0.f);
                     }
                     if (a.mask) {
-                        const bf16 *mb = a.mask + grp_off(b, y, x, c0 / 8, a.H, a.W, a.mask_cstride);
-                        const uint4 m2[2] = {__ldg(reinterpret_cast<const uint4 *>(mb)),
-                                             __ldg(reinterpret_cast<const uint4 *>(mb + (size_t)a.W * 8))};
+                        const uint4 *mp = reinterpret_cast<const uint4 *>(a.mask + pix * a.mask_cstride + c0);
+                        const uint4 m2[2] = {__ldg(mp), __ldg(mp + 1)};
                         const bf16 *m = reinterpret_cast<const bf16 *>(m2);
 #pragma unroll
                         for (int i = 0; i < 16; i++) v[i] = __bfloat162float(m[i]) > 0.f ? v[i] : 0.f;
@@ -273,10 +260,9 @@ __global__ void __launch_bounds__(THREADS, 1) k_conv3x3(const __grid_constant__ 
                         for (int i = 0; i < 4; i++) o[i] = make_float4(v[4 * i], v[4 * i + 1], v[4 * i + 2], v[4 * i + 3]);
                     }
                     if (a.out) {
-                        bf16 *ob = a.out + grp_off(b, y, x, (a.out_coff + c0) / 8, a.H, a.W, a.out_cstride);
-                        uint4 *o0 = reinterpret_cast<uint4 *>(ob), *o1 = reinterpret_cast<uint4 *>(ob + (size_t)a.W * 8);
+                        uint4 *o = reinterpret_cast<uint4 *>(a.out + pix * a.out_cstride + a.out_coff + c0);
                         if (a.accumulate) {
-                            const uint4 p2[2] = {*o0, *o1};
+                            const uint4 p2[2] = {o[0], o[1]};
                             const bf16 *p = reinterpret_cast<const bf16 *>(p2);
 #pragma unroll
                             for (int i = 0; i < 16; i++) v[i] += __bfloat162float(p[i]);
@@ -285,8 +271,8 @@ __global__ void __launch_bounds__(THREADS, 1) k_conv3x3(const __grid_constant__ 
                         __nv_bfloat162 *w = reinterpret_cast<__nv_bfloat162 *>(w2);
 #pragma unroll
                         for (int i = 0; i < 8; i++) w[i] = __floats2bfloat162_rn(v[2 * i], v[2 * i + 1]);
-                        *o0 = w2[0];
-                        *o1 = w2[1];
+                        o[0] = w2[0];
+                        o[1] = w2[1];
                     }
                 }
             }
@@ -351,9 +337,9 @@ __global__ void __launch_bounds__(THREADS, 1) k_wgrad3x3(const __grid_constant__
                 unsigned char *st = smem + (size_t)s * a.stage_bytes;
                 tc::mbar_arrive_expect_tx(&full_bar[s], tx_bytes);
                 for (int g = 0; g < a.cout / 8; g++)
-                    tc::tma_load_5d(st + g * DYREG, &dymap, 0, x0, g, y0, b, &full_bar[s]);
+                    tc::tma_load_4d(st + g * DYREG, &dymap, 8 * g, x0, y0, b, &full_bar[s]);
                 for (int j = 0; j < a.nci / 8; j++)
-                    tc::tma_load_5d(st + dy_bytes + j * KCOL, &xmap, 0, x0 - 1, (chunk * a.nci) / 8 + j, y0 - 1, b,
+                    tc::tma_load_4d(st + dy_bytes + j * KCOL, &xmap, chunk * a.nci + 8 * j, x0 - 1, y0 - 1, b,
                                     &full_bar[s]);
             }
             const uint32_t last = it;
@@ -470,9 +456,8 @@ __global__ void k_pack(const float *__restrict__ w, int cout, int cin, int trans
     out[i] = __float2bfloat16_rn(v);
 }
 
-// 2x2 average pooling (8 channels per thread) of channels [in_coff,
-// in_coff + C) of a tensor with in_cstride channels into a tensor with C.
-// Threads run along x within a channel group (contiguous in this layout).
+// 2x2 average pooling (NHWC, 8 channels per thread) of channels
+// [in_coff, in_coff + C) of a tensor with in_cstride channels.
 __global__ void k_pool2(const bf16 *__restrict__ in, int B, int H, int W, int C, int in_cstride, int in_coff,
                         bf16 *__restrict__ out)
 {
@@ -480,17 +465,18 @@ __global__ void k_pool2(const bf16 *__restrict__ in, int B, int H, int W, int C,
     const long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
     const long long total = (long long)B * Ho * Wo * cg;
     if (i >= total) return;
-    const int x = (int)(i % Wo);
-    const long long r = i / Wo;
-    const int g = (int)(r % cg), y = (int)((r / cg) % Ho), b = (int)(r / ((long long)cg * Ho));
+    const int g = (int)(i % cg);
+    const long long p = i / cg;
+    const int x = (int)(p % Wo), y = (int)((p / Wo) % Ho), b = (int)(p / ((long long)Wo * Ho));
     float acc[8] = {0, 0, 0, 0, 0, 0, 0, 0};
 #pragma unroll
     for (int dy = 0; dy < 2; dy++)
 #pragma unroll
         for (int dx = 0; dx < 2; dx++) {
-            const uint4 rv = __ldg(reinterpret_cast<const uint4 *>(
-                in + grp_off(b, 2 * y + dy, 2 * x + dx, in_coff / 8 + g, H, W, in_cstride)));
-            const bf16 *v = reinterpret_cast<const bf16 *>(&rv);
+            const uint4 r =
+                __ldg(reinterpret_cast<const uint4 *>(in + (((size_t)b * H + 2 * y + dy) * W + 2 * x + dx) * in_cstride +
+                                                      in_coff + 8 * g));
+            const bf16 *v = reinterpret_cast<const bf16 *>(&r);
 #pragma unroll
             for (int k = 0; k < 8; k++) acc[k] += __bfloat162float(v[k]);
         }
@@ -498,7 +484,7 @@ __global__ void k_pool2(const bf16 *__restrict__ in, int B, int H, int W, int C,
     __nv_bfloat162 *w = reinterpret_cast<__nv_bfloat162 *>(&o);
 #pragma unroll
     for (int k = 0; k < 4; k++) w[k] = __floats2bfloat162_rn(0.25f * acc[2 * k], 0.25f * acc[2 * k + 1]);
-    *reinterpret_cast<uint4 *>(out + grp_off(b, y, x, g, Ho, Wo, C)) = o;
+    *reinterpret_cast<uint4 *>(out + (((size_t)b * Ho + y) * Wo + x) * C + 8 * g) = o;
 }
 
 // Nearest 2x upsampling of in[B][H/2][W/2][C] into channels [coff, coff + C)
@@ -510,11 +496,12 @@ __global__ void k_upsample2(const bf16 *__restrict__ in, int B, int H, int W, in
     const long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
     const long long total = (long long)B * H * W * cg;
     if (i >= total) return;
-    const int x = (int)(i % W);
-    const long long r = i / W;
-    const int g = (int)(r % cg), y = (int)((r / cg) % H), b = (int)(r / ((long long)cg * H));
-    const uint4 v = __ldg(reinterpret_cast<const uint4 *>(in + grp_off(b, y / 2, x / 2, g, H / 2, W / 2, C)));
-    *reinterpret_cast<uint4 *>(out + grp_off(b, y, x, coff / 8 + g, H, W, Cs)) = v;
+    const int g = (int)(i % cg);
+    const long long p = i / cg;
+    const int x = (int)(p % W), y = (int)((p / W) % H), b = (int)(p / ((long long)W * H));
+    const uint4 r = __ldg(
+        reinterpret_cast<const uint4 *>(in + (((size_t)b * (H / 2) + y / 2) * (W / 2) + x / 2) * C + 8 * g));
+    *reinterpret_cast<uint4 *>(out + (((size_t)b * H + y) * W + x) * Cs + coff + 8 * g) = r;
 }
 
 // Backward of nearest upsampling followed by the ReLU mask of the upsampled
@@ -526,20 +513,21 @@ __global__ void k_downsum2_mask(const bf16 *__restrict__ g, int B, int H, int W,
     const long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
     const long long total = (long long)B * Ho * Wo * cg;
     if (i >= total) return;
-    const int x = (int)(i % Wo);
-    const long long r = i / Wo;
-    const int k8 = (int)(r % cg), y = (int)((r / cg) % Ho), b = (int)(r / ((long long)cg * Ho));
+    const int k8 = (int)(i % cg);
+    const long long p = i / cg;
+    const int x = (int)(p % Wo), y = (int)((p / Wo) % Ho), b = (int)(p / ((long long)Wo * Ho));
     float acc[8] = {0, 0, 0, 0, 0, 0, 0, 0};
 #pragma unroll
     for (int dy = 0; dy < 2; dy++)
 #pragma unroll
         for (int dx = 0; dx < 2; dx++) {
-            const uint4 rv = __ldg(reinterpret_cast<const uint4 *>(g + grp_off(b, 2 * y + dy, 2 * x + dx, k8, H, W, C)));
-            const bf16 *v = reinterpret_cast<const bf16 *>(&rv);
+            const uint4 r =
+                __ldg(reinterpret_cast<const uint4 *>(g + (((size_t)b * H + 2 * y + dy) * W + 2 * x + dx) * C + 8 * k8));
+            const bf16 *v = reinterpret_cast<const bf16 *>(&r);
 #pragma unroll
             for (int k = 0; k < 8; k++) acc[k] += __bfloat162float(v[k]);
         }
-    const size_t o = grp_off(b, y, x, k8, Ho, Wo, C);
+    const size_t o = (((size_t)b * Ho + y) * Wo + x) * C + 8 * k8;
     const uint4 ra = __ldg(reinterpret_cast<const uint4 *>(act + o));
     const bf16 *av = reinterpret_cast<const bf16 *>(&ra);
     uint4 res;
@@ -563,14 +551,14 @@ __global__ void k_unpool_add_mask(bf16 *__restrict__ g, const bf16 *__restrict__
     const long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
     const long long total = (long long)B * H * W * cg;
     if (i >= total) return;
-    const int x = (int)(i % W);
-    const long long r = i / W;
-    const int k8 = (int)(r % cg), y = (int)((r / cg) % H), b = (int)(r / ((long long)cg * H));
-    const size_t o = grp_off(b, y, x, k8, H, W, C);
+    const int k8 = (int)(i % cg);
+    const long long p = i / cg;
+    const int x = (int)(p % W), y = (int)((p / W) % H), b = (int)(p / ((long long)W * H));
+    const size_t o = (size_t)p * C + 8 * k8;
     uint4 rg = *reinterpret_cast<const uint4 *>(g + o);
-    const uint4 ra = __ldg(reinterpret_cast<const uint4 *>(act + grp_off(b, y, x, act_coff / 8 + k8, H, W, act_cstride)));
+    const uint4 ra = __ldg(reinterpret_cast<const uint4 *>(act + (size_t)p * act_cstride + act_coff + 8 * k8));
     uint4 rp = make_uint4(0, 0, 0, 0);
-    if (gp) rp = __ldg(reinterpret_cast<const uint4 *>(gp + grp_off(b, y / 2, x / 2, k8, H / 2, W / 2, C)));
+    if (gp) rp = __ldg(reinterpret_cast<const uint4 *>(gp + (((size_t)b * (H / 2) + y / 2) * (W / 2) + x / 2) * C + 8 * k8));
     const bf16 *gv = reinterpret_cast<const bf16 *>(&rg), *av = reinterpret_cast<const bf16 *>(&ra),
                *pv = reinterpret_cast<const bf16 *>(&rp);
     uint4 res;
@@ -586,21 +574,17 @@ __global__ void k_unpool_add_mask(bf16 *__restrict__ g, const bf16 *__restrict__
     *reinterpret_cast<uint4 *>(g + o) = res;
 }
 
-// Per-channel sums over all pixels of a row-blocked g (npix pixels in rows of
-// W; bias gradient), two passes with a fixed order: blocks write partials,
-// one block adds them.
-__global__ void k_colsum_partial(const bf16 *__restrict__ g, long long npix, int W, int C, float *__restrict__ partial)
+// Per-channel sums over all pixels of g[npix][C] (bias gradient), two passes
+// with a fixed order: blocks write partials, one block adds them.
+__global__ void k_colsum_partial(const bf16 *__restrict__ g, long long npix, int C, float *__restrict__ partial)
 {
     __shared__ float s[256];
     const int per_row = 256 / C;  // pixels handled per step by the block
     const int c = threadIdx.x % C, r = threadIdx.x / C;
     float acc = 0.f;
     if (r < per_row)
-        for (long long p = (long long)blockIdx.x * per_row + r; p < npix; p += (long long)gridDim.x * per_row) {
-            const long long row = p / W;
-            const int x = (int)(p - row * W);
-            acc += __bfloat162float(g[((row * (C >> 3) + (c >> 3)) * W + x) * 8 + (c & 7)]);
-        }
+        for (long long p = (long long)blockIdx.x * per_row + r; p < npix; p += (long long)gridDim.x * per_row)
+            acc += __bfloat162float(g[p * C + c]);
     s[threadIdx.x] = acc;
     __syncthreads();
     if (threadIdx.x < C) {
@@ -667,9 +651,9 @@ __global__ void k_features(const int16_t *__restrict__ coef, int cpitch, long lo
                     w[4 + k] = __float2bfloat16_rn(__ldg(qt + r * 8 + u) * (1.f / 64.f));
                 }
             }
-            bf16 *f = feat + grp_off(b, by * 4 + yy, bx * 4 + xx, 0, H0, W0, 16);
-            *reinterpret_cast<uint4 *>(f) = o[0];
-            *reinterpret_cast<uint4 *>(f + (size_t)W0 * 8) = o[1];
+            uint4 *f = reinterpret_cast<uint4 *>(feat + (((size_t)b * H0 + by * 4 + yy) * W0 + bx * 4 + xx) * 16);
+            f[0] = o[0];
+            f[1] = o[1];
         }
 }
 
@@ -706,9 +690,9 @@ __global__ void k_residual(const float *__restrict__ r, int rstride, const float
             }
         }
         if (target) {
-            bf16 *g = grad + grp_off(b, y, x, 0, H0, W0, 16);
-            *reinterpret_cast<uint4 *>(g) = o[0];
-            *reinterpret_cast<uint4 *>(g + (size_t)W0 * 8) = o[1];
+            uint4 *g = reinterpret_cast<uint4 *>(grad + p * 16);
+            g[0] = o[0];
+            g[1] = o[1];
         }
     }
     s[threadIdx.x] = acc;
@@ -773,10 +757,7 @@ PFN_cuTensorMapEncodeTiled_v12000 encode_fn()
     return fn;
 }
 
-// Tensor map over a row-blocked bf16 tensor of B x H x W pixels and C
-// channels, as 5 dimensions {8 channels, W, C/8 groups, H, B} (innermost
-// first), with a box of one channel group over bw pixels x bh rows: in shared
-// memory [bh][bw][8 channels], 16 bytes per pixel.
+// Tensor map over an NHWC bf16 tensor [B][H][W][C] with box {8, bw, bh, 1}.
 bool make_map(CUtensorMap *m, const void *base, int B, int H, int W, int C, int bw, int bh, std::string &err)
 {
     auto fn = encode_fn();
@@ -788,12 +769,11 @@ bool make_map(CUtensorMap *m, const void *base, int B, int H, int W, int C, int 
         err = "tensor base must be 16-byte aligned and channels a multiple of 8";
         return false;
     }
-    const cuuint64_t row = (cuuint64_t)W * C * 2;  // bytes of one image row, all channel groups
-    cuuint64_t dims[5] = {8, (cuuint64_t)W, (cuuint64_t)(C / 8), (cuuint64_t)H, (cuuint64_t)B};
-    cuuint64_t strides[4] = {16, (cuuint64_t)W * 16, row, row * (cuuint64_t)H};
-    cuuint32_t box[5] = {8, (cuuint32_t)bw, 1, (cuuint32_t)bh, 1};
-    cuuint32_t es[5] = {1, 1, 1, 1, 1};
-    const CUresult r = fn(m, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 5, const_cast<void *>(base), dims, strides, box, es,
+    cuuint64_t dims[4] = {(cuuint64_t)C, (cuuint64_t)W, (cuuint64_t)H, (cuuint64_t)B};
+    cuuint64_t strides[3] = {(cuuint64_t)C * 2, (cuuint64_t)W * C * 2, (cuuint64_t)H * W * C * 2};
+    cuuint32_t box[4] = {8, (cuuint32_t)bw, (cuuint32_t)bh, 1};
+    cuuint32_t es[4] = {1, 1, 1, 1};
+    const CUresult r = fn(m, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 4, const_cast<void *>(base), dims, strides, box, es,
                           CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
                           CU_TENSOR_MAP_L2_PROMOTION_L2_128B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
     if (r != CUDA_SUCCESS) {
@@ -1016,15 +996,14 @@ int32_t art_cnn_unpool_add_mask(void *g, const void *gp, int32_t B, int32_t H, i
     return check_launch("k_unpool_add_mask");
 }
 
-int32_t art_cnn_bias_grad(const void *g, int64_t npix, int32_t W, int32_t C, float *workspace,
-                          int64_t workspace_bytes, float *out, int32_t accumulate, void *stream)
+int32_t art_cnn_bias_grad(const void *g, int64_t npix, int32_t C, float *workspace, int64_t workspace_bytes,
+                          float *out, int32_t accumulate, void *stream)
 {
-    if (!g || !workspace || !out || C < 8 || C > 256 || C % 8 || W < 1 || npix % W)
-        return fail(ART_ERR_INVALID_ARGUMENT, "bias_grad: bad arguments");
+    if (!g || !workspace || !out || C < 1 || C > 256) return fail(ART_ERR_INVALID_ARGUMENT, "bias_grad: bad arguments");
     int nblk = (int)std::min<long long>(2 * num_sms(), workspace_bytes / (4LL * C));
     if (nblk < 1) return fail(ART_ERR_INVALID_ARGUMENT, "bias_grad: workspace too small");
     cudaStream_t s = static_cast<cudaStream_t>(stream);
-    k_colsum_partial<<<nblk, 256, 0, s>>>(static_cast<const bf16 *>(g), npix, W, C, workspace);
+    k_colsum_partial<<<nblk, 256, 0, s>>>(static_cast<const bf16 *>(g), npix, C, workspace);
     int32_t rc = check_launch("k_colsum_partial");
     if (rc) return rc;
     k_colsum_final<<<1, 256, 0, s>>>(workspace, nblk, C, out, accumulate);
@@ -1290,7 +1269,7 @@ int32_t wgrad(ArtNet *net, int layer, const void *x, const void *g, int B, int H
     d.err = net->errflag.as<int>();
     int32_t rc = wgrad3x3(&d, s);
     if (rc) return rc;
-    return art_cnn_bias_grad(g, (int64_t)B * H * W, W, L.cout, net->workspace.as<float>(), (int64_t)net->workspace.n,
+    return art_cnn_bias_grad(g, (int64_t)B * H * W, L.cout, net->workspace.as<float>(), (int64_t)net->workspace.n,
                              net->grads.as<float>() + net->b_off[layer], 0, s);
 }
 

@@ -251,10 +251,8 @@ int32_t art_jpeg_channel(const ArtJpeg *jpeg, uint32_t c, ArtChannel *out);
 /* ------------------------------------------------------------------------
  * Warm-start network kernels (no counterpart in the reference: the network
  * only chooses the solver's starting point). All pointers are device
- * pointers; activation tensors are bf16 in a row-blocked NHWC8 layout unless
- * stated: element (b, y, x, c) of a tensor with C channels (a multiple of 8)
- * at (((b * H + y) * (C / 8) + c / 8) * W + x) * 8 + c % 8, written
- * [B][H][W][C] below for its logical shape; `stream` is a cudaStream_t (NULL = legacy default stream). `err`
+ * pointers; tensors are NHWC bf16 ([B][H][W][C], channels innermost) unless
+ * stated; `stream` is a cudaStream_t (NULL = legacy default stream). `err`
  * is a device int that a kernel sets to 1 if one of its bounded waits gave up.
  * ------------------------------------------------------------------------ */
 
@@ -318,9 +316,9 @@ int32_t art_cnn_downsum2_mask(const void *g, int32_t B, int32_t H, int32_t W, in
  * [act_coff, act_coff + C) of a tensor with act_cstride channels. */
 int32_t art_cnn_unpool_add_mask(void *g, const void *gp, int32_t B, int32_t H, int32_t W, int32_t C, const void *act,
                                 int32_t act_cstride, int32_t act_coff, void *stream);
-/* out[c] (+)= sum over npix pixels (rows of W) of g[p][c] (bf16), fixed reduction order. */
-int32_t art_cnn_bias_grad(const void *g, int64_t npix, int32_t W, int32_t C, float *workspace,
-                          int64_t workspace_bytes, float *out, int32_t accumulate, void *stream);
+/* out[c] (+)= sum over npix pixels of g[p][c] (bf16), fixed reduction order. */
+int32_t art_cnn_bias_grad(const void *g, int64_t npix, int32_t C, float *workspace, int64_t workspace_bytes,
+                          float *out, int32_t accumulate, void *stream);
 /* Network input from B int16 coefficient images (rows of cpitch, images
  * img_stride elements apart, coefficient (v,u) of block (bx,by) at
  * (8by+v, 8bx+u)) and B quantisation tables q[B][64]: dec = IDCT(c q) per

@@ -3,11 +3,6 @@
 The oracle rounds to bf16 wherever the GPU stores bf16, so forward values
 agree up to the GPU's fp32 accumulation order (a rare flip of one bf16 ulp,
 2^-8 relative); weight gradients are fp32 sums of exact bf16 products.
-
-The oracle works on NHWC arrays; the kernels' activations are row-blocked
-(per image row, 8-channel groups of contiguous pixels), so the helpers below
-convert on the way in and out: a device activation is held as a
-[B][H][C/8][W][8] tensor.
 """
 import ctypes as C
 import sys
@@ -31,28 +26,9 @@ def _torch():
     return torch
 
 
-def _blocked(a):
-    """NHWC [B][H][W][C] -> row-blocked [B][H][C/8][W][8]."""
-    B, H, W, C = a.shape
-    return np.ascontiguousarray(np.asarray(a).reshape(B, H, W, C // 8, 8).transpose(0, 1, 3, 2, 4))
-
-
 def _bf(a):
-    """A device bf16 activation (row-blocked) from an NHWC array."""
     torch = _torch()
-    return torch.from_numpy(_blocked(np.asarray(a, np.float32))).to(torch.bfloat16).cuda()
-
-
-def _act(B, H, W, C):
-    """A zeroed device activation of logical shape [B][H][W][C]."""
-    torch = _torch()
-    return torch.zeros((B, H, C // 8, W, 8), dtype=torch.bfloat16, device="cuda")
-
-
-def _shape(t):
-    """Logical NHWC shape of a device activation."""
-    B, H, G, W, _ = t.shape
-    return B, H, W, G * 8
+    return torch.from_numpy(np.ascontiguousarray(a, np.float32)).to(torch.bfloat16).cuda()
 
 
 def _f32(a):
@@ -61,11 +37,7 @@ def _f32(a):
 
 
 def _np(t):
-    a = t.float().cpu().numpy().astype(np.float64)
-    if t.dim() == 5:  # row-blocked activation -> NHWC
-        B, H, G, W, _ = a.shape
-        a = a.transpose(0, 1, 3, 2, 4).reshape(B, H, W, G * 8)
-    return a
+    return t.float().cpu().numpy().astype(np.float64)
 
 
 def _ptr(t):
@@ -86,10 +58,10 @@ def _pack(w, transpose=0, ci0=0, n=None, ck=32):
 def _conv(x, wpack, cin, ck, n, bias=None, relu=0, mask=None, out=None, out_cstride=None, out_coff=0, f32=None,
           accumulate=0):
     torch = _torch()
-    B, H, W, _ = _shape(x)
+    B, H, W, _ = x.shape
     err = torch.zeros(1, dtype=torch.int32, device="cuda")
     if out is None and f32 is None:
-        out = _act(B, H, W, n)
+        out = torch.zeros((B, H, W, n), dtype=torch.bfloat16, device="cuda")
     d = N.ArtCnnConv()
     d.B, d.H, d.W, d.cin, d.ck, d.n, d.n_store = B, H, W, cin, ck, n, n
     d.x, d.wpack = x.data_ptr(), wpack.data_ptr()
@@ -100,7 +72,7 @@ def _conv(x, wpack, cin, ck, n, bias=None, relu=0, mask=None, out=None, out_cstr
     d.out_f32 = f32.data_ptr() if f32 is not None else None
     d.f32_cstride = n
     d.mask = mask.data_ptr() if mask is not None else None
-    d.mask_cstride = _shape(mask)[-1] if mask is not None else 0
+    d.mask_cstride = mask.shape[-1] if mask is not None else 0
     d.relu, d.accumulate = relu, accumulate
     d.err = err.data_ptr()
     N.check(N.lib().art_cnn_conv3x3(C.byref(d), None))
@@ -194,7 +166,7 @@ def test_memory_kernels(gpu):
     # pointer is taken, and the next input could be placed in the same memory.
     a = O.bf16(rng.standard_normal((B, H, W, 48)))
     a_d = _bf(a)
-    out = _act(B, H // 2, W // 2, C)
+    out = torch.empty((B, H // 2, W // 2, C), dtype=torch.bfloat16, device="cuda")
     N.check(N.lib().art_cnn_pool2(_ptr(a_d), B, H, W, C, 48, 16, _ptr(out), None))
     np.testing.assert_array_equal(_np(out), O.bf16(O.pool(a[..., 16:32])))
     lo = O.bf16(rng.standard_normal((B, H // 2, W // 2, C)))
@@ -205,7 +177,7 @@ def test_memory_kernels(gpu):
     g = O.bf16(rng.standard_normal((B, H, W, C)))
     act = O.bf16(rng.standard_normal((B, H // 2, W // 2, C)))
     g_d, act_d = _bf(g), _bf(act)
-    ds = _act(B, H // 2, W // 2, C)
+    ds = torch.empty((B, H // 2, W // 2, C), dtype=torch.bfloat16, device="cuda")
     N.check(N.lib().art_cnn_downsum2_mask(_ptr(g_d), B, H, W, C, _ptr(act_d), _ptr(ds), None))
     np.testing.assert_array_equal(_np(ds), O.bf16(O.downsum(g) * (act > 0)))
     gs = O.bf16(rng.standard_normal((B, H, W, C)))
