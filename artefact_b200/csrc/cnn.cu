@@ -42,12 +42,11 @@ namespace cnn {
 using bf16 = __nv_bfloat16;
 
 constexpr int TPX = 128;                    // output pixels per tile row (MMA M)
-constexpr int TROWS = 2;                    // weight gradient: output rows per tile
-constexpr int MAX_TROWS = 2;                // convolution: output rows per tile, chosen per launch (1..MAX_TROWS;
-                                            // taller tiles measured slower: fewer tiles balance worse over the SMs)
+constexpr int TROWS = 2;                    // output rows per tile (taller tiles measured slower: fewer tiles
+                                            // balance worse over the SMs)
 constexpr int HPX = TPX + 2;                // halo tile width
-constexpr int HROWS = TROWS + 2;            // weight gradient: halo tile height
-constexpr uint32_t KCOL = HROWS * HPX * 16; // weight gradient: bytes of one 8-channel column of a halo tile (8320)
+constexpr int HROWS = TROWS + 2;            // halo tile height
+constexpr uint32_t KCOL = HROWS * HPX * 16; // bytes of one 8-channel column of a halo tile (8320, 65 x 128)
 constexpr uint32_t DYREG = TROWS * TPX * 16;// bytes of one 8-channel region of a gradient tile (4096)
 constexpr int THREADS = 192;                // warp 0 loads, warp 1 MMA, warps 2-5 epilogue
 constexpr uint32_t SMEM_BUDGET = 220 * 1024;  // pipeline stages; 1 KB more is requested for alignment
@@ -66,11 +65,9 @@ struct ConvArgs {
     const bf16 *mask;   // optional: zero where mask <= 0 (ReLU backward)
     int mask_cstride;
     int relu, accumulate;
+    bf16 *pool_out;     // optional: 2x2 average of the stored output, [B][H/2][W/2][n_store]
+    int up2;            // out is 2H x 2W: each pixel stored to its 2x2 cell
     int stages;
-    int trows;          // output rows per tile; accumulators of 2 * trows rows x n columns fit TMEM's 512
-    uint32_t kcol;      // shared-memory stride of the 8-channel columns of a halo tile: (trows + 2) * HPX * 16
-                        // bytes rounded up to 128 (TMA destinations stay 128-byte aligned)
-    uint32_t tx_bytes;  // bytes the TMA and bulk copies of one stage deliver
     uint32_t stage_bytes, halo_bytes;
     int *err;
 };
@@ -119,9 +116,7 @@ __global__ void __launch_bounds__(THREADS, 1) k_conv3x3(const __grid_constant__ 
     volatile int *abort_p = &abort_s;
 
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const int TR = a.trows;
-    const uint32_t kcol = a.kcol;
-    const int tiles_x = (a.W + TPX - 1) / TPX, tiles_y = (a.H + TR - 1) / TR;
+    const int tiles_x = (a.W + TPX - 1) / TPX, tiles_y = (a.H + TROWS - 1) / TROWS;
     const int ntiles = a.B * tiles_x * tiles_y;
     const int nchunks = a.cin / a.ck;
     const int S = a.stages;
@@ -151,7 +146,7 @@ __global__ void __launch_bounds__(THREADS, 1) k_conv3x3(const __grid_constant__ 
             bool ok = true;
             for (int tile = blockIdx.x; tile < ntiles && ok; tile += gridDim.x) {
                 int b, y0, x0;
-                tile_coords(tile, tiles_x, tiles_y, TR, b, y0, x0);
+                tile_coords(tile, tiles_x, tiles_y, TROWS, b, y0, x0);
                 for (int c = 0; c < nchunks; c++, it++) {
                     const int s = it % S;
                     const uint32_t use = it / S;
@@ -160,9 +155,9 @@ __global__ void __launch_bounds__(THREADS, 1) k_conv3x3(const __grid_constant__ 
                         break;
                     }
                     unsigned char *st = smem + (size_t)s * a.stage_bytes;
-                    tc::mbar_arrive_expect_tx(&full_bar[s], a.tx_bytes);
+                    tc::mbar_arrive_expect_tx(&full_bar[s], a.stage_bytes);
                     for (int j = 0; j < a.ck / 8; j++)
-                        tc::tma_load_4d(st + j * kcol, &xmap, c * a.ck + 8 * j, x0 - 1, y0 - 1, b, &full_bar[s]);
+                        tc::tma_load_4d(st + j * KCOL, &xmap, c * a.ck + 8 * j, x0 - 1, y0 - 1, b, &full_bar[s]);
                     tc::bulk_load(st + a.halo_bytes, a.wpack + (size_t)c * 9 * a.ck * a.n, 18u * a.ck * a.n,
                                   &full_bar[s]);
                 }
@@ -176,6 +171,14 @@ __global__ void __launch_bounds__(THREADS, 1) k_conv3x3(const __grid_constant__ 
     } else if (warp == 1) {
         if (lane == 0) {
             const uint32_t idesc = tc::idesc_bf16(128, a.n, 0, 0);
+            // Descriptors are built once with address 0 and offset per MMA by
+            // adding the operand's address / 16 to the low 14-bit field (shared
+            // memory addresses stay below 256 KB, so the add never carries), which
+            // keeps the issuing thread to a few instructions per MMA.
+            const uint64_t adesc0 = tc::smem_desc(0, KCOL, 128);
+            const uint64_t bdesc0 = tc::smem_desc(0, (uint32_t)a.n * 16, 128);
+            const uint32_t nk = (uint32_t)a.ck / 16;     // K = 16 slices per 8-channel column pair
+            const uint32_t bcol = (uint32_t)a.n;          // weights: descriptor units (16 B) per 8-channel column
             uint32_t it = 0, tcount = 0;
             bool ok = true;
             for (int tile = blockIdx.x; tile < ntiles && ok; tile += gridDim.x, tcount++) {
@@ -183,6 +186,7 @@ __global__ void __launch_bounds__(THREADS, 1) k_conv3x3(const __grid_constant__ 
                 const uint32_t ause = tcount >> 1;
                 if (ause > 0 && !tc::mbar_wait(&acce_bar[ab], (ause - 1) & 1, abort_p)) break;
                 tc::tc_fence_after();
+                const uint32_t d0 = tbase + (uint32_t)(ab * TROWS * 128), d1 = d0 + 128;
                 for (int c = 0; c < nchunks; c++, it++) {
                     const int s = it % S;
                     if (!tc::mbar_wait(&full_bar[s], (it / S) & 1, abort_p)) {
@@ -190,20 +194,20 @@ __global__ void __launch_bounds__(THREADS, 1) k_conv3x3(const __grid_constant__ 
                         break;
                     }
                     tc::tc_fence_after();
-                    const uint32_t st = tc::smem_u32(smem + (size_t)s * a.stage_bytes);
-                    const uint32_t wst = st + a.halo_bytes;
+                    const uint32_t st4 = tc::smem_u32(smem + (size_t)s * a.stage_bytes) >> 4;
+                    const uint32_t wst4 = st4 + (a.halo_bytes >> 4);
+#pragma unroll
                     for (int tap = 0; tap < 9; tap++) {
-                        const int ty = tap / 3, tx = tap % 3;
-                        for (int kk = 0; kk < a.ck / 16; kk++) {
-                            const uint64_t bdesc =
-                                tc::smem_desc(wst + (uint32_t)((tap * (a.ck / 8) + 2 * kk) * a.n * 16), a.n * 16, 128);
-#pragma unroll 1
-                            for (int t = 0; t < TR; t++) {
-                                const uint64_t adesc = tc::smem_desc(
-                                    st + 2 * kk * kcol + (uint32_t)(((t + ty) * HPX + tx) * 16), kcol, 128);
-                                tc::mma_bf16(tbase + (uint32_t)((ab * TR + t) * a.n), adesc, bdesc, idesc,
-                                             (c | tap | kk) != 0);
-                            }
+                        const uint32_t ty = tap / 3, tx = tap % 3;
+#pragma unroll
+                        for (uint32_t kk = 0; kk < 2; kk++) {
+                            if (kk >= nk) continue;
+                            const uint64_t bdesc = bdesc0 + (uint64_t)(wst4 + (tap * 2 * nk + 2 * kk) * bcol);
+                            const uint64_t adesc =
+                                adesc0 + (uint64_t)(st4 + 2 * kk * (KCOL >> 4) + ty * HPX + tx);
+                            const uint32_t acc = (c | tap | kk) != 0;
+                            tc::mma_bf16(d0, adesc, bdesc, idesc, acc);
+                            tc::mma_bf16(d1, adesc + HPX, bdesc, idesc, acc);
                         }
                     }
                     tc::mma_commit(&empty_bar[s]);
@@ -228,49 +232,93 @@ __global__ void __launch_bounds__(THREADS, 1) k_conv3x3(const __grid_constant__ 
             tc::mbar_wait(&accf_bar[ab], (tcount >> 1) & 1, abort_p);  // completes at once: every lane observes the phase
             tc::tc_fence_after();
             int b, y0, x0;
-            tile_coords(tile, tiles_x, tiles_y, TR, b, y0, x0);
+            tile_coords(tile, tiles_x, tiles_y, TROWS, b, y0, x0);
+            const int x = x0 + px;
 #pragma unroll 1
-            for (int t = 0; t < TR; t++) {
-                const int y = y0 + t, x = x0 + px;
-                const bool in = y < a.H && x < a.W;
-                const size_t pix = ((size_t)b * a.H + (in ? y : 0)) * a.W + (in ? x : 0);
-#pragma unroll 1
-                for (int c0 = 0; c0 < a.n; c0 += 16) {
-                    float v[16];
-                    tc::tmem_ld16(tbase + ((uint32_t)(q * 32) << 16) + (uint32_t)((ab * TR + t) * a.n + c0), v);
-                    if (!in || c0 >= a.n_store) continue;
+            for (int c0 = 0; c0 < a.n; c0 += 16) {
+                float v[TROWS][16];
+#pragma unroll
+                for (int t = 0; t < TROWS; t++)
+                    tc::tmem_ld16(tbase + ((uint32_t)(q * 32) << 16) + (uint32_t)((ab * TROWS + t) * 128 + c0), v[t]);
+                if (c0 >= a.n_store) continue;  // warp-uniform
+#pragma unroll
+                for (int t = 0; t < TROWS; t++) {
+                    const int y = y0 + t;
+                    const bool in = y < a.H && x < a.W;
                     if (a.bias) {
 #pragma unroll
-                        for (int i = 0; i < 16; i++) v[i] += __ldg(a.bias + c0 + i);
+                        for (int i = 0; i < 16; i++) v[t][i] += __ldg(a.bias + c0 + i);
                     }
                     if (a.relu) {
 #pragma unroll
-                        for (int i = 0; i < 16; i++) v[i] = fmaxf(v[i], 0.f);
+                        for (int i = 0; i < 16; i++) v[t][i] = fmaxf(v[t][i], 0.f);
                     }
+                    if (!in) continue;
+                    const size_t pix = ((size_t)b * a.H + y) * a.W + x;
                     if (a.mask) {
                         const uint4 *mp = reinterpret_cast<const uint4 *>(a.mask + pix * a.mask_cstride + c0);
                         const uint4 m2[2] = {__ldg(mp), __ldg(mp + 1)};
                         const bf16 *m = reinterpret_cast<const bf16 *>(m2);
 #pragma unroll
-                        for (int i = 0; i < 16; i++) v[i] = __bfloat162float(m[i]) > 0.f ? v[i] : 0.f;
+                        for (int i = 0; i < 16; i++) v[t][i] = __bfloat162float(m[i]) > 0.f ? v[t][i] : 0.f;
                     }
                     if (a.out_f32) {
                         float4 *o = reinterpret_cast<float4 *>(a.out_f32 + pix * a.f32_cstride + c0);
 #pragma unroll
-                        for (int i = 0; i < 4; i++) o[i] = make_float4(v[4 * i], v[4 * i + 1], v[4 * i + 2], v[4 * i + 3]);
+                        for (int i = 0; i < 4; i++)
+                            o[i] = make_float4(v[t][4 * i], v[t][4 * i + 1], v[t][4 * i + 2], v[t][4 * i + 3]);
                     }
                     if (a.out) {
-                        uint4 *o = reinterpret_cast<uint4 *>(a.out + pix * a.out_cstride + a.out_coff + c0);
-                        if (a.accumulate) {
-                            const uint4 p2[2] = {o[0], o[1]};
-                            const bf16 *p = reinterpret_cast<const bf16 *>(p2);
+                        uint4 w2[2];
+                        __nv_bfloat162 *w = reinterpret_cast<__nv_bfloat162 *>(w2);
+                        if (a.up2) {
 #pragma unroll
-                            for (int i = 0; i < 16; i++) v[i] += __bfloat162float(p[i]);
+                            for (int i = 0; i < 8; i++) w[i] = __floats2bfloat162_rn(v[t][2 * i], v[t][2 * i + 1]);
+#pragma unroll
+                            for (int dy = 0; dy < 2; dy++)
+#pragma unroll
+                                for (int dx = 0; dx < 2; dx++) {
+                                    uint4 *o = reinterpret_cast<uint4 *>(
+                                        a.out + (((size_t)b * 2 * a.H + 2 * y + dy) * 2 * a.W + 2 * x + dx) * a.out_cstride +
+                                        a.out_coff + c0);
+                                    o[0] = w2[0];
+                                    o[1] = w2[1];
+                                }
+                        } else {
+                            uint4 *o = reinterpret_cast<uint4 *>(a.out + pix * a.out_cstride + a.out_coff + c0);
+                            if (a.accumulate) {
+                                const uint4 p2[2] = {o[0], o[1]};
+                                const bf16 *p = reinterpret_cast<const bf16 *>(p2);
+#pragma unroll
+                                for (int i = 0; i < 16; i++) v[t][i] += __bfloat162float(p[i]);
+                            }
+#pragma unroll
+                            for (int i = 0; i < 8; i++) w[i] = __floats2bfloat162_rn(v[t][2 * i], v[t][2 * i + 1]);
+                            o[0] = w2[0];
+                            o[1] = w2[1];
                         }
+                    }
+                }
+                if (a.pool_out) {
+                    // 2x2 average of the stored (bf16-rounded) values: the two rows are
+                    // this thread's, the column pair is this lane and its neighbour
+                    // (x0 and 128-pixel tiles are even, H and W even).
+                    float pv[16];
+#pragma unroll
+                    for (int i = 0; i < 16; i++) {
+                        float sum = 0.f;
+#pragma unroll
+                        for (int t = 0; t < TROWS; t++) sum += __bfloat162float(__float2bfloat16_rn(v[t][i]));
+                        pv[i] = sum + __shfl_xor_sync(0xffffffffu, sum, 1);
+                    }
+                    const bool in = y0 < a.H && x < a.W;
+                    if (in && (x & 1) == 0) {
                         uint4 w2[2];
                         __nv_bfloat162 *w = reinterpret_cast<__nv_bfloat162 *>(w2);
 #pragma unroll
-                        for (int i = 0; i < 8; i++) w[i] = __floats2bfloat162_rn(v[2 * i], v[2 * i + 1]);
+                        for (int i = 0; i < 8; i++) w[i] = __floats2bfloat162_rn(0.25f * pv[2 * i], 0.25f * pv[2 * i + 1]);
+                        uint4 *o = reinterpret_cast<uint4 *>(
+                            a.pool_out + (((size_t)b * (a.H / 2) + y0 / 2) * (a.W / 2) + x / 2) * a.n_store + c0);
                         o[0] = w2[0];
                         o[1] = w2[1];
                     }
@@ -783,6 +831,20 @@ bool make_map(CUtensorMap *m, const void *base, int B, int H, int W, int C, int 
     return true;
 }
 
+// Raises a kernel's dynamic shared-memory limit to the pipeline budget, once
+// per device (slot: which kernel).
+void set_smem_attribute_once(const void *fn, int slot)
+{
+    static std::mutex mu;
+    static bool done[64][2] = {};
+    int dev = 0;
+    cudaGetDevice(&dev);
+    std::lock_guard<std::mutex> lock(mu);
+    if (dev >= 0 && dev < 64 && done[dev][slot]) return;
+    cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)(SMEM_BUDGET + 1024));
+    if (dev >= 0 && dev < 64) done[dev][slot] = true;
+}
+
 int num_sms()
 {
     static int n = 0;
@@ -826,27 +888,14 @@ int32_t conv3x3(const ArtCnnConv *d, cudaStream_t s)
         return fail(ART_ERR_INVALID_ARGUMENT, "conv: bad mask stride");
     if ((long long)d->B * d->H * d->W * (long long)d->cin >= (1LL << 40))
         return fail(ART_ERR_INVALID_ARGUMENT, "conv: tensor too large");
-    // Output rows per tile: as many as TMEM (2 tiles in flight x trows
-    // accumulators of n columns <= 512) and three pipeline stages (else two)
-    // allow, up to MAX_TROWS.
-    const int tiles_x = (d->W + TPX - 1) / TPX;
-    int trows = 0;
-    auto col_stride = [](int t) { return ((uint32_t)((t + 2) * HPX * 16) + 127u) / 128u * 128u; };
-    for (int want = 3; want >= 2 && !trows; want--)
-        for (int t = MAX_TROWS; t >= 1; t--) {
-            const uint32_t sb = (uint32_t)(d->ck / 8) * col_stride(t) + 18u * d->ck * d->n;
-            if (2 * t * d->n <= 512 && SMEM_BUDGET / sb >= (uint32_t)want) {
-                trows = t;
-                break;
-            }
-        }
-    if (!trows) return fail(ART_ERR_INVALID_ARGUMENT, "conv: stage does not fit shared memory");
+    if (d->pool_out && (d->H % 2 || d->W % 2 || d->mask))
+        return fail(ART_ERR_INVALID_ARGUMENT, "conv: pooled output needs even H and W and no mask");
+    if (d->up2 && (!d->out || d->accumulate || d->mask))
+        return fail(ART_ERR_INVALID_ARGUMENT, "conv: upsampled output needs out, no accumulate and no mask");
     CUtensorMap map;
     std::string err;
-    if (!make_map(&map, d->x, d->B, d->H, d->W, d->cin, HPX, trows + 2, err)) return fail(ART_ERR_CUDA, "conv: " + err);
+    if (!make_map(&map, d->x, d->B, d->H, d->W, d->cin, HPX, HROWS, err)) return fail(ART_ERR_CUDA, "conv: " + err);
     ConvArgs a{};
-    a.trows = trows;
-    a.kcol = col_stride(trows);
     a.B = d->B;
     a.H = d->H;
     a.W = d->W;
@@ -865,15 +914,16 @@ int32_t conv3x3(const ArtCnnConv *d, cudaStream_t s)
     a.mask_cstride = d->mask_cstride;
     a.relu = d->relu;
     a.accumulate = d->accumulate;
-    a.halo_bytes = (uint32_t)(d->ck / 8) * a.kcol;
+    a.pool_out = static_cast<bf16 *>(d->pool_out);
+    a.up2 = d->up2;
+    a.halo_bytes = (uint32_t)(d->ck / 8) * KCOL;
     a.stage_bytes = a.halo_bytes + 18u * d->ck * d->n;
-    a.tx_bytes = (uint32_t)(d->ck / 8) * (uint32_t)((trows + 2) * HPX * 16) + 18u * d->ck * d->n;
     a.stages = (int)std::min<uint32_t>(MAX_STAGES, SMEM_BUDGET / a.stage_bytes);
     a.err = d->err;
     if (a.stages < 2) return fail(ART_ERR_INVALID_ARGUMENT, "conv: stage does not fit shared memory");
     const uint32_t smem = a.stages * a.stage_bytes + 1024;
-    cudaFuncSetAttribute(k_conv3x3, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)(SMEM_BUDGET + 1024));
-    const long long ntiles = (long long)d->B * ((d->H + trows - 1) / trows) * tiles_x;
+    set_smem_attribute_once(reinterpret_cast<const void *>(k_conv3x3), 0);
+    const long long ntiles = (long long)d->B * ((d->H + TROWS - 1) / TROWS) * ((d->W + TPX - 1) / TPX);
     const int grid = (int)std::min<long long>(ntiles, num_sms());
     k_conv3x3<<<grid, THREADS, smem, s>>>(map, a);
     return check_launch("k_conv3x3");
@@ -911,7 +961,7 @@ int32_t wgrad3x3(const ArtCnnWgrad *d, cudaStream_t s)
     a.stage_bytes = 16 * DYREG + (uint32_t)(nci / 8) * KCOL;
     a.stages = (int)std::min<uint32_t>(MAX_STAGES, SMEM_BUDGET / a.stage_bytes);
     a.err = d->err;
-    cudaFuncSetAttribute(k_wgrad3x3, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)(SMEM_BUDGET + 1024));
+    set_smem_attribute_once(reinterpret_cast<const void *>(k_wgrad3x3), 1);
     k_wgrad3x3<<<dim3(bands, nchunk), THREADS, a.stages * a.stage_bytes + 1024, s>>>(dymap, xmap, a);
     int32_t rc = check_launch("k_wgrad3x3");
     if (rc) return rc;
@@ -1201,8 +1251,11 @@ int32_t net_pack(ArtNet *net, bool backward, cudaStream_t s)
     return ART_OK;
 }
 
+// Forward convolution of `layer`: bf16 output into channels [coff, coff + cout)
+// of `out` (cstride channels; 2H x 2W, each pixel stored to its 2x2 cell,
+// when up2), optionally also the fp32 output and the 2x2-pooled output.
 int32_t conv(ArtNet *net, int layer, const void *x, int B, int H, int W, void *out, int cstride, int coff,
-             float *out_f32, cudaStream_t s)
+             float *out_f32, cudaStream_t s, void *pool_out = nullptr, int up2 = 0)
 {
     const LayerDef &L = LAYERS[layer];
     ArtCnnConv d{};
@@ -1223,6 +1276,8 @@ int32_t conv(ArtNet *net, int layer, const void *x, int B, int H, int W, void *o
     d.f32_cstride = L.cout;
     d.relu = L.relu;
     d.err = net->errflag.as<int>();
+    d.pool_out = pool_out;
+    d.up2 = up2;
     return conv3x3(&d, s);
 }
 
@@ -1279,21 +1334,28 @@ int32_t wgrad(ArtNet *net, int layer, const void *x, const void *g, int B, int H
         if (rc_) return rc_;      \
     } while (0)
 
-int32_t net_forward(ArtNet *net, int B, int H, int W, cudaStream_t s)
+// Forward pass on level-0 size H x W. The encoder convolutions also write
+// their pooled outputs. For inference the e4/d3/d2 convolutions store their
+// outputs upsampled straight into the next concatenation; training keeps
+// them whole (the backward pass reads them as ReLU masks) and upsamples after.
+int32_t net_forward(ArtNet *net, int B, int H, int W, cudaStream_t s, bool train)
 {
     const int H1 = H / 2, W1 = W / 2, H2 = H / 4, W2 = W / 4, H3 = H / 8, W3 = W / 8;
-    NET_TRY(conv(net, E1, net->feat.p, B, H, W, net->cat1.p, 96, 0, nullptr, s));
-    NET_TRY(art_cnn_pool2(net->cat1.p, B, H, W, 32, 96, 0, net->p1.p, s));
-    NET_TRY(conv(net, E2, net->p1.p, B, H1, W1, net->cat2.p, 160, 0, nullptr, s));
-    NET_TRY(art_cnn_pool2(net->cat2.p, B, H1, W1, 64, 160, 0, net->p2.p, s));
-    NET_TRY(conv(net, E3, net->p2.p, B, H2, W2, net->cat3.p, 224, 0, nullptr, s));
-    NET_TRY(art_cnn_pool2(net->cat3.p, B, H2, W2, 96, 224, 0, net->p3.p, s));
-    NET_TRY(conv(net, E4, net->p3.p, B, H3, W3, net->e4.p, 128, 0, nullptr, s));
-    NET_TRY(art_cnn_upsample2(net->e4.p, B, H2, W2, 128, net->cat3.p, 224, 96, s));
-    NET_TRY(conv(net, D3, net->cat3.p, B, H2, W2, net->d3.p, 96, 0, nullptr, s));
-    NET_TRY(art_cnn_upsample2(net->d3.p, B, H1, W1, 96, net->cat2.p, 160, 64, s));
-    NET_TRY(conv(net, D2, net->cat2.p, B, H1, W1, net->d2.p, 64, 0, nullptr, s));
-    NET_TRY(art_cnn_upsample2(net->d2.p, B, H, W, 64, net->cat1.p, 96, 32, s));
+    NET_TRY(conv(net, E1, net->feat.p, B, H, W, net->cat1.p, 96, 0, nullptr, s, net->p1.p));
+    NET_TRY(conv(net, E2, net->p1.p, B, H1, W1, net->cat2.p, 160, 0, nullptr, s, net->p2.p));
+    NET_TRY(conv(net, E3, net->p2.p, B, H2, W2, net->cat3.p, 224, 0, nullptr, s, net->p3.p));
+    if (train) {
+        NET_TRY(conv(net, E4, net->p3.p, B, H3, W3, net->e4.p, 128, 0, nullptr, s));
+        NET_TRY(art_cnn_upsample2(net->e4.p, B, H2, W2, 128, net->cat3.p, 224, 96, s));
+        NET_TRY(conv(net, D3, net->cat3.p, B, H2, W2, net->d3.p, 96, 0, nullptr, s));
+        NET_TRY(art_cnn_upsample2(net->d3.p, B, H1, W1, 96, net->cat2.p, 160, 64, s));
+        NET_TRY(conv(net, D2, net->cat2.p, B, H1, W1, net->d2.p, 64, 0, nullptr, s));
+        NET_TRY(art_cnn_upsample2(net->d2.p, B, H, W, 64, net->cat1.p, 96, 32, s));
+    } else {
+        NET_TRY(conv(net, E4, net->p3.p, B, H3, W3, net->cat3.p, 224, 96, nullptr, s, nullptr, 1));
+        NET_TRY(conv(net, D3, net->cat3.p, B, H2, W2, net->cat2.p, 160, 64, nullptr, s, nullptr, 1));
+        NET_TRY(conv(net, D2, net->cat2.p, B, H1, W1, net->cat1.p, 96, 32, nullptr, s, nullptr, 1));
+    }
     NET_TRY(conv(net, D1, net->cat1.p, B, H, W, net->d1.p, 32, 0, nullptr, s));
     NET_TRY(conv(net, HEAD, net->d1.p, B, H, W, nullptr, 0, 0, net->r.as<float>(), s));
     return ART_OK;
@@ -1369,9 +1431,9 @@ int32_t net_predict(ArtNet *net, const int16_t *coef, int cpitch, long long img_
     NET_TRY(net_alloc(net, (long long)B * H0 * W0, (long long)B * H * W, false));
     if (!net->packed) NET_TRY(net_pack(net, false, s));
     NET_TRY(art_cnn_features(coef, cpitch, img_stride, q, B, H, W, net->dec.as<float>(), net->feat.p, s));
-    NET_TRY(net_forward(net, B, H0, W0, s));
+    NET_TRY(net_forward(net, B, H0, W0, s, false));
     return art_cnn_residual(net->r.as<float>(), 16, net->dec.as<float>(), nullptr, B, H, W,
-                            pred ? pred : net->pred.as<float>(), nullptr, nullptr, 148, s);
+                            pred ? pred : net->pred.as<float>(), nullptr, nullptr, 8 * num_sms(), s);
 }
 
 int32_t net_predict_async(ArtNet *net, const int16_t *coef, int cpitch, long long img_stride, const float *q, int B,
@@ -1496,7 +1558,7 @@ int32_t art_net_train_step(ArtNet *net, const int16_t *coef, int32_t cpitch, int
     }
     NET_TRY(net_pack(net, true, s));
     NET_TRY(art_cnn_features(coef, cpitch, img_stride, q, B, H, W, net->dec.as<float>(), net->feat.p, s));
-    NET_TRY(net_forward(net, B, H0, W0, s));
+    NET_TRY(net_forward(net, B, H0, W0, s, true));
     const long long npix = (long long)B * H * W;
     NET_TRY(art_cnn_residual(net->r.as<float>(), 16, net->dec.as<float>(), target, B, H, W, net->pred.as<float>(),
                              net->dr.p, net->loss_partial.as<float>(), LOSS_BLOCKS, s));

@@ -1338,19 +1338,33 @@ static int prepare_batch(ArtContext *ctx, const std::vector<ImageSpec> &specs, u
         // (g = 0, sigma = 0): x_0 = y_0 = P(prediction), and the DCT-distance
         // plane of the projected prediction for the first gradient.
         size_t need = 0;
-        for (const auto &sp : specs)
-            for (uint32_t c = 0; c < sp.nch; c++)
-                need = std::max(need, (size_t)sp.ch[c].rounded_px_w * sp.ch[c].rounded_px_h);
+        for (const auto &sp : specs) {
+            size_t img = 0;
+            for (uint32_t c = 0; c < sp.nch; c++) img += (size_t)sp.ch[c].rounded_px_w * sp.ch[c].rounded_px_h;
+            need = std::max(need, img);
+        }
         if ((rc = ctx->pred.ensure(need * sizeof(float)))) return rc;
         float *pred = static_cast<float *>(ctx->pred.p);
         for (int i = 0; i < nimg; i++) {
             const ImgDev &d = ctx->h_desc[i];
-            for (int c = 0; c < d.nch; c++) {
+            for (int c = 0; c < d.nch;) {
+                // Components of one size (the two chroma planes of 4:2:0 or
+                // 4:2:2) go through the network as one batch: their coefficient
+                // images lie a fixed distance apart and their quantisation
+                // tables are consecutive in the descriptor.
                 const ChanDev &cd = d.ch[c];
-                rc = cnn::net_predict_async(ctx->net, cd.coef, cd.cpitch, 0, &ddesc[i].q[c][0], 1, cd.chh, cd.cw,
+                const long long stride = c + 1 < d.nch ? (long long)(d.ch[c + 1].coef - cd.coef) : 0;
+                int nb = 1;
+                while (c + nb < d.nch && d.ch[c + nb].cw == cd.cw && d.ch[c + nb].chh == cd.chh &&
+                       d.ch[c + nb].cpitch == cd.cpitch && d.ch[c + nb].coef - d.ch[c + nb - 1].coef == stride)
+                    nb++;
+                rc = cnn::net_predict_async(ctx->net, cd.coef, cd.cpitch, stride, &ddesc[i].q[c][0], nb, cd.chh, cd.cw,
                                             pred, s);
                 if (rc) return rc;
-                k_upsample<<<(int)(((long long)d.W * d.H + 255) / 256), 256, 0, s>>>(pred, ddesc + i, c);
+                for (int k = 0; k < nb; k++)
+                    k_upsample<<<(int)(((long long)d.W * d.H + 255) / 256), 256, 0, s>>>(
+                        pred + (size_t)k * cd.cw * cd.chh, ddesc + i, c + k);
+                c += nb;
             }
             ART_CUDA(cudaMemsetAsync(d.g, 0, (size_t)d.nch * d.cstride * sizeof(float), s));
         }

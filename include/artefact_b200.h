@@ -278,6 +278,10 @@ typedef struct ArtCnnConv {
     int32_t mask_cstride;
     int32_t relu, accumulate;
     int32_t *err;
+    void *pool_out; /* optional: also the 2x2 average of the bf16 output (after bias / ReLU / mask),
+                       [B][H/2][W/2][n_store]; H and W even */
+    int32_t up2;    /* nonzero: `out` is 2H x 2W and each output pixel is stored to its 2x2 cell
+                       (nearest upsampling fused into the store; not with accumulate) */
 } ArtCnnConv;
 int32_t art_cnn_conv3x3(const ArtCnnConv *desc, void *stream);
 

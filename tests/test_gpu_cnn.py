@@ -56,7 +56,7 @@ def _pack(w, transpose=0, ci0=0, n=None, ck=32):
 
 
 def _conv(x, wpack, cin, ck, n, bias=None, relu=0, mask=None, out=None, out_cstride=None, out_coff=0, f32=None,
-          accumulate=0):
+          accumulate=0, pool_out=None, up2=0):
     torch = _torch()
     B, H, W, _ = x.shape
     err = torch.zeros(1, dtype=torch.int32, device="cuda")
@@ -75,6 +75,8 @@ def _conv(x, wpack, cin, ck, n, bias=None, relu=0, mask=None, out=None, out_cstr
     d.mask_cstride = mask.shape[-1] if mask is not None else 0
     d.relu, d.accumulate = relu, accumulate
     d.err = err.data_ptr()
+    d.pool_out = pool_out.data_ptr() if pool_out is not None else None
+    d.up2 = up2
     N.check(N.lib().art_cnn_conv3x3(C.byref(d), None))
     torch.cuda.synchronize()
     assert int(err.item()) == 0, "a pipeline wait timed out"
@@ -120,6 +122,29 @@ def test_conv_channel_offset_accumulate_and_f32(gpu):
     f = torch.zeros((B, H, W, cout), dtype=torch.float32, device="cuda")
     _conv(_bf(x), wp, cin, 32, cout, f32=f)
     np.testing.assert_allclose(_np(f), O.conv(x, w), rtol=1e-4, atol=1e-4 * float(np.abs(O.conv(x, w)).max()))
+
+
+@pytest.mark.parametrize("B,H,W,cin,cout", [(1, 8, 130, 16, 32), (2, 6, 64, 64, 96), (1, 4, 40, 96, 128)])
+def test_conv_fused_pool_and_upsample(gpu, B, H, W, cin, cout):
+    """The epilogue's 2x2-pooled output equals pooling the stored activation,
+    and the upsampled store equals nearest upsampling of the plain store."""
+    torch = _torch()
+    rng = np.random.default_rng(cin + cout + H)
+    x = O.bf16(rng.standard_normal((B, H, W, cin)))
+    w = O.bf16(rng.standard_normal((cout, 9, cin)) * np.sqrt(2 / (9 * cin)))
+    b = rng.standard_normal(cout) * 0.1
+    ck = 32 if cin % 32 == 0 else 16
+    wp, xt, bt = _pack(w, ck=ck), _bf(x), _f32(b)
+    pooled = torch.zeros((B, H // 2, W // 2, cout), dtype=torch.bfloat16, device="cuda")
+    plain = _conv(xt, wp, cin, ck, cout, bias=bt, relu=1, pool_out=pooled)
+    ref = O.bf16(np.maximum(O.conv(x, w, b), 0))
+    _close(_np(plain), ref)
+    np.testing.assert_array_equal(_np(pooled), O.bf16(O.pool(_np(plain))))
+    big = torch.zeros((B, 2 * H, 2 * W, cout + 16), dtype=torch.bfloat16, device="cuda")
+    _conv(xt, wp, cin, ck, cout, bias=bt, relu=1, out=big, out_cstride=cout + 16, out_coff=16, up2=1)
+    got = _np(big)
+    np.testing.assert_array_equal(got[..., 16:], O.up(_np(plain)))
+    assert np.all(got[..., :16] == 0)
 
 
 def test_conv_backward_data_with_mask(gpu):
