@@ -67,7 +67,8 @@ WORKLOADS["network"] = dict(
 LEARNED_QUALITIES = (30, 50, 75)
 REFINE_ITERATIONS = 8
 REFINE_STEP_ITERATIONS = 4         # first refinement phase: steps of a 4-iteration run
-REFINE_TAIL_STEP_ITERATIONS = 100  # last quarter: steps of a 100-iteration run
+REFINE_TAIL = 2                    # last two iterations: FISTA restarted ...
+REFINE_TAIL_STEP_ITERATIONS = 100  # ... with steps of a 100-iteration run
 WEIGHT, PWEIGHT = 0.3, 0.001
 
 
@@ -259,11 +260,13 @@ class DeviceImage:
 
 
 def refine_schedule(k):
-    """Refinement after a learned start: k plain iterations, the first k - k/4
+    """Refinement after a learned start: k plain iterations, the first k - 2
     with the step of a REFINE_STEP_ITERATIONS-iteration run (large: they remove
-    the prediction's error), the last k/4 restarted with the step of a
-    REFINE_TAIL_STEP_ITERATIONS-iteration run (small: they settle)."""
-    return dict(step=REFINE_STEP_ITERATIONS, tail=max(1, k // 4), tail_step=REFINE_TAIL_STEP_ITERATIONS)
+    the prediction's error), the last 2 restarted with the step of a
+    REFINE_TAIL_STEP_ITERATIONS-iteration run (small: they settle). Chosen on a
+    grid over the first step (1-4 iterations' worth), the tail length (2-6)
+    and the tail step (50-200) on the three 1080p images."""
+    return dict(step=REFINE_STEP_ITERATIONS, tail=min(REFINE_TAIL, k - 1), tail_step=REFINE_TAIL_STEP_ITERATIONS)
 
 
 def learned_comparison(lib, device, steps, warmup, refine=REFINE_ITERATIONS, qualities=LEARNED_QUALITIES):

@@ -154,8 +154,8 @@ def test_learned_start_needs_a_network(gpu, ctx):
 def test_trained_network_gain(gpu, ctx, quality):
     """The trained network's start against the decoded start on an image it
     was not trained on (seed outside the training range), with the same
-    refinement (8 and 24 iterations: steps of a 4-iteration run, the last
-    quarter restarted with steps of a 100-iteration run): the learned path's
+    refinement (8 and 24 iterations: steps of a 4-iteration run, the last two
+    restarted with steps of a 100-iteration run): the learned path's
     objective is below the decoded path's, both stay feasible, and with 24
     iterations the learned path is within 0.1 % of the plain 50-iteration
     objective while the decoded path is not closer."""
@@ -165,7 +165,7 @@ def test_trained_network_gain(gpu, ctx, quality):
     ctx.compute(3, j.coefs, WEIGHT, PW, 50, W, H)
     e50 = ctx.evaluate()["E"]
     for k in (8, 24):
-        sched = dict(step_iterations=4, tail_iterations=k // 4, tail_step_iterations=100)
+        sched = dict(step_iterations=4, tail_iterations=2, tail_step_iterations=100)
         ctx.set_warm_start(net)
         try:
             ctx.compute(3, j.coefs, WEIGHT, PW, k, W, H, init_mode=N.ART_INIT_LEARNED, **sched)
