@@ -10,6 +10,10 @@ Workloads (``--workload``; seeded synthetic JPEGs, ``artefact_b200.synth``):
   set (~1.7 GB) exceeds L2, so the iteration runs against HBM.
 * ``batch256``: 256 JPEGs, W, H ~ U[256, 2048] rounded to 16, 4:2:0 or 4:4:4
   with p = 0.5, quality ~ U[20, 90], 50 iterations, solved as one batch.
+* ``learned``: 1920x1080 4:2:0 at quality 30/50/75: the learned warm start +
+  8 plain iterations against the plain 50-iteration solve, and the fewest
+  iterations whose objective reaches the plain 50-iteration one.
+* ``network``: the warm-start network's forward pass alone (TFLOP/s).
 
 A step is one solve of the whole workload. Metric: megapixels per second of
 real image area.
@@ -27,6 +31,10 @@ real image area.
               host thread; a bounded sample, extrapolated when stated.
 * --impl reference -- the oracle as the reference arm, steps spread over the
               host's threads.
+* learned_warm_start (1080p, one GPU) -- the same image through the learned
+              warm start: 8 refinement iterations, and the fewest of 8/16/24/32
+              that reach the plain 50-iteration objective within 1e-4, with
+              their MPix/s (objectives from art_context_evaluate).
 
 Multi-GPU (torchrun): replicas only -- every rank solves its own copy; value
 is all ranks' megapixels over the slowest rank's time.
@@ -269,7 +277,8 @@ def refine_schedule(k):
     return dict(step=REFINE_STEP_ITERATIONS, tail=min(REFINE_TAIL, k - 1), tail_step=REFINE_TAIL_STEP_ITERATIONS)
 
 
-def learned_comparison(lib, device, steps, warmup, refine=REFINE_ITERATIONS, qualities=LEARNED_QUALITIES):
+def learned_comparison(lib, device, steps, warmup, refine=REFINE_ITERATIONS, qualities=LEARNED_QUALITIES,
+                       images=None, ladder=(8, 12, 16, 20, 24, 28, 32, 40, 48)):
     """Learned warm start + `refine` plain iterations against the plain
     50-iteration solve, per quality, on seeded 1920x1080 4:2:0 JPEGs (seeds
     5000 + quality, outside the network's training seeds). Each path is timed
@@ -278,7 +287,8 @@ def learned_comparison(lib, device, steps, warmup, refine=REFINE_ITERATIONS, qua
     art_context_evaluate. Also finds the fewest refinement iterations (of a
     fixed ladder) whose objective reaches the plain 50-iteration one within
     1e-4 relative, and times that. The decoded start with the same schedule
-    is the control. None when the package holds no trained weights."""
+    is the control. `images` (a list of (label, Jpeg)) replaces the seeded
+    1080p images. None when the package holds no trained weights."""
     import torch
 
     from artefact_b200 import _native as N
@@ -324,9 +334,10 @@ def learned_comparison(lib, device, steps, warmup, refine=REFINE_ITERATIONS, qua
         return statistics.median(ms)
 
     rows = []
-    ladder = (8, 12, 16, 20, 24, 28, 32, 40, 48)
-    for q in qualities:
-        j = Jpeg.from_source(JpegSource.Buffer(synth.make_jpeg(1920, 1080, q, "4:2:0", False, seed=5000 + q)))
+    if images is None:
+        images = [(q, Jpeg.from_source(JpegSource.Buffer(synth.make_jpeg(1920, 1080, q, "4:2:0", False, seed=5000 + q))))
+                  for q in qualities]
+    for q, j in images:
         img = DeviceImage(j)
         mpix = j.real_px_w * j.real_px_h / 1e6
         plain_ms = timed(img, 50, N.ART_INIT_DECODED, None)
@@ -370,7 +381,7 @@ def learned_comparison(lib, device, steps, warmup, refine=REFINE_ITERATIONS, qua
     lib.art_context_set_warm_start(ctx, None)
     lib.art_context_destroy(ctx)
     net.close()
-    mp_total = sum(1920 * 1080 / 1e6 for _ in rows)
+    mp_total = sum(j.real_px_w * j.real_px_h / 1e6 for _, j in images)
     reach = all(r["min_refine_to_reach"] for r in rows)
     return dict(refine_iterations=refine, schedule=refine_schedule(refine), images=rows,
                 plain50_mpix_s=mp_total / sum(r["plain50_ms"] for r in rows) * 1e3,
@@ -554,6 +565,7 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--workload", default="1080p", choices=sorted(WORKLOADS))
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-learned", action="store_true", help="skip the learned warm-start comparison")
     args = ap.parse_args()
 
     rank = int(os.environ.get("RANK", "0"))
@@ -758,6 +770,23 @@ def main():
         v, desc = cpu_sample(args.workload, jpegs, iters)
         cpu = {"value": v, "unit": "MPix/s", "cores": 1, "kind": "port", "sample": desc}
 
+    # Learned warm start on the same image (1080p only, one GPU): 8 and the
+    # fewest ladder iterations that reach the plain 50-iteration objective.
+    learned = None
+    if args.workload == "1080p" and world == 1 and not args.no_learned:
+        res = learned_comparison(lib, local, min(args.steps, 10), args.warmup, images=[(75, jpegs[0])],
+                                 ladder=(8, 16, 24, 32))
+        if res is not None:
+            r = res["images"][0]
+            learned = {"schedule": res["schedule"], "refine_iterations": res["refine_iterations"],
+                       "mpix_s": r["learned_mpix_s"], "ms": r["learned_ms"], "E_rel_to_plain50": r["E_learned_rel"],
+                       "speedup_vs_plain50": r["speedup"],
+                       "iterations_to_reach_plain50": r["min_refine_to_reach"],
+                       "reach_mpix_s": (mpix / r["min_refine_ms"] * 1e3) if r["min_refine_ms"] else None,
+                       "reach_speedup_vs_plain50": r["min_refine_speedup"],
+                       "reach_E_rel": r["min_refine_E_rel"],
+                       "decoded_start_same_iterations_E_rel": r["min_refine_decoded_same_schedule_E_rel"]}
+
     modes = len({(c.horizontal_samp_factor, c.vertical_samp_factor) for j in jpegs for c in j.coefs})
     nchs = len({j.nchannel for j in jpegs})
     per_step = sum(j.nchannel for j in jpegs) + 1 + (nchs + modes) * iters
@@ -780,6 +809,8 @@ def main():
                           "frac_of_hbm": iter_bytes / (loop / iters * 1e-3) / 1e9 / peak},
             "cpu_baseline": cpu, "gpu_launches": args.steps * per_step, "clocks": clocks, "wall_s": wall,
         }
+        if learned is not None:
+            line["learned_warm_start"] = learned
         print(json.dumps(line), flush=True)
     lib.art_context_destroy(ctx)
     if dist:
