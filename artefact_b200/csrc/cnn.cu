@@ -774,6 +774,61 @@ __global__ void k_wait_selftest(int *err, long long limit)
     }
 }
 
+// Gradient of the training loss with a smoothness term: with e = (pred -
+// target) / 16 per sample, L = (sum e^2 + lambda sum over horizontally and
+// vertically adjacent pairs (e_p - e_q)^2) / n, so dL/de_p = (2 e_p + 2 lambda
+// sum_{q adjacent to p} (e_p - e_q)) / n. Overwrites channels 0-3 of
+// grad[B][H0][W0][16] and writes per-block partial sums of the pair term
+// (times lambda). One thread per level-0 pixel (its 2x2 cell).
+__global__ void k_residual_smooth_grad(const float *__restrict__ pred, const float *__restrict__ target, int B, int H,
+                                       int W, float lambda, float inv_count, bf16 *__restrict__ grad,
+                                       float *__restrict__ loss_partial)
+{
+    __shared__ float s[256];
+    const int W0 = (W + 15) / 16 * 8, H0 = (H + 15) / 16 * 8;
+    const long long n0 = (long long)B * H0 * W0;
+    auto err = [&](int b, int Y, int X) {
+        const size_t q = ((size_t)b * H + Y) * W + X;
+        return (pred[q] - target[q]) * (1.f / 16.f);
+    };
+    float acc = 0.f;
+    for (long long p = blockIdx.x * (long long)blockDim.x + threadIdx.x; p < n0; p += (long long)gridDim.x * blockDim.x) {
+        const int x = (int)(p % W0), y = (int)((p / W0) % H0), b = (int)(p / ((long long)W0 * H0));
+        uint4 o[2] = {make_uint4(0, 0, 0, 0), make_uint4(0, 0, 0, 0)};
+        bf16 *gv = reinterpret_cast<bf16 *>(o);
+#pragma unroll
+        for (int k = 0; k < 4; k++) {
+            const int Y = 2 * y + (k >> 1), X = 2 * x + (k & 1);
+            if (Y >= H || X >= W) continue;
+            const float e = err(b, Y, X);
+            float lap = 0.f;
+            if (X > 0) lap += e - err(b, Y, X - 1);
+            if (X < W - 1) {
+                const float d = e - err(b, Y, X + 1);
+                lap += d;
+                acc += d * d;
+            }
+            if (Y > 0) lap += e - err(b, Y - 1, X);
+            if (Y < H - 1) {
+                const float d = e - err(b, Y + 1, X);
+                lap += d;
+                acc += d * d;
+            }
+            gv[k] = __float2bfloat16_rn((2.f * e + 2.f * lambda * lap) * inv_count);
+        }
+        uint4 *g = reinterpret_cast<uint4 *>(grad + p * 16);
+        g[0] = o[0];
+        g[1] = o[1];
+    }
+    s[threadIdx.x] = lambda * acc;
+    __syncthreads();
+    for (int k = 128; k > 0; k >>= 1) {
+        if (threadIdx.x < k) s[threadIdx.x] += s[threadIdx.x + k];
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) loss_partial[blockIdx.x] = s[0];
+}
+
 // Adam on flat fp32 parameters (decoupled from the bf16 copies the convs read).
 __global__ void k_adam(float *__restrict__ w, const float *__restrict__ g, float *__restrict__ m, float *__restrict__ v,
                        long long n, float lr, float b1, float b2, float eps, float c1, float c2)
@@ -1181,6 +1236,7 @@ struct ArtNet {
     // activations (forward) and gradients (training)
     art::cnn::Buf feat, dec, cat1, cat2, cat3, p1, p2, p3, e4, d3, d2, d1, r, pred;
     art::cnn::Buf dr, gd1, ge1, gup1, gd2, ge2, gup2, gd3, ge3, gup3, ge4, gp3, gp2, gp1;
+    float smooth_weight = 0.f;  // lambda of the training loss's smoothness term (art_net_set_loss)
     long long cap_px = 0;    // level-0 pixels the activation buffers hold
     long long cap_full = 0;  // full-resolution samples the decoded/prediction buffers hold
     bool cap_train = false;
@@ -1482,7 +1538,7 @@ int32_t art_net_create(int32_t device, const float *params, int64_t nparams, Art
     }
     const size_t pb = (size_t)nparams * 4;
     if (!net->params.ensure(pb) || !net->errflag.ensure(64) || !net->workspace.ensure(WORKSPACE_BYTES) ||
-        !net->loss_partial.ensure(LOSS_BLOCKS * 4) ||
+        !net->loss_partial.ensure(2 * LOSS_BLOCKS * 4) ||
         cudaMemcpy(net->params.p, params, pb, cudaMemcpyHostToDevice) != cudaSuccess ||
         cudaMemset(net->errflag.p, 0, 64) != cudaSuccess) {
         art_net_destroy(net);
@@ -1540,6 +1596,14 @@ int32_t art_net_predict(ArtNet *net, const int16_t *coef, int32_t cpitch, int64_
     return read_err(net, s);
 }
 
+int32_t art_net_set_loss(ArtNet *net, float smooth_weight)
+{
+    if (!net || !(smooth_weight >= 0.f) || !std::isfinite(smooth_weight))
+        return fail(ART_ERR_INVALID_ARGUMENT, "net_set_loss: weight must be finite and >= 0");
+    net->smooth_weight = smooth_weight;
+    return ART_OK;
+}
+
 int32_t art_net_train_step(ArtNet *net, const int16_t *coef, int32_t cpitch, int64_t img_stride, const float *q,
                            const float *target, int32_t B, int32_t H, int32_t W, float lr, float *loss, void *stream)
 {
@@ -1562,6 +1626,12 @@ int32_t art_net_train_step(ArtNet *net, const int16_t *coef, int32_t cpitch, int
     const long long npix = (long long)B * H * W;
     NET_TRY(art_cnn_residual(net->r.as<float>(), 16, net->dec.as<float>(), target, B, H, W, net->pred.as<float>(),
                              net->dr.p, net->loss_partial.as<float>(), LOSS_BLOCKS, s));
+    if (net->smooth_weight > 0.f) {
+        k_residual_smooth_grad<<<LOSS_BLOCKS, 256, 0, s>>>(net->pred.as<float>(), target, B, H, W, net->smooth_weight,
+                                                           1.f / (float)npix, static_cast<bf16 *>(net->dr.p),
+                                                           net->loss_partial.as<float>() + LOSS_BLOCKS);
+        NET_TRY(check_launch("k_residual_smooth_grad"));
+    }
     NET_TRY(net_backward(net, B, H0, W0, s));
     if (lr > 0.f) {
         net->step++;
@@ -1570,12 +1640,13 @@ int32_t art_net_train_step(ArtNet *net, const int16_t *coef, int32_t cpitch, int
         net->packed = false;
     }
     if (loss) {
-        float h[LOSS_BLOCKS];
-        if (cudaMemcpyAsync(h, net->loss_partial.p, sizeof(h), cudaMemcpyDeviceToHost, s) != cudaSuccess)
+        float h[2 * LOSS_BLOCKS];
+        const int nparts = net->smooth_weight > 0.f ? 2 * LOSS_BLOCKS : LOSS_BLOCKS;
+        if (cudaMemcpyAsync(h, net->loss_partial.p, nparts * sizeof(float), cudaMemcpyDeviceToHost, s) != cudaSuccess)
             return fail(ART_ERR_CUDA, "net_train_step: loss copy failed");
         NET_TRY(read_err(net, s));
         double t = 0;
-        for (int i = 0; i < LOSS_BLOCKS; i++) t += h[i];
+        for (int i = 0; i < nparts; i++) t += h[i];
         *loss = (float)(t / (double)npix);
         return ART_OK;
     }

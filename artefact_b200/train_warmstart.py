@@ -202,6 +202,9 @@ def main(argv=None):
     ap.add_argument("--seed", type=int, default=0)
     ap.add_argument("--out", required=True)
     ap.add_argument("--init", default=None, help="start from these weights instead of a fresh initialisation")
+    ap.add_argument("--smooth", type=float, default=0.0,
+                    help="weight of the loss's smoothness term (squared differences of the error between adjacent "
+                         "samples); 0 = plain MSE")
     args = ap.parse_args(argv)
 
     def log(*a):
@@ -212,6 +215,7 @@ def main(argv=None):
 
     ctx = Context(0)
     net = WS.WarmStartNet(WS.load_params(args.init) if args.init else WS.init_params(args.seed))
+    net.set_loss(args.smooth)
     t0 = time.time()
     data = build_pools(args.crops, SEED0, ctx, log=log)
     val = build_pools(args.val, SEED0 + 10_000_000, ctx, log=log)

@@ -146,6 +146,11 @@ class WarmStartNet:
     def save(self, path) -> None:
         save_params(path, self.params())
 
+    def set_loss(self, smooth_weight: float) -> None:
+        """Training loss = MSE + smooth_weight * mean squared difference of the
+        error between adjacent samples (art_net_set_loss; 0 = plain MSE)."""
+        N.check(N.lib().art_net_set_loss(self._h, float(smooth_weight)))
+
     def train_step(self, coef, q, target, lr: float, stream=None) -> float:
         """One step on a batch: coef int16 [B][H][W], q float32 [B][64] and
         target float32 [B][H][W] CUDA tensors. Returns the mean loss."""

@@ -370,6 +370,12 @@ int32_t art_net_gradients(ArtNet *net, float *host, int64_t n);
 /* Warm start: pred[B][H][W] (fp32, level-shifted samples) = decoded + 16 * residual. */
 int32_t art_net_predict(ArtNet *net, const int16_t *coef, int32_t cpitch, int64_t img_stride, const float *q,
                         int32_t B, int32_t H, int32_t W, float *pred, void *stream);
+/* Training loss: mean squared error (in units of 16 levels) plus
+ * smooth_weight times the mean over samples of the squared differences of the
+ * error between horizontally and vertically adjacent samples (0, the default,
+ * is plain MSE). The smoothness term penalises prediction errors that vary
+ * from sample to sample, which the TV/TGV objective penalises most. */
+int32_t art_net_set_loss(ArtNet *net, float smooth_weight);
 /* One training step on the mean squared error against target[B][H][W]
  * (in units of 16 levels): forward, backward, then Adam with learning rate
  * lr (lr <= 0: gradients only). *loss (may be NULL) receives the mean loss. */

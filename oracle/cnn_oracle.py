@@ -16,7 +16,8 @@ each level-0 pixel carries a 2x2 cell of the component (space to depth).
   d2 = relu(conv([e2 | up(d3)], 160 -> 64))         level 1
   d1 = relu(conv([e1 | up(d2)], 96 -> 32))          level 0
   r  = depth_to_space(conv(d1, 32 -> 16)[..., 0:4]) cropped to H x W
-  prediction = decoded + 16 r, loss = mean((r - (target - decoded) / 16)^2)
+  prediction = decoded + 16 r, e = r - (target - decoded) / 16,
+  loss = (sum e^2 + smooth * sum over adjacent sample pairs (e_p - e_q)^2) / n
 
 conv = 3x3, stride 1, zero padding 1, weights W[cout][tap = 3 (dy+1) + (dx+1)][cin];
 pool = 2x2 mean; up = nearest 2x. F = (space_to_depth(decoded) / 128,
@@ -152,7 +153,24 @@ def features(coef_img, q):
     return dec, F
 
 
-def forward(params, F, dec, target=None, bf=True):
+def _pair_sum(e):
+    """Sum over horizontally and vertically adjacent samples of (e_p - e_q)^2."""
+    return float(np.sum((e[:, :, 1:] - e[:, :, :-1]) ** 2) + np.sum((e[:, 1:, :] - e[:, :-1, :]) ** 2))
+
+
+def _pair_grad(e):
+    """d/de_p of the pair sum: 2 sum over the neighbours q of p of (e_p - e_q)."""
+    g = np.zeros_like(e)
+    dx = e[:, :, 1:] - e[:, :, :-1]
+    dy = e[:, 1:, :] - e[:, :-1, :]
+    g[:, :, 1:] += 2 * dx
+    g[:, :, :-1] -= 2 * dx
+    g[:, 1:, :] += 2 * dy
+    g[:, :-1, :] -= 2 * dy
+    return g
+
+
+def forward(params, F, dec, target=None, bf=True, smooth=0.0):
     """Activations (dict), prediction and, with a target, the loss."""
     rnd = bf16 if bf else (lambda a: np.asarray(a, np.float64))
     P = unpack(params)
@@ -182,19 +200,20 @@ def forward(params, F, dec, target=None, bf=True):
     loss = None
     if target is not None:
         e = rf - (target - dec) / 16.0
-        loss = float(np.mean(e * e))
+        loss = float(np.mean(e * e)) + smooth * _pair_sum(e) / e.size
         a["e"] = e
     return a, pred, loss, Wq
 
 
-def gradients(params, F, dec, target, bf=True):
+def gradients(params, F, dec, target, bf=True, smooth=0.0):
     """Loss and d loss / d params (flat, same layout as params)."""
     rnd = bf16 if bf else (lambda v: np.asarray(v, np.float64))
-    a, _, loss, Wq = forward(params, F, dec, target, bf)
+    a, _, loss, Wq = forward(params, F, dec, target, bf, smooth)
     npix = dec.size
     mask = lambda g, act: g * (act > 0)
     dr = np.zeros(a["r"].shape)
-    dr[..., 0:4] = space_to_depth(2.0 * a["e"] / npix, *a["r"].shape[1:3])
+    dlde = (2.0 * a["e"] + smooth * _pair_grad(a["e"])) / npix
+    dr[..., 0:4] = space_to_depth(dlde, *a["r"].shape[1:3])
     if bf:
         dr[..., 0:4] = bf16(dr[..., 0:4].astype(np.float32))
     grads = {}

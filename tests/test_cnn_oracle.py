@@ -82,3 +82,18 @@ def test_bf16_rounding_is_nearest_even():
     x = np.array([1.0, 1.0 + 2 ** -8, 1.0 + 3 * 2 ** -8, -2.5, 0.0], np.float64)
     r = O.bf16(x)
     assert r[0] == 1.0 and r[1] == 1.0 and r[2] == 1.0 + 2 ** -6 and r[3] == -2.5 and r[4] == 0.0
+
+
+def test_smooth_loss_gradient_matches_finite_differences():
+    """The smoothness term of the training loss, checked on the whole network."""
+    params, F, dec, target = _case(5, H=16, W=24)
+    loss, g = O.gradients(params, F, dec, target, bf=False, smooth=2.0)
+    assert loss > O.forward(params, F, dec, target, bf=False)[2]
+    rng = np.random.default_rng(8)
+    for _ in range(3):
+        v = rng.standard_normal(params.size)
+        eps = 1e-8
+        lp = O.forward(params + eps * v, F, dec, target, bf=False, smooth=2.0)[2]
+        lm = O.forward(params - eps * v, F, dec, target, bf=False, smooth=2.0)[2]
+        fd = (lp - lm) / (2 * eps)
+        assert abs(fd - g @ v) <= 1e-5 * max(1.0, abs(fd)), (fd, g @ v)

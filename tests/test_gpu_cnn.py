@@ -237,9 +237,11 @@ def test_features_and_prediction(gpu):
     np.testing.assert_allclose(pred, ref, rtol=0, atol=2e-3 * max(1.0, float(np.abs(ref - dec).max())) + 1e-3)
 
 
-def test_network_gradients_match_oracle(gpu):
+@pytest.mark.parametrize("smooth", [0.0, 2.0])
+def test_network_gradients_match_oracle(gpu, smooth):
     """The full forward + backward on the GPU against the oracle's FP64 backward
-    (bf16 storage emulated): per layer, cosine >= 0.999 and relative error <= 3e-2."""
+    (bf16 storage emulated), with and without the loss's smoothness term: per
+    layer, cosine >= 0.999 and relative error <= 3e-2."""
     torch = _torch()
     coef, q, target = _batch(2)
     params = WS.init_params(4)
@@ -249,10 +251,11 @@ def test_network_gradients_match_oracle(gpu):
     params[wo:bo] = (rng.standard_normal(bo - wo) * 0.05).astype(np.float32)  # a head that passes gradient
     params[wo + 4 * 32 * 9:bo] = 0.0  # outputs 4-15 are unused (outputs 0-3: the 2x2 cell)
     net = WS.WarmStartNet(params)
+    net.set_loss(smooth)
     loss = net.train_step(torch.from_numpy(coef).cuda(), _f32(q), _f32(target), lr=0.0)
     g = net.gradients().astype(np.float64)
     dec, F = O.features(coef, q)
-    ref_loss, ref = O.gradients(params.astype(np.float64), F, dec, target.astype(np.float64))
+    ref_loss, ref = O.gradients(params.astype(np.float64), F, dec, target.astype(np.float64), smooth=smooth)
     assert abs(loss - ref_loss) <= 1e-3 * ref_loss, (loss, ref_loss)
     for name, cin, cout, _, _ in O.LAYERS:
         for lo, hi in ((offs[name][0], offs[name][1]), (offs[name][1], offs[name][1] + cout)):
