@@ -42,11 +42,10 @@ namespace cnn {
 using bf16 = __nv_bfloat16;
 
 constexpr int TPX = 128;                    // output pixels per tile row (MMA M)
-constexpr int TROWS = 2;                    // output rows per tile (taller tiles measured slower: fewer tiles
-                                            // balance worse over the SMs)
+constexpr int TROWS = 2;                    // weight gradient: output rows per tile (the convolution takes 2 or 4)
 constexpr int HPX = TPX + 2;                // halo tile width
-constexpr int HROWS = TROWS + 2;            // halo tile height
-constexpr uint32_t KCOL = HROWS * HPX * 16; // bytes of one 8-channel column of a halo tile (8320, 65 x 128)
+constexpr int HROWS = TROWS + 2;            // weight gradient: halo tile height
+constexpr uint32_t KCOL = HROWS * HPX * 16; // weight gradient: bytes of one 8-channel halo column (8320, 65 x 128)
 constexpr uint32_t DYREG = TROWS * TPX * 16;// bytes of one 8-channel region of a gradient tile (4096)
 constexpr int THREADS = 192;                // warp 0 loads, warp 1 MMA, warps 2-5 epilogue
 constexpr uint32_t SMEM_BUDGET = 220 * 1024;  // pipeline stages; 1 KB more is requested for alignment
@@ -69,6 +68,7 @@ struct ConvArgs {
     int up2;            // out is 2H x 2W: each pixel stored to its 2x2 cell
     int stages;
     uint32_t stage_bytes, halo_bytes;
+    uint32_t tx_bytes;  // bytes the TMA and bulk copies of one stage deliver
     int *err;
 };
 
@@ -105,8 +105,19 @@ __device__ __forceinline__ unsigned char *aligned_smem(unsigned char *p)
     return p + ((1024 - (a & 1023)) & 1023);
 }
 
+// Shared-memory stride of one 8-channel column of a halo tile for TR output
+// rows: (TR + 2) x HPX pixels x 16 bytes, rounded up to 128 (TMA destinations
+// stay 128-byte aligned); and the bytes the TMA writes into it.
+template <int TR>
+struct HaloCol {
+    static constexpr uint32_t TX = (uint32_t)(TR + 2) * HPX * 16;
+    static constexpr uint32_t STRIDE = (TX + 127u) / 128u * 128u;
+};
+
+template <int TR>
 __global__ void __launch_bounds__(THREADS, 1) k_conv3x3(const __grid_constant__ CUtensorMap xmap, const ConvArgs a)
 {
+    constexpr uint32_t KC = HaloCol<TR>::STRIDE;
     extern __shared__ __align__(1024) unsigned char smem_raw[];
     unsigned char *smem = aligned_smem(smem_raw);
     __shared__ __align__(8) uint64_t full_bar[MAX_STAGES], empty_bar[MAX_STAGES], accf_bar[2], acce_bar[2],
@@ -116,7 +127,7 @@ __global__ void __launch_bounds__(THREADS, 1) k_conv3x3(const __grid_constant__ 
     volatile int *abort_p = &abort_s;
 
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const int tiles_x = (a.W + TPX - 1) / TPX, tiles_y = (a.H + TROWS - 1) / TROWS;
+    const int tiles_x = (a.W + TPX - 1) / TPX, tiles_y = (a.H + TR - 1) / TR;
     const int ntiles = a.B * tiles_x * tiles_y;
     const int nchunks = a.cin / a.ck;
     const int S = a.stages;
@@ -146,7 +157,7 @@ __global__ void __launch_bounds__(THREADS, 1) k_conv3x3(const __grid_constant__ 
             bool ok = true;
             for (int tile = blockIdx.x; tile < ntiles && ok; tile += gridDim.x) {
                 int b, y0, x0;
-                tile_coords(tile, tiles_x, tiles_y, TROWS, b, y0, x0);
+                tile_coords(tile, tiles_x, tiles_y, TR, b, y0, x0);
                 for (int c = 0; c < nchunks; c++, it++) {
                     const int s = it % S;
                     const uint32_t use = it / S;
@@ -155,9 +166,9 @@ __global__ void __launch_bounds__(THREADS, 1) k_conv3x3(const __grid_constant__ 
                         break;
                     }
                     unsigned char *st = smem + (size_t)s * a.stage_bytes;
-                    tc::mbar_arrive_expect_tx(&full_bar[s], a.stage_bytes);
+                    tc::mbar_arrive_expect_tx(&full_bar[s], a.tx_bytes);
                     for (int j = 0; j < a.ck / 8; j++)
-                        tc::tma_load_4d(st + j * KCOL, &xmap, c * a.ck + 8 * j, x0 - 1, y0 - 1, b, &full_bar[s]);
+                        tc::tma_load_4d(st + j * KC, &xmap, c * a.ck + 8 * j, x0 - 1, y0 - 1, b, &full_bar[s]);
                     tc::bulk_load(st + a.halo_bytes, a.wpack + (size_t)c * 9 * a.ck * a.n, 18u * a.ck * a.n,
                                   &full_bar[s]);
                 }
@@ -175,7 +186,7 @@ __global__ void __launch_bounds__(THREADS, 1) k_conv3x3(const __grid_constant__ 
             // adding the operand's address / 16 to the low 14-bit field (shared
             // memory addresses stay below 256 KB, so the add never carries), which
             // keeps the issuing thread to a few instructions per MMA.
-            const uint64_t adesc0 = tc::smem_desc(0, KCOL, 128);
+            const uint64_t adesc0 = tc::smem_desc(0, KC, 128);
             const uint64_t bdesc0 = tc::smem_desc(0, (uint32_t)a.n * 16, 128);
             const uint32_t nk = (uint32_t)a.ck / 16;     // K = 16 slices per 8-channel column pair
             const uint32_t bcol = (uint32_t)a.n;          // weights: descriptor units (16 B) per 8-channel column
@@ -186,7 +197,8 @@ __global__ void __launch_bounds__(THREADS, 1) k_conv3x3(const __grid_constant__ 
                 const uint32_t ause = tcount >> 1;
                 if (ause > 0 && !tc::mbar_wait(&acce_bar[ab], (ause - 1) & 1, abort_p)) break;
                 tc::tc_fence_after();
-                const uint32_t d0 = tbase + (uint32_t)(ab * TROWS * 128), d1 = d0 + 128;
+                // Accumulator of tile row t: TMEM columns (ab * TR + t) * n, n wide.
+                const uint32_t dbase = tbase + (uint32_t)(ab * TR * a.n);
                 for (int c = 0; c < nchunks; c++, it++) {
                     const int s = it % S;
                     if (!tc::mbar_wait(&full_bar[s], (it / S) & 1, abort_p)) {
@@ -203,11 +215,11 @@ __global__ void __launch_bounds__(THREADS, 1) k_conv3x3(const __grid_constant__ 
                         for (uint32_t kk = 0; kk < 2; kk++) {
                             if (kk >= nk) continue;
                             const uint64_t bdesc = bdesc0 + (uint64_t)(wst4 + (tap * 2 * nk + 2 * kk) * bcol);
-                            const uint64_t adesc =
-                                adesc0 + (uint64_t)(st4 + 2 * kk * (KCOL >> 4) + ty * HPX + tx);
+                            const uint64_t adesc = adesc0 + (uint64_t)(st4 + 2 * kk * (KC >> 4) + ty * HPX + tx);
                             const uint32_t acc = (c | tap | kk) != 0;
-                            tc::mma_bf16(d0, adesc, bdesc, idesc, acc);
-                            tc::mma_bf16(d1, adesc + HPX, bdesc, idesc, acc);
+#pragma unroll
+                            for (int t = 0; t < TR; t++)
+                                tc::mma_bf16(dbase + (uint32_t)(t * a.n), adesc + (uint64_t)(t * HPX), bdesc, idesc, acc);
                         }
                     }
                     tc::mma_commit(&empty_bar[s]);
@@ -232,17 +244,17 @@ __global__ void __launch_bounds__(THREADS, 1) k_conv3x3(const __grid_constant__ 
             tc::mbar_wait(&accf_bar[ab], (tcount >> 1) & 1, abort_p);  // completes at once: every lane observes the phase
             tc::tc_fence_after();
             int b, y0, x0;
-            tile_coords(tile, tiles_x, tiles_y, TROWS, b, y0, x0);
+            tile_coords(tile, tiles_x, tiles_y, TR, b, y0, x0);
             const int x = x0 + px;
 #pragma unroll 1
             for (int c0 = 0; c0 < a.n; c0 += 16) {
-                float v[TROWS][16];
+                float v[TR][16];
 #pragma unroll
-                for (int t = 0; t < TROWS; t++)
-                    tc::tmem_ld16(tbase + ((uint32_t)(q * 32) << 16) + (uint32_t)((ab * TROWS + t) * 128 + c0), v[t]);
+                for (int t = 0; t < TR; t++)
+                    tc::tmem_ld16(tbase + ((uint32_t)(q * 32) << 16) + (uint32_t)((ab * TR + t) * a.n + c0), v[t]);
                 if (c0 >= a.n_store) continue;  // warp-uniform
 #pragma unroll
-                for (int t = 0; t < TROWS; t++) {
+                for (int t = 0; t < TR; t++) {
                     const int y = y0 + t;
                     const bool in = y < a.H && x < a.W;
                     if (a.bias) {
@@ -300,27 +312,30 @@ __global__ void __launch_bounds__(THREADS, 1) k_conv3x3(const __grid_constant__ 
                     }
                 }
                 if (a.pool_out) {
-                    // 2x2 average of the stored (bf16-rounded) values: the two rows are
-                    // this thread's, the column pair is this lane and its neighbour
-                    // (x0 and 128-pixel tiles are even, H and W even).
-                    float pv[16];
+                    // 2x2 average of the stored (bf16-rounded) values: each row pair
+                    // (2 tp, 2 tp + 1) is this thread's, the column pair is this lane and
+                    // its neighbour (tiles start at even rows and columns; H, W even).
 #pragma unroll
-                    for (int i = 0; i < 16; i++) {
-                        float sum = 0.f;
+                    for (int tp = 0; tp < TR / 2; tp++) {
+                        float pv[16];
 #pragma unroll
-                        for (int t = 0; t < TROWS; t++) sum += __bfloat162float(__float2bfloat16_rn(v[t][i]));
-                        pv[i] = sum + __shfl_xor_sync(0xffffffffu, sum, 1);
-                    }
-                    const bool in = y0 < a.H && x < a.W;
-                    if (in && (x & 1) == 0) {
-                        uint4 w2[2];
-                        __nv_bfloat162 *w = reinterpret_cast<__nv_bfloat162 *>(w2);
+                        for (int i = 0; i < 16; i++) {
+                            const float sum = __bfloat162float(__float2bfloat16_rn(v[2 * tp][i])) +
+                                              __bfloat162float(__float2bfloat16_rn(v[2 * tp + 1][i]));
+                            pv[i] = sum + __shfl_xor_sync(0xffffffffu, sum, 1);
+                        }
+                        const int yp = y0 + 2 * tp;
+                        if (yp < a.H && x < a.W && (x & 1) == 0) {
+                            uint4 w2[2];
+                            __nv_bfloat162 *w = reinterpret_cast<__nv_bfloat162 *>(w2);
 #pragma unroll
-                        for (int i = 0; i < 8; i++) w[i] = __floats2bfloat162_rn(0.25f * pv[2 * i], 0.25f * pv[2 * i + 1]);
-                        uint4 *o = reinterpret_cast<uint4 *>(
-                            a.pool_out + (((size_t)b * (a.H / 2) + y0 / 2) * (a.W / 2) + x / 2) * a.n_store + c0);
-                        o[0] = w2[0];
-                        o[1] = w2[1];
+                            for (int i = 0; i < 8; i++)
+                                w[i] = __floats2bfloat162_rn(0.25f * pv[2 * i], 0.25f * pv[2 * i + 1]);
+                            uint4 *o = reinterpret_cast<uint4 *>(
+                                a.pool_out + (((size_t)b * (a.H / 2) + yp / 2) * (a.W / 2) + x / 2) * a.n_store + c0);
+                            o[0] = w2[0];
+                            o[1] = w2[1];
+                        }
                     }
                 }
             }
@@ -891,7 +906,7 @@ bool make_map(CUtensorMap *m, const void *base, int B, int H, int W, int C, int 
 void set_smem_attribute_once(const void *fn, int slot)
 {
     static std::mutex mu;
-    static bool done[64][2] = {};
+    static bool done[64][3] = {};
     int dev = 0;
     cudaGetDevice(&dev);
     std::lock_guard<std::mutex> lock(mu);
@@ -947,9 +962,15 @@ int32_t conv3x3(const ArtCnnConv *d, cudaStream_t s)
         return fail(ART_ERR_INVALID_ARGUMENT, "conv: pooled output needs even H and W and no mask");
     if (d->up2 && (!d->out || d->accumulate || d->mask))
         return fail(ART_ERR_INVALID_ARGUMENT, "conv: upsampled output needs out, no accumulate and no mask");
+    // Tile height: 4 output rows for narrow layers (n <= 32: their accumulators,
+    // 2 tiles x 4 rows x n columns, fit TMEM's 512 and the halo is re-read for
+    // 1.5x rather than 2x the rows), else 2.
+    const int trows = d->n <= 32 ? 4 : 2;
+    const uint32_t kc = trows == 4 ? HaloCol<4>::STRIDE : HaloCol<2>::STRIDE;
+    const uint32_t kc_tx = trows == 4 ? HaloCol<4>::TX : HaloCol<2>::TX;
     CUtensorMap map;
     std::string err;
-    if (!make_map(&map, d->x, d->B, d->H, d->W, d->cin, HPX, HROWS, err)) return fail(ART_ERR_CUDA, "conv: " + err);
+    if (!make_map(&map, d->x, d->B, d->H, d->W, d->cin, HPX, trows + 2, err)) return fail(ART_ERR_CUDA, "conv: " + err);
     ConvArgs a{};
     a.B = d->B;
     a.H = d->H;
@@ -971,16 +992,22 @@ int32_t conv3x3(const ArtCnnConv *d, cudaStream_t s)
     a.accumulate = d->accumulate;
     a.pool_out = static_cast<bf16 *>(d->pool_out);
     a.up2 = d->up2;
-    a.halo_bytes = (uint32_t)(d->ck / 8) * KCOL;
+    a.halo_bytes = (uint32_t)(d->ck / 8) * kc;
     a.stage_bytes = a.halo_bytes + 18u * d->ck * d->n;
+    a.tx_bytes = (uint32_t)(d->ck / 8) * kc_tx + 18u * d->ck * d->n;
     a.stages = (int)std::min<uint32_t>(MAX_STAGES, SMEM_BUDGET / a.stage_bytes);
     a.err = d->err;
     if (a.stages < 2) return fail(ART_ERR_INVALID_ARGUMENT, "conv: stage does not fit shared memory");
     const uint32_t smem = a.stages * a.stage_bytes + 1024;
-    set_smem_attribute_once(reinterpret_cast<const void *>(k_conv3x3), 0);
-    const long long ntiles = (long long)d->B * ((d->H + TROWS - 1) / TROWS) * ((d->W + TPX - 1) / TPX);
+    const long long ntiles = (long long)d->B * ((d->H + trows - 1) / trows) * ((d->W + TPX - 1) / TPX);
     const int grid = (int)std::min<long long>(ntiles, num_sms());
-    k_conv3x3<<<grid, THREADS, smem, s>>>(map, a);
+    if (trows == 4) {
+        set_smem_attribute_once(reinterpret_cast<const void *>(k_conv3x3<4>), 2);
+        k_conv3x3<4><<<grid, THREADS, smem, s>>>(map, a);
+    } else {
+        set_smem_attribute_once(reinterpret_cast<const void *>(k_conv3x3<2>), 0);
+        k_conv3x3<2><<<grid, THREADS, smem, s>>>(map, a);
+    }
     return check_launch("k_conv3x3");
 }
 

@@ -74,7 +74,7 @@ WORKLOADS["network"] = dict(
     metric="TFLOP/s (warm-start network forward, 1080p 4:2:0)", iterations=0)
 LEARNED_QUALITIES = (30, 50, 75)
 REFINE_ITERATIONS = 8
-REFINE_STEP_ITERATIONS = 4         # first refinement phase: steps of a 4-iteration run
+REFINE_STEP_ITERATIONS = 4         # first refinement phase (more than 12 iterations): steps of a 4-iteration run
 REFINE_TAIL = 2                    # last two iterations: FISTA restarted ...
 REFINE_TAIL_STEP_ITERATIONS = 100  # ... with steps of a 100-iteration run
 WEIGHT, PWEIGHT = 0.3, 0.001
@@ -269,12 +269,14 @@ class DeviceImage:
 
 def refine_schedule(k):
     """Refinement after a learned start: k plain iterations, the first k - 2
-    with the step of a REFINE_STEP_ITERATIONS-iteration run (large: they remove
-    the prediction's error), the last 2 restarted with the step of a
-    REFINE_TAIL_STEP_ITERATIONS-iteration run (small: they settle). Chosen on a
-    grid over the first step (1-4 iterations' worth), the tail length (2-6)
-    and the tail step (50-200) on the three 1080p images."""
-    return dict(step=REFINE_STEP_ITERATIONS, tail=min(REFINE_TAIL, k - 1), tail_step=REFINE_TAIL_STEP_ITERATIONS)
+    with the step of a short run (large: they remove the prediction's error;
+    2 iterations' worth for k <= 12, REFINE_STEP_ITERATIONS for more), the last
+    2 restarted with the step of a REFINE_TAIL_STEP_ITERATIONS-iteration run
+    (small: they settle). Chosen on a grid over the first step (1-4
+    iterations' worth), the tail length (2-6) and the tail step (50-200) on the
+    three 1080p images."""
+    return dict(step=2 if k <= 12 else REFINE_STEP_ITERATIONS, tail=min(REFINE_TAIL, k - 1),
+                tail_step=REFINE_TAIL_STEP_ITERATIONS)
 
 
 def learned_comparison(lib, device, steps, warmup, refine=REFINE_ITERATIONS, qualities=LEARNED_QUALITIES,
