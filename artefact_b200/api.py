@@ -270,8 +270,9 @@ class Artefact:
 
 def process_jpeg(jpeg: Jpeg, weight: Sequence[float], pweight: Sequence[float], iterations: Sequence[int],
                  separate: bool, benchmark: bool = False, *, init_mode: int = N.ART_INIT_DECODED,
-                 device: int = -1) -> np.ndarray:
-    """Solver dispatch and output stage of ``Artefact::process`` on decoded data."""
+                 device: int = -1, context: Optional["Context"] = None) -> np.ndarray:
+    """Solver dispatch and output stage of ``Artefact::process`` on decoded
+    data, on `context` (default: the calling thread's own context)."""
     lib = N.lib()
     keep: list = []
     n = jpeg.nchannel
@@ -281,7 +282,8 @@ def process_jpeg(jpeg: Jpeg, weight: Sequence[float], pweight: Sequence[float], 
     it = (C.c_uint32 * 3)(*[int(v) for v in iterations])
     rgb = None if benchmark else np.empty((jpeg.real_px_h, jpeg.real_px_w, 3), dtype=np.uint8)
     opts = _options(init_mode, device)
-    rc = lib.art_context_process(_context(device), n, chans, w, pw, it, int(bool(separate)), jpeg.real_px_w,
+    handle = context.handle if context is not None else _context(device)
+    rc = lib.art_context_process(handle, n, chans, w, pw, it, int(bool(separate)), jpeg.real_px_w,
                                  jpeg.real_px_h, None if rgb is None else rgb.ctypes.data, C.byref(opts))
     N.check(rc)
     if benchmark:
