@@ -105,12 +105,15 @@ def read_traffic(workload, kernel):
     return None
 
 
-def make_workload(kind):
-    """List of decoded Jpeg objects for the workload."""
+def make_workload(kind, keep_bytes=None):
+    """List of decoded Jpeg objects for the workload (their encoded bytes are
+    appended to `keep_bytes` when given)."""
     from artefact_b200 import synth
     from artefact_b200.api import Jpeg, JpegSource
 
     def dec(data):
+        if keep_bytes is not None:
+            keep_bytes.append(data)
         return Jpeg.from_source(JpegSource.Buffer(data))
 
     if kind == "1080p":
@@ -488,6 +491,36 @@ def run_learned(args, lib, local, rank, world, dist):
         print(json.dumps(line), flush=True)
 
 
+def pipeline_e2e(datas, iterations, device):
+    """JPEG bytes to RGB8 for every image of the workload through
+    Artefact::process semantics, host decode included: one image after the
+    other (decode, then process_jpeg), and overlapped (artefact_b200.pipeline:
+    4 decoder threads, 2 solver contexts). Wall clock, MPix/s of real area."""
+    from artefact_b200 import process_jpeg
+    from artefact_b200.api import Context, Jpeg, JpegSource
+    from artefact_b200.pipeline import process_stream
+
+    mpix = 0.0
+    ctx = Context(device)
+    for d in datas[:4]:  # warm-up: buffers and graphs for the first shapes
+        process_jpeg(Jpeg.from_source(JpegSource.Buffer(d)), [WEIGHT] * 3, [PWEIGHT] * 3, [iterations] * 3, False,
+                     context=ctx)
+    t = time.perf_counter()
+    for d in datas:
+        j = Jpeg.from_source(JpegSource.Buffer(d))
+        mpix += j.real_px_w * j.real_px_h / 1e6
+        process_jpeg(j, [WEIGHT] * 3, [PWEIGHT] * 3, [iterations] * 3, False, context=ctx)
+    serial = time.perf_counter() - t
+    ctx.close()
+    t = time.perf_counter()
+    n = sum(1 for _ in process_stream(datas, [WEIGHT] * 3, [PWEIGHT] * 3, [iterations] * 3, decoders=4, solvers=2,
+                                      depth=8, device=device))
+    piped = time.perf_counter() - t
+    assert n == len(datas)
+    return {"serial_mpix_s": mpix / serial, "pipelined_mpix_s": mpix / piped, "images": len(datas),
+            "decoders": 4, "solver_contexts": 2, "what": "JPEG bytes -> RGB8 (host decode, H2D, solve, RGB, D2H)"}
+
+
 def cpu_sample(kind, jpegs, iterations):
     """Bounded CPU measurement of the oracle: (MPix/s, description)."""
     real = sum(j.real_px_w * j.real_px_h for j in jpegs) / 1e6
@@ -612,7 +645,8 @@ def main():
                                            "algorithmic_flops_per_launch": flops, "launch_ms": ms}}), flush=True)
         return
     iters = wl["iterations"]
-    jpegs = make_workload(args.workload)
+    encoded = []
+    jpegs = make_workload(args.workload, encoded)
     nimg = len(jpegs)
     mpix = sum(j.real_px_w * j.real_px_h for j in jpegs) / 1e6
 
@@ -789,6 +823,11 @@ def main():
                        "reach_E_rel": r["min_refine_E_rel"],
                        "decoded_start_same_iterations_E_rel": r["min_refine_decoded_same_schedule_E_rel"]}
 
+    # Host decode overlapped with solving (batch workload, one GPU).
+    pipe = None
+    if args.workload == "batch256" and world == 1:
+        pipe = pipeline_e2e(encoded, iters, local)
+
     modes = len({(c.horizontal_samp_factor, c.vertical_samp_factor) for j in jpegs for c in j.coefs})
     nchs = len({j.nchannel for j in jpegs})
     per_step = sum(j.nchannel for j in jpegs) + 1 + (nchs + modes) * iters
@@ -813,6 +852,8 @@ def main():
         }
         if learned is not None:
             line["learned_warm_start"] = learned
+        if pipe is not None:
+            line["decode_pipeline"] = pipe
         print(json.dumps(line), flush=True)
     lib.art_context_destroy(ctx)
     if dist:
