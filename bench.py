@@ -495,7 +495,8 @@ def pipeline_e2e(datas, iterations, device):
     """JPEG bytes to RGB8 for every image of the workload through
     Artefact::process semantics, host decode included: one image after the
     other (decode, then process_jpeg), and overlapped (artefact_b200.pipeline:
-    4 decoder threads, 2 solver contexts). Wall clock, MPix/s of real area."""
+    host threads for decoding -- all but two, at most 12 -- and 2 solver
+    contexts). Wall clock, MPix/s of real area."""
     from artefact_b200 import process_jpeg
     from artefact_b200.api import Context, Jpeg, JpegSource
     from artefact_b200.pipeline import process_stream
@@ -512,13 +513,15 @@ def pipeline_e2e(datas, iterations, device):
         process_jpeg(j, [WEIGHT] * 3, [PWEIGHT] * 3, [iterations] * 3, False, context=ctx)
     serial = time.perf_counter() - t
     ctx.close()
+    decoders = max(1, min(12, (os.cpu_count() or 4) - 2))
     t = time.perf_counter()
-    n = sum(1 for _ in process_stream(datas, [WEIGHT] * 3, [PWEIGHT] * 3, [iterations] * 3, decoders=4, solvers=2,
-                                      depth=8, device=device))
+    n = sum(1 for _ in process_stream(datas, [WEIGHT] * 3, [PWEIGHT] * 3, [iterations] * 3, decoders=decoders,
+                                      solvers=2, depth=2 * decoders, device=device))
     piped = time.perf_counter() - t
     assert n == len(datas)
     return {"serial_mpix_s": mpix / serial, "pipelined_mpix_s": mpix / piped, "images": len(datas),
-            "decoders": 4, "solver_contexts": 2, "what": "JPEG bytes -> RGB8 (host decode, H2D, solve, RGB, D2H)"}
+            "decoders": decoders, "solver_contexts": 2,
+            "what": "JPEG bytes -> RGB8 (host decode, H2D, solve, RGB, D2H)"}
 
 
 def cpu_sample(kind, jpegs, iterations):
