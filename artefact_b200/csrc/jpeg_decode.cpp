@@ -10,9 +10,13 @@
 //   * quantised coefficients as int16 in natural (row-major, v*8+u) order within
 //     each 8x8 block, blocks in raster order over the component plane;
 //   * quantisation tables in natural order.
-// Sequential Huffman (SOF0/SOF1, 8-bit samples) with restart markers and
-// interleaved or single-component scans. Progressive and arithmetic coded
-// streams are rejected with an error.
+// Sequential (SOF0/SOF1) and progressive (SOF2) Huffman coding, 8-bit samples,
+// restart markers, interleaved or single-component scans. Progressive scans
+// follow ITU-T T.81 Annex G (zune-jpeg's mcu_prog.rs decodes the same
+// streams): DC first/refinement scans, AC spectral-selection first scans with
+// end-of-band runs, and AC successive-approximation refinement; the
+// coefficients accumulate over the scans into the same output contract.
+// Arithmetic-coded, lossless and hierarchical streams are rejected.
 #include <cstdint>
 #include <cstring>
 #include <string>
@@ -98,6 +102,8 @@ class Decoder {
     Huffman dc_[4], ac_[4];
     std::vector<Component> comps_;
     bool have_sof_ = false;
+    bool progressive_ = false;
+    int eobrun_ = 0;  // progressive AC scans: blocks left in the current end-of-band run
     int width_ = 0, height_ = 0;
     int hmax_ = 1, vmax_ = 1;
     int restart_interval_ = 0;
@@ -121,6 +127,11 @@ class Decoder {
     void parse_sof(int marker);
     void parse_sos();
     void decode_scan(const std::vector<int> &scomp);
+    void decode_scan_progressive(const std::vector<int> &scomp, int ss, int se, int ah, int al);
+    void prog_dc_first(Component &c, int16_t *blk, int al);
+    void prog_dc_refine(int16_t *blk, int al);
+    void prog_ac_first(Component &c, int16_t *blk, int ss, int se, int al);
+    void prog_ac_refine(Component &c, int16_t *blk, int ss, int se, int al);
     void fill_bits();
     int get_bits(int n);
     int decode_huff(const Huffman &h);
@@ -178,9 +189,11 @@ void Decoder::parse_dht()
 
 void Decoder::parse_sof(int marker)
 {
-    if (marker == 0xC2 || marker == 0xC6 || marker == 0xCA || marker == 0xCE)
-        fail("Progressive JPEG is not supported by this decoder");
-    if (marker != 0xC0 && marker != 0xC1) fail("Unsupported JPEG coding process (lossless or arithmetic)");
+    if (marker == 0xC6 || marker == 0xCA || marker == 0xCE)
+        fail("Differential or arithmetic progressive JPEG is not supported by this decoder");
+    if (marker != 0xC0 && marker != 0xC1 && marker != 0xC2)
+        fail("Unsupported JPEG coding process (lossless or arithmetic)");
+    progressive_ = marker == 0xC2;
     if (have_sof_) fail("Duplicate start of frame");
     int len = u16();
     int prec = u8();
@@ -364,6 +377,166 @@ void Decoder::decode_scan(const std::vector<int> &scomp)
         }
 }
 
+// Progressive DC first scan: the DC difference as in a sequential scan, the
+// coefficient stored shifted left by the scan's point transform Al (G.1.2.1).
+void Decoder::prog_dc_first(Component &c, int16_t *blk, int al)
+{
+    const Huffman &dc = dc_[c.td];
+    if (!dc.present) fail("No DC table for component");
+    int t = decode_huff(dc);
+    if (t > 11) fail("Bad DC magnitude category");
+    int diff = t ? extend(get_bits(t), t) : 0;
+    c.dc_pred += diff;
+    blk[0] = (int16_t)(c.dc_pred * (1 << al));
+}
+
+// Progressive DC refinement: one more bit of the DC coefficient (G.1.2.1).
+void Decoder::prog_dc_refine(int16_t *blk, int al)
+{
+    if (get_bits(1)) blk[0] = (int16_t)(blk[0] | (1 << al));
+}
+
+// Progressive AC first scan over zigzag positions ss..se (G.1.2.2): run/size
+// symbols as in a sequential scan, values shifted by Al; a symbol with size 0
+// and run r < 15 starts an end-of-band run of 2^r + (r extra bits) - 1 more
+// blocks whose band is all zero.
+void Decoder::prog_ac_first(Component &c, int16_t *blk, int ss, int se, int al)
+{
+    if (eobrun_ > 0) {
+        eobrun_--;
+        return;
+    }
+    const Huffman &ac = ac_[c.ta];
+    if (!ac.present) fail("No AC table for component");
+    for (int k = ss; k <= se;) {
+        int rs = decode_huff(ac);
+        int r = rs >> 4, sz = rs & 15;
+        if (sz == 0) {
+            if (r < 15) {
+                eobrun_ = (1 << r) - 1;
+                if (r) eobrun_ += get_bits(r);
+                break;
+            }
+            k += 16;
+            continue;
+        }
+        k += r;
+        if (k > se) fail("Coefficient index out of range: corrupt JPEG");
+        blk[kZigzagToNatural[k]] = (int16_t)(extend(get_bits(sz), sz) * (1 << al));
+        k++;
+    }
+}
+
+// Progressive AC refinement over zigzag positions ss..se (G.1.2.3). Each
+// coefficient already non-zero gets one correction bit (adding 2^Al in its
+// own sign's direction when set and that bit is not yet in it); the zero run
+// of a symbol counts only coefficients still zero, and the symbol's new
+// coefficient (size 1: +-2^Al by one sign bit) lands on the zero after that
+// run. Inside an end-of-band run only the correction bits are read.
+void Decoder::prog_ac_refine(Component &c, int16_t *blk, int ss, int se, int al)
+{
+    const int p1 = 1 << al, m1 = -(1 << al);
+    auto correct = [&](int16_t &coef) {
+        if (get_bits(1) && (coef & p1) == 0) coef = (int16_t)(coef + (coef >= 0 ? p1 : m1));
+    };
+    int k = ss;
+    if (eobrun_ == 0) {
+        const Huffman &ac = ac_[c.ta];
+        if (!ac.present) fail("No AC table for component");
+        for (; k <= se;) {
+            int rs = decode_huff(ac);
+            int r = rs >> 4, sz = rs & 15;
+            int value = 0;
+            if (sz) {
+                if (sz != 1) fail("Bad AC refinement symbol: corrupt JPEG");
+                value = get_bits(1) ? p1 : m1;
+            } else if (r != 15) {
+                eobrun_ = 1 << r;
+                if (r) eobrun_ += get_bits(r);
+                break;  // the rest of this block is in the end-of-band run
+            }
+            // Skip r still-zero coefficients (correcting the non-zero ones
+            // passed on the way), then place `value` on the next zero.
+            while (k <= se) {
+                int16_t &coef = blk[kZigzagToNatural[k]];
+                if (coef != 0) {
+                    correct(coef);
+                } else {
+                    if (r == 0) {
+                        if (value) coef = (int16_t)value;
+                        k++;
+                        break;
+                    }
+                    r--;
+                }
+                k++;
+            }
+        }
+    }
+    if (eobrun_ > 0) {
+        for (; k <= se; k++) {
+            int16_t &coef = blk[kZigzagToNatural[k]];
+            if (coef != 0) correct(coef);
+        }
+        eobrun_--;
+    }
+}
+
+// One progressive scan: DC scans may interleave components (MCU order as in a
+// sequential scan); AC scans cover one component in its own block order.
+void Decoder::decode_scan_progressive(const std::vector<int> &scomp, int ss, int se, int ah, int al)
+{
+    reset_bits();
+    for (auto &c : comps_) c.dc_pred = 0;
+    eobrun_ = 0;
+    int todo = restart_interval_;
+    auto restart_if_due = [&]() {
+        if (restart_interval_ && todo == 0) {
+            handle_restart();
+            eobrun_ = 0;
+            todo = restart_interval_;
+        }
+    };
+    auto one_block = [&](Component &c, uint32_t bx, uint32_t by) {
+        int16_t scratch[64] = {0};
+        const bool inside = bx < c.block_w && by < c.block_h;
+        int16_t *blk = inside ? &c.coefs[((size_t)by * c.block_w + bx) * 64] : scratch;
+        if (ss == 0) {
+            if (ah == 0)
+                prog_dc_first(c, blk, al);
+            else
+                prog_dc_refine(blk, al);
+        } else if (ah == 0) {
+            prog_ac_first(c, blk, ss, se, al);
+        } else {
+            prog_ac_refine(c, blk, ss, se, al);
+        }
+    };
+    if (scomp.size() == 1) {
+        Component &c = comps_[scomp[0]];
+        int cw = (width_ * c.h + hmax_ - 1) / hmax_, chh = (height_ * c.v + vmax_ - 1) / vmax_;
+        int bw = (cw + 7) / 8, bh = (chh + 7) / 8;
+        for (int by = 0; by < bh; by++)
+            for (int bx = 0; bx < bw; bx++) {
+                restart_if_due();
+                one_block(c, (uint32_t)bx, (uint32_t)by);
+                if (restart_interval_) todo--;
+            }
+        return;
+    }
+    int mcu_w = (width_ + 8 * hmax_ - 1) / (8 * hmax_), mcu_h = (height_ + 8 * vmax_ - 1) / (8 * vmax_);
+    for (int my = 0; my < mcu_h; my++)
+        for (int mx = 0; mx < mcu_w; mx++) {
+            restart_if_due();
+            for (int ci : scomp) {
+                Component &c = comps_[ci];
+                for (int v = 0; v < c.v; v++)
+                    for (int u = 0; u < c.h; u++) one_block(c, (uint32_t)(mx * c.h + u), (uint32_t)(my * c.v + v));
+            }
+            if (restart_interval_) todo--;
+        }
+}
+
 void Decoder::parse_sos()
 {
     int len = u16();
@@ -384,13 +557,22 @@ void Decoder::parse_sos()
         comps_[idx].td = t >> 4;
         comps_[idx].ta = t & 15;
         if (comps_[idx].td > 3 || comps_[idx].ta > 3) fail("Invalid Huffman table index in scan");
-        if (!dc_[comps_[idx].td].present) fail("No DC table for component");
-        if (!ac_[comps_[idx].ta].present) fail("No AC table for component");
+        if (!progressive_) {
+            if (!dc_[comps_[idx].td].present) fail("No DC table for component");
+            if (!ac_[comps_[idx].ta].present) fail("No AC table for component");
+        }
         scomp.push_back(idx);
     }
     int ss = u8(), se = u8(), ahal = u8();
-    if (ss != 0 || se != 63 || ahal != 0) fail("Invalid spectral selection for a sequential scan");
-    decode_scan(scomp);
+    if (!progressive_) {
+        if (ss != 0 || se != 63 || ahal != 0) fail("Invalid spectral selection for a sequential scan");
+        decode_scan(scomp);
+        return;
+    }
+    const int ah = ahal >> 4, al = ahal & 15;
+    if (se > 63 || ss > se || (ss == 0 && se != 0) || (ss > 0 && ns != 1) || al > 13 || ah > 13)
+        fail("Invalid progressive scan parameters");
+    decode_scan_progressive(scomp, ss, se, ah, al);
 }
 
 void Decoder::run(JpegImage &out)

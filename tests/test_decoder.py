@@ -92,16 +92,71 @@ def test_rounded_sizes_follow_max_sampling():
         (1920, 1088, 1), (960, 544, 2), (960, 544, 2)]
 
 
-def test_progressive_is_reported_unsupported():
+def _pillow(img, quality, subsampling, progressive, **kw):
     from PIL import Image
 
     buf = io.BytesIO()
-    Image.fromarray(synth.channel_image(32, 32, 1)).save(buf, "JPEG", quality=80, progressive=True)
-    with pytest.raises(ArtefactError, match="Progressive"):
-        Jpeg.from_source(JpegSource.Buffer(buf.getvalue()))
+    opts = dict(format="JPEG", quality=quality, optimize=False, progressive=progressive, **kw)
+    if img.ndim == 3:
+        opts["subsampling"] = subsampling
+    Image.fromarray(img).save(buf, **opts)
+    return buf.getvalue()
+
+
+@pytest.mark.parametrize("w,h,q,sub,gray,restart", [
+    (72, 40, 75, 2, False, {}), (131, 67, 30, 0, False, {}), (64, 48, 50, 0, True, {}),
+    (200, 136, 90, 2, False, {}), (33, 17, 20, 1, False, {}), (130, 70, 60, 2, False, {"restart_marker_blocks": 3}),
+    (96, 80, 40, 0, False, {"restart_marker_rows": 1}), (57, 91, 85, 0, True, {"restart_marker_blocks": 5}),
+])
+def test_progressive_equals_sequential(w, h, q, sub, gray, restart):
+    """A progressive stream (libjpeg's default script: spectral selection and
+    successive approximation for DC and AC, EOB runs) of the same image carries
+    the same quantised coefficients as the sequential one: the decoder must
+    return them bit for bit, with the same tables and sizes."""
+    img = synth.channel_image(h, w, 7) if gray else synth.rgb_image(h, w, 7)
+    a = Jpeg.from_source(JpegSource.Buffer(_pillow(img, q, sub, False, **restart)))
+    pdata = _pillow(img, q, sub, True, **restart)
+    assert pdata[:2] == b"\xff\xd8" and b"\xff\xc2" in pdata  # really progressive (SOF2)
+    b = Jpeg.from_source(JpegSource.Buffer(pdata))
+    assert (a.nchannel, a.real_px_w, a.real_px_h) == (b.nchannel, b.real_px_w, b.real_px_h)
+    for x, y in zip(a.coefs, b.coefs):
+        assert (x.rounded_px_w, x.rounded_px_h, x.horizontal_samp_factor, x.vertical_samp_factor) == (
+            y.rounded_px_w, y.rounded_px_h, y.horizontal_samp_factor, y.vertical_samp_factor)
+        np.testing.assert_array_equal(x.quant_table, y.quant_table)
+        np.testing.assert_array_equal(x.dct_coefs, y.dct_coefs)
+
+
+def test_truncated_progressive_stream_is_an_error_or_partial():
+    """A progressive stream cut inside its scans decodes what it holds or fails
+    with a decode error; it never crashes."""
+    data = _pillow(synth.rgb_image(64, 64, 3), 75, 2, True)
+    for cut in (len(data) // 4, len(data) // 2, len(data) - 10):
+        try:
+            Jpeg.from_source(JpegSource.Buffer(data[:cut]))
+        except ArtefactError:
+            pass
 
 
 def test_truncated_stream_is_an_error():
     data = synth.make_jpeg(64, 64, 75, "4:2:0", False, seed=2)
     with pytest.raises(ArtefactError):
         Jpeg.from_source(JpegSource.Buffer(data[:200]))
+
+
+@pytest.mark.parametrize("progressive", [False, True])
+def test_corrupted_streams_never_crash(progressive):
+    """Seeded byte flips in the entropy-coded data: each decode returns
+    coefficients or a decode error (the decoder reads only inside the buffer
+    and writes only inside its planes)."""
+    rng = np.random.default_rng(17 + progressive)
+    data = _pillow(synth.rgb_image(48, 80, 5), 70, 2, progressive, restart_marker_blocks=4)
+    start = data.index(b"\xff\xda")
+    for _ in range(150):
+        d = bytearray(data)
+        for _ in range(int(rng.integers(1, 6))):
+            d[int(rng.integers(start + 10, len(d) - 2))] = int(rng.integers(0, 256))
+        try:
+            j = Jpeg.from_source(JpegSource.Buffer(bytes(d)))
+            assert all(c.dct_coefs.size == c.block_w * c.block_h * 64 for c in j.coefs)
+        except ArtefactError:
+            pass
