@@ -350,7 +350,8 @@ class Context:
         return outs
 
     def compute_batch(self, jobs: Sequence[dict], iterations: int, init_mode: int = N.ART_INIT_DECODED,
-                      step_iterations: int = 0) -> List[List[np.ndarray]]:
+                      step_iterations: int = 0, tail_iterations: int = 0,
+                      tail_step_iterations: int = 0) -> List[List[np.ndarray]]:
         """Solve many images together (one launch per kernel and iteration over
         all of them, the loop in one CUDA graph). Each job is a dict with keys
         ``coefs`` (list of :class:`Coefficient`), ``weight``, ``pweight`` and
@@ -376,7 +377,8 @@ class Context:
             im.out_planes = C.cast(ptrs, C.POINTER(C.c_void_p))
             results.append(outs)
         N.check(N.lib().art_context_compute_batch(self._h, len(jobs), imgs, int(iterations),
-                                                  C.byref(_options(init_mode, -1, step_iterations))))
+                                                  C.byref(_options(init_mode, -1, step_iterations, tail_iterations,
+                                                                   tail_step_iterations))))
         return results
 
     def autotune(self, nchannel: int, samp_h: Sequence[int], samp_v: Sequence[int], max_w: int, max_h: int,

@@ -76,3 +76,29 @@ def test_sweep_variants_agree(gpu, monkeypatch, shape):
                 b = ctx.compute(j.nchannel, j.coefs, 0.3, [0.001] * 3, 30, W, H)
             assert all(np.array_equal(x, y) for x, y in zip(a, b))
             check_parity(j, 30, label=f"sweep variant {kind} rows {rows}", gpu=a)
+
+
+def test_learned_batch_matches_single_learned_solves(gpu):
+    """The learned start in a batch (each image's components through the
+    network, the chroma pair as one batch) equals the learned start of each
+    image alone, with the two-phase refinement schedule."""
+    from artefact_b200 import _native as N
+    from artefact_b200 import warmstart as WS
+
+    shapes = [(96, 64, 75, "4:2:0", False), (40, 24, 50, "4:4:4", True), (130, 70, 30, "4:4:4", False),
+              (64, 48, 60, "4:2:2", False)]
+    jpegs = [_jpeg(*s, seed=700 + i) for i, s in enumerate(shapes)]
+    jobs = [dict(coefs=j.coefs, weight=0.3, pweight=[0.001] * 3) for j in jpegs]
+    net = WS.WarmStartNet.load() if WS.DEFAULT_WEIGHTS.exists() else WS.WarmStartNet(WS.init_params(2))
+    sched = dict(step_iterations=2, tail_iterations=2, tail_step_iterations=100)
+    with Context(0) as ctx:
+        ctx.set_warm_start(net)
+        batch = ctx.compute_batch(jobs, 8, init_mode=N.ART_INIT_LEARNED, **sched)
+        for j, got in zip(jpegs, batch):
+            W, H, _ = j.max_rounded()
+            single = ctx.compute(j.nchannel, j.coefs, 0.3, [0.001] * 3, 8, W, H, init_mode=N.ART_INIT_LEARNED, **sched)
+            d = max(float(np.abs(a - b).max()) for a, b in zip(got, single))
+            assert d <= 1e-2, (j.real_px_w, j.real_px_h, d)
+            ev = O.feasibility(j.nchannel, j.coefs, W, H, got)
+            assert ev <= 1e-3
+        ctx.set_warm_start(None)
