@@ -47,7 +47,9 @@ constexpr int HPX = TPX + 2;                // halo tile width
 constexpr int HROWS = TROWS + 2;            // weight gradient: halo tile height
 constexpr uint32_t KCOL = HROWS * HPX * 16; // weight gradient: bytes of one 8-channel halo column (8320, 65 x 128)
 constexpr uint32_t DYREG = TROWS * TPX * 16;// bytes of one 8-channel region of a gradient tile (4096)
-constexpr int THREADS = 192;                // warp 0 loads, warp 1 MMA, warps 2-5 epilogue
+constexpr int THREADS = 192;                // weight gradient: warp 0 loads, warp 1 MMA, warps 2-5 epilogue
+constexpr int CONV_THREADS = 320;           // convolution: warp 0 loads, warp 1 MMA, warps 2-9 epilogue
+constexpr int EPI_THREADS = CONV_THREADS - 64;
 constexpr uint32_t SMEM_BUDGET = 220 * 1024;  // pipeline stages; 1 KB more is requested for alignment
 constexpr int MAX_STAGES = 4;
 
@@ -55,7 +57,7 @@ struct ConvArgs {
     int B, H, W;
     int cin, ck;      // input channels (multiple of ck), channels per pipeline stage (16 or 32)
     int n, n_store;   // MMA N (multiple of 16, <= 128), channels stored (multiple of 16, <= n)
-    const bf16 *wpack;  // [cin/ck][9][ck/8][n][8]
+    const bf16 *wpack;  // [cin/ck][3 tap columns][ck/8][3 tap rows][n][8]
     const float *bias;  // [n] or null
     bf16 *out;
     int out_cstride, out_coff;
@@ -105,19 +107,35 @@ __device__ __forceinline__ unsigned char *aligned_smem(unsigned char *p)
     return p + ((1024 - (a & 1023)) & 1023);
 }
 
-// Shared-memory stride of one 8-channel column of a halo tile for TR output
-// rows: (TR + 2) x HPX pixels x 16 bytes, rounded up to 128 (TMA destinations
-// stay 128-byte aligned); and the bytes the TMA writes into it.
-template <int TR>
-struct HaloCol {
-    static constexpr uint32_t TX = (uint32_t)(TR + 2) * HPX * 16;
-    static constexpr uint32_t STRIDE = (TX + 127u) / 128u * 128u;
-};
+// Halo tile of one input-channel chunk (ck = 16 or 32 channels) for TR output
+// rows: (TR + 2) x HPX pixels, one row of ck x 2 bytes per pixel, written by one
+// TMA box with the 32- or 64-byte swizzle and read by the MMAs through swizzled
+// K-major descriptors. Rounded up to 1 KB so that every stage starts on a 1 KB
+// boundary.
+__host__ __device__ constexpr uint32_t halo_rows(int tr) { return (uint32_t)(tr + 2) * HPX; }
+__host__ __device__ constexpr uint32_t halo_bytes(int tr, int ck) { return (halo_rows(tr) * (uint32_t)ck * 2u + 1023u) / 1024u * 1024u; }
+
+// The stacked MMAs of one (tap column, K slice) for TR output rows: halo row r
+// times tap rows lo..hi (those with 0 <= r - ty < TR, from tap row LO0 on),
+// into the accumulators of output rows r - hi .. r - lo (reverse column order,
+// see the MMA warp in k_conv3x3). All bounds are compile-time.
+template <int TR, int LO0>
+__device__ __forceinline__ void issue_halo_rows(uint32_t dbase, uint64_t at, uint64_t bt, uint32_t n, uint32_t rstep,
+                                                const uint32_t (&idesc)[3])
+{
+#pragma unroll
+    for (int r = 0; r < TR + 2; r++) {
+        const int lo = r - TR + 1 > LO0 ? r - TR + 1 : LO0;
+        const int hi = r < 2 ? r : 2;
+        if (lo > hi) continue;
+        tc::mma_bf16(dbase + (uint32_t)(TR - 1 - r + lo) * n, at + (uint64_t)(r * rstep), bt + (uint64_t)lo * n,
+                     idesc[hi - lo], 1);
+    }
+}
 
 template <int TR>
-__global__ void __launch_bounds__(THREADS, 1) k_conv3x3(const __grid_constant__ CUtensorMap xmap, const ConvArgs a)
+__global__ void __launch_bounds__(CONV_THREADS, 1) k_conv3x3(const __grid_constant__ CUtensorMap xmap, const ConvArgs a)
 {
-    constexpr uint32_t KC = HaloCol<TR>::STRIDE;
     extern __shared__ __align__(1024) unsigned char smem_raw[];
     unsigned char *smem = aligned_smem(smem_raw);
     __shared__ __align__(8) uint64_t full_bar[MAX_STAGES], empty_bar[MAX_STAGES], accf_bar[2], acce_bar[2],
@@ -140,7 +158,7 @@ __global__ void __launch_bounds__(THREADS, 1) k_conv3x3(const __grid_constant__ 
         }
         for (int b = 0; b < 2; b++) {
             tc::mbar_init(&accf_bar[b], 1);
-            tc::mbar_init(&acce_bar[b], 128);
+            tc::mbar_init(&acce_bar[b], EPI_THREADS);
         }
         tc::mbar_init(&done_bar, 1);
         tc::fence_barrier_init();
@@ -167,8 +185,7 @@ __global__ void __launch_bounds__(THREADS, 1) k_conv3x3(const __grid_constant__ 
                     }
                     unsigned char *st = smem + (size_t)s * a.stage_bytes;
                     tc::mbar_arrive_expect_tx(&full_bar[s], a.tx_bytes);
-                    for (int j = 0; j < a.ck / 8; j++)
-                        tc::tma_load_4d(st + j * KC, &xmap, c * a.ck + 8 * j, x0 - 1, y0 - 1, b, &full_bar[s]);
+                    tc::tma_load_4d(st, &xmap, c * a.ck, x0 - 1, y0 - 1, b, &full_bar[s]);
                     tc::bulk_load(st + a.halo_bytes, a.wpack + (size_t)c * 9 * a.ck * a.n, 18u * a.ck * a.n,
                                   &full_bar[s]);
                 }
@@ -181,15 +198,31 @@ __global__ void __launch_bounds__(THREADS, 1) k_conv3x3(const __grid_constant__ 
         __syncwarp();
     } else if (warp == 1) {
         if (lane == 0) {
-            const uint32_t idesc = tc::idesc_bf16(128, a.n, 0, 0);
+            // Accumulator of output row t: TMEM columns (ab * TR + TR - 1 - t) * n,
+            // n wide (rows in reverse order). Halo row r times the three tap rows
+            // of one tap column stacked along N (weights of tap row ty in operand
+            // rows ty*n..) adds tap row ty's products to output row r - ty, whose
+            // accumulator sits ty * n columns after row r's: one MMA of up to 3n
+            // columns covers every (output row, tap row) pair of that halo row
+            // (the rows with r - ty outside the tile are left out of the N range).
+            // A halo row meets at most min(3, TR) tap rows, and 4-row tiles have
+            // n <= 64, so one MMA spans at most 256 columns.
+            const uint32_t n = (uint32_t)a.n;
+            const uint32_t idesc[3] = {tc::idesc_bf16(128, a.n, 0, 0),
+                                       tc::idesc_bf16(128, TR >= 2 ? 2 * a.n : a.n, 0, 0),
+                                       tc::idesc_bf16(128, TR >= 3 ? 3 * a.n : a.n, 0, 0)};
             // Descriptors are built once with address 0 and offset per MMA by
             // adding the operand's address / 16 to the low 14-bit field (shared
             // memory addresses stay below 256 KB, so the add never carries), which
-            // keeps the issuing thread to a few instructions per MMA.
-            const uint64_t adesc0 = tc::smem_desc(0, KC, 128);
-            const uint64_t bdesc0 = tc::smem_desc(0, (uint32_t)a.n * 16, 128);
-            const uint32_t nk = (uint32_t)a.ck / 16;     // K = 16 slices per 8-channel column pair
-            const uint32_t bcol = (uint32_t)a.n;          // weights: descriptor units (16 B) per 8-channel column
+            // keeps the issuing thread to a few instructions per MMA. The halo's
+            // pixel rows are ck x 2 bytes (ru descriptor units): tap column tx and
+            // halo row r start r x HPX + tx rows in. Weights: 8-channel columns
+            // 3n x 16 bytes apart, tap row ty at + ty * n units.
+            const uint32_t ru = (uint32_t)a.ck / 8;
+            const uint64_t adesc0 = tc::smem_desc_sw(0, 8u * (uint32_t)a.ck * 2u, a.ck == 32 ? 4u : 6u);
+            const uint64_t bdesc0 = tc::smem_desc(0, 3u * n * 16u, 128);
+            const uint32_t nk = (uint32_t)a.ck / 16;     // K = 16 slices per chunk
+            const uint32_t kcols = (uint32_t)a.ck / 8;
             uint32_t it = 0, tcount = 0;
             bool ok = true;
             for (int tile = blockIdx.x; tile < ntiles && ok; tile += gridDim.x, tcount++) {
@@ -197,8 +230,7 @@ __global__ void __launch_bounds__(THREADS, 1) k_conv3x3(const __grid_constant__ 
                 const uint32_t ause = tcount >> 1;
                 if (ause > 0 && !tc::mbar_wait(&acce_bar[ab], (ause - 1) & 1, abort_p)) break;
                 tc::tc_fence_after();
-                // Accumulator of tile row t: TMEM columns (ab * TR + t) * n, n wide.
-                const uint32_t dbase = tbase + (uint32_t)(ab * TR * a.n);
+                const uint32_t dbase = tbase + (uint32_t)(ab * TR) * n;
                 for (int c = 0; c < nchunks; c++, it++) {
                     const int s = it % S;
                     if (!tc::mbar_wait(&full_bar[s], (it / S) & 1, abort_p)) {
@@ -209,17 +241,24 @@ __global__ void __launch_bounds__(THREADS, 1) k_conv3x3(const __grid_constant__ 
                     const uint32_t st4 = tc::smem_u32(smem + (size_t)s * a.stage_bytes) >> 4;
                     const uint32_t wst4 = st4 + (a.halo_bytes >> 4);
 #pragma unroll
-                    for (int tap = 0; tap < 9; tap++) {
-                        const uint32_t ty = tap / 3, tx = tap % 3;
+                    for (uint32_t tx = 0; tx < 3; tx++) {
 #pragma unroll
                         for (uint32_t kk = 0; kk < 2; kk++) {
                             if (kk >= nk) continue;
-                            const uint64_t bdesc = bdesc0 + (uint64_t)(wst4 + (tap * 2 * nk + 2 * kk) * bcol);
-                            const uint64_t adesc = adesc0 + (uint64_t)(st4 + 2 * kk * (KC >> 4) + ty * HPX + tx);
-                            const uint32_t acc = (c | tap | kk) != 0;
+                            const uint64_t at = adesc0 + (uint64_t)(st4 + 2 * kk + tx * ru);
+                            const uint64_t bt = bdesc0 + (uint64_t)(wst4 + (tx * kcols + 2 * kk) * 3u * n);
+                            // The first K slice of a tile initialises every accumulator
+                            // with tap row 0 alone; everything after accumulates.
+                            const uint32_t rstep = HPX * ru;
+                            if (c == 0 && tx == 0 && kk == 0) {
 #pragma unroll
-                            for (int t = 0; t < TR; t++)
-                                tc::mma_bf16(dbase + (uint32_t)(t * a.n), adesc + (uint64_t)(t * HPX), bdesc, idesc, acc);
+                                for (int t = 0; t < TR; t++)
+                                    tc::mma_bf16(dbase + (uint32_t)(TR - 1 - t) * n, at + (uint64_t)(t * rstep), bt,
+                                                 idesc[0], 0);
+                                issue_halo_rows<TR, 1>(dbase, at, bt, n, rstep, idesc);
+                            } else {
+                                issue_halo_rows<TR, 0>(dbase, at, bt, n, rstep, idesc);
+                            }
                         }
                     }
                     tc::mma_commit(&empty_bar[s]);
@@ -231,8 +270,12 @@ __global__ void __launch_bounds__(THREADS, 1) k_conv3x3(const __grid_constant__ 
         }
         __syncwarp();
     } else {
+        // Two warps per TMEM lane quarter (a warp reaches lanes 32 (warp % 4) ..
+        // + 31 only), splitting the 16-channel groups between them.
         const int q = warp & 3;  // TMEM lanes 32q..32q+31 belong to this warp
+        const int half = (warp - 2) >> 2;
         const int px = q * 32 + lane;
+        constexpr int G = TR < 4 ? TR : 4;
         uint32_t tcount = 0;
         for (int tile = blockIdx.x; tile < ntiles; tile += gridDim.x, tcount++) {
             const int ab = tcount & 1;
@@ -247,94 +290,109 @@ __global__ void __launch_bounds__(THREADS, 1) k_conv3x3(const __grid_constant__ 
             tile_coords(tile, tiles_x, tiles_y, TR, b, y0, x0);
             const int x = x0 + px;
 #pragma unroll 1
-            for (int c0 = 0; c0 < a.n; c0 += 16) {
-                float v[TR][16];
+            for (int c0 = half * 16; c0 < a.n_store; c0 += 32) {
+                float bias[16];
 #pragma unroll
-                for (int t = 0; t < TR; t++)
-                    tc::tmem_ld16(tbase + ((uint32_t)(q * 32) << 16) + (uint32_t)((ab * TR + t) * a.n + c0), v[t]);
-                if (c0 >= a.n_store) continue;  // warp-uniform
+                for (int i = 0; i < 16; i++) bias[i] = a.bias ? __ldg(a.bias + c0 + i) : 0.f;
+                // Rows of this channel group in groups of G (accumulator of row t
+                // at column (ab * TR + TR - 1 - t) * n + c0), one wait per group.
+                const uint32_t lane_base = tbase + ((uint32_t)(q * 32) << 16) + (uint32_t)c0;
 #pragma unroll
-                for (int t = 0; t < TR; t++) {
-                    const int y = y0 + t;
-                    const bool in = y < a.H && x < a.W;
-                    if (a.bias) {
+                for (int g = 0; g < TR; g += G) {
+                    float v[G][16];
+                    if constexpr (G == 1) {
+                        tc::tmem_ld16(lane_base + (uint32_t)(ab * a.n), v[0]);
+                    } else if constexpr (G == 2) {
+                        const uint32_t ad[2] = {lane_base + (uint32_t)((ab * TR + TR - 1 - g) * a.n),
+                                                lane_base + (uint32_t)((ab * TR + TR - 2 - g) * a.n)};
+                        tc::tmem_ld16x2(ad, v);
+                    } else {
+                        uint32_t ad[4];
 #pragma unroll
-                        for (int i = 0; i < 16; i++) v[t][i] += __ldg(a.bias + c0 + i);
+                        for (int k = 0; k < 4; k++) ad[k] = lane_base + (uint32_t)((ab * TR + TR - 1 - (g + k)) * a.n);
+                        tc::tmem_ld16x4(ad, v);
                     }
-                    if (a.relu) {
 #pragma unroll
-                        for (int i = 0; i < 16; i++) v[t][i] = fmaxf(v[t][i], 0.f);
-                    }
-                    if (!in) continue;
-                    const size_t pix = ((size_t)b * a.H + y) * a.W + x;
-                    if (a.mask) {
-                        const uint4 *mp = reinterpret_cast<const uint4 *>(a.mask + pix * a.mask_cstride + c0);
-                        const uint4 m2[2] = {__ldg(mp), __ldg(mp + 1)};
-                        const bf16 *m = reinterpret_cast<const bf16 *>(m2);
+                    for (int t = 0; t < G; t++) {
+                        const int y = y0 + g + t;
+                        const bool in = y < a.H && x < a.W;
 #pragma unroll
-                        for (int i = 0; i < 16; i++) v[t][i] = __bfloat162float(m[i]) > 0.f ? v[t][i] : 0.f;
-                    }
-                    if (a.out_f32) {
-                        float4 *o = reinterpret_cast<float4 *>(a.out_f32 + pix * a.f32_cstride + c0);
+                        for (int i = 0; i < 16; i++) v[t][i] += bias[i];
+                        if (a.relu) {
 #pragma unroll
-                        for (int i = 0; i < 4; i++)
-                            o[i] = make_float4(v[t][4 * i], v[t][4 * i + 1], v[t][4 * i + 2], v[t][4 * i + 3]);
-                    }
-                    if (a.out) {
-                        uint4 w2[2];
-                        __nv_bfloat162 *w = reinterpret_cast<__nv_bfloat162 *>(w2);
-                        if (a.up2) {
-#pragma unroll
-                            for (int i = 0; i < 8; i++) w[i] = __floats2bfloat162_rn(v[t][2 * i], v[t][2 * i + 1]);
-#pragma unroll
-                            for (int dy = 0; dy < 2; dy++)
-#pragma unroll
-                                for (int dx = 0; dx < 2; dx++) {
-                                    uint4 *o = reinterpret_cast<uint4 *>(
-                                        a.out + (((size_t)b * 2 * a.H + 2 * y + dy) * 2 * a.W + 2 * x + dx) * a.out_cstride +
-                                        a.out_coff + c0);
-                                    o[0] = w2[0];
-                                    o[1] = w2[1];
-                                }
-                        } else {
-                            uint4 *o = reinterpret_cast<uint4 *>(a.out + pix * a.out_cstride + a.out_coff + c0);
-                            if (a.accumulate) {
-                                const uint4 p2[2] = {o[0], o[1]};
-                                const bf16 *p = reinterpret_cast<const bf16 *>(p2);
-#pragma unroll
-                                for (int i = 0; i < 16; i++) v[t][i] += __bfloat162float(p[i]);
-                            }
-#pragma unroll
-                            for (int i = 0; i < 8; i++) w[i] = __floats2bfloat162_rn(v[t][2 * i], v[t][2 * i + 1]);
-                            o[0] = w2[0];
-                            o[1] = w2[1];
+                            for (int i = 0; i < 16; i++) v[t][i] = fmaxf(v[t][i], 0.f);
                         }
-                    }
-                }
-                if (a.pool_out) {
-                    // 2x2 average of the stored (bf16-rounded) values: each row pair
-                    // (2 tp, 2 tp + 1) is this thread's, the column pair is this lane and
-                    // its neighbour (tiles start at even rows and columns; H, W even).
+                        if (!in) continue;
+                        const size_t pix = ((size_t)b * a.H + y) * a.W + x;
+                        if (a.mask) {
+                            const uint4 *mp = reinterpret_cast<const uint4 *>(a.mask + pix * a.mask_cstride + c0);
+                            const uint4 m2[2] = {__ldg(mp), __ldg(mp + 1)};
+                            const bf16 *m = reinterpret_cast<const bf16 *>(m2);
 #pragma unroll
-                    for (int tp = 0; tp < TR / 2; tp++) {
-                        float pv[16];
-#pragma unroll
-                        for (int i = 0; i < 16; i++) {
-                            const float sum = __bfloat162float(__float2bfloat16_rn(v[2 * tp][i])) +
-                                              __bfloat162float(__float2bfloat16_rn(v[2 * tp + 1][i]));
-                            pv[i] = sum + __shfl_xor_sync(0xffffffffu, sum, 1);
+                            for (int i = 0; i < 16; i++) v[t][i] = __bfloat162float(m[i]) > 0.f ? v[t][i] : 0.f;
                         }
-                        const int yp = y0 + 2 * tp;
-                        if (yp < a.H && x < a.W && (x & 1) == 0) {
+                        if (a.out_f32) {
+                            float4 *o = reinterpret_cast<float4 *>(a.out_f32 + pix * a.f32_cstride + c0);
+#pragma unroll
+                            for (int i = 0; i < 4; i++)
+                                o[i] = make_float4(v[t][4 * i], v[t][4 * i + 1], v[t][4 * i + 2], v[t][4 * i + 3]);
+                        }
+                        if (a.out) {
                             uint4 w2[2];
                             __nv_bfloat162 *w = reinterpret_cast<__nv_bfloat162 *>(w2);
+                            if (a.up2) {
 #pragma unroll
-                            for (int i = 0; i < 8; i++)
-                                w[i] = __floats2bfloat162_rn(0.25f * pv[2 * i], 0.25f * pv[2 * i + 1]);
-                            uint4 *o = reinterpret_cast<uint4 *>(
-                                a.pool_out + (((size_t)b * (a.H / 2) + yp / 2) * (a.W / 2) + x / 2) * a.n_store + c0);
-                            o[0] = w2[0];
-                            o[1] = w2[1];
+                                for (int i = 0; i < 8; i++) w[i] = __floats2bfloat162_rn(v[t][2 * i], v[t][2 * i + 1]);
+#pragma unroll
+                                for (int dy = 0; dy < 2; dy++)
+#pragma unroll
+                                    for (int dx = 0; dx < 2; dx++) {
+                                        uint4 *o = reinterpret_cast<uint4 *>(
+                                            a.out + (((size_t)b * 2 * a.H + 2 * y + dy) * 2 * a.W + 2 * x + dx) * a.out_cstride +
+                                            a.out_coff + c0);
+                                        o[0] = w2[0];
+                                        o[1] = w2[1];
+                                    }
+                            } else {
+                                uint4 *o = reinterpret_cast<uint4 *>(a.out + pix * a.out_cstride + a.out_coff + c0);
+                                if (a.accumulate) {
+                                    const uint4 p2[2] = {o[0], o[1]};
+                                    const bf16 *p = reinterpret_cast<const bf16 *>(p2);
+#pragma unroll
+                                    for (int i = 0; i < 16; i++) v[t][i] += __bfloat162float(p[i]);
+                                }
+#pragma unroll
+                                for (int i = 0; i < 8; i++) w[i] = __floats2bfloat162_rn(v[t][2 * i], v[t][2 * i + 1]);
+                                o[0] = w2[0];
+                                o[1] = w2[1];
+                            }
+                        }
+                    }
+                    if (G >= 2 && a.pool_out) {
+                        // 2x2 average of the stored (bf16-rounded) values: each row pair
+                        // (2 tp, 2 tp + 1) is this thread's, the column pair is this lane and
+                        // its neighbour (tiles start at even rows and columns; H, W even).
+#pragma unroll
+                        for (int tp = 0; tp < G / 2; tp++) {
+                            float pv[16];
+#pragma unroll
+                            for (int i = 0; i < 16; i++) {
+                                const float sum = __bfloat162float(__float2bfloat16_rn(v[2 * tp][i])) +
+                                                  __bfloat162float(__float2bfloat16_rn(v[2 * tp + 1][i]));
+                                pv[i] = sum + __shfl_xor_sync(0xffffffffu, sum, 1);
+                            }
+                            const int yp = y0 + g + 2 * tp;
+                            if (yp < a.H && x < a.W && (x & 1) == 0) {
+                                uint4 w2[2];
+                                __nv_bfloat162 *w = reinterpret_cast<__nv_bfloat162 *>(w2);
+#pragma unroll
+                                for (int i = 0; i < 8; i++)
+                                    w[i] = __floats2bfloat162_rn(0.25f * pv[2 * i], 0.25f * pv[2 * i + 1]);
+                                uint4 *o = reinterpret_cast<uint4 *>(
+                                    a.pool_out + (((size_t)b * (a.H / 2) + yp / 2) * (a.W / 2) + x / 2) * a.n_store + c0);
+                                o[0] = w2[0];
+                                o[1] = w2[1];
+                            }
                         }
                     }
                 }
@@ -494,9 +552,10 @@ __global__ void k_wgrad_reduce(const float *__restrict__ partial, int bands, int
 }
 
 // Packs fp32 master weights W[cout][9][cin] into the bf16 layout a conv stage
-// copies in one piece: [chunk][tap][ck/8][n][8]. Forward: n = output channel,
-// k = input channel. Transposed (backward-data): n = input channel ci0 + n,
-// k = output channel, taps mirrored.
+// copies in one piece: [chunk][tx][ck/8][ty][n][8] with tap = 3 ty + tx, so
+// the three tap rows of a tap column are one K-major operand of 3n rows.
+// Forward: n = output channel, k = input channel. Transposed (backward-data):
+// n = input channel ci0 + n, k = output channel, taps mirrored.
 __global__ void k_pack(const float *__restrict__ w, int cout, int cin, int transpose, int ci0, int n_out, int ck,
                        bf16 *__restrict__ out)
 {
@@ -506,10 +565,12 @@ __global__ void k_pack(const float *__restrict__ w, int cout, int cin, int trans
     if (i >= total) return;
     const int e = i % 8;
     const int n = (i / 8) % n_out;
-    const int rest = i / (8 * n_out);  // (chunk * 9 + tap) * (ck/8) + kcol
-    const int kcol = rest % (ck / 8);
-    const int tap = (rest / (ck / 8)) % 9;
-    const int chunk = rest / ((ck / 8) * 9);
+    const int rest = i / (8 * n_out);  // ((chunk * 3 + tx) * (ck/8) + kcol) * 3 + ty
+    const int ty = rest % 3;
+    const int kcol = (rest / 3) % (ck / 8);
+    const int tx = (rest / (3 * (ck / 8))) % 3;
+    const int chunk = rest / (9 * (ck / 8));
+    const int tap = 3 * ty + tx;
     const int k = chunk * ck + kcol * 8 + e;
     float v;
     if (!transpose)
@@ -674,50 +735,73 @@ __global__ void k_colsum_final(const float *__restrict__ partial, int nblk, int 
 // (y, x) holds the 2x2 cell of samples (2y + dy, 2x + dx) -- channel 2 dy + dx
 // = decoded / 128, channel 4 + 2 dy + dx = the quantisation step of that
 // sample's frequency position / 64, channels 8-15 = 0; cells outside the
-// component are zero. One thread per 8x8 block of the padded block grid
-// (4x4 level-0 pixels).
-__global__ void k_features(const int16_t *__restrict__ coef, int cpitch, long long img_stride, const float *__restrict__ q,
-                           int B, int H, int W, float *__restrict__ dec, bf16 *__restrict__ feat)
+// component are zero. One warp per four 8x8 blocks of a row of the padded
+// block grid (4x4 level-0 pixels each): lane group g = lane / 8 takes block
+// 4 w + g, lane r = lane % 8 its sample row r; the 2-D IDCT runs columns then
+// rows with 8x8 transposes in shared memory (the same operations, in the same
+// order, as idct8x8_regs). Lane r then writes level-0 row r / 2, columns
+// 2 (r % 2) and 2 (r % 2) + 1 of its block, taking the other sample row of
+// each cell from lane r ^ 1.
+__global__ void __launch_bounds__(128) k_features(const int16_t *__restrict__ coef, int cpitch, long long img_stride,
+                                                  const float *__restrict__ q, int B, int H, int W,
+                                                  float *__restrict__ dec, bf16 *__restrict__ feat)
 {
+    __shared__ float s_t[4][4][8][9];
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int bw = W / 8, bh = H / 8;
     const int W0 = (W + 15) / 16 * 8, H0 = (H + 15) / 16 * 8;
     const int pbw = W0 / 4, pbh = H0 / 4;  // padded block grid
-    const long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
-    if (i >= (long long)B * pbw * pbh) return;
-    const int bx = (int)(i % pbw), by = (int)((i / pbw) % pbh), b = (int)(i / ((long long)pbw * pbh));
+    const int gx = (pbw + 3) / 4;          // warps per padded block row
+    const long long wi = blockIdx.x * 4LL + warp;
+    if (wi >= (long long)B * pbh * gx) return;  // warp-uniform
+    const int grp = lane >> 3, r = lane & 7;
+    const int bx = (int)(wi % gx) * 4 + grp, by = (int)((wi / gx) % pbh), b = (int)(wi / ((long long)gx * pbh));
     const bool real = bx < bw && by < bh;
     const float *qt = q + (size_t)b * 64;
-    float a[64];
+    float(*T)[9] = s_t[warp][grp];
+    float a[8];
     if (real) {
-        for (int r = 0; r < 8; r++) {
-            float c8[8];
-            load_coef_row(coef + b * img_stride + (size_t)(by * 8 + r) * cpitch + bx * 8, c8);
+        load_coef_row(coef + b * img_stride + (size_t)(by * 8 + r) * cpitch + bx * 8, a);
 #pragma unroll
-            for (int u = 0; u < 8; u++) a[r * 8 + u] = c8[u] * __ldg(qt + r * 8 + u);
-        }
-        idct8x8_regs(a);
-        for (int r = 0; r < 8; r++) {
-            const size_t p0 = ((size_t)b * H + by * 8 + r) * W + bx * 8;
+        for (int u = 0; u < 8; u++) a[u] *= __ldg(qt + r * 8 + u);
+    } else {
 #pragma unroll
-            for (int u = 0; u < 8; u++) dec[p0 + u] = a[r * 8 + u];
-        }
+        for (int u = 0; u < 8; u++) a[u] = 0.f;
     }
-    for (int yy = 0; yy < 4; yy++)
-        for (int xx = 0; xx < 4; xx++) {
-            uint4 o[2] = {make_uint4(0, 0, 0, 0), make_uint4(0, 0, 0, 0)};
-            if (real) {
-                bf16 *w = reinterpret_cast<bf16 *>(o);
+    transpose8(T, r, a);
+    idct8(a);
+    transpose8(T, r, a);
+    idct8(a);
+    if (real) {
+        float4 *d = reinterpret_cast<float4 *>(dec + ((size_t)b * H + by * 8 + r) * W + bx * 8);
+        d[0] = make_float4(a[0], a[1], a[2], a[3]);
+        d[1] = make_float4(a[4], a[5], a[6], a[7]);
+    }
+    float o8[8];
 #pragma unroll
-                for (int k = 0; k < 4; k++) {
-                    const int r = 2 * yy + (k >> 1), u = 2 * xx + (k & 1);
-                    w[k] = __float2bfloat16_rn(a[r * 8 + u] * (1.f / 128.f));
-                    w[4 + k] = __float2bfloat16_rn(__ldg(qt + r * 8 + u) * (1.f / 64.f));
-                }
+    for (int u = 0; u < 8; u++) o8[u] = __shfl_xor_sync(0xffffffffu, a[u], 1);
+    if (bx >= pbw) return;
+    const int yy = r >> 1, h = r & 1;
+#pragma unroll
+    for (int k2 = 0; k2 < 2; k2++) {
+        const int xx = 2 * h + k2;
+        uint4 o[2] = {make_uint4(0, 0, 0, 0), make_uint4(0, 0, 0, 0)};
+        if (real) {
+            bf16 *w = reinterpret_cast<bf16 *>(o);
+#pragma unroll
+            for (int k = 0; k < 4; k++) {
+                const int dy = k >> 1, dx = k & 1;
+                const int clo = 2 * k2 + dx, chi = 4 + 2 * k2 + dx;  // sample column for h = 0 / 1
+                // Row 2 yy is this lane's for h = 0, its partner's for h = 1.
+                const float v = dy == 0 ? (h ? o8[chi] : a[clo]) : (h ? a[chi] : o8[clo]);
+                w[k] = __float2bfloat16_rn(v * (1.f / 128.f));
+                w[4 + k] = __float2bfloat16_rn(__ldg(qt + (2 * yy + dy) * 8 + 2 * xx + dx) * (1.f / 64.f));
             }
-            uint4 *f = reinterpret_cast<uint4 *>(feat + (((size_t)b * H0 + by * 4 + yy) * W0 + bx * 4 + xx) * 16);
-            f[0] = o[0];
-            f[1] = o[1];
         }
+        uint4 *f = reinterpret_cast<uint4 *>(feat + (((size_t)b * H0 + by * 4 + yy) * W0 + bx * 4 + xx) * 16);
+        f[0] = o[0];
+        f[1] = o[1];
+    }
 }
 
 // Residual head output r (fp32 [B][H0][W0][rstride], channels 0-3 = the 2x2
@@ -876,7 +960,10 @@ PFN_cuTensorMapEncodeTiled_v12000 encode_fn()
 }
 
 // Tensor map over an NHWC bf16 tensor [B][H][W][C] with box {8, bw, bh, 1}.
-bool make_map(CUtensorMap *m, const void *base, int B, int H, int W, int C, int bw, int bh, std::string &err)
+// NHWC bf16 tensor map with boxes of bc channels x bw pixels x bh rows; bc = 8
+// unswizzled, 16 with the 32-byte swizzle, 32 with the 64-byte swizzle.
+bool make_map(CUtensorMap *m, const void *base, int B, int H, int W, int C, int bw, int bh, std::string &err,
+              int bc = 8)
 {
     auto fn = encode_fn();
     if (!fn) {
@@ -889,10 +976,13 @@ bool make_map(CUtensorMap *m, const void *base, int B, int H, int W, int C, int 
     }
     cuuint64_t dims[4] = {(cuuint64_t)C, (cuuint64_t)W, (cuuint64_t)H, (cuuint64_t)B};
     cuuint64_t strides[3] = {(cuuint64_t)C * 2, (cuuint64_t)W * C * 2, (cuuint64_t)H * W * C * 2};
-    cuuint32_t box[4] = {8, (cuuint32_t)bw, (cuuint32_t)bh, 1};
+    cuuint32_t box[4] = {(cuuint32_t)bc, (cuuint32_t)bw, (cuuint32_t)bh, 1};
     cuuint32_t es[4] = {1, 1, 1, 1};
+    const CUtensorMapSwizzle sw = bc == 32 ? CU_TENSOR_MAP_SWIZZLE_64B
+                                  : bc == 16 ? CU_TENSOR_MAP_SWIZZLE_32B
+                                             : CU_TENSOR_MAP_SWIZZLE_NONE;
     const CUresult r = fn(m, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 4, const_cast<void *>(base), dims, strides, box, es,
-                          CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
+                          CU_TENSOR_MAP_INTERLEAVE_NONE, sw,
                           CU_TENSOR_MAP_L2_PROMOTION_L2_128B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
     if (r != CUDA_SUCCESS) {
         err = "cuTensorMapEncodeTiled failed (" + std::to_string((int)r) + ")";
@@ -906,7 +996,7 @@ bool make_map(CUtensorMap *m, const void *base, int B, int H, int W, int C, int 
 void set_smem_attribute_once(const void *fn, int slot)
 {
     static std::mutex mu;
-    static bool done[64][3] = {};
+    static bool done[64][5] = {};
     int dev = 0;
     cudaGetDevice(&dev);
     std::lock_guard<std::mutex> lock(mu);
@@ -940,6 +1030,22 @@ int32_t check_launch(const char *what)
     return ART_OK;
 }
 
+// Output rows per tile when the caller leaves it open. Taller tiles re-read
+// fewer halo rows, reload the chunk's weights for more output rows and give
+// the stacked tap-row MMAs more rows to span; shorter ones give small layers
+// enough tiles to occupy the SMs. Two tiles' accumulators (2 x rows x n
+// columns) fit TMEM's 512. Measured on the network's 1080p layers: 8 rows
+// best or tied for n <= 32 without a pooled output, 4 rows for n <= 64, and
+// for n > 64 one row where 2-row tiles would cover under half the SMs.
+int auto_tile_rows(int B, int H, int W, int n, bool pooled)
+{
+    const long long tiles2 = (long long)B * ((H + 1) / 2) * ((W + TPX - 1) / TPX);
+    if (n <= 32 && !pooled) return 8;
+    if (n <= 64) return 4;
+    if (2 * tiles2 < num_sms() && !pooled) return 1;
+    return 2;
+}
+
 int32_t conv3x3(const ArtCnnConv *d, cudaStream_t s)
 {
     if (!d || !d->x || !d->wpack || !d->err) return fail(ART_ERR_INVALID_ARGUMENT, "conv: null pointer");
@@ -962,15 +1068,17 @@ int32_t conv3x3(const ArtCnnConv *d, cudaStream_t s)
         return fail(ART_ERR_INVALID_ARGUMENT, "conv: pooled output needs even H and W and no mask");
     if (d->up2 && (!d->out || d->accumulate || d->mask))
         return fail(ART_ERR_INVALID_ARGUMENT, "conv: upsampled output needs out, no accumulate and no mask");
-    // Tile height: 4 output rows for narrow layers (n <= 32: their accumulators,
-    // 2 tiles x 4 rows x n columns, fit TMEM's 512 and the halo is re-read for
-    // 1.5x rather than 2x the rows), else 2.
-    const int trows = d->n <= 32 ? 4 : 2;
-    const uint32_t kc = trows == 4 ? HaloCol<4>::STRIDE : HaloCol<2>::STRIDE;
-    const uint32_t kc_tx = trows == 4 ? HaloCol<4>::TX : HaloCol<2>::TX;
+    if (d->tile_rows != 0 && d->tile_rows != 1 && d->tile_rows != 2 && d->tile_rows != 4 && d->tile_rows != 8)
+        return fail(ART_ERR_INVALID_ARGUMENT, "conv: tile_rows must be 0, 1, 2, 4 or 8");
+    if (d->tile_rows * d->n > 256)
+        return fail(ART_ERR_INVALID_ARGUMENT, "conv: tile_rows x n must be at most 256 (TMEM holds 2 tiles' accumulators)");
+    if (d->tile_rows == 1 && d->pool_out)
+        return fail(ART_ERR_INVALID_ARGUMENT, "conv: a pooled output needs 2- or 4-row tiles");
+    const int trows = d->tile_rows ? d->tile_rows : auto_tile_rows(d->B, d->H, d->W, d->n, d->pool_out != nullptr);
     CUtensorMap map;
     std::string err;
-    if (!make_map(&map, d->x, d->B, d->H, d->W, d->cin, HPX, trows + 2, err)) return fail(ART_ERR_CUDA, "conv: " + err);
+    if (!make_map(&map, d->x, d->B, d->H, d->W, d->cin, HPX, trows + 2, err, d->ck))
+        return fail(ART_ERR_CUDA, "conv: " + err);
     ConvArgs a{};
     a.B = d->B;
     a.H = d->H;
@@ -992,21 +1100,27 @@ int32_t conv3x3(const ArtCnnConv *d, cudaStream_t s)
     a.accumulate = d->accumulate;
     a.pool_out = static_cast<bf16 *>(d->pool_out);
     a.up2 = d->up2;
-    a.halo_bytes = (uint32_t)(d->ck / 8) * kc;
-    a.stage_bytes = a.halo_bytes + 18u * d->ck * d->n;
-    a.tx_bytes = (uint32_t)(d->ck / 8) * kc_tx + 18u * d->ck * d->n;
+    a.halo_bytes = halo_bytes(trows, d->ck);
+    a.stage_bytes = (a.halo_bytes + 18u * d->ck * d->n + 1023u) / 1024u * 1024u;
+    a.tx_bytes = halo_rows(trows) * (uint32_t)d->ck * 2u + 18u * d->ck * d->n;
     a.stages = (int)std::min<uint32_t>(MAX_STAGES, SMEM_BUDGET / a.stage_bytes);
     a.err = d->err;
     if (a.stages < 2) return fail(ART_ERR_INVALID_ARGUMENT, "conv: stage does not fit shared memory");
     const uint32_t smem = a.stages * a.stage_bytes + 1024;
     const long long ntiles = (long long)d->B * ((d->H + trows - 1) / trows) * ((d->W + TPX - 1) / TPX);
     const int grid = (int)std::min<long long>(ntiles, num_sms());
-    if (trows == 4) {
+    if (trows == 8) {
+        set_smem_attribute_once(reinterpret_cast<const void *>(k_conv3x3<8>), 4);
+        k_conv3x3<8><<<grid, CONV_THREADS, smem, s>>>(map, a);
+    } else if (trows == 4) {
         set_smem_attribute_once(reinterpret_cast<const void *>(k_conv3x3<4>), 2);
-        k_conv3x3<4><<<grid, THREADS, smem, s>>>(map, a);
+        k_conv3x3<4><<<grid, CONV_THREADS, smem, s>>>(map, a);
+    } else if (trows == 1) {
+        set_smem_attribute_once(reinterpret_cast<const void *>(k_conv3x3<1>), 3);
+        k_conv3x3<1><<<grid, CONV_THREADS, smem, s>>>(map, a);
     } else {
         set_smem_attribute_once(reinterpret_cast<const void *>(k_conv3x3<2>), 0);
-        k_conv3x3<2><<<grid, THREADS, smem, s>>>(map, a);
+        k_conv3x3<2><<<grid, CONV_THREADS, smem, s>>>(map, a);
     }
     return check_launch("k_conv3x3");
 }
@@ -1145,11 +1259,14 @@ int32_t art_cnn_bias_grad(const void *g, int64_t npix, int32_t C, float *workspa
 int32_t art_cnn_features(const int16_t *coef, int32_t cpitch, int64_t img_stride, const float *q, int32_t B,
                          int32_t H, int32_t W, float *dec, void *feat, void *stream)
 {
-    if (!coef || !q || !dec || !feat || H % 8 || W % 8 || cpitch < W || cpitch % 8)
+    if (!coef || !q || !dec || !feat || H % 8 || W % 8 || cpitch < W || cpitch % 8 || img_stride % 8)
         return fail(ART_ERR_INVALID_ARGUMENT, "features: bad arguments");
-    const long long n = (long long)B * ((H + 15) / 16 * 2) * ((W + 15) / 16 * 2);
-    k_features<<<blocks_for(n, 128), 128, 0, static_cast<cudaStream_t>(stream)>>>(coef, cpitch, img_stride, q, B, H, W,
-                                                                                dec, static_cast<bf16 *>(feat));
+    if ((reinterpret_cast<uintptr_t>(coef) | reinterpret_cast<uintptr_t>(dec) | reinterpret_cast<uintptr_t>(feat)) & 15)
+        return fail(ART_ERR_INVALID_ARGUMENT, "features: coef, dec and feat must be 16-byte aligned");
+    // One warp per 4 blocks of a padded block row (ceil(W / 16) * 2 blocks wide).
+    const long long warps = (long long)B * ((H + 15) / 16 * 2) * (((W + 15) / 16 * 2 + 3) / 4);
+    k_features<<<blocks_for(warps * 32, 128), 128, 0, static_cast<cudaStream_t>(stream)>>>(
+        coef, cpitch, img_stride, q, B, H, W, dec, static_cast<bf16 *>(feat));
     return check_launch("k_features");
 }
 

@@ -282,6 +282,8 @@ typedef struct ArtCnnConv {
                        [B][H/2][W/2][n_store]; H and W even */
     int32_t up2;    /* nonzero: `out` is 2H x 2W and each output pixel is stored to its 2x2 cell
                        (nearest upsampling fused into the store; not with accumulate) */
+    int32_t tile_rows; /* output rows per 128-pixel tile: 1, 2, 4 or 8 with tile_rows x n <= 256
+                          (a pooled output needs an even count); 0 picks by layer shape */
 } ArtCnnConv;
 int32_t art_cnn_conv3x3(const ArtCnnConv *desc, void *stream);
 
@@ -302,7 +304,9 @@ typedef struct ArtCnnWgrad {
 int32_t art_cnn_wgrad3x3(const ArtCnnWgrad *desc, void *stream);
 
 /* Pack fp32 weights w[cout][9][cin] into the bf16 stage layout of
- * art_cnn_conv3x3 ([cin/ck][9][ck/8][n][8]). transpose != 0 packs the
+ * art_cnn_conv3x3: [cin/ck][tap column tx][ck/8][tap row ty][n][8] (tap =
+ * 3 ty + tx), so that the three tap rows of one tap column form one operand
+ * of 3n rows. transpose != 0 packs the
  * backward-data weights of input channels [ci0, ci0 + n) (taps mirrored,
  * reduction over cout). */
 int32_t art_cnn_pack_weights(const float *w, int32_t cout, int32_t cin, int32_t transpose, int32_t ci0, int32_t n,
@@ -330,7 +334,8 @@ int32_t art_cnn_bias_grad(const void *g, int64_t npix, int32_t C, float *workspa
  * level, H0 = ceil(H / 16) * 8, W0 = ceil(W / 16) * 8 (space to depth):
  * level-0 pixel (y, x) holds samples (2y + dy, 2x + dx) as channels
  * 2 dy + dx = dec / 128 and 4 + 2 dy + dx = q / 64 (zero outside the image;
- * channels 8-15 zero). */
+ * channels 8-15 zero). coef, dec and feat 16-byte aligned; cpitch and
+ * img_stride multiples of 8. */
 int32_t art_cnn_features(const int16_t *coef, int32_t cpitch, int64_t img_stride, const float *q, int32_t B,
                          int32_t H, int32_t W, float *dec, void *feat, void *stream);
 /* Prediction pred[B][H][W] = dec + 16 r, r the depth-to-space of channels

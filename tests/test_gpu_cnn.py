@@ -56,7 +56,7 @@ def _pack(w, transpose=0, ci0=0, n=None, ck=32):
 
 
 def _conv(x, wpack, cin, ck, n, bias=None, relu=0, mask=None, out=None, out_cstride=None, out_coff=0, f32=None,
-          accumulate=0, pool_out=None, up2=0):
+          accumulate=0, pool_out=None, up2=0, tile_rows=0):
     torch = _torch()
     B, H, W, _ = x.shape
     err = torch.zeros(1, dtype=torch.int32, device="cuda")
@@ -77,6 +77,7 @@ def _conv(x, wpack, cin, ck, n, bias=None, relu=0, mask=None, out=None, out_cstr
     d.err = err.data_ptr()
     d.pool_out = pool_out.data_ptr() if pool_out is not None else None
     d.up2 = up2
+    d.tile_rows = tile_rows
     N.check(N.lib().art_cnn_conv3x3(C.byref(d), None))
     torch.cuda.synchronize()
     assert int(err.item()) == 0, "a pipeline wait timed out"
@@ -91,17 +92,34 @@ def _close(got, ref, rel=1.2e-2):
     assert float(np.abs(got - ref).mean()) <= 1e-3 * scale
 
 
-@pytest.mark.parametrize("B,H,W,cin,cout", [(1, 8, 128, 16, 16), (2, 10, 200, 32, 64), (1, 6, 40, 64, 96),
-                                            (1, 4, 260, 224, 96), (2, 16, 96, 96, 128), (1, 3, 130, 160, 32)])
-def test_conv_forward(gpu, B, H, W, cin, cout):
+CONV_SHAPES = [(1, 8, 128, 16, 16), (2, 10, 200, 32, 64), (1, 6, 40, 64, 96), (1, 4, 260, 224, 96),
+               (2, 16, 96, 96, 128), (1, 3, 130, 160, 32), (1, 7, 1100, 64, 64)]
+
+
+@pytest.mark.parametrize("tile_rows", [0, 1, 2, 4, 8])
+@pytest.mark.parametrize("B,H,W,cin,cout", CONV_SHAPES)
+def test_conv_forward(gpu, B, H, W, cin, cout, tile_rows):
+    """Every tile height (0: the automatic choice) on ragged heights and widths."""
+    if tile_rows * cout > 256:
+        pytest.skip("two tiles' accumulators hold 2 x tile_rows x n TMEM columns: at most 512")
     rng = np.random.default_rng(cin * 7 + cout)
     x = O.bf16(rng.standard_normal((B, H, W, cin)))
     w = O.bf16(rng.standard_normal((cout, 9, cin)) * np.sqrt(2 / (9 * cin)))
     b = rng.standard_normal(cout) * 0.1
     ck = 32 if cin % 32 == 0 else 16
-    got = _np(_conv(_bf(x), _pack(w, ck=ck), cin, ck, cout, bias=_f32(b), relu=1))
+    got = _np(_conv(_bf(x), _pack(w, ck=ck), cin, ck, cout, bias=_f32(b), relu=1, tile_rows=tile_rows))
     ref = O.bf16(np.maximum(O.conv(x, w, b), 0))
     _close(got, ref)
+
+
+def test_conv_rejects_bad_tile_rows(gpu):
+    torch = _torch()
+    x = torch.zeros((1, 4, 16, 16), dtype=torch.bfloat16, device="cuda")
+    wp = torch.zeros(9 * 16 * 96, dtype=torch.bfloat16, device="cuda")
+    pooled = torch.zeros((1, 2, 8, 96), dtype=torch.bfloat16, device="cuda")
+    for kw in ({"tile_rows": 3}, {"tile_rows": 4}, {"tile_rows": 16}, {"tile_rows": 1, "pool_out": pooled}):
+        with pytest.raises(N.ArtError):
+            _conv(x, wp, 16, 16, 96, **kw)
 
 
 def test_conv_channel_offset_accumulate_and_f32(gpu):
@@ -124,10 +142,15 @@ def test_conv_channel_offset_accumulate_and_f32(gpu):
     np.testing.assert_allclose(_np(f), O.conv(x, w), rtol=1e-4, atol=1e-4 * float(np.abs(O.conv(x, w)).max()))
 
 
-@pytest.mark.parametrize("B,H,W,cin,cout", [(1, 8, 130, 16, 32), (2, 6, 64, 64, 96), (1, 4, 40, 96, 128)])
-def test_conv_fused_pool_and_upsample(gpu, B, H, W, cin, cout):
+@pytest.mark.parametrize("tile_rows", [0, 2, 4, 8])
+@pytest.mark.parametrize("B,H,W,cin,cout", [(1, 8, 130, 16, 32), (2, 6, 64, 64, 96), (1, 4, 40, 96, 128),
+                                            (1, 10, 260, 32, 64)])
+def test_conv_fused_pool_and_upsample(gpu, B, H, W, cin, cout, tile_rows):
     """The epilogue's 2x2-pooled output equals pooling the stored activation,
-    and the upsampled store equals nearest upsampling of the plain store."""
+    and the upsampled store equals nearest upsampling of the plain store (the
+    upsampled store also with 1-row tiles)."""
+    if tile_rows * cout > 256:
+        pytest.skip("two tiles' accumulators hold 2 x tile_rows x n TMEM columns: at most 512")
     torch = _torch()
     rng = np.random.default_rng(cin + cout + H)
     x = O.bf16(rng.standard_normal((B, H, W, cin)))
@@ -136,15 +159,17 @@ def test_conv_fused_pool_and_upsample(gpu, B, H, W, cin, cout):
     ck = 32 if cin % 32 == 0 else 16
     wp, xt, bt = _pack(w, ck=ck), _bf(x), _f32(b)
     pooled = torch.zeros((B, H // 2, W // 2, cout), dtype=torch.bfloat16, device="cuda")
-    plain = _conv(xt, wp, cin, ck, cout, bias=bt, relu=1, pool_out=pooled)
+    plain = _conv(xt, wp, cin, ck, cout, bias=bt, relu=1, pool_out=pooled, tile_rows=tile_rows)
     ref = O.bf16(np.maximum(O.conv(x, w, b), 0))
     _close(_np(plain), ref)
     np.testing.assert_array_equal(_np(pooled), O.bf16(O.pool(_np(plain))))
-    big = torch.zeros((B, 2 * H, 2 * W, cout + 16), dtype=torch.bfloat16, device="cuda")
-    _conv(xt, wp, cin, ck, cout, bias=bt, relu=1, out=big, out_cstride=cout + 16, out_coff=16, up2=1)
-    got = _np(big)
-    np.testing.assert_array_equal(got[..., 16:], O.up(_np(plain)))
-    assert np.all(got[..., :16] == 0)
+    for up_rows in ((tile_rows, 1) if tile_rows == 2 else (tile_rows,)):
+        big = torch.zeros((B, 2 * H, 2 * W, cout + 16), dtype=torch.bfloat16, device="cuda")
+        _conv(xt, wp, cin, ck, cout, bias=bt, relu=1, out=big, out_cstride=cout + 16, out_coff=16, up2=1,
+              tile_rows=up_rows)
+        got = _np(big)
+        np.testing.assert_array_equal(got[..., 16:], O.up(_np(plain)))
+        assert np.all(got[..., :16] == 0)
 
 
 def test_conv_backward_data_with_mask(gpu):
@@ -224,6 +249,36 @@ def _batch(seed, B=2, H=64, W=48):
     dec, _ = O.features(coef, q)
     target = (dec + rng.standard_normal(dec.shape) * 3.0).astype(np.float32)
     return coef, q, target
+
+
+@pytest.mark.parametrize("B,H,W", [(1, 8, 8), (2, 40, 56), (1, 64, 48), (3, 24, 136), (1, 136, 72)])
+def test_features_match_oracle(gpu, B, H, W):
+    """art_cnn_features on ragged component sizes (padded block grids whose
+    rows are not a multiple of the 4 blocks one warp takes): the decoded image
+    to fp32 rounding, the quantisation-step channels exactly, zeros in channels
+    8-15 and in cells outside the component (the output starts as garbage)."""
+    torch = _torch()
+    rng = np.random.default_rng(B * 1000 + H * 10 + W)
+    coef = np.zeros((B, H, W), np.int16)
+    for b in range(B):
+        blk = coef[b].reshape(H // 8, 8, W // 8, 8)
+        blk[:, 0, :, 0] = rng.integers(-60, 60, size=(H // 8, W // 8))
+        blk[:, :4, :, :4] += rng.integers(-5, 6, size=(H // 8, 4, W // 8, 4)).astype(np.int16)
+    q = rng.integers(1, 80, size=(B, 64)).astype(np.float32)
+    H0, W0 = O.level0(H, W)
+    coef_d = torch.from_numpy(coef).cuda()
+    q_d = _f32(q)
+    dec_d = torch.full((B, H, W), 7.0, dtype=torch.float32, device="cuda")
+    feat_d = torch.full((B, H0, W0, 16), 3.0, dtype=torch.bfloat16, device="cuda")
+    N.check(N.lib().art_cnn_features(_ptr(coef_d), W, H * W, _ptr(q_d), B, H, W, _ptr(dec_d), _ptr(feat_d), None))
+    torch.cuda.synchronize()
+    dec_ref, F_ref = O.features(coef, q)
+    dec = dec_d.cpu().numpy().astype(np.float64)
+    np.testing.assert_allclose(dec, dec_ref, rtol=0, atol=2e-3)
+    F = _np(feat_d)
+    np.testing.assert_array_equal(F[..., 0:4], O.bf16(O.space_to_depth(dec, H0, W0) / 128.0))
+    np.testing.assert_array_equal(F[..., 4:8], O.bf16(F_ref[..., 4:8]))
+    assert np.all(F[..., 8:] == 0)
 
 
 def test_features_and_prediction(gpu):
