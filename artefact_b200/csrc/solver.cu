@@ -478,10 +478,12 @@ __global__ void __launch_bounds__(SWEEP_WARPS_N * 32, SWEEP_MIN_BLOCKS_N) k_grad
 // DCT-distance gradient (compute_step_prob.rs:20-57) from the clamped
 // coefficients the reference keeps as cos (compute_projection.rs:82).
 // One warp per task {image, channel, block row, first block} covering four
-// blocks. The warp's region of y, g and x (8 SV rows x 32 SH columns) is
-// staged into shared memory with asynchronous 16-byte copies, one round trip;
-// then lane group g = lane / 8 takes block first + g and lane j = lane % 8 its
-// component column j (SH full-resolution columns). The separable 1-D
+// blocks. The warp's region of y and g (8 SV rows x 32 SH columns) is staged
+// into shared memory with asynchronous 16-byte copies, one round trip; once g
+// is consumed (x' = y - sigma g), the same plane receives the region of x,
+// again asynchronously, while the block transforms run. Lane group
+// g = lane / 8 takes block first + g and lane j = lane % 8 its component
+// column j (SH full-resolution columns). The separable 1-D
 // transforms run on columns or rows of the block, switching with 8x8
 // transposes in shared memory, in the reference's order (columns first).
 template <int SH, int SV>
@@ -504,8 +506,8 @@ __global__ void __launch_bounds__(PROJ_WARPS * 32) k_project(const ImgDev *__res
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int w = blockIdx.x * PROJ_WARPS + warp;
     if (w >= ntasks) return;  // warp-uniform
-    float *sy_ = reinterpret_cast<float *>(s_dyn) + warp * 3 * S::REGION;  // y, g, x regions
-    float *sg_ = sy_ + S::REGION, *sx_ = sg_ + S::REGION;
+    float *sy_ = reinterpret_cast<float *>(s_dyn) + warp * 2 * S::REGION;  // y region; g, then x region
+    float *sg_ = sy_ + S::REGION, *sx_ = sg_;
     const int4 tk = tasks[w];
     const ImgDev &im = imgs[tk.x];
     const int c = tk.y, by = tk.z, grp = lane >> 3, j = lane & 7;
@@ -519,20 +521,16 @@ __global__ void __launch_bounds__(PROJ_WARPS * 32) k_project(const ImgDev *__res
     const float *gb = im.g + c * cs;
     // Stage the region: rows of NC floats, 16-byte chunks; chunks of blocks
     // past the end of the block row are skipped.
-    {
-        const int X0 = tk.w * 8 * SH;
-        const int ncol = min(NC, (bw - tk.w) * 8 * SH);  // valid columns, a multiple of 8
-        const long long r0 = (long long)(by * 8 * SV) * pitch + X0;
-        constexpr int CPR = NC / 4;  // 16-byte chunks per row
-        for (int i = lane; i < NR * CPR; i += 32) {
-            const int row = i / CPR, ch = i - row * CPR;
-            if (ch * 4 < ncol) {
-                const long long go = r0 + (long long)row * pitch + ch * 4;
-                const int so = row * RS + ch * 4;
-                cp_async16(sy_ + so, yw + go);
-                cp_async16(sg_ + so, gb + go);
-                cp_async16(sx_ + so, xw + go);
-            }
+    const int ncol = min(NC, (bw - tk.w) * 8 * SH);  // valid columns, a multiple of 8
+    const long long r0 = (long long)(by * 8 * SV) * pitch + tk.w * 8 * SH;
+    constexpr int CPR = NC / 4;  // 16-byte chunks per row
+    for (int i = lane; i < NR * CPR; i += 32) {
+        const int row = i / CPR, ch = i - row * CPR;
+        if (ch * 4 < ncol) {
+            const long long go = r0 + (long long)row * pitch + ch * 4;
+            const int so = row * RS + ch * 4;
+            cp_async16(sy_ + so, yw + go);
+            cp_async16(sg_ + so, gb + go);
         }
     }
     // Meanwhile: coefficient row j of this lane's block and its quantisation steps.
@@ -569,6 +567,12 @@ __global__ void __launch_bounds__(PROJ_WARPS * 32) k_project(const ImgDev *__res
         mean[k] = SUB ? acc / (float)(SH * SV) : acc;
         m[k] = mean[k];
     }
+    // g is consumed: stage x_k into its plane while the transforms run.
+    __syncwarp();
+    for (int i = lane; i < NR * CPR; i += 32) {
+        const int row = i / CPR, ch = i - row * CPR;
+        if (ch * 4 < ncol) cp_async16(sx_ + row * RS + ch * 4, xw + r0 + (long long)row * pitch + ch * 4);
+    }
     // DCT, columns then rows (dct8x8s); the lane then holds coefficient row j.
     dct8(m);
     transpose8(T0, j, m);
@@ -593,6 +597,8 @@ __global__ void __launch_bounds__(PROJ_WARPS * 32) k_project(const ImgDev *__res
     if (ap != 0.f) idct8(d);
     transpose8(T0, j, m);
     if (ap != 0.f) transpose8(T1, j, d);
+    cp_async_wait_all();
+    __syncwarp();
     if (!act) return;
     if (ap != 0.f) {
         float *P = cd.P + by * 8 * cd.ppitch + bx * 8 + j;
@@ -1068,7 +1074,7 @@ std::pair<int, int> pick_sweep(const ArtContext *ctx, const ImageSpec &sp, long 
 template <int SH, int SV>
 constexpr int proj_smem()
 {
-    return PROJ_WARPS * 3 * ProjShape<SH, SV>::REGION * (int)sizeof(float);
+    return PROJ_WARPS * 2 * ProjShape<SH, SV>::REGION * (int)sizeof(float);
 }
 
 // Raises the dynamic shared-memory limit of the projection kernels, once per device.
