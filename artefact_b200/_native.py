@@ -74,7 +74,7 @@ class ArtCnnConv(C.Structure):
         ("mask", C.c_void_p), ("mask_cstride", C.c_int32),
         ("relu", C.c_int32), ("accumulate", C.c_int32),
         ("err", C.c_void_p),
-        ("pool_out", C.c_void_p), ("up2", C.c_int32), ("tile_rows", C.c_int32),
+        ("pool_out", C.c_void_p), ("up2", C.c_int32), ("tile_rows", C.c_int32), ("f32_channels", C.c_int32),
     ]
 
 

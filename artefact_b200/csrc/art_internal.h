@@ -32,6 +32,14 @@ namespace cnn {
 // (a cudaStream_t) without waiting for it.
 int32_t net_predict_async(ArtNet *net, const int16_t *coef, int cpitch, long long img_stride, const float *q, int B,
                           int H, int W, float *pred, void *stream);
+// Allocation and weight packing that a prediction of B x H x W would do,
+// done now (so that a later net_predict_async only launches kernels and can
+// be captured into a CUDA graph).
+int32_t net_prepare(ArtNet *net, int B, int H, int W, void *stream);
+// Process-wide serial of the network's activation buffers: renewed whenever
+// they are (re)allocated, never shared by two networks (a graph holding their
+// addresses is stale once it changes).
+unsigned long long net_generation(const ArtNet *net);
 int net_device(const ArtNet *net);
 // Reads the network's device error flag (synchronous): ART_OK, or an error if
 // one of its bounded tensor-core waits gave up.

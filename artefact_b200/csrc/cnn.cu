@@ -28,6 +28,7 @@
 
 #include <cmath>
 #include <cstdint>
+#include <atomic>
 #include <mutex>
 #include <string>
 
@@ -52,6 +53,7 @@ constexpr int CONV_THREADS = 320;           // convolution: warp 0 loads, warp 1
 constexpr int EPI_THREADS = CONV_THREADS - 64;
 constexpr uint32_t SMEM_BUDGET = 220 * 1024;  // pipeline stages; 1 KB more is requested for alignment
 constexpr int MAX_STAGES = 4;
+constexpr int RSTRIDE = 4;                  // channels per pixel of the head's fp32 residual output
 
 struct ConvArgs {
     int B, H, W;
@@ -62,7 +64,7 @@ struct ConvArgs {
     bf16 *out;
     int out_cstride, out_coff;
     float *out_f32;
-    int f32_cstride;
+    int f32_cstride, f32_n;  // fp32 output: channel stride, channels written (multiple of 4)
     const bf16 *mask;   // optional: zero where mask <= 0 (ReLU backward)
     int mask_cstride;
     int relu, accumulate;
@@ -331,11 +333,12 @@ __global__ void __launch_bounds__(CONV_THREADS, 1) k_conv3x3(const __grid_consta
 #pragma unroll
                             for (int i = 0; i < 16; i++) v[t][i] = __bfloat162float(m[i]) > 0.f ? v[t][i] : 0.f;
                         }
-                        if (a.out_f32) {
+                        if (a.out_f32 && c0 < a.f32_n) {
                             float4 *o = reinterpret_cast<float4 *>(a.out_f32 + pix * a.f32_cstride + c0);
 #pragma unroll
                             for (int i = 0; i < 4; i++)
-                                o[i] = make_float4(v[t][4 * i], v[t][4 * i + 1], v[t][4 * i + 2], v[t][4 * i + 3]);
+                                if (c0 + 4 * i < a.f32_n)
+                                    o[i] = make_float4(v[t][4 * i], v[t][4 * i + 1], v[t][4 * i + 2], v[t][4 * i + 3]);
                         }
                         if (a.out) {
                             uint4 w2[2];
@@ -1058,8 +1061,10 @@ int32_t conv3x3(const ArtCnnConv *d, cudaStream_t s)
     if (!d->out && !d->out_f32) return fail(ART_ERR_INVALID_ARGUMENT, "conv: no output");
     if (d->out && (d->out_cstride % 8 || d->out_coff % 8 || d->out_coff + d->n_store > d->out_cstride))
         return fail(ART_ERR_INVALID_ARGUMENT, "conv: bad output channel stride/offset");
-    if (d->out_f32 && (d->f32_cstride % 4 || d->f32_cstride < d->n_store))
-        return fail(ART_ERR_INVALID_ARGUMENT, "conv: bad fp32 output stride");
+    const int f32_n = d->f32_channels ? d->f32_channels : d->n_store;
+    if (d->out_f32 && (d->f32_channels < 0 || f32_n % 4 || f32_n > d->n_store || d->f32_cstride % 4 ||
+                       d->f32_cstride < f32_n))
+        return fail(ART_ERR_INVALID_ARGUMENT, "conv: bad fp32 output channels or stride");
     if (d->mask && (d->mask_cstride % 8 || d->mask_cstride < d->n_store))
         return fail(ART_ERR_INVALID_ARGUMENT, "conv: bad mask stride");
     if ((long long)d->B * d->H * d->W * (long long)d->cin >= (1LL << 40))
@@ -1094,6 +1099,7 @@ int32_t conv3x3(const ArtCnnConv *d, cudaStream_t s)
     a.out_coff = d->out_coff;
     a.out_f32 = d->out_f32;
     a.f32_cstride = d->f32_cstride;
+    a.f32_n = f32_n;
     a.mask = static_cast<const bf16 *>(d->mask);
     a.mask_cstride = d->mask_cstride;
     a.relu = d->relu;
@@ -1381,6 +1387,7 @@ struct ArtNet {
     art::cnn::Buf feat, dec, cat1, cat2, cat3, p1, p2, p3, e4, d3, d2, d1, r, pred;
     art::cnn::Buf dr, gd1, ge1, gup1, gd2, ge2, gup2, gd3, ge3, gup3, ge4, gp3, gp2, gp1;
     float smooth_weight = 0.f;  // lambda of the training loss's smoothness term (art_net_set_loss)
+    unsigned long long gen = 0;  // process-wide serial, renewed whenever the activation buffers are (re)allocated
     long long cap_px = 0;    // level-0 pixels the activation buffers hold
     long long cap_full = 0;  // full-resolution samples the decoded/prediction buffers hold
     bool cap_train = false;
@@ -1409,7 +1416,7 @@ int32_t net_alloc(ArtNet *net, long long px, long long full, bool train)
         {&net->feat, P0 * 16 * 2}, {&net->dec, PF * 4},       {&net->cat1, P0 * 96 * 2}, {&net->cat2, P1 * 160 * 2},
         {&net->cat3, P2 * 224 * 2}, {&net->p1, P1 * 32 * 2},   {&net->p2, P2 * 64 * 2},   {&net->p3, P3 * 96 * 2},
         {&net->e4, P3 * 128 * 2},  {&net->d3, P2 * 96 * 2},   {&net->d2, P1 * 64 * 2},   {&net->d1, P0 * 32 * 2},
-        {&net->r, P0 * 16 * 4},    {&net->pred, PF * 4},
+        {&net->r, P0 * RSTRIDE * 4}, {&net->pred, PF * 4},
     };
     if (train) {
         std::vector<Req> t = {
@@ -1420,6 +1427,11 @@ int32_t net_alloc(ArtNet *net, long long px, long long full, bool train)
         };
         req.insert(req.end(), t.begin(), t.end());
     }
+    // A process-wide serial, not a per-network count: a network created later
+    // at the same host address must never match a graph recorded with another
+    // network's (freed) buffers.
+    static std::atomic<unsigned long long> serial{0};
+    net->gen = ++serial;
     for (auto &q : req)
         if (!q.b->ensure(q.bytes)) return fail(ART_ERR_CUDA, "network buffers: cudaMalloc failed");
     net->cap_px = px;
@@ -1473,7 +1485,10 @@ int32_t conv(ArtNet *net, int layer, const void *x, int B, int H, int W, void *o
     d.out_cstride = cstride;
     d.out_coff = coff;
     d.out_f32 = out_f32;
-    d.f32_cstride = L.cout;
+    // The fp32 output is the head's: only its first 4 channels (the 2x2 cell
+    // residuals) are used, stored densely.
+    d.f32_cstride = RSTRIDE;
+    d.f32_channels = RSTRIDE;
     d.relu = L.relu;
     d.err = net->errflag.as<int>();
     d.pool_out = pool_out;
@@ -1632,7 +1647,7 @@ int32_t net_predict(ArtNet *net, const int16_t *coef, int cpitch, long long img_
     if (!net->packed) NET_TRY(net_pack(net, false, s));
     NET_TRY(art_cnn_features(coef, cpitch, img_stride, q, B, H, W, net->dec.as<float>(), net->feat.p, s));
     NET_TRY(net_forward(net, B, H0, W0, s, false));
-    return art_cnn_residual(net->r.as<float>(), 16, net->dec.as<float>(), nullptr, B, H, W,
+    return art_cnn_residual(net->r.as<float>(), RSTRIDE, net->dec.as<float>(), nullptr, B, H, W,
                             pred ? pred : net->pred.as<float>(), nullptr, nullptr, 8 * num_sms(), s);
 }
 
@@ -1641,6 +1656,16 @@ int32_t net_predict_async(ArtNet *net, const int16_t *coef, int cpitch, long lon
 {
     return net_predict(net, coef, cpitch, img_stride, q, B, H, W, pred, static_cast<cudaStream_t>(stream));
 }
+
+int32_t net_prepare(ArtNet *net, int B, int H, int W, void *stream)
+{
+    NET_TRY(check_geometry(B, H, W));
+    NET_TRY(net_alloc(net, (long long)B * level0(H) * level0(W), (long long)B * H * W, false));
+    if (!net->packed) NET_TRY(net_pack(net, false, static_cast<cudaStream_t>(stream)));
+    return ART_OK;
+}
+
+unsigned long long net_generation(const ArtNet *net) { return net->gen; }
 
 int net_device(const ArtNet *net) { return net->device; }
 
@@ -1768,7 +1793,7 @@ int32_t art_net_train_step(ArtNet *net, const int16_t *coef, int32_t cpitch, int
     NET_TRY(art_cnn_features(coef, cpitch, img_stride, q, B, H, W, net->dec.as<float>(), net->feat.p, s));
     NET_TRY(net_forward(net, B, H0, W0, s, true));
     const long long npix = (long long)B * H * W;
-    NET_TRY(art_cnn_residual(net->r.as<float>(), 16, net->dec.as<float>(), target, B, H, W, net->pred.as<float>(),
+    NET_TRY(art_cnn_residual(net->r.as<float>(), RSTRIDE, net->dec.as<float>(), target, B, H, W, net->pred.as<float>(),
                              net->dr.p, net->loss_partial.as<float>(), LOSS_BLOCKS, s));
     if (net->smooth_weight > 0.f) {
         k_residual_smooth_grad<<<LOSS_BLOCKS, 256, 0, s>>>(net->pred.as<float>(), target, B, H, W, net->smooth_weight,

@@ -1007,6 +1007,10 @@ struct ArtContext {
     cudaEvent_t fork = nullptr, join = nullptr;
     art::DevBuf xbuf, pbuf, coefimg, stage, misc, desc, work, tasks, compat, sepplanes, rgb, pred;
     ArtNet *net = nullptr;            // warm-start network for ART_INIT_LEARNED (not owned)
+    // The learned start's launches (network, upsampling, zero-step projection)
+    // as a graph: captured the second time one key is seen, then replayed.
+    cudaGraphExec_t init_exec = nullptr;
+    std::vector<unsigned long long> init_key, init_seen;
     bool net_used = false;            // the last solve ran the network (its error flag is checked)
     std::vector<art::ImgDev> h_desc;  // per image (pageable: copies of it are staged)
     std::vector<std::array<float, 4>> h_weights;  // per image: weight, pweight[3]
@@ -1014,6 +1018,7 @@ struct ArtContext {
     std::vector<int2> h_work;         // sweep blocks {image, block in image}, grouped by variant and channel count
     int wstart[2][4] = {}, wcount[2][4] = {};  // by sweep variant (0 narrow, 1 wide) and channel count
     std::vector<int4> h_tasks;        // block warps {image, channel, block row, first block}
+    std::vector<long long> geo_key;   // geometry h_work / h_tasks (and their device copies) were built for
     int mode_off[5] = {0, 0, 0, 0, 0};  // h_tasks grouped by sampling mode (1x1, 2x2, 2x1, 1x2)
     unsigned *errflag = nullptr;
     cudaGraphExec_t exec = nullptr;
@@ -1266,6 +1271,16 @@ static int prepare_batch(ArtContext *ctx, const std::vector<ImageSpec> &specs, u
     float *xb = static_cast<float *>(ctx->xbuf.p);
     char *misc = static_cast<char *>(ctx->misc.p);
     ctx->errflag = reinterpret_cast<unsigned *>(misc);
+    // The sweep blocks and projection tasks depend on the geometry alone: a
+    // solve with the geometry of the previous one reuses them (host lists and
+    // device copies) instead of rebuilding and uploading ~16 B per 4 blocks.
+    std::vector<long long> geo = {nimg};
+    for (int i = 0; i < nimg; i++) {
+        const ImgDev &d = ctx->h_desc[i];
+        geo.insert(geo.end(), {d.W, d.H, d.nch, d.sweep_kind, d.strip_rows});
+        for (int c = 0; c < d.nch; c++) geo.insert(geo.end(), {d.ch[c].cw, d.ch[c].chh, d.ch[c].sh, d.ch[c].sv});
+    }
+    const bool same_geo = geo == ctx->geo_key && ctx->work.p && ctx->tasks.p;
     std::vector<int2> wk[2][4];
     std::vector<int4> per_mode[4];
     for (int i = 0; i < nimg; i++) {
@@ -1280,30 +1295,35 @@ static int prepare_batch(ArtContext *ctx, const std::vector<ImageSpec> &specs, u
             d.ch[c].coef = reinterpret_cast<const int16_t *>(static_cast<char *>(ctx->coefimg.p) + o_coef[i][c]);
             d.ch[c].P = static_cast<float *>(ctx->pbuf.p) + o_p[i][c];
         }
+        if (same_geo) continue;
         for (int b = 0; b < d.ncta; b++) wk[d.sweep_kind][d.nch].push_back(make_int2(i, b));
         build_tasks(d, i, per_mode);
     }
-    ctx->h_work.clear();
-    for (int kd = 0; kd < 2; kd++)
-        for (int n = 3; n >= 1; n--) {
-            ctx->wstart[kd][n] = (int)ctx->h_work.size();
-            ctx->wcount[kd][n] = (int)wk[kd][n].size();
-            ctx->h_work.insert(ctx->h_work.end(), wk[kd][n].begin(), wk[kd][n].end());
-        }
-    ctx->h_tasks.clear();
-    for (int m = 0; m < 4; m++) {
-        ctx->mode_off[m] = (int)ctx->h_tasks.size();
-        ctx->h_tasks.insert(ctx->h_tasks.end(), per_mode[m].begin(), per_mode[m].end());
-    }
-    ctx->mode_off[4] = (int)ctx->h_tasks.size();
-    const int nwork = (int)ctx->h_work.size(), ntasks = (int)ctx->h_tasks.size();
-    if ((rc = ctx->work.ensure(nwork * sizeof(int2)))) return rc;
-    if ((rc = ctx->tasks.ensure(ntasks * sizeof(int4)))) return rc;
-
     cudaStream_t s = ctx->stream;
+    if (!same_geo) {
+        ctx->geo_key.clear();
+        ctx->h_work.clear();
+        for (int kd = 0; kd < 2; kd++)
+            for (int n = 3; n >= 1; n--) {
+                ctx->wstart[kd][n] = (int)ctx->h_work.size();
+                ctx->wcount[kd][n] = (int)wk[kd][n].size();
+                ctx->h_work.insert(ctx->h_work.end(), wk[kd][n].begin(), wk[kd][n].end());
+            }
+        ctx->h_tasks.clear();
+        for (int m = 0; m < 4; m++) {
+            ctx->mode_off[m] = (int)ctx->h_tasks.size();
+            ctx->h_tasks.insert(ctx->h_tasks.end(), per_mode[m].begin(), per_mode[m].end());
+        }
+        ctx->mode_off[4] = (int)ctx->h_tasks.size();
+        const int nwork = (int)ctx->h_work.size(), ntasks = (int)ctx->h_tasks.size();
+        if ((rc = ctx->work.ensure(nwork * sizeof(int2)))) return rc;
+        if ((rc = ctx->tasks.ensure(ntasks * sizeof(int4)))) return rc;
+        ART_CUDA(cudaMemcpyAsync(ctx->work.p, ctx->h_work.data(), nwork * sizeof(int2), cudaMemcpyHostToDevice, s));
+        ART_CUDA(cudaMemcpyAsync(ctx->tasks.p, ctx->h_tasks.data(), ntasks * sizeof(int4), cudaMemcpyHostToDevice, s));
+        ctx->geo_key = geo;
+    }
+    const int ntasks = (int)ctx->h_tasks.size();
     ART_CUDA(cudaMemcpyAsync(ctx->desc.p, ctx->h_desc.data(), nimg * sizeof(ImgDev), cudaMemcpyHostToDevice, s));
-    ART_CUDA(cudaMemcpyAsync(ctx->work.p, ctx->h_work.data(), nwork * sizeof(int2), cudaMemcpyHostToDevice, s));
-    ART_CUDA(cudaMemcpyAsync(ctx->tasks.p, ctx->h_tasks.data(), ntasks * sizeof(int4), cudaMemcpyHostToDevice, s));
     ART_CUDA(cudaMemsetAsync(ctx->misc.p, 0, misc_bytes, s));
     // The first DCT-distance gradient is zero: the reference starts from cos = c q (coef.rs:94-104).
     ART_CUDA(cudaMemsetAsync(ctx->pbuf.p, 0, p_floats * sizeof(float), s));
@@ -1351,30 +1371,95 @@ static int prepare_batch(ArtContext *ctx, const std::vector<ImageSpec> &specs, u
         }
         if ((rc = ctx->pred.ensure(need * sizeof(float)))) return rc;
         float *pred = static_cast<float *>(ctx->pred.p);
+        // Components of one size (the two chroma planes of 4:2:0 or 4:2:2) go
+        // through the network as one batch: their coefficient images lie a
+        // fixed distance apart and their quantisation tables are consecutive
+        // in the descriptor.
+        struct Group {
+            int i, c, nb;
+            long long stride;
+        };
+        std::vector<Group> groups;
         for (int i = 0; i < nimg; i++) {
             const ImgDev &d = ctx->h_desc[i];
             for (int c = 0; c < d.nch;) {
-                // Components of one size (the two chroma planes of 4:2:0 or
-                // 4:2:2) go through the network as one batch: their coefficient
-                // images lie a fixed distance apart and their quantisation
-                // tables are consecutive in the descriptor.
                 const ChanDev &cd = d.ch[c];
                 const long long stride = c + 1 < d.nch ? (long long)(d.ch[c + 1].coef - cd.coef) : 0;
                 int nb = 1;
                 while (c + nb < d.nch && d.ch[c + nb].cw == cd.cw && d.ch[c + nb].chh == cd.chh &&
                        d.ch[c + nb].cpitch == cd.cpitch && d.ch[c + nb].coef - d.ch[c + nb - 1].coef == stride)
                     nb++;
-                rc = cnn::net_predict_async(ctx->net, cd.coef, cd.cpitch, stride, &ddesc[i].q[c][0], nb, cd.chh, cd.cw,
-                                            pred, s);
-                if (rc) return rc;
-                for (int k = 0; k < nb; k++)
-                    k_upsample<<<(int)(((long long)d.W * d.H + 255) / 256), 256, 0, s>>>(
-                        pred + (size_t)k * cd.cw * cd.chh, ddesc + i, c + k);
+                groups.push_back({i, c, nb, stride});
+                if ((rc = cnn::net_prepare(ctx->net, nb, cd.chh, cd.cw, s))) return rc;
                 c += nb;
             }
-            ART_CUDA(cudaMemsetAsync(d.g, 0, (size_t)d.nch * d.cstride * sizeof(float), s));
         }
-        launch_projections(ctx, 0.0f);
+        // Everything the launches below bake in: buffers, geometry, tasks.
+        std::vector<unsigned long long> key = {
+            (unsigned long long)(uintptr_t)ctx->net, cnn::net_generation(ctx->net), (uintptr_t)ctx->desc.p,
+            (uintptr_t)ctx->tasks.p, (uintptr_t)pred, (uintptr_t)ctx->xbuf.p, (uintptr_t)ctx->coefimg.p,
+            (unsigned long long)nimg};
+        for (int m = 0; m < 5; m++) key.push_back((unsigned long long)ctx->mode_off[m]);
+        for (int i = 0; i < nimg; i++) {
+            const ImgDev &d = ctx->h_desc[i];
+            key.insert(key.end(), {(unsigned long long)d.W, (unsigned long long)d.H, (unsigned long long)d.nch,
+                                   (unsigned long long)d.cstride, (uintptr_t)d.g});
+            for (int c = 0; c < d.nch; c++)
+                key.insert(key.end(), {(unsigned long long)d.ch[c].cw, (unsigned long long)d.ch[c].chh,
+                                       (unsigned long long)d.ch[c].cpitch, (uintptr_t)d.ch[c].coef});
+        }
+        // Prediction per component at its own resolution, repeated to full
+        // resolution into x and y, then one projection with a zero step
+        // (g = 0, sigma = 0): x_0 = y_0 = P(prediction), and the DCT-distance
+        // plane of the projected prediction for the first gradient.
+        auto launch_init = [&]() -> int {
+            for (const Group &gr : groups) {
+                const ImgDev &d = ctx->h_desc[gr.i];
+                const ChanDev &cd = d.ch[gr.c];
+                const int r = cnn::net_predict_async(ctx->net, cd.coef, cd.cpitch, gr.stride, &ddesc[gr.i].q[gr.c][0],
+                                                     gr.nb, cd.chh, cd.cw, pred, s);
+                if (r) return r;
+                for (int k = 0; k < gr.nb; k++)
+                    k_upsample<<<(int)(((long long)d.W * d.H + 255) / 256), 256, 0, s>>>(
+                        pred + (size_t)k * cd.cw * cd.chh, ddesc + gr.i, gr.c + k);
+            }
+            for (int i = 0; i < nimg; i++) {
+                const ImgDev &d = ctx->h_desc[i];
+                ART_CUDA(cudaMemsetAsync(d.g, 0, (size_t)d.nch * d.cstride * sizeof(float), s));
+            }
+            launch_projections(ctx, 0.0f);
+            ART_CUDA(cudaGetLastError());
+            return ART_OK;
+        };
+        if (ctx->init_exec && key == ctx->init_key) {
+            ART_CUDA(cudaGraphLaunch(ctx->init_exec, s));
+        } else if (key == ctx->init_seen) {
+            if (ctx->init_exec) {
+                cudaGraphExecDestroy(ctx->init_exec);
+                ctx->init_exec = nullptr;
+            }
+            ctx->init_key.clear();
+            cudaGraph_t graph = nullptr;
+            ART_CUDA(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
+            const int r = launch_init();
+            const cudaError_t ce = cudaStreamEndCapture(s, &graph);
+            if (r) {
+                if (graph) cudaGraphDestroy(graph);
+                return r;
+            }
+            if (ce != cudaSuccess) return fail(ART_ERR_CUDA, std::string("learned start capture: ") + cudaGetErrorString(ce));
+            const cudaError_t ie = cudaGraphInstantiate(&ctx->init_exec, graph, 0);
+            cudaGraphDestroy(graph);
+            if (ie != cudaSuccess) {
+                ctx->init_exec = nullptr;
+                return fail(ART_ERR_CUDA, std::string("learned start graph: ") + cudaGetErrorString(ie));
+            }
+            ctx->init_key = key;
+            ART_CUDA(cudaGraphLaunch(ctx->init_exec, s));
+        } else {
+            if ((rc = launch_init())) return rc;
+            ctx->init_seen = key;
+        }
         ctx->net_used = true;
     } else {
         k_init<<<(ntasks + PROJ_WARPS - 1) / PROJ_WARPS, PROJ_WARPS * 32, 0, s>>>(
@@ -1561,6 +1646,7 @@ void art_context_destroy(ArtContext *ctx)
     cudaSetDevice(ctx->device);
     if (ctx->stream) cudaStreamSynchronize(ctx->stream);
     if (ctx->exec) cudaGraphExecDestroy(ctx->exec);
+    if (ctx->init_exec) cudaGraphExecDestroy(ctx->init_exec);
     for (auto e : ctx->events) cudaEventDestroy(e);
     ctx->xbuf.release();
     ctx->pbuf.release();

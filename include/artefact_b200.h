@@ -284,6 +284,8 @@ typedef struct ArtCnnConv {
                        (nearest upsampling fused into the store; not with accumulate) */
     int32_t tile_rows; /* output rows per 128-pixel tile: 1, 2, 4 or 8 with tile_rows x n <= 256
                           (a pooled output needs an even count); 0 picks by layer shape */
+    int32_t f32_channels; /* channels 0 .. f32_channels-1 go to out_f32: a multiple of 4 up to n_store;
+                             0 = n_store */
 } ArtCnnConv;
 int32_t art_cnn_conv3x3(const ArtCnnConv *desc, void *stream);
 

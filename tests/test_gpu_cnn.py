@@ -56,7 +56,7 @@ def _pack(w, transpose=0, ci0=0, n=None, ck=32):
 
 
 def _conv(x, wpack, cin, ck, n, bias=None, relu=0, mask=None, out=None, out_cstride=None, out_coff=0, f32=None,
-          accumulate=0, pool_out=None, up2=0, tile_rows=0):
+          accumulate=0, pool_out=None, up2=0, tile_rows=0, f32_channels=0):
     torch = _torch()
     B, H, W, _ = x.shape
     err = torch.zeros(1, dtype=torch.int32, device="cuda")
@@ -70,7 +70,8 @@ def _conv(x, wpack, cin, ck, n, bias=None, relu=0, mask=None, out=None, out_cstr
     d.out_cstride = out_cstride if out_cstride is not None else n
     d.out_coff = out_coff
     d.out_f32 = f32.data_ptr() if f32 is not None else None
-    d.f32_cstride = n
+    d.f32_cstride = f32_channels or n
+    d.f32_channels = f32_channels
     d.mask = mask.data_ptr() if mask is not None else None
     d.mask_cstride = mask.shape[-1] if mask is not None else 0
     d.relu, d.accumulate = relu, accumulate
@@ -140,6 +141,18 @@ def test_conv_channel_offset_accumulate_and_f32(gpu):
     f = torch.zeros((B, H, W, cout), dtype=torch.float32, device="cuda")
     _conv(_bf(x), wp, cin, 32, cout, f32=f)
     np.testing.assert_allclose(_np(f), O.conv(x, w), rtol=1e-4, atol=1e-4 * float(np.abs(O.conv(x, w)).max()))
+    # Only the first f32_channels channels, densely (stride f32_channels); the
+    # buffer's tail past B H W x 4 floats stays untouched.
+    f4 = torch.full((B * H * W * 4 + 64,), 5.0, dtype=torch.float32, device="cuda")
+    for tr in (0, 1, 2, 4, 8):
+        _conv(_bf(x), wp, cin, 32, cout, f32=f4, f32_channels=4, tile_rows=tr)
+        got4 = f4[:B * H * W * 4].reshape(B, H, W, 4).cpu().numpy().astype(np.float64)
+        np.testing.assert_allclose(got4, O.conv(x, w)[..., :4], rtol=1e-4,
+                                   atol=1e-4 * float(np.abs(O.conv(x, w)).max()))
+        assert np.all(f4[B * H * W * 4:].cpu().numpy() == 5.0)
+    for bad in (6, 48, -4):
+        with pytest.raises(N.ArtError):
+            _conv(_bf(x), wp, cin, 32, cout, f32=f4, f32_channels=bad)
 
 
 @pytest.mark.parametrize("tile_rows", [0, 2, 4, 8])

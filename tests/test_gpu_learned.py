@@ -142,6 +142,68 @@ def test_zero_residual_start_equals_decoded_start(gpu, ctx, shape):
     assert d <= 1e-2, d
 
 
+def test_learned_start_graph_replay(gpu):
+    """The learned start runs eagerly the first time a geometry is seen, is
+    captured into a CUDA graph the second time and replayed after that. Every
+    run gives the same planes, across a change of geometry, and after a
+    training step changes the weights (and reallocates the network's buffers)
+    the replayed context agrees with a fresh one."""
+    import torch
+
+    c = Context(0)
+    fresh = Context(0)
+    net = WS.WarmStartNet(_strong_params(11))
+    try:
+        c.set_warm_start(net)
+        fresh.set_warm_start(net)
+
+        def run(ctx_, j):
+            W, H, _ = j.max_rounded()
+            return ctx_.compute(j.nchannel, j.coefs, WEIGHT, PW, 6, W, H, init_mode=N.ART_INIT_LEARNED,
+                                step_iterations=2, tail_iterations=2, tail_step_iterations=100)
+
+        def same(a, b):
+            return all(np.array_equal(x, y) for x, y in zip(a, b))
+
+        ja, jb = jpeg_of(*CASES[3]), jpeg_of(*CASES[1])
+        ref_a = run(c, ja)
+        for _ in range(3):  # captured, then replayed
+            assert same(run(c, ja), ref_a)
+        ref_b = run(c, jb)
+        assert same(run(c, jb), ref_b) and same(run(c, jb), ref_b)
+        assert same(run(c, ja), ref_a) and same(run(c, ja), ref_a)
+        # A training step: new weights (repacked before the next prediction).
+        jt = jpeg_of(256, 256, 50, "4:4:4", True, seed=3)
+        co = jt.coefs[0]
+        coef = torch.from_numpy(WS.coef_image(co)[None]).cuda()
+        q = torch.from_numpy(np.asarray(co.quant_table, np.float32)[None].copy()).cuda()
+        target = net.predict_decoded(coef, q) + 1.0
+        net.train_step(coef, q, target, lr=1e-3)
+        got = [run(c, ja) for _ in range(3)]
+        want = run(fresh, ja)
+        assert not same(want, ref_a)
+        assert all(same(g, want) for g in got)
+        # Another network in place of the first (often at the same host
+        # address once the first is freed): the graph recorded with the first
+        # network's buffers must not be replayed.
+        for seed in (13, 14):
+            c.set_warm_start(None)
+            fresh.set_warm_start(None)
+            net.close()
+            net = WS.WarmStartNet(_strong_params(seed))
+            c.set_warm_start(net)
+            fresh.set_warm_start(net)
+            got = [run(c, ja) for _ in range(3)]
+            want = run(fresh, ja)
+            assert all(same(g, want) for g in got)
+    finally:
+        c.set_warm_start(None)
+        fresh.set_warm_start(None)
+        c.close()
+        fresh.close()
+        net.close()
+
+
 def test_learned_start_needs_a_network(gpu, ctx):
     j = jpeg_of(*CASES[0])
     W, H, _ = j.max_rounded()
