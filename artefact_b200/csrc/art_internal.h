@@ -29,17 +29,19 @@ void set_error(const std::string &msg);
 namespace cnn {
 // Warm-start prediction for the solver: features + forward + residual of B
 // coefficient images into pred (dense [B][H][W] floats), queued on `stream`
-// (a cudaStream_t) without waiting for it.
-int32_t net_predict_async(ArtNet *net, const int16_t *coef, int cpitch, long long img_stride, const float *q, int B,
-                          int H, int W, float *pred, void *stream);
-// Allocation and weight packing that a prediction of B x H x W would do,
-// done now (so that a later net_predict_async only launches kernels and can
-// be captured into a CUDA graph).
-int32_t net_prepare(ArtNet *net, int B, int H, int W, void *stream);
-// Process-wide serial of the network's activation buffers: renewed whenever
-// they are (re)allocated, never shared by two networks (a graph holding their
+// (a cudaStream_t) without waiting for it. `slot` (0 or 1) picks one of the
+// network's two activation sets: predictions on different sets may run on
+// two streams at once.
+int32_t net_predict_async(ArtNet *net, int slot, const int16_t *coef, int cpitch, long long img_stride, const float *q,
+                          int B, int H, int W, float *pred, void *stream);
+// Allocation and weight packing that a prediction of B x H x W on activation
+// set `slot` would do, done now (so that a later net_predict_async only
+// launches kernels and can be captured into a CUDA graph).
+int32_t net_prepare(ArtNet *net, int slot, int B, int H, int W, void *stream);
+// Process-wide serial of activation set `slot`: renewed whenever its buffers
+// are (re)allocated, never shared by two networks (a graph holding their
 // addresses is stale once it changes).
-unsigned long long net_generation(const ArtNet *net);
+unsigned long long net_generation(const ArtNet *net, int slot);
 int net_device(const ArtNet *net);
 // Reads the network's device error flag (synchronous): ART_OK, or an error if
 // one of its bounded tensor-core waits gave up.

@@ -1374,6 +1374,21 @@ struct Buf {
 }  // namespace cnn
 }  // namespace art
 
+namespace art {
+namespace cnn {
+// One set of forward activations. A network holds two, so that two
+// predictions (e.g. the luma and the chroma planes of one image) can run on
+// two streams at once; training uses set 0 (its gradients live in ArtNet).
+struct NetActs {
+    Buf feat, dec, cat1, cat2, cat3, p1, p2, p3, e4, d3, d2, d1, r, pred;
+    unsigned long long gen = 0;  // process-wide serial, renewed whenever these buffers are (re)allocated
+    long long cap_px = 0;        // level-0 pixels the activation buffers hold
+    long long cap_full = 0;      // full-resolution samples the decoded/prediction buffers hold
+};
+constexpr int NSLOT = 2;
+}  // namespace cnn
+}  // namespace art
+
 struct ArtNet {
     int device = 0;
     long long nparam = 0;
@@ -1383,14 +1398,11 @@ struct ArtNet {
     art::cnn::Buf wf[art::cnn::NLAYER];     // forward packs
     art::cnn::Buf wb[art::cnn::NLAYER][2];  // backward-data packs (skip part, upsampled part or whole input)
     bool packed = false;
-    // activations (forward) and gradients (training)
-    art::cnn::Buf feat, dec, cat1, cat2, cat3, p1, p2, p3, e4, d3, d2, d1, r, pred;
+    art::cnn::NetActs act[art::cnn::NSLOT];  // forward activations
+    // gradients (training, with activation set 0)
     art::cnn::Buf dr, gd1, ge1, gup1, gd2, ge2, gup2, gd3, ge3, gup3, ge4, gp3, gp2, gp1;
     float smooth_weight = 0.f;  // lambda of the training loss's smoothness term (art_net_set_loss)
-    unsigned long long gen = 0;  // process-wide serial, renewed whenever the activation buffers are (re)allocated
-    long long cap_px = 0;    // level-0 pixels the activation buffers hold
-    long long cap_full = 0;  // full-resolution samples the decoded/prediction buffers hold
-    bool cap_train = false;
+    bool cap_train = false;     // the gradient buffers match act[0]
 };
 
 namespace art {
@@ -1399,24 +1411,27 @@ namespace cnn {
 constexpr int LOSS_BLOCKS = 296;
 constexpr size_t WORKSPACE_BYTES = 64ull << 20;
 
-// Buffers for px level-0 pixels (activations) and full full-resolution
-// samples (decoded image, prediction).
-int32_t net_alloc(ArtNet *net, long long px, long long full, bool train)
+// Activation set `slot` for px level-0 pixels and full full-resolution
+// samples (decoded image, prediction); with train, also the gradient
+// buffers (slot 0 only).
+int32_t net_alloc(ArtNet *net, int slot, long long px, long long full, bool train)
 {
-    if (px <= net->cap_px && full <= net->cap_full && (!train || net->cap_train)) return ART_OK;
-    px = std::max(px, net->cap_px);
-    full = std::max(full, net->cap_full);
-    train = train || net->cap_train;
+    if (slot < 0 || slot >= NSLOT || (train && slot != 0)) return fail(ART_ERR_INVALID_ARGUMENT, "network: bad activation set");
+    NetActs &A = net->act[slot];
+    if (px <= A.cap_px && full <= A.cap_full && (!train || net->cap_train)) return ART_OK;
+    px = std::max(px, A.cap_px);
+    full = std::max(full, A.cap_full);
+    train = train || (slot == 0 && net->cap_train);
     const size_t P0 = (size_t)px, P1 = P0 / 4 + 64, P2 = P0 / 16 + 64, P3 = P0 / 64 + 64, PF = (size_t)full;
     struct Req {
         Buf *b;
         size_t bytes;
     };
     std::vector<Req> req = {
-        {&net->feat, P0 * 16 * 2}, {&net->dec, PF * 4},       {&net->cat1, P0 * 96 * 2}, {&net->cat2, P1 * 160 * 2},
-        {&net->cat3, P2 * 224 * 2}, {&net->p1, P1 * 32 * 2},   {&net->p2, P2 * 64 * 2},   {&net->p3, P3 * 96 * 2},
-        {&net->e4, P3 * 128 * 2},  {&net->d3, P2 * 96 * 2},   {&net->d2, P1 * 64 * 2},   {&net->d1, P0 * 32 * 2},
-        {&net->r, P0 * RSTRIDE * 4}, {&net->pred, PF * 4},
+        {&A.feat, P0 * 16 * 2}, {&A.dec, PF * 4},       {&A.cat1, P0 * 96 * 2}, {&A.cat2, P1 * 160 * 2},
+        {&A.cat3, P2 * 224 * 2}, {&A.p1, P1 * 32 * 2},   {&A.p2, P2 * 64 * 2},   {&A.p3, P3 * 96 * 2},
+        {&A.e4, P3 * 128 * 2},  {&A.d3, P2 * 96 * 2},   {&A.d2, P1 * 64 * 2},   {&A.d1, P0 * 32 * 2},
+        {&A.r, P0 * RSTRIDE * 4}, {&A.pred, PF * 4},
     };
     if (train) {
         std::vector<Req> t = {
@@ -1431,12 +1446,12 @@ int32_t net_alloc(ArtNet *net, long long px, long long full, bool train)
     // at the same host address must never match a graph recorded with another
     // network's (freed) buffers.
     static std::atomic<unsigned long long> serial{0};
-    net->gen = ++serial;
+    A.gen = ++serial;
     for (auto &q : req)
         if (!q.b->ensure(q.bytes)) return fail(ART_ERR_CUDA, "network buffers: cudaMalloc failed");
-    net->cap_px = px;
-    net->cap_full = full;
-    net->cap_train = train;
+    A.cap_px = px;
+    A.cap_full = full;
+    if (slot == 0) net->cap_train = train;
     return ART_OK;
 }
 
@@ -1553,64 +1568,65 @@ int32_t wgrad(ArtNet *net, int layer, const void *x, const void *g, int B, int H
 // their pooled outputs. For inference the e4/d3/d2 convolutions store their
 // outputs upsampled straight into the next concatenation; training keeps
 // them whole (the backward pass reads them as ReLU masks) and upsamples after.
-int32_t net_forward(ArtNet *net, int B, int H, int W, cudaStream_t s, bool train)
+int32_t net_forward(ArtNet *net, NetActs &A, int B, int H, int W, cudaStream_t s, bool train)
 {
     const int H1 = H / 2, W1 = W / 2, H2 = H / 4, W2 = W / 4, H3 = H / 8, W3 = W / 8;
-    NET_TRY(conv(net, E1, net->feat.p, B, H, W, net->cat1.p, 96, 0, nullptr, s, net->p1.p));
-    NET_TRY(conv(net, E2, net->p1.p, B, H1, W1, net->cat2.p, 160, 0, nullptr, s, net->p2.p));
-    NET_TRY(conv(net, E3, net->p2.p, B, H2, W2, net->cat3.p, 224, 0, nullptr, s, net->p3.p));
+    NET_TRY(conv(net, E1, A.feat.p, B, H, W, A.cat1.p, 96, 0, nullptr, s, A.p1.p));
+    NET_TRY(conv(net, E2, A.p1.p, B, H1, W1, A.cat2.p, 160, 0, nullptr, s, A.p2.p));
+    NET_TRY(conv(net, E3, A.p2.p, B, H2, W2, A.cat3.p, 224, 0, nullptr, s, A.p3.p));
     if (train) {
-        NET_TRY(conv(net, E4, net->p3.p, B, H3, W3, net->e4.p, 128, 0, nullptr, s));
-        NET_TRY(art_cnn_upsample2(net->e4.p, B, H2, W2, 128, net->cat3.p, 224, 96, s));
-        NET_TRY(conv(net, D3, net->cat3.p, B, H2, W2, net->d3.p, 96, 0, nullptr, s));
-        NET_TRY(art_cnn_upsample2(net->d3.p, B, H1, W1, 96, net->cat2.p, 160, 64, s));
-        NET_TRY(conv(net, D2, net->cat2.p, B, H1, W1, net->d2.p, 64, 0, nullptr, s));
-        NET_TRY(art_cnn_upsample2(net->d2.p, B, H, W, 64, net->cat1.p, 96, 32, s));
+        NET_TRY(conv(net, E4, A.p3.p, B, H3, W3, A.e4.p, 128, 0, nullptr, s));
+        NET_TRY(art_cnn_upsample2(A.e4.p, B, H2, W2, 128, A.cat3.p, 224, 96, s));
+        NET_TRY(conv(net, D3, A.cat3.p, B, H2, W2, A.d3.p, 96, 0, nullptr, s));
+        NET_TRY(art_cnn_upsample2(A.d3.p, B, H1, W1, 96, A.cat2.p, 160, 64, s));
+        NET_TRY(conv(net, D2, A.cat2.p, B, H1, W1, A.d2.p, 64, 0, nullptr, s));
+        NET_TRY(art_cnn_upsample2(A.d2.p, B, H, W, 64, A.cat1.p, 96, 32, s));
     } else {
-        NET_TRY(conv(net, E4, net->p3.p, B, H3, W3, net->cat3.p, 224, 96, nullptr, s, nullptr, 1));
-        NET_TRY(conv(net, D3, net->cat3.p, B, H2, W2, net->cat2.p, 160, 64, nullptr, s, nullptr, 1));
-        NET_TRY(conv(net, D2, net->cat2.p, B, H1, W1, net->cat1.p, 96, 32, nullptr, s, nullptr, 1));
+        NET_TRY(conv(net, E4, A.p3.p, B, H3, W3, A.cat3.p, 224, 96, nullptr, s, nullptr, 1));
+        NET_TRY(conv(net, D3, A.cat3.p, B, H2, W2, A.cat2.p, 160, 64, nullptr, s, nullptr, 1));
+        NET_TRY(conv(net, D2, A.cat2.p, B, H1, W1, A.cat1.p, 96, 32, nullptr, s, nullptr, 1));
     }
-    NET_TRY(conv(net, D1, net->cat1.p, B, H, W, net->d1.p, 32, 0, nullptr, s));
-    NET_TRY(conv(net, HEAD, net->d1.p, B, H, W, nullptr, 0, 0, net->r.as<float>(), s));
+    NET_TRY(conv(net, D1, A.cat1.p, B, H, W, A.d1.p, 32, 0, nullptr, s));
+    NET_TRY(conv(net, HEAD, A.d1.p, B, H, W, nullptr, 0, 0, A.r.as<float>(), s));
     return ART_OK;
 }
 
 int32_t net_backward(ArtNet *net, int B, int H, int W, cudaStream_t s)
 {
+    NetActs &A = net->act[0];
     const int H1 = H / 2, W1 = W / 2, H2 = H / 4, W2 = W / 4, H3 = H / 8, W3 = W / 8;
     // head
-    NET_TRY(wgrad(net, HEAD, net->d1.p, net->dr.p, B, H, W, s));
-    NET_TRY(dgrad(net, HEAD, 0, net->dr.p, B, H, W, net->gd1.p, net->d1.p, 32, s));
+    NET_TRY(wgrad(net, HEAD, A.d1.p, net->dr.p, B, H, W, s));
+    NET_TRY(dgrad(net, HEAD, 0, net->dr.p, B, H, W, net->gd1.p, A.d1.p, 32, s));
     // d1 (level 0): input cat1 = [e1 | up(d2)]
-    NET_TRY(wgrad(net, D1, net->cat1.p, net->gd1.p, B, H, W, s));
+    NET_TRY(wgrad(net, D1, A.cat1.p, net->gd1.p, B, H, W, s));
     NET_TRY(dgrad(net, D1, 0, net->gd1.p, B, H, W, net->ge1.p, nullptr, 0, s));
     NET_TRY(dgrad(net, D1, 1, net->gd1.p, B, H, W, net->gup1.p, nullptr, 0, s));
-    NET_TRY(art_cnn_downsum2_mask(net->gup1.p, B, H, W, 64, net->d2.p, net->gd2.p, s));
+    NET_TRY(art_cnn_downsum2_mask(net->gup1.p, B, H, W, 64, A.d2.p, net->gd2.p, s));
     // d2 (level 1): input cat2 = [e2 | up(d3)]
-    NET_TRY(wgrad(net, D2, net->cat2.p, net->gd2.p, B, H1, W1, s));
+    NET_TRY(wgrad(net, D2, A.cat2.p, net->gd2.p, B, H1, W1, s));
     NET_TRY(dgrad(net, D2, 0, net->gd2.p, B, H1, W1, net->ge2.p, nullptr, 0, s));
     NET_TRY(dgrad(net, D2, 1, net->gd2.p, B, H1, W1, net->gup2.p, nullptr, 0, s));
-    NET_TRY(art_cnn_downsum2_mask(net->gup2.p, B, H1, W1, 96, net->d3.p, net->gd3.p, s));
+    NET_TRY(art_cnn_downsum2_mask(net->gup2.p, B, H1, W1, 96, A.d3.p, net->gd3.p, s));
     // d3 (level 2): input cat3 = [e3 | up(e4)]
-    NET_TRY(wgrad(net, D3, net->cat3.p, net->gd3.p, B, H2, W2, s));
+    NET_TRY(wgrad(net, D3, A.cat3.p, net->gd3.p, B, H2, W2, s));
     NET_TRY(dgrad(net, D3, 0, net->gd3.p, B, H2, W2, net->ge3.p, nullptr, 0, s));
     NET_TRY(dgrad(net, D3, 1, net->gd3.p, B, H2, W2, net->gup3.p, nullptr, 0, s));
-    NET_TRY(art_cnn_downsum2_mask(net->gup3.p, B, H2, W2, 128, net->e4.p, net->ge4.p, s));
+    NET_TRY(art_cnn_downsum2_mask(net->gup3.p, B, H2, W2, 128, A.e4.p, net->ge4.p, s));
     // e4 (level 3)
-    NET_TRY(wgrad(net, E4, net->p3.p, net->ge4.p, B, H3, W3, s));
+    NET_TRY(wgrad(net, E4, A.p3.p, net->ge4.p, B, H3, W3, s));
     NET_TRY(dgrad(net, E4, 0, net->ge4.p, B, H3, W3, net->gp3.p, nullptr, 0, s));
-    NET_TRY(art_cnn_unpool_add_mask(net->ge3.p, net->gp3.p, B, H2, W2, 96, net->cat3.p, 224, 0, s));
+    NET_TRY(art_cnn_unpool_add_mask(net->ge3.p, net->gp3.p, B, H2, W2, 96, A.cat3.p, 224, 0, s));
     // e3 (level 2)
-    NET_TRY(wgrad(net, E3, net->p2.p, net->ge3.p, B, H2, W2, s));
+    NET_TRY(wgrad(net, E3, A.p2.p, net->ge3.p, B, H2, W2, s));
     NET_TRY(dgrad(net, E3, 0, net->ge3.p, B, H2, W2, net->gp2.p, nullptr, 0, s));
-    NET_TRY(art_cnn_unpool_add_mask(net->ge2.p, net->gp2.p, B, H1, W1, 64, net->cat2.p, 160, 0, s));
+    NET_TRY(art_cnn_unpool_add_mask(net->ge2.p, net->gp2.p, B, H1, W1, 64, A.cat2.p, 160, 0, s));
     // e2 (level 1)
-    NET_TRY(wgrad(net, E2, net->p1.p, net->ge2.p, B, H1, W1, s));
+    NET_TRY(wgrad(net, E2, A.p1.p, net->ge2.p, B, H1, W1, s));
     NET_TRY(dgrad(net, E2, 0, net->ge2.p, B, H1, W1, net->gp1.p, nullptr, 0, s));
-    NET_TRY(art_cnn_unpool_add_mask(net->ge1.p, net->gp1.p, B, H, W, 32, net->cat1.p, 96, 0, s));
+    NET_TRY(art_cnn_unpool_add_mask(net->ge1.p, net->gp1.p, B, H, W, 32, A.cat1.p, 96, 0, s));
     // e1 (level 0)
-    NET_TRY(wgrad(net, E1, net->feat.p, net->ge1.p, B, H, W, s));
+    NET_TRY(wgrad(net, E1, A.feat.p, net->ge1.p, B, H, W, s));
     return ART_OK;
 }
 
@@ -1638,34 +1654,35 @@ int32_t read_err(ArtNet *net, cudaStream_t s)
 
 // Features + forward for B coefficient images; prediction into pred (or the
 // net's own buffer when pred is null).
-int32_t net_predict(ArtNet *net, const int16_t *coef, int cpitch, long long img_stride, const float *q, int B, int H,
-                    int W, float *pred, cudaStream_t s)
+int32_t net_predict(ArtNet *net, int slot, const int16_t *coef, int cpitch, long long img_stride, const float *q, int B,
+                    int H, int W, float *pred, cudaStream_t s)
 {
     NET_TRY(check_geometry(B, H, W));
     const int H0 = level0(H), W0 = level0(W);
-    NET_TRY(net_alloc(net, (long long)B * H0 * W0, (long long)B * H * W, false));
+    NET_TRY(net_alloc(net, slot, (long long)B * H0 * W0, (long long)B * H * W, false));
     if (!net->packed) NET_TRY(net_pack(net, false, s));
-    NET_TRY(art_cnn_features(coef, cpitch, img_stride, q, B, H, W, net->dec.as<float>(), net->feat.p, s));
-    NET_TRY(net_forward(net, B, H0, W0, s, false));
-    return art_cnn_residual(net->r.as<float>(), RSTRIDE, net->dec.as<float>(), nullptr, B, H, W,
-                            pred ? pred : net->pred.as<float>(), nullptr, nullptr, 8 * num_sms(), s);
+    NetActs &A = net->act[slot];
+    NET_TRY(art_cnn_features(coef, cpitch, img_stride, q, B, H, W, A.dec.as<float>(), A.feat.p, s));
+    NET_TRY(net_forward(net, A, B, H0, W0, s, false));
+    return art_cnn_residual(A.r.as<float>(), RSTRIDE, A.dec.as<float>(), nullptr, B, H, W,
+                            pred ? pred : A.pred.as<float>(), nullptr, nullptr, 8 * num_sms(), s);
 }
 
-int32_t net_predict_async(ArtNet *net, const int16_t *coef, int cpitch, long long img_stride, const float *q, int B,
-                          int H, int W, float *pred, void *stream)
+int32_t net_predict_async(ArtNet *net, int slot, const int16_t *coef, int cpitch, long long img_stride, const float *q,
+                          int B, int H, int W, float *pred, void *stream)
 {
-    return net_predict(net, coef, cpitch, img_stride, q, B, H, W, pred, static_cast<cudaStream_t>(stream));
+    return net_predict(net, slot, coef, cpitch, img_stride, q, B, H, W, pred, static_cast<cudaStream_t>(stream));
 }
 
-int32_t net_prepare(ArtNet *net, int B, int H, int W, void *stream)
+int32_t net_prepare(ArtNet *net, int slot, int B, int H, int W, void *stream)
 {
     NET_TRY(check_geometry(B, H, W));
-    NET_TRY(net_alloc(net, (long long)B * level0(H) * level0(W), (long long)B * H * W, false));
+    NET_TRY(net_alloc(net, slot, (long long)B * level0(H) * level0(W), (long long)B * H * W, false));
     if (!net->packed) NET_TRY(net_pack(net, false, static_cast<cudaStream_t>(stream)));
     return ART_OK;
 }
 
-unsigned long long net_generation(const ArtNet *net) { return net->gen; }
+unsigned long long net_generation(const ArtNet *net, int slot) { return net->act[slot].gen; }
 
 int net_device(const ArtNet *net) { return net->device; }
 
@@ -1722,11 +1739,14 @@ void art_net_destroy(ArtNet *net)
     if (!net) return;
     cudaSetDevice(net->device);
     art::cnn::Buf *all[] = {&net->params, &net->grads, &net->adam_m, &net->adam_v, &net->errflag, &net->workspace,
-                            &net->loss_partial, &net->feat, &net->dec, &net->cat1, &net->cat2, &net->cat3, &net->p1,
-                            &net->p2, &net->p3, &net->e4, &net->d3, &net->d2, &net->d1, &net->r, &net->pred,
-                            &net->dr, &net->gd1, &net->ge1, &net->gup1, &net->gd2, &net->ge2, &net->gup2, &net->gd3,
-                            &net->ge3, &net->gup3, &net->ge4, &net->gp3, &net->gp2, &net->gp1};
+                            &net->loss_partial, &net->dr, &net->gd1, &net->ge1, &net->gup1, &net->gd2, &net->ge2,
+                            &net->gup2, &net->gd3, &net->ge3, &net->gup3, &net->ge4, &net->gp3, &net->gp2, &net->gp1};
     for (auto *b : all) b->release();
+    for (auto &A : net->act) {
+        art::cnn::Buf *acts[] = {&A.feat, &A.dec, &A.cat1, &A.cat2, &A.cat3, &A.p1, &A.p2,
+                                 &A.p3,   &A.e4,  &A.d3,   &A.d2,   &A.d1,   &A.r,  &A.pred};
+        for (auto *b : acts) b->release();
+    }
     for (int i = 0; i < art::cnn::NLAYER; i++) {
         net->wf[i].release();
         net->wb[i][0].release();
@@ -1761,7 +1781,7 @@ int32_t art_net_predict(ArtNet *net, const int16_t *coef, int32_t cpitch, int64_
     if (!net || !coef || !q || !pred) return fail(ART_ERR_INVALID_ARGUMENT, "net_predict: null pointer");
     cudaSetDevice(net->device);
     cudaStream_t s = static_cast<cudaStream_t>(stream);
-    NET_TRY(net_predict(net, coef, cpitch, img_stride, q, B, H, W, pred, s));
+    NET_TRY(net_predict(net, 0, coef, cpitch, img_stride, q, B, H, W, pred, s));
     return read_err(net, s);
 }
 
@@ -1782,7 +1802,8 @@ int32_t art_net_train_step(ArtNet *net, const int16_t *coef, int32_t cpitch, int
     cudaStream_t s = static_cast<cudaStream_t>(stream);
     NET_TRY(check_geometry(B, H, W));
     const int H0 = level0(H), W0 = level0(W);
-    NET_TRY(net_alloc(net, (long long)B * H0 * W0, (long long)B * H * W, true));
+    NET_TRY(net_alloc(net, 0, (long long)B * H0 * W0, (long long)B * H * W, true));
+    NetActs &A = net->act[0];
     const size_t pb = (size_t)net->nparam * 4;
     if (!net->grads.p) {
         if (!net->grads.ensure(pb) || !net->adam_m.ensure(pb) || !net->adam_v.ensure(pb) ||
@@ -1790,13 +1811,13 @@ int32_t art_net_train_step(ArtNet *net, const int16_t *coef, int32_t cpitch, int
             return fail(ART_ERR_CUDA, "net_train_step: allocation failed");
     }
     NET_TRY(net_pack(net, true, s));
-    NET_TRY(art_cnn_features(coef, cpitch, img_stride, q, B, H, W, net->dec.as<float>(), net->feat.p, s));
-    NET_TRY(net_forward(net, B, H0, W0, s, true));
+    NET_TRY(art_cnn_features(coef, cpitch, img_stride, q, B, H, W, A.dec.as<float>(), A.feat.p, s));
+    NET_TRY(net_forward(net, A, B, H0, W0, s, true));
     const long long npix = (long long)B * H * W;
-    NET_TRY(art_cnn_residual(net->r.as<float>(), RSTRIDE, net->dec.as<float>(), target, B, H, W, net->pred.as<float>(),
+    NET_TRY(art_cnn_residual(A.r.as<float>(), RSTRIDE, A.dec.as<float>(), target, B, H, W, A.pred.as<float>(),
                              net->dr.p, net->loss_partial.as<float>(), LOSS_BLOCKS, s));
     if (net->smooth_weight > 0.f) {
-        k_residual_smooth_grad<<<LOSS_BLOCKS, 256, 0, s>>>(net->pred.as<float>(), target, B, H, W, net->smooth_weight,
+        k_residual_smooth_grad<<<LOSS_BLOCKS, 256, 0, s>>>(A.pred.as<float>(), target, B, H, W, net->smooth_weight,
                                                            1.f / (float)npix, static_cast<bf16 *>(net->dr.p),
                                                            net->loss_partial.as<float>() + LOSS_BLOCKS);
         NET_TRY(check_launch("k_residual_smooth_grad"));

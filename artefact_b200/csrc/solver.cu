@@ -1375,13 +1375,18 @@ static int prepare_batch(ArtContext *ctx, const std::vector<ImageSpec> &specs, u
         // through the network as one batch: their coefficient images lie a
         // fixed distance apart and their quantisation tables are consecutive
         // in the descriptor.
+        // Groups alternate between the network's two activation sets and the
+        // context's two streams (luma and chroma of one image run side by side;
+        // each group's prediction has its own region of `pred`, by channel).
         struct Group {
             int i, c, nb;
             long long stride;
+            size_t poff;
         };
         std::vector<Group> groups;
         for (int i = 0; i < nimg; i++) {
             const ImgDev &d = ctx->h_desc[i];
+            size_t poff = 0;
             for (int c = 0; c < d.nch;) {
                 const ChanDev &cd = d.ch[c];
                 const long long stride = c + 1 < d.nch ? (long long)(d.ch[c + 1].coef - cd.coef) : 0;
@@ -1389,16 +1394,18 @@ static int prepare_batch(ArtContext *ctx, const std::vector<ImageSpec> &specs, u
                 while (c + nb < d.nch && d.ch[c + nb].cw == cd.cw && d.ch[c + nb].chh == cd.chh &&
                        d.ch[c + nb].cpitch == cd.cpitch && d.ch[c + nb].coef - d.ch[c + nb - 1].coef == stride)
                     nb++;
-                groups.push_back({i, c, nb, stride});
-                if ((rc = cnn::net_prepare(ctx->net, nb, cd.chh, cd.cw, s))) return rc;
+                const int slot = (int)(groups.size() % 2);
+                groups.push_back({i, c, nb, stride, poff});
+                if ((rc = cnn::net_prepare(ctx->net, slot, nb, cd.chh, cd.cw, s))) return rc;
+                poff += (size_t)nb * cd.cw * cd.chh;
                 c += nb;
             }
         }
         // Everything the launches below bake in: buffers, geometry, tasks.
         std::vector<unsigned long long> key = {
-            (unsigned long long)(uintptr_t)ctx->net, cnn::net_generation(ctx->net), (uintptr_t)ctx->desc.p,
-            (uintptr_t)ctx->tasks.p, (uintptr_t)pred, (uintptr_t)ctx->xbuf.p, (uintptr_t)ctx->coefimg.p,
-            (unsigned long long)nimg};
+            (unsigned long long)(uintptr_t)ctx->net, cnn::net_generation(ctx->net, 0), cnn::net_generation(ctx->net, 1),
+            (uintptr_t)ctx->desc.p, (uintptr_t)ctx->tasks.p, (uintptr_t)pred, (uintptr_t)ctx->xbuf.p,
+            (uintptr_t)ctx->coefimg.p, (unsigned long long)nimg};
         for (int m = 0; m < 5; m++) key.push_back((unsigned long long)ctx->mode_off[m]);
         for (int i = 0; i < nimg; i++) {
             const ImgDev &d = ctx->h_desc[i];
@@ -1413,15 +1420,27 @@ static int prepare_batch(ArtContext *ctx, const std::vector<ImageSpec> &specs, u
         // (g = 0, sigma = 0): x_0 = y_0 = P(prediction), and the DCT-distance
         // plane of the projected prediction for the first gradient.
         auto launch_init = [&]() -> int {
-            for (const Group &gr : groups) {
+            if (groups.size() > 1) {
+                ART_CUDA(cudaEventRecord(ctx->fork, s));
+                ART_CUDA(cudaStreamWaitEvent(ctx->side, ctx->fork, 0));
+            }
+            for (size_t g = 0; g < groups.size(); g++) {
+                const Group &gr = groups[g];
+                const int slot = (int)(g % 2);
+                cudaStream_t gs = slot ? ctx->side : s;
                 const ImgDev &d = ctx->h_desc[gr.i];
                 const ChanDev &cd = d.ch[gr.c];
-                const int r = cnn::net_predict_async(ctx->net, cd.coef, cd.cpitch, gr.stride, &ddesc[gr.i].q[gr.c][0],
-                                                     gr.nb, cd.chh, cd.cw, pred, s);
+                float *gp = pred + gr.poff;
+                const int r = cnn::net_predict_async(ctx->net, slot, cd.coef, cd.cpitch, gr.stride,
+                                                     &ddesc[gr.i].q[gr.c][0], gr.nb, cd.chh, cd.cw, gp, gs);
                 if (r) return r;
                 for (int k = 0; k < gr.nb; k++)
-                    k_upsample<<<(int)(((long long)d.W * d.H + 255) / 256), 256, 0, s>>>(
-                        pred + (size_t)k * cd.cw * cd.chh, ddesc + gr.i, gr.c + k);
+                    k_upsample<<<(int)(((long long)d.W * d.H + 255) / 256), 256, 0, gs>>>(
+                        gp + (size_t)k * cd.cw * cd.chh, ddesc + gr.i, gr.c + k);
+            }
+            if (groups.size() > 1) {
+                ART_CUDA(cudaEventRecord(ctx->join, ctx->side));
+                ART_CUDA(cudaStreamWaitEvent(s, ctx->join, 0));
             }
             for (int i = 0; i < nimg; i++) {
                 const ImgDev &d = ctx->h_desc[i];
