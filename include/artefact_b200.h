@@ -185,6 +185,11 @@ int32_t art_context_tune_cache(ArtContext *ctx, const char *path, int32_t save);
  * repeated to full resolution like the decoded start, projected onto the
  * quantisation box, and the solve's `iterations` plain iterations refine it
  * with the FISTA sequence restarted. No reference counterpart.
+ * The predictions of one solve run on the context's two streams, each with
+ * one of the network's two sets of activation buffers; so learned solves on
+ * different contexts that share one network must not overlap in time. The
+ * second learned solve of one geometry on a context records the prediction
+ * launches as a CUDA graph, which later solves of that geometry replay.
  */
 int32_t art_context_set_warm_start(ArtContext *ctx, ArtNet *net);
 
