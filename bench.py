@@ -11,8 +11,9 @@ Workloads (``--workload``; seeded synthetic JPEGs, ``artefact_b200.synth``):
 * ``batch256``: 256 JPEGs, W, H ~ U[256, 2048] rounded to 16, 4:2:0 or 4:4:4
   with p = 0.5, quality ~ U[20, 90], 50 iterations, solved as one batch.
 * ``learned``: 1920x1080 4:2:0 at quality 30/50/75: the learned warm start +
-  8 plain iterations against the plain 50-iteration solve, and the fewest
-  iterations whose objective reaches the plain 50-iteration one.
+  the fewest refinement iterations whose objective reaches the plain
+  50-iteration one (the value), against the plain 50-iteration solve; a fixed
+  8-iteration refinement beside it.
 * ``network``: the warm-start network's forward pass alone (TFLOP/s).
 
 A step is one solve of the whole workload. Metric: megapixels per second of
@@ -64,10 +65,10 @@ WORKLOADS = {
                  metric="MPix/s (plain 100-iteration solve, 6000x4000 4:4:4 q30)", iterations=100),
     "batch256": dict(name="256 JPEGs, W,H~U[256,2048] (x16), 4:2:0|4:4:4 p=.5, q~U[20,90], one batch, 50 iterations",
                      metric="MPix/s (plain 50-iteration batched solve, 256 images)", iterations=50),
-    "learned": dict(name="1920x1080 YCbCr 4:2:0 baseline JPEGs at q30/50/75: learned warm start + 8 plain "
-                         "iterations against the plain 50-iteration solve",
-                    metric="MPix/s to the plain 50-iteration objective (learned warm start + 8 iterations, "
-                           "1080p 4:2:0 q30/50/75)", iterations=8),
+    "learned": dict(name="1920x1080 YCbCr 4:2:0 baseline JPEGs at q30/50/75: learned warm start + refinement "
+                         "against the plain 50-iteration solve",
+                    metric="MPix/s to the plain 50-iteration objective (learned warm start + the fewest refinement "
+                           "iterations that reach it, 1080p 4:2:0 q30/50/75)", iterations=8),
 }
 WORKLOADS["network"] = dict(
     name="warm-start network forward on one 1920x1080 4:2:0 JPEG (luma 1920x1088, chroma 2 x 960x544)",
@@ -447,7 +448,9 @@ def time_network(device, steps, warmup):
 
 
 def run_learned(args, lib, local, rank, world, dist):
-    """Config 5: learned warm start + 8 plain iterations vs the plain 50-iteration solve."""
+    """Config 5: learned warm start + the fewest refinement iterations that reach
+    the plain 50-iteration objective, against the plain 50-iteration solve (the
+    fixed 8-iteration refinement is reported beside it)."""
     import torch
 
     wl = WORKLOADS["learned"]
@@ -460,27 +463,38 @@ def run_learned(args, lib, local, rank, world, dist):
     net_ms, net_tflops, net_flops = time_network(local, args.steps, args.warmup)
     peaks = json.loads((ROOT / "MEASURED_PEAKS.json").read_text()) if (ROOT / "MEASURED_PEAKS.json").exists() else {}
     tc_peak = float(peaks.get("bf16_tflops", 1590.0))
-    value = res["learned_mpix_s"]
-    total_ms = sum(r["learned_ms"] for r in res["images"])
+    # The headline: each image solved to the plain 50-iteration objective
+    # (learned start + the fewest ladder iterations that reach it). The fixed
+    # 8-iteration refinement, which stops short of that objective, is
+    # reported beside it.
+    reach = all(r["min_refine_ms"] for r in res["images"])
+    total_ms = sum(r["min_refine_ms"] for r in res["images"]) if reach else float("nan")
+    k8_ms = sum(r["learned_ms"] for r in res["images"])
     if dist:
-        t = torch.tensor([total_ms], device="cuda", dtype=torch.float64)
+        t = torch.tensor([total_ms, k8_ms], device="cuda", dtype=torch.float64)
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        total_ms = float(t.item())
-        value = world * len(res["images"]) * 1920 * 1080 / 1e6 / (total_ms * 1e-3)
+        total_ms, k8_ms = float(t[0].item()), float(t[1].item())
+    mpix = world * len(res["images"]) * 1920 * 1080 / 1e6
+    value = mpix / (total_ms * 1e-3) if reach else None
+    k8 = mpix / (k8_ms * 1e-3)
     if rank == 0:
         line = {
             "metric": wl["metric"], "value": value, "unit": "MPix/s", "n_gpus": world, "steps": args.steps,
-            "warmup": args.warmup, "ms_per_step": total_ms / len(res["images"]), "higher_is_better": True,
+            "warmup": args.warmup, "ms_per_step": (total_ms / len(res["images"])) if reach else None,
+            "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f32 solver, bf16 network (fp32 accumulation)",
             "data": "synthetic",
             "config": {"workload": wl["name"], "refine_iterations": res["refine_iterations"],
                        "refine_schedule": res["schedule"],
                        "l2": "flushed between steps (256 MiB write outside the timed events)",
                        "parallelism": f"replicas x{world}"},
-            "plain50_mpix_s": res["plain50_mpix_s"], "speedup_vs_plain50": value / res["plain50_mpix_s"],
-            "all_reach_plain50": res["all_reach_plain50"],
-            "reach_plain50_mpix_s": res["reach_mpix_s"],
-            "reach_speedup_vs_plain50": (res["reach_mpix_s"] / res["plain50_mpix_s"]) if res["reach_mpix_s"] else None,
+            "plain50_mpix_s": res["plain50_mpix_s"],
+            "speedup_vs_plain50": (value / res["plain50_mpix_s"]) if value else None,
+            "refine_iterations_to_reach": [r["min_refine_to_reach"] for r in res["images"]],
+            "fixed_refine": {"iterations": res["refine_iterations"], "mpix_s": k8,
+                             "speedup_vs_plain50": k8 / res["plain50_mpix_s"],
+                             "all_reach_plain50": res["all_reach_plain50"],
+                             "max_E_rel_to_plain50": max(r["E_learned_rel"] for r in res["images"])},
             "images": res["images"],
             "roofline": {"bound": "tensor", "kernel": "warm-start network forward (k_conv3x3 and glue)",
                          "achieved": net_tflops, "peak": tc_peak, "unit": "TFLOP/s", "frac": net_tflops / tc_peak,
