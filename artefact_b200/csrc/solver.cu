@@ -340,6 +340,7 @@ __global__ void __launch_bounds__(SWEEP_WARPS_N * 32, SWEEP_MIN_BLOCKS_N) k_grad
                 Gm[c] = G0[c] = Gp[c] = 0.f;
             }
         }
+#pragma unroll 2
         for (int t = ys - 1; t <= ys + R; t++) {
             float yn[NCH], pr[NCH];
             {
