@@ -232,7 +232,8 @@ int32_t art_context_last_timing(ArtContext *ctx, float *loop_ms, float *gradient
  * ART_ERR_INVALID_ARGUMENT. dct_coefs and out_planes_device are device
  * pointers, quant_table a host pointer; work runs on `stream` (NULL = legacy
  * default stream) and the call returns when it is done. The first call on a
- * device resolves the array's address there. All calls share the array, so
+ * device resolves the array's address there (cudaGetSymbolAddress), so make
+ * that first call before any CUDA stream capture. All calls share the array, so
  * calls whose GPU work overlaps race; each call clears what must start at zero.
  */
 int32_t art_solve_noalloc(uint32_t nchannel, const ArtChannel *coefs, float weight, const float pweight[3],
