@@ -2,18 +2,48 @@
 #pragma once
 
 #include <cstdint>
+#include <memory>
+#include <new>
 #include <string>
+#include <utility>
 #include <vector>
 
 struct ArtNet;
 
 namespace art {
 
+// Allocator whose value-less construct leaves elements uninitialised, so
+// resize() of a coefficient plane that every block decode fills anyway does
+// not write the whole plane first.
+template <class T>
+struct NoInitAlloc : std::allocator<T> {
+    template <class U>
+    struct rebind {
+        using other = NoInitAlloc<U>;
+    };
+    NoInitAlloc() = default;
+    template <class U>
+    NoInitAlloc(const NoInitAlloc<U> &) noexcept
+    {
+    }
+    template <class U>
+    void construct(U *p) noexcept
+    {
+        ::new (static_cast<void *>(p)) U;
+    }
+    template <class U, class... A>
+    void construct(U *p, A &&...a)
+    {
+        ::new (static_cast<void *>(p)) U(std::forward<A>(a)...);
+    }
+};
+using CoefVec = std::vector<int16_t, NoInitAlloc<int16_t>>;
+
 struct JpegChannel {
     uint32_t rounded_px_w = 0, rounded_px_h = 0, block_w = 0, block_h = 0;
     uint32_t samp_h = 1, samp_v = 1;
     float quant[64];
-    std::vector<int16_t> coefs;  // block raster, natural order inside a block
+    CoefVec coefs;  // block raster, natural order inside a block
 };
 
 struct JpegImage {

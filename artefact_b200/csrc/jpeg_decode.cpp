@@ -48,11 +48,29 @@ struct Huffman {
     uint8_t vals[256];
     // 9-bit lookahead: (length << 8) | value, 0 when the code is longer.
     uint16_t fast[512];
+    // AC tables: 11-bit lookahead decoding a code and its magnitude bits at
+    // once (see ac_entry); empty for DC tables.
+    std::vector<uint32_t> fast_ac;
 };
 
-void build_huffman(Huffman &h, const uint8_t counts[16], const uint8_t *symbols, int nsym)
+// Combined AC lookahead entries: bits 0-4 the bits consumed, 5-8 the run,
+// 9-10 the kind (1: a coefficient whose value is in bits 16-31, 2: end of
+// block; 0: no shortcut -- a longer code, ZRL, or magnitude bits beyond the
+// window), 16-31 the sign-extended coefficient.
+constexpr int AC_LOOK = 11;
+constexpr uint32_t AC_COEF = 1u << 9, AC_EOB = 2u << 9;
+
+static inline int extend(int v, int t) { return v < (1 << (t - 1)) ? v - (1 << t) + 1 : v; }
+
+void build_huffman(Huffman &h, const uint8_t counts[16], const uint8_t *symbols, int nsym, bool ac)
 {
-    memset(&h, 0, sizeof(h));
+    h.present = false;
+    memset(h.maxcode, 0, sizeof(h.maxcode));
+    memset(h.valptr, 0, sizeof(h.valptr));
+    memset(h.mincode, 0, sizeof(h.mincode));
+    memset(h.vals, 0, sizeof(h.vals));
+    memset(h.fast, 0, sizeof(h.fast));
+    h.fast_ac.clear();
     memcpy(h.vals, symbols, nsym);
     int code = 0, k = 0;
     for (int len = 1; len <= 16; len++) {
@@ -75,6 +93,27 @@ void build_huffman(Huffman &h, const uint8_t counts[16], const uint8_t *symbols,
             for (int f = 0; f < (1 << shift); f++) h.fast[(c << shift) | f] = (uint16_t)((len << 8) | symbols[k]);
         }
     }
+    if (ac) {
+        h.fast_ac.assign(1u << AC_LOOK, 0u);
+        k = 0;
+        for (int len = 1; len <= AC_LOOK; len++) {
+            for (int i = 0; i < counts[len - 1]; i++, k++) {
+                const int c = h.mincode[len] + i, rs = symbols[k], r = rs >> 4, sz = rs & 15;
+                const int shift = AC_LOOK - len;
+                for (int f = 0; f < (1 << shift); f++) {
+                    uint32_t e = 0;
+                    if (sz == 0) {
+                        if (r != 15) e = (uint32_t)len | AC_EOB;  // end of block; ZRL takes the general path
+                    } else if (len + sz <= AC_LOOK) {
+                        const int mag = f >> (shift - sz);  // the sz bits after the code
+                        const int v = extend(mag, sz);
+                        e = (uint32_t)(len + sz) | ((uint32_t)r << 5) | AC_COEF | ((uint32_t)(uint16_t)(int16_t)v << 16);
+                    }
+                    h.fast_ac[(c << shift) | f] = e;
+                }
+            }
+        }
+    }
     h.present = true;
 }
 
@@ -84,7 +123,8 @@ struct Component {
     int td = 0, ta = 0;
     int dc_pred = 0;
     uint32_t rounded_w = 0, rounded_h = 0, block_w = 0, block_h = 0;
-    std::vector<int16_t> coefs;
+    CoefVec coefs;
+    bool defined = false;  // every element of coefs has been written (else they are uninitialised)
 };
 
 class Decoder {
@@ -107,8 +147,9 @@ class Decoder {
     int width_ = 0, height_ = 0;
     int hmax_ = 1, vmax_ = 1;
     int restart_interval_ = 0;
-    // Bit reader state.
-    uint32_t bitbuf_ = 0;
+    // Bit reader state: the next bitcnt_ bits of the entropy-coded data,
+    // MSB-aligned in a 64-bit word.
+    uint64_t bitbuf_ = 0;
     int bitcnt_ = 0;
     bool hit_marker_ = false;
 
@@ -135,6 +176,14 @@ class Decoder {
     void fill_bits();
     int get_bits(int n);
     int decode_huff(const Huffman &h);
+    int decode_huff_nofill(const Huffman &h);
+    int take_bits(int n)  // n <= bitcnt_, 1 <= n <= 16
+    {
+        const int v = (int)(bitbuf_ >> (64 - n));
+        bitbuf_ <<= n;
+        bitcnt_ -= n;
+        return v;
+    }
     void decode_block(Component &c, int16_t *blk);
     void reset_bits()
     {
@@ -182,7 +231,7 @@ void Decoder::parse_dht()
         if (total > 256 || 17 + total > len) fail("Invalid Huffman length in image");
         uint8_t syms[256];
         for (int i = 0; i < total; i++) syms[i] = u8();
-        build_huffman(tc ? ac_[th] : dc_[th], counts, syms, total);
+        build_huffman(tc ? ac_[th] : dc_[th], counts, syms, total, tc != 0);
         len -= 17 + total;
     }
 }
@@ -234,15 +283,41 @@ void Decoder::parse_sof(int marker)
         c.rounded_h = rh / sf_v;
         c.block_w = c.rounded_w / 8;
         c.block_h = c.rounded_h / 8;
-        c.coefs.assign((size_t)c.rounded_w * c.rounded_h, 0);
+        // Progressive scans refine what earlier scans left, so they start from
+        // zeros. A sequential scan writes each block it codes in full (zeros
+        // included); blocks no scan codes are zeroed when that is known.
+        if (progressive_) {
+            c.coefs.assign((size_t)c.rounded_w * c.rounded_h, 0);
+            c.defined = true;
+        } else {
+            c.coefs.resize((size_t)c.rounded_w * c.rounded_h);
+            c.defined = false;
+        }
     }
     have_sof_ = true;
 }
 
+// Tops the buffer up to at least 57 bits. Byte stuffing (FF 00) is undone;
+// at a marker (FF followed by anything else) the reader stops in front of it
+// and feeds zero bytes from then on (T.81 F.2.2.5). Eight bytes without an FF
+// are appended in one step.
 void Decoder::fill_bits()
 {
-    while (bitcnt_ <= 24) {
-        uint32_t byte = 0;
+    if (!hit_marker_ && bitcnt_ <= 56 && pos_ + 8 <= n_) {
+        uint64_t w;
+        memcpy(&w, d_ + pos_, 8);
+        const uint64_t x = ~w;  // a byte of w is FF exactly when this byte of x is 0
+        if (!((x - 0x0101010101010101ULL) & ~x & 0x8080808080808080ULL)) {
+            const int nb = (64 - bitcnt_) >> 3;  // whole bytes that fit: 1..8
+            const uint64_t be = __builtin_bswap64(w);  // first byte of the stream in the top byte
+            bitbuf_ |= (be >> (64 - 8 * nb)) << (64 - 8 * nb - bitcnt_);
+            pos_ += (size_t)nb;
+            bitcnt_ += 8 * nb;
+            return;
+        }
+    }
+    while (bitcnt_ <= 56) {
+        uint64_t byte = 0;
         if (!hit_marker_ && pos_ < n_) {
             byte = d_[pos_];
             if (byte == 0xFF) {
@@ -257,7 +332,7 @@ void Decoder::fill_bits()
                 pos_++;
             }
         }
-        bitbuf_ |= byte << (24 - bitcnt_);
+        bitbuf_ |= byte << (56 - bitcnt_);
         bitcnt_ += 8;
     }
 }
@@ -265,27 +340,23 @@ void Decoder::fill_bits()
 int Decoder::get_bits(int n)
 {
     if (n == 0) return 0;
-    fill_bits();
-    int v = (int)(bitbuf_ >> (32 - n));
-    bitbuf_ <<= n;
-    bitcnt_ -= n;
-    return v;
+    if (bitcnt_ < n) fill_bits();
+    return take_bits(n);
 }
 
-int Decoder::decode_huff(const Huffman &h)
+// Huffman symbol from a buffer holding at least 16 bits.
+int Decoder::decode_huff_nofill(const Huffman &h)
 {
-    fill_bits();
-    uint32_t look = bitbuf_ >> 23;
-    uint16_t f = h.fast[look];
+    const uint16_t f = h.fast[bitbuf_ >> 55];
     if (f) {
-        int l = f >> 8;
+        const int l = f >> 8;
         bitbuf_ <<= l;
         bitcnt_ -= l;
         return f & 0xFF;
     }
     int code = 0;
     for (int len = 1; len <= 16; len++) {
-        code = (code << 1) | (int)(bitbuf_ >> 31);
+        code = (code << 1) | (int)(bitbuf_ >> 63);
         bitbuf_ <<= 1;
         bitcnt_--;
         if (h.maxcode[len] >= 0 && code <= h.maxcode[len] && code >= h.mincode[len])
@@ -294,18 +365,46 @@ int Decoder::decode_huff(const Huffman &h)
     fail("Bad Huffman code: corrupt JPEG entropy data");
 }
 
-static inline int extend(int v, int t) { return v < (1 << (t - 1)) ? v - (1 << t) + 1 : v; }
+int Decoder::decode_huff(const Huffman &h)
+{
+    if (bitcnt_ < 16) fill_bits();
+    return decode_huff_nofill(h);
+}
 
+// One block of a sequential scan into blk (zeroed here). The buffer is
+// topped up to 32+ bits before each Huffman code, which leaves 16+ bits for
+// the code's magnitude bits (at most 15).
 void Decoder::decode_block(Component &c, int16_t *blk)
 {
     const Huffman &dc = dc_[c.td], &ac = ac_[c.ta];
-    int t = decode_huff(dc);
+    memset(blk, 0, 64 * sizeof(int16_t));
+    if (bitcnt_ < 32) fill_bits();
+    int t = decode_huff_nofill(dc);
     if (t > 11) fail("Bad DC magnitude category");
-    int diff = t ? extend(get_bits(t), t) : 0;
+    int diff = t ? extend(take_bits(t), t) : 0;
     c.dc_pred += diff;
     blk[0] = (int16_t)c.dc_pred;
+    const uint32_t *fast_ac = ac.fast_ac.data();
     for (int k = 1; k < 64;) {
-        int rs = decode_huff(ac);
+        if (bitcnt_ < 32) fill_bits();
+        const uint32_t e = fast_ac[bitbuf_ >> (64 - AC_LOOK)];
+        if (e & AC_COEF) {  // code and magnitude bits in one step
+            k += (int)((e >> 5) & 15);
+            if (k > 63) fail("Coefficient index out of range: corrupt JPEG");
+            blk[kZigzagToNatural[k]] = (int16_t)(e >> 16);
+            const int l = (int)(e & 31);
+            bitbuf_ <<= l;
+            bitcnt_ -= l;
+            k++;
+            continue;
+        }
+        if (e & AC_EOB) {
+            const int l = (int)(e & 31);
+            bitbuf_ <<= l;
+            bitcnt_ -= l;
+            break;
+        }
+        int rs = decode_huff_nofill(ac);
         int r = rs >> 4, s = rs & 15;
         if (s == 0) {
             if (r != 15) break;  // EOB
@@ -314,7 +413,7 @@ void Decoder::decode_block(Component &c, int16_t *blk)
         }
         k += r;
         if (k > 63) fail("Coefficient index out of range: corrupt JPEG");
-        blk[kZigzagToNatural[k]] = (int16_t)extend(get_bits(s), s);
+        blk[kZigzagToNatural[k]] = (int16_t)extend(take_bits(s), s);
         k++;
     }
 }
@@ -341,21 +440,30 @@ void Decoder::decode_scan(const std::vector<int> &scomp)
         Component &c = comps_[scomp[0]];
         int cw = (width_ * c.h + hmax_ - 1) / hmax_, chh = (height_ * c.v + vmax_ - 1) / vmax_;
         int bw = (cw + 7) / 8, bh = (chh + 7) / 8;
+        if (!c.defined) {
+            // Blocks of the rounded plane that this scan does not code stay zero.
+            for (uint32_t by = 0; by < c.block_h; by++)
+                for (uint32_t bx = (by < (uint32_t)bh ? (uint32_t)bw : 0); bx < c.block_w; bx++)
+                    memset(&c.coefs[((size_t)by * c.block_w + bx) * 64], 0, 64 * sizeof(int16_t));
+            c.defined = true;
+        }
         for (int by = 0; by < bh; by++)
             for (int bx = 0; bx < bw; bx++) {
                 if (restart_interval_ && todo == 0) {
                     handle_restart();
                     todo = restart_interval_;
                 }
-                int16_t blk[64] = {0};
-                decode_block(c, blk);
-                if ((uint32_t)bx < c.block_w && (uint32_t)by < c.block_h)
-                    memcpy(&c.coefs[((size_t)by * c.block_w + bx) * 64], blk, sizeof(blk));
+                int16_t pad[64];  // blocks past the component's rounded size are decoded and dropped
+                const bool in = (uint32_t)bx < c.block_w && (uint32_t)by < c.block_h;
+                decode_block(c, in ? &c.coefs[((size_t)by * c.block_w + bx) * 64] : pad);
                 if (restart_interval_) todo--;
             }
         return;
     }
     int mcu_w = (width_ + 8 * hmax_ - 1) / (8 * hmax_), mcu_h = (height_ + 8 * vmax_ - 1) / (8 * vmax_);
+    // The MCUs of an interleaved scan cover every block of its components'
+    // rounded planes (block_w = mcu_w * h, block_h = mcu_h * v).
+    for (int ci : scomp) comps_[ci].defined = true;
     for (int my = 0; my < mcu_h; my++)
         for (int mx = 0; mx < mcu_w; mx++) {
             if (restart_interval_ && todo == 0) {
@@ -366,11 +474,10 @@ void Decoder::decode_scan(const std::vector<int> &scomp)
                 Component &c = comps_[ci];
                 for (int v = 0; v < c.v; v++)
                     for (int u = 0; u < c.h; u++) {
-                        int16_t blk[64] = {0};
-                        decode_block(c, blk);
-                        uint32_t bx = (uint32_t)(mx * c.h + u), by = (uint32_t)(my * c.v + v);
-                        if (bx < c.block_w && by < c.block_h)
-                            memcpy(&c.coefs[((size_t)by * c.block_w + bx) * 64], blk, sizeof(blk));
+                        int16_t pad[64];  // blocks past the component's rounded size are decoded and dropped
+                        const uint32_t bx = (uint32_t)(mx * c.h + u), by = (uint32_t)(my * c.v + v);
+                        const bool in = bx < c.block_w && by < c.block_h;
+                        decode_block(c, in ? &c.coefs[((size_t)by * c.block_w + bx) * 64] : pad);
                     }
             }
             if (restart_interval_) todo--;
@@ -516,6 +623,13 @@ void Decoder::decode_scan_progressive(const std::vector<int> &scomp, int ss, int
         Component &c = comps_[scomp[0]];
         int cw = (width_ * c.h + hmax_ - 1) / hmax_, chh = (height_ * c.v + vmax_ - 1) / vmax_;
         int bw = (cw + 7) / 8, bh = (chh + 7) / 8;
+        if (!c.defined) {
+            // Blocks of the rounded plane that this scan does not code stay zero.
+            for (uint32_t by = 0; by < c.block_h; by++)
+                for (uint32_t bx = (by < (uint32_t)bh ? (uint32_t)bw : 0); bx < c.block_w; bx++)
+                    memset(&c.coefs[((size_t)by * c.block_w + bx) * 64], 0, 64 * sizeof(int16_t));
+            c.defined = true;
+        }
         for (int by = 0; by < bh; by++)
             for (int bx = 0; bx < bw; bx++) {
                 restart_if_due();
@@ -525,6 +639,9 @@ void Decoder::decode_scan_progressive(const std::vector<int> &scomp, int ss, int
         return;
     }
     int mcu_w = (width_ + 8 * hmax_ - 1) / (8 * hmax_), mcu_h = (height_ + 8 * vmax_ - 1) / (8 * vmax_);
+    // The MCUs of an interleaved scan cover every block of its components'
+    // rounded planes (block_w = mcu_w * h, block_h = mcu_h * v).
+    for (int ci : scomp) comps_[ci].defined = true;
     for (int my = 0; my < mcu_h; my++)
         for (int mx = 0; mx < mcu_w; mx++) {
             restart_if_due();
@@ -630,6 +747,7 @@ void Decoder::run(JpegImage &out)
         jc.samp_h = (uint32_t)(hmax_ / c.h);
         jc.samp_v = (uint32_t)(vmax_ / c.v);
         for (int j = 0; j < 64; j++) jc.quant[j] = (float)qt_[c.tq][j];
+        if (!c.defined) c.coefs.assign(c.coefs.size(), 0);  // a component no scan coded
         jc.coefs = std::move(c.coefs);
         out.channels.push_back(std::move(jc));
     }
