@@ -92,11 +92,11 @@ def test_rounded_sizes_follow_max_sampling():
         (1920, 1088, 1), (960, 544, 2), (960, 544, 2)]
 
 
-def _pillow(img, quality, subsampling, progressive, **kw):
+def _pillow(img, quality, subsampling, progressive, optimize=False, **kw):
     from PIL import Image
 
     buf = io.BytesIO()
-    opts = dict(format="JPEG", quality=quality, optimize=False, progressive=progressive, **kw)
+    opts = dict(format="JPEG", quality=quality, optimize=optimize, progressive=progressive, **kw)
     if img.ndim == 3:
         opts["subsampling"] = subsampling
     Image.fromarray(img).save(buf, **opts)
@@ -122,6 +122,25 @@ def test_progressive_equals_sequential(w, h, q, sub, gray, restart):
     for x, y in zip(a.coefs, b.coefs):
         assert (x.rounded_px_w, x.rounded_px_h, x.horizontal_samp_factor, x.vertical_samp_factor) == (
             y.rounded_px_w, y.rounded_px_h, y.horizontal_samp_factor, y.vertical_samp_factor)
+        np.testing.assert_array_equal(x.quant_table, y.quant_table)
+        np.testing.assert_array_equal(x.dct_coefs, y.dct_coefs)
+
+
+@pytest.mark.parametrize("seed,w,h,q,sub,restart", [
+    (0, 320, 200, 95, 0, {}), (1, 257, 131, 60, 2, {"restart_marker_blocks": 2}), (2, 96, 512, 15, 1, {}),
+    (3, 641, 97, 100, 2, {"restart_marker_rows": 1}), (4, 33, 47, 80, 0, {}),
+])
+def test_optimised_tables_sequential_equals_progressive(seed, w, h, q, sub, restart):
+    """Streams with image-specific (optimised) Huffman tables -- long codes and,
+    on a noisy image, large magnitudes: the sequential path (its combined
+    code-and-magnitude lookup) and the progressive path decode the same
+    coefficients."""
+    rng = np.random.default_rng(seed)
+    img = synth.rgb_image(h, w, 11 + seed).astype(np.int16) + rng.integers(-70, 71, size=(h, w, 3))
+    img = np.clip(img, 0, 255).astype(np.uint8)
+    a = Jpeg.from_source(JpegSource.Buffer(_pillow(img, q, sub, False, optimize=True, **restart)))
+    b = Jpeg.from_source(JpegSource.Buffer(_pillow(img, q, sub, True, **restart)))
+    for x, y in zip(a.coefs, b.coefs):
         np.testing.assert_array_equal(x.quant_table, y.quant_table)
         np.testing.assert_array_equal(x.dct_coefs, y.dct_coefs)
 
