@@ -91,6 +91,31 @@ class JpegSource:
             raise ArtefactError(f"Failed to read JPEG file '{self.path}': {e}") from e
 
 
+class _NativeJpeg:
+    """Owns a decoded image of art_jpeg_decode; freed when the last coefficient
+    array viewing its memory is gone."""
+
+    def __init__(self, lib, handle):
+        self._lib, self._h = lib, handle
+
+    def __del__(self):
+        h, self._h = self._h, None
+        if h:
+            try:
+                self._lib.art_jpeg_free(h)
+            except Exception:  # interpreter shutdown
+                pass
+
+
+class _NativePlane:
+    """int16 plane inside a _NativeJpeg, exposed to numpy without a copy; the
+    array keeps this object (and so the decoded image) alive."""
+
+    def __init__(self, owner: _NativeJpeg, address: int, n: int):
+        self._owner = owner
+        self.__array_interface__ = {"data": (address, False), "shape": (n,), "typestr": "<i2", "version": 3}
+
+
 @dataclass
 class Jpeg:
     """Decoded coefficient data of a JPEG (jpeg/mod.rs:29-36, jpeg/zune.rs:5-55)."""
@@ -108,21 +133,21 @@ class Jpeg:
         rc = lib.art_jpeg_decode(data, len(data), C.byref(handle))
         if rc != N.ART_OK:
             raise ArtefactError(lib.art_last_error().decode("utf-8", "replace"))
-        try:
-            nch, rw, rh = C.c_uint32(), C.c_uint32(), C.c_uint32()
-            N.check(lib.art_jpeg_info(handle, C.byref(nch), C.byref(rw), C.byref(rh)))
-            coefs = []
-            for c in range(nch.value):
-                ch = N.ArtChannel()
-                N.check(lib.art_jpeg_channel(handle, c, C.byref(ch)))
-                n = ch.block_w * ch.block_h * 64
-                arr = np.ctypeslib.as_array(C.cast(ch.dct_coefs, C.POINTER(C.c_int16)), shape=(n,)).copy()
-                q = np.ctypeslib.as_array(ch.quant_table, shape=(64,)).copy()
-                coefs.append(Coefficient(ch.rounded_px_w, ch.rounded_px_h, ch.block_w, ch.block_h,
-                                         ch.samp_h, ch.samp_v, arr, q))
-            return Jpeg(nch.value, rw.value, rh.value, coefs)
-        finally:
-            lib.art_jpeg_free(handle)
+        # The coefficient arrays view the decoder's planes (no copy); the
+        # decoded image is freed with the last of them.
+        owner = _NativeJpeg(lib, handle)
+        nch, rw, rh = C.c_uint32(), C.c_uint32(), C.c_uint32()
+        N.check(lib.art_jpeg_info(handle, C.byref(nch), C.byref(rw), C.byref(rh)))
+        coefs = []
+        for c in range(nch.value):
+            ch = N.ArtChannel()
+            N.check(lib.art_jpeg_channel(handle, c, C.byref(ch)))
+            n = ch.block_w * ch.block_h * 64
+            arr = np.asarray(_NativePlane(owner, ch.dct_coefs, n))
+            q = np.ctypeslib.as_array(ch.quant_table, shape=(64,)).copy()
+            coefs.append(Coefficient(ch.rounded_px_w, ch.rounded_px_h, ch.block_w, ch.block_h,
+                                     ch.samp_h, ch.samp_v, arr, q))
+        return Jpeg(nch.value, rw.value, rh.value, coefs)
 
     def max_rounded(self):
         """Largest rounded component size (lib.rs:108-116)."""
