@@ -623,13 +623,6 @@ void Decoder::decode_scan_progressive(const std::vector<int> &scomp, int ss, int
         Component &c = comps_[scomp[0]];
         int cw = (width_ * c.h + hmax_ - 1) / hmax_, chh = (height_ * c.v + vmax_ - 1) / vmax_;
         int bw = (cw + 7) / 8, bh = (chh + 7) / 8;
-        if (!c.defined) {
-            // Blocks of the rounded plane that this scan does not code stay zero.
-            for (uint32_t by = 0; by < c.block_h; by++)
-                for (uint32_t bx = (by < (uint32_t)bh ? (uint32_t)bw : 0); bx < c.block_w; bx++)
-                    memset(&c.coefs[((size_t)by * c.block_w + bx) * 64], 0, 64 * sizeof(int16_t));
-            c.defined = true;
-        }
         for (int by = 0; by < bh; by++)
             for (int bx = 0; bx < bw; bx++) {
                 restart_if_due();
