@@ -54,9 +54,10 @@ struct Huffman {
 };
 
 // Combined AC lookahead entries: bits 0-4 the bits consumed, 5-8 the run,
-// 9-10 the kind (1: a coefficient whose value is in bits 16-31, 2: end of
-// block; 0: no shortcut -- a longer code, ZRL, or magnitude bits beyond the
-// window), 16-31 the sign-extended coefficient.
+// 9-10 the kind (1: a coefficient whose value is in bits 16-31, 2: a size-0
+// symbol with run r < 15 -- end of block, or in a progressive scan the start
+// of an end-of-band run; 0: no shortcut -- a longer code, ZRL, or magnitude
+// bits beyond the window), 16-31 the sign-extended coefficient.
 constexpr int AC_LOOK = 11;
 constexpr uint32_t AC_COEF = 1u << 9, AC_EOB = 2u << 9;
 
@@ -103,7 +104,7 @@ void build_huffman(Huffman &h, const uint8_t counts[16], const uint8_t *symbols,
                 for (int f = 0; f < (1 << shift); f++) {
                     uint32_t e = 0;
                     if (sz == 0) {
-                        if (r != 15) e = (uint32_t)len | AC_EOB;  // end of block; ZRL takes the general path
+                        if (r != 15) e = (uint32_t)len | ((uint32_t)r << 5) | AC_EOB;  // ZRL: general path
                     } else if (len + sz <= AC_LOOK) {
                         const int mag = f >> (shift - sz);  // the sz bits after the code
                         const int v = extend(mag, sz);
@@ -515,8 +516,27 @@ void Decoder::prog_ac_first(Component &c, int16_t *blk, int ss, int se, int al)
     }
     const Huffman &ac = ac_[c.ta];
     if (!ac.present) fail("No AC table for component");
+    const uint32_t *fast_ac = ac.fast_ac.data();
     for (int k = ss; k <= se;) {
-        int rs = decode_huff(ac);
+        if (bitcnt_ < 32) fill_bits();
+        const uint32_t e = fast_ac[bitbuf_ >> (64 - AC_LOOK)];
+        if (e & AC_COEF) {  // code and magnitude bits in one step
+            k += (int)((e >> 5) & 15);
+            if (k > se) fail("Coefficient index out of range: corrupt JPEG");
+            blk[kZigzagToNatural[k]] = (int16_t)((int32_t)(int16_t)(e >> 16) * (1 << al));
+            const int l = (int)(e & 31);
+            bitbuf_ <<= l;
+            bitcnt_ -= l;
+            k++;
+            continue;
+        }
+        if ((e & AC_EOB) && ((e >> 5) & 15) == 0) {  // end of band, no run
+            const int l = (int)(e & 31);
+            bitbuf_ <<= l;
+            bitcnt_ -= l;
+            break;
+        }
+        int rs = decode_huff_nofill(ac);
         int r = rs >> 4, sz = rs & 15;
         if (sz == 0) {
             if (r < 15) {
@@ -605,8 +625,9 @@ void Decoder::decode_scan_progressive(const std::vector<int> &scomp, int ss, int
         }
     };
     auto one_block = [&](Component &c, uint32_t bx, uint32_t by) {
-        int16_t scratch[64] = {0};
+        int16_t scratch[64];
         const bool inside = bx < c.block_w && by < c.block_h;
+        if (!inside) memset(scratch, 0, sizeof(scratch));  // blocks past the rounded plane are decoded and dropped
         int16_t *blk = inside ? &c.coefs[((size_t)by * c.block_w + bx) * 64] : scratch;
         if (ss == 0) {
             if (ah == 0)
