@@ -81,8 +81,10 @@ class Component:
 
 
 def encode(width: int, height: int, comps: List[Component], restart_interval: int = 0,
-           qt_16bit: Optional[Sequence[bool]] = None) -> bytes:
-    """Encode components (coefs shaped (block_h*block_w, 64), natural order)."""
+           qt_16bit: Optional[Sequence[bool]] = None, separate_scans: bool = False) -> bytes:
+    """Encode components (coefs shaped (block_h*block_w, 64), natural order).
+    separate_scans: one non-interleaved scan per component (T.81 A.2.2), each
+    coding the ceil(component samples / 8) blocks of its rows and columns only."""
     out = bytearray(b"\xff\xd8")
     ntab = max(c.table for c in comps) + 1
     for t in range(ntab):
@@ -107,11 +109,38 @@ def encode(width: int, height: int, comps: List[Component], restart_interval: in
     if restart_interval:
         out += b"\xff\xdd" + struct.pack(">HH", 4, restart_interval)
     sel = [0 if i == 0 else 1 for i in range(len(comps))]
-    body = bytes([len(comps)])
-    for i in range(len(comps)):
+    if separate_scans and len(comps) > 1:
+        for ci, c in enumerate(comps):
+            cw = -(-width * c.h // hmax)
+            ch = -(-height * c.v // vmax)
+            units = [[(ci, by * c.block_w + bx)] for by in range(-(-ch // 8)) for bx in range(-(-cw // 8))]
+            out += _scan(comps, [ci], sel, units, restart_interval)
+        return bytes(out + b"\xff\xd9")
+    if len(comps) == 1:
+        c = comps[0]
+        units = [[(0, by * c.block_w + bx)] for by in range((height + 7) // 8) for bx in range((width + 7) // 8)]
+    else:
+        mcu_w = (width + 8 * hmax - 1) // (8 * hmax)
+        mcu_h = (height + 8 * vmax - 1) // (8 * vmax)
+        units = []
+        for my in range(mcu_h):
+            for mx in range(mcu_w):
+                u = []
+                for ci, c in enumerate(comps):
+                    for vv in range(c.v):
+                        for hh in range(c.h):
+                            u.append((ci, (my * c.v + vv) * c.block_w + mx * c.h + hh))
+                units.append(u)
+    return bytes(out + _scan(comps, list(range(len(comps))), sel, units, restart_interval) + b"\xff\xd9")
+
+
+def _scan(comps: List[Component], members: List[int], sel: List[int], units, restart_interval: int) -> bytes:
+    """SOS header for the scan's components plus its entropy-coded data."""
+    body = bytes([len(members)])
+    for i in members:
         body += bytes([i + 1, (sel[i] << 4) | sel[i]])
     body += bytes([0, 63, 0])
-    out += b"\xff\xda" + struct.pack(">H", len(body) + 2) + body
+    out = bytearray(b"\xff\xda" + struct.pack(">H", len(body) + 2) + body)
 
     dc_codes = [_codes(DC_LUMA_BITS, DC_VALS), _codes(DC_CHROMA_BITS, DC_VALS)]
     ac_codes = [_codes(AC_LUMA_BITS, AC_LUMA_VALS), _codes(AC_CHROMA_BITS, AC_CHROMA_VALS)]
@@ -146,32 +175,17 @@ def encode(width: int, height: int, comps: List[Component], restart_interval: in
             code, ln = ac_codes[sel[ci]][0x00]
             bw.put(code, ln)
 
-    if len(comps) == 1:
-        c = comps[0]
-        units = [[(0, by * c.block_w + bx)] for by in range((height + 7) // 8) for bx in range((width + 7) // 8)]
-    else:
-        mcu_w = (width + 8 * hmax - 1) // (8 * hmax)
-        mcu_h = (height + 8 * vmax - 1) // (8 * vmax)
-        units = []
-        for my in range(mcu_h):
-            for mx in range(mcu_w):
-                u = []
-                for ci, c in enumerate(comps):
-                    for vv in range(c.v):
-                        for hh in range(c.h):
-                            u.append((ci, (my * c.v + vv) * c.block_w + mx * c.h + hh))
-                units.append(u)
     rst = 0
     for n, u in enumerate(units):
         if restart_interval and n and n % restart_interval == 0:
             bw.flush()
             bw.out += bytes([0xFF, 0xD0 + (rst & 7)])
             rst += 1
-            preds = [0] * len(comps)
+            preds[:] = [0] * len(comps)
         for ci, bi in u:
             block(ci, comps[ci].coefs[bi])
     bw.flush()
-    out += bw.out + b"\xff\xd9"
+    out += bw.out
     return bytes(out)
 
 

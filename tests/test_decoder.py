@@ -56,6 +56,34 @@ def test_random_roundtrip_bit_exact(seed):
         assert np.array_equal(c.quant_table, qt)
 
 
+@pytest.mark.parametrize("seed,w,h,samp,restart", [
+    (0, 33, 17, [(2, 2), (1, 1), (1, 1)], 0),   # luma: an uncoded block column and row
+    (1, 41, 23, [(2, 2), (1, 1), (1, 1)], 3),   # luma: an uncoded block row
+    (2, 17, 11, [(2, 1), (1, 1), (1, 1)], 0),   # 4:2:2 luma: an uncoded block column
+    (3, 27, 30, [(1, 1), (1, 1), (1, 1)], 2),   # 4:4:4: every block coded
+    (4, 97, 9, [(2, 2), (1, 1), (1, 1)], 5),    # luma: an uncoded block column
+])
+def test_separate_component_scans(seed, w, h, samp, restart):
+    """A sequential stream with one non-interleaved scan per component: each
+    scan codes only the blocks covering its component's samples (T.81 A.2.2),
+    and the blocks of the rounded plane past them decode as zeros."""
+    rng = np.random.default_rng(900 + seed)
+    comps, expect, _ = E.random_image(rng, w, h, samp)
+    hmax, vmax = max(c.h for c in comps), max(c.v for c in comps)
+    for c, (coefs, _, bw, bh, _, _) in zip(comps, expect):
+        coded_w, coded_h = -(-(-(-w * c.h // hmax)) // 8), -(-(-(-h * c.v // vmax)) // 8)
+        for grid in (c.coefs.reshape(bh, bw, 64), coefs.reshape(bh, bw, 64)):
+            grid[:, coded_w:] = 0
+            grid[coded_h:, :] = 0
+    data = E.encode(w, h, comps, restart_interval=restart, separate_scans=True)
+    assert data.count(b"\xff\xda") == len(comps)
+    j = Jpeg.from_source(JpegSource.Buffer(data))
+    for c, (coefs, qt, bw, bh, sh, sv) in zip(j.coefs, expect):
+        assert (c.block_w, c.block_h, c.horizontal_samp_factor, c.vertical_samp_factor) == (bw, bh, sh, sv)
+        assert np.array_equal(c.dct_coefs.reshape(-1, 64), coefs)
+        assert np.array_equal(c.quant_table, qt)
+
+
 def _pixels(c):
     blocks = c.dct_coefs.reshape(-1, 64).astype(np.float64) * c.quant_table[None, :]
     img = np.zeros((c.rounded_px_h, c.rounded_px_w))
