@@ -81,10 +81,12 @@ class Component:
 
 
 def encode(width: int, height: int, comps: List[Component], restart_interval: int = 0,
-           qt_16bit: Optional[Sequence[bool]] = None, separate_scans: bool = False) -> bytes:
+           qt_16bit: Optional[Sequence[bool]] = None, separate_scans: bool = False,
+           omit_scans: Sequence[int] = ()) -> bytes:
     """Encode components (coefs shaped (block_h*block_w, 64), natural order).
     separate_scans: one non-interleaved scan per component (T.81 A.2.2), each
-    coding the ceil(component samples / 8) blocks of its rows and columns only."""
+    coding the ceil(component samples / 8) blocks of its rows and columns only;
+    the components listed in omit_scans get no scan (an incomplete stream)."""
     out = bytearray(b"\xff\xd8")
     ntab = max(c.table for c in comps) + 1
     for t in range(ntab):
@@ -111,6 +113,8 @@ def encode(width: int, height: int, comps: List[Component], restart_interval: in
     sel = [0 if i == 0 else 1 for i in range(len(comps))]
     if separate_scans and len(comps) > 1:
         for ci, c in enumerate(comps):
+            if ci in omit_scans:
+                continue
             cw = -(-width * c.h // hmax)
             ch = -(-height * c.v // vmax)
             units = [[(ci, by * c.block_w + bx)] for by in range(-(-ch // 8)) for bx in range(-(-cw // 8))]

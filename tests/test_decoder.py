@@ -84,6 +84,18 @@ def test_separate_component_scans(seed, w, h, samp, restart):
         assert np.array_equal(c.quant_table, qt)
 
 
+def test_component_without_a_scan_is_zero():
+    """A stream whose last component has no scan: that component's plane
+    decodes as zeros, the others as coded."""
+    rng = np.random.default_rng(77)
+    comps, expect, _ = E.random_image(rng, 48, 32, [(2, 2), (1, 1), (1, 1)])  # every block coded
+    data = E.encode(48, 32, comps, separate_scans=True, omit_scans=(2,))
+    j = Jpeg.from_source(JpegSource.Buffer(data))
+    assert np.array_equal(j.coefs[0].dct_coefs.reshape(-1, 64), expect[0][0])
+    assert np.array_equal(j.coefs[1].dct_coefs.reshape(-1, 64), expect[1][0])
+    assert not np.any(j.coefs[2].dct_coefs)
+
+
 def _pixels(c):
     blocks = c.dct_coefs.reshape(-1, 64).astype(np.float64) * c.quant_table[None, :]
     img = np.zeros((c.rounded_px_h, c.rounded_px_w))
