@@ -31,7 +31,8 @@ class Coefficient:
     block_h: int
     horizontal_samp_factor: int
     vertical_samp_factor: int
-    dct_coefs: np.ndarray  # block_w*block_h*64 values (float32 or int16), block raster, natural order
+    dct_coefs: np.ndarray  # block_w*block_h*64 values (float32 or int16), block raster, natural order;
+    #                        read-only when it views a decoded JPEG (Jpeg.from_source): copy() before editing
     quant_table: np.ndarray  # 64 float32, natural order
 
     @property
@@ -108,12 +109,13 @@ class _NativeJpeg:
 
 
 class _NativePlane:
-    """int16 plane inside a _NativeJpeg, exposed to numpy without a copy; the
-    array keeps this object (and so the decoded image) alive."""
+    """int16 plane inside a _NativeJpeg, exposed to numpy without a copy as a
+    read-only array (copy() it before editing coefficients); the array keeps
+    this object (and so the decoded image) alive."""
 
     def __init__(self, owner: _NativeJpeg, address: int, n: int):
         self._owner = owner
-        self.__array_interface__ = {"data": (address, False), "shape": (n,), "typestr": "<i2", "version": 3}
+        self.__array_interface__ = {"data": (address, True), "shape": (n,), "typestr": "<i2", "version": 3}
 
 
 @dataclass
@@ -133,8 +135,8 @@ class Jpeg:
         rc = lib.art_jpeg_decode(data, len(data), C.byref(handle))
         if rc != N.ART_OK:
             raise ArtefactError(lib.art_last_error().decode("utf-8", "replace"))
-        # The coefficient arrays view the decoder's planes (no copy); the
-        # decoded image is freed with the last of them.
+        # The coefficient arrays are read-only views of the decoder's planes
+        # (no copy); the decoded image is freed with the last of them.
         owner = _NativeJpeg(lib, handle)
         nch, rw, rh = C.c_uint32(), C.c_uint32(), C.c_uint32()
         N.check(lib.art_jpeg_info(handle, C.byref(nch), C.byref(rw), C.byref(rh)))

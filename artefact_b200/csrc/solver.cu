@@ -2250,8 +2250,12 @@ extern "C" int32_t art_compute(uint32_t nchannel, const ArtChannel *coefs, float
 
 // ============================================ allocation-free entry point ====
 //
-// art_solve_noalloc runs the same kernels as art_context_compute_device, but
-// takes every scratch buffer (iterate, FISTA point, gradient, DCT-distance and
+// art_solve_noalloc runs the iteration of a default-options
+// art_context_compute_device solve (decoded start, one FISTA phase) with the
+// narrow gradient sweep and 32-row strips at every size -- equal to it within
+// the parity tolerance, not bit for bit, since the sweep variant and strip
+// height set the summation order -- and takes every scratch buffer (iterate,
+// FISTA point, gradient, DCT-distance and
 // coefficient planes, norm partials, descriptor, work lists) from one
 // file-scope device array of ART_NOALLOC_SCRATCH_BYTES instead of cudaMalloc.
 // It is for callers that must not allocate device memory themselves: callers
@@ -2318,6 +2322,18 @@ int noalloc_scratch(int device, unsigned char **out)
 
 }  // namespace
 }  // namespace art
+
+// Once work is queued on the caller's stream, an error return first waits for
+// that work (ignoring its status), so a later call cannot overlap it on the
+// shared scratch array.
+#define NOALLOC_CUDA(call)                                                                   \
+    do {                                                                                     \
+        cudaError_t e_ = (call);                                                             \
+        if (e_ != cudaSuccess) {                                                             \
+            cudaStreamSynchronize(s);                                                        \
+            return fail(ART_ERR_CUDA, std::string(#call) + ": " + cudaGetErrorString(e_));   \
+        }                                                                                    \
+    } while (0)
 
 extern "C" int32_t art_solve_noalloc(uint32_t nchannel, const ArtChannel *coefs, float weight,
                                      const float pweight[3], uint32_t iterations, uint32_t max_w, uint32_t max_h,
@@ -2429,9 +2445,9 @@ extern "C" int32_t art_solve_noalloc(uint32_t nchannel, const ArtChannel *coefs,
 
     // Clear what must start at zero: the norm partials, counter and error flag,
     // and the first DCT-distance gradient planes.
-    ART_CUDA(cudaMemsetAsync(misc, 0, o_desc - o_misc, s));
+    NOALLOC_CUDA(cudaMemsetAsync(misc, 0, o_desc - o_misc, s));
     for (uint32_t c = 0; c < nch; c++)
-        ART_CUDA(cudaMemsetAsync(d.ch[c].P, 0, (size_t)ppitch[c] * coefs[c].rounded_px_h * sizeof(float), s));
+        NOALLOC_CUDA(cudaMemsetAsync(d.ch[c].P, 0, (size_t)ppitch[c] * coefs[c].rounded_px_h * sizeof(float), s));
     const int nset = std::max(ncta, ntasks);
     k_noalloc_setup<<<(nset + 255) / 256, 256, 0, s>>>(d, ddesc, work, ncta, tasks, ntasks, plan);
     for (uint32_t c = 0; c < nch; c++) {
@@ -2475,14 +2491,14 @@ extern "C" int32_t art_solve_noalloc(uint32_t nchannel, const ArtChannel *coefs,
                 k_project<1, 2><<<grid, PROJ_WARPS * 32, proj_smem<1, 2>(), s>>>(ddesc, tk, n, fnext);
         }
     }
-    ART_CUDA(cudaGetLastError());
+    NOALLOC_CUDA(cudaGetLastError());
     for (uint32_t c = 0; c < nch; c++)
-        ART_CUDA(cudaMemcpy2DAsync(out_planes_device[c], (size_t)out_pitch * sizeof(float), d.x + c * cstride,
+        NOALLOC_CUDA(cudaMemcpy2DAsync(out_planes_device[c], (size_t)out_pitch * sizeof(float), d.x + c * cstride,
                                    (size_t)pitch * sizeof(float), (size_t)W * sizeof(float), H,
                                    cudaMemcpyDeviceToDevice, s));
     unsigned flag = 0;
-    ART_CUDA(cudaMemcpyAsync(&flag, errflag, sizeof(flag), cudaMemcpyDeviceToHost, s));
-    ART_CUDA(cudaStreamSynchronize(s));
+    NOALLOC_CUDA(cudaMemcpyAsync(&flag, errflag, sizeof(flag), cudaMemcpyDeviceToHost, s));
+    NOALLOC_CUDA(cudaStreamSynchronize(s));
     if (flag) return fail(ART_ERR_INVALID_DATA, "coefficients must be integers in [-32768, 32767]");
     return ART_OK;
 }

@@ -28,10 +28,17 @@ real image area.
 * roofline -- the dominant kernel's own I/O bytes per launch over its mean
               launch time, from CUDA event nodes inside the captured graph,
               taken in a separate pass so they do not perturb `value`.
+* iteration -- timed step / iterations against the algorithmic bytes
+              sum_c (20 N + 4 N_c) (the two-sweep minimum).
 * cpu_baseline -- the oracle (fp32 C restatement of pipeline_scalar) on one
-              host thread; a bounded sample, extrapolated when stated.
+              host thread; a bounded sample, extrapolated when stated; with the
+              host's CPU model and core counts.
 * --impl reference -- the oracle as the reference arm, steps spread over the
-              host's threads.
+              host's threads, on inputs from the oracle's own JPEG decoder
+              (oracle/jpeg_oracle.py): that arm never loads the product library.
+* hbm_iteration (1080p run, one GPU) -- the 6000x4000 4:4:4 q30 100-iteration
+              solve, whose working set exceeds L2: iteration time and its
+              fraction of the measured HBM bandwidth on the algorithmic bytes.
 * learned_warm_start (1080p, one GPU) -- the same image through the learned
               warm start: 8 refinement iterations, and the fewest of 8/16/24/32
               that reach the plain 50-iteration objective within 1e-4, with
@@ -106,28 +113,63 @@ def read_traffic(workload, kernel):
     return None
 
 
-def make_workload(kind, keep_bytes=None):
-    """List of decoded Jpeg objects for the workload (their encoded bytes are
-    appended to `keep_bytes` when given)."""
-    from artefact_b200 import synth
-    from artefact_b200.api import Jpeg, JpegSource
+def host_cpu():
+    """Host CPU model, logical CPUs and the CPUs this process may use."""
+    model = "unknown"
+    try:
+        for line in Path("/proc/cpuinfo").read_text().splitlines():
+            if line.startswith("model name"):
+                model = line.split(":", 1)[1].strip()
+                break
+    except OSError:
+        pass
+    try:
+        usable = len(os.sched_getaffinity(0))
+    except AttributeError:
+        usable = os.cpu_count() or 1
+    return {"cpu_model": model, "host_logical_cpus": os.cpu_count() or 1, "host_usable_cpus": usable}
 
-    def dec(data):
-        if keep_bytes is not None:
-            keep_bytes.append(data)
-        return Jpeg.from_source(JpegSource.Buffer(data))
+
+def workload_bytes(kind):
+    """Encoded JPEG bytes of the workload's images (seeded synthetic)."""
+    from artefact_b200 import synth
 
     if kind == "1080p":
-        return [dec(synth.make_jpeg(1920, 1080, 75, "4:2:0", False, seed=2000))]
+        return [synth.make_jpeg(1920, 1080, 75, "4:2:0", False, seed=2000)]
     if kind == "24mp":
-        return [dec(synth.make_jpeg(6000, 4000, 30, "4:4:4", False, seed=3000))]
+        return [synth.make_jpeg(6000, 4000, 30, "4:4:4", False, seed=3000)]
+    if kind == "learned":
+        return [synth.make_jpeg(1920, 1080, q, "4:2:0", False, seed=5000 + q) for q in LEARNED_QUALITIES]
     from concurrent.futures import ThreadPoolExecutor
 
     specs = synth.batch_specs(256, seed=4000)
     with ThreadPoolExecutor(max_workers=min(32, os.cpu_count() or 1)) as ex:
-        datas = list(ex.map(lambda s: synth.make_jpeg(s.width, s.height, s.quality, s.subsampling, False, s.seed),
-                            specs))
-    return [dec(d) for d in datas]
+        return list(ex.map(lambda s: synth.make_jpeg(s.width, s.height, s.quality, s.subsampling, False, s.seed),
+                           specs))
+
+
+def make_workload(kind, keep_bytes=None):
+    """List of decoded Jpeg objects for the workload (the product's host
+    decoder; their encoded bytes are appended to `keep_bytes` when given)."""
+    from artefact_b200.api import Jpeg, JpegSource
+
+    datas = workload_bytes(kind)
+    if keep_bytes is not None:
+        keep_bytes.extend(datas)
+    return [Jpeg.from_source(JpegSource.Buffer(d)) for d in datas]
+
+
+def workload_config(kind, world):
+    """The `config` object of the bench line, the same for both arms."""
+    wl = WORKLOADS[kind]
+    cfg = {"workload": wl["name"], "iterations": 50 if kind == "learned" else wl["iterations"],
+           "images": 256 if kind == "batch256" else (len(LEARNED_QUALITIES) if kind == "learned" else 1),
+           "l2": "flushed between steps (256 MiB write outside the timed events)",
+           "parallelism": f"replicas x{world}"}
+    if kind == "learned":
+        cfg["refine_schedule"] = refine_schedule(REFINE_ITERATIONS)
+        cfg["refine_iterations"] = REFINE_ITERATIONS
+    return cfg
 
 
 class Clocks:
@@ -396,6 +438,74 @@ def learned_comparison(lib, device, steps, warmup, refine=REFINE_ITERATIONS, qua
                 reach_mpix_s=(mp_total / sum(r["min_refine_ms"] for r in rows) * 1e3) if reach else None)
 
 
+def iteration_bytes(jpegs):
+    """Algorithmic bytes of one iteration, sum over images and channels of
+    20 N + 4 N_c (the two-sweep minimum: read x_k, x_{k-1} and the int16
+    coefficients twice, write x_{k+1})."""
+    total = 0
+    for j in jpegs:
+        W, H, _ = j.max_rounded()
+        total += sum(20 * W * H + 4 * co.rounded_px_w * co.rounded_px_h for co in j.coefs)
+    return total
+
+
+def hbm_iteration(lib, device, steps, warmup, peak):
+    """The HBM-bound configuration inside the default run: one 6000x4000
+    4:4:4 q30 image, 100 plain iterations (its ~1.3 GB working set exceeds
+    L2). Whole solves timed with CUDA events (L2 flushed between them), the
+    iteration as solve time / 100 against the algorithmic bytes, and the two
+    kernels' mean launch times from the graph's event nodes (separate pass)."""
+    import torch
+
+    from artefact_b200 import _native as N
+
+    jpegs = make_workload("24mp")
+    j = jpegs[0]
+    iters = WORKLOADS["24mp"]["iterations"]
+    img = DeviceImage(j)
+    ctx = C.c_void_p()
+    N.check(lib.art_context_create(device, C.byref(ctx)))
+    stream = torch.cuda.current_stream()
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")
+    for _ in range(warmup):
+        img.solve(lib, ctx, iters, N.ART_INIT_DECODED, 0, stream)
+    torch.cuda.synchronize()
+    ms = []
+    for k in range(steps):
+        flush.fill_(float(k))
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record(stream)
+        img.solve(lib, ctx, iters, N.ART_INIT_DECODED, 0, stream)
+        b.record(stream)
+        b.synchronize()
+        ms.append(a.elapsed_time(b))
+    N.check(lib.art_context_synchronize(ctx))
+    N.check(lib.art_context_set_timing(ctx, 1))
+    lm, gm, um, nl = C.c_float(), C.c_float(), C.c_float(), C.c_uint32()
+    gs, us = [], []
+    for k in range(2):
+        flush.fill_(float(k))
+        img.solve(lib, ctx, iters, N.ART_INIT_DECODED, 0, stream)
+        N.check(lib.art_context_synchronize(ctx))
+        N.check(lib.art_context_last_timing(ctx, C.byref(lm), C.byref(gm), C.byref(um), C.byref(nl)))
+        gs.append(gm.value / iters)
+        us.append(um.value / iters)
+    N.check(lib.art_context_set_timing(ctx, 0))
+    lib.art_context_destroy(ctx)
+    solve_ms = statistics.median(ms)
+    it_ms = solve_ms / iters
+    ib = iteration_bytes(jpegs)
+    W, H, _ = j.max_rounded()
+    moved = sum(28 * W * H + 10 * co.rounded_px_w * co.rounded_px_h for co in j.coefs)
+    return {"workload": WORKLOADS["24mp"]["name"], "solve_ms": solve_ms, "steps": steps,
+            "mpix_s": j.real_px_w * j.real_px_h / 1e6 / solve_ms * 1e3,
+            "iteration_ms": it_ms, "algorithmic_bytes_per_iteration": ib,
+            "gbs": ib / (it_ms * 1e-3) / 1e9, "frac_of_hbm": ib / (it_ms * 1e-3) / 1e9 / peak,
+            "bytes_moved_per_iteration": moved, "moved_gbs": moved / (it_ms * 1e-3) / 1e9,
+            "gradient_launch_ms": statistics.mean(gs), "projection_launch_ms": statistics.mean(us),
+            "source": "whole 100-iteration solves, CUDA events, L2 flushed between solves; iteration = solve / 100"}
+
+
 def network_flops(H, W):
     """Multiply-add FLOPs (x2) of one forward pass of the warm-start network
     on an H x W component, as executed: its first level is H0 x W0 =
@@ -484,10 +594,7 @@ def run_learned(args, lib, local, rank, world, dist):
             "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f32 solver, bf16 network (fp32 accumulation)",
             "data": "synthetic",
-            "config": {"workload": wl["name"], "refine_iterations": res["refine_iterations"],
-                       "refine_schedule": res["schedule"],
-                       "l2": "flushed between steps (256 MiB write outside the timed events)",
-                       "parallelism": f"replicas x{world}"},
+            "config": workload_config("learned", world),
             "plain50_mpix_s": res["plain50_mpix_s"],
             "speedup_vs_plain50": (value / res["plain50_mpix_s"]) if value else None,
             "refine_iterations_to_reach": [r["min_refine_to_reach"] for r in res["images"]],
@@ -565,27 +672,40 @@ def cpu_sample(kind, jpegs, iterations):
 
 
 def run_reference(args, rank, world):
-    """Reference arm: the oracle port of pipeline_scalar on the host cores."""
+    """Reference arm: the oracle port of pipeline_scalar on the host cores.
+
+    Its inputs come from the oracle's own JPEG decoder (oracle/jpeg_oracle.py)
+    on the same seeded JPEG bytes as the GPU arm, so this arm never loads the
+    product library; only the oracle runs in its timed region."""
     if rank != 0:
         return
     from concurrent.futures import ThreadPoolExecutor
 
     wl = WORKLOADS[args.workload]
-    jpegs = make_workload(args.workload)
-    iters = wl["iterations"]
-    threads = max(1, min(os.cpu_count() or 1, 64))
-    if args.workload == "1080p":
-        work = [jpegs[0]] * args.steps
-        warm = [jpegs[0]] * min(args.warmup, threads)
-        mpix = jpegs[0].real_px_w * jpegs[0].real_px_h / 1e6 * args.steps
-        sample = f"{args.steps} full solves of the workload spread over {threads} host threads"
+    if args.workload == "network":
+        print(json.dumps({"impl": "reference", "metric": wl["metric"],
+                          "unavailable": "the warm-start network has no counterpart in the reference"}), flush=True)
+        return
+    sys.path.insert(0, str(ROOT / "oracle"))
+    import jpeg_oracle
+
+    jpegs = [jpeg_oracle.decode(d) for d in workload_bytes(args.workload)]
+    iters = 50 if args.workload == "learned" else wl["iterations"]
+    cpu = host_cpu()
+    threads = max(1, min(cpu["host_usable_cpus"], 64))
+    if args.workload in ("1080p", "learned"):
+        # Full solves: one image per step (the three qualities in turn for the
+        # learned workload, which the reference solves with plain iterations).
+        work = [jpegs[k % len(jpegs)] for k in range(args.steps)]
+        warm = [jpegs[k % len(jpegs)] for k in range(min(args.warmup, threads))]
+        sample = f"{args.steps} full {iters}-iteration solves of the workload's images spread over {threads} host threads"
     else:
         # Bounded: one image-solve per step (the batch's first images, or a
         # 4-iteration solve of the 24 MP image scaled per iteration).
         work = jpegs[:args.steps] if args.workload == "batch256" else [jpegs[0]] * min(args.steps, 4)
         warm = []
-        mpix = sum(j.real_px_w * j.real_px_h for j in work) / 1e6
         sample = f"{len(work)} image solves of the workload spread over {threads} host threads"
+    mpix = sum(j.real_px_w * j.real_px_h for j in work) / 1e6
     its = iters if args.workload != "24mp" else 4
     with ThreadPoolExecutor(max_workers=threads) as ex:
         list(ex.map(lambda j: oracle_solve(j, its), warm))
@@ -600,10 +720,10 @@ def run_reference(args, rank, world):
         "impl": "reference", "metric": wl["metric"], "value": value, "unit": "MPix/s", "n_gpus": world,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": dt * 1e3 / max(1, len(work)),
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-        "config": {"workload": wl["name"], "iterations": iters},
-        "cpu_baseline": {"value": value, "unit": "MPix/s", "cores": threads, "kind": "port",
-                         "sample": sample + " (fp32 C restatement of pipeline_scalar; the Rust reference is not "
-                                            "buildable here)"},
+        "config": workload_config(args.workload, world),
+        "cpu_baseline": {"value": value, "unit": "MPix/s", "cores": threads, "kind": "port", **cpu,
+                         "sample": sample + " (fp32 C restatement of pipeline_scalar, inputs from the oracle's JPEG "
+                                            "decoder; the Rust reference is not buildable here)"},
         "e2e": {"value": value, "unit": "MPix/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line), flush=True)
@@ -618,6 +738,7 @@ def main():
     ap.add_argument("--workload", default="1080p", choices=sorted(WORKLOADS))
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-learned", action="store_true", help="skip the learned warm-start comparison")
+    ap.add_argument("--no-hbm", action="store_true", help="skip the 6000x4000 HBM iteration block of the default run")
     args = ap.parse_args()
 
     rank = int(os.environ.get("RANK", "0"))
@@ -655,7 +776,7 @@ def main():
             print(json.dumps({"metric": wl["metric"], "value": tflops, "unit": "TFLOP/s", "n_gpus": world,
                               "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True,
                               "scaling": "weak", "vs_baseline": None, "dtype": "bf16 (fp32 accumulation)",
-                              "data": "synthetic", "config": {"workload": wl["name"]},
+                              "data": "synthetic", "config": workload_config("network", world),
                               "roofline": {"bound": "tensor", "achieved": tflops, "peak": peak, "unit": "TFLOP/s",
                                            "frac": tflops / peak, "traffic": None,
                                            "peak_kind": "measured" if peaks else "fallback",
@@ -794,6 +915,7 @@ def main():
         e2e_total = float(t.item())
     e2e_value = world * e2e_steps * mpix / (e2e_total / 1e3)
 
+    it_ms = total_ms / args.steps / iters
     g_launch = statistics.mean(grad_ms) / iters
     u_launch = statistics.mean(upd_ms) / iters
     loop = statistics.mean(loop_ms)
@@ -821,7 +943,14 @@ def main():
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         v, desc = cpu_sample(args.workload, jpegs, iters)
-        cpu = {"value": v, "unit": "MPix/s", "cores": 1, "kind": "port", "sample": desc}
+        cpu = {"value": v, "unit": "MPix/s", "cores": 1, "kind": "port", **host_cpu(),
+               "sample": desc + " on one host thread"}
+
+    # The HBM-bound configuration (6000x4000, 100 iterations) inside the
+    # default run, one GPU.
+    hbm = None
+    if args.workload == "1080p" and world == 1 and not args.no_hbm:
+        hbm = hbm_iteration(lib, local, 3, 1, peak)
 
     # Learned warm start on the same image (1080p only, one GPU): 8 and the
     # fewest ladder iterations that reach the plain 50-iteration objective.
@@ -853,20 +982,25 @@ def main():
             "metric": wl["metric"], "value": value, "unit": "MPix/s", "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": total_ms / args.steps, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-            "config": {"workload": wl["name"], "iterations": iters, "images": nimg,
-                       "l2": "flushed between steps (256 MiB write outside the timed events)",
-                       "parallelism": f"replicas x{world}"},
+            "config": workload_config(args.workload, world),
             "e2e": {"value": e2e_value, "unit": "MPix/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
                     "ms_per_step": e2e_total / e2e_steps,
                     "api": "art_context_compute" if nimg == 1 else "art_context_compute_batch"},
             "roofline": {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": achieved / peak, "traffic": traffic, "peak_kind": peak_kind,
                          "algorithmic_bytes_per_launch": dbytes, "launch_ms": dms},
-            "iteration": {"ms": loop / iters, "gradient_ms": g_launch, "update_ms": u_launch,
-                          "algorithmic_bytes": iter_bytes, "gbs": iter_bytes / (loop / iters * 1e-3) / 1e9,
-                          "frac_of_hbm": iter_bytes / (loop / iters * 1e-3) / 1e9 / peak},
+            # From the timed steps: step time / iterations (the step's start-up
+            # launches included, so this slightly understates the iteration).
+            "iteration": {"ms": it_ms, "algorithmic_bytes": iter_bytes, "gbs": iter_bytes / (it_ms * 1e-3) / 1e9,
+                          "frac_of_hbm": iter_bytes / (it_ms * 1e-3) / 1e9 / peak,
+                          "source": "timed step / iterations"},
+            # Separate pass with event nodes in the graph (not the timed steps).
+            "event_timing_pass": {"loop_ms_per_iteration": loop / iters, "gradient_ms": g_launch,
+                                  "update_ms": u_launch},
             "cpu_baseline": cpu, "gpu_launches": args.steps * per_step, "clocks": clocks, "wall_s": wall,
         }
+        if hbm is not None:
+            line["hbm_iteration"] = hbm
         if learned is not None:
             line["learned_warm_start"] = learned
         if pipe is not None:

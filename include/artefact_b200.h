@@ -225,8 +225,12 @@ int32_t art_context_last_timing(ArtContext *ctx, float *loop_ms, float *gradient
  * memory -- their GPU memory belongs to another allocator (a framework's
  * caching allocator, a server that partitions each GPU up front), or they
  * cannot afford the device-wide synchronisation cudaMalloc/cudaFree may
- * imply. Same kernels and results as art_context_compute_device, but every
- * scratch buffer comes from one fixed 64 MiB array in device memory that the
+ * imply. It runs the iteration of a default-options solve (decoded start, the
+ * reference's step size and one FISTA phase) with the narrow gradient sweep
+ * and 32-row strips whatever the image size, so its result equals
+ * art_context_compute_device's within the parity tolerance (the sweep
+ * variant and strip height change the summation order), not bit for bit.
+ * Every scratch buffer comes from one fixed 64 MiB array in device memory that the
  * library holds on every GPU it is loaded on until the process exits; images
  * that need more (about 1 megapixel per channel) are rejected with
  * ART_ERR_INVALID_ARGUMENT. dct_coefs and out_planes_device are device
@@ -235,6 +239,7 @@ int32_t art_context_last_timing(ArtContext *ctx, float *loop_ms, float *gradient
  * device resolves the array's address there (cudaGetSymbolAddress), so make
  * that first call before any CUDA stream capture. All calls share the array, so
  * calls whose GPU work overlaps race; each call clears what must start at zero.
+ * A call that fails after queueing work waits for that work before returning.
  */
 int32_t art_solve_noalloc(uint32_t nchannel, const ArtChannel *coefs, float weight, const float pweight[3],
                           uint32_t iterations, uint32_t max_rounded_px_w, uint32_t max_rounded_px_h,

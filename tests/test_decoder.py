@@ -219,3 +219,16 @@ def test_corrupted_streams_never_crash(progressive):
             assert all(c.dct_coefs.size == c.block_w * c.block_h * 64 for c in j.coefs)
         except ArtefactError:
             pass
+
+
+def test_decoded_coefficients_are_read_only_views():
+    """Coefficient arrays of a decoded JPEG view the decoder's planes without a
+    copy and are read-only: editing needs an explicit copy()."""
+    j = Jpeg.from_source(JpegSource.Buffer(synth.make_jpeg(40, 24, 50, "4:4:4", True, seed=3)))
+    a = j.coefs[0].dct_coefs
+    assert not a.flags.writeable
+    with pytest.raises(ValueError):
+        a[0] = 1
+    b = a.copy()
+    b[0] += 1
+    assert b[0] == a[0] + 1

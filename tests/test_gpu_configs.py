@@ -1,0 +1,135 @@
+"""Parity at the benchmark configurations' own sizes (GPU).
+
+* 6000-wide 4:4:4 q30 at 100 iterations: a full-width 6000x512 band cut from
+  the 6000x4000 benchmark image (same generator and seed), which stays
+  well-conditioned, so the fixed bar applies: max |GPU - oracle fp32| <= 1.0
+  in 0..255 units, objective within 1e-4 relative, feasibility <= 1e-3.
+* The 256-image batch (seed 4000) solved as one batch through the public
+  batch API: its 4 largest and 4 smallest images against the oracle at 50
+  iterations, with the same bar.
+* The learned path with the shipped trained network on 1920x1080 4:2:0 at
+  q30/50/75: the GPU's ART_INIT_LEARNED solve against the oracle's iteration
+  from the same (GPU-predicted) start (oracle compute_from), at 8 iterations
+  and at the fewest ladder iterations that reach the plain 50-iteration
+  objective within 1e-4; each must be feasible, and the objective reached
+  there must hold on the oracle's planes too.
+
+Oracle runs of different images go to host threads (the oracle releases the
+interpreter lock while it computes).
+"""
+from concurrent.futures import ThreadPoolExecutor
+
+import numpy as np
+import pytest
+
+import oracle_lib as O
+from artefact_b200 import _native as N
+from artefact_b200 import synth
+from artefact_b200 import warmstart as WS
+from artefact_b200.api import Context, Jpeg, JpegSource
+from parity import check_parity
+
+pytestmark = pytest.mark.gpu
+
+WEIGHT, PW = 0.3, [0.001] * 3
+
+
+def _jpeg(data):
+    return Jpeg.from_source(JpegSource.Buffer(data))
+
+
+def test_config3_band_100_iterations(gpu):
+    img = synth.rgb_image(4000, 6000, 3000)[:512]
+    j = _jpeg(synth.encode_jpeg(np.ascontiguousarray(img), 30, "4:4:4"))
+    assert (j.real_px_w, j.real_px_h) == (6000, 512)
+    check_parity(j, 100, label="6000x512 band of the 6000x4000 4:4:4 q30 image")
+
+
+def test_config4_batch_extremes(gpu):
+    specs = synth.batch_specs(256, seed=4000)
+    with ThreadPoolExecutor(max_workers=16) as ex:
+        datas = list(ex.map(lambda s: synth.make_jpeg(s.width, s.height, s.quality, s.subsampling, False, s.seed),
+                            specs))
+    jpegs = [_jpeg(d) for d in datas]
+    with Context(0) as ctx:
+        out = ctx.compute_batch([dict(coefs=j.coefs, weight=WEIGHT, pweight=PW) for j in jpegs], 50)
+    order = sorted(range(len(jpegs)), key=lambda i: jpegs[i].real_px_w * jpegs[i].real_px_h)
+    picks = order[:4] + order[-4:]
+
+    def check(i):
+        j = jpegs[i]
+        check_parity(j, 50, label=f"batch image {i} {j.real_px_w}x{j.real_px_h} q{specs[i].quality} "
+                                  f"{specs[i].subsampling}", gpu=out[i])
+        return i
+
+    with ThreadPoolExecutor(max_workers=len(picks)) as ex:
+        assert sorted(ex.map(check, picks)) == sorted(picks)
+
+
+def _refine(k):
+    """The bench's refinement schedule for k iterations after a learned start."""
+    return dict(step_iterations=2 if k <= 12 else 4, tail_iterations=min(2, k - 1), tail_step_iterations=100)
+
+
+def _prediction(net, j):
+    import torch
+
+    W, H, _ = j.max_rounded()
+    out = []
+    for co in j.coefs:
+        ci = torch.from_numpy(WS.coef_image(co)[None]).cuda()
+        q = torch.from_numpy(np.asarray(co.quant_table, np.float32)[None].copy()).cuda()
+        p = net.predict(ci, q)[0].cpu().numpy()
+        out.append(np.repeat(np.repeat(p, co.vertical_samp_factor, 0), co.horizontal_samp_factor, 1).reshape(H, W))
+    return out
+
+
+@pytest.mark.skipif(not WS.DEFAULT_WEIGHTS.exists(), reason="no trained weights in the package")
+@pytest.mark.parametrize("quality", [30, 50, 75])
+def test_config5_trained_learned_1080p(gpu, quality):
+    j = _jpeg(synth.make_jpeg(1920, 1080, quality, "4:2:0", False, seed=5000 + quality))
+    W, H, _ = j.max_rounded()
+    net = WS.WarmStartNet.load()
+    ctx = Context(0)
+    try:
+        ctx.compute(3, j.coefs, WEIGHT, PW, 50, W, H)
+        e50 = ctx.evaluate()["E"]
+        ctx.set_warm_start(net)
+        reach = None
+        for k in (8, 12, 16, 20, 24, 28, 32, 40, 48):
+            ctx.compute(3, j.coefs, WEIGHT, PW, k, W, H, init_mode=N.ART_INIT_LEARNED, **_refine(k))
+            ev = ctx.evaluate()
+            if ev["E"] <= e50 * (1 + 1e-4) and ev["infeasibility"] <= 1e-3:
+                reach = k
+                break
+        assert reach is not None, "the learned path never reached the plain 50-iteration objective"
+        runs = {}
+        for k in sorted({8, reach}):
+            runs[k] = ctx.compute(3, j.coefs, WEIGHT, PW, k, W, H, init_mode=N.ART_INIT_LEARNED, **_refine(k))
+            runs[k] = (runs[k], ctx.evaluate())
+        ctx.set_warm_start(None)
+        start = _prediction(net, j)
+    finally:
+        ctx.set_warm_start(None)
+        ctx.close()
+        net.close()
+
+    def oracle(k):
+        s = _refine(k)
+        return k, O.compute_from(3, j.coefs, WEIGHT, PW, k, W, H, start, s["step_iterations"],
+                                 tail_iterations=s["tail_iterations"], tail_step_iterations=s["tail_step_iterations"])
+
+    with ThreadPoolExecutor(max_workers=2) as ex:
+        refs = dict(ex.map(oracle, list(runs)))
+    for k, (planes, ev) in runs.items():
+        ref = refs[k]
+        d = max(float(np.abs(a.astype(np.float64) - b).max()) for a, b in zip(planes, ref))
+        er = O.objective(3, j.coefs, WEIGHT, PW, W, H, ref)
+        feas = O.feasibility(3, j.coefs, W, H, planes)
+        print(f"q{quality} K={k}: max|gpu-oracle|={d:.3g} E gpu {ev['E']:.9g} oracle {er:.9g} "
+              f"rel to plain-50 {ev['E'] / e50 - 1:+.2e} feas {feas:.2g} (reaches at K={reach})")
+        assert d <= 1.0
+        assert abs(ev["E"] - er) <= 1e-4 * abs(er)
+        assert feas <= 1e-3 and ev["infeasibility"] <= 1e-3
+        if k == reach:
+            assert er <= e50 * (1 + 2e-4)  # the oracle's planes reach it too (within the parity bar)

@@ -4,10 +4,11 @@ Some callers cannot allocate device memory: their GPU memory belongs to
 another allocator (a framework's caching allocator, or a server that splits
 each GPU up front), or they cannot afford the device-wide synchronisation that
 cudaMalloc and cudaFree may cause. For them the library runs the solver out of
-one fixed device array. This test calls that entry point through the C ABI,
-twice in a row on different images and once more on the first, and checks
-each result against the regular device-resident entry point with the parity
-tolerance the other GPU tests use. It lives in its own file, collected last,
+one fixed device array. This test calls that entry point through the C ABI
+on consecutive calls and checks each result against the regular
+device-resident entry point with the parity
+tolerance the other GPU tests use: 4:2:0, grayscale, 4:4:4 and 4:2:2 images
+one after the other, then the first again. It lives in its own file, collected last,
 and works alone in a fresh process as well as after the other tests.
 """
 import ctypes as C
@@ -68,7 +69,10 @@ def test_noalloc_matches_regular_entry_point_on_consecutive_calls():
     try:
         first = Jpeg.from_source(JpegSource.Buffer(synth.make_jpeg(200, 136, 75, "4:2:0", False, seed=41)))
         second = Jpeg.from_source(JpegSource.Buffer(synth.make_jpeg(96, 80, 50, "4:4:4", True, seed=42)))
-        for j, iters in ((first, 20), (second, 12), (first, 20)):
+        third = Jpeg.from_source(JpegSource.Buffer(synth.make_jpeg(130, 70, 30, "4:4:4", False, seed=43)))
+        fourth = Jpeg.from_source(JpegSource.Buffer(synth.make_jpeg(64, 48, 60, "4:2:2", False, seed=44)))
+        assert second.nchannel == 1 and fourth.coefs[1].horizontal_samp_factor == 2
+        for j, iters in ((first, 20), (second, 12), (third, 15), (fourth, 10), (first, 20)):
             got = _solve("noalloc", j, iters, torch)
             ref = _solve("regular", j, iters, torch, ctx)
             for a, b in zip(got, ref):
