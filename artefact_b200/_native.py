@@ -47,7 +47,8 @@ class ArtOptions(C.Structure):
         ("step_iterations", C.c_uint32),
         ("tail_iterations", C.c_uint32),
         ("tail_step_iterations", C.c_uint32),
-        ("reserved", C.c_uint32 * 3),
+        ("step_decay", C.c_float),
+        ("reserved", C.c_uint32 * 2),
     ]
 
 
@@ -61,6 +62,27 @@ class ArtImage(C.Structure):
         ("weight", C.c_float),
         ("pweight", C.c_float * 3),
         ("out_planes", C.POINTER(C.c_void_p)),
+    ]
+
+
+class ArtProcessImage(C.Structure):
+    _fields_ = [
+        ("nchannel", C.c_uint32),
+        ("real_w", C.c_uint32),
+        ("real_h", C.c_uint32),
+        ("reserved", C.c_uint32),
+        ("channels", C.POINTER(ArtChannel)),
+        ("weight", C.c_float * 3),
+        ("pweight", C.c_float * 3),
+        ("rgb_out", C.c_void_p),
+    ]
+
+
+class ArtTuneResult(C.Structure):
+    _fields_ = [
+        ("variant", C.c_uint32), ("strip_rows", C.c_uint32), ("proj_warps", C.c_uint32),
+        ("candidates", C.c_uint32), ("best_ms", C.c_float), ("heuristic_ms", C.c_float),
+        ("heuristic_variant", C.c_uint32), ("heuristic_strip_rows", C.c_uint32),
     ]
 
 
@@ -119,9 +141,14 @@ EXPORTS = {
                                               C.POINTER(ArtOptions)]),
     "art_context_compute_batch_device": (C.c_int32, [C.c_void_p, C.c_uint32, C.POINTER(ArtImage), C.c_uint32,
                                                      C.POINTER(ArtOptions), C.c_void_p]),
+    "art_context_process_batch": (C.c_int32, [C.c_void_p, C.c_uint32, C.POINTER(ArtProcessImage), C.c_uint32,
+                                              C.c_int32, C.POINTER(ArtOptions)]),
     "art_context_autotune": (C.c_int32, [C.c_void_p, C.c_uint32, C.POINTER(C.c_uint32), C.POINTER(C.c_uint32),
                                          C.c_uint32, C.c_uint32, C.c_uint32, C.POINTER(C.c_uint32),
                                          C.POINTER(C.c_uint32)]),
+    "art_context_autotune_batch": (C.c_int32, [C.c_void_p, C.c_uint32, C.POINTER(ArtImage), C.c_uint32,
+                                               C.POINTER(ArtTuneResult)]),
+    "art_context_last_tune": (C.c_int32, [C.c_void_p, C.POINTER(ArtTuneResult)]),
     "art_context_tune_cache": (C.c_int32, [C.c_void_p, C.c_char_p, C.c_int32]),
     "art_context_synchronize": (C.c_int32, [C.c_void_p]),
     "art_context_set_warm_start": (C.c_int32, [C.c_void_p, C.c_void_p]),

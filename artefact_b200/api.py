@@ -163,13 +163,14 @@ class ArtefactError(RuntimeError):
 
 
 def _options(init_mode: int, device: int, step_iterations: int = 0, tail_iterations: int = 0,
-             tail_step_iterations: int = 0) -> N.ArtOptions:
+             tail_step_iterations: int = 0, step_decay: float = 0.0) -> N.ArtOptions:
     o = N.ArtOptions()
     o.init_mode = init_mode
     o.device = device
     o.step_iterations = int(step_iterations)
     o.tail_iterations = int(tail_iterations)
     o.tail_step_iterations = int(tail_step_iterations)
+    o.step_decay = float(step_decay)
     return o
 
 
@@ -318,6 +319,53 @@ def process_jpeg(jpeg: Jpeg, weight: Sequence[float], pweight: Sequence[float], 
     return rgb
 
 
+def process_jpegs(jpegs: Sequence[Jpeg], weight: Sequence[float], pweight: Sequence[float],
+                  iterations: Sequence[int], separate: bool, *, init_mode: int = N.ART_INIT_DECODED,
+                  device: int = -1, context: Optional["Context"] = None) -> List[np.ndarray]:
+    """:func:`process_jpeg` for many decoded images, solved as one batch
+    (``art_context_process_batch``): the RGB8 image of each, in order, equal
+    to what :func:`process_jpeg` returns for it. The batch runs one iteration
+    count: ``iterations[0]`` for joint solves (as the reference, lib.rs:122-132);
+    in separate mode with different per-component counts the images go one by
+    one through :func:`process_jpeg` instead."""
+    jpegs = list(jpegs)
+    if not jpegs:
+        return []
+    its = [int(v) for v in iterations]
+    counts = {its[0]} if not separate and all(j.nchannel == 3 for j in jpegs) else set(
+        its[min(c, len(its) - 1)] for j in jpegs for c in range(j.nchannel if j.nchannel != 3 or separate else 1))
+    if len(counts) != 1:
+        return [process_jpeg(j, weight, pweight, iterations, separate, init_mode=init_mode, device=device,
+                             context=context) for j in jpegs]
+    lib = N.lib()
+    keep: list = []
+    imgs = (N.ArtProcessImage * len(jpegs))()
+    outs = []
+    w3 = [float(v) for v in (list(weight) + [0.0] * 3)[:3]]
+    pw3 = [float(v) for v in (list(pweight) + [0.0] * 3)[:3]]
+    for i, j in enumerate(jpegs):
+        chans = (N.ArtChannel * j.nchannel)(*[c.as_c(keep) for c in j.coefs])
+        keep.append(chans)
+        rgb = np.empty((j.real_px_h, j.real_px_w, 3), dtype=np.uint8)
+        outs.append(rgb)
+        im = imgs[i]
+        im.nchannel, im.real_w, im.real_h = j.nchannel, j.real_px_w, j.real_px_h
+        im.channels = C.cast(chans, C.POINTER(N.ArtChannel))
+        im.weight = (C.c_float * 3)(*w3)
+        im.pweight = (C.c_float * 3)(*pw3)
+        im.rgb_out = rgb.ctypes.data
+    handle = context.handle if context is not None else _context(device)
+    N.check(lib.art_context_process_batch(handle, len(jpegs), imgs, counts.pop(), int(bool(separate)),
+                                          C.byref(_options(init_mode, device))))
+    return outs
+
+
+def _tune_dict(r) -> dict:
+    return dict(variant=r.variant, strip_rows=r.strip_rows, proj_warps=r.proj_warps, candidates=r.candidates,
+                best_ms=r.best_ms, heuristic_ms=r.heuristic_ms, heuristic_variant=r.heuristic_variant,
+                heuristic_strip_rows=r.heuristic_strip_rows)
+
+
 class Context:
     """An explicit solver context (``art_context_*``): one CUDA stream, device
     buffers, the captured iteration graph and the autotuner's cache, reused
@@ -364,7 +412,7 @@ class Context:
     def compute(self, nchannel: int, coefs: Sequence[Coefficient], weight: float, pweight: Sequence[float],
                 iterations: int, max_rounded_px_w: int, max_rounded_px_h: int,
                 init_mode: int = N.ART_INIT_DECODED, step_iterations: int = 0, tail_iterations: int = 0,
-                tail_step_iterations: int = 0) -> List[np.ndarray]:
+                tail_step_iterations: int = 0, step_decay: float = 0.0) -> List[np.ndarray]:
         keep: list = []
         chans = (N.ArtChannel * nchannel)(*[coefs[c].as_c(keep) for c in range(nchannel)])
         pw = (C.c_float * 3)(*[float(v) for v in list(pweight)[:3]])
@@ -373,17 +421,25 @@ class Context:
         N.check(N.lib().art_context_compute(self._h, nchannel, chans, float(weight), pw, int(iterations),
                                             max_rounded_px_w, max_rounded_px_h, ptrs,
                                             C.byref(_options(init_mode, -1, step_iterations, tail_iterations,
-                                                             tail_step_iterations))))
+                                                             tail_step_iterations, step_decay))))
         return outs
 
     def compute_batch(self, jobs: Sequence[dict], iterations: int, init_mode: int = N.ART_INIT_DECODED,
                       step_iterations: int = 0, tail_iterations: int = 0,
-                      tail_step_iterations: int = 0) -> List[List[np.ndarray]]:
+                      tail_step_iterations: int = 0, step_decay: float = 0.0) -> List[List[np.ndarray]]:
         """Solve many images together (one launch per kernel and iteration over
         all of them, the loop in one CUDA graph). Each job is a dict with keys
         ``coefs`` (list of :class:`Coefficient`), ``weight``, ``pweight`` and
         optionally ``nchannel``, ``max_w``, ``max_h`` (default: from the coefs)."""
         keep: list = []
+        imgs, results = self._images(jobs, keep)
+        N.check(N.lib().art_context_compute_batch(self._h, len(jobs), imgs, int(iterations),
+                                                  C.byref(_options(init_mode, -1, step_iterations, tail_iterations,
+                                                                   tail_step_iterations, step_decay))))
+        return results
+
+    def _images(self, jobs: Sequence[dict], keep: list):
+        """ArtImage array of host coefficients (and host output planes) for `jobs`."""
         imgs = (N.ArtImage * len(jobs))()
         results = []
         for i, job in enumerate(jobs):
@@ -403,10 +459,23 @@ class Context:
             im.pweight = (C.c_float * 3)(*[float(v) for v in (pw + [0.0] * 3)[:3]])
             im.out_planes = C.cast(ptrs, C.POINTER(C.c_void_p))
             results.append(outs)
-        N.check(N.lib().art_context_compute_batch(self._h, len(jobs), imgs, int(iterations),
-                                                  C.byref(_options(init_mode, -1, step_iterations, tail_iterations,
-                                                                   tail_step_iterations))))
-        return results
+        return imgs, results
+
+    def autotune_batch(self, jobs: Sequence[dict], iterations: int = 10) -> dict:
+        """Tune the launch shapes on this batch of images (jobs as for
+        :meth:`compute_batch`); later batches of its bucket use the choice.
+        Returns the choice and the timings (``art_context_autotune_batch``)."""
+        keep: list = []
+        imgs, _ = self._images(jobs, keep)
+        r = N.ArtTuneResult()
+        N.check(N.lib().art_context_autotune_batch(self._h, len(jobs), imgs, int(iterations), C.byref(r)))
+        return _tune_dict(r)
+
+    def last_tune(self) -> dict:
+        """Choice and timings of the last autotune run on this context."""
+        r = N.ArtTuneResult()
+        N.check(N.lib().art_context_last_tune(self._h, C.byref(r)))
+        return _tune_dict(r)
 
     def autotune(self, nchannel: int, samp_h: Sequence[int], samp_v: Sequence[int], max_w: int, max_h: int,
                  iterations: int = 10) -> tuple:

@@ -474,6 +474,283 @@ __global__ void __launch_bounds__(SWEEP_WARPS_N * 32, SWEEP_MIN_BLOCKS_N) k_grad
     }
 }
 
+// Quad variant of the gradient sweep: lane L holds the four columns
+// x0 = xs - 4 + 4L .. x0 + 3 as two float2 pairs, loaded and stored as float4,
+// with packed FP32x2 arithmetic. Horizontal neighbours inside a lane are
+// registers; across lanes each row needs two shuffles for the y values (the
+// next row's edge values, carried to the following step) and four for the
+// gathered terms, against seven per pixel in the narrow variant. Lanes 1..30
+// write g, so a warp's strip is SWEEP_OUT_Q = 120 columns and every access is
+// 16-byte aligned (W is a multiple of 8, so a lane's four columns are all
+// inside the image or all outside it). Every per-pixel expression is the wide
+// variant's, in the same order, so both give the same g. Rows and columns
+// outside the image are read clamped and their terms are zero, as in the
+// other variants.
+__device__ __forceinline__ float4 ldg4_clamped(const float *row, int x0, bool inside, int W)
+{
+    if (inside) return __ldg(reinterpret_cast<const float4 *>(row + x0));
+    const float v = __ldg(row + (x0 < 0 ? 0 : W - 1));
+    return make_float4(v, v, v, v);
+}
+
+template <int NCH>
+__global__ void __launch_bounds__(SWEEP_WARPS_Q * 32, SWEEP_MIN_BLOCKS_Q) k_grad_sweep_q(
+    const ImgDev *__restrict__ imgs, const int2 *__restrict__ work, float stepmul)
+{
+    __shared__ float s_red[SWEEP_WARPS_Q][NCH];
+    __shared__ double s_dred[SWEEP_WARPS_Q][NCH];
+    __shared__ int s_last;
+    const unsigned FULL = 0xffffffffu;
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int2 wk = work[blockIdx.x];
+    const ImgDev &im = imgs[wk.x];
+    const int W = im.W, H = im.H, pitch = im.pitch, R = im.strip_rows;
+    const int strip = wk.y * SWEEP_WARPS_Q + warp;
+    float2 ssq[NCH];
+#pragma unroll
+    for (int c = 0; c < NCH; c++) ssq[c] = make_float2(0.f, 0.f);
+
+    if (strip < im.nstrips) {
+        const int sxi = strip % im.strips_x, syi = strip / im.strips_x;
+        const int xs = sxi * SWEEP_OUT_Q, ys = syi * R;
+        const int x0 = xs - 4 + 4 * lane;
+        const bool colin = x0 >= 0 && x0 < W;      // all four columns inside (W % 8 == 0)
+        const bool outlane = lane >= 1 && lane <= 30 && x0 < W;
+        const bool lft = x0 > 0;                   // column x0 has a left neighbour in the image
+        const int cs = (int)im.cstride;
+        float *gout = im.g + (outlane ? x0 : 0);
+        const float2 at = make_float2(im.alpha_tv, im.alpha_tv), ag = make_float2(im.alpha_tgv, im.alpha_tgv);
+        const float2 half2 = make_float2(0.5f, 0.5f), two2 = make_float2(2.f, 2.f);
+        const float *pbase = im.ch[0].P;
+        int pcol[NCH], psh[NCH], ppitch[NCH];
+        bool pon[NCH], pshare[NCH];
+#pragma unroll
+        for (int c = 0; c < NCH; c++) {
+            const ChanDev &cd = im.ch[c];
+            pon[c] = cd.alpha_p != 0.f;
+            psh[c] = cd.sv - 1;
+            ppitch[c] = cd.ppitch;
+            pshare[c] = cd.sh == 2;  // columns 2k, 2k + 1 are one component sample
+            pcol[c] = (int)(cd.P - pbase) + (outlane ? (x0 >> (cd.sh - 1)) : 0);
+        }
+        const int Hm1 = H - 1;
+        auto ld = [&](int c, int off) -> float4 { return ldg4_clamped(im.y + c * cs + off, x0, colin, W); };
+        auto pld = [&](int c, int row) -> float4 {
+            if (!pon[c] || !outlane) return make_float4(0.f, 0.f, 0.f, 0.f);
+            const float *p = pbase + pcol[c] + (row >> psh[c]) * ppitch[c];
+            if (pshare[c]) {
+                const float2 v = __ldg(reinterpret_cast<const float2 *>(p));
+                return make_float4(v.x, v.x, v.y, v.y);
+            }
+            return __ldg(reinterpret_cast<const float4 *>(p));
+        };
+        auto lo2 = [](float4 v) { return make_float2(v.x, v.y); };
+        auto hi2 = [](float4 v) { return make_float2(v.z, v.w); };
+
+        // Per channel: the current row yv, its neighbours' edge values yl =
+        // y[x0 - 1], yr = y[x0 + 4], the previous row's differences, the three
+        // output-row accumulators and the rows in flight (ring: y rows t + 1 + k,
+        // pring: DCT-distance rows t - 1 + k at step t).
+        float4 yv[NCH], ring[NCH][SWEEP_PF_Q], pring[NCH][SWEEP_PPF_Q];
+        float yl[NCH], yr[NCH];
+        float2 dxpa[NCH], dxpb[NCH], dypa[NCH], dypb[NCH];
+        float2 Gma[NCH], Gmb[NCH], G0a[NCH], G0b[NCH], Gpa[NCH], Gpb[NCH];
+        {
+            const int o0 = min(max(ys - 2, 0), Hm1) * pitch, o1 = min(max(ys - 1, 0), Hm1) * pitch;
+#pragma unroll
+            for (int c = 0; c < NCH; c++) {
+                const float4 y0 = ld(c, o0);
+                yv[c] = ld(c, o1);
+#pragma unroll
+                for (int k = 0; k < SWEEP_PF_Q; k++) ring[c][k] = ld(c, min(ys + k, Hm1) * pitch);
+#pragma unroll
+                for (int k = 0; k < SWEEP_PPF_Q; k++) pring[c][k] = pld(c, min(max(ys - 2 + k, 0), Hm1));
+                // Differences of row ys - 2 (the first step's previous row).
+                const float y0r = __shfl_down_sync(FULL, y0.x, 1);
+                dxpa[c] = f2sub(make_float2(y0.y, y0.z), lo2(y0));
+                dxpb[c] = f2sub(make_float2(y0.w, y0r), hi2(y0));
+                dypa[c] = f2sub(lo2(yv[c]), lo2(y0));
+                dypb[c] = f2sub(hi2(yv[c]), hi2(y0));
+                yl[c] = __shfl_up_sync(FULL, yv[c].w, 1);
+                yr[c] = __shfl_down_sync(FULL, yv[c].x, 1);
+                Gma[c] = Gmb[c] = G0a[c] = G0b[c] = Gpa[c] = Gpb[c] = make_float2(0.f, 0.f);
+            }
+        }
+#pragma unroll 1
+        for (int t = ys - 1; t <= ys + R; t++) {
+            float4 yn[NCH], pr[NCH];
+            float nl[NCH], nr[NCH];
+            {
+                const int o = min(t + 1 + SWEEP_PF_Q, Hm1) * pitch;
+                const int prow = min(max(t - 1 + SWEEP_PPF_Q, 0), Hm1);
+#pragma unroll
+                for (int c = 0; c < NCH; c++) {
+                    yn[c] = ring[c][0];
+#pragma unroll
+                    for (int k = 0; k + 1 < SWEEP_PF_Q; k++) ring[c][k] = ring[c][k + 1];
+                    ring[c][SWEEP_PF_Q - 1] = ld(c, o);
+                    pr[c] = pring[c][0];
+#pragma unroll
+                    for (int k = 0; k + 1 < SWEEP_PPF_Q; k++) pring[c][k] = pring[c][k + 1];
+                    pring[c][SWEEP_PPF_Q - 1] = pld(c, prow);
+                    nl[c] = __shfl_up_sync(FULL, yn[c].w, 1);
+                    nr[c] = __shfl_down_sync(FULL, yn[c].x, 1);
+                }
+            }
+            const bool rowin = colin && t >= 0 && t < H, ty0 = t > 0;
+            float2 dxa[NCH], dxb[NCH], dya[NCH], dyb[NCH], gxxa[NCH], gxxb[NCH], gyya[NCH], gyyb[NCH];
+            float2 gsa[NCH], gsb[NCH];
+            float2 n1a = make_float2(0.f, 0.f), n1b = n1a, n2a = n1a, n2b = n1a;
+#pragma unroll
+            for (int c = 0; c < NCH; c++) {
+                const float4 y = yv[c];
+                dxa[c] = f2sub(make_float2(y.y, y.z), lo2(y));
+                dxb[c] = f2sub(make_float2(y.w, yr[c]), hi2(y));
+                dya[c] = f2sub(lo2(yn[c]), lo2(y));
+                dyb[c] = f2sub(hi2(yn[c]), hi2(y));
+                n1a = f2fma(dxa[c], dxa[c], n1a);
+                n1a = f2fma(dya[c], dya[c], n1a);
+                n1b = f2fma(dxb[c], dxb[c], n1b);
+                n1b = f2fma(dyb[c], dyb[c], n1b);
+            }
+#pragma unroll
+            for (int c = 0; c < NCH; c++) {
+                // Backward differences are zero at the left edge and the top row
+                // (compute_step_tv2.rs:53-69): take the neighbour equal to self.
+                const float dxs = yv[c].x - yl[c], dys = nl[c] - yl[c];  // dx, dy at x0 - 1
+                const float2 dxla = make_float2(lft ? dxs : dxa[c].x, dxa[c].x);
+                const float2 dyla = make_float2(lft ? dys : dya[c].x, dya[c].x);
+                const float2 dxlb = make_float2(dxa[c].y, dxb[c].x);
+                const float2 dylb = make_float2(dya[c].y, dyb[c].x);
+                const float2 dxua = ty0 ? dxpa[c] : dxa[c], dyua = ty0 ? dypa[c] : dya[c];
+                const float2 dxub = ty0 ? dxpb[c] : dxb[c], dyub = ty0 ? dypb[c] : dyb[c];
+                const float2 axxa = f2sub(dxa[c], dxla), ayxa = f2sub(dya[c], dyla);
+                const float2 axxb = f2sub(dxb[c], dxlb), ayxb = f2sub(dyb[c], dylb);
+                const float2 ayya = f2sub(dya[c], dyua), axya = f2sub(dxa[c], dxua);
+                const float2 ayyb = f2sub(dyb[c], dyub), axyb = f2sub(dxb[c], dxub);
+                const float2 sa = f2mul(half2, f2add(axya, ayxa)), sb = f2mul(half2, f2add(axyb, ayxb));
+                n2a = f2add(n2a, f2fma(ayya, ayya, f2fma(two2, f2mul(sa, sa), f2mul(axxa, axxa))));
+                n2b = f2add(n2b, f2fma(ayyb, ayyb, f2fma(two2, f2mul(sb, sb), f2mul(axxb, axxb))));
+                gxxa[c] = axxa;
+                gxxb[c] = axxb;
+                gyya[c] = ayya;
+                gyyb[c] = ayyb;
+                gsa[c] = sa;
+                gsb[c] = sb;
+            }
+            float2 inv1a, inv1b, inv2a, inv2b;
+            inv1a.x = (rowin && n1a.x > 0.f) ? rsqrtf(n1a.x) : 0.f;
+            inv1a.y = (rowin && n1a.y > 0.f) ? rsqrtf(n1a.y) : 0.f;
+            inv1b.x = (rowin && n1b.x > 0.f) ? rsqrtf(n1b.x) : 0.f;
+            inv1b.y = (rowin && n1b.y > 0.f) ? rsqrtf(n1b.y) : 0.f;
+            inv2a.x = (rowin && n2a.x > 0.f) ? rsqrtf(n2a.x) : 0.f;
+            inv2a.y = (rowin && n2a.y > 0.f) ? rsqrtf(n2a.y) : 0.f;
+            inv2b.x = (rowin && n2b.x > 0.f) ? rsqrtf(n2b.x) : 0.f;
+            inv2b.y = (rowin && n2b.y > 0.f) ? rsqrtf(n2b.y) : 0.f;
+            const float2 at1a = f2mul(at, inv1a), at1b = f2mul(at, inv1b);
+            const float2 ag2a = f2mul(ag, inv2a), ag2b = f2mul(ag, inv2b);
+#pragma unroll
+            for (int c = 0; c < NCH; c++) {
+                const float2 aa = f2mul(at1a, dxa[c]), ab = f2mul(at1b, dxb[c]);
+                const float2 ba = f2mul(at1a, dya[c]), bb = f2mul(at1b, dyb[c]);
+                const float2 ua = f2mul(ag2a, f2add(gsa[c], gxxa[c])), ub = f2mul(ag2b, f2add(gsb[c], gxxb[c]));
+                const float2 va = f2mul(ag2a, f2add(gyya[c], gsa[c])), vb = f2mul(ag2b, f2add(gyyb[c], gsb[c]));
+                const float2 wa = f2mul(ag2a, gsa[c]), wb = f2mul(ag2b, gsb[c]);
+                const float2 aua = f2add(aa, ua), aub = f2add(ab, ub);
+                const float aul = __shfl_up_sync(FULL, aub.y, 1);   // (a + u) at x0 - 1
+                const float ur = __shfl_down_sync(FULL, ua.x, 1);   // u at x0 + 4
+                const float wr = __shfl_down_sync(FULL, wa.x, 1);   // w at x0 + 4
+                const float wl = __shfl_up_sync(FULL, wb.y, 1);     // w at x0 - 1
+                // centre term -(a + b) - 2 (u + v - w), then the neighbours' a + u and u
+                const float2 cena = f2fma(two2, f2sub(f2add(ua, va), wa), f2add(aa, ba));
+                const float2 cenb = f2fma(two2, f2sub(f2add(ub, vb), wb), f2add(ab, bb));
+                G0a[c] = f2add(f2sub(G0a[c], cena), f2add(make_float2(aul, aua.x), make_float2(ua.y, ub.x)));
+                G0b[c] = f2add(f2sub(G0b[c], cenb), f2add(make_float2(aua.y, aub.x), make_float2(ub.y, ur)));
+                Gpa[c] = f2add(Gpa[c], f2sub(f2add(ba, va), make_float2(wa.y, wb.x)));
+                Gpb[c] = f2add(Gpb[c], f2sub(f2add(bb, vb), make_float2(wb.y, wr)));
+                Gma[c] = f2add(Gma[c], f2sub(va, make_float2(wl, wa.x)));
+                Gmb[c] = f2add(Gmb[c], f2sub(vb, make_float2(wa.y, wb.x)));
+                dxpa[c] = dxa[c];
+                dxpb[c] = dxb[c];
+                dypa[c] = dya[c];
+                dypb[c] = dyb[c];
+                yv[c] = yn[c];
+                yl[c] = nl[c];
+                yr[c] = nr[c];
+            }
+            const int ro = t - 1;
+            if (outlane && ro >= ys && ro < ys + R && ro < H) {
+                const int go = ro * pitch;
+#pragma unroll
+                for (int c = 0; c < NCH; c++) {
+                    const float2 ga = f2add(Gma[c], lo2(pr[c])), gb = f2add(Gmb[c], hi2(pr[c]));
+                    *reinterpret_cast<float4 *>(gout + c * cs + go) = make_float4(ga.x, ga.y, gb.x, gb.y);
+                    ssq[c] = f2fma(ga, ga, ssq[c]);
+                    ssq[c] = f2fma(gb, gb, ssq[c]);
+                }
+            }
+#pragma unroll
+            for (int c = 0; c < NCH; c++) {
+                Gma[c] = G0a[c];
+                Gmb[c] = G0b[c];
+                G0a[c] = Gpa[c];
+                G0b[c] = Gpb[c];
+                Gpa[c] = Gpb[c] = make_float2(0.f, 0.f);
+            }
+        }
+    }
+
+    // Fixed-order reduction: warp tree, then warps in order, then blocks in order.
+#pragma unroll
+    for (int c = 0; c < NCH; c++) {
+        float s = ssq[c].x + ssq[c].y;
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(FULL, s, o);
+        if (lane == 0) s_red[warp][c] = s;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+#pragma unroll
+        for (int c = 0; c < NCH; c++) {
+            float s = 0.f;
+            for (int w = 0; w < SWEEP_WARPS_Q; w++) s += s_red[w][c];
+            im.partial[wk.y * 4 + c] = s;
+        }
+        __threadfence();
+        const unsigned done = atomicAdd(im.counter, 1u);
+        s_last = done == (unsigned)(im.ncta - 1);
+    }
+    __syncthreads();
+    if (s_last) {
+        __threadfence();
+        double acc[NCH];
+#pragma unroll
+        for (int c = 0; c < NCH; c++) acc[c] = 0.0;
+        for (int t = threadIdx.x; t < im.ncta; t += SWEEP_WARPS_Q * 32) {
+#pragma unroll
+            for (int c = 0; c < NCH; c++) acc[c] += (double)__ldcg(im.partial + t * 4 + c);
+        }
+#pragma unroll
+        for (int c = 0; c < NCH; c++) {
+            double s = acc[c];
+#pragma unroll
+            for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(FULL, s, o);
+            if (lane == 0) s_dred[warp][c] = s;
+        }
+        __syncthreads();
+        if (threadIdx.x == 0) {
+#pragma unroll
+            for (int c = 0; c < NCH; c++) {
+                double s = 0.0;
+                for (int w = 0; w < SWEEP_WARPS_Q; w++) s += s_dred[w][c];
+                const double nrm = sqrt(s);
+                im.sigma[c] = nrm > 0.0 ? (float)((double)(im.step * stepmul) / nrm) : 0.f;
+            }
+            atomicExch(im.counter, 0u);
+        }
+    }
+}
+
 // Descent step and projection of coefficient blocks (compute_step.rs:60-71,
 // compute_projection.rs:8-122), the next FISTA point, and the next
 // DCT-distance gradient (compute_step_prob.rs:20-57) from the clamped
@@ -495,17 +772,17 @@ struct ProjShape {
     static constexpr int REGION = NR * RS;  // floats per staged plane
 };
 
-template <int SH, int SV>
-__global__ void __launch_bounds__(PROJ_WARPS * 32) k_project(const ImgDev *__restrict__ imgs,
-                                                            const int4 *__restrict__ tasks, int ntasks, float fnext)
+template <int SH, int SV, int PW = PROJ_WARPS>
+__global__ void __launch_bounds__(PW * 32) k_project(const ImgDev *__restrict__ imgs,
+                                                    const int4 *__restrict__ tasks, int ntasks, float fnext)
 {
     using S = ProjShape<SH, SV>;
     constexpr bool SUB = SH * SV > 1;
     constexpr int NR = S::NR, NC = S::NC, RS = S::RS;
     extern __shared__ float4 s_dyn[];
-    __shared__ float s_t[PROJ_WARPS][2][4][8][9];
+    __shared__ float s_t[PW][2][4][8][9];
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const int w = blockIdx.x * PROJ_WARPS + warp;
+    const int w = blockIdx.x * PW + warp;
     if (w >= ntasks) return;  // warp-uniform
     float *sy_ = reinterpret_cast<float *>(s_dyn) + warp * 2 * S::REGION;  // y region; g, then x region
     float *sg_ = sy_ + S::REGION, *sx_ = sg_;
@@ -972,17 +1249,18 @@ std::vector<float> fista_factors(uint32_t iterations)
 }
 
 struct GraphKey {
-    int nimg = 0, wcount[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+    int nimg = 0, proj_warps = 0, wcount[12] = {0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0};
     int mode_off[5] = {0, 0, 0, 0, 0};
     uint32_t iterations = 0, tail = 0;
-    float tail_stepmul = 1.0f;
+    float tail_stepmul = 1.0f, decay = 0.0f;
     bool timing = false;
     const void *desc = nullptr, *work = nullptr, *tasks = nullptr;
     bool operator==(const GraphKey &o) const
     {
-        return nimg == o.nimg && iterations == o.iterations && tail == o.tail && tail_stepmul == o.tail_stepmul &&
+        return nimg == o.nimg && proj_warps == o.proj_warps && iterations == o.iterations && tail == o.tail &&
+               tail_stepmul == o.tail_stepmul && decay == o.decay &&
                timing == o.timing && desc == o.desc &&
-               work == o.work && tasks == o.tasks && std::equal(wcount, wcount + 8, o.wcount) &&
+               work == o.work && tasks == o.tasks && std::equal(wcount, wcount + 12, o.wcount) &&
                std::equal(mode_off, mode_off + 5, o.mode_off);
     }
 };
@@ -998,6 +1276,12 @@ struct ImageSpec {
 };
 
 }  // namespace
+
+// Launch shapes of one geometry bucket: gradient-sweep variant (0 narrow, 1
+// wide), strip rows, projection warps per block.
+struct TuneChoice {
+    int kind = 0, rows = 0, proj_warps = PROJ_WARPS;
+};
 
 }  // namespace art
 
@@ -1017,7 +1301,7 @@ struct ArtContext {
     std::vector<std::array<float, 4>> h_weights;  // per image: weight, pweight[3]
     art::DevBuf evalbuf;              // partial sums of art_context_evaluate
     std::vector<int2> h_work;         // sweep blocks {image, block in image}, grouped by variant and channel count
-    int wstart[2][4] = {}, wcount[2][4] = {};  // by sweep variant (0 narrow, 1 wide) and channel count
+    int wstart[3][4] = {}, wcount[3][4] = {};  // by sweep variant (0 narrow, 1 wide, 2 quad) and channel count
     std::vector<int4> h_tasks;        // block warps {image, channel, block row, first block}
     std::vector<long long> geo_key;   // geometry h_work / h_tasks (and their device copies) were built for
     int mode_off[5] = {0, 0, 0, 0, 0};  // h_tasks grouped by sampling mode (1x1, 2x2, 2x1, 1x2)
@@ -1029,7 +1313,10 @@ struct ArtContext {
     uint32_t timed_iterations = 0;
     int strip_rows_override = 0;      // 0 = tuning cache, else size heuristic
     int sweep_kind_override = 0;
-    std::map<std::string, std::pair<int, int>> tune;  // autotuned (sweep variant, strip rows) by geometry bucket
+    int proj_warps = art::PROJ_WARPS; // projection warps per block of the current solve
+    int proj_warps_override = 0;      // set while the autotuner times a candidate
+    std::map<std::string, art::TuneChoice> tune;  // autotuned launch shapes by geometry bucket
+    ArtTuneResult last_tune{};        // the last autotune run's choice and timings
 };
 
 namespace art {
@@ -1052,35 +1339,114 @@ std::string tune_key(uint32_t nch, const uint32_t *sh, const uint32_t *sv, uint3
     return k;
 }
 
-// Gradient-sweep variant and strip height for one image: the autotuner's
-// choice for its bucket, else by size -- the wide packed sweep once the batch
-// has enough pixels to fill every SM with its fewer, wider strips, and strips
-// as tall as that allows (the 3 extra rows a strip reads stay small).
-std::pair<int, int> pick_sweep(const ArtContext *ctx, const ImageSpec &sp, long long batch_px)
+// Key of a whole batch (more than one image) for the autotuner: image count
+// and total pixels, each rounded up to a power of two.
+std::string batch_tune_key(int nimg, long long batch_px)
 {
-    const char *ek = getenv("ART_SWEEP_KIND");
-    const char *er = getenv("ART_STRIP_ROWS");
-    int kind = batch_px >= 8LL * 1024 * 1024 ? 1 : 0;
-    if (ctx->strip_rows_override > 0) return {ctx->sweep_kind_override, ctx->strip_rows_override};
-    if (ek && (atoi(ek) == 0 || atoi(ek) == 1)) kind = atoi(ek);
-    if (er && atoi(er) > 0) return {kind, atoi(er)};
-    uint32_t sh[3], sv[3];
-    for (uint32_t c = 0; c < sp.nch; c++) {
-        sh[c] = sp.ch[c].samp_h;
-        sv[c] = sp.ch[c].samp_v;
-    }
-    auto it = ctx->tune.find(tune_key(sp.nch, sh, sv, sp.W, sp.H));
-    if (it != ctx->tune.end()) return it->second;
-    const long long cols = kind ? SWEEP_OUT : SWEEP_OUT_N;
-    int R = 128;
-    while (R > 16 && batch_px / (cols * R) < 148LL * 12) R /= 2;
-    return {kind, R};
+    long long n = 1, px = 1 << 20;
+    while (n < nimg) n *= 2;
+    while (px < batch_px) px *= 2;
+    return "batch-i" + std::to_string(n) + "-p" + std::to_string(px);
 }
 
-template <int SH, int SV>
+// Launch shapes for one image of a solve of `nimg` images: environment
+// overrides (ART_SWEEP_KIND, ART_STRIP_ROWS, ART_PROJ_WARPS), the candidate
+// the autotuner is timing, the autotuner's choice for the batch's bucket
+// (several images) or the image's bucket (one image), else by size -- the
+// wide packed sweep once the batch has enough pixels to fill every SM with its
+// fewer, wider strips, strips as tall as that allows (the 3 extra rows a strip
+// reads stay small), and 4 projection warps per block.
+TuneChoice pick_shape(const ArtContext *ctx, const ImageSpec &sp, long long batch_px, int nimg)
+{
+    TuneChoice t;
+    t.kind = batch_px >= 8LL * 1024 * 1024 ? 1 : 0;
+    if (ctx->strip_rows_override > 0) {
+        t.kind = ctx->sweep_kind_override;
+        t.rows = ctx->strip_rows_override;
+        t.proj_warps = ctx->proj_warps_override > 0 ? ctx->proj_warps_override : PROJ_WARPS;
+        return t;
+    }
+    const char *ek = getenv("ART_SWEEP_KIND");
+    const char *er = getenv("ART_STRIP_ROWS");
+    const char *ep = getenv("ART_PROJ_WARPS");
+    const int env_pw = ep ? atoi(ep) : 0;
+    const bool env_pw_ok = env_pw == 2 || env_pw == 4 || env_pw == 8;
+    if (ek && atoi(ek) >= 0 && atoi(ek) <= 2) t.kind = atoi(ek);
+    if (er && atoi(er) > 0) {
+        t.rows = atoi(er);
+        if (env_pw_ok) t.proj_warps = env_pw;
+        return t;
+    }
+    std::map<std::string, TuneChoice>::const_iterator it = ctx->tune.end();
+    if (nimg > 1) it = ctx->tune.find(batch_tune_key(nimg, batch_px));
+    if (it == ctx->tune.end()) {
+        uint32_t sh[3], sv[3];
+        for (uint32_t c = 0; c < sp.nch; c++) {
+            sh[c] = sp.ch[c].samp_h;
+            sv[c] = sp.ch[c].samp_v;
+        }
+        it = ctx->tune.find(tune_key(sp.nch, sh, sv, sp.W, sp.H));
+    }
+    if (it != ctx->tune.end()) {
+        t = it->second;
+        if (env_pw_ok) t.proj_warps = env_pw;
+        return t;
+    }
+    const long long cols = t.kind == 2 ? SWEEP_OUT_Q : t.kind == 1 ? SWEEP_OUT : SWEEP_OUT_N;
+    int R = 128;
+    while (R > 16 && batch_px / (cols * R) < 148LL * 12) R /= 2;
+    t.rows = R;
+    if (env_pw_ok) t.proj_warps = env_pw;
+    return t;
+}
+
+template <int SH, int SV, int PW = PROJ_WARPS>
 constexpr int proj_smem()
 {
-    return PROJ_WARPS * 2 * ProjShape<SH, SV>::REGION * (int)sizeof(float);
+    return PW * 2 * ProjShape<SH, SV>::REGION * (int)sizeof(float);
+}
+
+// Projection block shapes the autotuner may choose: warps per block (each
+// warp takes 4 coefficient blocks of one block row).
+constexpr int PROJ_WARP_CHOICES[3] = {2, 4, 8};
+
+template <int PW>
+static cudaError_t set_proj_smem()
+{
+    cudaError_t e = cudaFuncSetAttribute(k_project<1, 1, PW>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         proj_smem<1, 1, PW>());
+    if (e == cudaSuccess)
+        e = cudaFuncSetAttribute(k_project<2, 2, PW>, cudaFuncAttributeMaxDynamicSharedMemorySize, proj_smem<2, 2, PW>());
+    if (e == cudaSuccess)
+        e = cudaFuncSetAttribute(k_project<2, 1, PW>, cudaFuncAttributeMaxDynamicSharedMemorySize, proj_smem<2, 1, PW>());
+    if (e == cudaSuccess)
+        e = cudaFuncSetAttribute(k_project<1, 2, PW>, cudaFuncAttributeMaxDynamicSharedMemorySize, proj_smem<1, 2, PW>());
+    return e;
+}
+
+// One projection launch over n tasks of sampling mode m with PW warps per block.
+template <int PW>
+static void launch_project_mode(int m, int n, const ImgDev *ddesc, const int4 *tk, float fnext, cudaStream_t s)
+{
+    const int grid = (n + PW - 1) / PW;
+    if (m == 0)
+        k_project<1, 1, PW><<<grid, PW * 32, proj_smem<1, 1, PW>(), s>>>(ddesc, tk, n, fnext);
+    else if (m == 1)
+        k_project<2, 2, PW><<<grid, PW * 32, proj_smem<2, 2, PW>(), s>>>(ddesc, tk, n, fnext);
+    else if (m == 2)
+        k_project<2, 1, PW><<<grid, PW * 32, proj_smem<2, 1, PW>(), s>>>(ddesc, tk, n, fnext);
+    else
+        k_project<1, 2, PW><<<grid, PW * 32, proj_smem<1, 2, PW>(), s>>>(ddesc, tk, n, fnext);
+}
+
+static void launch_project(int pw, int m, int n, const ImgDev *ddesc, const int4 *tk, float fnext, cudaStream_t s)
+{
+    if (pw == 2)
+        launch_project_mode<2>(m, n, ddesc, tk, fnext, s);
+    else if (pw == 8)
+        launch_project_mode<8>(m, n, ddesc, tk, fnext, s);
+    else
+        launch_project_mode<4>(m, n, ddesc, tk, fnext, s);
 }
 
 // Raises the dynamic shared-memory limit of the projection kernels, once per device.
@@ -1091,13 +1457,9 @@ int configure_kernels(int device)
     std::lock_guard<std::mutex> lock(mu);
     if ((int)done.size() <= device) done.resize(device + 1, 0);
     if (done[device]) return ART_OK;
-    cudaError_t e = cudaFuncSetAttribute(k_project<1, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, proj_smem<1, 1>());
-    if (e == cudaSuccess)
-        e = cudaFuncSetAttribute(k_project<2, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize, proj_smem<2, 2>());
-    if (e == cudaSuccess)
-        e = cudaFuncSetAttribute(k_project<2, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, proj_smem<2, 1>());
-    if (e == cudaSuccess)
-        e = cudaFuncSetAttribute(k_project<1, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize, proj_smem<1, 2>());
+    cudaError_t e = set_proj_smem<2>();
+    if (e == cudaSuccess) e = set_proj_smem<4>();
+    if (e == cudaSuccess) e = set_proj_smem<8>();
     if (e != cudaSuccess) return fail(ART_ERR_CUDA, std::string("cudaFuncSetAttribute: ") + cudaGetErrorString(e));
     done[device] = 1;
     return ART_OK;
@@ -1180,16 +1542,7 @@ static void launch_projections(ArtContext *ctx, float fnext)
         const int n = ctx->mode_off[m + 1] - ctx->mode_off[m];
         if (n == 0) continue;
         cudaStream_t s = split && m > 0 ? ctx->side : ctx->stream;
-        const int4 *tk = tasks + ctx->mode_off[m];
-        const int grid = (n + PROJ_WARPS - 1) / PROJ_WARPS;
-        if (m == 0)
-            k_project<1, 1><<<grid, PROJ_WARPS * 32, proj_smem<1, 1>(), s>>>(ddesc, tk, n, fnext);
-        else if (m == 1)
-            k_project<2, 2><<<grid, PROJ_WARPS * 32, proj_smem<2, 2>(), s>>>(ddesc, tk, n, fnext);
-        else if (m == 2)
-            k_project<2, 1><<<grid, PROJ_WARPS * 32, proj_smem<2, 1>(), s>>>(ddesc, tk, n, fnext);
-        else
-            k_project<1, 2><<<grid, PROJ_WARPS * 32, proj_smem<1, 2>(), s>>>(ddesc, tk, n, fnext);
+        launch_project(ctx->proj_warps, m, n, ddesc, tasks + ctx->mode_off[m], fnext, s);
     }
     if (split) {
         cudaEventRecord(ctx->join, ctx->side);
@@ -1220,14 +1573,16 @@ static int prepare_batch(ArtContext *ctx, const std::vector<ImageSpec> &specs, u
         ctx->h_weights[i] = {sp.weight, sp.pweight[0], sp.pweight[1], sp.pweight[2]};
         const int pitch = (int)align_up(sp.W, 32);
         const long long cstride = (long long)pitch * (long long)align_up(sp.H, 32);
-        const std::pair<int, int> sw = pick_sweep(ctx, sp, batch_px);
-        const int R = sw.second, out_cols = sw.first ? SWEEP_OUT : SWEEP_OUT_N;
-        const int warps = sw.first ? SWEEP_WARPS : SWEEP_WARPS_N;
+        const TuneChoice sw = pick_shape(ctx, sp, batch_px, nimg);
+        if (i == 0) ctx->proj_warps = sw.proj_warps;
+        const int R = sw.rows;
+        const int out_cols = sw.kind == 2 ? SWEEP_OUT_Q : sw.kind == 1 ? SWEEP_OUT : SWEEP_OUT_N;
+        const int warps = sw.kind == 2 ? SWEEP_WARPS_Q : sw.kind == 1 ? SWEEP_WARPS : SWEEP_WARPS_N;
         d.nch = (int)sp.nch;
         d.W = (int)sp.W;
         d.H = (int)sp.H;
         d.pitch = pitch;
-        d.sweep_kind = sw.first;
+        d.sweep_kind = sw.kind;
         d.strip_rows = R;
         d.strips_x = (int)((sp.W + out_cols - 1) / out_cols);
         d.strips_y = (int)((sp.H + R - 1) / R);
@@ -1282,7 +1637,7 @@ static int prepare_batch(ArtContext *ctx, const std::vector<ImageSpec> &specs, u
         for (int c = 0; c < d.nch; c++) geo.insert(geo.end(), {d.ch[c].cw, d.ch[c].chh, d.ch[c].sh, d.ch[c].sv});
     }
     const bool same_geo = geo == ctx->geo_key && ctx->work.p && ctx->tasks.p;
-    std::vector<int2> wk[2][4];
+    std::vector<int2> wk[3][4];
     std::vector<int4> per_mode[4];
     for (int i = 0; i < nimg; i++) {
         ImgDev &d = ctx->h_desc[i];
@@ -1304,7 +1659,7 @@ static int prepare_batch(ArtContext *ctx, const std::vector<ImageSpec> &specs, u
     if (!same_geo) {
         ctx->geo_key.clear();
         ctx->h_work.clear();
-        for (int kd = 0; kd < 2; kd++)
+        for (int kd = 0; kd < 3; kd++)
             for (int n = 3; n >= 1; n--) {
                 ctx->wstart[kd][n] = (int)ctx->h_work.size();
                 ctx->wcount[kd][n] = (int)wk[kd][n].size();
@@ -1406,7 +1761,7 @@ static int prepare_batch(ArtContext *ctx, const std::vector<ImageSpec> &specs, u
         std::vector<unsigned long long> key = {
             (unsigned long long)(uintptr_t)ctx->net, cnn::net_generation(ctx->net, 0), cnn::net_generation(ctx->net, 1),
             (uintptr_t)ctx->desc.p, (uintptr_t)ctx->tasks.p, (uintptr_t)pred, (uintptr_t)ctx->xbuf.p,
-            (uintptr_t)ctx->coefimg.p, (unsigned long long)nimg};
+            (uintptr_t)ctx->coefimg.p, (unsigned long long)nimg, (unsigned long long)ctx->proj_warps};
         for (int m = 0; m < 5; m++) key.push_back((unsigned long long)ctx->mode_off[m]);
         for (int i = 0; i < nimg; i++) {
             const ImgDev &d = ctx->h_desc[i];
@@ -1504,6 +1859,12 @@ static void launch_iteration(ArtContext *ctx, int it, float fnext, float stepmul
         k_grad_sweep<2><<<ctx->wcount[1][2], SWEEP_WARPS * 32, 0, s>>>(ddesc, work + ctx->wstart[1][2], stepmul);
     if (ctx->wcount[1][1])
         k_grad_sweep<1><<<ctx->wcount[1][1], SWEEP_WARPS * 32, 0, s>>>(ddesc, work + ctx->wstart[1][1], stepmul);
+    if (ctx->wcount[2][3])
+        k_grad_sweep_q<3><<<ctx->wcount[2][3], SWEEP_WARPS_Q * 32, 0, s>>>(ddesc, work + ctx->wstart[2][3], stepmul);
+    if (ctx->wcount[2][2])
+        k_grad_sweep_q<2><<<ctx->wcount[2][2], SWEEP_WARPS_Q * 32, 0, s>>>(ddesc, work + ctx->wstart[2][2], stepmul);
+    if (ctx->wcount[2][1])
+        k_grad_sweep_q<1><<<ctx->wcount[2][1], SWEEP_WARPS_Q * 32, 0, s>>>(ddesc, work + ctx->wstart[2][1], stepmul);
     if (ctx->wcount[0][3])
         k_grad_sweep_n<3><<<ctx->wcount[0][3], SWEEP_WARPS_N * 32, 0, s>>>(ddesc, work + ctx->wstart[0][3], stepmul);
     if (ctx->wcount[0][2])
@@ -1518,7 +1879,8 @@ static void launch_iteration(ArtContext *ctx, int it, float fnext, float stepmul
 
 // Replays (capturing first if the work changed shape) the fixed-count
 // iteration loop as one CUDA graph.
-static int run_iterations(ArtContext *ctx, uint32_t iterations, uint32_t tail = 0, float tail_stepmul = 1.0f)
+static int run_iterations(ArtContext *ctx, uint32_t iterations, uint32_t tail = 0, float tail_stepmul = 1.0f,
+                          float decay = 0.0f)
 {
     if (iterations == 0) return ART_OK;
     tail = std::min(tail, iterations);
@@ -1532,11 +1894,13 @@ static int run_iterations(ArtContext *ctx, uint32_t iterations, uint32_t tail = 
     }
     GraphKey key;
     key.nimg = (int)ctx->h_desc.size();
-    std::copy(&ctx->wcount[0][0], &ctx->wcount[0][0] + 8, key.wcount);
+    key.proj_warps = ctx->proj_warps;
+    std::copy(&ctx->wcount[0][0], &ctx->wcount[0][0] + 12, key.wcount);
     std::copy(ctx->mode_off, ctx->mode_off + 5, key.mode_off);
     key.iterations = iterations;
     key.tail = tail;
     key.tail_stepmul = tail_stepmul;
+    key.decay = decay;
     key.timing = ctx->timing;
     key.desc = ctx->desc.p;
     key.work = ctx->work.p;
@@ -1557,11 +1921,16 @@ static int run_iterations(ArtContext *ctx, uint32_t iterations, uint32_t tail = 
         ART_CUDA(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
         if (ctx->timing) cudaEventRecordWithFlags(ctx->events[0], s, cudaEventRecordExternal);
         // y_0 = x_0 (f_0 = 0); the projection of iteration k forms y_{k+1} with f_{k+1}.
+        // With decay > 0 the first phase's steps shrink geometrically: step
+        // k of that phase is decay^k times the solve's step (fp32 product).
+        float mul = 1.0f;
         for (uint32_t it = 0; it < iterations; it++) {
-            if (it < k1)
-                launch_iteration(ctx, (int)it, it + 1 < k1 ? fs1[it + 1] : 0.0f, 1.0f);
-            else
+            if (it < k1) {
+                launch_iteration(ctx, (int)it, it + 1 < k1 ? fs1[it + 1] : 0.0f, mul);
+                if (decay > 0.0f) mul *= decay;
+            } else {
                 launch_iteration(ctx, (int)it, it - k1 + 1 < tail ? fs2[it - k1 + 1] : 0.0f, tail_stepmul);
+            }
         }
         if (ctx->timing) cudaEventRecordWithFlags(ctx->events[1], s, cudaEventRecordExternal);
         cudaError_t e = cudaStreamEndCapture(s, &graph);
@@ -1603,6 +1972,7 @@ struct InitSpec {
     int mode = ART_INIT_DECODED;
     uint32_t step_iterations = 0;
     uint32_t tail_iterations = 0, tail_step_iterations = 0;
+    float step_decay = 0.0f;  // > 0: first-phase steps shrink by this factor per iteration
     // Step of the tail phase relative to the first phase's, for `iterations` in all.
     float tail_stepmul(uint32_t iterations) const
     {
@@ -1618,6 +1988,9 @@ static int init_spec(const ArtContext *ctx, const ArtOptions *opts, InitSpec *ou
     out->step_iterations = opts ? opts->step_iterations : 0;
     out->tail_iterations = opts ? opts->tail_iterations : 0;
     out->tail_step_iterations = opts ? opts->tail_step_iterations : 0;
+    out->step_decay = opts ? opts->step_decay : 0.0f;
+    if (!(out->step_decay >= 0.0f && out->step_decay <= 1.0f))
+        return fail(ART_ERR_INVALID_ARGUMENT, "step_decay must lie in [0, 1]");
     if (out->mode != ART_INIT_DECODED && out->mode != ART_INIT_SCALAR_COMPAT && out->mode != ART_INIT_LEARNED)
         return fail(ART_ERR_INVALID_ARGUMENT, "unknown init mode");
     if (out->mode == ART_INIT_LEARNED && !ctx->net)
@@ -1745,7 +2118,7 @@ int32_t art_context_compute_device(ArtContext *ctx, uint32_t nchannel, const Art
                  max_h};
     for (uint32_t c = 0; c < nchannel; c++) sp.src[c] = coefs[c].dct_coefs;
     rc = prepare_batch(ctx, {sp}, iterations, ini.mode, ini.step_iterations);
-    if (!rc) rc = run_iterations(ctx, iterations, ini.tail_iterations, ini.tail_stepmul(iterations));
+    if (!rc) rc = run_iterations(ctx, iterations, ini.tail_iterations, ini.tail_stepmul(iterations), ini.step_decay);
     if (!rc) {
         const float *fb;
         int fp;
@@ -1867,7 +2240,7 @@ static int solve_host(ArtContext *ctx, uint32_t nchannel, const ArtChannel *coef
         sp.src[c] = dst;
     }
     rc = prepare_batch(ctx, {sp}, iterations, ini.mode, ini.step_iterations);
-    if (!rc) rc = run_iterations(ctx, iterations, ini.tail_iterations, ini.tail_stepmul(iterations));
+    if (!rc) rc = run_iterations(ctx, iterations, ini.tail_iterations, ini.tail_stepmul(iterations), ini.step_decay);
     return rc;
 }
 
@@ -2022,7 +2395,7 @@ int32_t art_context_compute_batch(ArtContext *ctx, uint32_t nimages, const ArtIm
             off += align_up(n, 256);
         }
     rc = prepare_batch(ctx, specs, iterations, ini.mode, ini.step_iterations);
-    if (!rc) rc = run_iterations(ctx, iterations, ini.tail_iterations, ini.tail_stepmul(iterations));
+    if (!rc) rc = run_iterations(ctx, iterations, ini.tail_iterations, ini.tail_stepmul(iterations), ini.step_decay);
     if (rc) {
         cudaStreamSynchronize(ctx->stream);
         return rc;
@@ -2065,7 +2438,7 @@ int32_t art_context_compute_batch_device(ArtContext *ctx, uint32_t nimages, cons
         ART_CUDA(cudaStreamWaitEvent(ctx->stream, join, 0));
     }
     rc = prepare_batch(ctx, specs, iterations, ini.mode, ini.step_iterations);
-    if (!rc) rc = run_iterations(ctx, iterations, ini.tail_iterations, ini.tail_stepmul(iterations));
+    if (!rc) rc = run_iterations(ctx, iterations, ini.tail_iterations, ini.tail_stepmul(iterations), ini.step_decay);
     for (uint32_t i = 0; !rc && i < nimages; i++) {
         const float *fb;
         int fp;
@@ -2089,7 +2462,239 @@ int32_t art_context_compute_batch_device(ArtContext *ctx, uint32_t nimages, cons
     return rc;
 }
 
+int32_t art_context_process_batch(ArtContext *ctx, uint32_t nimages, const ArtProcessImage *images,
+                                  uint32_t iterations, int32_t separate, const ArtOptions *opts)
+{
+    if (!ctx || !images || nimages == 0) return fail(ART_ERR_INVALID_ARGUMENT, "null context or empty batch");
+    ART_CUDA(cudaSetDevice(ctx->device));
+    InitSpec ini;
+    int rc = init_spec(ctx, opts, &ini);
+    if (rc) return rc;
+    ctx->net_used = false;
+    // lib.rs:122-153 per image: a joint solve of a 3-component image, else one
+    // solve per component (each reads pweight[0], as compute(1, ...) does).
+    // Every solve becomes one image of the batch.
+    struct Out {
+        uint32_t first, nout;  // first batch image of this input, planes to convert
+        bool joint;
+    };
+    std::vector<ImageSpec> specs;
+    std::vector<Out> outs(nimages);
+    for (uint32_t i = 0; i < nimages; i++) {
+        const ArtProcessImage &im = images[i];
+        const std::string at = "image " + std::to_string(i) + ": ";
+        if (im.nchannel < 1 || im.nchannel > 4 || !im.channels)
+            return fail(ART_ERR_INVALID_ARGUMENT, at + "nchannel must be 1 to 4 with channels given");
+        uint32_t W = 0, H = 0;
+        for (uint32_t c = 0; c < im.nchannel; c++) {
+            W = std::max(W, im.channels[c].rounded_px_w);
+            H = std::max(H, im.channels[c].rounded_px_h);
+        }
+        if (im.real_w == 0 || im.real_h == 0 || im.real_w > W || im.real_h > H)
+            return fail(ART_ERR_INVALID_ARGUMENT, at + "real size must be positive and within the rounded size");
+        const bool joint = im.nchannel == 3 && !separate;
+        outs[i] = {(uint32_t)specs.size(), im.nchannel == 3 ? 3u : 1u, joint};
+        const uint32_t njobs = joint ? 1 : im.nchannel;
+        for (uint32_t k = 0; k < njobs; k++) {
+            const uint32_t nch = joint ? 3 : 1;
+            const ArtChannel *ch = joint ? im.channels : &im.channels[k];
+            const float w = joint ? im.weight[0] : im.weight[std::min(k, 2u)];
+            if ((rc = validate(nch, ch, w, im.pweight, W, H))) return fail(rc, at + g_err);
+            ImageSpec sp{nch, ch, {nullptr, nullptr, nullptr}, w, {im.pweight[0], im.pweight[1], im.pweight[2]},
+                         W, H};
+            for (uint32_t c = 0; c < nch; c++) sp.src[c] = ch[c].dct_coefs;
+            specs.push_back(sp);
+        }
+    }
+    // Host coefficients through one device staging buffer.
+    size_t total = 0;
+    for (auto &sp : specs)
+        for (uint32_t c = 0; c < sp.nch; c++)
+            total += align_up((size_t)sp.ch[c].block_w * sp.ch[c].block_h * 64 *
+                                  (sp.ch[c].coef_type == ART_COEF_I16 ? 2 : 4), 256);
+    if ((rc = ctx->stage.ensure(total))) return rc;
+    size_t off = 0;
+    for (auto &sp : specs)
+        for (uint32_t c = 0; c < sp.nch; c++) {
+            const size_t n = (size_t)sp.ch[c].block_w * sp.ch[c].block_h * 64 * (sp.ch[c].coef_type == ART_COEF_I16 ? 2 : 4);
+            char *dst = static_cast<char *>(ctx->stage.p) + off;
+            ART_CUDA(cudaMemcpyAsync(dst, sp.ch[c].dct_coefs, n, cudaMemcpyHostToDevice, ctx->stream));
+            sp.src[c] = dst;
+            off += align_up(n, 256);
+        }
+    rc = prepare_batch(ctx, specs, iterations, ini.mode, ini.step_iterations);
+    if (!rc) rc = run_iterations(ctx, iterations, ini.tail_iterations, ini.tail_stepmul(iterations), ini.step_decay);
+    if (rc) {
+        cudaStreamSynchronize(ctx->stream);
+        return rc;
+    }
+    // Output stage per image (lib.rs:159-211) into one device buffer, then
+    // one copy per image to its host buffer.
+    size_t rgb_total = 0;
+    for (uint32_t i = 0; i < nimages; i++)
+        if (images[i].rgb_out) rgb_total += align_up((size_t)images[i].real_w * images[i].real_h * 3, 256);
+    if (rgb_total) {
+        if ((rc = ctx->rgb.ensure(rgb_total))) {
+            cudaStreamSynchronize(ctx->stream);
+            return rc;
+        }
+        size_t ro = 0;
+        for (uint32_t i = 0; i < nimages; i++) {
+            const ArtProcessImage &im = images[i];
+            if (!im.rgb_out) continue;
+            const float *pl[3] = {nullptr, nullptr, nullptr};
+            long long pitch = 0;
+            for (uint32_t c = 0; c < outs[i].nout; c++) {
+                const float *fb;
+                int fp;
+                long long fcs;
+                result_planes(ctx, (int)(outs[i].first + (outs[i].joint ? 0 : c)), &fb, &fp, &fcs);
+                pl[c] = outs[i].joint ? fb + c * fcs : fb;
+                pitch = fp;
+            }
+            const long long n = (long long)im.real_w * im.real_h;
+            uint8_t *dst = static_cast<uint8_t *>(ctx->rgb.p) + ro;
+            k_rgb<<<(int)((n + 255) / 256), 256, 0, ctx->stream>>>(pl[0], pl[1], pl[2], pitch, (int)outs[i].nout,
+                                                                   (int)im.real_w, (int)im.real_h, dst);
+            const cudaError_t e = cudaGetLastError();
+            const cudaError_t e2 = e == cudaSuccess ? cudaMemcpyAsync(im.rgb_out, dst, (size_t)n * 3,
+                                                                      cudaMemcpyDeviceToHost, ctx->stream)
+                                                    : e;
+            if (e2 != cudaSuccess) {
+                cudaStreamSynchronize(ctx->stream);
+                return fail(ART_ERR_CUDA, std::string("output stage: ") + cudaGetErrorString(e2));
+            }
+            ro += align_up((size_t)n * 3, 256);
+        }
+    }
+    ART_CUDA(cudaStreamSynchronize(ctx->stream));
+    return check_errflag(ctx);
+}
+
 // -------------------------------------------------------------- autotuner --
+
+}  // extern "C"
+
+namespace art {
+namespace {
+
+constexpr int TUNE_REPS = 5;          // timed repetitions per candidate (median)
+constexpr float TUNE_TIE = 0.02f;     // candidates within 2 % of the fastest count as ties
+
+// Times the launch-shape candidates on prepared specs (coefficients already on
+// the device): first the gradient sweep (variant x strip rows, projection at 4
+// warps), then the projection's warps per block with the chosen sweep. Each
+// candidate is captured and warmed once, then timed TUNE_REPS times; its time
+// is the median. Candidates are tried in a fixed order that starts with the
+// size heuristic's choice, and the first one within TUNE_TIE of the fastest
+// wins, so a choice changes only for a clear gain.
+int tune_specs(ArtContext *ctx, const std::vector<ImageSpec> &specs, uint32_t iterations, bool skip_tall,
+               TuneChoice *best, ArtTuneResult *res)
+{
+    long long batch_px = 0;
+    uint32_t max_h = 0;
+    for (const auto &sp : specs) {
+        batch_px += (long long)sp.W * sp.H;
+        max_h = std::max(max_h, sp.H);
+    }
+    const TuneChoice heur = pick_shape(ctx, specs[0], batch_px, (int)specs.size());
+    cudaEvent_t e0, e1;
+    ART_CUDA(cudaEventCreate(&e0));
+    ART_CUDA(cudaEventCreate(&e1));
+    const bool timing = ctx->timing;
+    ctx->timing = false;
+    int rc = ART_OK;
+    auto time_one = [&](const TuneChoice &t, float *ms) -> int {
+        ctx->sweep_kind_override = t.kind;
+        ctx->strip_rows_override = t.rows;
+        ctx->proj_warps_override = t.proj_warps;
+        int r = prepare_batch(ctx, specs, iterations, ART_INIT_DECODED, 0);
+        if (!r) r = run_iterations(ctx, iterations);  // captures and warms up
+        std::vector<float> v;
+        for (int rep = 0; rep < TUNE_REPS && !r; rep++) {
+            cudaEventRecord(e0, ctx->stream);
+            r = run_iterations(ctx, iterations);
+            cudaEventRecord(e1, ctx->stream);
+            if (cudaEventSynchronize(e1) != cudaSuccess) r = fail(ART_ERR_CUDA, "autotune: timing failed");
+            float t_ms = 0.f;
+            cudaEventElapsedTime(&t_ms, e0, e1);
+            v.push_back(t_ms);
+        }
+        if (!r) {
+            std::sort(v.begin(), v.end());
+            *ms = v[v.size() / 2];
+        }
+        return r;
+    };
+    auto pick = [](const std::vector<std::pair<TuneChoice, float>> &c) {
+        float lo = c[0].second;
+        for (const auto &x : c) lo = std::min(lo, x.second);
+        for (const auto &x : c)
+            if (x.second <= lo * (1.0f + TUNE_TIE)) return x;
+        return c[0];
+    };
+    // Phase 1: the sweep, heuristic first.
+    std::vector<TuneChoice> cands = {TuneChoice{heur.kind, heur.rows, PROJ_WARPS}};
+    for (int kind = 0; kind < 3; kind++)
+        for (int R : {16, 32, 64, 128}) {
+            if (skip_tall && (int)max_h < R && R > 16) continue;
+            if (kind == heur.kind && R == heur.rows) continue;
+            cands.push_back(TuneChoice{kind, R, PROJ_WARPS});
+        }
+    std::vector<std::pair<TuneChoice, float>> timed1, timed2;
+    for (const auto &t : cands) {
+        float ms = 0.f;
+        if ((rc = time_one(t, &ms))) break;
+        timed1.push_back({t, ms});
+    }
+    TuneChoice chosen;
+    float chosen_ms = 0.f, default_ms = 0.f;
+    if (!rc) {
+        const auto p1 = pick(timed1);
+        // Phase 2: projection warps per block, 4 (already timed) first.
+        timed2.push_back(p1);
+        for (int pw : PROJ_WARP_CHOICES) {
+            if (pw == PROJ_WARPS) continue;
+            TuneChoice t = p1.first;
+            t.proj_warps = pw;
+            float ms = 0.f;
+            if ((rc = time_one(t, &ms))) break;
+            timed2.push_back({t, ms});
+        }
+        if (!rc) {
+            const auto p2 = pick(timed2);
+            chosen = p2.first;
+            chosen_ms = p2.second;
+            default_ms = timed1[0].second;
+        }
+    }
+    ctx->strip_rows_override = 0;
+    ctx->sweep_kind_override = 0;
+    ctx->proj_warps_override = 0;
+    ctx->timing = timing;
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    if (rc) return rc;
+    ART_CUDA(cudaStreamSynchronize(ctx->stream));
+    *best = chosen;
+    if (res) {
+        memset(res, 0, sizeof(*res));
+        res->variant = (uint32_t)chosen.kind;
+        res->strip_rows = (uint32_t)chosen.rows;
+        res->proj_warps = (uint32_t)chosen.proj_warps;
+        res->candidates = (uint32_t)(timed1.size() + timed2.size() - 1);
+        res->best_ms = chosen_ms;
+        res->heuristic_ms = default_ms;
+        res->heuristic_variant = (uint32_t)heur.kind;
+        res->heuristic_strip_rows = (uint32_t)heur.rows;
+    }
+    return ART_OK;
+}
+
+}  // namespace
+}  // namespace art
+
+extern "C" {
 
 int32_t art_context_autotune(ArtContext *ctx, uint32_t nchannel, const uint32_t *samp_h, const uint32_t *samp_v,
                              uint32_t max_w, uint32_t max_h, uint32_t iterations, uint32_t *variant_out,
@@ -2100,7 +2705,7 @@ int32_t art_context_autotune(ArtContext *ctx, uint32_t nchannel, const uint32_t 
     ART_CUDA(cudaSetDevice(ctx->device));
     if (iterations == 0) iterations = 10;
     // A deterministic synthetic image of this geometry: sparse small
-    // coefficients, unit quantisation steps.
+    // coefficients, quantisation steps of 8.
     ArtChannel ch[3];
     std::vector<int16_t> host[3];
     float q[64];
@@ -2127,7 +2732,9 @@ int32_t art_context_autotune(ArtContext *ctx, uint32_t nchannel, const uint32_t 
         }
         total += align_up(host[c].size() * 2, 256);
     }
-    int rc;
+    const float pw3[3] = {0.001f, 0.001f, 0.001f};
+    int rc = validate(nchannel, ch, 0.3f, pw3, max_w, max_h);
+    if (rc) return rc;
     if ((rc = ctx->stage.ensure(total))) return rc;
     ImageSpec sp{nchannel, ch, {nullptr, nullptr, nullptr}, 0.3f, {0.001f, 0.001f, 0.001f}, max_w, max_h};
     size_t off = 0;
@@ -2137,48 +2744,61 @@ int32_t art_context_autotune(ArtContext *ctx, uint32_t nchannel, const uint32_t 
         sp.src[c] = dst;
         off += align_up(host[c].size() * 2, 256);
     }
-    cudaEvent_t e0, e1;
-    ART_CUDA(cudaEventCreate(&e0));
-    ART_CUDA(cudaEventCreate(&e1));
-    const bool timing = ctx->timing;
-    ctx->timing = false;
-    int best = 0, best_kind = 0;
-    float best_ms = 0.f;
-    const int candidates[8][2] = {{0, 16}, {0, 32}, {0, 64}, {0, 128}, {1, 16}, {1, 32}, {1, 64}, {1, 128}};
-    for (const auto &cand : candidates) {
-        const int R = cand[1];
-        if ((int)max_h < R && R > 16) continue;
-        ctx->sweep_kind_override = cand[0];
-        ctx->strip_rows_override = R;
-        rc = prepare_batch(ctx, {sp}, iterations, ART_INIT_DECODED, 0);
-        if (!rc) rc = run_iterations(ctx, iterations);  // captures and warms up
-        float ms = 1e30f;
-        for (int rep = 0; rep < 3 && !rc; rep++) {
-            cudaEventRecord(e0, ctx->stream);
-            rc = run_iterations(ctx, iterations);
-            cudaEventRecord(e1, ctx->stream);
-            cudaEventSynchronize(e1);
-            float t = 0.f;
-            cudaEventElapsedTime(&t, e0, e1);
-            ms = std::min(ms, t);
-        }
-        if (rc) break;
-        if (!best || ms < best_ms) {
-            best = R;
-            best_kind = cand[0];
-            best_ms = ms;
-        }
-    }
-    ctx->strip_rows_override = 0;
-    ctx->sweep_kind_override = 0;
-    ctx->timing = timing;
-    cudaEventDestroy(e0);
-    cudaEventDestroy(e1);
+    TuneChoice best;
+    if ((rc = tune_specs(ctx, {sp}, iterations, true, &best, &ctx->last_tune))) return rc;
+    ctx->tune[tune_key(nchannel, samp_h, samp_v, max_w, max_h)] = best;
+    if (variant_out) *variant_out = (uint32_t)best.kind;
+    if (strip_rows_out) *strip_rows_out = (uint32_t)best.rows;
+    return ART_OK;
+}
+
+int32_t art_context_autotune_batch(ArtContext *ctx, uint32_t nimages, const ArtImage *images, uint32_t iterations,
+                                   ArtTuneResult *out)
+{
+    if (!ctx || !images || nimages == 0) return fail(ART_ERR_INVALID_ARGUMENT, "null context or empty batch");
+    ART_CUDA(cudaSetDevice(ctx->device));
+    if (iterations == 0) iterations = 10;
+    std::vector<ImageSpec> specs;
+    int rc = batch_specs(images, nimages, specs);
     if (rc) return rc;
-    ART_CUDA(cudaStreamSynchronize(ctx->stream));
-    ctx->tune[tune_key(nchannel, samp_h, samp_v, max_w, max_h)] = {best_kind, best};
-    if (variant_out) *variant_out = (uint32_t)best_kind;
-    if (strip_rows_out) *strip_rows_out = (uint32_t)best;
+    size_t total = 0;
+    for (auto &sp : specs)
+        for (uint32_t c = 0; c < sp.nch; c++)
+            total += align_up((size_t)sp.ch[c].block_w * sp.ch[c].block_h * 64 *
+                                  (sp.ch[c].coef_type == ART_COEF_I16 ? 2 : 4), 256);
+    if ((rc = ctx->stage.ensure(total))) return rc;
+    size_t off = 0;
+    for (auto &sp : specs)
+        for (uint32_t c = 0; c < sp.nch; c++) {
+            const size_t n = (size_t)sp.ch[c].block_w * sp.ch[c].block_h * 64 * (sp.ch[c].coef_type == ART_COEF_I16 ? 2 : 4);
+            char *dst = static_cast<char *>(ctx->stage.p) + off;
+            ART_CUDA(cudaMemcpyAsync(dst, sp.ch[c].dct_coefs, n, cudaMemcpyHostToDevice, ctx->stream));
+            sp.src[c] = dst;
+            off += align_up(n, 256);
+        }
+    TuneChoice best;
+    if ((rc = tune_specs(ctx, specs, iterations, false, &best, &ctx->last_tune))) return rc;
+    long long batch_px = 0;
+    for (const auto &sp : specs) batch_px += (long long)sp.W * sp.H;
+    if (nimages > 1) {
+        ctx->tune[batch_tune_key((int)nimages, batch_px)] = best;
+    } else {
+        uint32_t sh[3], sv[3];
+        for (uint32_t c = 0; c < specs[0].nch; c++) {
+            sh[c] = specs[0].ch[c].samp_h;
+            sv[c] = specs[0].ch[c].samp_v;
+        }
+        ctx->tune[tune_key(specs[0].nch, sh, sv, specs[0].W, specs[0].H)] = best;
+    }
+    if (out) *out = ctx->last_tune;
+    return ART_OK;
+}
+
+int32_t art_context_last_tune(ArtContext *ctx, ArtTuneResult *out)
+{
+    if (!ctx || !out) return fail(ART_ERR_INVALID_ARGUMENT, "null argument");
+    if (!ctx->last_tune.candidates) return fail(ART_ERR_INVALID_ARGUMENT, "no autotune run on this context");
+    *out = ctx->last_tune;
     return ART_OK;
 }
 
@@ -2188,8 +2808,9 @@ int32_t art_context_tune_cache(ArtContext *ctx, const char *path, int32_t save)
     if (save) {
         std::ofstream f(path);
         if (!f) return fail(ART_ERR_INVALID_ARGUMENT, std::string("cannot write ") + path);
-        f << "# artefact_b200 autotune cache: <geometry bucket> <sweep variant 0|1> <strip rows>\n";
-        for (const auto &kv : ctx->tune) f << kv.first << " " << kv.second.first << " " << kv.second.second << "\n";
+        f << "# artefact_b200 autotune cache: <geometry bucket> <sweep variant 0|1|2> <strip rows> <projection warps>\n";
+        for (const auto &kv : ctx->tune)
+            f << kv.first << " " << kv.second.kind << " " << kv.second.rows << " " << kv.second.proj_warps << "\n";
         return f.good() ? ART_OK : fail(ART_ERR_INVALID_ARGUMENT, std::string("cannot write ") + path);
     }
     std::ifstream f(path);
@@ -2199,11 +2820,13 @@ int32_t art_context_tune_cache(ArtContext *ctx, const char *path, int32_t save)
         if (line.empty() || line[0] == '#') continue;
         std::istringstream ls(line);
         std::string key;
-        int kind = -1, rows = 0;
-        if (!(ls >> key >> kind >> rows) || (kind != 0 && kind != 1) ||
+        int kind = -1, rows = 0, pw = PROJ_WARPS;
+        if (!(ls >> key >> kind >> rows) || kind < 0 || kind > 2 ||
             (rows != 16 && rows != 32 && rows != 64 && rows != 128))
             return fail(ART_ERR_INVALID_ARGUMENT, "malformed tune cache line: " + line);
-        ctx->tune[key] = {kind, rows};
+        if (!(ls >> pw)) pw = PROJ_WARPS;  // three-field lines: the default projection shape
+        if (pw != 2 && pw != 4 && pw != 8) return fail(ART_ERR_INVALID_ARGUMENT, "malformed tune cache line: " + line);
+        ctx->tune[key] = TuneChoice{kind, rows, pw};
     }
     return ART_OK;
 }

@@ -44,7 +44,7 @@ struct ImgDev {
     int nch, W, H, pitch;  // full-resolution plane size; pitch in floats
     int strips_x, strips_y, nstrips, strip_rows;  // gradient sweep strips (28 or 60 columns x strip_rows)
     int ncta;              // gradient-sweep blocks of this image
-    int sweep_kind;        // 0 = narrow sweep (one column per lane), 1 = wide (two, packed FP32x2)
+    int sweep_kind;        // 0 = narrow sweep (one column per lane), 1 = wide (two, packed FP32x2), 2 = quad (four)
     long long cstride;     // floats between channel planes
     float *x;              // iterate x_k; channel c at x + c * cstride
     float *y;              // FISTA point y_k = x_k + f_k (x_k - x_{k-1})
@@ -71,6 +71,11 @@ constexpr int SWEEP_PF_N = 2;     // narrow sweep: y rows loaded ahead of use
 constexpr int SWEEP_PPF_N = 1;    // narrow sweep: DCT-distance rows loaded ahead of use
 constexpr int SWEEP_OUT_N = 28;   // narrow sweep: 32 lanes x 1 column, 2 of halo each side
 constexpr int SWEEP_WARPS_N = 8;  // narrow sweep: warps per block
+constexpr int SWEEP_OUT_Q = 120;  // quad sweep: output columns per warp strip (32 lanes x 4 columns, 4 of halo each side)
+constexpr int SWEEP_WARPS_Q = 4;  // quad sweep: warps per block
+constexpr int SWEEP_MIN_BLOCKS_Q = 2;
+constexpr int SWEEP_PF_Q = 2;     // quad sweep: y rows loaded ahead of use
+constexpr int SWEEP_PPF_Q = 1;    // quad sweep: DCT-distance rows loaded ahead of use
 constexpr int PROJ_WARPS = 4;   // warps per projection block (4 coefficient blocks per warp)
 
 // ---------------------------------------------------------------- transforms

@@ -399,12 +399,12 @@ def learned_comparison(lib, device, steps, warmup, refine=REFINE_ITERATIONS, qua
         el_plain_step = evaluate()[0]
         run(img, 0, N.ART_INIT_LEARNED, None)
         e_start = evaluate()[0]
-        kmin, ek_min = None, None
+        kmin, ek_min, fk_min = None, None, None
         for k in ladder:
             run(img, k, N.ART_INIT_LEARNED, refine_schedule(k))
             ek, fk = evaluate()
             if ek <= e50 * (1 + 1e-4) and fk <= 1e-3:
-                kmin, ek_min = k, ek
+                kmin, ek_min, fk_min = k, ek, fk
                 break
         kmin_ms = timed(img, kmin, N.ART_INIT_LEARNED, refine_schedule(kmin)) if kmin else None
         dk = None
@@ -421,6 +421,7 @@ def learned_comparison(lib, device, steps, warmup, refine=REFINE_ITERATIONS, qua
                          reaches_plain50=bool(el <= e50 * (1 + 1e-4) and fl <= 1e-3),
                          min_refine_to_reach=kmin,
                          min_refine_E_rel=((ek_min - e50) / e50) if kmin else None,
+                         min_refine_infeasibility=fk_min,
                          min_refine_decoded_same_schedule_E_rel=dk,
                          min_refine_ms=kmin_ms, min_refine_speedup=(plain_ms / kmin_ms) if kmin_ms else None))
         log(f"learned q{q}: plain50 {plain_ms:.3f} ms E {e50:.7g}; learned+{refine} {learned_ms:.3f} ms "
@@ -504,6 +505,89 @@ def hbm_iteration(lib, device, steps, warmup, peak):
             "bytes_moved_per_iteration": moved, "moved_gbs": moved / (it_ms * 1e-3) / 1e9,
             "gradient_launch_ms": statistics.mean(gs), "projection_launch_ms": statistics.mean(us),
             "source": "whole 100-iteration solves, CUDA events, L2 flushed between solves; iteration = solve / 100"}
+
+
+def batch_block(lib, device, steps, warmup, peak):
+    """The 256-image batch inside the default run: its device-resident batched
+    solve (CUDA events, L2 flushed between solves, 50 iterations), the
+    iteration against the algorithmic bytes, and JPEG bytes -> RGB8 through
+    the decode pipeline (batched solves)."""
+    import torch
+
+    from artefact_b200 import _native as N
+
+    encoded = []
+    jpegs = make_workload("batch256", encoded)
+    iters = WORKLOADS["batch256"]["iterations"]
+    keep = []
+    imgs = (N.ArtImage * len(jpegs))()
+    for i, j in enumerate(jpegs):
+        W, H, _ = j.max_rounded()
+        n = j.nchannel
+        cd = (N.ArtChannel * n)()
+        for c, co in enumerate(j.coefs):
+            dev = torch.from_numpy(co.dct_coefs.copy()).cuda()
+            q = np.ascontiguousarray(co.quant_table, np.float32)
+            keep += [dev, q]
+            a = cd[c]
+            a.rounded_px_w, a.rounded_px_h, a.block_w, a.block_h = co.rounded_px_w, co.rounded_px_h, co.block_w, co.block_h
+            a.samp_h, a.samp_v, a.coef_type = co.horizontal_samp_factor, co.vertical_samp_factor, N.ART_COEF_I16
+            a.dct_coefs = dev.data_ptr()
+            a.quant_table = q.ctypes.data_as(C.POINTER(C.c_float))
+        pitch = (W + 31) // 32 * 32
+        outs = [torch.empty(H, pitch, device="cuda") for _ in range(n)]
+        ptrs = (C.c_void_p * n)(*[o.data_ptr() for o in outs])
+        keep += [cd, outs, ptrs]
+        im = imgs[i]
+        im.nchannel, im.max_rounded_px_w, im.max_rounded_px_h, im.out_pitch = n, W, H, pitch
+        im.channels = C.cast(cd, C.POINTER(N.ArtChannel))
+        im.weight = WEIGHT
+        im.pweight = (C.c_float * 3)(PWEIGHT, PWEIGHT, PWEIGHT)
+        im.out_planes = C.cast(ptrs, C.POINTER(C.c_void_p))
+    from artefact_b200.api import Context
+
+    context = Context(device)
+    ctx = context.handle
+    stream = torch.cuda.current_stream()
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")
+    # Autotune on the batch itself (host coefficients, 5 iterations per candidate).
+    tr = context.autotune_batch([dict(coefs=j.coefs, weight=WEIGHT, pweight=[PWEIGHT] * 3) for j in jpegs], 5)
+    tuned = {"sweep_variant": "wide" if tr["variant"] else "narrow", "strip_rows": tr["strip_rows"],
+             "projection_warps": tr["proj_warps"], "candidates": tr["candidates"],
+             "tuned_ms_per_5_iterations": tr["best_ms"], "heuristic_ms_per_5_iterations": tr["heuristic_ms"]}
+
+    def solve():
+        N.check(lib.art_context_compute_batch_device(ctx, len(jpegs), imgs, iters, None, C.c_void_p(stream.cuda_stream)))
+
+    for _ in range(warmup):
+        solve()
+    torch.cuda.synchronize()
+    ms = []
+    for k in range(steps):
+        flush.fill_(float(k))
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record(stream)
+        solve()
+        b.record(stream)
+        b.synchronize()
+        ms.append(a.elapsed_time(b))
+    N.check(lib.art_context_synchronize(ctx))
+    context.close()
+    del keep, flush
+    torch.cuda.empty_cache()
+    mpix = sum(j.real_px_w * j.real_px_h for j in jpegs) / 1e6
+    solve_ms = statistics.median(ms)
+    ib = iteration_bytes(jpegs)
+    it_ms = solve_ms / iters
+    pipe = pipeline_e2e(encoded, iters, device)
+    return {"workload": WORKLOADS["batch256"]["name"], "images": len(jpegs), "mpix": mpix, "solve_ms": solve_ms,
+            "steps": steps, "mpix_s": mpix / solve_ms * 1e3, "iteration_ms": it_ms,
+            "algorithmic_bytes_per_iteration": ib, "gbs": ib / (it_ms * 1e-3) / 1e9,
+            "frac_of_hbm": ib / (it_ms * 1e-3) / 1e9 / peak,
+            "source": "device-resident batched solves (art_context_compute_batch_device), CUDA events, L2 flushed "
+                      "between solves; iteration = solve / 50",
+            "autotuned": tuned,
+            "decode_pipeline": pipe}
 
 
 def network_flops(H, W):
@@ -634,15 +718,29 @@ def pipeline_e2e(datas, iterations, device):
         process_jpeg(j, [WEIGHT] * 3, [PWEIGHT] * 3, [iterations] * 3, False, context=ctx)
     serial = time.perf_counter() - t
     ctx.close()
-    decoders = max(1, min(12, (os.cpu_count() or 4) - 2))
+    decoders = max(1, min(16, (os.cpu_count() or 4) - 2))
+    batch_images, batch_pixels = 32, 32 << 20
+    # Warm-up of the batched path, then the timed stream.
+    sum(1 for _ in process_stream(datas[:8], [WEIGHT] * 3, [PWEIGHT] * 3, [iterations] * 3, decoders=decoders,
+                                  solvers=2, batch_images=4, device=device))
     t = time.perf_counter()
     n = sum(1 for _ in process_stream(datas, [WEIGHT] * 3, [PWEIGHT] * 3, [iterations] * 3, decoders=decoders,
-                                      solvers=2, depth=2 * decoders, device=device))
+                                      solvers=2, batch_images=batch_images, batch_pixels=batch_pixels,
+                                      device=device))
     piped = time.perf_counter() - t
     assert n == len(datas)
+    # Host decode alone on the same threads, for the bound it sets.
+    from concurrent.futures import ThreadPoolExecutor
+
+    t = time.perf_counter()
+    with ThreadPoolExecutor(decoders) as ex:
+        list(ex.map(lambda d: Jpeg.from_source(JpegSource.Buffer(d)), datas))
+    decode = time.perf_counter() - t
     return {"serial_mpix_s": mpix / serial, "pipelined_mpix_s": mpix / piped, "images": len(datas),
-            "decoders": decoders, "solver_contexts": 2,
-            "what": "JPEG bytes -> RGB8 (host decode, H2D, solve, RGB, D2H)"}
+            "decode_only_mpix_s": mpix / decode, "decoders": decoders, "solver_contexts": 2,
+            "batch_images": batch_images, "batch_pixels": batch_pixels,
+            "what": "JPEG bytes -> RGB8 (host decode, H2D, batched solve, RGB, D2H), wall clock; serial = one "
+                    "image after the other through process_jpeg"}
 
 
 def cpu_sample(kind, jpegs, iterations):
@@ -739,6 +837,8 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-learned", action="store_true", help="skip the learned warm-start comparison")
     ap.add_argument("--no-hbm", action="store_true", help="skip the 6000x4000 HBM iteration block of the default run")
+    ap.add_argument("--no-batch", action="store_true", help="skip the 256-image batch block of the default run")
+    ap.add_argument("--no-tune", action="store_true", help="solve with the size heuristic's launch shapes")
     args = ap.parse_args()
 
     rank = int(os.environ.get("RANK", "0"))
@@ -829,6 +929,17 @@ def main():
     ctx = C.c_void_p()
     N.check(lib.art_context_create(local, C.byref(ctx)))
     stream = torch.cuda.current_stream()
+    # Autotune the launch shapes on the workload itself (10 iterations per
+    # candidate, host coefficients); the solves below use the choice.
+    tuned = None
+    if not args.no_tune:
+        tr = N.ArtTuneResult()
+        N.check(lib.art_context_autotune_batch(ctx, nimg, imgs_host, 10, C.byref(tr)))
+        tuned = {"sweep_variant": "wide" if tr.variant else "narrow", "strip_rows": tr.strip_rows,
+                 "projection_warps": tr.proj_warps, "candidates": tr.candidates,
+                 "tuned_ms_per_10_iterations": tr.best_ms, "heuristic_ms_per_10_iterations": tr.heuristic_ms,
+                 "heuristic": {"sweep_variant": "wide" if tr.heuristic_variant else "narrow",
+                               "strip_rows": tr.heuristic_strip_rows, "projection_warps": 4}}
 
     def solve_device():
         if nimg == 1:
@@ -951,23 +1062,31 @@ def main():
     hbm = None
     if args.workload == "1080p" and world == 1 and not args.no_hbm:
         hbm = hbm_iteration(lib, local, 3, 1, peak)
+    # The 256-image batch and its decode pipeline inside the default run.
+    batch = None
+    if args.workload == "1080p" and world == 1 and not args.no_batch:
+        batch = batch_block(lib, local, 3, 1, peak)
 
-    # Learned warm start on the same image (1080p only, one GPU): 8 and the
-    # fewest ladder iterations that reach the plain 50-iteration objective.
+    # Learned warm start (one GPU) on the learned workload's 1080p 4:2:0
+    # images at q30/50/75: 8 iterations, and the fewest ladder iterations that
+    # reach the plain 50-iteration objective.
     learned = None
     if args.workload == "1080p" and world == 1 and not args.no_learned:
-        res = learned_comparison(lib, local, min(args.steps, 10), args.warmup, images=[(75, jpegs[0])],
-                                 ladder=(8, 16, 24, 32))
+        res = learned_comparison(lib, local, min(args.steps, 10), args.warmup,
+                                 ladder=(8, 10, 12, 14, 16, 20, 24, 28, 32, 40, 48))
         if res is not None:
-            r = res["images"][0]
-            learned = {"schedule": res["schedule"], "refine_iterations": res["refine_iterations"],
-                       "mpix_s": r["learned_mpix_s"], "ms": r["learned_ms"], "E_rel_to_plain50": r["E_learned_rel"],
-                       "speedup_vs_plain50": r["speedup"],
-                       "iterations_to_reach_plain50": r["min_refine_to_reach"],
-                       "reach_mpix_s": (mpix / r["min_refine_ms"] * 1e3) if r["min_refine_ms"] else None,
-                       "reach_speedup_vs_plain50": r["min_refine_speedup"],
-                       "reach_E_rel": r["min_refine_E_rel"],
-                       "decoded_start_same_iterations_E_rel": r["min_refine_decoded_same_schedule_E_rel"]}
+            rows = res["images"]
+            learned = {"workload": WORKLOADS["learned"]["name"], "schedule": res["schedule"],
+                       "refine_iterations": res["refine_iterations"], "plain50_mpix_s": res["plain50_mpix_s"],
+                       "mpix_s": res["learned_mpix_s"], "speedup_vs_plain50": res["learned_mpix_s"] / res["plain50_mpix_s"],
+                       "max_E_rel_to_plain50": max(r["E_learned_rel"] for r in rows),
+                       "iterations_to_reach_plain50": [r["min_refine_to_reach"] for r in rows],
+                       "reach_mpix_s": res["reach_mpix_s"],
+                       "reach_speedup_vs_plain50": (res["reach_mpix_s"] / res["plain50_mpix_s"]) if res["reach_mpix_s"] else None,
+                       "reach_E_rel": [r["min_refine_E_rel"] for r in rows],
+                       "reach_infeasibility": [r["min_refine_infeasibility"] for r in rows],
+                       "decoded_start_same_iterations_E_rel": [r["min_refine_decoded_same_schedule_E_rel"] for r in rows],
+                       "images": rows}
 
     # Host decode overlapped with solving (batch workload, one GPU).
     pipe = None
@@ -998,9 +1117,12 @@ def main():
             "event_timing_pass": {"loop_ms_per_iteration": loop / iters, "gradient_ms": g_launch,
                                   "update_ms": u_launch},
             "cpu_baseline": cpu, "gpu_launches": args.steps * per_step, "clocks": clocks, "wall_s": wall,
+            "autotuned": tuned,
         }
         if hbm is not None:
             line["hbm_iteration"] = hbm
+        if batch is not None:
+            line["batch256"] = batch
         if learned is not None:
             line["learned_warm_start"] = learned
         if pipe is not None:

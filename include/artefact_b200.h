@@ -68,7 +68,10 @@ typedef struct ArtOptions {
                                  radius / sqrt(1 + tail_step_iterations) -- large steps first to remove a warm
                                  start's error, then small ones to settle. No reference counterpart. */
     uint32_t tail_step_iterations;
-    uint32_t reserved[3];
+    float step_decay;         /* 0: constant steps in the first phase (the reference). In (0, 1]: step k of the
+                                 first phase is step_decay^k times the solve's step, so a warm start's
+                                 refinement can shrink its steps geometrically. No reference counterpart. */
+    uint32_t reserved[2];
 } ArtOptions;
 
 typedef struct ArtContext ArtContext;
@@ -161,20 +164,69 @@ int32_t art_context_compute_batch_device(ArtContext *ctx, uint32_t nimages, cons
                                          uint32_t iterations, const ArtOptions *opts, void *stream);
 
 /*
- * Autotuner. Times both gradient-sweep variants (0 = narrow, one column per
- * lane; 1 = wide, two columns per lane on packed FP32x2 arithmetic) at each
- * strip height (16, 32, 64, 128 rows) on a deterministic synthetic image of
- * the given geometry (`iterations` steps, 0 = 10) and caches the fastest pair
- * for the geometry's bucket (channel count, sampling, width and height rounded
- * up to powers of two); later solves of images in that bucket use it. The two
- * variants sum the same terms in a different order (results agree to fp32
- * rounding), and each is deterministic. art_context_tune_cache saves
- * (save != 0) or loads the cache as a text file of
- * "<bucket> <variant> <rows>" lines. Either output pointer may be NULL.
+ * art_context_process for many decoded images at once: each image's solves
+ * (one joint solve of a 3-component image unless `separate`, else one per
+ * component reading pweight[0], lib.rs:122-153) all run in one batched solve
+ * of `iterations` steps, then the fused output stage (lib.rs:159-211) writes
+ * each image's real_h*real_w*3 RGB bytes to its host rgb_out (NULL skips it).
+ * Per image the RGB equals art_context_process's with iterations[c] =
+ * `iterations`. Host coefficients; returns when done.
+ * Replaces: a loop of Artefact::process calls after Jpeg::from,
+ * backend/artefact-lib/lib.rs:105-212.
  */
+typedef struct ArtProcessImage {
+    uint32_t nchannel;          /* 1..4 components */
+    uint32_t real_w, real_h;    /* real image size (crop of the rounded planes) */
+    uint32_t reserved;
+    const ArtChannel *channels; /* host coefficients */
+    float weight[3];            /* joint solve: weight[0]; separate: weight[c] (weight[2] for a 4th) */
+    float pweight[3];
+    uint8_t *rgb_out;
+} ArtProcessImage;
+int32_t art_context_process_batch(ArtContext *ctx, uint32_t nimages, const ArtProcessImage *images,
+                                  uint32_t iterations, int32_t separate, const ArtOptions *opts);
+
+/*
+ * Autotuner (no reference counterpart). It picks the launch shapes of the two
+ * kernels of an iteration: the gradient sweep's variant (0 = narrow, one
+ * column per lane; 1 = wide, two columns per lane on packed FP32x2
+ * arithmetic; 2 = quad, four columns per lane, float4 loads and stores and
+ * packed FP32x2 arithmetic) and strip height (16, 32, 64 or 128 rows), then the
+ * projection's warps per block (2, 4 or 8; blocks per SM follow from it and
+ * the shared memory a warp stages). Candidates are timed on the GPU
+ * (`iterations` steps, 0 = 10; each captured and warmed once, then timed 5
+ * times, median), sweep first with the projection at 4 warps, then the
+ * projection with the chosen sweep. The size heuristic's choice is tried
+ * first and the first candidate within 2 % of the fastest wins, so the
+ * choice changes only for a clear gain and repeats from run to run. The
+ * variants sum the same terms in different orders (results agree to fp32
+ * rounding), and each is deterministic.
+ *
+ * art_context_autotune tunes one geometry on a deterministic synthetic image
+ * and caches the choice for its bucket (channel count, sampling, width and
+ * height rounded up to powers of two); later solves of images in that bucket
+ * use it. art_context_autotune_batch tunes on the given batch itself (host
+ * coefficients, as art_context_compute_batch takes them) and caches the
+ * choice for batches of its bucket (image count and total pixels rounded up to
+ * powers of two), which takes precedence over the per-image buckets in batched
+ * solves. art_context_last_tune returns the last run's choice and timings.
+ * art_context_tune_cache saves (save != 0) or loads the cache as a text file
+ * of "<bucket> <variant> <rows> <projection warps>" lines (three-field lines
+ * keep 4 projection warps). Output pointers may be NULL.
+ */
+typedef struct ArtTuneResult {
+    uint32_t variant, strip_rows, proj_warps; /* the choice */
+    uint32_t candidates;                      /* candidates timed */
+    float best_ms;                            /* the choice's median time for `iterations` steps */
+    float heuristic_ms;                       /* the size heuristic's shape (4 projection warps), same measure */
+    uint32_t heuristic_variant, heuristic_strip_rows;
+} ArtTuneResult;
 int32_t art_context_autotune(ArtContext *ctx, uint32_t nchannel, const uint32_t *samp_h, const uint32_t *samp_v,
                              uint32_t max_rounded_px_w, uint32_t max_rounded_px_h, uint32_t iterations,
                              uint32_t *variant_out, uint32_t *strip_rows_out);
+int32_t art_context_autotune_batch(ArtContext *ctx, uint32_t nimages, const ArtImage *images, uint32_t iterations,
+                                   ArtTuneResult *out);
+int32_t art_context_last_tune(ArtContext *ctx, ArtTuneResult *out);
 int32_t art_context_tune_cache(ArtContext *ctx, const char *path, int32_t save);
 
 /*

@@ -51,7 +51,7 @@ def lib() -> C.CDLL:
             f2 = getattr(h, f"oracle_{prec}_compute_from")
             f2.restype = C.c_int
             f2.argtypes = [C.c_uint32, CH, C.c_float, FP, C.c_uint32, C.c_uint32, C.c_uint32, C.c_uint32,
-                           C.c_uint32, C.c_uint32, C.c_int, C.POINTER(FP), C.POINTER(P)]
+                           C.c_float, C.c_uint32, C.c_uint32, C.c_int, C.POINTER(FP), C.POINTER(P)]
             g = getattr(h, f"oracle_{prec}_gradient")
             g.restype = C.c_int
             g.argtypes = [C.c_uint32, CH, C.c_float, FP, C.c_uint32, C.c_uint32, C.POINTER(P), C.POINTER(P)]
@@ -108,10 +108,11 @@ def compute(nch: int, coefs, weight: float, pweight, iterations: int, W: int, H:
 
 def compute_from(nch: int, coefs, weight: float, pweight, iterations: int, W: int, H: int, start,
                  step_iterations: int = 0, fp64: bool = False, tail_iterations: int = 0,
-                 tail_step_iterations: int = 0) -> List[np.ndarray]:
+                 tail_step_iterations: int = 0, step_decay: float = 0.0) -> List[np.ndarray]:
     """The oracle's iteration from given full-resolution start planes (a warm
     start): projection of the start, then `iterations` steps of size
-    radius / sqrt(1 + (step_iterations or iterations)); the last
+    radius / sqrt(1 + (step_iterations or iterations)), step k of the first
+    phase scaled by step_decay^k when step_decay > 0; the last
     `tail_iterations` restart FISTA with steps radius / sqrt(1 + tail_step_iterations)."""
     h = lib()
     chans, keep = _channels(coefs[:nch])
@@ -123,7 +124,7 @@ def compute_from(nch: int, coefs, weight: float, pweight, iterations: int, W: in
     ptrs = (C.POINTER(ct) * nch)(*[o.ctypes.data_as(C.POINTER(ct)) for o in outs])
     fn = h.oracle_f64_compute_from if fp64 else h.oracle_f32_compute_from
     rc = fn(nch, chans, float(weight), _pw(pweight), int(iterations), int(step_iterations), int(tail_iterations),
-            int(tail_step_iterations), W, H, 0, sp, ptrs)
+            int(tail_step_iterations), float(step_decay), W, H, 0, sp, ptrs)
     if rc != 0:
         raise ValueError("oracle rejected its input")
     return outs

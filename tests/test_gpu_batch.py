@@ -46,10 +46,13 @@ def test_autotune_and_cache_roundtrip(gpu, tmp_path):
     W, H, N_ = j.max_rounded()
     with Context(0) as ctx:
         kind, rows = ctx.autotune(3, [1, 2, 2], [1, 2, 2], W, H, iterations=5)
-        assert kind in (0, 1) and rows in (16, 32, 64, 128)
+        assert kind in (0, 1, 2) and rows in (16, 32, 64, 128)
+        res = ctx.last_tune()
+        assert (res["variant"], res["strip_rows"]) == (kind, rows) and res["proj_warps"] in (2, 4, 8)
+        assert res["candidates"] >= 3 and res["best_ms"] <= res["heuristic_ms"] * 1.0001
         path = tmp_path / "tune.txt"
         ctx.save_tune_cache(path)
-        assert f" {kind} {rows}\n" in path.read_text()
+        assert f" {kind} {rows} {res['proj_warps']}\n" in path.read_text()
         tuned = ctx.compute(3, j.coefs, 0.3, [0.001] * 3, 20, W, H)
     with Context(0) as ctx2:
         ctx2.load_tune_cache(path)
@@ -57,25 +60,67 @@ def test_autotune_and_cache_roundtrip(gpu, tmp_path):
     assert all(np.array_equal(a, b) for a, b in zip(tuned, again))
     ref = O.compute(3, j.coefs, 0.3, [0.001] * 3, 20, W, H)
     assert max(float(np.abs(a - b).max()) for a, b in zip(tuned, ref)) <= MAX_ABS
+    # Three-field lines (no projection shape) still load.
+    old = tmp_path / "old.txt"
+    old.write_text("n3-s112222-w512-h512 0 32\n")
+    with Context(0) as ctx3:
+        ctx3.load_tune_cache(old)
+
+
+def test_autotune_batch(gpu, tmp_path):
+    """The batch tuner times the shapes on the batch itself; later batches of
+    its bucket use the choice, and their results still match the oracle."""
+    shapes = [(96, 64, 75, "4:2:0", False), (40, 24, 50, "4:4:4", True), (130, 70, 30, "4:4:4", False),
+              (200, 136, 90, "4:2:0", False), (64, 48, 60, "4:2:2", False)]
+    jpegs = [_jpeg(*s, seed=800 + i) for i, s in enumerate(shapes)]
+    jobs = [dict(coefs=j.coefs) for j in jpegs]
+    with Context(0) as ctx:
+        res = ctx.autotune_batch(jobs, iterations=5)
+        assert res["variant"] in (0, 1, 2) and res["strip_rows"] in (16, 32, 64, 128) and res["proj_warps"] in (2, 4, 8)
+        assert res["best_ms"] <= res["heuristic_ms"] * 1.0001
+        path = tmp_path / "tune.txt"
+        ctx.save_tune_cache(path)
+        assert "batch-i8-" in path.read_text()
+        a = ctx.compute_batch(jobs, 12)
+        b = ctx.compute_batch(jobs, 12)
+    assert all(np.array_equal(x, y) for pa, pb in zip(a, b) for x, y in zip(pa, pb))
+    for j, got in zip(jpegs, a):
+        check_parity(j, 12, label=f"tuned batch {j.real_px_w}x{j.real_px_h}", gpu=got)
 
 
 @pytest.mark.parametrize("shape", [(72, 40, "4:2:0", False), (200, 136, "4:4:4", False), (128, 96, "4:2:2", False),
                                    (96, 64, "4:4:4", True)])
-def test_sweep_variants_agree(gpu, monkeypatch, shape):
-    """The narrow and the wide gradient sweep at every strip height match the
-    oracle, and each (variant, height) is deterministic."""
+def test_every_tuning_candidate_agrees(gpu, monkeypatch, shape):
+    """Every launch shape the autotuner may choose -- narrow, wide and quad
+    sweep at each strip height, and 2, 4 or 8 projection warps per block --
+    matches the oracle, and each is deterministic."""
     w, h, sub, gray = shape
     j = _jpeg(w, h, 80, sub, gray, seed=900 + w)
     W, H, N_ = j.max_rounded()
-    for kind in (0, 1):
+    n = j.nchannel
+    its = 30
+    for kind in (0, 1, 2):
         for rows in (16, 32, 64, 128):
-            monkeypatch.setenv("ART_SWEEP_KIND", str(kind))
-            monkeypatch.setenv("ART_STRIP_ROWS", str(rows))
-            with Context(0) as ctx:
-                a = ctx.compute(j.nchannel, j.coefs, 0.3, [0.001] * 3, 30, W, H)
-                b = ctx.compute(j.nchannel, j.coefs, 0.3, [0.001] * 3, 30, W, H)
-            assert all(np.array_equal(x, y) for x, y in zip(a, b))
-            check_parity(j, 30, label=f"sweep variant {kind} rows {rows}", gpu=a)
+            for pw in (2, 4, 8):
+                monkeypatch.setenv("ART_SWEEP_KIND", str(kind))
+                monkeypatch.setenv("ART_STRIP_ROWS", str(rows))
+                monkeypatch.setenv("ART_PROJ_WARPS", str(pw))
+                with Context(0) as ctx:
+                    a = ctx.compute(n, j.coefs, 0.3, [0.001] * 3, its, W, H)
+                    b = ctx.compute(n, j.coefs, 0.3, [0.001] * 3, its, W, H)
+                label = f"{shape} sweep {kind} rows {rows} projection warps {pw}"
+                assert all(np.array_equal(x, y) for x, y in zip(a, b)), label
+                check_parity(j, its, label=label, gpu=a)
+    # The projection shape does not change the arithmetic: 2, 4 and 8 warps
+    # give identical planes for one sweep shape.
+    outs = []
+    for pw in (2, 4, 8):
+        monkeypatch.setenv("ART_SWEEP_KIND", "0")
+        monkeypatch.setenv("ART_STRIP_ROWS", "32")
+        monkeypatch.setenv("ART_PROJ_WARPS", str(pw))
+        with Context(0) as ctx:
+            outs.append(ctx.compute(n, j.coefs, 0.3, [0.001] * 3, its, W, H))
+    assert all(np.array_equal(x, y) for o in outs[1:] for x, y in zip(o, outs[0]))
 
 
 def test_learned_batch_matches_single_learned_solves(gpu):

@@ -45,6 +45,28 @@ def test_config3_band_100_iterations(gpu):
     check_parity(j, 100, label="6000x512 band of the 6000x4000 4:4:4 q30 image")
 
 
+def test_config2_every_sweep_variant(gpu, monkeypatch):
+    """1920x1080 4:2:0 q75 at 50 iterations with each gradient-sweep variant
+    the autotuner may pick (narrow, wide, quad) at 16- and 32-row strips,
+    against one oracle run."""
+    j = _jpeg(synth.make_jpeg(1920, 1080, 75, "4:2:0", False, seed=2000))
+    W, H, _ = j.max_rounded()
+    ref = O.compute(3, j.coefs, WEIGHT, PW, 50, W, H)
+    er = O.objective(3, j.coefs, WEIGHT, PW, W, H, ref)
+    for kind in (0, 1, 2):
+        for rows in (16, 32):
+            monkeypatch.setenv("ART_SWEEP_KIND", str(kind))
+            monkeypatch.setenv("ART_STRIP_ROWS", str(rows))
+            with Context(0) as ctx:
+                got = ctx.compute(3, j.coefs, WEIGHT, PW, 50, W, H)
+            d = max(float(np.abs(a - b).max()) for a, b in zip(got, ref))
+            eg = O.objective(3, j.coefs, WEIGHT, PW, W, H, got)
+            feas = O.feasibility(3, j.coefs, W, H, got)
+            print(f"sweep {kind} rows {rows}: max|gpu-oracle|={d:.3g} objective rel {abs(eg - er) / er:.2g} "
+                  f"feasibility {feas:.2g}")
+            assert d <= 1.0 and abs(eg - er) <= 1e-4 * er and feas <= 1e-3, (kind, rows)
+
+
 def test_config4_batch_extremes(gpu):
     specs = synth.batch_specs(256, seed=4000)
     with ThreadPoolExecutor(max_workers=16) as ex:

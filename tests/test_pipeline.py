@@ -1,7 +1,9 @@
 """Overlapped decode + solve of many JPEGs (artefact_b200.pipeline).
 
-CPU: order, depth and error propagation with a stand-in solver (the host
-decoder is real). GPU: the images equal process_jpeg's, one by one.
+CPU: order, depth, batch budgets and error propagation with a stand-in solver
+(the host decoder is real). GPU: the images equal process_jpeg's, one by one,
+whether solved in batches (art_context_process_batch) or image by image, in
+joint and separate mode.
 """
 import numpy as np
 import pytest
@@ -24,11 +26,13 @@ def test_order_and_depth_with_stand_in_solver():
         seen.append((j.real_px_w, j.real_px_h))
         return np.full((j.real_px_h, j.real_px_w, 3), len(seen), np.uint8)
 
-    for depth in (1, 2, 5, 16):
-        seen.clear()
-        outs = list(process_stream(_datas(), decoders=3, solvers=2, depth=depth, solve=fake))
-        assert [(o.shape[1], o.shape[0]) for o in outs] == [(w, h) for w, h, _, _ in SHAPES]
-        assert sorted(seen) == sorted((w, h) for w, h, _, _ in SHAPES)
+    for depth in (0, 1, 2, 5, 16):
+        for batch_images, batch_pixels in ((1, 1 << 30), (2, 1 << 30), (32, 3000), (32, 1 << 30)):
+            seen.clear()
+            outs = list(process_stream(_datas(), decoders=3, solvers=2, depth=depth, batch_images=batch_images,
+                                       batch_pixels=batch_pixels, solve=fake))
+            assert [(o.shape[1], o.shape[0]) for o in outs] == [(w, h) for w, h, _, _ in SHAPES]
+            assert sorted(seen) == sorted((w, h) for w, h, _, _ in SHAPES)
 
 
 def test_decode_errors_surface_in_order():
@@ -46,16 +50,21 @@ def test_decode_errors_surface_in_order():
 
 
 def test_rejects_bad_arguments():
-    with pytest.raises(ValueError):
-        list(process_stream(_datas(), depth=0))
+    for kw in (dict(depth=-1), dict(batch_images=0), dict(batch_pixels=0), dict(solvers=0), dict(decoders=0)):
+        with pytest.raises(ValueError):
+            list(process_stream(_datas(), **kw))
 
 
 @pytest.mark.gpu
-def test_stream_equals_process_jpeg(gpu):
-    datas = _datas()
-    outs = list(process_stream(datas, (0.3,) * 3, (0.001,) * 3, (20,) * 3, decoders=3, solvers=2, depth=4,
-                               device=0))
+@pytest.mark.parametrize("batch_images", [1, 3, 32])
+@pytest.mark.parametrize("separate,iterations", [(False, (20, 20, 20)), (True, (12, 12, 12)), (True, (15, 8, 4))])
+def test_stream_equals_process_jpeg(gpu, batch_images, separate, iterations):
+    datas = _datas() + [synth.make_jpeg(37, 21, 50, "4:4:4", True, seed=44)]
+    weight, pweight = (0.3, 0.5, 0.2), (0.001, 0.002, 0.003)
+    outs = list(process_stream(datas, weight, pweight, iterations, separate, decoders=3, solvers=2,
+                               batch_images=batch_images, device=0))
+    assert len(outs) == len(datas)
     for d, o in zip(datas, outs):
         j = Jpeg.from_source(JpegSource.Buffer(d))
-        ref = process_jpeg(j, [0.3] * 3, [0.001] * 3, [20] * 3, False, device=0)
+        ref = process_jpeg(j, list(weight), list(pweight), list(iterations), separate, device=0)
         np.testing.assert_array_equal(o, ref)
