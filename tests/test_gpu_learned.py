@@ -118,6 +118,45 @@ def test_learned_start_matches_oracle(gpu, ctx, shape, iterations, step_iteratio
     assert ev["infeasibility"] <= 1e-3
 
 
+@pytest.mark.parametrize("shape", CASES[1:4], ids=IDS[1:4])
+@pytest.mark.parametrize("iterations,step_iterations,tail,tail_step,decay",
+                         [(8, 2, 2, 100, 0.8), (10, 1, 0, 0, 0.6), (6, 4, 2, 50, 0.95)])
+def test_step_decay_matches_oracle(gpu, ctx, shape, iterations, step_iterations, tail, tail_step, decay):
+    """A geometric first-phase step schedule (ArtOptions.step_decay) after a
+    learned start, against the oracle's iteration with the same schedule."""
+    j = jpeg_of(*shape)
+    W, H, _ = j.max_rounded()
+    n = j.nchannel
+    net = WS.WarmStartNet(_strong_params(7))
+    ctx.set_warm_start(net)
+    try:
+        got = ctx.compute(n, j.coefs, WEIGHT, PW, iterations, W, H, init_mode=N.ART_INIT_LEARNED,
+                          step_iterations=step_iterations, tail_iterations=tail, tail_step_iterations=tail_step,
+                          step_decay=decay)
+        ev = ctx.evaluate()
+    finally:
+        ctx.set_warm_start(None)
+    start = _upsampled_prediction(net, j)
+    ref = O.compute_from(n, j.coefs, WEIGHT, PW, iterations, W, H, start, step_iterations, tail_iterations=tail,
+                         tail_step_iterations=tail_step, step_decay=decay)
+    d = max(float(np.abs(a.astype(np.float64) - b).max()) for a, b in zip(got, ref))
+    er = O.objective(n, j.coefs, WEIGHT, PW, W, H, ref)
+    assert d <= 1.0
+    assert abs(ev["E"] - er) <= 1e-4 * abs(er)
+    assert ev["infeasibility"] <= 1e-3
+    # The schedule changes the result: without the decay it differs.
+    plain = O.compute_from(n, j.coefs, WEIGHT, PW, iterations, W, H, start, step_iterations, tail_iterations=tail,
+                           tail_step_iterations=tail_step)
+    assert max(float(np.abs(a - b).max()) for a, b in zip(plain, ref)) > 0
+
+
+def test_step_decay_is_validated(gpu, ctx):
+    j = jpeg_of(*CASES[0])
+    W, H, _ = j.max_rounded()
+    with pytest.raises(N.ArtError, match="step_decay"):
+        ctx.compute(j.nchannel, j.coefs, WEIGHT, PW, 2, W, H, step_decay=1.5)
+
+
 @pytest.mark.parametrize("shape", CASES[:3], ids=IDS[:3])
 def test_zero_residual_start_equals_decoded_start(gpu, ctx, shape):
     """With a zero head the prediction is the decoded image, whose projection

@@ -120,3 +120,22 @@ def test_rgb_output_stage_truncates():
     assert out[0, 2].tolist() == [140, 137, 138]
     gray = O.rgb(1, 4, 4, 1, planes[:1])
     assert gray[0, 2].tolist() == [138, 138, 138]
+
+
+def test_compute_from_step_decay():
+    """A step decay of 1 is the constant schedule; a smaller one changes the
+    result and keeps the planes feasible."""
+    from artefact_b200 import synth
+    from artefact_b200.api import Jpeg, JpegSource
+
+    j = Jpeg.from_source(JpegSource.Buffer(synth.make_jpeg(48, 32, 60, "4:2:0", False, seed=9)))
+    W, H, _ = j.max_rounded()
+    start = O.compute(3, j.coefs, 0.3, [0.001] * 3, 0, W, H)
+    a = O.compute_from(3, j.coefs, 0.3, [0.001] * 3, 6, W, H, start, 2, tail_iterations=2, tail_step_iterations=50)
+    b = O.compute_from(3, j.coefs, 0.3, [0.001] * 3, 6, W, H, start, 2, tail_iterations=2, tail_step_iterations=50,
+                       step_decay=1.0)
+    c = O.compute_from(3, j.coefs, 0.3, [0.001] * 3, 6, W, H, start, 2, tail_iterations=2, tail_step_iterations=50,
+                       step_decay=0.5)
+    assert all(np.array_equal(x, y) for x, y in zip(a, b))
+    assert any(not np.array_equal(x, y) for x, y in zip(a, c))
+    assert O.feasibility(3, j.coefs, W, H, c) <= 1e-3
