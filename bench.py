@@ -25,9 +25,12 @@ real image area.
 * e2e      -- the same through the public C ABI with host buffers
               (art_context_compute, or art_context_compute_batch), pinned host
               coefficients in and host planes out, copies inside the timed region.
-* roofline -- the dominant kernel's own I/O bytes per launch over its mean
+* roofline -- the dominant kernel's algorithmic bytes per launch (its
+              sweep of the two-sweep minimum: 8 N + 2 N_c per channel for the
+              gradient sweep, 12 N + 2 N_c for the projection) over its mean
               launch time, from CUDA event nodes inside the captured graph,
-              taken in a separate pass so they do not perturb `value`.
+              taken in a separate pass so they do not perturb `value`; the
+              kernel's own I/O bytes beside it.
 * iteration -- timed step / iterations against the algorithmic bytes
               sum_c (20 N + 4 N_c) (the two-sweep minimum).
 * cpu_baseline -- the oracle (fp32 C restatement of pipeline_scalar) on one
@@ -1030,24 +1033,29 @@ def main():
     g_launch = statistics.mean(grad_ms) / iters
     u_launch = statistics.mean(upd_ms) / iters
     loop = statistics.mean(loop_ms)
-    # Algorithmic bytes per launch (summed over the workload's images): the
-    # gradient sweep reads y and the DCT-distance plane (component resolution)
-    # and writes g; the projection reads y, g, x and the int16 coefficients and
-    # writes x, y and the DCT-distance plane. The iteration figure is the
-    # two-sweep minimum sum_c (20 N + 4 N_c).
-    grad_bytes = upd_bytes = iter_bytes = 0
+    # Algorithmic bytes per launch (summed over the workload's images), the
+    # two-sweep minimum per kernel: the gradient sweep reads x_k, x_{k-1} and
+    # the int16 coefficients (8 N + 2 N_c per channel), the projection the same
+    # again and writes x_{k+1} (12 N + 2 N_c); together sum_c (20 N + 4 N_c)
+    # per iteration. The kernels' own I/O is reported beside it: the sweep
+    # reads y and the DCT-distance plane and writes g (8 N + 4 N_c), the
+    # projection reads y, g, x and the coefficients and writes x, y and the
+    # DCT-distance plane (20 N + 6 N_c).
+    grad_bytes = upd_bytes = iter_bytes = grad_io = upd_io = 0
     for j in jpegs:
         W, H, _ = j.max_rounded()
         for co in j.coefs:
             nc = co.rounded_px_w * co.rounded_px_h
-            grad_bytes += 8 * W * H + 4 * nc
-            upd_bytes += 20 * W * H + 6 * nc
+            grad_bytes += 8 * W * H + 2 * nc
+            upd_bytes += 12 * W * H + 2 * nc
             iter_bytes += 20 * W * H + 4 * nc
+            grad_io += 8 * W * H + 4 * nc
+            upd_io += 20 * W * H + 6 * nc
     peak, peak_kind = load_peaks()
     if g_launch >= u_launch:
-        dom, dbytes, dms = "k_grad_sweep", grad_bytes, g_launch
+        dom, dbytes, dio, dms = "k_grad_sweep", grad_bytes, grad_io, g_launch
     else:
-        dom, dbytes, dms = "k_project", upd_bytes, u_launch
+        dom, dbytes, dio, dms = "k_project", upd_bytes, upd_io, u_launch
     achieved = dbytes / (dms * 1e-3) / 1e9
     traffic = read_traffic(args.workload, dom)
 
@@ -1107,7 +1115,8 @@ def main():
                     "api": "art_context_compute" if nimg == 1 else "art_context_compute_batch"},
             "roofline": {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": achieved / peak, "traffic": traffic, "peak_kind": peak_kind,
-                         "algorithmic_bytes_per_launch": dbytes, "launch_ms": dms},
+                         "algorithmic_bytes_per_launch": dbytes, "kernel_io_bytes_per_launch": dio,
+                         "kernel_io_gbs": dio / (dms * 1e-3) / 1e9, "launch_ms": dms},
             # From the timed steps: step time / iterations (the step's start-up
             # launches included, so this slightly understates the iteration).
             "iteration": {"ms": it_ms, "algorithmic_bytes": iter_bytes, "gbs": iter_bytes / (it_ms * 1e-3) / 1e9,
