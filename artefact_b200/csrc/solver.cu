@@ -2726,6 +2726,7 @@ int32_t art_context_autotune(ArtContext *ctx, uint32_t nchannel, const uint32_t 
         ch[c].coef_type = ART_COEF_I16;
         ch[c].quant_table = q;
         host[c].assign((size_t)ch[c].block_w * ch[c].block_h * 64, 0);
+        ch[c].dct_coefs = host[c].data();  // host values; staged to the device below
         for (size_t i = 0; i < host[c].size(); i++) {
             lcg = lcg * 1664525u + 1013904223u;
             if ((i & 63) == 0 || (lcg >> 28) == 0) host[c][i] = (int16_t)((int)((lcg >> 16) & 255) - 128);
