@@ -86,6 +86,10 @@ class ArtTuneResult(C.Structure):
     ]
 
 
+class ArtTuneCandidate(C.Structure):
+    _fields_ = [("variant", C.c_uint32), ("strip_rows", C.c_uint32), ("proj_warps", C.c_uint32), ("ms", C.c_float)]
+
+
 class ArtCnnConv(C.Structure):
     _fields_ = [
         ("B", C.c_int32), ("H", C.c_int32), ("W", C.c_int32),
@@ -149,6 +153,8 @@ EXPORTS = {
     "art_context_autotune_batch": (C.c_int32, [C.c_void_p, C.c_uint32, C.POINTER(ArtImage), C.c_uint32,
                                                C.POINTER(ArtTuneResult)]),
     "art_context_last_tune": (C.c_int32, [C.c_void_p, C.POINTER(ArtTuneResult)]),
+    "art_context_tune_candidates": (C.c_int32, [C.c_void_p, C.POINTER(ArtTuneCandidate), C.c_uint32,
+                                                C.POINTER(C.c_uint32)]),
     "art_context_tune_cache": (C.c_int32, [C.c_void_p, C.c_char_p, C.c_int32]),
     "art_context_synchronize": (C.c_int32, [C.c_void_p]),
     "art_context_set_warm_start": (C.c_int32, [C.c_void_p, C.c_void_p]),

@@ -469,13 +469,25 @@ class Context:
         imgs, _ = self._images(jobs, keep)
         r = N.ArtTuneResult()
         N.check(N.lib().art_context_autotune_batch(self._h, len(jobs), imgs, int(iterations), C.byref(r)))
-        return _tune_dict(r)
+        d = _tune_dict(r)
+        d["candidates_ms"] = self.tune_candidates()
+        return d
 
     def last_tune(self) -> dict:
         """Choice and timings of the last autotune run on this context."""
         r = N.ArtTuneResult()
         N.check(N.lib().art_context_last_tune(self._h, C.byref(r)))
-        return _tune_dict(r)
+        d = _tune_dict(r)
+        d["candidates_ms"] = self.tune_candidates()
+        return d
+
+    def tune_candidates(self) -> list:
+        """Every (variant, strip_rows, proj_warps, ms) the last autotune run timed."""
+        n = C.c_uint32()
+        N.check(N.lib().art_context_tune_candidates(self._h, None, 0, C.byref(n)))
+        arr = (N.ArtTuneCandidate * max(1, n.value))()
+        N.check(N.lib().art_context_tune_candidates(self._h, arr, n.value, C.byref(n)))
+        return [(c.variant, c.strip_rows, c.proj_warps, c.ms) for c in arr[:n.value]]
 
     def autotune(self, nchannel: int, samp_h: Sequence[int], samp_v: Sequence[int], max_w: int, max_h: int,
                  iterations: int = 10) -> tuple:

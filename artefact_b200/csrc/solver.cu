@@ -1317,6 +1317,7 @@ struct ArtContext {
     int proj_warps_override = 0;      // set while the autotuner times a candidate
     std::map<std::string, art::TuneChoice> tune;  // autotuned launch shapes by geometry bucket
     ArtTuneResult last_tune{};        // the last autotune run's choice and timings
+    std::vector<ArtTuneCandidate> tune_log;  // every candidate the last autotune run timed
 };
 
 namespace art {
@@ -2598,6 +2599,7 @@ int tune_specs(ArtContext *ctx, const std::vector<ImageSpec> &specs, uint32_t it
         max_h = std::max(max_h, sp.H);
     }
     const TuneChoice heur = pick_shape(ctx, specs[0], batch_px, (int)specs.size());
+    ctx->tune_log.clear();
     cudaEvent_t e0, e1;
     ART_CUDA(cudaEventCreate(&e0));
     ART_CUDA(cudaEventCreate(&e1));
@@ -2646,6 +2648,7 @@ int tune_specs(ArtContext *ctx, const std::vector<ImageSpec> &specs, uint32_t it
         float ms = 0.f;
         if ((rc = time_one(t, &ms))) break;
         timed1.push_back({t, ms});
+        ctx->tune_log.push_back(ArtTuneCandidate{(uint32_t)t.kind, (uint32_t)t.rows, (uint32_t)t.proj_warps, ms});
     }
     TuneChoice chosen;
     float chosen_ms = 0.f, default_ms = 0.f;
@@ -2660,6 +2663,7 @@ int tune_specs(ArtContext *ctx, const std::vector<ImageSpec> &specs, uint32_t it
             float ms = 0.f;
             if ((rc = time_one(t, &ms))) break;
             timed2.push_back({t, ms});
+            ctx->tune_log.push_back(ArtTuneCandidate{(uint32_t)t.kind, (uint32_t)t.rows, (uint32_t)t.proj_warps, ms});
         }
         if (!rc) {
             const auto p2 = pick(timed2);
@@ -2792,6 +2796,14 @@ int32_t art_context_autotune_batch(ArtContext *ctx, uint32_t nimages, const ArtI
         ctx->tune[tune_key(specs[0].nch, sh, sv, specs[0].W, specs[0].H)] = best;
     }
     if (out) *out = ctx->last_tune;
+    return ART_OK;
+}
+
+int32_t art_context_tune_candidates(ArtContext *ctx, ArtTuneCandidate *out, uint32_t capacity, uint32_t *count)
+{
+    if (!ctx || !count || (capacity && !out)) return fail(ART_ERR_INVALID_ARGUMENT, "null argument");
+    *count = (uint32_t)ctx->tune_log.size();
+    for (uint32_t i = 0; i < capacity && i < *count; i++) out[i] = ctx->tune_log[i];
     return ART_OK;
 }
 

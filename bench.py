@@ -116,6 +116,21 @@ def read_traffic(workload, kernel):
     return None
 
 
+SWEEP_NAMES = {0: "narrow", 1: "wide", 2: "quad"}
+
+
+def tune_candidates(lib, ctx):
+    """Every launch shape the context's last autotune run timed, with its time."""
+    from artefact_b200 import _native as N
+
+    n = C.c_uint32()
+    N.check(lib.art_context_tune_candidates(ctx, None, 0, C.byref(n)))
+    arr = (N.ArtTuneCandidate * max(1, n.value))()
+    N.check(lib.art_context_tune_candidates(ctx, arr, n.value, C.byref(n)))
+    return [{"sweep": SWEEP_NAMES[c.variant], "rows": c.strip_rows, "projection_warps": c.proj_warps, "ms": c.ms}
+            for c in arr[:n.value]]
+
+
 def host_cpu():
     """Host CPU model, logical CPUs and the CPUs this process may use."""
     model = "unknown"
@@ -467,10 +482,19 @@ def hbm_iteration(lib, device, steps, warmup, peak):
     j = jpegs[0]
     iters = WORKLOADS["24mp"]["iterations"]
     img = DeviceImage(j)
-    ctx = C.c_void_p()
-    N.check(lib.art_context_create(device, C.byref(ctx)))
+    from artefact_b200.api import Context
+
+    context = Context(device)
+    ctx = context.handle
     stream = torch.cuda.current_stream()
     flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")
+    # Autotune on the image itself (10 iterations per candidate).
+    tr = context.autotune_batch([dict(coefs=j.coefs, weight=WEIGHT, pweight=[PWEIGHT] * 3)], 10)
+    tuned = {"sweep_variant": SWEEP_NAMES[tr["variant"]], "strip_rows": tr["strip_rows"],
+             "projection_warps": tr["proj_warps"], "tuned_ms_per_10_iterations": tr["best_ms"],
+             "heuristic_ms_per_10_iterations": tr["heuristic_ms"],
+             "candidates_ms_per_10_iterations": [
+                 {"sweep": SWEEP_NAMES[k], "rows": r, "projection_warps": p, "ms": m} for k, r, p, m in tr["candidates_ms"]]}
     for _ in range(warmup):
         img.solve(lib, ctx, iters, N.ART_INIT_DECODED, 0, stream)
     torch.cuda.synchronize()
@@ -495,7 +519,7 @@ def hbm_iteration(lib, device, steps, warmup, peak):
         gs.append(gm.value / iters)
         us.append(um.value / iters)
     N.check(lib.art_context_set_timing(ctx, 0))
-    lib.art_context_destroy(ctx)
+    context.close()
     solve_ms = statistics.median(ms)
     it_ms = solve_ms / iters
     ib = iteration_bytes(jpegs)
@@ -506,7 +530,7 @@ def hbm_iteration(lib, device, steps, warmup, peak):
             "iteration_ms": it_ms, "algorithmic_bytes_per_iteration": ib,
             "gbs": ib / (it_ms * 1e-3) / 1e9, "frac_of_hbm": ib / (it_ms * 1e-3) / 1e9 / peak,
             "bytes_moved_per_iteration": moved, "moved_gbs": moved / (it_ms * 1e-3) / 1e9,
-            "gradient_launch_ms": statistics.mean(gs), "projection_launch_ms": statistics.mean(us),
+            "gradient_launch_ms": statistics.mean(gs), "projection_launch_ms": statistics.mean(us), "autotuned": tuned,
             "source": "whole 100-iteration solves, CUDA events, L2 flushed between solves; iteration = solve / 100"}
 
 
@@ -555,9 +579,11 @@ def batch_block(lib, device, steps, warmup, peak):
     flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")
     # Autotune on the batch itself (host coefficients, 5 iterations per candidate).
     tr = context.autotune_batch([dict(coefs=j.coefs, weight=WEIGHT, pweight=[PWEIGHT] * 3) for j in jpegs], 5)
-    tuned = {"sweep_variant": "wide" if tr["variant"] else "narrow", "strip_rows": tr["strip_rows"],
+    tuned = {"sweep_variant": SWEEP_NAMES[tr["variant"]], "strip_rows": tr["strip_rows"],
              "projection_warps": tr["proj_warps"], "candidates": tr["candidates"],
-             "tuned_ms_per_5_iterations": tr["best_ms"], "heuristic_ms_per_5_iterations": tr["heuristic_ms"]}
+             "tuned_ms_per_5_iterations": tr["best_ms"], "heuristic_ms_per_5_iterations": tr["heuristic_ms"],
+             "candidates_ms_per_5_iterations": [
+                 {"sweep": SWEEP_NAMES[k], "rows": r, "projection_warps": p, "ms": m} for k, r, p, m in tr["candidates_ms"]]}
 
     def solve():
         N.check(lib.art_context_compute_batch_device(ctx, len(jpegs), imgs, iters, None, C.c_void_p(stream.cuda_stream)))
@@ -938,11 +964,12 @@ def main():
     if not args.no_tune:
         tr = N.ArtTuneResult()
         N.check(lib.art_context_autotune_batch(ctx, nimg, imgs_host, 10, C.byref(tr)))
-        tuned = {"sweep_variant": "wide" if tr.variant else "narrow", "strip_rows": tr.strip_rows,
+        tuned = {"sweep_variant": SWEEP_NAMES[tr.variant], "strip_rows": tr.strip_rows,
                  "projection_warps": tr.proj_warps, "candidates": tr.candidates,
                  "tuned_ms_per_10_iterations": tr.best_ms, "heuristic_ms_per_10_iterations": tr.heuristic_ms,
-                 "heuristic": {"sweep_variant": "wide" if tr.heuristic_variant else "narrow",
-                               "strip_rows": tr.heuristic_strip_rows, "projection_warps": 4}}
+                 "heuristic": {"sweep_variant": SWEEP_NAMES[tr.heuristic_variant],
+                               "strip_rows": tr.heuristic_strip_rows, "projection_warps": 4},
+                 "candidates_ms_per_10_iterations": tune_candidates(lib, ctx)}
 
     def solve_device():
         if nimg == 1:

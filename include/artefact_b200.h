@@ -209,7 +209,8 @@ int32_t art_context_process_batch(ArtContext *ctx, uint32_t nimages, const ArtPr
  * coefficients, as art_context_compute_batch takes them) and caches the
  * choice for batches of its bucket (image count and total pixels rounded up to
  * powers of two), which takes precedence over the per-image buckets in batched
- * solves. art_context_last_tune returns the last run's choice and timings.
+ * solves. art_context_last_tune returns the last run's choice and timings,
+ * art_context_tune_candidates the timing of every candidate it tried.
  * art_context_tune_cache saves (save != 0) or loads the cache as a text file
  * of "<bucket> <variant> <rows> <projection warps>" lines (three-field lines
  * keep 4 projection warps). Output pointers may be NULL.
@@ -227,6 +228,13 @@ int32_t art_context_autotune(ArtContext *ctx, uint32_t nchannel, const uint32_t 
 int32_t art_context_autotune_batch(ArtContext *ctx, uint32_t nimages, const ArtImage *images, uint32_t iterations,
                                    ArtTuneResult *out);
 int32_t art_context_last_tune(ArtContext *ctx, ArtTuneResult *out);
+/* Every candidate the last autotune run timed, in the order it timed them:
+ * up to `capacity` entries into out; *count receives the number timed. */
+typedef struct ArtTuneCandidate {
+    uint32_t variant, strip_rows, proj_warps;
+    float ms; /* median time for the run's `iterations` steps */
+} ArtTuneCandidate;
+int32_t art_context_tune_candidates(ArtContext *ctx, ArtTuneCandidate *out, uint32_t capacity, uint32_t *count);
 int32_t art_context_tune_cache(ArtContext *ctx, const char *path, int32_t save);
 
 /*

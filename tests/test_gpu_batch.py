@@ -50,6 +50,10 @@ def test_autotune_and_cache_roundtrip(gpu, tmp_path):
         res = ctx.last_tune()
         assert (res["variant"], res["strip_rows"]) == (kind, rows) and res["proj_warps"] in (2, 4, 8)
         assert res["candidates"] >= 3 and res["best_ms"] <= res["heuristic_ms"] * 1.0001
+        cands = res["candidates_ms"]
+        assert len(cands) == res["candidates"] and all(m > 0 for *_, m in cands)
+        assert (cands[0][0], cands[0][1]) == (res["heuristic_variant"], res["heuristic_strip_rows"])
+        assert any(c[:3] == (kind, rows, res["proj_warps"]) for c in cands)
         path = tmp_path / "tune.txt"
         ctx.save_tune_cache(path)
         assert f" {kind} {rows} {res['proj_warps']}\n" in path.read_text()
