@@ -85,11 +85,14 @@ def test_autotune_batch(gpu, tmp_path):
         path = tmp_path / "tune.txt"
         ctx.save_tune_cache(path)
         assert "batch-i8-" in path.read_text()
-        a = ctx.compute_batch(jobs, 12)
-        b = ctx.compute_batch(jobs, 12)
+        # 30 iterations, as the candidate test below: at a dozen, the 130x70 q30
+        # image is so ill-conditioned that the oracle's own fp32 and fp64 runs
+        # differ by more than a level.
+        a = ctx.compute_batch(jobs, 30)
+        b = ctx.compute_batch(jobs, 30)
     assert all(np.array_equal(x, y) for pa, pb in zip(a, b) for x, y in zip(pa, pb))
     for j, got in zip(jpegs, a):
-        check_parity(j, 12, label=f"tuned batch {j.real_px_w}x{j.real_px_h}", gpu=got)
+        check_parity(j, 30, label=f"tuned batch {j.real_px_w}x{j.real_px_h}", gpu=got)
 
 
 @pytest.mark.parametrize("shape", [(72, 40, "4:2:0", False), (200, 136, "4:4:4", False), (128, 96, "4:2:2", False),
