@@ -25,6 +25,7 @@
 #include <mutex>
 #include <sstream>
 #include <string>
+#include <thread>
 #include <vector>
 
 #include "../../include/artefact_b200.h"
@@ -1205,12 +1206,19 @@ int fail(int code, const std::string &msg)
             return fail(ART_ERR_CUDA, std::string(#call) + ": " + cudaGetErrorString(e_));   \
     } while (0)
 
+// A device buffer that only grows. It grows by at least half its size (in
+// 2 MiB steps), so a stream of solves of slowly growing size -- batches of a
+// decode pipeline -- reallocates rarely: cudaFree waits for the whole device,
+// which would serialise contexts working side by side, and a new address
+// forces the iteration graph to be captured again.
 struct DevBuf {
     void *p = nullptr;
     size_t n = 0;
     int ensure(size_t bytes)
     {
         if (bytes <= n) return ART_OK;
+        if (n) bytes = std::max(bytes, n + n / 2);
+        bytes = (bytes + (2u << 20) - 1) / (2u << 20) * (2u << 20);
         if (p) cudaFree(p);
         p = nullptr;
         n = 0;
@@ -1231,6 +1239,70 @@ struct DevBuf {
 };
 
 inline size_t align_up(size_t v, size_t a) { return (v + a - 1) / a * a; }
+
+// Pinned host buffer that only grows, like DevBuf: host-device copies from it
+// run asynchronously at full link speed, where pageable ones are staged by the
+// driver one call at a time.
+struct HostBuf {
+    void *p = nullptr;
+    size_t n = 0;
+    int ensure(size_t bytes)
+    {
+        if (bytes <= n) return ART_OK;
+        if (n) bytes = std::max(bytes, n + n / 2);
+        bytes = (bytes + (2u << 20) - 1) / (2u << 20) * (2u << 20);
+        if (p) cudaFreeHost(p);
+        p = nullptr;
+        n = 0;
+        cudaError_t e = cudaHostAlloc(&p, bytes, cudaHostAllocDefault);
+        if (e != cudaSuccess) {
+            p = nullptr;
+            return fail(ART_ERR_CUDA, std::string("cudaHostAlloc: ") + cudaGetErrorString(e));
+        }
+        n = bytes;
+        return ART_OK;
+    }
+    void release()
+    {
+        if (p) cudaFreeHost(p);
+        p = nullptr;
+        n = 0;
+    }
+};
+
+struct CopyJob {
+    void *dst;
+    const void *src;
+    size_t n;
+};
+
+// Host copies of many buffers, split by bytes over up to 8 threads when they
+// add up to more than a few megabytes (one thread streams ~10 GB/s).
+void parallel_copy(const std::vector<CopyJob> &jobs)
+{
+    size_t total = 0;
+    for (const auto &j : jobs) total += j.n;
+    const unsigned hw = std::max(1u, std::thread::hardware_concurrency());
+    const unsigned nt = total >= (8u << 20) ? std::min(8u, hw) : 1u;
+    auto run = [&](size_t lo, size_t hi) {
+        size_t at = 0;
+        for (const auto &j : jobs) {
+            const size_t a = std::max(lo, at), b = std::min(hi, at + j.n);
+            if (a < b)
+                memcpy(static_cast<char *>(j.dst) + (a - at), static_cast<const char *>(j.src) + (a - at), b - a);
+            at += j.n;
+            if (at >= hi) break;
+        }
+    };
+    if (nt <= 1) {
+        run(0, total);
+        return;
+    }
+    std::vector<std::thread> th;
+    for (unsigned t = 1; t < nt; t++) th.emplace_back(run, total * t / nt, total * (t + 1) / nt);
+    run(0, total / nt);
+    for (auto &t : th) t.join();
+}
 
 // FISTA factors of pipeline_scalar/mod.rs:46-61, in fp32 like the reference:
 // t' = midpoint(1, sqrt(4 t^2 + 1)), f = (t - 1) / t'.
@@ -1291,6 +1363,7 @@ struct ArtContext {
     cudaStream_t side = nullptr;      // second stream: projections of different sampling modes run side by side
     cudaEvent_t fork = nullptr, join = nullptr;
     art::DevBuf xbuf, pbuf, coefimg, stage, misc, desc, work, tasks, compat, sepplanes, rgb, pred;
+    art::HostBuf hstage, hrgb;        // pinned host staging of art_context_process_batch
     ArtNet *net = nullptr;            // warm-start network for ART_INIT_LEARNED (not owned)
     // The learned start's launches (network, upsampling, zero-step projection)
     // as a graph: captured the second time one key is seen, then replayed.
@@ -1507,21 +1580,29 @@ static int samp_mode(int sh, int sv) { return sh == 1 ? (sv == 1 ? 0 : 3) : (sv 
 // projection starts on the rows the gradient sweep touched last (still in L2).
 static void build_tasks(const ImgDev &d, int img, std::vector<int4> per_mode[4])
 {
-    struct Key {
-        int mode, row, c, by, bx0;
-    };
-    std::vector<Key> keys;
+    // Each channel's block rows, walked from the bottom, are already in
+    // descending row order; merging the channels (ties to the lower channel)
+    // gives the order in linear time.
+    int by[3], mode[3];
     for (int c = 0; c < d.nch; c++) {
-        const ChanDev &cd = d.ch[c];
-        const int bw = cd.cw / 8, bh = cd.chh / 8;
-        for (int by = 0; by < bh; by++)
-            for (int bx0 = 0; bx0 < bw; bx0 += 4) keys.push_back({samp_mode(cd.sh, cd.sv), by * 8 * cd.sv, c, by, bx0});
+        by[c] = d.ch[c].chh / 8 - 1;
+        mode[c] = samp_mode(d.ch[c].sh, d.ch[c].sv);
     }
-    std::stable_sort(keys.begin(), keys.end(), [](const Key &a, const Key &b) {
-        if (a.row != b.row) return a.row > b.row;
-        return a.c < b.c;
-    });
-    for (const Key &k : keys) per_mode[k.mode].push_back(make_int4(img, k.c, k.by, k.bx0));
+    for (;;) {
+        int best = -1, row = -1;
+        for (int c = 0; c < d.nch; c++) {
+            if (by[c] < 0) continue;
+            const int r = by[c] * 8 * d.ch[c].sv;
+            if (r > row) {
+                row = r;
+                best = c;
+            }
+        }
+        if (best < 0) break;
+        const int bw = d.ch[best].cw / 8;
+        for (int bx0 = 0; bx0 < bw; bx0 += 4) per_mode[mode[best]].push_back(make_int4(img, best, by[best], bx0));
+        by[best]--;
+    }
 }
 
 // Step + projection of every image, one launch per sampling mode present.
@@ -2055,6 +2136,8 @@ void art_context_destroy(ArtContext *ctx)
     ctx->rgb.release();
     ctx->pred.release();
     ctx->evalbuf.release();
+    ctx->hstage.release();
+    ctx->hrgb.release();
     if (ctx->fork) cudaEventDestroy(ctx->fork);
     if (ctx->join) cudaEventDestroy(ctx->join);
     if (ctx->side) cudaStreamDestroy(ctx->side);
@@ -2513,29 +2596,35 @@ int32_t art_context_process_batch(ArtContext *ctx, uint32_t nimages, const ArtPr
         for (uint32_t c = 0; c < sp.nch; c++)
             total += align_up((size_t)sp.ch[c].block_w * sp.ch[c].block_h * 64 *
                                   (sp.ch[c].coef_type == ART_COEF_I16 ? 2 : 4), 256);
-    if ((rc = ctx->stage.ensure(total))) return rc;
+    if ((rc = ctx->stage.ensure(total)) || (rc = ctx->hstage.ensure(total))) return rc;
+    // Gathered into pinned memory by host threads, then one asynchronous copy.
+    // The previous call on this context returned only after its copies ended,
+    // so the pinned buffer is free.
+    std::vector<CopyJob> up;
     size_t off = 0;
     for (auto &sp : specs)
         for (uint32_t c = 0; c < sp.nch; c++) {
             const size_t n = (size_t)sp.ch[c].block_w * sp.ch[c].block_h * 64 * (sp.ch[c].coef_type == ART_COEF_I16 ? 2 : 4);
-            char *dst = static_cast<char *>(ctx->stage.p) + off;
-            ART_CUDA(cudaMemcpyAsync(dst, sp.ch[c].dct_coefs, n, cudaMemcpyHostToDevice, ctx->stream));
-            sp.src[c] = dst;
+            up.push_back({static_cast<char *>(ctx->hstage.p) + off, sp.ch[c].dct_coefs, n});
+            sp.src[c] = static_cast<char *>(ctx->stage.p) + off;
             off += align_up(n, 256);
         }
+    parallel_copy(up);
+    ART_CUDA(cudaMemcpyAsync(ctx->stage.p, ctx->hstage.p, off, cudaMemcpyHostToDevice, ctx->stream));
     rc = prepare_batch(ctx, specs, iterations, ini.mode, ini.step_iterations);
     if (!rc) rc = run_iterations(ctx, iterations, ini.tail_iterations, ini.tail_stepmul(iterations), ini.step_decay);
     if (rc) {
         cudaStreamSynchronize(ctx->stream);
         return rc;
     }
-    // Output stage per image (lib.rs:159-211) into one device buffer, then
-    // one copy per image to its host buffer.
+    // Output stage per image (lib.rs:159-211) into one device buffer, one
+    // copy of it to pinned memory, then host threads copy each image out.
     size_t rgb_total = 0;
     for (uint32_t i = 0; i < nimages; i++)
         if (images[i].rgb_out) rgb_total += align_up((size_t)images[i].real_w * images[i].real_h * 3, 256);
+    std::vector<CopyJob> down;
     if (rgb_total) {
-        if ((rc = ctx->rgb.ensure(rgb_total))) {
+        if ((rc = ctx->rgb.ensure(rgb_total)) || (rc = ctx->hrgb.ensure(rgb_total))) {
             cudaStreamSynchronize(ctx->stream);
             return rc;
         }
@@ -2558,18 +2647,23 @@ int32_t art_context_process_batch(ArtContext *ctx, uint32_t nimages, const ArtPr
             k_rgb<<<(int)((n + 255) / 256), 256, 0, ctx->stream>>>(pl[0], pl[1], pl[2], pitch, (int)outs[i].nout,
                                                                    (int)im.real_w, (int)im.real_h, dst);
             const cudaError_t e = cudaGetLastError();
-            const cudaError_t e2 = e == cudaSuccess ? cudaMemcpyAsync(im.rgb_out, dst, (size_t)n * 3,
-                                                                      cudaMemcpyDeviceToHost, ctx->stream)
-                                                    : e;
-            if (e2 != cudaSuccess) {
+            if (e != cudaSuccess) {
                 cudaStreamSynchronize(ctx->stream);
-                return fail(ART_ERR_CUDA, std::string("output stage: ") + cudaGetErrorString(e2));
+                return fail(ART_ERR_CUDA, std::string("output stage: ") + cudaGetErrorString(e));
             }
+            down.push_back({im.rgb_out, static_cast<char *>(ctx->hrgb.p) + ro, (size_t)n * 3});
             ro += align_up((size_t)n * 3, 256);
+        }
+        const cudaError_t e = cudaMemcpyAsync(ctx->hrgb.p, ctx->rgb.p, ro, cudaMemcpyDeviceToHost, ctx->stream);
+        if (e != cudaSuccess) {
+            cudaStreamSynchronize(ctx->stream);
+            return fail(ART_ERR_CUDA, std::string("output copy: ") + cudaGetErrorString(e));
         }
     }
     ART_CUDA(cudaStreamSynchronize(ctx->stream));
-    return check_errflag(ctx);
+    if ((rc = check_errflag(ctx))) return rc;
+    parallel_copy(down);
+    return ART_OK;
 }
 
 // -------------------------------------------------------------- autotuner --

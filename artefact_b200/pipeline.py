@@ -11,7 +11,8 @@ Decoded images are grouped, in input order, into batches of at most
 the fused RGB stage) on one of `solvers` contexts, each with its own CUDA
 stream, so one batch's copies overlap another's kernels. Results come back
 in input order, exactly as ``process_jpeg`` returns them for the same
-options; the contexts are closed when the stream ends.
+options. Contexts created here are closed when the stream ends; contexts the
+caller passes in stay open, with their buffers sized and graphs captured.
 """
 from __future__ import annotations
 
@@ -33,22 +34,30 @@ def process_stream(datas: Iterable[bytes], weight: Sequence[float] = (0.3,) * 3,
                    pweight: Sequence[float] = (0.001,) * 3, iterations: Sequence[int] = (50,) * 3,
                    separate: bool = False, *, decoders: int = 4, solvers: int = 2, depth: int = 0,
                    batch_images: int = 32, batch_pixels: int = 32 << 20, device: int = -1,
-                   solve: Optional[Callable[[Jpeg], np.ndarray]] = None) -> Iterator[np.ndarray]:
+                   solve: Optional[Callable[[Jpeg], np.ndarray]] = None,
+                   contexts: Optional[Sequence[Context]] = None) -> Iterator[np.ndarray]:
     """Yields the RGB8 image of each JPEG in `datas`, in order, keeping up to
     `depth` decoded or decoding images ahead of the batches being solved
     (0: twice a batch). `batch_images` = 1 solves image by image
-    (``art_context_process``). `solve` replaces the GPU call per image (tests)."""
+    (``art_context_process``). `contexts` (one per solver; default: created
+    here and closed at the end) lets a long-running caller keep their device
+    buffers and captured graphs from one stream to the next. `solve` replaces
+    the GPU call per image (tests)."""
     if decoders < 1 or solvers < 1 or batch_images < 1 or batch_pixels < 1 or depth < 0:
         raise ValueError("decoders, solvers, batch_images and batch_pixels must be at least 1, depth at least 0")
+    if contexts is not None and len(contexts) != solvers:
+        raise ValueError("give one context per solver")
     depth = depth or 2 * batch_images
-    contexts: list = []
+    owned: list = []
     if solve is not None:
         def solve_batch(group: List[Jpeg]) -> List[np.ndarray]:
             return [solve(j) for j in group]
     else:
         # One explicit context (stream, buffers, graph) per solver slot, lent
-        # to whichever solver thread runs the next batch and closed at the end.
-        contexts = [Context(device) for _ in range(solvers)]
+        # to whichever solver thread runs the next batch.
+        if contexts is None:
+            owned = [Context(device) for _ in range(solvers)]
+            contexts = owned
         free: queue.Queue = queue.Queue()
         for c in contexts:
             free.put(c)
@@ -65,7 +74,7 @@ def process_stream(datas: Iterable[bytes], weight: Sequence[float] = (0.3,) * 3,
     try:
         yield from _run(iter(datas), solve_batch, decoders, solvers, depth, batch_images, batch_pixels)
     finally:
-        for c in contexts:
+        for c in owned:
             c.close()
 
 

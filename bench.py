@@ -729,7 +729,7 @@ def pipeline_e2e(datas, iterations, device):
     """JPEG bytes to RGB8 for every image of the workload through
     Artefact::process semantics, host decode included: one image after the
     other (decode, then process_jpeg), and overlapped (artefact_b200.pipeline:
-    host threads for decoding -- all but two, at most 12 -- and 2 solver
+    host threads for decoding -- all but two, at most 16 -- and 2 solver
     contexts). Wall clock, MPix/s of real area."""
     from artefact_b200 import process_jpeg
     from artefact_b200.api import Context, Jpeg, JpegSource
@@ -748,15 +748,20 @@ def pipeline_e2e(datas, iterations, device):
     serial = time.perf_counter() - t
     ctx.close()
     decoders = max(1, min(16, (os.cpu_count() or 4) - 2))
-    batch_images, batch_pixels = 32, 32 << 20
-    # Warm-up of the batched path, then the timed stream.
-    sum(1 for _ in process_stream(datas[:8], [WEIGHT] * 3, [PWEIGHT] * 3, [iterations] * 3, decoders=decoders,
-                                  solvers=2, batch_images=4, device=device))
+    batch_images, batch_pixels, solvers = 32, 32 << 20, 2
+    # Two solver contexts kept across streams, as a long-running server keeps
+    # them: one untimed pass over the stream sizes their buffers and captures
+    # their graphs, then the timed pass.
+    contexts = [Context(device) for _ in range(solvers)]
+    stream = lambda: process_stream(datas, [WEIGHT] * 3, [PWEIGHT] * 3, [iterations] * 3, decoders=decoders,
+                                    solvers=solvers, batch_images=batch_images, batch_pixels=batch_pixels,
+                                    device=device, contexts=contexts)
+    sum(1 for _ in stream())
     t = time.perf_counter()
-    n = sum(1 for _ in process_stream(datas, [WEIGHT] * 3, [PWEIGHT] * 3, [iterations] * 3, decoders=decoders,
-                                      solvers=2, batch_images=batch_images, batch_pixels=batch_pixels,
-                                      device=device))
+    n = sum(1 for _ in stream())
     piped = time.perf_counter() - t
+    for c in contexts:
+        c.close()
     assert n == len(datas)
     # Host decode alone on the same threads, for the bound it sets.
     from concurrent.futures import ThreadPoolExecutor
@@ -766,10 +771,11 @@ def pipeline_e2e(datas, iterations, device):
         list(ex.map(lambda d: Jpeg.from_source(JpegSource.Buffer(d)), datas))
     decode = time.perf_counter() - t
     return {"serial_mpix_s": mpix / serial, "pipelined_mpix_s": mpix / piped, "images": len(datas),
-            "decode_only_mpix_s": mpix / decode, "decoders": decoders, "solver_contexts": 2,
+            "decode_only_mpix_s": mpix / decode, "decoders": decoders, "solver_contexts": solvers,
             "batch_images": batch_images, "batch_pixels": batch_pixels,
-            "what": "JPEG bytes -> RGB8 (host decode, H2D, batched solve, RGB, D2H), wall clock; serial = one "
-                    "image after the other through process_jpeg"}
+            "what": "JPEG bytes -> RGB8 (host decode, H2D, batched solve, RGB, D2H), wall clock, the second of two "
+                    "passes over the stream on the same two contexts; serial = one image after the other through "
+                    "process_jpeg"}
 
 
 def cpu_sample(kind, jpegs, iterations):

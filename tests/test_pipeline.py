@@ -50,7 +50,8 @@ def test_decode_errors_surface_in_order():
 
 
 def test_rejects_bad_arguments():
-    for kw in (dict(depth=-1), dict(batch_images=0), dict(batch_pixels=0), dict(solvers=0), dict(decoders=0)):
+    for kw in (dict(depth=-1), dict(batch_images=0), dict(batch_pixels=0), dict(solvers=0), dict(decoders=0),
+               dict(solvers=2, contexts=[object()])):
         with pytest.raises(ValueError):
             list(process_stream(_datas(), **kw))
 
@@ -67,4 +68,30 @@ def test_stream_equals_process_jpeg(gpu, batch_images, separate, iterations):
     for d, o in zip(datas, outs):
         j = Jpeg.from_source(JpegSource.Buffer(d))
         ref = process_jpeg(j, list(weight), list(pweight), list(iterations), separate, device=0)
+        np.testing.assert_array_equal(o, ref)
+
+
+@pytest.mark.gpu
+def test_caller_contexts_serve_two_streams(gpu):
+    """Contexts passed in stay open after the stream and give the same images
+    on the next one (buffers and graphs reused, shapes changing between
+    batches)."""
+    from artefact_b200.api import Context
+
+    datas = _datas()
+    weight, pweight, iterations = (0.3, 0.3, 0.3), (0.001, 0.001, 0.001), (16, 16, 16)
+    ctxs = [Context(0), Context(0)]
+    try:
+        first = list(process_stream(datas, weight, pweight, iterations, decoders=2, solvers=2, batch_images=2,
+                                    contexts=ctxs))
+        second = list(process_stream(datas[::-1], weight, pweight, iterations, decoders=2, solvers=2,
+                                     batch_images=3, contexts=ctxs))
+    finally:
+        for c in ctxs:
+            c.close()
+    for a, b in zip(first, second[::-1]):
+        np.testing.assert_array_equal(a, b)
+    for d, o in zip(datas, first):
+        ref = process_jpeg(Jpeg.from_source(JpegSource.Buffer(d)), list(weight), list(pweight), list(iterations),
+                           False, device=0)
         np.testing.assert_array_equal(o, ref)
