@@ -931,6 +931,189 @@ __global__ void k_residual_smooth_grad(const float *__restrict__ pred, const flo
     if (threadIdx.x == 0) loss_partial[blockIdx.x] = s[0];
 }
 
+// ---------------------------------------------------------------------------
+// Objective term of the training loss. The solver judges a start by its
+// objective, not by its distance to a converged image, so training can add
+// lambda E(x) / n to the mean squared error, where x = proj(pred) is the
+// prediction projected onto the quantisation box per 8x8 block (DCT, clamp to
+// [(c - 1/2) q, (c + 1/2) q], IDCT: compute_projection.rs:8-122 on a component
+// at its own resolution) and E is the solver's objective of one channel:
+// a_tv sum |grad x| (compute_step_tv.rs:29-93), a_tgv sum of the second-order
+// norm (compute_step_tv2.rs:32-136) and a_p sum (DCT(x) - c q)^2 / (2 q^2)
+// (compute_step_prob.rs:5-60). Its gradient with respect to pred is
+// J^T grad E(x) with J = IDCT diag(m) DCT, m = 1 on the coefficients the clamp
+// left alone; the transform is orthonormal, so J^T = J. Three kernels:
+// project (per block), terms (per sample), gather + back-projection.
+
+__device__ __forceinline__ void block_reduce_store(float acc, float *out)
+{
+    __shared__ float s[256];
+    s[threadIdx.x] = acc;
+    __syncthreads();
+    for (int k = 128; k > 0; k >>= 1) {
+        if (threadIdx.x < k) s[threadIdx.x] += s[threadIdx.x + k];
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) out[blockIdx.x] = s[0];
+}
+
+// One thread per 8x8 block: x = proj(pred), the DCT-distance gradient plane
+// P = a_p IDCT((cos - c q) / q^2) of the clamped coefficients cos, the mask of
+// unclamped coefficients, and partial sums of the DCT-distance value.
+__global__ void __launch_bounds__(256) k_obj_project(const float *__restrict__ pred, const int16_t *__restrict__ coef,
+                                                     int cpitch, long long img_stride, const float *__restrict__ q,
+                                                     int B, int H, int W, float a_p, float *__restrict__ x,
+                                                     float *__restrict__ P, unsigned long long *__restrict__ mask,
+                                                     float *__restrict__ partial)
+{
+    const int bw = W / 8, bh = H / 8;
+    const long long nblk = (long long)B * bw * bh;
+    float acc = 0.f;
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < nblk; i += (long long)gridDim.x * blockDim.x) {
+        const int bx = (int)(i % bw), by = (int)((i / bw) % bh), b = (int)(i / ((long long)bw * bh));
+        const size_t o = ((size_t)b * H + by * 8) * W + bx * 8;
+        float a[64], d[64];
+#pragma unroll
+        for (int r = 0; r < 8; r++) {
+            const float4 *s = reinterpret_cast<const float4 *>(pred + o + (size_t)r * W);
+            const float4 u = s[0], v = s[1];
+            a[r * 8 + 0] = u.x, a[r * 8 + 1] = u.y, a[r * 8 + 2] = u.z, a[r * 8 + 3] = u.w;
+            a[r * 8 + 4] = v.x, a[r * 8 + 5] = v.y, a[r * 8 + 6] = v.z, a[r * 8 + 7] = v.w;
+        }
+        dct8x8_regs(a);
+        const float *qt = q + (size_t)b * 64;
+        unsigned long long m = 0;
+#pragma unroll
+        for (int r = 0; r < 8; r++) {
+            float c[8];
+            load_coef_row(coef + b * img_stride + (size_t)(by * 8 + r) * cpitch + bx * 8, c);
+#pragma unroll
+            for (int u = 0; u < 8; u++) {
+                const int j = r * 8 + u;
+                const float qj = __ldg(qt + j), cq = c[u] * qj;
+                const float lo = (c[u] - 0.5f) * qj, hi = (c[u] + 0.5f) * qj;
+                const float v = fminf(fmaxf(a[j], lo), hi);
+                if (v == a[j]) m |= 1ull << j;
+                a[j] = v;
+                d[j] = (v - cq) / (qj * qj);
+                acc += 0.5f * a_p * d[j] * (v - cq);
+            }
+        }
+        idct8x8_regs(a);
+        idct8x8_regs(d);
+#pragma unroll
+        for (int r = 0; r < 8; r++) {
+            float4 *xs = reinterpret_cast<float4 *>(x + o + (size_t)r * W);
+            float4 *ps = reinterpret_cast<float4 *>(P + o + (size_t)r * W);
+            xs[0] = make_float4(a[r * 8 + 0], a[r * 8 + 1], a[r * 8 + 2], a[r * 8 + 3]);
+            xs[1] = make_float4(a[r * 8 + 4], a[r * 8 + 5], a[r * 8 + 6], a[r * 8 + 7]);
+            ps[0] = make_float4(a_p * d[r * 8 + 0], a_p * d[r * 8 + 1], a_p * d[r * 8 + 2], a_p * d[r * 8 + 3]);
+            ps[1] = make_float4(a_p * d[r * 8 + 4], a_p * d[r * 8 + 5], a_p * d[r * 8 + 6], a_p * d[r * 8 + 7]);
+        }
+        mask[i] = m;
+    }
+    block_reduce_store(acc, partial);
+}
+
+// One thread per sample of x: the TV and TGV terms centred on it, scaled by
+// their weights and divided by their norms, as five planes
+// T = [a_tv dx/n, a_tv dy/n, a_tgv xx/n2, a_tgv yy/n2, a_tgv s/n2] (zero where a
+// norm is zero), with the edge rules of the reference's scatter: forward
+// differences vanish on the last column / row, backward ones on the first.
+// Partial sums of a_tv n + a_tgv n2.
+__global__ void __launch_bounds__(256) k_obj_terms(const float *__restrict__ x, int B, int H, int W, float a_tv,
+                                                   float a_tgv, float *__restrict__ T, float *__restrict__ partial)
+{
+    const long long n = (long long)B * H * W;
+    float acc = 0.f;
+    for (long long p = blockIdx.x * (long long)blockDim.x + threadIdx.x; p < n; p += (long long)gridDim.x * blockDim.x) {
+        const int X = (int)(p % W), Y = (int)((p / W) % H);
+        const float *im = x + (p - (long long)Y * W - X);
+        auto at = [&](int yy, int xx) { return __ldg(im + (size_t)yy * W + xx); };
+        const float v = at(Y, X);
+        const float dX = X < W - 1 ? at(Y, X + 1) - v : 0.f, dY = Y < H - 1 ? at(Y + 1, X) - v : 0.f;
+        float xx = 0.f, yy = 0.f, gyx = 0.f, gxy = 0.f;
+        if (X > 0) {
+            const float l = at(Y, X - 1);
+            const float dYl = Y < H - 1 ? at(Y + 1, X - 1) - l : 0.f;
+            xx = dX - (v - l);
+            gyx = dY - dYl;
+        }
+        if (Y > 0) {
+            const float u = at(Y - 1, X);
+            const float dXu = X < W - 1 ? at(Y - 1, X + 1) - u : 0.f;
+            yy = dY - (v - u);
+            gxy = dX - dXu;
+        }
+        const float s = 0.5f * (gxy + gyx);
+        const float n1 = sqrtf(dX * dX + dY * dY), n2 = sqrtf(yy * yy + 2.f * s * s + xx * xx);
+        const float i1 = n1 > 0.f ? a_tv / n1 : 0.f, i2 = n2 > 0.f ? a_tgv / n2 : 0.f;
+        T[p] = i1 * dX;
+        T[n + p] = i1 * dY;
+        T[2 * n + p] = i2 * xx;
+        T[3 * n + p] = i2 * yy;
+        T[4 * n + p] = i2 * s;
+        acc += a_tv * n1 + a_tgv * n2;
+    }
+    block_reduce_store(acc, partial);
+}
+
+// One thread per 8x8 block: g = grad E(x) at its 64 samples (the gather of the
+// terms' scatter, plus P), then J g = IDCT(m DCT(g)), and the loss gradient
+// with respect to the residual head's four cell outputs,
+// 2 e / n + lambda 16 (J g) / n with e = (pred - target) / 16, written over
+// channels 0-3 of grad[B][H0][W0][16].
+__global__ void __launch_bounds__(256) k_obj_back(const float *__restrict__ T, const float *__restrict__ P,
+                                                  const unsigned long long *__restrict__ mask,
+                                                  const float *__restrict__ pred, const float *__restrict__ target,
+                                                  int B, int H, int W, float lambda, float inv_count,
+                                                  bf16 *__restrict__ grad)
+{
+    const int bw = W / 8, bh = H / 8;
+    const int W0 = (W + 15) / 16 * 8, H0 = (H + 15) / 16 * 8;
+    const long long nblk = (long long)B * bw * bh, n = (long long)B * H * W;
+    const float *T0 = T, *T1 = T + n, *T2 = T + 2 * n, *T3 = T + 3 * n, *T4 = T + 4 * n;
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < nblk; i += (long long)gridDim.x * blockDim.x) {
+        const int bx = (int)(i % bw), by = (int)((i / bw) % bh), b = (int)(i / ((long long)bw * bh));
+        const size_t base = (size_t)b * H * W;
+        float a[64];
+#pragma unroll
+        for (int r = 0; r < 8; r++) {
+#pragma unroll
+            for (int u = 0; u < 8; u++) {
+                const int Y = by * 8 + r, X = bx * 8 + u;
+                const size_t p = base + (size_t)Y * W + X;
+                float g = -(T0[p] + T1[p]) - 2.f * (T3[p] + T2[p] + T4[p]) + P[p];
+                if (X > 0) g += T0[p - 1] + T4[p - 1] + T2[p - 1];
+                if (Y > 0) g += T1[p - W] + T3[p - W] + T4[p - W];
+                if (X < W - 1) g += T4[p + 1] + T2[p + 1];
+                if (Y < H - 1) g += T3[p + W] + T4[p + W];
+                if (X > 0 && Y < H - 1) g -= T4[p + W - 1];
+                if (X < W - 1 && Y > 0) g -= T4[p - W + 1];
+                a[r * 8 + u] = g;
+            }
+        }
+        dct8x8_regs(a);
+        const unsigned long long m = mask[i];
+#pragma unroll
+        for (int j = 0; j < 64; j++)
+            if (!((m >> j) & 1ull)) a[j] = 0.f;
+        idct8x8_regs(a);
+#pragma unroll
+        for (int r = 0; r < 8; r++) {
+#pragma unroll
+            for (int u = 0; u < 8; u++) {
+                const int Y = by * 8 + r, X = bx * 8 + u;
+                const size_t p = base + (size_t)Y * W + X;
+                const float e = (pred[p] - target[p]) * (1.f / 16.f);
+                const float gr = (2.f * e + lambda * 16.f * a[r * 8 + u]) * inv_count;
+                grad[(((size_t)b * H0 + (Y >> 1)) * W0 + (X >> 1)) * 16 + ((Y & 1) << 1) + (X & 1)] =
+                    __float2bfloat16_rn(gr);
+            }
+        }
+    }
+}
+
 // Adam on flat fp32 parameters (decoupled from the bf16 copies the convs read).
 __global__ void k_adam(float *__restrict__ w, const float *__restrict__ g, float *__restrict__ m, float *__restrict__ v,
                        long long n, float lr, float b1, float b2, float eps, float c1, float c2)
@@ -1402,6 +1585,11 @@ struct ArtNet {
     // gradients (training, with activation set 0)
     art::cnn::Buf dr, gd1, ge1, gup1, gd2, ge2, gup2, gd3, ge3, gup3, ge4, gp3, gp2, gp1;
     float smooth_weight = 0.f;  // lambda of the training loss's smoothness term (art_net_set_loss)
+    // Objective term of the training loss (art_net_set_objective): its weight
+    // and the objective's term weights; obj holds x, P, the five term planes
+    // and the clamp masks.
+    float obj_lambda = 0.f, obj_tv = 0.f, obj_tgv = 0.f, obj_p = 0.f;
+    art::cnn::Buf obj;
     bool cap_train = false;     // the gradient buffers match act[0]
 };
 
@@ -1724,7 +1912,7 @@ int32_t art_net_create(int32_t device, const float *params, int64_t nparams, Art
     }
     const size_t pb = (size_t)nparams * 4;
     if (!net->params.ensure(pb) || !net->errflag.ensure(64) || !net->workspace.ensure(WORKSPACE_BYTES) ||
-        !net->loss_partial.ensure(2 * LOSS_BLOCKS * 4) ||
+        !net->loss_partial.ensure(3 * LOSS_BLOCKS * 4) ||
         cudaMemcpy(net->params.p, params, pb, cudaMemcpyHostToDevice) != cudaSuccess ||
         cudaMemset(net->errflag.p, 0, 64) != cudaSuccess) {
         art_net_destroy(net);
@@ -1740,7 +1928,8 @@ void art_net_destroy(ArtNet *net)
     cudaSetDevice(net->device);
     art::cnn::Buf *all[] = {&net->params, &net->grads, &net->adam_m, &net->adam_v, &net->errflag, &net->workspace,
                             &net->loss_partial, &net->dr, &net->gd1, &net->ge1, &net->gup1, &net->gd2, &net->ge2,
-                            &net->gup2, &net->gd3, &net->ge3, &net->gup3, &net->ge4, &net->gp3, &net->gp2, &net->gp1};
+                            &net->gup2, &net->gd3, &net->ge3, &net->gup3, &net->ge4, &net->gp3, &net->gp2, &net->gp1,
+                            &net->obj};
     for (auto *b : all) b->release();
     for (auto &A : net->act) {
         art::cnn::Buf *acts[] = {&A.feat, &A.dec, &A.cat1, &A.cat2, &A.cat3, &A.p1, &A.p2,
@@ -1793,6 +1982,20 @@ int32_t art_net_set_loss(ArtNet *net, float smooth_weight)
     return ART_OK;
 }
 
+int32_t art_net_set_objective(ArtNet *net, float lambda, float weight, float pweight, int32_t nch)
+{
+    if (!net || !(lambda >= 0.f) || !std::isfinite(lambda) || !(weight >= 0.f) || !std::isfinite(weight) ||
+        !(pweight >= 0.f) || !std::isfinite(pweight) || nch < 1 || nch > 3)
+        return fail(ART_ERR_INVALID_ARGUMENT, "net_set_objective: weights must be finite and >= 0, nch 1..3");
+    // The solver's term weights for an nch-channel image (compute_step.rs:8-72).
+    const double r = 1.0 / std::sqrt((double)nch);
+    net->obj_lambda = lambda;
+    net->obj_tv = (float)r;
+    net->obj_tgv = (float)(weight * r);
+    net->obj_p = (float)(pweight * 2.0 * 255.0 * std::sqrt(2.0));
+    return ART_OK;
+}
+
 int32_t art_net_train_step(ArtNet *net, const int16_t *coef, int32_t cpitch, int64_t img_stride, const float *q,
                            const float *target, int32_t B, int32_t H, int32_t W, float lr, float *loss, void *stream)
 {
@@ -1816,7 +2019,22 @@ int32_t art_net_train_step(ArtNet *net, const int16_t *coef, int32_t cpitch, int
     const long long npix = (long long)B * H * W;
     NET_TRY(art_cnn_residual(A.r.as<float>(), RSTRIDE, A.dec.as<float>(), target, B, H, W, A.pred.as<float>(),
                              net->dr.p, net->loss_partial.as<float>(), LOSS_BLOCKS, s));
-    if (net->smooth_weight > 0.f) {
+    const bool objective = net->obj_lambda > 0.f;
+    if (objective) {
+        const size_t n = (size_t)npix, nblk = n / 64;
+        if (!net->obj.ensure(n * 7 * 4 + nblk * 8)) return fail(ART_ERR_CUDA, "net_train_step: allocation failed");
+        float *x = net->obj.as<float>(), *P = x + n, *T = P + n;
+        auto *mask = reinterpret_cast<unsigned long long *>(T + 5 * n);
+        float *lp = net->loss_partial.as<float>();
+        k_obj_project<<<LOSS_BLOCKS, 256, 0, s>>>(A.pred.as<float>(), coef, cpitch, img_stride, q, B, H, W,
+                                                  net->obj_p, x, P, mask, lp + LOSS_BLOCKS);
+        NET_TRY(check_launch("k_obj_project"));
+        k_obj_terms<<<LOSS_BLOCKS, 256, 0, s>>>(x, B, H, W, net->obj_tv, net->obj_tgv, T, lp + 2 * LOSS_BLOCKS);
+        NET_TRY(check_launch("k_obj_terms"));
+        k_obj_back<<<LOSS_BLOCKS, 256, 0, s>>>(T, P, mask, A.pred.as<float>(), target, B, H, W, net->obj_lambda,
+                                               1.f / (float)npix, static_cast<bf16 *>(net->dr.p));
+        NET_TRY(check_launch("k_obj_back"));
+    } else if (net->smooth_weight > 0.f) {
         k_residual_smooth_grad<<<LOSS_BLOCKS, 256, 0, s>>>(A.pred.as<float>(), target, B, H, W, net->smooth_weight,
                                                            1.f / (float)npix, static_cast<bf16 *>(net->dr.p),
                                                            net->loss_partial.as<float>() + LOSS_BLOCKS);
@@ -1830,13 +2048,13 @@ int32_t art_net_train_step(ArtNet *net, const int16_t *coef, int32_t cpitch, int
         net->packed = false;
     }
     if (loss) {
-        float h[2 * LOSS_BLOCKS];
-        const int nparts = net->smooth_weight > 0.f ? 2 * LOSS_BLOCKS : LOSS_BLOCKS;
+        float h[3 * LOSS_BLOCKS];
+        const int nparts = objective ? 3 * LOSS_BLOCKS : net->smooth_weight > 0.f ? 2 * LOSS_BLOCKS : LOSS_BLOCKS;
         if (cudaMemcpyAsync(h, net->loss_partial.p, nparts * sizeof(float), cudaMemcpyDeviceToHost, s) != cudaSuccess)
             return fail(ART_ERR_CUDA, "net_train_step: loss copy failed");
         NET_TRY(read_err(net, s));
         double t = 0;
-        for (int i = 0; i < nparts; i++) t += h[i];
+        for (int i = 0; i < nparts; i++) t += (objective && i >= LOSS_BLOCKS ? (double)net->obj_lambda : 1.0) * h[i];
         *loss = (float)(t / (double)npix);
         return ART_OK;
     }

@@ -9,8 +9,9 @@ component's own resolution (cell means of the full-resolution result for a
 subsampled component), which is where the network predicts.
 
 Training: Adam on the mean squared error of ``art_net_train_step`` (the
-library's own BF16 tensor-core forward and backward kernels), batches of one
-shape at a time, cosine learning-rate decay.
+library's own BF16 tensor-core forward and backward kernels), optionally plus
+the solver's objective of the projected prediction (``--objective``), batches
+of one shape at a time, cosine learning-rate decay.
 
 Usage::
 
@@ -205,6 +206,9 @@ def main(argv=None):
     ap.add_argument("--smooth", type=float, default=0.0,
                     help="weight of the loss's smoothness term (squared differences of the error between adjacent "
                          "samples); 0 = plain MSE")
+    ap.add_argument("--objective", type=float, default=0.0,
+                    help="weight of the loss's objective term (the solver's objective of the projected "
+                         "prediction, per sample); 0 = off")
     args = ap.parse_args(argv)
 
     def log(*a):
@@ -216,6 +220,7 @@ def main(argv=None):
     ctx = Context(0)
     net = WS.WarmStartNet(WS.load_params(args.init) if args.init else WS.init_params(args.seed))
     net.set_loss(args.smooth)
+    net.set_objective(args.objective, WEIGHT, PWEIGHT)
     t0 = time.time()
     data = build_pools(args.crops, SEED0, ctx, log=log)
     val = build_pools(args.val, SEED0 + 10_000_000, ctx, log=log)

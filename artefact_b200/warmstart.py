@@ -151,6 +151,11 @@ class WarmStartNet:
         error between adjacent samples (art_net_set_loss; 0 = plain MSE)."""
         N.check(N.lib().art_net_set_loss(self._h, float(smooth_weight)))
 
+    def set_objective(self, lam: float, weight: float = 0.3, pweight: float = 0.001, nch: int = 3) -> None:
+        """Training loss += lam / n * the solver's objective of the projected
+        prediction (art_net_set_objective; 0 = off)."""
+        N.check(N.lib().art_net_set_objective(self._h, float(lam), float(weight), float(pweight), int(nch)))
+
     def train_step(self, coef, q, target, lr: float, stream=None) -> float:
         """One step on a batch: coef int16 [B][H][W], q float32 [B][64] and
         target float32 [B][H][W] CUDA tensors. Returns the mean loss."""

@@ -454,6 +454,16 @@ int32_t art_net_predict(ArtNet *net, const int16_t *coef, int32_t cpitch, int64_
  * is plain MSE). The smoothness term penalises prediction errors that vary
  * from sample to sample, which the TV/TGV objective penalises most. */
 int32_t art_net_set_loss(ArtNet *net, float smooth_weight);
+/* Objective term of the training loss: adds lambda / (B H W) times the
+ * solver's objective of each sample's prediction after projection onto its
+ * quantisation box (per 8x8 block: DCT, clamp to [(c - 1/2) q, (c + 1/2) q],
+ * IDCT), with the term weights the solver uses for an nch-channel image with
+ * these weight and pweight options: TV 1/sqrt(nch), second-order TGV
+ * weight/sqrt(nch), DCT distance pweight * 2 * 255 * sqrt(2)
+ * (pipeline_scalar/compute_step.rs:8-72). The gradient is the objective's,
+ * taken through the projection. lambda = 0 (the default) turns it off; while
+ * it is on, the smoothness term is not used. */
+int32_t art_net_set_objective(ArtNet *net, float lambda, float weight, float pweight, int32_t nch);
 /* One training step on the mean squared error against target[B][H][W]
  * (in units of 16 levels): forward, backward, then Adam with learning rate
  * lr (lr <= 0: gradients only). *loss (may be NULL) receives the mean loss. */

@@ -18,6 +18,7 @@ each level-0 pixel carries a 2x2 cell of the component (space to depth).
   r  = depth_to_space(conv(d1, 32 -> 16)[..., 0:4]) cropped to H x W
   prediction = decoded + 16 r, e = r - (target - decoded) / 16,
   loss = (sum e^2 + smooth * sum over adjacent sample pairs (e_p - e_q)^2) / n
+         [+ lam * E(proj(prediction)) / n, the objective term, see objective_value]
 
 conv = 3x3, stride 1, zero padding 1, weights W[cout][tap = 3 (dy+1) + (dx+1)][cin];
 pool = 2x2 mean; up = nearest 2x. F = (space_to_depth(decoded) / 128,
@@ -153,6 +154,88 @@ def features(coef_img, q):
     return dec, F
 
 
+def project(pred, coef_img, q):
+    """Per 8x8 block of pred [B][H][W]: orthonormal DCT, clamp to
+    [(c - 1/2) q, (c + 1/2) q], inverse DCT (pipeline_scalar/compute_projection.rs:8-122
+    on one component at its own resolution). Returns x, the clamped
+    coefficients minus c q over q^2 (block layout [B][by][bx][v][u]) and the
+    mask of unclamped coefficients."""
+    m = _dct_matrix()
+    B, H, W = pred.shape
+    blk = pred.reshape(B, H // 8, 8, W // 8, 8).transpose(0, 1, 3, 2, 4)
+    C = np.einsum("vy,bijyx,ux->bijvu", m, blk, m)
+    c = coef_img.reshape(B, H // 8, 8, W // 8, 8).transpose(0, 1, 3, 2, 4).astype(np.float64)
+    qq = q.reshape(B, 1, 1, 8, 8).astype(np.float64)
+    Cc = np.clip(C, (c - 0.5) * qq, (c + 0.5) * qq)
+    inv = lambda a: np.einsum("vy,bijvu,ux->bijyx", m, a, m).transpose(0, 1, 3, 2, 4).reshape(B, H, W)
+    return inv(Cc), (Cc - c * qq) / (qq * qq), Cc == C, inv
+
+
+def objective_value(x, d, qq_d_cq, a_tv, a_tgv, a_p):
+    """The solver's objective of one channel at x: a_tv sum |grad x|
+    (compute_step_tv.rs:29-93) + a_tgv sum of the second-order norm
+    (compute_step_tv2.rs:32-136) + a_p sum (DCT(x) - c q)^2 / (2 q^2)
+    (compute_step_prob.rs:5-60), with the reference's edge rules: forward
+    differences vanish on the last column / row, backward ones on the first.
+    d = (cos - c q) / q^2 and qq_d_cq = cos - c q per coefficient.
+    Returns the value and the terms the gradient needs."""
+    dX = np.zeros_like(x)
+    dX[:, :, :-1] = x[:, :, 1:] - x[:, :, :-1]
+    dY = np.zeros_like(x)
+    dY[:, :-1, :] = x[:, 1:, :] - x[:, :-1, :]
+    xx = np.zeros_like(x)
+    xx[:, :, 1:] = dX[:, :, 1:] - dX[:, :, :-1]
+    gyx = np.zeros_like(x)
+    gyx[:, :, 1:] = dY[:, :, 1:] - dY[:, :, :-1]
+    yy = np.zeros_like(x)
+    yy[:, 1:, :] = dY[:, 1:, :] - dY[:, :-1, :]
+    gxy = np.zeros_like(x)
+    gxy[:, 1:, :] = dX[:, 1:, :] - dX[:, :-1, :]
+    s = 0.5 * (gxy + gyx)
+    n1 = np.sqrt(dX * dX + dY * dY)
+    n2 = np.sqrt(yy * yy + 2 * s * s + xx * xx)
+    value = float(a_tv * n1.sum() + a_tgv * n2.sum() + 0.5 * a_p * np.sum(d * qq_d_cq))
+    with np.errstate(divide="ignore", invalid="ignore"):
+        i1 = np.where(n1 > 0, a_tv / n1, 0.0)
+        i2 = np.where(n2 > 0, a_tgv / n2, 0.0)
+    return value, (i1 * dX, i1 * dY, i2 * xx, i2 * yy, i2 * s)
+
+
+def objective_gradient(T):
+    """d E / d x from the terms: the reference's scatter of each term centred
+    on a sample to its neighbours (compute_step_tv.rs:64-88,
+    compute_step_tv2.rs:106-134), without the DCT-distance part."""
+    T0, T1, T2, T3, T4 = T
+    g = -(T0 + T1) - 2 * (T3 + T2 + T4)
+    g[:, :, 1:] += T0[:, :, :-1] + T4[:, :, :-1] + T2[:, :, :-1]
+    g[:, 1:, :] += T1[:, :-1, :] + T3[:, :-1, :] + T4[:, :-1, :]
+    g[:, :, :-1] += T4[:, :, 1:] + T2[:, :, 1:]
+    g[:, :-1, :] += T3[:, 1:, :] + T4[:, 1:, :]
+    g[:, :-1, 1:] -= T4[:, 1:, :-1]
+    g[:, 1:, :-1] -= T4[:, :-1, 1:]
+    return g
+
+
+def objective_and_back(pred, coef_img, q, a_tv, a_tgv, a_p):
+    """E(proj(pred)) and its gradient with respect to pred through the
+    projection: J^T grad E with J = IDCT diag(mask) DCT (= J^T)."""
+    m = _dct_matrix()
+    B, H, W = pred.shape
+    x, d, mask, inv = project(pred, coef_img, q)
+    qq = q.reshape(B, 1, 1, 8, 8).astype(np.float64)
+    value, T = objective_value(x, d, d * qq * qq, a_tv, a_tgv, a_p)
+    g = objective_gradient(T) + a_p * inv(d)
+    gb = g.reshape(B, H // 8, 8, W // 8, 8).transpose(0, 1, 3, 2, 4)
+    G = np.einsum("vy,bijyx,ux->bijvu", m, gb, m) * mask
+    return value, inv(G)
+
+
+def solver_weights(weight=0.3, pweight=0.001, nch=3):
+    """(a_tv, a_tgv, a_p) of the solver for an nch-channel image (compute_step.rs:8-72)."""
+    r = 1.0 / np.sqrt(nch)
+    return r, weight * r, pweight * 2.0 * 255.0 * np.sqrt(2.0)
+
+
 def _pair_sum(e):
     """Sum over horizontally and vertically adjacent samples of (e_p - e_q)^2."""
     return float(np.sum((e[:, :, 1:] - e[:, :, :-1]) ** 2) + np.sum((e[:, 1:, :] - e[:, :-1, :]) ** 2))
@@ -170,8 +253,10 @@ def _pair_grad(e):
     return g
 
 
-def forward(params, F, dec, target=None, bf=True, smooth=0.0):
-    """Activations (dict), prediction and, with a target, the loss."""
+def forward(params, F, dec, target=None, bf=True, smooth=0.0, objective=None):
+    """Activations (dict), prediction and, with a target, the loss.
+    objective = (lam, coef_img, q, a_tv, a_tgv, a_p) adds the objective term
+    (and replaces the smoothness term, as the GPU does)."""
     rnd = bf16 if bf else (lambda a: np.asarray(a, np.float64))
     P = unpack(params)
     Wq = {k: (rnd(w), b) for k, (w, b) in P.items()}
@@ -200,19 +285,28 @@ def forward(params, F, dec, target=None, bf=True, smooth=0.0):
     loss = None
     if target is not None:
         e = rf - (target - dec) / 16.0
-        loss = float(np.mean(e * e)) + smooth * _pair_sum(e) / e.size
         a["e"] = e
+        if objective is not None:
+            lam, coef_img, q, a_tv, a_tgv, a_p = objective
+            val, dpred = objective_and_back(pred, coef_img, q, a_tv, a_tgv, a_p)
+            loss = float(np.mean(e * e)) + lam * val / e.size
+            a["obj_grad"] = lam * 16.0 * dpred
+        else:
+            loss = float(np.mean(e * e)) + smooth * _pair_sum(e) / e.size
     return a, pred, loss, Wq
 
 
-def gradients(params, F, dec, target, bf=True, smooth=0.0):
+def gradients(params, F, dec, target, bf=True, smooth=0.0, objective=None):
     """Loss and d loss / d params (flat, same layout as params)."""
     rnd = bf16 if bf else (lambda v: np.asarray(v, np.float64))
-    a, _, loss, Wq = forward(params, F, dec, target, bf, smooth)
+    a, _, loss, Wq = forward(params, F, dec, target, bf, smooth, objective)
     npix = dec.size
     mask = lambda g, act: g * (act > 0)
     dr = np.zeros(a["r"].shape)
-    dlde = (2.0 * a["e"] + smooth * _pair_grad(a["e"])) / npix
+    if objective is not None:
+        dlde = (2.0 * a["e"] + a["obj_grad"]) / npix
+    else:
+        dlde = (2.0 * a["e"] + smooth * _pair_grad(a["e"])) / npix
     dr[..., 0:4] = space_to_depth(dlde, *a["r"].shape[1:3])
     if bf:
         dr[..., 0:4] = bf16(dr[..., 0:4].astype(np.float32))

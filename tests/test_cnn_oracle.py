@@ -97,3 +97,78 @@ def test_smooth_loss_gradient_matches_finite_differences():
         lm = O.forward(params - eps * v, F, dec, target, bf=False, smooth=2.0)[2]
         fd = (lp - lm) / (2 * eps)
         assert abs(fd - g @ v) <= 1e-5 * max(1.0, abs(fd)), (fd, g @ v)
+
+
+def _interior(shape, ring, rng):
+    d = np.zeros(shape)
+    d[:, ring:-ring, ring:-ring] = rng.standard_normal((shape[0], shape[1] - 2 * ring, shape[2] - 2 * ring))
+    return d
+
+
+def test_objective_gradient_matches_finite_differences():
+    """The training loss's objective term: the gradient the reference's scatter
+    gives (TV, TGV) against central differences of the objective, for
+    perturbations off the first and last rows and columns (where the
+    reference's second-order edge rule is not the derivative of its value)."""
+    rng = np.random.default_rng(11)
+    B, H, W = 2, 24, 32
+    x = rng.standard_normal((B, H, W)) * 10
+    a_tv, a_tgv, _ = O.solver_weights()
+    zero = np.zeros((B, H // 8, W // 8, 8, 8))
+    val, T = O.objective_value(x, zero, zero, a_tv, a_tgv, 0.0)
+    g = O.objective_gradient(T)
+    for _ in range(3):
+        d = _interior(x.shape, 1, rng)
+        eps = 1e-6
+        fp = O.objective_value(x + eps * d, zero, zero, a_tv, a_tgv, 0.0)[0]
+        fm = O.objective_value(x - eps * d, zero, zero, a_tv, a_tgv, 0.0)[0]
+        fd = (fp - fm) / (2 * eps)
+        assert abs(fd - float(np.sum(g * d))) <= 1e-6 * max(1.0, abs(fd)), (fd, float(np.sum(g * d)))
+
+
+def test_objective_through_projection_matches_finite_differences():
+    """E(proj(pred)) and its gradient through the projection (J = IDCT diag(m)
+    DCT, symmetric), DCT-distance term included, with some coefficients
+    clamped: perturbations confined to blocks off the image border."""
+    rng = np.random.default_rng(12)
+    B, H, W = 1, 32, 32
+    coef = rng.integers(-6, 6, size=(B, H, W)).astype(np.int16)
+    q = rng.integers(4, 30, size=(B, 64)).astype(np.float64)
+    dec, _ = O.features(coef, q)
+    pred = dec + rng.standard_normal(dec.shape) * 6
+    a_tv, a_tgv, a_p = O.solver_weights()
+    _, _, mask, _ = O.project(pred, coef, q)
+    assert 0.05 < mask.mean() < 0.95  # some coefficients clamped, some free
+    val, grad = O.objective_and_back(pred, coef, q, a_tv, a_tgv, a_p)
+    assert val > 0
+    for _ in range(3):
+        d = np.zeros_like(pred)
+        d[:, 8:24, 8:24] = rng.standard_normal((B, 16, 16))
+        eps = 1e-6
+        fp = O.objective_and_back(pred + eps * d, coef, q, a_tv, a_tgv, a_p)[0]
+        fm = O.objective_and_back(pred - eps * d, coef, q, a_tv, a_tgv, a_p)[0]
+        fd = (fp - fm) / (2 * eps)
+        assert abs(fd - float(np.sum(grad * d))) <= 1e-5 * max(1.0, abs(fd)), (fd, float(np.sum(grad * d)))
+
+
+def test_objective_loss_gradient_matches_finite_differences():
+    """The objective term of the training loss on the whole network. The
+    perturbed parameters move every sample, edges included, where the
+    reference's second-order edge rule differs from the derivative of the
+    value (a few 1e-4 here), so the bar is 2e-3; a wrong scale of the term
+    would miss it by orders of magnitude."""
+    params, F, dec, target = _case(6, H=16, W=24)
+    rng = np.random.default_rng(9)
+    coef = rng.integers(-20, 20, size=(1, 16, 24)).astype(np.int16)
+    q = rng.integers(2, 40, size=(1, 64)).astype(np.float64)
+    dec, F = O.features(coef, q)
+    obj = (0.05, coef, q) + O.solver_weights()
+    loss, g = O.gradients(params, F, dec, target, bf=False, objective=obj)
+    assert loss > O.forward(params, F, dec, target, bf=False)[2]
+    for _ in range(3):
+        v = rng.standard_normal(params.size)
+        eps = 1e-8
+        lp = O.forward(params + eps * v, F, dec, target, bf=False, objective=obj)[2]
+        lm = O.forward(params - eps * v, F, dec, target, bf=False, objective=obj)[2]
+        fd = (lp - lm) / (2 * eps)
+        assert abs(fd - g @ v) <= 2e-3 * max(1.0, abs(fd)), (fd, g @ v)

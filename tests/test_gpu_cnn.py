@@ -337,6 +337,43 @@ def test_network_gradients_match_oracle(gpu, smooth):
             assert cos >= 0.999 and rel <= 3e-2, (name, cos, rel)
 
 
+@pytest.mark.parametrize("lam", [0.02, 0.2])
+def test_objective_loss_gradients_match_oracle(gpu, lam):
+    """The loss's objective term (art_net_set_objective: the solver's objective
+    of the projected prediction) through the whole backward pass, against the
+    oracle's FP64 gradient of the same loss: loss within 1e-3, per layer cosine
+    >= 0.999 and relative error <= 3e-2."""
+    torch = _torch()
+    coef, q, target = _batch(5)
+    params = WS.init_params(5)
+    rng = np.random.default_rng(5)
+    offs, _ = O.offsets()
+    wo, bo = offs["head"]
+    params[wo:bo] = (rng.standard_normal(bo - wo) * 0.05).astype(np.float32)
+    params[wo + 4 * 32 * 9:bo] = 0.0
+    net = WS.WarmStartNet(params)
+    net.set_objective(lam, 0.3, 0.001, 3)
+    loss = net.train_step(torch.from_numpy(coef).cuda(), _f32(q), _f32(target), lr=0.0)
+    g = net.gradients().astype(np.float64)
+    dec, F = O.features(coef, q)
+    obj = (lam, coef, q.astype(np.float64)) + O.solver_weights(0.3, 0.001, 3)
+    ref_loss, ref = O.gradients(params.astype(np.float64), F, dec, target.astype(np.float64), objective=obj)
+    assert abs(loss - ref_loss) <= 1e-3 * ref_loss, (loss, ref_loss)
+    for name, cin, cout, _, _ in O.LAYERS:
+        for lo, hi in ((offs[name][0], offs[name][1]), (offs[name][1], offs[name][1] + cout)):
+            a, b = g[lo:hi], ref[lo:hi]
+            nb = float(np.linalg.norm(b))
+            if nb == 0:
+                assert float(np.abs(a).max()) == 0
+                continue
+            cos = float(a @ b) / (float(np.linalg.norm(a)) * nb)
+            rel = float(np.linalg.norm(a - b)) / nb
+            assert cos >= 0.999 and rel <= 3e-2, (name, cos, rel)
+    net.set_objective(0.0)
+    plain = net.train_step(torch.from_numpy(coef).cuda(), _f32(q), _f32(target), lr=0.0)
+    assert plain < loss
+
+
 def test_training_reduces_loss(gpu):
     """A residual the network can represent -- the decoded image smoothed by a
     3x3 box filter, minus itself -- is learned: the loss falls well below its
