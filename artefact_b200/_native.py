@@ -158,6 +158,7 @@ EXPORTS = {
     "art_context_tune_cache": (C.c_int32, [C.c_void_p, C.c_char_p, C.c_int32]),
     "art_context_synchronize": (C.c_int32, [C.c_void_p]),
     "art_context_set_warm_start": (C.c_int32, [C.c_void_p, C.c_void_p]),
+    "art_context_set_joint_warm_start": (C.c_int32, [C.c_void_p, C.c_void_p]),
     "art_context_evaluate": (C.c_int32, [C.c_void_p, C.c_uint32, C.POINTER(C.c_double)]),
     "art_context_set_timing": (C.c_int32, [C.c_void_p, C.c_int32]),
     "art_context_last_timing": (C.c_int32, [C.c_void_p, C.POINTER(C.c_float), C.POINTER(C.c_float),
@@ -174,6 +175,12 @@ EXPORTS = {
     "art_net_gradients": (C.c_int32, [C.c_void_p, C.c_void_p, C.c_int64]),
     "art_net_predict": (C.c_int32, [C.c_void_p, C.c_void_p, C.c_int32, C.c_int64, C.c_void_p, C.c_int32, C.c_int32,
                                     C.c_int32, C.c_void_p, C.c_void_p]),
+    "art_net_predict_joint": (C.c_int32, [C.c_void_p, C.c_void_p, C.c_int32, C.c_int64, C.c_void_p, C.c_int32,
+                                          C.c_int64, C.c_void_p, C.c_void_p, C.c_int32, C.c_int32, C.c_int32,
+                                          C.c_void_p, C.c_void_p]),
+    "art_net_train_step_joint": (C.c_int32, [C.c_void_p, C.c_void_p, C.c_int32, C.c_int64, C.c_void_p, C.c_int32,
+                                             C.c_int64, C.c_void_p, C.c_void_p, C.c_void_p, C.c_int32, C.c_int32,
+                                             C.c_int32, C.c_float, C.POINTER(C.c_float), C.c_void_p]),
     "art_net_set_loss": (C.c_int32, [C.c_void_p, C.c_float]),
     "art_net_set_objective": (C.c_int32, [C.c_void_p, C.c_float, C.c_float, C.c_float, C.c_int32]),
     "art_net_train_step": (C.c_int32, [C.c_void_p, C.c_void_p, C.c_int32, C.c_int64, C.c_void_p, C.c_void_p,

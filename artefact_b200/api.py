@@ -402,6 +402,13 @@ class Context:
         self._net = net
         N.check(N.lib().art_context_set_warm_start(self._h, net.handle if net is not None else None))
 
+    def set_joint_warm_start(self, net) -> None:
+        """Attach a joint 4:2:0 network (or None): learned solves of 4:2:0
+        images predict all three components with it in one pass
+        (``art_context_set_joint_warm_start``)."""
+        self._net_joint = net
+        N.check(N.lib().art_context_set_joint_warm_start(self._h, net.handle if net is not None else None))
+
     def evaluate(self, image: int = 0) -> dict:
         """Objective and feasibility of the last solve's result for `image`
         (``art_context_evaluate``, fp64 on the GPU): keys E, tv, tgv, prob, infeasibility."""

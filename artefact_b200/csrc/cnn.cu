@@ -28,6 +28,7 @@
 
 #include <cmath>
 #include <cstdint>
+#include <cstring>
 #include <atomic>
 #include <mutex>
 #include <string>
@@ -54,6 +55,7 @@ constexpr int EPI_THREADS = CONV_THREADS - 64;
 constexpr uint32_t SMEM_BUDGET = 220 * 1024;  // pipeline stages; 1 KB more is requested for alignment
 constexpr int MAX_STAGES = 4;
 constexpr int RSTRIDE = 4;                  // channels per pixel of the head's fp32 residual output
+constexpr int JOINT_RSTRIDE = 12;           // the same for the joint 4:2:0 network (three components' 2x2 cells)
 
 struct ConvArgs {
     int B, H, W;
@@ -783,7 +785,7 @@ __global__ void __launch_bounds__(128) k_features(const int16_t *__restrict__ co
     float o8[8];
 #pragma unroll
     for (int u = 0; u < 8; u++) o8[u] = __shfl_xor_sync(0xffffffffu, a[u], 1);
-    if (bx >= pbw) return;
+    if (bx >= pbw || !feat) return;
     const int yy = r >> 1, h = r & 1;
 #pragma unroll
     for (int k2 = 0; k2 < 2; k2++) {
@@ -929,6 +931,99 @@ __global__ void k_residual_smooth_grad(const float *__restrict__ pred, const flo
         __syncthreads();
     }
     if (threadIdx.x == 0) loss_partial[blockIdx.x] = s[0];
+}
+
+// ---------------------------------------------------------------------------
+// Joint 4:2:0 network input and output. The luma's level-0 grid (a 2x2 luma
+// cell per pixel) is the chroma components' sample grid, so one pass over it
+// sees all three components: each level-0 pixel also carries one sample of
+// Cb and of Cr, and the head's outputs 4-7 / 8-11 are the 2x2 full-resolution
+// chroma cells, which the chroma's own resolution cannot express.
+
+// Smooth 2x upsampling weights of the solver's learned start: 3/4 of the own
+// cell, 1/4 of the neighbour on the sample's side, each product and sum
+// rounded on its own.
+__device__ __forceinline__ float tri_mix(float a, float b) { return __fadd_rn(__fmul_rn(0.75f, a), __fmul_rn(0.25f, b)); }
+
+// One thread per level-0 pixel (y, x) of image b: channels 8-11 of feat
+// [B][H0][W0][16] = decoded Cb sample / 128, its quantisation step / 64 (the
+// step of its frequency position in its block), the same for Cr; and the
+// chroma bases, the decoded chroma upsampled smoothly to full resolution,
+// into planes 1 and 2 of dec[3][B][H][W]. decC[B][2][H/2][W/2] holds the
+// decoded chroma, qc[B][2][64] their tables. H, W multiples of 16.
+__global__ void k_features_joint(const float *__restrict__ decC, const float *__restrict__ qc, int B, int H, int W,
+                                 float *__restrict__ dec, bf16 *__restrict__ feat)
+{
+    const int Wc = W / 2, Hc = H / 2;
+    const long long n0 = (long long)B * Hc * Wc, plane = (long long)B * H * W;
+    for (long long p = blockIdx.x * (long long)blockDim.x + threadIdx.x; p < n0; p += (long long)gridDim.x * blockDim.x) {
+        const int x = (int)(p % Wc), y = (int)((p / Wc) % Hc), b = (int)(p / ((long long)Wc * Hc));
+        bf16 f[4];
+#pragma unroll
+        for (int k = 0; k < 2; k++) {
+            const float *c = decC + ((size_t)b * 2 + k) * Hc * Wc;
+            f[2 * k] = __float2bfloat16_rn(c[(size_t)y * Wc + x] * (1.f / 128.f));
+            f[2 * k + 1] = __float2bfloat16_rn(__ldg(qc + ((size_t)b * 2 + k) * 64 + (y & 7) * 8 + (x & 7)) * (1.f / 64.f));
+#pragma unroll
+            for (int d = 0; d < 4; d++) {
+                const int dy = d >> 1, dx = d & 1;
+                const int nx = dx ? min(x + 1, Wc - 1) : max(x - 1, 0), ny = dy ? min(y + 1, Hc - 1) : max(y - 1, 0);
+                const float *r0 = c + (size_t)y * Wc, *r1 = c + (size_t)ny * Wc;
+                const float v = tri_mix(tri_mix(r0[x], r0[nx]), tri_mix(r1[x], r1[nx]));
+                dec[(1 + k) * plane + ((size_t)b * H + 2 * y + dy) * W + 2 * x + dx] = v;
+            }
+        }
+        uint2 o;
+        memcpy(&o, f, 8);
+        *reinterpret_cast<uint2 *>(feat + p * 16 + 8) = o;
+    }
+}
+
+// Joint residual head output r (fp32 [B][H0][W0][rstride], channels 4 c + 2 dy
+// + dx = sample (2 y + dy, 2 x + dx) of component c) -> prediction
+// pred[3][B][H][W] = dec + 16 r; with a target: gradient of the mean squared
+// error over the 3 B H W samples into channels 0-11 of grad[B][H0][W0][16],
+// per-block partial sums of the squared error.
+__global__ void k_residual_joint(const float *__restrict__ r, int rstride, const float *__restrict__ dec,
+                                 const float *__restrict__ target, int B, int H, int W, float inv_count,
+                                 float *__restrict__ pred, bf16 *__restrict__ grad, float *__restrict__ loss_partial)
+{
+    __shared__ float s[256];
+    const int W0 = W / 2, H0 = H / 2;
+    const long long n0 = (long long)B * H0 * W0, plane = (long long)B * H * W;
+    float acc = 0.f;
+    for (long long p = blockIdx.x * (long long)blockDim.x + threadIdx.x; p < n0; p += (long long)gridDim.x * blockDim.x) {
+        const int x = (int)(p % W0), y = (int)((p / W0) % H0), b = (int)(p / ((long long)W0 * H0));
+        uint4 o[2] = {make_uint4(0, 0, 0, 0), make_uint4(0, 0, 0, 0)};
+        bf16 *gv = reinterpret_cast<bf16 *>(o);
+#pragma unroll
+        for (int c = 0; c < 3; c++) {
+#pragma unroll
+            for (int k = 0; k < 4; k++) {
+                const size_t q = c * plane + ((size_t)b * H + 2 * y + (k >> 1)) * W + 2 * x + (k & 1);
+                const float rv = r[p * rstride + 4 * c + k];
+                const float d = dec[q];
+                if (pred) pred[q] = d + 16.f * rv;
+                if (target) {
+                    const float e = rv - (target[q] - d) * (1.f / 16.f);
+                    acc += e * e;
+                    gv[4 * c + k] = __float2bfloat16_rn(2.f * e * inv_count);
+                }
+            }
+        }
+        if (target) {
+            uint4 *g = reinterpret_cast<uint4 *>(grad + p * 16);
+            g[0] = o[0];
+            g[1] = o[1];
+        }
+    }
+    s[threadIdx.x] = acc;
+    __syncthreads();
+    for (int k = 128; k > 0; k >>= 1) {
+        if (threadIdx.x < k) s[threadIdx.x] += s[threadIdx.x + k];
+        __syncthreads();
+    }
+    if (threadIdx.x == 0 && loss_partial) loss_partial[blockIdx.x] = s[0];
 }
 
 // ---------------------------------------------------------------------------
@@ -1448,7 +1543,7 @@ int32_t art_cnn_bias_grad(const void *g, int64_t npix, int32_t C, float *workspa
 int32_t art_cnn_features(const int16_t *coef, int32_t cpitch, int64_t img_stride, const float *q, int32_t B,
                          int32_t H, int32_t W, float *dec, void *feat, void *stream)
 {
-    if (!coef || !q || !dec || !feat || H % 8 || W % 8 || cpitch < W || cpitch % 8 || img_stride % 8)
+    if (!coef || !q || !dec || H % 8 || W % 8 || cpitch < W || cpitch % 8 || img_stride % 8)
         return fail(ART_ERR_INVALID_ARGUMENT, "features: bad arguments");
     if ((reinterpret_cast<uintptr_t>(coef) | reinterpret_cast<uintptr_t>(dec) | reinterpret_cast<uintptr_t>(feat)) & 15)
         return fail(ART_ERR_INVALID_ARGUMENT, "features: coef, dec and feat must be 16-byte aligned");
@@ -1619,7 +1714,7 @@ int32_t net_alloc(ArtNet *net, int slot, long long px, long long full, bool trai
         {&A.feat, P0 * 16 * 2}, {&A.dec, PF * 4},       {&A.cat1, P0 * 96 * 2}, {&A.cat2, P1 * 160 * 2},
         {&A.cat3, P2 * 224 * 2}, {&A.p1, P1 * 32 * 2},   {&A.p2, P2 * 64 * 2},   {&A.p3, P3 * 96 * 2},
         {&A.e4, P3 * 128 * 2},  {&A.d3, P2 * 96 * 2},   {&A.d2, P1 * 64 * 2},   {&A.d1, P0 * 32 * 2},
-        {&A.r, P0 * RSTRIDE * 4}, {&A.pred, PF * 4},
+        {&A.r, P0 * JOINT_RSTRIDE * 4}, {&A.pred, PF * 4},
     };
     if (train) {
         std::vector<Req> t = {
@@ -1670,7 +1765,7 @@ int32_t net_pack(ArtNet *net, bool backward, cudaStream_t s)
 // of `out` (cstride channels; 2H x 2W, each pixel stored to its 2x2 cell,
 // when up2), optionally also the fp32 output and the 2x2-pooled output.
 int32_t conv(ArtNet *net, int layer, const void *x, int B, int H, int W, void *out, int cstride, int coff,
-             float *out_f32, cudaStream_t s, void *pool_out = nullptr, int up2 = 0)
+             float *out_f32, cudaStream_t s, void *pool_out = nullptr, int up2 = 0, int f32_channels = RSTRIDE)
 {
     const LayerDef &L = LAYERS[layer];
     ArtCnnConv d{};
@@ -1689,9 +1784,10 @@ int32_t conv(ArtNet *net, int layer, const void *x, int B, int H, int W, void *o
     d.out_coff = coff;
     d.out_f32 = out_f32;
     // The fp32 output is the head's: only its first 4 channels (the 2x2 cell
-    // residuals) are used, stored densely.
-    d.f32_cstride = RSTRIDE;
-    d.f32_channels = RSTRIDE;
+    // residuals; 12 for the joint 4:2:0 network, three components' cells) are
+    // used, stored densely.
+    d.f32_cstride = f32_channels;
+    d.f32_channels = f32_channels;
     d.relu = L.relu;
     d.err = net->errflag.as<int>();
     d.pool_out = pool_out;
@@ -1756,7 +1852,7 @@ int32_t wgrad(ArtNet *net, int layer, const void *x, const void *g, int B, int H
 // their pooled outputs. For inference the e4/d3/d2 convolutions store their
 // outputs upsampled straight into the next concatenation; training keeps
 // them whole (the backward pass reads them as ReLU masks) and upsamples after.
-int32_t net_forward(ArtNet *net, NetActs &A, int B, int H, int W, cudaStream_t s, bool train)
+int32_t net_forward(ArtNet *net, NetActs &A, int B, int H, int W, cudaStream_t s, bool train, int rch = RSTRIDE)
 {
     const int H1 = H / 2, W1 = W / 2, H2 = H / 4, W2 = W / 4, H3 = H / 8, W3 = W / 8;
     NET_TRY(conv(net, E1, A.feat.p, B, H, W, A.cat1.p, 96, 0, nullptr, s, A.p1.p));
@@ -1775,7 +1871,7 @@ int32_t net_forward(ArtNet *net, NetActs &A, int B, int H, int W, cudaStream_t s
         NET_TRY(conv(net, D2, A.cat2.p, B, H1, W1, A.cat1.p, 96, 32, nullptr, s, nullptr, 1));
     }
     NET_TRY(conv(net, D1, A.cat1.p, B, H, W, A.d1.p, 32, 0, nullptr, s));
-    NET_TRY(conv(net, HEAD, A.d1.p, B, H, W, nullptr, 0, 0, A.r.as<float>(), s));
+    NET_TRY(conv(net, HEAD, A.d1.p, B, H, W, nullptr, 0, 0, A.r.as<float>(), s, nullptr, 0, rch));
     return ART_OK;
 }
 
@@ -1866,6 +1962,65 @@ int32_t net_prepare(ArtNet *net, int slot, int B, int H, int W, void *stream)
 {
     NET_TRY(check_geometry(B, H, W));
     NET_TRY(net_alloc(net, slot, (long long)B * level0(H) * level0(W), (long long)B * H * W, false));
+    if (!net->packed) NET_TRY(net_pack(net, false, static_cast<cudaStream_t>(stream)));
+    return ART_OK;
+}
+
+// Joint 4:2:0 geometry: H x W luma (multiples of 16), chroma H/2 x W/2.
+int32_t check_joint_geometry(int B, int H, int W)
+{
+    if (B < 1 || H < 16 || W < 16 || H % 16 || W % 16)
+        return fail(ART_ERR_INVALID_ARGUMENT, "joint network input must be at least 16x16 and a multiple of 16 on each side");
+    if ((long long)B * H * W * 4 > (1LL << 28)) return fail(ART_ERR_INVALID_ARGUMENT, "network input too large");
+    return ART_OK;
+}
+
+// Level-0 pixels and full-resolution floats (bases [3][B][H][W] plus the
+// decoded chroma at component resolution) of a joint pass.
+inline long long joint_px(int B, int H, int W) { return (long long)B * (H / 2) * (W / 2); }
+inline long long joint_full(int B, int H, int W) { return 4LL * B * H * W; }
+
+// Features of B joint 4:2:0 images into A.feat and the bases into A.dec
+// ([3][B][H][W], then the decoded chroma [B][2][H/2][W/2]).
+int32_t joint_features(NetActs &A, const int16_t *cy, int py, long long sy, const int16_t *cc, int pc, long long sc,
+                       const float *qy, const float *qc, int B, int H, int W, cudaStream_t s)
+{
+    float *dec = A.dec.as<float>();
+    float *decC = dec + 3 * (size_t)B * H * W;
+    NET_TRY(art_cnn_features(cy, py, sy, qy, B, H, W, dec, A.feat.p, s));
+    NET_TRY(art_cnn_features(cc, pc, sc, qc, 2 * B, H / 2, W / 2, decC, nullptr, s));
+    k_features_joint<<<blocks_for(joint_px(B, H, W), 256), 256, 0, s>>>(decC, qc, B, H, W, dec,
+                                                                        static_cast<bf16 *>(A.feat.p));
+    return check_launch("k_features_joint");
+}
+
+int32_t net_predict_joint(ArtNet *net, int slot, const int16_t *cy, int py, long long sy, const int16_t *cc, int pc,
+                          long long sc, const float *qy, const float *qc, int B, int H, int W, float *pred,
+                          cudaStream_t s)
+{
+    NET_TRY(check_joint_geometry(B, H, W));
+    NET_TRY(net_alloc(net, slot, joint_px(B, H, W), joint_full(B, H, W), false));
+    if (!net->packed) NET_TRY(net_pack(net, false, s));
+    NetActs &A = net->act[slot];
+    NET_TRY(joint_features(A, cy, py, sy, cc, pc, sc, qy, qc, B, H, W, s));
+    NET_TRY(net_forward(net, A, B, H / 2, W / 2, s, false, JOINT_RSTRIDE));
+    k_residual_joint<<<8 * num_sms(), 256, 0, s>>>(A.r.as<float>(), JOINT_RSTRIDE, A.dec.as<float>(), nullptr, B, H,
+                                                  W, 0.f, pred ? pred : A.pred.as<float>(), nullptr, nullptr);
+    return check_launch("k_residual_joint");
+}
+
+int32_t net_predict_joint_async(ArtNet *net, int slot, const int16_t *cy, int py, long long sy, const int16_t *cc,
+                                int pc, long long sc, const float *qy, const float *qc, int H, int W, float *pred,
+                                void *stream)
+{
+    return net_predict_joint(net, slot, cy, py, sy, cc, pc, sc, qy, qc, 1, H, W, pred,
+                             static_cast<cudaStream_t>(stream));
+}
+
+int32_t net_prepare_joint(ArtNet *net, int slot, int H, int W, void *stream)
+{
+    NET_TRY(check_joint_geometry(1, H, W));
+    NET_TRY(net_alloc(net, slot, joint_px(1, H, W), joint_full(1, H, W), false));
     if (!net->packed) NET_TRY(net_pack(net, false, static_cast<cudaStream_t>(stream)));
     return ART_OK;
 }
@@ -1971,6 +2126,68 @@ int32_t art_net_predict(ArtNet *net, const int16_t *coef, int32_t cpitch, int64_
     cudaSetDevice(net->device);
     cudaStream_t s = static_cast<cudaStream_t>(stream);
     NET_TRY(net_predict(net, 0, coef, cpitch, img_stride, q, B, H, W, pred, s));
+    return read_err(net, s);
+}
+
+int32_t art_net_predict_joint(ArtNet *net, const int16_t *coef_y, int32_t cpitch_y, int64_t stride_y,
+                              const int16_t *coef_c, int32_t cpitch_c, int64_t stride_c, const float *q_y,
+                              const float *q_c, int32_t B, int32_t H, int32_t W, float *pred, void *stream)
+{
+    using namespace art::cnn;
+    if (!net || !coef_y || !coef_c || !q_y || !q_c || !pred)
+        return fail(ART_ERR_INVALID_ARGUMENT, "net_predict_joint: null pointer");
+    cudaSetDevice(net->device);
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    NET_TRY(net_predict_joint(net, 0, coef_y, cpitch_y, stride_y, coef_c, cpitch_c, stride_c, q_y, q_c, B, H, W, pred,
+                              s));
+    return read_err(net, s);
+}
+
+int32_t art_net_train_step_joint(ArtNet *net, const int16_t *coef_y, int32_t cpitch_y, int64_t stride_y,
+                                 const int16_t *coef_c, int32_t cpitch_c, int64_t stride_c, const float *q_y,
+                                 const float *q_c, const float *target, int32_t B, int32_t H, int32_t W, float lr,
+                                 float *loss, void *stream)
+{
+    using namespace art::cnn;
+    if (!net || !coef_y || !coef_c || !q_y || !q_c || !target)
+        return fail(ART_ERR_INVALID_ARGUMENT, "net_train_step_joint: null pointer");
+    cudaSetDevice(net->device);
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    NET_TRY(check_joint_geometry(B, H, W));
+    const int H0 = H / 2, W0 = W / 2;
+    NET_TRY(net_alloc(net, 0, joint_px(B, H, W), joint_full(B, H, W), true));
+    NetActs &A = net->act[0];
+    const size_t pb = (size_t)net->nparam * 4;
+    if (!net->grads.p) {
+        if (!net->grads.ensure(pb) || !net->adam_m.ensure(pb) || !net->adam_v.ensure(pb) ||
+            cudaMemsetAsync(net->adam_m.p, 0, pb, s) != cudaSuccess || cudaMemsetAsync(net->adam_v.p, 0, pb, s) != cudaSuccess)
+            return fail(ART_ERR_CUDA, "net_train_step_joint: allocation failed");
+    }
+    NET_TRY(net_pack(net, true, s));
+    NET_TRY(joint_features(A, coef_y, cpitch_y, stride_y, coef_c, cpitch_c, stride_c, q_y, q_c, B, H, W, s));
+    NET_TRY(net_forward(net, A, B, H0, W0, s, true, JOINT_RSTRIDE));
+    const long long n = 3LL * B * H * W;
+    k_residual_joint<<<LOSS_BLOCKS, 256, 0, s>>>(A.r.as<float>(), JOINT_RSTRIDE, A.dec.as<float>(), target, B, H, W,
+                                                 1.f / (float)n, A.pred.as<float>(), static_cast<bf16 *>(net->dr.p),
+                                                 net->loss_partial.as<float>());
+    NET_TRY(check_launch("k_residual_joint"));
+    NET_TRY(net_backward(net, B, H0, W0, s));
+    if (lr > 0.f) {
+        net->step++;
+        NET_TRY(art_cnn_adam(net->params.as<float>(), net->grads.as<float>(), net->adam_m.as<float>(),
+                             net->adam_v.as<float>(), net->nparam, lr, 0.9f, 0.999f, 1e-8f, net->step, s));
+        net->packed = false;
+    }
+    if (loss) {
+        float h[LOSS_BLOCKS];
+        if (cudaMemcpyAsync(h, net->loss_partial.p, sizeof(h), cudaMemcpyDeviceToHost, s) != cudaSuccess)
+            return fail(ART_ERR_CUDA, "net_train_step_joint: loss copy failed");
+        NET_TRY(read_err(net, s));
+        double t = 0;
+        for (float v : h) t += v;
+        *loss = (float)(t / (double)n);
+        return ART_OK;
+    }
     return read_err(net, s);
 }
 

@@ -1154,6 +1154,49 @@ __global__ void k_upsample(const float *__restrict__ img, const ImgDev *__restri
     im.y[off] = v;
 }
 
+// A full-resolution plane (dense rows of W) into both state buffers of
+// channel c (the joint learned start).
+__global__ void k_place(const float *__restrict__ img, const ImgDev *__restrict__ imgs, int c)
+{
+    const ImgDev &im = imgs[0];
+    const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= (long long)im.W * im.H) return;
+    const int y = (int)(i / im.W), x = (int)(i % im.W);
+    const float v = img[i];
+    const long long off = c * im.cstride + (long long)y * im.pitch + x;
+    im.x[off] = v;
+    im.y[off] = v;
+}
+
+// Smooth upsampling of a component image to both state buffers (the learned
+// start). Along each subsampled axis, full-resolution sample 2 i + d of cell i
+// takes 3/4 of cell i and 1/4 of its neighbour on that side (cell i - 1 for
+// d = 0, i + 1 for d = 1), clamped at the component's edges: linear
+// interpolation between cell centres, horizontal first, each product and sum
+// rounded on its own (no contraction), so a float32 host restatement is exact.
+// Replicating the cells instead (k_upsample) leaves a step at every cell edge
+// that the second-order term prices high and the iterations are slow to
+// remove; the projection that follows restores the cells' means.
+__device__ __forceinline__ float tri_mix(float a, float b) { return __fadd_rn(__fmul_rn(0.75f, a), __fmul_rn(0.25f, b)); }
+
+__global__ void k_upsample_smooth(const float *__restrict__ img, const ImgDev *__restrict__ imgs, int c)
+{
+    const ImgDev &im = imgs[0];
+    const ChanDev &cd = im.ch[c];
+    const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= (long long)im.W * im.H) return;
+    const int y = (int)(i / im.W), x = (int)(i % im.W);
+    const int cy = min(y / cd.sv, cd.chh - 1), cx = min(x / cd.sh, cd.cw - 1);
+    const int nx = cd.sh == 2 ? ((x & 1) ? min(cx + 1, cd.cw - 1) : max(cx - 1, 0)) : cx;
+    const int ny = cd.sv == 2 ? ((y & 1) ? min(cy + 1, cd.chh - 1) : max(cy - 1, 0)) : cy;
+    const float *r0 = img + (long long)cy * cd.cw, *r1 = img + (long long)ny * cd.cw;
+    float v = cd.sh == 2 ? tri_mix(r0[cx], r0[nx]) : r0[cx];
+    if (cd.sv == 2) v = tri_mix(v, cd.sh == 2 ? tri_mix(r1[cx], r1[nx]) : r1[cx]);
+    const long long off = c * im.cstride + (long long)y * im.pitch + x;
+    im.x[off] = v;
+    im.y[off] = v;
+}
+
 // Output stage of Artefact::process (lib.rs:159-211): luma + 128, YCbCr ->
 // RGB with unfused multiply-adds, clamp to [0, 255], truncating u8 cast (NaN
 // -> 0), crop to the real size. A single channel is replicated to gray RGB.
@@ -1365,6 +1408,7 @@ struct ArtContext {
     art::DevBuf xbuf, pbuf, coefimg, stage, misc, desc, work, tasks, compat, sepplanes, rgb, pred;
     art::HostBuf hstage, hrgb;        // pinned host staging of art_context_process_batch
     ArtNet *net = nullptr;            // warm-start network for ART_INIT_LEARNED (not owned)
+    ArtNet *net_joint = nullptr;      // joint 4:2:0 warm-start network, used for 4:2:0 images (not owned)
     // The learned start's launches (network, upsampling, zero-step projection)
     // as a graph: captured the second time one key is seen, then replayed.
     cudaGraphExec_t init_exec = nullptr;
@@ -1637,7 +1681,8 @@ static void launch_projections(ArtContext *ctx, float fnext)
 static int prepare_batch(ArtContext *ctx, const std::vector<ImageSpec> &specs, uint32_t iterations, int init_mode,
                          uint32_t step_iterations)
 {
-    if (init_mode == ART_INIT_LEARNED && !ctx->net) return fail(ART_ERR_INVALID_ARGUMENT, "learned start: no network attached");
+    if (init_mode == ART_INIT_LEARNED && !ctx->net && !ctx->net_joint)
+        return fail(ART_ERR_INVALID_ARGUMENT, "learned start: no network attached");
     const uint32_t step_its = step_iterations ? step_iterations : iterations;
     int rc;
     const int nimg = (int)specs.size();
@@ -1797,14 +1842,27 @@ static int prepare_batch(ArtContext *ctx, const std::vector<ImageSpec> &specs, u
             }
         }
     } else if (init_mode == ART_INIT_LEARNED) {
-        // Prediction per component at its own resolution, repeated to full
-        // resolution into x and y, then one projection with a zero step
+        // Prediction per component at its own resolution, upsampled smoothly
+        // to full resolution into x and y, then one projection with a zero step
         // (g = 0, sigma = 0): x_0 = y_0 = P(prediction), and the DCT-distance
         // plane of the projected prediction for the first gradient.
+        // A 4:2:0 image (luma H x W, both chroma H/2 x W/2, H and W multiples
+        // of 16) goes through the joint network when one is attached: one
+        // pass predicts all three components at full resolution.
+        auto joint_ok = [&](int i) {
+            const ImgDev &d = ctx->h_desc[i];
+            if (!ctx->net_joint || d.nch != 3 || d.W % 16 || d.H % 16) return false;
+            const ChanDev *ch = d.ch;
+            return ch[0].sh == 1 && ch[0].sv == 1 && ch[0].cw == d.W && ch[0].chh == d.H && ch[1].sh == 2 &&
+                   ch[1].sv == 2 && ch[2].sh == 2 && ch[2].sv == 2 && ch[1].cw * 2 == d.W && ch[1].chh * 2 == d.H &&
+                   ch[2].cw == ch[1].cw && ch[2].chh == ch[1].chh && ch[2].cpitch == ch[1].cpitch;
+        };
         size_t need = 0;
-        for (const auto &sp : specs) {
+        for (int i = 0; i < nimg; i++) {
+            const ImageSpec &sp = specs[i];
             size_t img = 0;
             for (uint32_t c = 0; c < sp.nch; c++) img += (size_t)sp.ch[c].rounded_px_w * sp.ch[c].rounded_px_h;
+            if (joint_ok(i)) img = 3 * (size_t)sp.W * sp.H;
             need = std::max(need, img);
         }
         if ((rc = ctx->pred.ensure(need * sizeof(float)))) return rc;
@@ -1820,10 +1878,20 @@ static int prepare_batch(ArtContext *ctx, const std::vector<ImageSpec> &specs, u
             int i, c, nb;
             long long stride;
             size_t poff;
+            bool joint;
         };
         std::vector<Group> groups;
         for (int i = 0; i < nimg; i++) {
             const ImgDev &d = ctx->h_desc[i];
+            if (joint_ok(i)) {
+                const int slot = (int)(groups.size() % 2);
+                groups.push_back({i, 0, 3, (long long)(d.ch[2].coef - d.ch[1].coef), 0, true});
+                if ((rc = cnn::net_prepare_joint(ctx->net_joint, slot, d.H, d.W, s))) return rc;
+                continue;
+            }
+            if (!ctx->net)
+                return fail(ART_ERR_INVALID_ARGUMENT,
+                            "learned start: no network attached for an image that is not 4:2:0 (art_context_set_warm_start)");
             size_t poff = 0;
             for (int c = 0; c < d.nch;) {
                 const ChanDev &cd = d.ch[c];
@@ -1833,15 +1901,17 @@ static int prepare_batch(ArtContext *ctx, const std::vector<ImageSpec> &specs, u
                        d.ch[c + nb].cpitch == cd.cpitch && d.ch[c + nb].coef - d.ch[c + nb - 1].coef == stride)
                     nb++;
                 const int slot = (int)(groups.size() % 2);
-                groups.push_back({i, c, nb, stride, poff});
+                groups.push_back({i, c, nb, stride, poff, false});
                 if ((rc = cnn::net_prepare(ctx->net, slot, nb, cd.chh, cd.cw, s))) return rc;
                 poff += (size_t)nb * cd.cw * cd.chh;
                 c += nb;
             }
         }
         // Everything the launches below bake in: buffers, geometry, tasks.
+        auto gen = [](ArtNet *n, int slot) { return n ? cnn::net_generation(n, slot) : 0ull; };
         std::vector<unsigned long long> key = {
-            (unsigned long long)(uintptr_t)ctx->net, cnn::net_generation(ctx->net, 0), cnn::net_generation(ctx->net, 1),
+            (unsigned long long)(uintptr_t)ctx->net, gen(ctx->net, 0), gen(ctx->net, 1),
+            (unsigned long long)(uintptr_t)ctx->net_joint, gen(ctx->net_joint, 0), gen(ctx->net_joint, 1),
             (uintptr_t)ctx->desc.p, (uintptr_t)ctx->tasks.p, (uintptr_t)pred, (uintptr_t)ctx->xbuf.p,
             (uintptr_t)ctx->coefimg.p, (unsigned long long)nimg, (unsigned long long)ctx->proj_warps};
         for (int m = 0; m < 5; m++) key.push_back((unsigned long long)ctx->mode_off[m]);
@@ -1853,8 +1923,8 @@ static int prepare_batch(ArtContext *ctx, const std::vector<ImageSpec> &specs, u
                 key.insert(key.end(), {(unsigned long long)d.ch[c].cw, (unsigned long long)d.ch[c].chh,
                                        (unsigned long long)d.ch[c].cpitch, (uintptr_t)d.ch[c].coef});
         }
-        // Prediction per component at its own resolution, repeated to full
-        // resolution into x and y, then one projection with a zero step
+        // Prediction per component at its own resolution, upsampled smoothly
+        // to full resolution into x and y, then one projection with a zero step
         // (g = 0, sigma = 0): x_0 = y_0 = P(prediction), and the DCT-distance
         // plane of the projected prediction for the first gradient.
         auto launch_init = [&]() -> int {
@@ -1869,11 +1939,22 @@ static int prepare_batch(ArtContext *ctx, const std::vector<ImageSpec> &specs, u
                 const ImgDev &d = ctx->h_desc[gr.i];
                 const ChanDev &cd = d.ch[gr.c];
                 float *gp = pred + gr.poff;
+                const int blocks = (int)(((long long)d.W * d.H + 255) / 256);
+                if (gr.joint) {
+                    const int r = cnn::net_predict_joint_async(ctx->net_joint, slot, cd.coef, cd.cpitch, 0,
+                                                               d.ch[1].coef, d.ch[1].cpitch, gr.stride,
+                                                               &ddesc[gr.i].q[0][0], &ddesc[gr.i].q[1][0], d.H, d.W,
+                                                               gp, gs);
+                    if (r) return r;
+                    for (int c = 0; c < 3; c++)
+                        k_place<<<blocks, 256, 0, gs>>>(gp + (size_t)c * d.W * d.H, ddesc + gr.i, c);
+                    continue;
+                }
                 const int r = cnn::net_predict_async(ctx->net, slot, cd.coef, cd.cpitch, gr.stride,
                                                      &ddesc[gr.i].q[gr.c][0], gr.nb, cd.chh, cd.cw, gp, gs);
                 if (r) return r;
                 for (int k = 0; k < gr.nb; k++)
-                    k_upsample<<<(int)(((long long)d.W * d.H + 255) / 256), 256, 0, gs>>>(
+                    k_upsample_smooth<<<(int)(((long long)d.W * d.H + 255) / 256), 256, 0, gs>>>(
                         gp + (size_t)k * cd.cw * cd.chh, ddesc + gr.i, gr.c + k);
             }
             if (groups.size() > 1) {
@@ -2045,7 +2126,11 @@ static int check_errflag(ArtContext *ctx)
     unsigned flag = 0;
     ART_CUDA(cudaMemcpy(&flag, ctx->errflag, sizeof(unsigned), cudaMemcpyDeviceToHost));
     if (flag) return fail(ART_ERR_INVALID_DATA, "coefficients must be integers in [-32768, 32767]");
-    if (ctx->net_used && ctx->net) return cnn::net_error(ctx->net);
+    if (ctx->net_used && ctx->net) {
+        const int r = cnn::net_error(ctx->net);
+        if (r) return r;
+    }
+    if (ctx->net_used && ctx->net_joint) return cnn::net_error(ctx->net_joint);
     return ART_OK;
 }
 
@@ -2075,7 +2160,7 @@ static int init_spec(const ArtContext *ctx, const ArtOptions *opts, InitSpec *ou
         return fail(ART_ERR_INVALID_ARGUMENT, "step_decay must lie in [0, 1]");
     if (out->mode != ART_INIT_DECODED && out->mode != ART_INIT_SCALAR_COMPAT && out->mode != ART_INIT_LEARNED)
         return fail(ART_ERR_INVALID_ARGUMENT, "unknown init mode");
-    if (out->mode == ART_INIT_LEARNED && !ctx->net)
+    if (out->mode == ART_INIT_LEARNED && !ctx->net && !ctx->net_joint)
         return fail(ART_ERR_INVALID_ARGUMENT, "learned start: no network attached (art_context_set_warm_start)");
     return ART_OK;
 }
@@ -2285,6 +2370,16 @@ int32_t art_context_set_warm_start(ArtContext *ctx, ArtNet *net)
     if (net && cnn::net_device(net) != ctx->device)
         return fail(ART_ERR_INVALID_ARGUMENT, "warm-start network lives on another device than the context");
     ctx->net = net;
+    ctx->net_used = false;
+    return ART_OK;
+}
+
+int32_t art_context_set_joint_warm_start(ArtContext *ctx, ArtNet *net)
+{
+    if (!ctx) return fail(ART_ERR_INVALID_ARGUMENT, "null context");
+    if (net && cnn::net_device(net) != ctx->device)
+        return fail(ART_ERR_INVALID_ARGUMENT, "warm-start network lives on another device than the context");
+    ctx->net_joint = net;
     ctx->net_used = false;
     return ART_OK;
 }

@@ -36,31 +36,32 @@ WEIGHT, PWEIGHT = 0.3, 0.001
 TARGET_ITERATIONS = 300
 
 
-def crop_spec(i: int, seed0: int = SEED0) -> Tuple[int, str, int]:
-    """(quality, subsampling, seed) of training crop i."""
+def crop_spec(i: int, seed0: int = SEED0, sub: str = "") -> Tuple[int, str, int]:
+    """(quality, subsampling, seed) of training crop i; `sub` fixes the
+    subsampling (the joint 4:2:0 network trains on 4:2:0 crops only)."""
     rng = np.random.default_rng(seed0 + i)
     q = int(rng.integers(20, 91))
-    sub = "4:2:0" if rng.random() < 0.5 else "4:4:4"
-    return q, sub, seed0 + i
+    s = "4:2:0" if rng.random() < 0.5 else "4:4:4"
+    return q, sub or s, seed0 + i
 
 
 def _make_crop(args):
-    i, seed0 = args
+    i, seed0, sub = args
     from . import synth
     from .api import Jpeg, JpegSource
 
-    q, sub, seed = crop_spec(i, seed0)
+    q, sub, seed = crop_spec(i, seed0, sub)
     return Jpeg.from_source(JpegSource.Buffer(synth.make_jpeg(CROP, CROP, q, sub, False, seed)))
 
 
-def make_crops(n: int, seed0: int = SEED0, workers: int = 0) -> list:
+def make_crops(n: int, seed0: int = SEED0, workers: int = 0, sub: str = "") -> list:
     """Decoded JPEGs of crops 0..n-1 (a spawn-started process pool, so it is
     safe before or after CUDA is initialised)."""
     workers = workers or max(1, min(32, os.cpu_count() or 1))
     if workers == 1:
-        return [_make_crop((i, seed0)) for i in range(n)]
+        return [_make_crop((i, seed0, sub)) for i in range(n)]
     with ProcessPoolExecutor(max_workers=workers, mp_context=mp.get_context("spawn")) as ex:
-        return list(ex.map(_make_crop, [(i, seed0) for i in range(n)], chunksize=64))
+        return list(ex.map(_make_crop, [(i, seed0, sub) for i in range(n)], chunksize=64))
 
 
 def cell_mean(plane: np.ndarray, sh: int, sv: int) -> np.ndarray:
@@ -130,6 +131,76 @@ def build_pools(n: int, seed0: int, ctx, chunk: int = 1024, log=print):
         log(f"crops {k + m}/{n}: decode {t1 - t0:.1f} s, solve {time.time() - t1:.1f} s")
         t0 = time.time()
     return pools.tensors()
+
+
+def build_joint_pools(n: int, seed0: int, ctx, chunk: int = 1024, log=print):
+    """Joint 4:2:0 samples on the GPU: coef_y int16 [N][H][W], coef_c int16
+    [N][2][H/2][W/2], q_y [N][64], q_c [N][2][64] and the full-resolution
+    300-iteration targets [N][3][H][W]."""
+    import torch
+
+    from .warmstart import coef_image
+
+    parts = []
+    t0 = time.time()
+    for k in range(0, n, chunk):
+        m = min(chunk, n - k)
+        jpegs = make_crops(m, seed0 + k, sub="4:2:0")
+        t1 = time.time()
+        planes = solve_targets(ctx, jpegs)
+        cy, cc, qy, qc, tg = [], [], [], [], []
+        for j, pl in zip(jpegs, planes):
+            W, H, _ = j.max_rounded()
+            cy.append(coef_image(j.coefs[0]))
+            cc.append(np.stack([coef_image(co) for co in j.coefs[1:]]))
+            qy.append(np.asarray(j.coefs[0].quant_table, np.float32))
+            qc.append(np.stack([np.asarray(co.quant_table, np.float32) for co in j.coefs[1:]]))
+            tg.append(np.stack([p.reshape(H, W) for p in pl]))
+        parts.append(tuple(torch.from_numpy(np.stack(a)).cuda() for a in (cy, cc, qy, qc, tg)))
+        log(f"joint crops {k + m}/{n}: decode {t1 - t0:.1f} s, solve {time.time() - t1:.1f} s")
+        t0 = time.time()
+    return tuple(torch.cat([p[i] for p in parts]) for i in range(5))
+
+
+def train_joint(net, data, epochs: int, lr: float = 1e-3, batch: int = 16, seed: int = 0, log=print):
+    """Adam with linear warm-up and cosine decay on the joint 4:2:0 loss."""
+    import torch
+
+    g = torch.Generator(device="cpu").manual_seed(seed)
+    n = data[0].shape[0]
+    nb = math.ceil(n / batch)
+    total = epochs * nb
+    warm = min(200, total // 10 + 1)
+    step, hist = 0, []
+    for ep in range(epochs):
+        perm = torch.randperm(n, generator=g)
+        acc, t0 = 0.0, time.time()
+        for b in range(nb):
+            idx = perm[b * batch:(b + 1) * batch].cuda()
+            cy, cc, qy, qc, tg = (t.index_select(0, idx) for t in data)
+            cur = lr * min(1.0, (step + 1) / warm) * (0.05 + 0.95 * 0.5 * (1 + math.cos(math.pi * step / total)))
+            loss = net.train_step_joint(cy.contiguous(), cc.contiguous(), qy.contiguous(), qc.contiguous(),
+                                        tg.permute(1, 0, 2, 3).contiguous(), cur)
+            acc += loss
+            step += 1
+            hist.append(loss)
+        log(f"joint epoch {ep + 1}/{epochs}: mean loss {acc / nb:.5f} ({nb} steps, {time.time() - t0:.1f} s)")
+    return hist
+
+
+def evaluate_joint(net, data, batch: int = 16):
+    """Mean squared error (levels^2) per component (luma, Cb, Cr) of the joint
+    prediction against the targets."""
+    import torch
+
+    se = torch.zeros(3, dtype=torch.float64, device="cuda")
+    n = data[0].shape[0]
+    for b in range(0, n, batch):
+        cy, cc, qy, qc, tg = (t[b:b + batch].contiguous() for t in data)
+        pred = net.predict_joint(cy, cc, qy, qc)
+        se += ((pred - tg.permute(1, 0, 2, 3)) ** 2).sum(dim=(1, 2, 3)).double()
+    torch.cuda.synchronize()
+    return (se / (n * data[0].shape[1] * data[0].shape[2])).tolist()
 
 
 def batch_size(shape, pixels_per_batch: int) -> int:
@@ -206,6 +277,9 @@ def main(argv=None):
     ap.add_argument("--smooth", type=float, default=0.0,
                     help="weight of the loss's smoothness term (squared differences of the error between adjacent "
                          "samples); 0 = plain MSE")
+    ap.add_argument("--joint", action="store_true",
+                    help="train the joint 4:2:0 network (all three components in one pass, full-resolution chroma) "
+                         "on 4:2:0 crops")
     ap.add_argument("--objective", type=float, default=0.0,
                     help="weight of the loss's objective term (the solver's objective of the projected "
                          "prediction, per sample); 0 = off")
@@ -219,6 +293,20 @@ def main(argv=None):
 
     ctx = Context(0)
     net = WS.WarmStartNet(WS.load_params(args.init) if args.init else WS.init_params(args.seed))
+    if args.joint:
+        t0 = time.time()
+        data = build_joint_pools(args.crops, SEED0, ctx, log=log)
+        val = build_joint_pools(args.val, SEED0 + 10_000_000, ctx, log=log)
+        log(f"data ready in {time.time() - t0:.1f} s: {data[0].shape[0]} crops")
+        mse0 = evaluate_joint(net, val)
+        t1 = time.time()
+        train_joint(net, data, args.epochs, args.lr, seed=args.seed, log=log)
+        log(f"training {time.time() - t1:.1f} s")
+        mse = evaluate_joint(net, val)
+        log(f"held-out MSE vs 300-iteration targets (levels^2, luma/Cb/Cr): untrained {mse0}, trained {mse}")
+        net.save(args.out)
+        print(f"{args.out}: held-out mse {mse}")
+        return
     net.set_loss(args.smooth)
     net.set_objective(args.objective, WEIGHT, PWEIGHT)
     t0 = time.time()

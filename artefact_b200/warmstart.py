@@ -84,6 +84,28 @@ def load_params(path=DEFAULT_WEIGHTS) -> np.ndarray:
     return np.frombuffer(data[16:], "<f4").copy()
 
 
+def upsample_component(plane: np.ndarray, sh: int, sv: int, H: int, W: int) -> np.ndarray:
+    """A component-resolution plane [h][w] upsampled to the full H x W grid as
+    the learned start places it: along each subsampled axis (factor 2), sample
+    2 i + d of cell i = 3/4 of cell i + 1/4 of its neighbour on that side
+    (i - 1 for d = 0, i + 1 for d = 1), clamped at the edges; horizontal first,
+    every product and sum rounded to float32 (bit-equal to the solver's
+    k_upsample_smooth)."""
+    p = np.asarray(plane, np.float32)
+    h, w = p.shape
+    y, x = np.arange(H), np.arange(W)
+    cy, cx = np.minimum(y // sv, h - 1), np.minimum(x // sh, w - 1)
+    nx = np.where(x & 1, np.minimum(cx + 1, w - 1), np.maximum(cx - 1, 0)) if sh == 2 else cx
+    ny = np.where(y & 1, np.minimum(cy + 1, h - 1), np.maximum(cy - 1, 0)) if sv == 2 else cy
+    a, b = np.float32(0.75), np.float32(0.25)
+    mix = lambda u, v: (a * u + b * v).astype(np.float32)
+    row = lambda r: mix(p[r][:, cx], p[r][:, nx]) if sh == 2 else p[r][:, cx]
+    out = row(cy)
+    if sv == 2:
+        out = mix(out, row(ny))
+    return np.ascontiguousarray(out, np.float32)
+
+
 def coef_image(coef) -> np.ndarray:
     """Block-raster coefficients of one component -> int16 coefficient image
     (coefficient (v,u) of block (bx,by) at row 8by+v, column 8bx+u)."""
@@ -164,6 +186,29 @@ class WarmStartNet:
         N.check(N.lib().art_net_train_step(self._h, _ptr(coef), W, H * W, _ptr(q), _ptr(target), B, H, W,
                                            float(lr), C.byref(loss), _stream(stream)))
         return float(loss.value)
+
+    def train_step_joint(self, coef_y, coef_c, q_y, q_c, target, lr: float, stream=None) -> float:
+        """One joint 4:2:0 step (art_net_train_step_joint): coef_y int16
+        [B][H][W], coef_c int16 [B][2][H/2][W/2], q_y [B][64], q_c [B][2][64],
+        target float32 [3][B][H][W] CUDA tensors. Returns the mean loss."""
+        B, H, W = coef_y.shape
+        loss = C.c_float()
+        N.check(N.lib().art_net_train_step_joint(self._h, _ptr(coef_y), W, H * W, _ptr(coef_c), W // 2,
+                                                 (H // 2) * (W // 2), _ptr(q_y), _ptr(q_c), _ptr(target), B, H, W,
+                                                 float(lr), C.byref(loss), _stream(stream)))
+        return float(loss.value)
+
+    def predict_joint(self, coef_y, coef_c, q_y, q_c, out=None, stream=None):
+        """Joint 4:2:0 prediction float32 [3][B][H][W] (art_net_predict_joint)."""
+        import torch
+
+        B, H, W = coef_y.shape
+        if out is None:
+            out = torch.empty((3, B, H, W), dtype=torch.float32, device=coef_y.device)
+        N.check(N.lib().art_net_predict_joint(self._h, _ptr(coef_y), W, H * W, _ptr(coef_c), W // 2,
+                                              (H // 2) * (W // 2), _ptr(q_y), _ptr(q_c), B, H, W, _ptr(out),
+                                              _stream(stream)))
+        return out
 
     def predict(self, coef, q, out=None, stream=None):
         """Prediction float32 [B][H][W] (a CUDA tensor) for coef int16 [B][H][W]."""

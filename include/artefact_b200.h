@@ -242,9 +242,12 @@ int32_t art_context_tune_cache(ArtContext *ctx, const char *path, int32_t save);
  * context (NULL detaches). The network must live on the context's device and
  * outlive its use; it is not owned by the context. With a learned start, each
  * component's prediction (art_net_predict at the component's resolution) is
- * repeated to full resolution like the decoded start, projected onto the
- * quantisation box, and the solve's `iterations` plain iterations refine it
- * with the FISTA sequence restarted. No reference counterpart.
+ * upsampled to full resolution along each subsampled axis by linear
+ * interpolation between cell centres (sample 2 i + d of cell i = 3/4 of cell i
+ * + 1/4 of cell i - 1 for d = 0, of cell i + 1 for d = 1, clamped at the
+ * edges; horizontal first, every product and sum rounded to float), projected
+ * onto the quantisation box, and the solve's `iterations` plain iterations
+ * refine it with the FISTA sequence restarted. No reference counterpart.
  * The predictions of one solve run on the context's two streams, each with
  * one of the network's two sets of activation buffers; so learned solves on
  * different contexts that share one network must not overlap in time. The
@@ -252,6 +255,14 @@ int32_t art_context_tune_cache(ArtContext *ctx, const char *path, int32_t save);
  * launches as a CUDA graph, which later solves of that geometry replay.
  */
 int32_t art_context_set_warm_start(ArtContext *ctx, ArtNet *net);
+/*
+ * Attach a joint 4:2:0 warm-start network (art_net_predict_joint; NULL
+ * detaches). ART_INIT_LEARNED solves of 4:2:0 images (three components, luma
+ * H x W and both chroma H/2 x W/2, H and W multiples of 16) then predict all
+ * three components at full resolution in one pass of it; other images use the
+ * network of art_context_set_warm_start. Same lifetime and sharing rules.
+ */
+int32_t art_context_set_joint_warm_start(ArtContext *ctx, ArtNet *net);
 
 /*
  * Objective and feasibility of image `image`'s result of the context's last
@@ -407,8 +418,8 @@ int32_t art_cnn_bias_grad(const void *g, int64_t npix, int32_t C, float *workspa
  * level, H0 = ceil(H / 16) * 8, W0 = ceil(W / 16) * 8 (space to depth):
  * level-0 pixel (y, x) holds samples (2y + dy, 2x + dx) as channels
  * 2 dy + dx = dec / 128 and 4 + 2 dy + dx = q / 64 (zero outside the image;
- * channels 8-15 zero). coef, dec and feat 16-byte aligned; cpitch and
- * img_stride multiples of 8. */
+ * channels 8-15 zero). feat may be NULL (decode only). coef, dec and feat
+ * 16-byte aligned; cpitch and img_stride multiples of 8. */
 int32_t art_cnn_features(const int16_t *coef, int32_t cpitch, int64_t img_stride, const float *q, int32_t B,
                          int32_t H, int32_t W, float *dec, void *feat, void *stream);
 /* Prediction pred[B][H][W] = dec + 16 r, r the depth-to-space of channels
@@ -448,6 +459,27 @@ int32_t art_net_gradients(ArtNet *net, float *host, int64_t n);
 /* Warm start: pred[B][H][W] (fp32, level-shifted samples) = decoded + 16 * residual. */
 int32_t art_net_predict(ArtNet *net, const int16_t *coef, int32_t cpitch, int64_t img_stride, const float *q,
                         int32_t B, int32_t H, int32_t W, float *pred, void *stream);
+/* Joint 4:2:0 warm start: one pass per image over the luma's level-0 grid
+ * (H/2 x W/2), whose pixels each carry a 2x2 luma cell and one sample of each
+ * chroma component (feature channels 8-11: decoded Cb / 128, its step / 64,
+ * the same for Cr). The head's outputs 4 c + 2 dy + dx are residuals of the
+ * full-resolution sample (2 y + dy, 2 x + dx) of component c, over the decoded
+ * luma and over the decoded chroma upsampled smoothly (as the learned start
+ * upsamples). Luma coefficient images coef_y[B] (H x W, rows of cpitch_y,
+ * stride_y apart), chroma coef_c[B][2] (H/2 x W/2, rows of cpitch_c; image b's
+ * Cb at coef_c + 2 b stride_c, its Cr stride_c after that), tables q_y[B][64]
+ * and q_c[B][2][64], all on the device; H, W multiples of 16.
+ * pred[3][B][H][W]: all luma planes, then all Cb, then all Cr. */
+int32_t art_net_predict_joint(ArtNet *net, const int16_t *coef_y, int32_t cpitch_y, int64_t stride_y,
+                              const int16_t *coef_c, int32_t cpitch_c, int64_t stride_c, const float *q_y,
+                              const float *q_c, int32_t B, int32_t H, int32_t W, float *pred, void *stream);
+/* One joint training step on the mean squared error (units of 16 levels) of
+ * all 3 B H W samples against target[3][B][H][W] (layout of pred above). The
+ * smoothness and objective terms are not used here. */
+int32_t art_net_train_step_joint(ArtNet *net, const int16_t *coef_y, int32_t cpitch_y, int64_t stride_y,
+                                 const int16_t *coef_c, int32_t cpitch_c, int64_t stride_c, const float *q_y,
+                                 const float *q_c, const float *target, int32_t B, int32_t H, int32_t W, float lr,
+                                 float *loss, void *stream);
 /* Training loss: mean squared error (in units of 16 levels) plus
  * smooth_weight times the mean over samples of the squared differences of the
  * error between horizontally and vertically adjacent samples (0, the default,

@@ -154,6 +154,39 @@ def features(coef_img, q):
     return dec, F
 
 
+def smooth_up2(c):
+    """[..., h, w] -> [..., 2h, 2w]: along each axis sample 2 i + d = 3/4 of
+    cell i + 1/4 of cell i - 1 (d = 0) or i + 1 (d = 1), clamped at the edges,
+    horizontal first (the learned start's chroma upsampling)."""
+    h, w = c.shape[-2:]
+    i = np.arange(2 * w)
+    cx = i // 2
+    nx = np.where(i & 1, np.minimum(cx + 1, w - 1), np.maximum(cx - 1, 0))
+    r = 0.75 * c[..., :, cx] + 0.25 * c[..., :, nx]
+    j = np.arange(2 * h)
+    cy = j // 2
+    ny = np.where(j & 1, np.minimum(cy + 1, h - 1), np.maximum(cy - 1, 0))
+    return 0.75 * r[..., cy, :] + 0.25 * r[..., ny, :]
+
+
+def features_joint(coef_y, q_y, coef_c, q_c):
+    """Joint 4:2:0 input: coef_y [B][H][W], q_y [B][64], coef_c [B][2][H/2][W/2],
+    q_c [B][2][64] (H, W multiples of 16). Returns dec [3][B][H][W] (the decoded
+    luma, then the decoded chroma upsampled by smooth_up2: the bases the
+    residuals are added to) and F [B][H/2][W/2][16]: the luma's features plus
+    channels 8 / 10 = decoded Cb / Cr sample / 128 and 9 / 11 = its step / 64."""
+    B, H, W = coef_y.shape
+    decY, F = features(coef_y, q_y)
+    decC, _ = features(coef_c.reshape(2 * B, H // 2, W // 2), np.asarray(q_c).reshape(2 * B, 64))
+    decC = decC.reshape(B, 2, H // 2, W // 2)
+    for k in range(2):
+        qt = np.tile(np.asarray(q_c)[:, k].reshape(B, 8, 8), (1, H // 16, W // 16)).astype(np.float64)
+        F[..., 8 + 2 * k] = decC[:, k] / 128.0
+        F[..., 9 + 2 * k] = qt / 64.0
+    dec = np.stack([decY, smooth_up2(decC[:, 0]), smooth_up2(decC[:, 1])])
+    return dec, F
+
+
 def project(pred, coef_img, q):
     """Per 8x8 block of pred [B][H][W]: orthonormal DCT, clamp to
     [(c - 1/2) q, (c + 1/2) q], inverse DCT (pipeline_scalar/compute_projection.rs:8-122
@@ -253,10 +286,12 @@ def _pair_grad(e):
     return g
 
 
-def forward(params, F, dec, target=None, bf=True, smooth=0.0, objective=None):
+def forward(params, F, dec, target=None, bf=True, smooth=0.0, objective=None, joint=False):
     """Activations (dict), prediction and, with a target, the loss.
     objective = (lam, coef_img, q, a_tv, a_tgv, a_p) adds the objective term
-    (and replaces the smoothness term, as the GPU does)."""
+    (and replaces the smoothness term, as the GPU does). joint: dec and
+    target are [3][B][H][W] and head outputs 4 c .. 4 c + 3 are component c's
+    2x2 full-resolution cells (the joint 4:2:0 network)."""
     rnd = bf16 if bf else (lambda a: np.asarray(a, np.float64))
     P = unpack(params)
     Wq = {k: (rnd(w), b) for k, (w, b) in P.items()}
@@ -279,8 +314,11 @@ def forward(params, F, dec, target=None, bf=True, smooth=0.0, objective=None):
     if bf:
         r = r.astype(np.float32).astype(np.float64)
     a["r"] = r
-    H, W = dec.shape[1:]
-    rf = depth_to_space(r[..., 0:4], H, W)
+    H, W = dec.shape[-2:]
+    if joint:
+        rf = np.stack([depth_to_space(r[..., 4 * c:4 * c + 4], H, W) for c in range(3)])
+    else:
+        rf = depth_to_space(r[..., 0:4], H, W)
     pred = dec + 16.0 * rf
     loss = None
     if target is not None:
@@ -296,20 +334,26 @@ def forward(params, F, dec, target=None, bf=True, smooth=0.0, objective=None):
     return a, pred, loss, Wq
 
 
-def gradients(params, F, dec, target, bf=True, smooth=0.0, objective=None):
+def gradients(params, F, dec, target, bf=True, smooth=0.0, objective=None, joint=False):
     """Loss and d loss / d params (flat, same layout as params)."""
     rnd = bf16 if bf else (lambda v: np.asarray(v, np.float64))
-    a, _, loss, Wq = forward(params, F, dec, target, bf, smooth, objective)
+    a, _, loss, Wq = forward(params, F, dec, target, bf, smooth, objective, joint)
     npix = dec.size
     mask = lambda g, act: g * (act > 0)
     dr = np.zeros(a["r"].shape)
-    if objective is not None:
-        dlde = (2.0 * a["e"] + a["obj_grad"]) / npix
+    if joint:
+        for c in range(3):
+            dr[..., 4 * c:4 * c + 4] = space_to_depth(2.0 * a["e"][c] / npix, *a["r"].shape[1:3])
+        if bf:
+            dr[..., 0:12] = bf16(dr[..., 0:12].astype(np.float32))
     else:
-        dlde = (2.0 * a["e"] + smooth * _pair_grad(a["e"])) / npix
-    dr[..., 0:4] = space_to_depth(dlde, *a["r"].shape[1:3])
-    if bf:
-        dr[..., 0:4] = bf16(dr[..., 0:4].astype(np.float32))
+        if objective is not None:
+            dlde = (2.0 * a["e"] + a["obj_grad"]) / npix
+        else:
+            dlde = (2.0 * a["e"] + smooth * _pair_grad(a["e"])) / npix
+        dr[..., 0:4] = space_to_depth(dlde, *a["r"].shape[1:3])
+        if bf:
+            dr[..., 0:4] = bf16(dr[..., 0:4].astype(np.float32))
     grads = {}
 
     def wb(name, x, g):

@@ -172,3 +172,44 @@ def test_objective_loss_gradient_matches_finite_differences():
         lm = O.forward(params - eps * v, F, dec, target, bf=False, objective=obj)[2]
         fd = (lp - lm) / (2 * eps)
         assert abs(fd - g @ v) <= 2e-3 * max(1.0, abs(fd)), (fd, g @ v)
+
+
+def _joint_case(seed, B=1, H=32, W=48):
+    rng = np.random.default_rng(seed)
+    params, _, _, _ = _case(seed)
+    cy = rng.integers(-20, 20, size=(B, H, W)).astype(np.int16)
+    cc = rng.integers(-20, 20, size=(B, 2, H // 2, W // 2)).astype(np.int16)
+    qy = rng.integers(2, 40, size=(B, 64)).astype(np.float64)
+    qc = rng.integers(2, 40, size=(B, 2, 64)).astype(np.float64)
+    dec, F = O.features_joint(cy, qy, cc, qc)
+    target = dec + rng.standard_normal(dec.shape) * 4.0
+    return params, F, dec, target, (cy, qy, cc, qc)
+
+
+def test_joint_features_layout():
+    """Channels 8-11 carry the chroma samples and steps at the luma's level 0;
+    the chroma bases are the decoded chroma upsampled as the learned start
+    upsamples (warmstart.upsample_component, float32)."""
+    from artefact_b200.warmstart import upsample_component
+
+    _, F, dec, _, (cy, qy, cc, qc) = _joint_case(3)
+    B, H, W = cy.shape
+    decC, _ = O.features(cc.reshape(2 * B, H // 2, W // 2), qc.reshape(2 * B, 64))
+    np.testing.assert_allclose(F[0, :, :, 8], decC[0] / 128.0)
+    np.testing.assert_allclose(F[0, 5, 11, 11], qc[0, 1, 5 * 8 + 3] / 64.0)
+    assert np.all(F[..., 12:] == 0)
+    up = upsample_component(decC[1].astype(np.float32), 2, 2, H, W)
+    np.testing.assert_allclose(dec[2, 0], up, atol=1e-3)
+
+
+def test_joint_loss_gradient_matches_finite_differences():
+    params, F, dec, target, _ = _joint_case(4)
+    loss, g = O.gradients(params, F, dec, target, bf=False, joint=True)
+    rng = np.random.default_rng(10)
+    for _ in range(3):
+        v = rng.standard_normal(params.size)
+        eps = 1e-8
+        lp = O.forward(params + eps * v, F, dec, target, bf=False, joint=True)[2]
+        lm = O.forward(params - eps * v, F, dec, target, bf=False, joint=True)[2]
+        fd = (lp - lm) / (2 * eps)
+        assert abs(fd - g @ v) <= 1e-5 * max(1.0, abs(fd)), (fd, g @ v)

@@ -305,6 +305,87 @@ def test_features_and_prediction(gpu):
     np.testing.assert_allclose(pred, ref, rtol=0, atol=2e-3 * max(1.0, float(np.abs(ref - dec).max())) + 1e-3)
 
 
+def _joint_batch(seed, B=2, H=64, W=96):
+    rng = np.random.default_rng(seed)
+
+    def coefs(b, h, w):
+        c = np.zeros((b, h, w), np.int16)
+        for i in range(b):
+            blk = c[i].reshape(h // 8, 8, w // 8, 8)
+            blk[:, 0, :, 0] = rng.integers(-60, 60, size=(h // 8, w // 8))
+            blk[:, :3, :, :3] += rng.integers(-3, 4, size=(h // 8, 3, w // 8, 3)).astype(np.int16)
+        return c
+
+    cy = coefs(B, H, W)
+    cc = coefs(2 * B, H // 2, W // 2).reshape(B, 2, H // 2, W // 2)
+    qy = rng.integers(4, 40, size=(B, 64)).astype(np.float32)
+    qc = rng.integers(4, 40, size=(B, 2, 64)).astype(np.float32)
+    dec, _ = O.features_joint(cy, qy, cc, qc)
+    target = (dec + rng.standard_normal(dec.shape) * 3.0).astype(np.float32)
+    return cy, cc, qy, qc, target
+
+
+def _joint_params(seed):
+    params = WS.init_params(seed)
+    rng = np.random.default_rng(seed)
+    offs, _ = O.offsets()
+    wo, bo = offs["head"]
+    params[wo:bo] = (rng.standard_normal(bo - wo) * 0.05).astype(np.float32)
+    params[wo + 12 * 32 * 9:bo] = 0.0  # outputs 12-15 are unused by the joint network
+    return params
+
+
+def test_joint_prediction_matches_oracle(gpu):
+    """art_net_predict_joint: luma and full-resolution chroma planes against the
+    oracle's joint forward pass (bf16 storage emulated)."""
+    torch = _torch()
+    cy, cc, qy, qc, _ = _joint_batch(6)
+    params = _joint_params(6)
+    net = WS.WarmStartNet(params)
+    pred = net.predict_joint(torch.from_numpy(cy).cuda(), torch.from_numpy(cc).cuda(), _f32(qy), _f32(qc))
+    pred = pred.cpu().numpy().astype(np.float64)
+    dec, F = O.features_joint(cy, qy, cc, qc)
+    _, ref, _, _ = O.forward(params.astype(np.float64), F, dec, joint=True)
+    assert pred.shape == ref.shape
+    np.testing.assert_allclose(pred, ref, rtol=0, atol=2e-3 * max(1.0, float(np.abs(ref - dec).max())) + 1e-3)
+
+
+def test_joint_gradients_match_oracle(gpu):
+    """art_net_train_step_joint's backward pass against the oracle's FP64
+    gradient of the joint loss: per layer cosine >= 0.999, relative <= 3e-2."""
+    torch = _torch()
+    cy, cc, qy, qc, target = _joint_batch(7)
+    params = _joint_params(7)
+    net = WS.WarmStartNet(params)
+    loss = net.train_step_joint(torch.from_numpy(cy).cuda(), torch.from_numpy(cc).cuda(), _f32(qy), _f32(qc),
+                                _f32(target), lr=0.0)
+    g = net.gradients().astype(np.float64)
+    dec, F = O.features_joint(cy, qy, cc, qc)
+    ref_loss, ref = O.gradients(params.astype(np.float64), F, dec, target.astype(np.float64), joint=True)
+    assert abs(loss - ref_loss) <= 1e-3 * ref_loss, (loss, ref_loss)
+    offs, _ = O.offsets()
+    for name, cin, cout, _, _ in O.LAYERS:
+        for lo, hi in ((offs[name][0], offs[name][1]), (offs[name][1], offs[name][1] + cout)):
+            a, b = g[lo:hi], ref[lo:hi]
+            nb = float(np.linalg.norm(b))
+            if nb == 0:
+                assert float(np.abs(a).max()) == 0
+                continue
+            cos = float(a @ b) / (float(np.linalg.norm(a)) * nb)
+            rel = float(np.linalg.norm(a - b)) / nb
+            assert cos >= 0.999 and rel <= 3e-2, (name, cos, rel)
+
+
+def test_joint_geometry_is_checked(gpu):
+    torch = _torch()
+    net = WS.WarmStartNet(WS.init_params(1))
+    cy = torch.zeros((1, 40, 48), dtype=torch.int16, device="cuda")
+    cc = torch.zeros((1, 2, 20, 24), dtype=torch.int16, device="cuda")
+    q = torch.ones((1, 64), device="cuda")
+    with pytest.raises(Exception, match="multiple of 16"):
+        net.predict_joint(cy, cc, q, torch.ones((1, 2, 64), device="cuda"))
+
+
 @pytest.mark.parametrize("smooth", [0.0, 2.0])
 def test_network_gradients_match_oracle(gpu, smooth):
     """The full forward + backward on the GPU against the oracle's FP64 backward

@@ -96,7 +96,7 @@ def _prediction(net, j):
         ci = torch.from_numpy(WS.coef_image(co)[None]).cuda()
         q = torch.from_numpy(np.asarray(co.quant_table, np.float32)[None].copy()).cuda()
         p = net.predict(ci, q)[0].cpu().numpy()
-        out.append(np.repeat(np.repeat(p, co.vertical_samp_factor, 0), co.horizontal_samp_factor, 1).reshape(H, W))
+        out.append(WS.upsample_component(p, co.horizontal_samp_factor, co.vertical_samp_factor, H, W))
     return out
 
 
