@@ -182,6 +182,7 @@ EXPORTS = {
                                              C.c_int64, C.c_void_p, C.c_void_p, C.c_void_p, C.c_int32, C.c_int32,
                                              C.c_int32, C.c_float, C.POINTER(C.c_float), C.c_void_p]),
     "art_net_set_loss": (C.c_int32, [C.c_void_p, C.c_float]),
+    "art_net_set_joint_loss": (C.c_int32, [C.c_void_p, C.c_float]),
     "art_net_set_objective": (C.c_int32, [C.c_void_p, C.c_float, C.c_float, C.c_float, C.c_int32]),
     "art_net_train_step": (C.c_int32, [C.c_void_p, C.c_void_p, C.c_int32, C.c_int64, C.c_void_p, C.c_void_p,
                                        C.c_int32, C.c_int32, C.c_int32, C.c_float, C.POINTER(C.c_float),

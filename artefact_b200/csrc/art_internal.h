@@ -66,11 +66,13 @@ int32_t net_predict_async(ArtNet *net, int slot, const int16_t *coef, int cpitch
                           int B, int H, int W, float *pred, void *stream);
 // Joint 4:2:0 prediction of one image (art_net_predict_joint with B = 1):
 // luma H x W, chroma H/2 x W/2 (Cb at cc, Cr sc elements after it), tables
-// qy[64] and qc[2][64]; full-resolution planes pred[3][H][W]. Queued on
-// `stream` on activation set `slot`, as net_predict_async.
+// qy[64] and qc[2][64]; full-resolution sample (c, Y, X) written to
+// x[c cstride + Y pitch + X] and to the same place of y (the solver's two
+// state buffers). Queued on `stream` on activation set `slot`, as
+// net_predict_async.
 int32_t net_predict_joint_async(ArtNet *net, int slot, const int16_t *cy, int py, long long sy, const int16_t *cc,
-                                int pc, long long sc, const float *qy, const float *qc, int H, int W, float *pred,
-                                void *stream);
+                                int pc, long long sc, const float *qy, const float *qc, int H, int W, float *x,
+                                float *y, long long cstride, int pitch, void *stream);
 // What net_predict_joint_async of one H x W image would allocate and pack.
 int32_t net_prepare_joint(ArtNet *net, int slot, int H, int W, void *stream);
 // Allocation and weight packing that a prediction of B x H x W on activation

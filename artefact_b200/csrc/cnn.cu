@@ -980,13 +980,16 @@ __global__ void k_features_joint(const float *__restrict__ decC, const float *__
 }
 
 // Joint residual head output r (fp32 [B][H0][W0][rstride], channels 4 c + 2 dy
-// + dx = sample (2 y + dy, 2 x + dx) of component c) -> prediction
-// pred[3][B][H][W] = dec + 16 r; with a target: gradient of the mean squared
-// error over the 3 B H W samples into channels 0-11 of grad[B][H0][W0][16],
-// per-block partial sums of the squared error.
+// + dx = sample (2 y + dy, 2 x + dx) of component c) -> prediction dec + 16 r
+// of sample (c, b, Y, X) at pred[c ocs + (b H + Y) opitch + X] (and at the
+// same place of pred2 when given: the solver's two state buffers); with a
+// target [3][B][H][W]: gradient of the mean squared error over the 3 B H W
+// samples (the luma's weighted by luma_w) into channels 0-11 of
+// grad[B][H0][W0][16], per-block partial sums of the weighted squared error.
 __global__ void k_residual_joint(const float *__restrict__ r, int rstride, const float *__restrict__ dec,
-                                 const float *__restrict__ target, int B, int H, int W, float inv_count,
-                                 float *__restrict__ pred, bf16 *__restrict__ grad, float *__restrict__ loss_partial)
+                                 const float *__restrict__ target, int B, int H, int W, float inv_count, float luma_w,
+                                 float *__restrict__ pred, float *__restrict__ pred2, long long ocs, int opitch,
+                                 bf16 *__restrict__ grad, float *__restrict__ loss_partial)
 {
     __shared__ float s[256];
     const int W0 = W / 2, H0 = H / 2;
@@ -1000,14 +1003,20 @@ __global__ void k_residual_joint(const float *__restrict__ r, int rstride, const
         for (int c = 0; c < 3; c++) {
 #pragma unroll
             for (int k = 0; k < 4; k++) {
-                const size_t q = c * plane + ((size_t)b * H + 2 * y + (k >> 1)) * W + 2 * x + (k & 1);
+                const int Y = 2 * y + (k >> 1), X = 2 * x + (k & 1);
+                const size_t q = c * plane + ((size_t)b * H + Y) * W + X;
                 const float rv = r[p * rstride + 4 * c + k];
                 const float d = dec[q];
-                if (pred) pred[q] = d + 16.f * rv;
+                if (pred) {
+                    const size_t o = c * ocs + ((size_t)b * H + Y) * opitch + X;
+                    const float v = d + 16.f * rv;
+                    pred[o] = v;
+                    if (pred2) pred2[o] = v;
+                }
                 if (target) {
-                    const float e = rv - (target[q] - d) * (1.f / 16.f);
-                    acc += e * e;
-                    gv[4 * c + k] = __float2bfloat16_rn(2.f * e * inv_count);
+                    const float e = rv - (target[q] - d) * (1.f / 16.f), wc = c == 0 ? luma_w : 1.f;
+                    acc += wc * e * e;
+                    gv[4 * c + k] = __float2bfloat16_rn(2.f * wc * e * inv_count);
                 }
             }
         }
@@ -1684,6 +1693,7 @@ struct ArtNet {
     // and the objective's term weights; obj holds x, P, the five term planes
     // and the clamp masks.
     float obj_lambda = 0.f, obj_tv = 0.f, obj_tgv = 0.f, obj_p = 0.f;
+    float joint_luma_w = 1.f;  // weight of the luma's squared errors in the joint loss (art_net_set_joint_loss)
     art::cnn::Buf obj;
     bool cap_train = false;     // the gradient buffers match act[0]
 };
@@ -1994,9 +2004,11 @@ int32_t joint_features(NetActs &A, const int16_t *cy, int py, long long sy, cons
     return check_launch("k_features_joint");
 }
 
+// Prediction of B joint images: sample (c, b, Y, X) to pred[c ocs + (b H + Y)
+// opitch + X] and, when pred2 is given, to the same place of pred2.
 int32_t net_predict_joint(ArtNet *net, int slot, const int16_t *cy, int py, long long sy, const int16_t *cc, int pc,
                           long long sc, const float *qy, const float *qc, int B, int H, int W, float *pred,
-                          cudaStream_t s)
+                          float *pred2, long long ocs, int opitch, cudaStream_t s)
 {
     NET_TRY(check_joint_geometry(B, H, W));
     NET_TRY(net_alloc(net, slot, joint_px(B, H, W), joint_full(B, H, W), false));
@@ -2005,15 +2017,15 @@ int32_t net_predict_joint(ArtNet *net, int slot, const int16_t *cy, int py, long
     NET_TRY(joint_features(A, cy, py, sy, cc, pc, sc, qy, qc, B, H, W, s));
     NET_TRY(net_forward(net, A, B, H / 2, W / 2, s, false, JOINT_RSTRIDE));
     k_residual_joint<<<8 * num_sms(), 256, 0, s>>>(A.r.as<float>(), JOINT_RSTRIDE, A.dec.as<float>(), nullptr, B, H,
-                                                  W, 0.f, pred ? pred : A.pred.as<float>(), nullptr, nullptr);
+                                                  W, 0.f, 1.f, pred, pred2, ocs, opitch, nullptr, nullptr);
     return check_launch("k_residual_joint");
 }
 
 int32_t net_predict_joint_async(ArtNet *net, int slot, const int16_t *cy, int py, long long sy, const int16_t *cc,
-                                int pc, long long sc, const float *qy, const float *qc, int H, int W, float *pred,
-                                void *stream)
+                                int pc, long long sc, const float *qy, const float *qc, int H, int W, float *x,
+                                float *y, long long cstride, int pitch, void *stream)
 {
-    return net_predict_joint(net, slot, cy, py, sy, cc, pc, sc, qy, qc, 1, H, W, pred,
+    return net_predict_joint(net, slot, cy, py, sy, cc, pc, sc, qy, qc, 1, H, W, x, y, cstride, pitch,
                              static_cast<cudaStream_t>(stream));
 }
 
@@ -2139,7 +2151,7 @@ int32_t art_net_predict_joint(ArtNet *net, const int16_t *coef_y, int32_t cpitch
     cudaSetDevice(net->device);
     cudaStream_t s = static_cast<cudaStream_t>(stream);
     NET_TRY(net_predict_joint(net, 0, coef_y, cpitch_y, stride_y, coef_c, cpitch_c, stride_c, q_y, q_c, B, H, W, pred,
-                              s));
+                              nullptr, (long long)B * H * W, W, s));
     return read_err(net, s);
 }
 
@@ -2168,8 +2180,9 @@ int32_t art_net_train_step_joint(ArtNet *net, const int16_t *coef_y, int32_t cpi
     NET_TRY(net_forward(net, A, B, H0, W0, s, true, JOINT_RSTRIDE));
     const long long n = 3LL * B * H * W;
     k_residual_joint<<<LOSS_BLOCKS, 256, 0, s>>>(A.r.as<float>(), JOINT_RSTRIDE, A.dec.as<float>(), target, B, H, W,
-                                                 1.f / (float)n, A.pred.as<float>(), static_cast<bf16 *>(net->dr.p),
-                                                 net->loss_partial.as<float>());
+                                                 1.f / (float)n, net->joint_luma_w, A.pred.as<float>(), nullptr,
+                                                 (long long)B * H * W, W,
+                                                 static_cast<bf16 *>(net->dr.p), net->loss_partial.as<float>());
     NET_TRY(check_launch("k_residual_joint"));
     NET_TRY(net_backward(net, B, H0, W0, s));
     if (lr > 0.f) {
@@ -2189,6 +2202,14 @@ int32_t art_net_train_step_joint(ArtNet *net, const int16_t *coef_y, int32_t cpi
         return ART_OK;
     }
     return read_err(net, s);
+}
+
+int32_t art_net_set_joint_loss(ArtNet *net, float luma_weight)
+{
+    if (!net || !(luma_weight > 0.f) || !std::isfinite(luma_weight))
+        return fail(ART_ERR_INVALID_ARGUMENT, "net_set_joint_loss: the luma weight must be finite and > 0");
+    net->joint_luma_w = luma_weight;
+    return ART_OK;
 }
 
 int32_t art_net_set_loss(ArtNet *net, float smooth_weight)

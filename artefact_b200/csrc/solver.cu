@@ -267,15 +267,49 @@ __global__ void __launch_bounds__(SWEEP_WARPS * 32, SWEEP_MIN_BLOCKS) k_grad_swe
     }
 }
 
-// Narrow variant of the gradient sweep: the same terms with one column per lane
-// and scalar arithmetic, so more warps cover an image and small images fill
-// the GPU better. One warp per strip of SWEEP_OUT_N output columns and
-// strip_rows rows; lane L holds column xs - 2 + L. Lanes 1..30 form the
-// per-pixel terms, lanes 2..29 write g. Rows and columns outside the image are
-// read clamped (replicated edges make the reference's last-row/column forward
-// differences vanish, compute_step_tv.rs:105-120) and their terms are zero,
-// which reproduces the reference's scatter guards. Rows are prefetched two
-// ahead of use.
+// Scalar and packed-pair forms of the sweep's arithmetic: one body serves a
+// single channel (float) and a pair of channels (float2, packed FP32x2, one
+// instruction for both). Every operation rounds on its own, in the order of
+// the wide variant, so a channel's terms are the same in either form.
+__device__ __forceinline__ float vadd(float a, float b) { return __fadd_rn(a, b); }
+__device__ __forceinline__ float2 vadd(float2 a, float2 b) { return f2add(a, b); }
+__device__ __forceinline__ float vsub(float a, float b) { return __fsub_rn(a, b); }
+__device__ __forceinline__ float2 vsub(float2 a, float2 b) { return f2sub(a, b); }
+__device__ __forceinline__ float vmul(float a, float b) { return __fmul_rn(a, b); }
+__device__ __forceinline__ float2 vmul(float2 a, float2 b) { return f2mul(a, b); }
+__device__ __forceinline__ float vfma(float a, float b, float c) { return __fmaf_rn(a, b, c); }
+__device__ __forceinline__ float2 vfma(float2 a, float2 b, float2 c) { return f2fma(a, b, c); }
+__device__ __forceinline__ void vsplat(float &d, float v) { d = v; }
+__device__ __forceinline__ void vsplat(float2 &d, float v) { d = make_float2(v, v); }
+__device__ __forceinline__ float vsel(bool p, float a, float b) { return p ? a : b; }
+__device__ __forceinline__ float2 vsel(bool p, float2 a, float2 b) { return make_float2(p ? a.x : b.x, p ? a.y : b.y); }
+__device__ __forceinline__ float vup(float v) { return __shfl_up_sync(0xffffffffu, v, 1); }
+__device__ __forceinline__ float2 vup(float2 v) { return make_float2(vup(v.x), vup(v.y)); }
+__device__ __forceinline__ float vdn(float v) { return __shfl_down_sync(0xffffffffu, v, 1); }
+__device__ __forceinline__ float2 vdn(float2 v) { return make_float2(vdn(v.x), vdn(v.y)); }
+// Channel-ordered sums over the channels of a group.
+__device__ __forceinline__ float n1_acc(float n, float dx, float dy) { return __fmaf_rn(dy, dy, __fmaf_rn(dx, dx, n)); }
+__device__ __forceinline__ float n1_acc(float n, float2 dx, float2 dy) { return n1_acc(n1_acc(n, dx.x, dy.x), dx.y, dy.y); }
+__device__ __forceinline__ float h_acc(float n, float t) { return __fadd_rn(n, t); }
+__device__ __forceinline__ float h_acc(float n, float2 t) { return __fadd_rn(__fadd_rn(n, t.x), t.y); }
+
+// Narrow sweep state of one group of channels (one channel, or a packed pair).
+template <class T>
+struct NarrowGroup {
+    T yv, dxp, dyp, Gm, G0, Gp, ssq, ring[SWEEP_PF_N], pring[SWEEP_PPF_N];
+    T yn, pr, dx, dy, gxx, gyy, gs;
+};
+
+// Narrow variant of the gradient sweep: the same terms with one column per
+// lane, so more warps cover an image and small images fill the GPU better.
+// One warp per strip of SWEEP_OUT_N output columns and strip_rows rows; lane L
+// holds column xs - 2 + L. Lanes 1..30 form the per-pixel terms, lanes 2..29
+// write g. Rows and columns outside the image are read clamped (replicated
+// edges make the reference's last-row/column forward differences vanish,
+// compute_step_tv.rs:105-120) and their terms are zero, which reproduces the
+// reference's scatter guards. Rows are prefetched two ahead of use. With two
+// or three channels, two of them run as a packed pair (channel 0 alone with
+// three), which halves their arithmetic instructions.
 template <int NCH>
 __global__ void __launch_bounds__(SWEEP_WARPS_N * 32, SWEEP_MIN_BLOCKS_N) k_grad_sweep_n(const ImgDev *__restrict__ imgs,
                                                                  const int2 *__restrict__ work, float stepmul)
@@ -284,14 +318,18 @@ __global__ void __launch_bounds__(SWEEP_WARPS_N * 32, SWEEP_MIN_BLOCKS_N) k_grad
     __shared__ double s_dred[SWEEP_WARPS_N][NCH];
     __shared__ int s_last;
     const unsigned FULL = 0xffffffffu;
+    constexpr bool SOLO = NCH & 1;     // channel 0 alone
+    constexpr bool PAIR = NCH >= 2;    // channels P0, P0 + 1 packed
+    constexpr int P0 = SOLO ? 1 : 0;
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int2 wk = work[blockIdx.x];
     const ImgDev &im = imgs[wk.x];
     const int W = im.W, H = im.H, pitch = im.pitch, R = im.strip_rows;
     const int strip = wk.y * SWEEP_WARPS_N + warp;
-    float ssq[NCH];
-#pragma unroll
-    for (int c = 0; c < NCH; c++) ssq[c] = 0.f;
+    NarrowGroup<float> A;
+    NarrowGroup<float2> B;
+    vsplat(A.ssq, 0.f);
+    vsplat(B.ssq, 0.f);
 
     if (strip < im.nstrips) {
         const int sxi = strip % im.strips_x, syi = strip / im.strips_x;
@@ -319,115 +357,143 @@ __global__ void __launch_bounds__(SWEEP_WARPS_N * 32, SWEEP_MIN_BLOCKS_N) k_grad
         }
         const int Hm1 = H - 1;
         auto yrow = [&](int row) -> int { return min(max(row, 0), Hm1) * pitch; };
-
-        // Rows in flight, as in the wide variant: ring[c][k] = y row t + 1 + k,
-        // pring[c][k] = DCT-distance row t - 1 + k at step t.
-        float yv[NCH], dxp[NCH], dyp[NCH], Gm[NCH], G0[NCH], Gp[NCH], ring[NCH][SWEEP_PF_N], pring[NCH][SWEEP_PPF_N];
-        {
-            const int o0 = yrow(ys - 2), o1 = yrow(ys - 1);
+        auto ly = [&](int c, int off) -> float { return __ldg(yp + c * cs + off); };
+        auto lp = [&](int c, int row) -> float {
+            return pon[c] ? __ldg(pbase + pcol[c] + (row >> psh[c]) * ppitch[c]) : 0.f;
+        };
+        auto ld_y = [&](auto &g, int off) {
+            if constexpr (sizeof(g) == sizeof(float)) g = ly(0, off);
+            else g = make_float2(ly(P0, off), ly(P0 + 1, off));
+        };
+        auto ld_p = [&](auto &g, int row) {
+            if constexpr (sizeof(g) == sizeof(float)) g = lp(0, row);
+            else g = make_float2(lp(P0, row), lp(P0 + 1, row));
+        };
+        // Rows in flight: ring[k] = y row t + 1 + k, pring[k] = DCT-distance
+        // row t - 1 + k at step t.
+        auto init = [&](auto &G) {
+            using T = decltype(G.yv);
+            T y0;
+            ld_y(y0, yrow(ys - 2));
+            ld_y(G.yv, yrow(ys - 1));
 #pragma unroll
-            for (int c = 0; c < NCH; c++) {
-                const float y0 = __ldg(yp + c * cs + o0);
-                yv[c] = __ldg(yp + c * cs + o1);
+            for (int k = 0; k < SWEEP_PF_N; k++) ld_y(G.ring[k], yrow(ys + k));
 #pragma unroll
-                for (int k = 0; k < SWEEP_PF_N; k++) ring[c][k] = __ldg(yp + c * cs + yrow(ys + k));
-#pragma unroll
-                for (int k = 0; k < SWEEP_PPF_N; k++) {
-                    const int r = min(max(ys - 2 + k, 0), Hm1);
-                    pring[c][k] = pon[c] ? __ldg(pbase + pcol[c] + (r >> psh[c]) * ppitch[c]) : 0.f;
-                }
-                dxp[c] = __shfl_down_sync(FULL, y0, 1) - y0;
-                dyp[c] = yv[c] - y0;
-                Gm[c] = G0[c] = Gp[c] = 0.f;
-            }
-        }
+            for (int k = 0; k < SWEEP_PPF_N; k++) ld_p(G.pring[k], min(max(ys - 2 + k, 0), Hm1));
+            G.dxp = vsub(vdn(y0), y0);
+            G.dyp = vsub(G.yv, y0);
+            vsplat(G.Gm, 0.f);
+            vsplat(G.G0, 0.f);
+            vsplat(G.Gp, 0.f);
+        };
+        if constexpr (SOLO) init(A);
+        if constexpr (PAIR) init(B);
 #pragma unroll 2
         for (int t = ys - 1; t <= ys + R; t++) {
-            float yn[NCH], pr[NCH];
-            {
-                const int o = min(t + 1 + SWEEP_PF_N, Hm1) * pitch;
-                const int pr1 = min(max(t - 1 + SWEEP_PPF_N, 0), Hm1);
+            const int o = min(t + 1 + SWEEP_PF_N, Hm1) * pitch;
+            const int pr1 = min(max(t - 1 + SWEEP_PPF_N, 0), Hm1);
+            auto load = [&](auto &G) {
+                G.yn = G.ring[0];
 #pragma unroll
-                for (int c = 0; c < NCH; c++) {
-                    yn[c] = ring[c][0];
+                for (int k = 0; k + 1 < SWEEP_PF_N; k++) G.ring[k] = G.ring[k + 1];
+                ld_y(G.ring[SWEEP_PF_N - 1], o);
+                G.pr = G.pring[0];
 #pragma unroll
-                    for (int k = 0; k + 1 < SWEEP_PF_N; k++) ring[c][k] = ring[c][k + 1];
-                    ring[c][SWEEP_PF_N - 1] = __ldg(yp + c * cs + o);
-                    pr[c] = pring[c][0];
-#pragma unroll
-                    for (int k = 0; k + 1 < SWEEP_PPF_N; k++) pring[c][k] = pring[c][k + 1];
-                    pring[c][SWEEP_PPF_N - 1] = pon[c] ? __ldg(pbase + pcol[c] + (pr1 >> psh[c]) * ppitch[c]) : 0.f;
-                }
-            }
+                for (int k = 0; k + 1 < SWEEP_PPF_N; k++) G.pring[k] = G.pring[k + 1];
+                ld_p(G.pring[SWEEP_PPF_N - 1], pr1);
+            };
+            if constexpr (SOLO) load(A);
+            if constexpr (PAIR) load(B);
             const bool inside = colin && t >= 0 && t < H;
-            float dx[NCH], dy[NCH], gxx[NCH], gyy[NCH], gs[NCH];
             float n1 = 0.f, n2 = 0.f;
-#pragma unroll
-            for (int c = 0; c < NCH; c++) {
-                dx[c] = __shfl_down_sync(FULL, yv[c], 1) - yv[c];
-                dy[c] = yn[c] - yv[c];
-                n1 += dx[c] * dx[c];
-                n1 += dy[c] * dy[c];
-            }
+            auto first = [&](auto &G) {
+                G.dx = vsub(vdn(G.yv), G.yv);
+                G.dy = vsub(G.yn, G.yv);
+                n1 = n1_acc(n1, G.dx, G.dy);
+            };
+            if constexpr (SOLO) first(A);
+            if constexpr (PAIR) first(B);
             const bool tx0 = gx > 0, ty0 = t > 0;
-#pragma unroll
-            for (int c = 0; c < NCH; c++) {
+            auto second = [&](auto &G) {
+                using T = decltype(G.yv);
                 // At the left edge and the top row the backward differences are
                 // zero (compute_step_tv2.rs:53-69): take the neighbour equal to self.
-                const float dxs = __shfl_up_sync(FULL, dx[c], 1), dys = __shfl_up_sync(FULL, dy[c], 1);
-                const float dxl = tx0 ? dxs : dx[c], dyl = tx0 ? dys : dy[c];
-                const float dxu = ty0 ? dxp[c] : dx[c], dyu = ty0 ? dyp[c] : dy[c];
-                const float axx = dx[c] - dxl, ayx = dy[c] - dyl;
-                const float ayy = dy[c] - dyu, axy = dx[c] - dxu;
-                const float s = 0.5f * (axy + ayx);
-                n2 += ayy * ayy + (2.f * (s * s) + axx * axx);
-                gxx[c] = axx;
-                gyy[c] = ayy;
-                gs[c] = s;
-            }
+                const T dxl = vsel(tx0, vup(G.dx), G.dx), dyl = vsel(tx0, vup(G.dy), G.dy);
+                const T dxu = vsel(ty0, G.dxp, G.dx), dyu = vsel(ty0, G.dyp, G.dy);
+                const T axx = vsub(G.dx, dxl), ayx = vsub(G.dy, dyl);
+                const T ayy = vsub(G.dy, dyu), axy = vsub(G.dx, dxu);
+                T half, two;
+                vsplat(half, 0.5f);
+                vsplat(two, 2.f);
+                const T sv = vmul(half, vadd(axy, ayx));
+                n2 = h_acc(n2, vfma(ayy, ayy, vfma(two, vmul(sv, sv), vmul(axx, axx))));
+                G.gxx = axx;
+                G.gyy = ayy;
+                G.gs = sv;
+            };
+            if constexpr (SOLO) second(A);
+            if constexpr (PAIR) second(B);
             const float inv1 = (inside && n1 > 0.f) ? rsqrtf(n1) : 0.f;
             const float inv2 = (inside && n2 > 0.f) ? rsqrtf(n2) : 0.f;
-            const float at1 = at * inv1, ag2 = ag * inv2;
-#pragma unroll
-            for (int c = 0; c < NCH; c++) {
-                const float a = at1 * dx[c], b = at1 * dy[c];
-                const float u = ag2 * (gs[c] + gxx[c]);
-                const float v = ag2 * (gyy[c] + gs[c]);
-                const float w = ag2 * gs[c];
-                const float aul = __shfl_up_sync(FULL, a + u, 1);
-                const float ur = __shfl_down_sync(FULL, u, 1);
-                const float wr = __shfl_down_sync(FULL, w, 1);
-                const float wl = __shfl_up_sync(FULL, w, 1);
-                G0[c] += (-(a + b) - 2.f * (u + v - w)) + (aul + ur);
-                Gp[c] += (b + v) - wr;
-                Gm[c] += v - wl;
-                dxp[c] = dx[c];
-                dyp[c] = dy[c];
-                yv[c] = yn[c];
-            }
+            const float at1 = __fmul_rn(at, inv1), ag2 = __fmul_rn(ag, inv2);
+            auto third = [&](auto &G) {
+                using T = decltype(G.yv);
+                T at1v, ag2v, two;
+                vsplat(at1v, at1);
+                vsplat(ag2v, ag2);
+                vsplat(two, 2.f);
+                const T a = vmul(at1v, G.dx), b = vmul(at1v, G.dy);
+                const T u = vmul(ag2v, vadd(G.gs, G.gxx));
+                const T v = vmul(ag2v, vadd(G.gyy, G.gs));
+                const T w = vmul(ag2v, G.gs);
+                const T au = vadd(a, u);
+                const T aul = vup(au), ur = vdn(u), wr = vdn(w), wl = vup(w);
+                // centre term -(a + b) - 2 (u + v - w), then the neighbours' a + u and u
+                const T cen = vfma(two, vsub(vadd(u, v), w), vadd(a, b));
+                G.G0 = vadd(vsub(G.G0, cen), vadd(aul, ur));
+                G.Gp = vadd(G.Gp, vsub(vadd(b, v), wr));
+                G.Gm = vadd(G.Gm, vsub(v, wl));
+                G.dxp = G.dx;
+                G.dyp = G.dy;
+                G.yv = G.yn;
+            };
+            if constexpr (SOLO) third(A);
+            if constexpr (PAIR) third(B);
             const int ro = t - 1;
             if (outlane && ro >= ys && ro < ys + R && ro < H) {
                 const int go = ro * pitch;
-#pragma unroll
-                for (int c = 0; c < NCH; c++) {
-                    const float gv = Gm[c] + pr[c];
-                    gout[c * cs + go] = gv;
-                    ssq[c] = fmaf(gv, gv, ssq[c]);
+                if constexpr (SOLO) {
+                    const float gv = vadd(A.Gm, A.pr);
+                    gout[go] = gv;
+                    A.ssq = vfma(gv, gv, A.ssq);
+                }
+                if constexpr (PAIR) {
+                    const float2 gv = vadd(B.Gm, B.pr);
+                    gout[P0 * cs + go] = gv.x;
+                    gout[(P0 + 1) * cs + go] = gv.y;
+                    B.ssq = vfma(gv, gv, B.ssq);
                 }
             }
-#pragma unroll
-            for (int c = 0; c < NCH; c++) {
-                Gm[c] = G0[c];
-                G0[c] = Gp[c];
-                Gp[c] = 0.f;
-            }
+            auto rotate = [&](auto &G) {
+                G.Gm = G.G0;
+                G.G0 = G.Gp;
+                vsplat(G.Gp, 0.f);
+            };
+            if constexpr (SOLO) rotate(A);
+            if constexpr (PAIR) rotate(B);
         }
+    }
+    float ssq_c[NCH];
+    if constexpr (SOLO) ssq_c[0] = A.ssq;
+    if constexpr (PAIR) {
+        ssq_c[P0] = B.ssq.x;
+        ssq_c[P0 + 1] = B.ssq.y;
     }
 
     // Fixed-order reduction: warp tree, then warps in order, then blocks in order.
 #pragma unroll
     for (int c = 0; c < NCH; c++) {
-        float s = ssq[c];
+        float s = ssq_c[c];
 #pragma unroll
         for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(FULL, s, o);
         if (lane == 0) s_red[warp][c] = s;
@@ -1154,20 +1220,6 @@ __global__ void k_upsample(const float *__restrict__ img, const ImgDev *__restri
     im.y[off] = v;
 }
 
-// A full-resolution plane (dense rows of W) into both state buffers of
-// channel c (the joint learned start).
-__global__ void k_place(const float *__restrict__ img, const ImgDev *__restrict__ imgs, int c)
-{
-    const ImgDev &im = imgs[0];
-    const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= (long long)im.W * im.H) return;
-    const int y = (int)(i / im.W), x = (int)(i % im.W);
-    const float v = img[i];
-    const long long off = c * im.cstride + (long long)y * im.pitch + x;
-    im.x[off] = v;
-    im.y[off] = v;
-}
-
 // Smooth upsampling of a component image to both state buffers (the learned
 // start). Along each subsampled axis, full-resolution sample 2 i + d of cell i
 // takes 3/4 of cell i and 1/4 of its neighbour on that side (cell i - 1 for
@@ -1862,7 +1914,6 @@ static int prepare_batch(ArtContext *ctx, const std::vector<ImageSpec> &specs, u
             const ImageSpec &sp = specs[i];
             size_t img = 0;
             for (uint32_t c = 0; c < sp.nch; c++) img += (size_t)sp.ch[c].rounded_px_w * sp.ch[c].rounded_px_h;
-            if (joint_ok(i)) img = 3 * (size_t)sp.W * sp.H;
             need = std::max(need, img);
         }
         if ((rc = ctx->pred.ensure(need * sizeof(float)))) return rc;
@@ -1939,15 +1990,12 @@ static int prepare_batch(ArtContext *ctx, const std::vector<ImageSpec> &specs, u
                 const ImgDev &d = ctx->h_desc[gr.i];
                 const ChanDev &cd = d.ch[gr.c];
                 float *gp = pred + gr.poff;
-                const int blocks = (int)(((long long)d.W * d.H + 255) / 256);
                 if (gr.joint) {
                     const int r = cnn::net_predict_joint_async(ctx->net_joint, slot, cd.coef, cd.cpitch, 0,
                                                                d.ch[1].coef, d.ch[1].cpitch, gr.stride,
                                                                &ddesc[gr.i].q[0][0], &ddesc[gr.i].q[1][0], d.H, d.W,
-                                                               gp, gs);
+                                                               d.x, d.y, d.cstride, d.pitch, gs);
                     if (r) return r;
-                    for (int c = 0; c < 3; c++)
-                        k_place<<<blocks, 256, 0, gs>>>(gp + (size_t)c * d.W * d.H, ddesc + gr.i, c);
                     continue;
                 }
                 const int r = cnn::net_predict_async(ctx->net, slot, cd.coef, cd.cpitch, gr.stride,

@@ -280,6 +280,8 @@ def main(argv=None):
     ap.add_argument("--joint", action="store_true",
                     help="train the joint 4:2:0 network (all three components in one pass, full-resolution chroma) "
                          "on 4:2:0 crops")
+    ap.add_argument("--luma-weight", type=float, default=1.0,
+                    help="joint network: weight of the luma's squared errors against the chroma's")
     ap.add_argument("--objective", type=float, default=0.0,
                     help="weight of the loss's objective term (the solver's objective of the projected "
                          "prediction, per sample); 0 = off")
@@ -294,6 +296,7 @@ def main(argv=None):
     ctx = Context(0)
     net = WS.WarmStartNet(WS.load_params(args.init) if args.init else WS.init_params(args.seed))
     if args.joint:
+        net.set_joint_loss(args.luma_weight)
         t0 = time.time()
         data = build_joint_pools(args.crops, SEED0, ctx, log=log)
         val = build_joint_pools(args.val, SEED0 + 10_000_000, ctx, log=log)

@@ -31,6 +31,9 @@ from . import _native as N
 
 MAGIC = b"ARTWS001"
 DEFAULT_WEIGHTS = Path(__file__).resolve().parent / "weights" / "warmstart.bin"
+# The joint 4:2:0 network (same architecture and file format, trained with
+# art_net_train_step_joint): used for 4:2:0 images when present.
+DEFAULT_JOINT_WEIGHTS = Path(__file__).resolve().parent / "weights" / "warmstart_joint420.bin"
 LAYERS = [("e1", 16, 32), ("e2", 32, 64), ("e3", 64, 96), ("e4", 96, 128), ("d3", 224, 96), ("d2", 160, 64),
           ("d1", 96, 32), ("head", 32, 16)]
 
@@ -172,6 +175,11 @@ class WarmStartNet:
         """Training loss = MSE + smooth_weight * mean squared difference of the
         error between adjacent samples (art_net_set_loss; 0 = plain MSE)."""
         N.check(N.lib().art_net_set_loss(self._h, float(smooth_weight)))
+
+    def set_joint_loss(self, luma_weight: float) -> None:
+        """Weight of the luma's squared errors in the joint 4:2:0 loss
+        (art_net_set_joint_loss; default 1)."""
+        N.check(N.lib().art_net_set_joint_loss(self._h, float(luma_weight)))
 
     def set_objective(self, lam: float, weight: float = 0.3, pweight: float = 0.001, nch: int = 3) -> None:
         """Training loss += lam / n * the solver's objective of the projected

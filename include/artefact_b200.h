@@ -474,12 +474,16 @@ int32_t art_net_predict_joint(ArtNet *net, const int16_t *coef_y, int32_t cpitch
                               const int16_t *coef_c, int32_t cpitch_c, int64_t stride_c, const float *q_y,
                               const float *q_c, int32_t B, int32_t H, int32_t W, float *pred, void *stream);
 /* One joint training step on the mean squared error (units of 16 levels) of
- * all 3 B H W samples against target[3][B][H][W] (layout of pred above). The
- * smoothness and objective terms are not used here. */
+ * all 3 B H W samples against target[3][B][H][W] (layout of pred above), the
+ * luma's weighted (art_net_set_joint_loss). The smoothness and objective terms
+ * are not used here. */
 int32_t art_net_train_step_joint(ArtNet *net, const int16_t *coef_y, int32_t cpitch_y, int64_t stride_y,
                                  const int16_t *coef_c, int32_t cpitch_c, int64_t stride_c, const float *q_y,
                                  const float *q_c, const float *target, int32_t B, int32_t H, int32_t W, float lr,
                                  float *loss, void *stream);
+/* Weight of the luma's squared errors in the joint training loss (default 1;
+ * the chroma's weigh 1): loss = (luma_weight sum e_Y^2 + sum e_C^2) / (3 B H W). */
+int32_t art_net_set_joint_loss(ArtNet *net, float luma_weight);
 /* Training loss: mean squared error (in units of 16 levels) plus
  * smooth_weight times the mean over samples of the squared differences of the
  * error between horizontally and vertically adjacent samples (0, the default,
