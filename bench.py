@@ -85,8 +85,9 @@ WORKLOADS["network"] = dict(
     metric="TFLOP/s (warm-start network forward, 1080p 4:2:0)", iterations=0)
 LEARNED_QUALITIES = (30, 50, 75)
 REFINE_ITERATIONS = 8
-REFINE_STEP_ITERATIONS = 4         # first refinement phase (more than 12 iterations): steps of a 4-iteration run
-REFINE_TAIL = 2                    # last two iterations: FISTA restarted ...
+REFINE_STEP_ITERATIONS = 1         # first refinement phase: steps of a 1-iteration run ...
+REFINE_STEP_DECAY = 0.9            # ... shrinking by this factor every iteration
+REFINE_TAIL = 2                    # runs of at most 12: the last two iterations restart FISTA ...
 REFINE_TAIL_STEP_ITERATIONS = 100  # ... with steps of a 100-iteration run
 WEIGHT, PWEIGHT = 0.3, 0.001
 
@@ -320,26 +321,28 @@ class DeviceImage:
         self.outs = [torch.empty(self.H, self.pitch, device="cuda") for _ in range(self.n)]
         self.ptrs = (C.c_void_p * self.n)(*[o.data_ptr() for o in self.outs])
 
-    def solve(self, lib, ctx, iterations, init_mode, step_iterations, stream, tail=0, tail_step=0):
+    def solve(self, lib, ctx, iterations, init_mode, step_iterations, stream, tail=0, tail_step=0, decay=0.0):
         from artefact_b200 import _native as N
 
         opts = N.ArtOptions()
         opts.init_mode, opts.device, opts.step_iterations = init_mode, -1, step_iterations
-        opts.tail_iterations, opts.tail_step_iterations = tail, tail_step
+        opts.tail_iterations, opts.tail_step_iterations, opts.step_decay = tail, tail_step, decay
         pw = (C.c_float * 3)(PWEIGHT, PWEIGHT, PWEIGHT)
         N.check(lib.art_context_compute_device(ctx, self.n, self.ch, WEIGHT, pw, iterations, self.W, self.H,
                                                self.ptrs, self.pitch, C.byref(opts), C.c_void_p(stream.cuda_stream)))
 
 
 def refine_schedule(k):
-    """Refinement after a learned start: k plain iterations, the first k - 2
-    with the step of a short run (large: they remove the prediction's error;
-    2 iterations' worth for k <= 12, REFINE_STEP_ITERATIONS for more), the last
-    2 restarted with the step of a REFINE_TAIL_STEP_ITERATIONS-iteration run
-    (small: they settle). Chosen on a grid over the first step (1-4
-    iterations' worth), the tail length (2-6) and the tail step (50-200) on the
-    three 1080p images."""
-    return dict(step=2 if k <= 12 else REFINE_STEP_ITERATIONS, tail=min(REFINE_TAIL, k - 1),
+    """Refinement after a learned start: k plain iterations whose step starts
+    at that of a REFINE_STEP_ITERATIONS-iteration run and shrinks by
+    REFINE_STEP_DECAY every iteration (large steps remove the prediction's
+    error, the shrinking lets the iterate settle); runs of at most 12 end with
+    REFINE_TAIL iterations restarted with the step of a
+    REFINE_TAIL_STEP_ITERATIONS-iteration run. Chosen on a grid over the
+    1080p evaluation images and six held-out ones (first-phase step of a 1-8
+    iteration run, decay 0, 0.8 or 0.9, tails of 0 or 2 iterations at 100- or
+    300-iteration steps)."""
+    return dict(step=REFINE_STEP_ITERATIONS, decay=REFINE_STEP_DECAY, tail=min(REFINE_TAIL, k - 1) if k <= 12 else 0,
                 tail_step=REFINE_TAIL_STEP_ITERATIONS)
 
 
@@ -368,6 +371,9 @@ def learned_comparison(lib, device, steps, warmup, refine=REFINE_ITERATIONS, qua
     ctx = C.c_void_p()
     N.check(lib.art_context_create(device, C.byref(ctx)))
     N.check(lib.art_context_set_warm_start(ctx, net.handle))
+    joint = WS.WarmStartNet.load(WS.DEFAULT_JOINT_WEIGHTS, device) if WS.DEFAULT_JOINT_WEIGHTS.exists() else None
+    if joint is not None:
+        N.check(lib.art_context_set_joint_warm_start(ctx, joint.handle))
     stream = torch.cuda.current_stream()
     flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")
 
@@ -380,7 +386,7 @@ def learned_comparison(lib, device, steps, warmup, refine=REFINE_ITERATIONS, qua
         if sched is None:
             img.solve(lib, ctx, its, mode, 0, stream)
         else:
-            img.solve(lib, ctx, its, mode, sched["step"], stream, sched["tail"], sched["tail_step"])
+            img.solve(lib, ctx, its, mode, sched["step"], stream, sched["tail"], sched["tail_step"], sched["decay"])
 
     def timed(img, its, mode, sched):
         for _ in range(warmup):
@@ -446,11 +452,16 @@ def learned_comparison(lib, device, steps, warmup, refine=REFINE_ITERATIONS, qua
             f"E {(el - e50) / e50:+.2e} (decoded start, same schedule {(ed - e50) / e50:+.2e}); "
             f"reaches at K={kmin} in {kmin_ms} ms")
     lib.art_context_set_warm_start(ctx, None)
+    lib.art_context_set_joint_warm_start(ctx, None)
     lib.art_context_destroy(ctx)
     net.close()
+    if joint is not None:
+        joint.close()
     mp_total = sum(j.real_px_w * j.real_px_h / 1e6 for _, j in images)
     reach = all(r["min_refine_to_reach"] for r in rows)
     return dict(refine_iterations=refine, schedule=refine_schedule(refine), images=rows,
+                network=("joint 4:2:0 (one pass, all three components at full resolution)" if joint is not None
+                         else "per component"),
                 plain50_mpix_s=mp_total / sum(r["plain50_ms"] for r in rows) * 1e3,
                 learned_mpix_s=mp_total / sum(r["learned_ms"] for r in rows) * 1e3,
                 all_reach_plain50=all(r["reaches_plain50"] for r in rows),
@@ -1114,10 +1125,10 @@ def main():
     learned = None
     if args.workload == "1080p" and world == 1 and not args.no_learned:
         res = learned_comparison(lib, local, min(args.steps, 10), args.warmup,
-                                 ladder=(8, 10, 12, 14, 16, 20, 24, 28, 32, 40, 48))
+                                 ladder=(8, 10, 12, 14, 16, 18, 20, 24, 28, 32, 40, 48))
         if res is not None:
             rows = res["images"]
-            learned = {"workload": WORKLOADS["learned"]["name"], "schedule": res["schedule"],
+            learned = {"workload": WORKLOADS["learned"]["name"], "network": res["network"], "schedule": res["schedule"],
                        "refine_iterations": res["refine_iterations"], "plain50_mpix_s": res["plain50_mpix_s"],
                        "mpix_s": res["learned_mpix_s"], "speedup_vs_plain50": res["learned_mpix_s"] / res["plain50_mpix_s"],
                        "max_E_rel_to_plain50": max(r["E_learned_rel"] for r in rows),

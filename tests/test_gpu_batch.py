@@ -130,6 +130,35 @@ def test_every_tuning_candidate_agrees(gpu, monkeypatch, shape):
     assert all(np.array_equal(x, y) for o in outs[1:] for x, y in zip(o, outs[0]))
 
 
+def test_joint_learned_batch_matches_single_learned_solves(gpu):
+    """With both networks attached, a batch mixing 4:2:0 images (joint pass)
+    and other samplings (per component) equals each image's learned solve
+    alone."""
+    from artefact_b200 import _native as N
+    from artefact_b200 import warmstart as WS
+
+    shapes = [(96, 64, 75, "4:2:0", False), (40, 24, 50, "4:4:4", True), (160, 96, 30, "4:2:0", False),
+              (64, 48, 60, "4:2:2", False), (96, 64, 40, "4:2:0", False)]
+    jpegs = [_jpeg(*s, seed=720 + i) for i, s in enumerate(shapes)]
+    jobs = [dict(coefs=j.coefs, weight=0.3, pweight=[0.001] * 3) for j in jpegs]
+    net = WS.WarmStartNet.load() if WS.DEFAULT_WEIGHTS.exists() else WS.WarmStartNet(WS.init_params(2))
+    joint = (WS.WarmStartNet.load(WS.DEFAULT_JOINT_WEIGHTS) if WS.DEFAULT_JOINT_WEIGHTS.exists()
+             else WS.WarmStartNet(WS.init_params(3)))
+    sched = dict(step_iterations=1, step_decay=0.9, tail_iterations=2, tail_step_iterations=100)
+    with Context(0) as ctx:
+        ctx.set_warm_start(net)
+        ctx.set_joint_warm_start(joint)
+        batch = ctx.compute_batch(jobs, 8, init_mode=N.ART_INIT_LEARNED, **sched)
+        for j, got in zip(jpegs, batch):
+            W, H, _ = j.max_rounded()
+            single = ctx.compute(j.nchannel, j.coefs, 0.3, [0.001] * 3, 8, W, H, init_mode=N.ART_INIT_LEARNED, **sched)
+            d = max(float(np.abs(a - b).max()) for a, b in zip(got, single))
+            assert d <= 1e-2, (j.real_px_w, j.real_px_h, d)
+            assert O.feasibility(j.nchannel, j.coefs, W, H, got) <= 1e-3
+        ctx.set_joint_warm_start(None)
+        ctx.set_warm_start(None)
+
+
 def test_learned_batch_matches_single_learned_solves(gpu):
     """The learned start in a batch (each image's components through the
     network, the chroma pair as one batch) equals the learned start of each

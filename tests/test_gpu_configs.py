@@ -84,7 +84,8 @@ def test_config4_batch_extremes(gpu):
 
 def _refine(k):
     """The bench's refinement schedule for k iterations after a learned start."""
-    return dict(step_iterations=2 if k <= 12 else 4, tail_iterations=min(2, k - 1), tail_step_iterations=100)
+    return dict(step_iterations=1, step_decay=0.9, tail_iterations=min(2, k - 1) if k <= 12 else 0,
+                tail_step_iterations=100)
 
 
 def _prediction(net, j):
@@ -100,17 +101,38 @@ def _prediction(net, j):
     return out
 
 
+def _joint_prediction(net, j):
+    import torch
+
+    W, H, _ = j.max_rounded()
+    cy = torch.from_numpy(WS.coef_image(j.coefs[0])[None]).cuda()
+    cc = torch.from_numpy(np.stack([WS.coef_image(co) for co in j.coefs[1:]])[None]).cuda()
+    qy = torch.from_numpy(np.asarray(j.coefs[0].quant_table, np.float32)[None].copy()).cuda()
+    qc = torch.from_numpy(np.stack([np.asarray(co.quant_table, np.float32) for co in j.coefs[1:]])[None]).cuda()
+    pred = net.predict_joint(cy, cc, qy, qc).cpu().numpy()
+    return [pred[c, 0].reshape(H, W) for c in range(3)]
+
+
 @pytest.mark.skipif(not WS.DEFAULT_WEIGHTS.exists(), reason="no trained weights in the package")
+@pytest.mark.parametrize("network", ["per-component", "joint"])
 @pytest.mark.parametrize("quality", [30, 50, 75])
-def test_config5_trained_learned_1080p(gpu, quality):
+def test_config5_trained_learned_1080p(gpu, quality, network):
+    """Config 5 with the shipped weights: the learned start (per-component
+    network, or the joint 4:2:0 network when it ships) refined with the bench's
+    schedule, against the oracle started from the same prediction, at 8
+    iterations and at the fewest that reach the plain 50-iteration objective."""
+    if network == "joint" and not WS.DEFAULT_JOINT_WEIGHTS.exists():
+        pytest.skip("no joint 4:2:0 weights in the package")
     j = _jpeg(synth.make_jpeg(1920, 1080, quality, "4:2:0", False, seed=5000 + quality))
     W, H, _ = j.max_rounded()
-    net = WS.WarmStartNet.load()
+    net = WS.WarmStartNet.load() if network == "per-component" else WS.WarmStartNet.load(WS.DEFAULT_JOINT_WEIGHTS)
+    attach = (lambda c, n: c.set_warm_start(n)) if network == "per-component" else \
+        (lambda c, n: c.set_joint_warm_start(n))
     ctx = Context(0)
     try:
         ctx.compute(3, j.coefs, WEIGHT, PW, 50, W, H)
         e50 = ctx.evaluate()["E"]
-        ctx.set_warm_start(net)
+        attach(ctx, net)
         reach = None
         for k in (8, 12, 16, 20, 24, 28, 32, 40, 48):
             ctx.compute(3, j.coefs, WEIGHT, PW, k, W, H, init_mode=N.ART_INIT_LEARNED, **_refine(k))
@@ -123,10 +145,10 @@ def test_config5_trained_learned_1080p(gpu, quality):
         for k in sorted({8, reach}):
             runs[k] = ctx.compute(3, j.coefs, WEIGHT, PW, k, W, H, init_mode=N.ART_INIT_LEARNED, **_refine(k))
             runs[k] = (runs[k], ctx.evaluate())
-        ctx.set_warm_start(None)
-        start = _prediction(net, j)
+        attach(ctx, None)
+        start = _prediction(net, j) if network == "per-component" else _joint_prediction(net, j)
     finally:
-        ctx.set_warm_start(None)
+        attach(ctx, None)
         ctx.close()
         net.close()
 
@@ -134,7 +156,8 @@ def test_config5_trained_learned_1080p(gpu, quality):
         k, fp64 = job
         s = _refine(k)
         return job, O.compute_from(3, j.coefs, WEIGHT, PW, k, W, H, start, s["step_iterations"], fp64=fp64,
-                                   tail_iterations=s["tail_iterations"], tail_step_iterations=s["tail_step_iterations"])
+                                   tail_iterations=s["tail_iterations"], tail_step_iterations=s["tail_step_iterations"],
+                                   step_decay=s["step_decay"])
 
     with ThreadPoolExecutor(max_workers=4) as ex:
         refs = dict(ex.map(oracle, [(k, fp64) for k in runs for fp64 in (False, True)]))

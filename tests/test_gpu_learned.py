@@ -149,6 +149,73 @@ def test_step_decay_matches_oracle(gpu, ctx, shape, iterations, step_iterations,
     assert max(float(np.abs(a - b).max()) for a, b in zip(plain, ref)) > 0
 
 
+def _joint_prediction(net, j):
+    """The joint network's full-resolution planes of a 4:2:0 image, as the
+    solver places them."""
+    import torch
+
+    W, H, _ = j.max_rounded()
+    cy = torch.from_numpy(WS.coef_image(j.coefs[0])[None]).cuda()
+    cc = torch.from_numpy(np.stack([WS.coef_image(co) for co in j.coefs[1:]])[None]).cuda()
+    qy = torch.from_numpy(np.asarray(j.coefs[0].quant_table, np.float32)[None].copy()).cuda()
+    qc = torch.from_numpy(np.stack([np.asarray(co.quant_table, np.float32) for co in j.coefs[1:]])[None]).cuda()
+    pred = net.predict_joint(cy, cc, qy, qc).cpu().numpy()
+    return [pred[c, 0].reshape(H, W) for c in range(3)]
+
+
+def _joint_strong_params(seed):
+    p = _strong_params(seed)
+    rng = np.random.default_rng(seed + 1)
+    o = 0
+    for name, cin, cout in WS.LAYERS:
+        if name == "head":
+            p[o + 4 * 9 * 32:o + 12 * 9 * 32] = (rng.standard_normal(8 * 9 * 32) * 0.05).astype(np.float32)
+        o += cout * 9 * cin + cout
+    return p
+
+
+@pytest.mark.parametrize("shape", [(96, 64, 75, "4:2:0", False), (200, 136, 30, "4:2:0", False)])
+@pytest.mark.parametrize("iterations,step_iterations,tail,tail_step", [(0, 0, 0, 0), (8, 2, 2, 100)])
+def test_joint_learned_start_matches_oracle(gpu, ctx, shape, iterations, step_iterations, tail, tail_step):
+    """A 4:2:0 image with a joint network attached: the solver's learned start
+    and refinement against the oracle started from the joint prediction."""
+    j = jpeg_of(*shape)
+    W, H, _ = j.max_rounded()
+    n = j.nchannel
+    net = WS.WarmStartNet(_joint_strong_params(8))
+    ctx.set_joint_warm_start(net)
+    try:
+        got = ctx.compute(n, j.coefs, WEIGHT, PW, iterations, W, H, init_mode=N.ART_INIT_LEARNED,
+                          step_iterations=step_iterations, tail_iterations=tail, tail_step_iterations=tail_step)
+        ev = ctx.evaluate()
+    finally:
+        ctx.set_joint_warm_start(None)
+    start = _joint_prediction(net, j)
+    ref = O.compute_from(n, j.coefs, WEIGHT, PW, iterations, W, H, start, step_iterations, tail_iterations=tail,
+                         tail_step_iterations=tail_step)
+    d = max(float(np.abs(a.astype(np.float64) - b).max()) for a, b in zip(got, ref))
+    er = O.objective(n, j.coefs, WEIGHT, PW, W, H, ref)
+    moved = max(float(np.abs(s.ravel() - a).max()) for s, a in zip(start, ref))
+    print(f"{shape} it={iterations}: max|gpu-oracle| {d:.3g}, start moved by {moved:.3g}")
+    assert d <= 1.0
+    assert abs(ev["E"] - er) <= 1e-4 * abs(er)
+    assert ev["infeasibility"] <= 1e-3
+
+
+def test_joint_network_needs_per_component_network_for_other_samplings(gpu, ctx):
+    """A joint network alone serves 4:2:0 images only; a 4:4:4 learned solve
+    then asks for the per-component network."""
+    j = jpeg_of(48, 32, 30, "4:4:4", False)
+    W, H, _ = j.max_rounded()
+    net = WS.WarmStartNet(_joint_strong_params(9))
+    ctx.set_joint_warm_start(net)
+    try:
+        with pytest.raises(N.ArtError, match="not 4:2:0"):
+            ctx.compute(j.nchannel, j.coefs, WEIGHT, PW, 2, W, H, init_mode=N.ART_INIT_LEARNED)
+    finally:
+        ctx.set_joint_warm_start(None)
+
+
 def test_step_decay_is_validated(gpu, ctx):
     j = jpeg_of(*CASES[0])
     W, H, _ = j.max_rounded()
