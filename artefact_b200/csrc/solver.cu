@@ -15,6 +15,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <type_traits>
 #include <cmath>
 #include <cstdio>
 #include <cstring>
@@ -127,6 +128,10 @@ __global__ void __launch_bounds__(SWEEP_WARPS * 32, SWEEP_MIN_BLOCKS) k_grad_swe
                 Gm[c] = G0[c] = Gp[c] = make_float2(0.f, 0.f);
             }
         }
+        // The row loop in two forms, as in the narrow variant: EDGE keeps the
+        // image-edge rules, interior strips run without them.
+        auto rows = [&](auto edge_tag) {
+        constexpr bool EDGE = decltype(edge_tag)::value;
         for (int t = ys - 1; t <= ys + R; t++) {
             float2 yn[NCH], pr[NCH];
             {
@@ -144,7 +149,7 @@ __global__ void __launch_bounds__(SWEEP_WARPS * 32, SWEEP_MIN_BLOCKS) k_grad_swe
                     pring[c][SWEEP_PPF - 1] = pld(c, prow);
                 }
             }
-            const bool rowin = t >= 0 && t < H, ty0 = t > 0;
+            const bool rowin = !EDGE || (t >= 0 && t < H), ty0 = !EDGE || t > 0;
             float2 dx[NCH], dy[NCH], gxx[NCH], gyy[NCH], gs[NCH];
             float2 n1 = make_float2(0.f, 0.f), n2 = make_float2(0.f, 0.f);
 #pragma unroll
@@ -160,8 +165,8 @@ __global__ void __launch_bounds__(SWEEP_WARPS * 32, SWEEP_MIN_BLOCKS) k_grad_swe
                 // Backward differences are zero at the left edge and the top row
                 // (compute_step_tv2.rs:53-69): take the neighbour equal to self.
                 const float dxs = __shfl_up_sync(FULL, dx[c].y, 1), dys = __shfl_up_sync(FULL, dy[c].y, 1);
-                const float2 dxl = make_float2(lft ? dxs : dx[c].x, dx[c].x);
-                const float2 dyl = make_float2(lft ? dys : dy[c].x, dy[c].x);
+                const float2 dxl = make_float2(!EDGE || lft ? dxs : dx[c].x, dx[c].x);
+                const float2 dyl = make_float2(!EDGE || lft ? dys : dy[c].x, dy[c].x);
                 const float2 dxu = ty0 ? dxp[c] : dx[c], dyu = ty0 ? dyp[c] : dy[c];
                 const float2 axx = f2sub(dx[c], dxl), ayx = f2sub(dy[c], dyl);
                 const float2 ayy = f2sub(dy[c], dyu), axy = f2sub(dx[c], dxu);
@@ -172,10 +177,11 @@ __global__ void __launch_bounds__(SWEEP_WARPS * 32, SWEEP_MIN_BLOCKS) k_grad_swe
                 gs[c] = s;
             }
             float2 inv1, inv2;
-            inv1.x = (rowin && ina && n1.x > 0.f) ? rsqrtf(n1.x) : 0.f;
-            inv1.y = (rowin && inb && n1.y > 0.f) ? rsqrtf(n1.y) : 0.f;
-            inv2.x = (rowin && ina && n2.x > 0.f) ? rsqrtf(n2.x) : 0.f;
-            inv2.y = (rowin && inb && n2.y > 0.f) ? rsqrtf(n2.y) : 0.f;
+            const bool ia = !EDGE || (rowin && ina), ib = !EDGE || (rowin && inb);
+            inv1.x = (ia && n1.x > 0.f) ? rsqrtf(n1.x) : 0.f;
+            inv1.y = (ib && n1.y > 0.f) ? rsqrtf(n1.y) : 0.f;
+            inv2.x = (ia && n2.x > 0.f) ? rsqrtf(n2.x) : 0.f;
+            inv2.y = (ib && n2.y > 0.f) ? rsqrtf(n2.y) : 0.f;
             const float2 at1 = f2mul(at, inv1), ag2 = f2mul(ag, inv2);
 #pragma unroll
             for (int c = 0; c < NCH; c++) {
@@ -214,6 +220,15 @@ __global__ void __launch_bounds__(SWEEP_WARPS * 32, SWEEP_MIN_BLOCKS) k_grad_swe
                 Gp[c] = make_float2(0.f, 0.f);
             }
         }
+        };
+        // Interior: every lane's two columns inside the image and off its
+        // first and last columns (ca >= 1, cb <= W - 2 for all lanes), rows
+        // off the first and last.
+        const bool interior = xs - 2 >= 1 && xs + 61 <= W - 2 && ys - 1 >= 1 && ys + R + 1 + SWEEP_PF <= H - 1;
+        if (interior)
+            rows(std::false_type{});
+        else
+            rows(std::true_type{});
     }
 
     // Fixed-order reduction: warp tree, then warps in order, then blocks in order.
@@ -388,6 +403,11 @@ __global__ void __launch_bounds__(SWEEP_WARPS_N * 32, SWEEP_MIN_BLOCKS_N) k_grad
         };
         if constexpr (SOLO) init(A);
         if constexpr (PAIR) init(B);
+        // The row loop in two forms: EDGE keeps the image-edge rules; a strip
+        // whose lanes and rows all lie inside the image, away from its first
+        // and last rows and columns, runs without them (warp-uniform choice).
+        auto rows = [&](auto edge_tag) {
+        constexpr bool EDGE = decltype(edge_tag)::value;
 #pragma unroll 2
         for (int t = ys - 1; t <= ys + R; t++) {
             const int o = min(t + 1 + SWEEP_PF_N, Hm1) * pitch;
@@ -404,7 +424,7 @@ __global__ void __launch_bounds__(SWEEP_WARPS_N * 32, SWEEP_MIN_BLOCKS_N) k_grad
             };
             if constexpr (SOLO) load(A);
             if constexpr (PAIR) load(B);
-            const bool inside = colin && t >= 0 && t < H;
+            const bool inside = !EDGE || (colin && t >= 0 && t < H);
             float n1 = 0.f, n2 = 0.f;
             auto first = [&](auto &G) {
                 G.dx = vsub(vdn(G.yv), G.yv);
@@ -418,8 +438,13 @@ __global__ void __launch_bounds__(SWEEP_WARPS_N * 32, SWEEP_MIN_BLOCKS_N) k_grad
                 using T = decltype(G.yv);
                 // At the left edge and the top row the backward differences are
                 // zero (compute_step_tv2.rs:53-69): take the neighbour equal to self.
-                const T dxl = vsel(tx0, vup(G.dx), G.dx), dyl = vsel(tx0, vup(G.dy), G.dy);
-                const T dxu = vsel(ty0, G.dxp, G.dx), dyu = vsel(ty0, G.dyp, G.dy);
+                T dxl = vup(G.dx), dyl = vup(G.dy), dxu = G.dxp, dyu = G.dyp;
+                if constexpr (EDGE) {
+                    dxl = vsel(tx0, dxl, G.dx);
+                    dyl = vsel(tx0, dyl, G.dy);
+                    dxu = vsel(ty0, dxu, G.dx);
+                    dyu = vsel(ty0, dyu, G.dy);
+                }
                 const T axx = vsub(G.dx, dxl), ayx = vsub(G.dy, dyl);
                 const T ayy = vsub(G.dy, dyu), axy = vsub(G.dx, dxu);
                 T half, two;
@@ -482,6 +507,12 @@ __global__ void __launch_bounds__(SWEEP_WARPS_N * 32, SWEEP_MIN_BLOCKS_N) k_grad
             if constexpr (SOLO) rotate(A);
             if constexpr (PAIR) rotate(B);
         }
+        };
+        const bool interior = xs - 2 >= 1 && xs + 29 <= W - 1 && ys - 1 >= 1 && ys + R + 1 + SWEEP_PF_N <= H - 1;
+        if (interior)
+            rows(std::false_type{});
+        else
+            rows(std::true_type{});
     }
     float ssq_c[NCH];
     if constexpr (SOLO) ssq_c[0] = A.ssq;
