@@ -895,6 +895,11 @@ __global__ void __launch_bounds__(PW * 32) k_project(const ImgDev *__restrict__ 
     const int pitch = im.pitch;
     float *xw = im.x + c * cs, *yw = im.y + c * cs;
     const float *gb = im.g + c * cs;
+    // A zero step (sigma = 0: the projection of a start image, or a gradient
+    // of norm zero) leaves x' = y: g is then neither staged nor read, so the
+    // projection of a start needs no zeroed g plane.
+    const float sg = im.sigma[c];
+    const bool stepped = sg != 0.f;  // warp-uniform
     // Stage the region: rows of NC floats, 16-byte chunks; chunks of blocks
     // past the end of the block row are skipped.
     const int ncol = min(NC, (bw - tk.w) * 8 * SH);  // valid columns, a multiple of 8
@@ -906,7 +911,7 @@ __global__ void __launch_bounds__(PW * 32) k_project(const ImgDev *__restrict__ 
             const long long go = r0 + (long long)row * pitch + ch * 4;
             const int so = row * RS + ch * 4;
             cp_async16(sy_ + so, yw + go);
-            cp_async16(sg_ + so, gb + go);
+            if (stepped) cp_async16(sg_ + so, gb + go);
         }
     }
     // Meanwhile: coefficient row j of this lane's block and its quantisation steps.
@@ -917,7 +922,6 @@ __global__ void __launch_bounds__(PW * 32) k_project(const ImgDev *__restrict__ 
         qv[u] = __ldg(&im.q[c][j * 8 + u]);
         iq[u] = __ldg(&im.invq2[c][j * 8 + u]);
     }
-    const float sg = im.sigma[c];
     const float ap = cd.alpha_p;  // warp-uniform
     float(*T0)[9] = s_t[warp][0][grp];
     float(*T1)[9] = s_t[warp][1][grp];
@@ -936,7 +940,7 @@ __global__ void __launch_bounds__(PW * 32) k_project(const ImgDev *__restrict__ 
 #pragma unroll
             for (int sx = 0; sx < SH; sx++) {
                 const int so = (k * SV + sy) * RS + cb + sx;
-                const float v = fmaf(-sg, sg_[so], sy_[so]);
+                const float v = stepped ? fmaf(-sg, sg_[so], sy_[so]) : sy_[so];
                 sy_[so] = v;
                 acc += v;
             }
@@ -1927,8 +1931,8 @@ static int prepare_batch(ArtContext *ctx, const std::vector<ImageSpec> &specs, u
     } else if (init_mode == ART_INIT_LEARNED) {
         // Prediction per component at its own resolution, upsampled smoothly
         // to full resolution into x and y, then one projection with a zero step
-        // (g = 0, sigma = 0): x_0 = y_0 = P(prediction), and the DCT-distance
-        // plane of the projected prediction for the first gradient.
+        // (sigma = 0): x_0 = y_0 = P(prediction), and the DCT-distance plane of
+        // the projected prediction for the first gradient.
         // A 4:2:0 image (luma H x W, both chroma H/2 x W/2, H and W multiples
         // of 16) goes through the joint network when one is attached: one
         // pass predicts all three components at full resolution.
@@ -2007,8 +2011,8 @@ static int prepare_batch(ArtContext *ctx, const std::vector<ImageSpec> &specs, u
         }
         // Prediction per component at its own resolution, upsampled smoothly
         // to full resolution into x and y, then one projection with a zero step
-        // (g = 0, sigma = 0): x_0 = y_0 = P(prediction), and the DCT-distance
-        // plane of the projected prediction for the first gradient.
+        // (sigma = 0): x_0 = y_0 = P(prediction), and the DCT-distance plane of
+        // the projected prediction for the first gradient.
         auto launch_init = [&]() -> int {
             if (groups.size() > 1) {
                 ART_CUDA(cudaEventRecord(ctx->fork, s));
@@ -2040,10 +2044,8 @@ static int prepare_batch(ArtContext *ctx, const std::vector<ImageSpec> &specs, u
                 ART_CUDA(cudaEventRecord(ctx->join, ctx->side));
                 ART_CUDA(cudaStreamWaitEvent(s, ctx->join, 0));
             }
-            for (int i = 0; i < nimg; i++) {
-                const ImgDev &d = ctx->h_desc[i];
-                ART_CUDA(cudaMemsetAsync(d.g, 0, (size_t)d.nch * d.cstride * sizeof(float), s));
-            }
+            // sigma is zero (misc was cleared): the projections neither read
+            // nor need g here.
             launch_projections(ctx, 0.0f);
             ART_CUDA(cudaGetLastError());
             return ART_OK;

@@ -67,8 +67,8 @@ constexpr int SWEEP_PF = 4;       // wide sweep: y rows loaded ahead of use
 constexpr int SWEEP_PPF = 3;      // wide sweep: DCT-distance rows loaded ahead of use
 constexpr int SWEEP_OUT = 60;     // wide sweep: output columns per warp strip (32 lanes x 2 columns, 2 of halo each side)
 constexpr int SWEEP_WARPS = 4;    // wide sweep: warps (strips) per block
-constexpr int SWEEP_PF_N = 2;     // narrow sweep: y rows loaded ahead of use
-constexpr int SWEEP_PPF_N = 1;    // narrow sweep: DCT-distance rows loaded ahead of use
+constexpr int SWEEP_PF_N = 3;     // narrow sweep: y rows loaded ahead of use
+constexpr int SWEEP_PPF_N = 2;    // narrow sweep: DCT-distance rows loaded ahead of use
 constexpr int SWEEP_OUT_N = 28;   // narrow sweep: 32 lanes x 1 column, 2 of halo each side
 constexpr int SWEEP_WARPS_N = 8;  // narrow sweep: warps per block
 constexpr int SWEEP_OUT_Q = 120;  // quad sweep: output columns per warp strip (32 lanes x 4 columns, 4 of halo each side)

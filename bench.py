@@ -642,10 +642,11 @@ def network_flops(H, W):
     return 2 * macs
 
 
-def time_network(device, steps, warmup):
-    """The network's forward pass on one 1080p 4:2:0 image (luma 1920x1088,
-    then both chroma planes of 960x544 as a batch of two), CUDA events:
-    (ms, TFLOP/s)."""
+def time_network(device, steps, warmup, joint=False):
+    """The network's forward pass on one 1080p 4:2:0 image, CUDA events:
+    (ms, TFLOP/s, FLOP). Per component: luma 1920x1088, then both chroma
+    planes of 960x544 as a batch of two; joint: one pass over the luma's
+    level-0 grid predicting all three components (the joint 4:2:0 network)."""
     import torch
 
     from artefact_b200 import synth
@@ -653,6 +654,28 @@ def time_network(device, steps, warmup):
     from artefact_b200.api import Jpeg, JpegSource
 
     j = Jpeg.from_source(JpegSource.Buffer(synth.make_jpeg(1920, 1080, 50, "4:2:0", False, seed=5050)))
+    if joint:
+        net = WS.WarmStartNet.load(WS.DEFAULT_JOINT_WEIGHTS, device)
+        cy = torch.from_numpy(WS.coef_image(j.coefs[0])[None]).cuda()
+        cc = torch.from_numpy(np.stack([WS.coef_image(co) for co in j.coefs[1:]])[None]).cuda()
+        qy = torch.from_numpy(np.asarray(j.coefs[0].quant_table, np.float32)[None].copy()).cuda()
+        qc = torch.from_numpy(np.stack([np.asarray(co.quant_table, np.float32) for co in j.coefs[1:]])[None]).cuda()
+        flops = network_flops(cy.shape[1], cy.shape[2])
+        out = net.predict_joint(cy, cc, qy, qc)
+        for _ in range(warmup):
+            net.predict_joint(cy, cc, qy, qc, out=out)
+        torch.cuda.synchronize()
+        ms = []
+        for _ in range(steps):
+            a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            a.record()
+            net.predict_joint(cy, cc, qy, qc, out=out)
+            b.record()
+            b.synchronize()
+            ms.append(a.elapsed_time(b))
+        net.close()
+        t = statistics.median(ms)
+        return t, flops / (t * 1e-3) / 1e12, flops
     net = WS.WarmStartNet.load(device=device) if WS.DEFAULT_WEIGHTS.exists() else WS.WarmStartNet(device=device)
     groups = [[j.coefs[0]], j.coefs[1:]]
     inputs = []
@@ -681,6 +704,12 @@ def time_network(device, steps, warmup):
     return t, flops / (t * 1e-3) / 1e12, flops
 
 
+def WS_joint_weights_exist():
+    from artefact_b200 import warmstart as WS
+
+    return WS.DEFAULT_JOINT_WEIGHTS.exists()
+
+
 def run_learned(args, lib, local, rank, world, dist):
     """Config 5: learned warm start + the fewest refinement iterations that reach
     the plain 50-iteration objective, against the plain 50-iteration solve (the
@@ -694,7 +723,8 @@ def run_learned(args, lib, local, rank, world, dist):
         if rank == 0:
             print(json.dumps({"metric": wl["metric"], "unavailable": "no trained warm-start weights in the package"}))
         return
-    net_ms, net_tflops, net_flops = time_network(local, args.steps, args.warmup)
+    net_ms, net_tflops, net_flops = time_network(local, args.steps, args.warmup,
+                                                 joint=WS_joint_weights_exist())
     peaks = json.loads((ROOT / "MEASURED_PEAKS.json").read_text()) if (ROOT / "MEASURED_PEAKS.json").exists() else {}
     tc_peak = float(peaks.get("bf16_tflops", 1590.0))
     # The headline: each image solved to the plain 50-iteration objective
@@ -1139,6 +1169,12 @@ def main():
                        "reach_infeasibility": [r["min_refine_infeasibility"] for r in rows],
                        "decoded_start_same_iterations_E_rel": [r["min_refine_decoded_same_schedule_E_rel"] for r in rows],
                        "images": rows}
+            nms, ntf, nfl = time_network(local, 10, 3, joint=WS_joint_weights_exist())
+            pk = json.loads((ROOT / "MEASURED_PEAKS.json").read_text()) if (ROOT / "MEASURED_PEAKS.json").exists() else {}
+            peak_tc = float(pk.get("bf16_tflops", 1590.0))
+            learned["network_forward"] = {"ms": nms, "tflops": ntf, "gflop": nfl / 1e9, "frac_of_bf16_peak": ntf / peak_tc,
+                                          "peak_kind": "measured" if "bf16_tflops" in pk else "fallback",
+                                          "network": "joint 4:2:0" if WS_joint_weights_exist() else "per component"}
 
     # Host decode overlapped with solving (batch workload, one GPU).
     pipe = None
