@@ -861,7 +861,8 @@ __global__ void __launch_bounds__(SWEEP_WARPS_Q * 32, SWEEP_MIN_BLOCKS_Q) k_grad
 // g = lane / 8 takes block first + g and lane j = lane % 8 its component
 // column j (SH full-resolution columns). The separable 1-D
 // transforms run on columns or rows of the block, switching with 8x8
-// transposes in shared memory, in the reference's order (columns first).
+// transposes in shared memory: the DCT in the reference's order (columns
+// first), the IDCTs rows first (one transpose each).
 template <int SH, int SV>
 struct ProjShape {
     static constexpr int NR = 8 * SV;       // rows of the region
@@ -965,18 +966,18 @@ __global__ void __launch_bounds__(PW * 32) k_project(const ImgDev *__restrict__ 
         m[u] = cl;
         d[u] = (cl - co[u] * qv[u]) * iq[u];
     }
-    // IDCT of the clamped coefficients and of d, columns then rows (idct8x8s),
-    // then back to this lane's column.
-    transpose8(T0, j, m);
-    if (ap != 0.f) transpose8(T1, j, d);
+    // IDCT of the clamped coefficients and of d: the row pass on the
+    // coefficient row this lane holds, one transpose to this lane's column,
+    // then the column pass. The reference runs columns first (idct8x8s); the
+    // two orders are the same transform and differ only in float rounding,
+    // and this one needs one transpose per plane instead of three (the
+    // transposes' shared-memory traffic bounds this kernel).
     idct8(m);
     if (ap != 0.f) idct8(d);
     transpose8(T0, j, m);
     if (ap != 0.f) transpose8(T1, j, d);
     idct8(m);
     if (ap != 0.f) idct8(d);
-    transpose8(T0, j, m);
-    if (ap != 0.f) transpose8(T1, j, d);
     cp_async_wait_all();
     __syncwarp();
     if (!act) return;

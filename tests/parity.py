@@ -7,8 +7,9 @@ error of both against the oracle's fp64 twin is measured on every case. Where
 the input is ill-conditioned (the oracle's own fp32 result more than 0.5 from
 its fp64 twin, or its objective more than 2.5e-5 relative) the bar becomes the
 spread of the oracle's own numerical variants around its fp64 result: fp32,
-and fp32/fp64 with the lagged DCT coefficients recomputed from x_k (equal in
-exact arithmetic). The GPU must lie within 2x that spread + 0.5 pixel units,
+fp32/fp64 with the lagged DCT coefficients recomputed from x_k, and fp32 with
+the projection's IDCTs run rows first (as the GPU runs them) -- each equal in
+exact arithmetic. The GPU must lie within 2x that spread + 0.5 pixel units,
 and its objective within 2x + 1e-4.
 """
 import numpy as np
@@ -45,8 +46,8 @@ class OracleRef:
         self.well = self.d_ref64 <= 0.5 and self.rel_ref64 <= 2.5e-5
         self.spread_d, self.spread_e = self.d_ref64, self.rel_ref64
         if not self.well:
-            for fp64 in (False, True):
-                v = O.compute(n, j.coefs, weight, pweight, iterations, W, H, init_mode=2, fp64=fp64)
+            for mode, fp64 in ((2, False), (2, True), (4, False), (6, False)):
+                v = O.compute(n, j.coefs, weight, pweight, iterations, W, H, init_mode=mode, fp64=fp64)
                 self.spread_d = max(self.spread_d, _maxdiff(v, self.r64))
                 self.spread_e = max(self.spread_e, abs(O.objective(*self.args, W, H, v) - self.e64) / abs(self.e64))
 
