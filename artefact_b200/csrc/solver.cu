@@ -929,8 +929,9 @@ __global__ void __launch_bounds__(PW * 32) k_project(const ImgDev *__restrict__ 
     cp_async_wait_all();
     __syncwarp();
 
-    // x' = y - sigma g (kept in the y region); cell means for subsampled
-    // components, summed sample by sample (compute_projection.rs:18-32).
+    // x' = y - sigma g (kept in the y region for a subsampled component, whose
+    // residual needs it); cell means for subsampled components, summed sample
+    // by sample (compute_projection.rs:18-32).
     const int cb = (grp * 8 + j) * SH;  // first region column of this lane
     float m[8], mean[8];
 #pragma unroll
@@ -942,7 +943,7 @@ __global__ void __launch_bounds__(PW * 32) k_project(const ImgDev *__restrict__ 
             for (int sx = 0; sx < SH; sx++) {
                 const int so = (k * SV + sy) * RS + cb + sx;
                 const float v = stepped ? fmaf(-sg, sg_[so], sy_[so]) : sy_[so];
-                sy_[so] = v;
+                if (SUB) sy_[so] = v;  // read back for the residual of a subsampled component
                 acc += v;
             }
         mean[k] = SUB ? acc / (float)(SH * SV) : acc;
