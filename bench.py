@@ -81,7 +81,8 @@ WORKLOADS = {
                            "iterations that reach it, 1080p 4:2:0 q30/50/75)", iterations=8),
 }
 WORKLOADS["network"] = dict(
-    name="warm-start network forward on one 1920x1080 4:2:0 JPEG (luma 1920x1088, chroma 2 x 960x544)",
+    name="warm-start network forward on one 1920x1080 4:2:0 JPEG (joint 4:2:0 pass over the luma's 960x544 level 0; "
+         "per component: luma 1920x1088, chroma 2 x 960x544)",
     metric="TFLOP/s (warm-start network forward, 1080p 4:2:0)", iterations=0)
 LEARNED_QUALITIES = (30, 50, 75)
 REFINE_ITERATIONS = 8
@@ -945,7 +946,11 @@ def main():
         run_learned(args, lib, local, rank, world, dist)
         return
     if args.workload == "network":
-        ms, tflops, flops = time_network(local, args.steps, args.warmup)
+        # The network the learned start uses on this workload's 4:2:0 image:
+        # the joint one when it ships, with the per-component passes beside it.
+        joint = WS_joint_weights_exist()
+        ms, tflops, flops = time_network(local, args.steps, args.warmup, joint=joint)
+        other = time_network(local, args.steps, args.warmup, joint=False) if joint else None
         if rank == 0:
             peaks = json.loads((ROOT / "MEASURED_PEAKS.json").read_text()) if (ROOT / "MEASURED_PEAKS.json").exists() else {}
             peak = float(peaks.get("bf16_tflops", 1590.0))
@@ -956,7 +961,10 @@ def main():
                               "roofline": {"bound": "tensor", "achieved": tflops, "peak": peak, "unit": "TFLOP/s",
                                            "frac": tflops / peak, "traffic": None,
                                            "peak_kind": "measured" if peaks else "fallback",
-                                           "algorithmic_flops_per_launch": flops, "launch_ms": ms}}), flush=True)
+                                           "algorithmic_flops_per_launch": flops, "launch_ms": ms},
+                              "network": "joint 4:2:0" if joint else "per component",
+                              "per_component_forward": ({"ms": other[0], "tflops": other[1], "gflop": other[2] / 1e9}
+                                                        if other else None)}), flush=True)
         return
     iters = wl["iterations"]
     encoded = []
