@@ -152,8 +152,10 @@ def test_joint_learned_batch_matches_single_learned_solves(gpu):
         for j, got in zip(jpegs, batch):
             W, H, _ = j.max_rounded()
             single = ctx.compute(j.nchannel, j.coefs, 0.3, [0.001] * 3, 8, W, H, init_mode=N.ART_INIT_LEARNED, **sched)
+            # The same network passes (one image per group, same activation set
+            # choice), kernels and strips as a solve of the image alone.
             d = max(float(np.abs(a - b).max()) for a, b in zip(got, single))
-            assert d <= 1e-2, (j.real_px_w, j.real_px_h, d)
+            assert all(np.array_equal(a, b) for a, b in zip(got, single)), (j.real_px_w, j.real_px_h, d)
             assert O.feasibility(j.nchannel, j.coefs, W, H, got) <= 1e-3
         ctx.set_joint_warm_start(None)
         ctx.set_warm_start(None)
@@ -178,8 +180,10 @@ def test_learned_batch_matches_single_learned_solves(gpu):
         for j, got in zip(jpegs, batch):
             W, H, _ = j.max_rounded()
             single = ctx.compute(j.nchannel, j.coefs, 0.3, [0.001] * 3, 8, W, H, init_mode=N.ART_INIT_LEARNED, **sched)
+            # The same network passes (one image per group, same activation set
+            # choice), kernels and strips as a solve of the image alone.
             d = max(float(np.abs(a - b).max()) for a, b in zip(got, single))
-            assert d <= 1e-2, (j.real_px_w, j.real_px_h, d)
+            assert all(np.array_equal(a, b) for a, b in zip(got, single)), (j.real_px_w, j.real_px_h, d)
             ev = O.feasibility(j.nchannel, j.coefs, W, H, got)
             assert ev <= 1e-3
         ctx.set_warm_start(None)
