@@ -152,8 +152,8 @@ def test_joint_learned_batch_matches_single_learned_solves(gpu):
         for j, got in zip(jpegs, batch):
             W, H, _ = j.max_rounded()
             single = ctx.compute(j.nchannel, j.coefs, 0.3, [0.001] * 3, 8, W, H, init_mode=N.ART_INIT_LEARNED, **sched)
-            # The same network passes (one image per group, same activation set
-            # choice), kernels and strips as a solve of the image alone.
+            # The same network passes (per image or component group), kernels and
+            # strips as a solve of the image alone.
             d = max(float(np.abs(a - b).max()) for a, b in zip(got, single))
             assert all(np.array_equal(a, b) for a, b in zip(got, single)), (j.real_px_w, j.real_px_h, d)
             assert O.feasibility(j.nchannel, j.coefs, W, H, got) <= 1e-3
@@ -180,8 +180,8 @@ def test_learned_batch_matches_single_learned_solves(gpu):
         for j, got in zip(jpegs, batch):
             W, H, _ = j.max_rounded()
             single = ctx.compute(j.nchannel, j.coefs, 0.3, [0.001] * 3, 8, W, H, init_mode=N.ART_INIT_LEARNED, **sched)
-            # The same network passes (one image per group, same activation set
-            # choice), kernels and strips as a solve of the image alone.
+            # The same network passes (per image or component group), kernels and
+            # strips as a solve of the image alone.
             d = max(float(np.abs(a - b).max()) for a, b in zip(got, single))
             assert all(np.array_equal(a, b) for a, b in zip(got, single)), (j.real_px_w, j.real_px_h, d)
             ev = O.feasibility(j.nchannel, j.coefs, W, H, got)
