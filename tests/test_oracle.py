@@ -139,3 +139,23 @@ def test_compute_from_step_decay():
     assert all(np.array_equal(x, y) for x, y in zip(a, b))
     assert any(not np.array_equal(x, y) for x, y in zip(a, c))
     assert O.feasibility(3, j.coefs, W, H, c) <= 1e-3
+
+
+def test_rows_first_idct_variant_is_a_rounding_variant():
+    """Mode bit 2 (the projection's IDCTs rows first, as the GPU runs them) is
+    the same iteration up to fp32 rounding: its result stays within the
+    reference-order fp32 result's own distance from fp64, and in fp64 the two
+    orders agree to rounding."""
+    from artefact_b200 import synth
+
+    j = Jpeg.from_source(JpegSource.Buffer(synth.make_jpeg(64, 48, 75, "4:2:0", False, seed=11)))
+    W, H, _ = j.max_rounded()
+    args = (3, j.coefs, 0.3, [0.001] * 3, 6, W, H)
+    ref = O.compute(*args)
+    rows = O.compute(*args, init_mode=4)
+    r64 = O.compute(*args, fp64=True)
+    r64_rows = O.compute(*args, init_mode=4, fp64=True)
+    d = max(float(np.abs(a.astype(np.float64) - b).max()) for a, b in zip(ref, rows))
+    spread = max(float(np.abs(a.astype(np.float64) - b).max()) for a, b in zip(ref, r64))
+    assert 0 < d <= max(4 * spread, 1e-3)
+    assert max(float(np.abs(a - b).max()) for a, b in zip(r64, r64_rows)) < 1e-9
