@@ -1560,13 +1560,14 @@ std::string batch_tune_key(int nimg, long long batch_px)
 // overrides (ART_SWEEP_KIND, ART_STRIP_ROWS, ART_PROJ_WARPS), the candidate
 // the autotuner is timing, the autotuner's choice for the batch's bucket
 // (several images) or the image's bucket (one image), else by size -- the
-// wide packed sweep once the batch has enough pixels to fill every SM with its
-// fewer, wider strips, strips as tall as that allows (the 3 extra rows a strip
-// reads stay small), and 4 projection warps per block.
+// narrow sweep (with its packed channel pair it is the fastest variant from
+// 1080p to 6000x4000 and on the 256-image batch), strips as tall as still
+// give every SM a dozen warps (the 3 extra rows a strip reads stay small), and
+// 4 projection warps per block.
 TuneChoice pick_shape(const ArtContext *ctx, const ImageSpec &sp, long long batch_px, int nimg)
 {
     TuneChoice t;
-    t.kind = batch_px >= 8LL * 1024 * 1024 ? 1 : 0;
+    t.kind = 0;
     if (ctx->strip_rows_override > 0) {
         t.kind = ctx->sweep_kind_override;
         t.rows = ctx->strip_rows_override;
